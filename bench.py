@@ -1,0 +1,377 @@
+"""Benchmark of the CNRK2 step (ChannelFlow.jl step!, rotational form) on B200.
+
+    python bench.py [--gpus N --steps K --warmup W --config c3 --impl engine|reference]
+
+Workload (default, config "c3"): Re_tau~590-sized Poiseuille at constant bulk
+flux, grid 384x257x384, Lx=2pi, Lz=pi, Re_bulk=10900, dt=0.002, seeded
+synthetic divergence-free initial state (amplitude 0.1, spectrum
+(1+k^2+l^2)^-1 0.8^n), plain FP64.  One "step" is one full three-stage CNRK2
+step.  The state (U, P, Q and the nonlinear work fields, >=3.9 GB) is far
+larger than the 126 MB L2, so no flush is needed between steps.
+
+The JSON line carries: value (steps/s, device-resident state, CUDA-graph step,
+timed with CUDA events on the engine stream, max over ranks), e2e (the same
+metric through the host-buffer C-ABI path: state upload, step, state download
+per step from pinned memory), roofline of the dominant kernel (algorithmic
+bytes from the fixed byte model / event-timed kernel time), the CPU baseline
+(the oracle port on this host's cores, a bounded sample of one CNRK2 stage),
+clocks sampled during the timed region, and the kernel-launch count.
+
+N > 1 (torchrun): independent replicas, one per GPU, no data-path collective
+(a single channel does not shard; the ensemble of replicas does).
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "channelflow.jl_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+CONFIGS = {
+    # plain FP64 Couette, Re=400 (c1 of the headline set)
+    "c1": dict(Nx=32, Ny=33, Nz=32, Lx=2 * math.pi / 1.14, Lz=2 * math.pi / 2.5, nu=1 / 400, dt=0.01,
+               profile="couette", constraint=None, amp=0.1, shape=0, rho=0.8),
+    # FP64 Poiseuille at constant flux, Re_bulk=2800
+    "c2": dict(Nx=128, Ny=129, Nz=128, Lx=4 * math.pi, Lz=4 * math.pi / 3, nu=(2 / 3) / 2800, dt=0.005,
+               profile="poiseuille", constraint=(2 / 3, 0.0), amp=0.2, shape=1, rho=0.7),
+    # Re_tau~590-sized Poiseuille at constant flux, Re_bulk=10900 (headline grid)
+    "c3": dict(Nx=384, Ny=257, Nz=384, Lx=2 * math.pi, Lz=math.pi, nu=(2 / 3) / 10900, dt=0.002,
+               profile="poiseuille", constraint=(2 / 3, 0.0), amp=0.1, shape=1, rho=0.8),
+    # large grid 512x385x512 (plain FP64 here)
+    "c5": dict(Nx=512, Ny=385, Nz=512, Lx=2 * math.pi, Lz=math.pi, nu=(2 / 3) / 10900, dt=0.0015,
+               profile="poiseuille", constraint=(2 / 3, 0.0), amp=0.1, shape=1, rho=0.8),
+}
+METRIC = "steps/s @384x257x384: mixed vs FP64 plain (<=1e-9 rel err); ensemble agg steps/s"
+
+
+def sizes(cfg):
+    Nxh = cfg["Nx"] // 2 + 1
+    Nzp = (3 * cfg["Nz"] + 1) // 2
+    Nr = Nxh * cfg["Nz"] * cfg["Ny"]
+    Nq = Nxh * Nzp * cfg["Ny"]
+    return Nr, Nq
+
+
+def model_bytes(cfg, s_nl=16):
+    """Algorithmic bytes per kernel launch (fixed byte model of the step).
+
+    per stage: 16*19*Nr (U, P, Q read/write 14; responses and factors 5)
+               + s_nl*(18*Nr + 18*Nq) (N read 3, nodes written 6, z-inverse
+               6->6, x-pass 6->3, z-forward 3->3)
+    """
+    Nr, Nq = sizes(cfg)
+    return {
+        "zinv": s_nl * (6 * Nr + 6 * Nq),
+        "xpass": s_nl * (9 * Nq),
+        "zfwd": s_nl * (3 * Nq + 3 * Nr),
+        "column": 16 * 19 * Nr + s_nl * 9 * Nr,
+    }
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def traffic_from_profiles(kernel, cfg_name):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        d = json.load(open(path))
+        return d[cfg_name][kernel]
+    except Exception:
+        return None
+
+
+# CPU sample size: each timed CPU "step" runs 1/SAMPLE_DIV of every independent
+# loop of one CNRK2 stage (columns, y-planes, rows, points) of the full grid.
+SAMPLE_DIV = {"c1": 1, "c2": 1, "c3": 16, "c5": 48}
+
+
+def make_oracle(cfg):
+    from oracle import oracle as O
+
+    c = cfg
+    if c["profile"] == "couette":
+        return O.couette(c["Nx"], c["Ny"], c["Nz"], c["Lx"], c["Lz"], c["nu"], c["dt"])
+    return O.poiseuille(c["Nx"], c["Ny"], c["Nz"], c["Lx"], c["Lz"], c["nu"], c["dt"], bulkvelocity=c["constraint"])
+
+
+def cpu_baseline(cfg, threads, div):
+    """Oracle port timed on this host: 1/div of one CNRK2 stage of the full workload."""
+    from oracle import oracle as O
+
+    O.set_threads(threads)
+    O.set_helmholtz_method("quasitri")
+    c = cfg
+    pb = make_oracle(cfg)
+    U = pb.synth(seed=1, amp=c["amp"], shape=c["shape"], rho=c["rho"])
+    P = pb.zeros()
+    pb.prepare()
+    O.set_sample_div(div)
+    pb.stage(U, P, 0)
+    t0 = time.perf_counter()
+    pb.stage(U, P, 1)
+    dt = time.perf_counter() - t0
+    O.set_sample_div(1)
+    return dt * div
+
+
+def run_reference(args, cfg, rank):
+    """--impl reference: the oracle port (the reference's algorithm restated on
+    the CPU) on this host's cores; each step is a bounded sample of one CNRK2
+    stage of the full workload; steps/s = 1 / (3 x stage time)."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    from oracle import oracle as O
+
+    O.set_threads(threads)
+    O.set_helmholtz_method("quasitri")
+    c = cfg
+    div = SAMPLE_DIV[args.config]
+    pb = make_oracle(cfg)
+    U = pb.synth(seed=1, amp=c["amp"], shape=c["shape"], rho=c["rho"])
+    P = pb.zeros()
+    pb.prepare()
+    O.set_sample_div(div)
+    for w in range(args.warmup):
+        pb.stage(U, P, w % 3)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        pb.stage(U, P, s % 3)
+    el = time.perf_counter() - t0
+    O.set_sample_div(1)
+    stage_s = div * el / max(args.steps, 1)
+    value = 1.0 / (3 * stage_s)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3 * stage_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.config, **workload_desc(cfg)},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
+                         "sample": f"each timed step runs 1/{div} of every independent loop of one CNRK2 stage of the "
+                                   f"full grid; steps/s = 1/(3 x {div} x sample time)"},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_desc(cfg):
+    return {"grid": [cfg["Nx"], cfg["Ny"], cfg["Nz"]], "Lx": cfg["Lx"], "Lz": cfg["Lz"], "nu": cfg["nu"],
+            "dt": cfg["dt"], "profile": cfg["profile"],
+            "constraint": ("bulkvelocity" if cfg["constraint"] else "pressuregradient(0,0)"),
+            "form": "rotational", "precision": "fp64 plain",
+            "l2": "state larger than L2 (no flush needed)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, cfg, rank)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import cfb200
+
+    g = cfb200.Grid(cfg["Nx"], cfg["Ny"], cfg["Nz"], cfg["Lx"], cfg["Lz"])
+    if cfg["profile"] == "couette":
+        pb = cfb200.CouetteFlow(g, cfg["nu"], cfg["dt"])
+    else:
+        pb = cfb200.PoiseuilleFlow(g, cfg["nu"], cfg["dt"], bulkvelocity=cfg["constraint"])
+    cfb200.lib().cf_random_state(pb.handle, 1000 + rank, cfg["amp"], cfg["shape"], cfg["rho"])
+    stream = torch.cuda.ExternalStream(pb.stream_ptr())
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (CUDA-graph step)
+    t = 0.0
+    t, _ = pb.advance(t, args.warmup)
+    pb.sync()
+
+    # ---- timed region: device-resident state, graph-launched steps
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    t, _ = pb.advance(t, args.steps)
+    launches = pb.launches()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(ms)
+    barrier()
+    ms_per_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+
+    # ---- per-kernel event timing over the same steps (roofline)
+    t, kms = pb.advance_profiled(t, args.steps)
+    launches_per_kernel = 3 * args.steps
+    kavg = {"zinv": kms[0] / launches_per_kernel, "xpass": kms[1] / launches_per_kernel,
+            "zfwd": kms[2] / launches_per_kernel, "column": kms[3] / launches_per_kernel}
+    mb = model_bytes(cfg)
+    dom = max(kavg, key=kavg.get)
+    peak, peak_kind = peaks()
+    achieved = mb[dom] / (kavg[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": {"zinv": "k_zinv", "xpass": "k_xpass", "zfwd": "k_zfwd",
+                                           "column": "k_column_stage"}[dom],
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind, "traffic": traffic_from_profiles(dom, args.config),
+                "algorithmic_bytes_per_launch": mb[dom],
+                "kernel_ms_per_launch": kavg,
+                "step_model_bytes": 3 * sum(mb.values()),
+                "step_model_frac": 3 * sum(mb.values()) / (ms_per_step * 1e-3) / 1e9 / peak}
+
+    # ---- end to end through the host-buffer C ABI (upload, step, download)
+    U_h = torch.empty((3,) + g.spectralsize + (2,), dtype=torch.float64, pin_memory=True).numpy()
+    P_h = torch.empty(g.spectralsize + (2,), dtype=torch.float64, pin_memory=True).numpy()
+    Uc, Pc = pb.get_state()
+    U_h[...] = Uc.view(np.float64).reshape(U_h.shape)
+    P_h[...] = Pc.view(np.float64).reshape(P_h.shape)
+    Uv = U_h.view(np.complex128).reshape((3,) + g.spectralsize)
+    Pv = P_h.view(np.complex128).reshape(g.spectralsize)
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        t = cfb200.step_(pb, Uv, Pv, t, 1)
+    f1.record(stream)
+    f1.synchronize()
+    ems = max_over_ranks(f0.elapsed_time(f1))
+    e2e_value = world * args.steps / (ems / 1e3)
+    Nr, _ = sizes(cfg)
+    state_bytes = 4 * 16 * Nr
+
+    diag = pb.diagnostics()
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.config, **workload_desc(cfg), "parallelism": f"replicas x{world}"},
+        "grid_point_steps_per_s": value * cfg["Nx"] * cfg["Ny"] * cfg["Nz"],
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes},
+        "roofline": roofline,
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "diagnostics": {"kinetic_energy": diag[0], "dissipation": diag[1], "max_div": diag[2]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        div = SAMPLE_DIV[args.config]
+        stage_s = cpu_baseline(cfg, threads, div)
+        line["cpu_baseline"] = {"value": 1.0 / (3 * stage_s), "unit": "steps/s", "cores": threads, "kind": "port",
+                                "sample": f"1/{div} of every independent loop of one CNRK2 stage of the full grid "
+                                          f"on the oracle; steps/s = 1/(3 x {div} x sample time)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    pb.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,298 @@
+"""cfb200 -- B200-native CNRK2 engine for ChannelFlow.jl's time step.
+
+Host-side mirror of the reference's Julia API for this path (ChannelFlow.jl
+src/grids.jl, src/problem.jl, src/initialization.jl, src/timesteppers/cnrk2.jl),
+bound to the C ABI of ``libcfb200.so`` (include/cfb200.h) with ctypes.  The
+compute runs only in the CUDA library: importing works without a GPU, but every
+operation that needs the engine raises if the library or the device is
+missing -- there is no CPU fallback.
+
+Arrays follow the reference storage: a spectral field is complex128 of shape
+``(Ny, Nz, Nx//2+1)`` in C order (Julia's ``(Nx/2+1, Nz, Ny)`` column-major
+with k fastest); a velocity is ``(3, Ny, Nz, Nx//2+1)``.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcfb200.so")
+_lib = None
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+class CFError(RuntimeError):
+    """Error returned by the engine (the reference raises ArgumentError/DimensionMismatch)."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"cfb200 error {code}: {msg}")
+        self.code = code
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int),
+                ("Lx", ctypes.c_double), ("Lz", ctypes.c_double),
+                ("nu", ctypes.c_double), ("dt", ctypes.c_double),
+                ("profile", ctypes.c_int), ("base_values", _D),
+                ("constraint", ctypes.c_int), ("c1", ctypes.c_double), ("c2", ctypes.c_double)]
+
+
+EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_get_state",
+           "cf_set_state_device", "cf_get_state_device", "cf_step", "cf_nonlinear", "cf_project",
+           "cf_pressure", "cf_random_state", "cf_diagnostics", "cf_sync", "cf_last_launch_count",
+           "cf_stream", "cf_last_error", "cf_step_profiled"]
+
+
+def lib():
+    """Load libcfb200.so (fails loudly when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+                               "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.cf_last_error.restype = ctypes.c_char_p
+        L.cf_create.argtypes = [ctypes.POINTER(_Config), ctypes.POINTER(ctypes.c_void_p)]
+        L.cf_destroy.argtypes = [ctypes.c_void_p]
+        L.cf_destroy.restype = None
+        L.cf_set_constraint.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.cf_set_state.argtypes = [ctypes.c_void_p, _D, _D]
+        L.cf_get_state.argtypes = [ctypes.c_void_p, _D, _D]
+        L.cf_set_state_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.cf_get_state_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.cf_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _D, _D]
+        L.cf_nonlinear.argtypes = [ctypes.c_void_p, _D, _D]
+        L.cf_project.argtypes = [ctypes.c_void_p, _D]
+        L.cf_pressure.argtypes = [ctypes.c_void_p, _D, _D]
+        L.cf_random_state.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_double, ctypes.c_int,
+                                      ctypes.c_double]
+        L.cf_diagnostics.argtypes = [ctypes.c_void_p, _D]
+        L.cf_step_profiled.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _D, _D]
+        L.cf_sync.argtypes = [ctypes.c_void_p]
+        L.cf_last_launch_count.argtypes = [ctypes.c_void_p]
+        L.cf_stream.argtypes = [ctypes.c_void_p]
+        L.cf_stream.restype = ctypes.c_void_p
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise CFError(rc, lib().cf_last_error().decode())
+
+
+def _ptr(a):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_D)
+
+
+class Grid:
+    """Grid(Nx, Ny, Nz, Lx, Lz) (src/grids.jl:27-30): Lobatto y, upper wall first."""
+
+    def __init__(self, Nx, Ny, Nz, Lx, Lz):
+        self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)
+        self.Lx, self.Lz = float(Lx), float(Lz)
+        n = np.arange(self.Ny)
+        self.y = np.cos(np.pi * n / (self.Ny - 1))
+        self.y[2 * n == self.Ny - 1] = 0.0
+
+    @property
+    def spectralsize(self):
+        return (self.Ny, self.Nz, self.Nx // 2 + 1)
+
+    def physicalsize(self, padded=True):
+        if padded:
+            return (self.Ny, (3 * self.Nz + 1) // 2, (3 * self.Nx + 1) // 2)
+        return (self.Ny, self.Nz, self.Nx)
+
+    def __eq__(self, other):
+        return isinstance(other, Grid) and (self.Nx, self.Ny, self.Nz, self.Lx, self.Lz) == (
+            other.Nx, other.Ny, other.Nz, other.Lx, other.Lz)
+
+    def __repr__(self):
+        return f"Grid({self.Nx}, {self.Ny}, {self.Nz}, {self.Lx}, {self.Lz})"
+
+
+class State:
+    """State(U, P) (src/state.jl:18-34): perturbation velocity and stage pressure."""
+
+    def __init__(self, U, P):
+        self.U = U
+        self.P = P
+
+    def velocity(self):
+        return self.U
+
+    def stagepressure(self):
+        return self.P
+
+    def copy(self):
+        return State(self.U.copy(), self.P.copy())
+
+
+def zero_state(grid):
+    """zero_state(grid) (src/initialization.jl:160)."""
+    return State(np.zeros((3,) + grid.spectralsize, np.complex128), np.zeros(grid.spectralsize, np.complex128))
+
+
+class ChannelFlowProblem:
+    """ChannelFlowProblem(grid, profile, nu, dt; pressuregradient | bulkvelocity)
+    (src/problem.jl:69-107) with the rotational form and NoForcing, on the B200.
+
+    ``profile`` is "couette", "poiseuille" or a callable Ub(y).
+    """
+
+    def __init__(self, grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None, forcing=None, form=None):
+        if pressuregradient is not None and bulkvelocity is not None:
+            raise ValueError("specify either pressuregradient or bulkvelocity")
+        if forcing is not None:
+            raise ValueError("only NoForcing is accelerated by the engine")
+        if form not in (None, "rotational"):
+            raise ValueError("only the rotational nonlinear form is accelerated by the engine")
+        self.grid = grid
+        self.nu, self.dt = float(nu), float(dt)
+        if bulkvelocity is not None:
+            self.constraint = ("bulkvelocity", tuple(float(v) for v in bulkvelocity))
+        else:
+            pg = (0.0, 0.0) if pressuregradient is None else pressuregradient
+            self.constraint = ("pressuregradient", tuple(float(v) for v in pg))
+        kind = 1 if self.constraint[0] == "bulkvelocity" else 0
+        cfg = _Config()
+        cfg.Nx, cfg.Ny, cfg.Nz = grid.Nx, grid.Ny, grid.Nz
+        cfg.Lx, cfg.Lz, cfg.nu, cfg.dt = grid.Lx, grid.Lz, self.nu, self.dt
+        self._base = None
+        if profile == "couette":
+            cfg.profile = 0
+        elif profile == "poiseuille":
+            cfg.profile = 1
+        else:
+            cfg.profile = 2
+            self._base = np.ascontiguousarray([float(profile(v)) for v in grid.y], dtype=np.float64)
+            cfg.base_values = _ptr(self._base)
+        cfg.constraint = kind
+        cfg.c1, cfg.c2 = self.constraint[1]
+        h = ctypes.c_void_p()
+        _check(lib().cf_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.cf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ------------------------------------------------ device-resident state
+    def set_state(self, U, P):
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        P = np.ascontiguousarray(P, dtype=np.complex128)
+        assert U.shape == (3,) + self.grid.spectralsize and P.shape == self.grid.spectralsize
+        _check(lib().cf_set_state(self._h, _ptr(U.view(np.float64)), _ptr(P.view(np.float64))))
+
+    def get_state(self):
+        U = np.zeros((3,) + self.grid.spectralsize, np.complex128)
+        P = np.zeros(self.grid.spectralsize, np.complex128)
+        _check(lib().cf_get_state(self._h, _ptr(U.view(np.float64)), _ptr(P.view(np.float64))))
+        return U, P
+
+    def advance(self, t, nsteps=1):
+        """Advance the engine-resident state nsteps steps; returns (t + nsteps*dt, last gradients)."""
+        tout = ctypes.c_double()
+        g = np.zeros(2)
+        _check(lib().cf_step(self._h, float(t), int(nsteps), ctypes.byref(tout), _ptr(g)))
+        return tout.value, tuple(g)
+
+    def advance_profiled(self, t, nsteps=1):
+        """As advance() without the graph; returns (t_out, ms per kernel class
+        [z-inverse, x-pass, z-forward, column] summed over the steps)."""
+        tout = ctypes.c_double()
+        ms = np.zeros(4)
+        _check(lib().cf_step_profiled(self._h, float(t), int(nsteps), ctypes.byref(tout), _ptr(ms)))
+        return tout.value, ms
+
+    def stream_ptr(self):
+        return lib().cf_stream(self._h)
+
+    def launches(self):
+        return lib().cf_last_launch_count(self._h)
+
+    def sync(self):
+        _check(lib().cf_sync(self._h))
+
+    # ------------------------------------------------ operators
+    def nonlinear(self, U):
+        """NonLinearTerm{RotatingForm}(t, U, N) (src/nonlinear.jl:173-193)."""
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        N = np.zeros_like(U)
+        _check(lib().cf_nonlinear(self._h, _ptr(U.view(np.float64)), _ptr(N.view(np.float64))))
+        return N
+
+    def diagnostics(self):
+        out = np.zeros(5)
+        _check(lib().cf_diagnostics(self._h, _ptr(out)))
+        return out
+
+
+def CouetteFlow(grid, nu, dt, **kw):
+    """CouetteFlow(grid, nu, dt) (src/problem.jl:122-123): Ub = y."""
+    return ChannelFlowProblem(grid, "couette", nu, dt, **kw)
+
+
+def PoiseuilleFlow(grid, nu, dt, bulkvelocity=None, pressuregradient=None, **kw):
+    """PoiseuilleFlow(grid, nu, dt) (src/problem.jl:137-144): Ub = 1 - y^2, default gradient (-2nu, 0)."""
+    if bulkvelocity is None and pressuregradient is None:
+        pressuregradient = (-2 * nu, 0.0)
+    return ChannelFlowProblem(grid, "poiseuille", nu, dt, bulkvelocity=bulkvelocity,
+                              pressuregradient=pressuregradient, **kw)
+
+
+def project_(U, problem):
+    """project!(U, problem) (src/pressure.jl:36-54); U updated in place and returned."""
+    assert U.dtype == np.complex128 and U.flags["C_CONTIGUOUS"]
+    _check(lib().cf_project(problem.handle, _ptr(U.view(np.float64))))
+    return U
+
+
+def pressure(U, problem):
+    """pressure(U, problem) (src/pressure.jl:95-104): modified pressure for the rotational form."""
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    P = np.zeros(problem.grid.spectralsize, np.complex128)
+    _check(lib().cf_pressure(problem.handle, _ptr(U.view(np.float64)), _ptr(P.view(np.float64))))
+    return P
+
+
+def random_state(problem, epsilon, seed=1, shape=0, rho=0.8):
+    """random_state(problem, epsilon) (src/initialization.jl:176-195) with a seeded
+    spectral generator: returns a host State and leaves it resident in the engine."""
+    if epsilon < 0:
+        raise ValueError("epsilon must be non-negative")
+    _check(lib().cf_random_state(problem.handle, int(seed), float(epsilon), int(shape), float(rho)))
+    U, P = problem.get_state()
+    return State(U, P)
+
+
+def step_(problem, U, P, t, nsteps=1):
+    """step!(scheme, nlterm, U, P, t; constraint...) (src/timesteppers/cnrk2.jl:567-625).
+
+    Host buffers U, P are advanced in place (upload, nsteps device steps,
+    download) and t + nsteps*dt is returned.
+    """
+    if U.shape != (3,) + problem.grid.spectralsize or P.shape != problem.grid.spectralsize:
+        raise ValueError("fields must have the resolved spectral size")
+    problem.set_state(U, P)
+    t2, _ = problem.advance(t, nsteps)
+    U2, P2 = problem.get_state()
+    U[...] = U2
+    P[...] = P2
+    return t2
+
+
+def kinetic_energy_of(problem):
+    return problem.diagnostics()[0]

@@ -1,0 +1,68 @@
+// cf_common.cuh -- shared device helpers for the CNRK2 engine (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define CF_DEV __device__ __forceinline__
+
+// ----------------------------------------------------------------- complex
+typedef double2 zd;
+
+CF_DEV zd zmake(double r, double i) { return make_double2(r, i); }
+CF_DEV zd zadd(zd a, zd b) { return make_double2(a.x + b.x, a.y + b.y); }
+CF_DEV zd zsub(zd a, zd b) { return make_double2(a.x - b.x, a.y - b.y); }
+CF_DEV zd zscale(zd a, double s) { return make_double2(a.x * s, a.y * s); }
+CF_DEV zd zmul(zd a, zd b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+CF_DEV zd zconj(zd a) { return make_double2(a.x, -a.y); }
+// i * a
+CF_DEV zd zmuli(zd a) { return make_double2(-a.y, a.x); }
+// s * i * a  (real s)
+CF_DEV zd zmulis(zd a, double s) { return make_double2(-a.y * s, a.x * s); }
+// a + s * b
+CF_DEV zd zaxpy(zd a, double s, zd b) { return make_double2(fma(s, b.x, a.x), fma(s, b.y, a.y)); }
+CF_DEV zd zzero() { return make_double2(0.0, 0.0); }
+
+// ------------------------------------------------------------- warp utils
+CF_DEV double shfl_up_d(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+CF_DEV double shfl_d(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+CF_DEV double shfl_xor_d(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+CF_DEV zd shfl_up_z(zd v, int d) { return make_double2(shfl_up_d(v.x, d), shfl_up_d(v.y, d)); }
+CF_DEV zd shfl_z(zd v, int src) { return make_double2(shfl_d(v.x, src), shfl_d(v.y, src)); }
+
+CF_DEV zd warp_sum_z(zd v) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) {
+        v.x += shfl_xor_d(v.x, m);
+        v.y += shfl_xor_d(v.y, m);
+    }
+    return v;
+}
+CF_DEV double warp_sum_d(double v) {
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) v += shfl_xor_d(v, m);
+    return v;
+}
+
+// Inclusive additive scan of complex values across the warp (lane order).
+CF_DEV zd warp_scan_z(zd v, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        zd o = shfl_up_z(v, d);
+        if (lane >= d) v = zadd(v, o);
+    }
+    return v;
+}
+
+// Inclusive scan of affine maps f_i(x) = G_i + M_i x under composition in
+// lane order: the result of lane j is f_j o ... o f_0.
+CF_DEV void warp_scan_affine(double& M, zd& G, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        double Mo = shfl_up_d(M, d);
+        zd Go = shfl_up_z(G, d);
+        if (lane >= d) {
+            G = zaxpy(G, M, Go);
+            M = M * Mo;
+        }
+    }
+}

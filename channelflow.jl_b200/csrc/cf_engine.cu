@@ -1,0 +1,966 @@
+// cf_engine.cu -- host side of the B200 CNRK2 engine: set-up of the Stokes
+// banks, transform plans, device buffers, the CUDA-graph step and the C ABI
+// declared in include/cfb200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/cfb200.h"
+#include "cf_fftkernels.cuh"
+#include "cf_kernels.cuh"
+
+#define CF_NCOL 4
+
+static thread_local std::string g_err;
+static int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+#define CU(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            return fail(e_ == cudaErrorMemoryAllocation ? CF_E_NOMEM : CF_E_CUDA,         \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
+        }                                                                                 \
+    } while (0)
+
+// ===========================================================================
+// Host numerics for the set-up (not timed): quasi-tridiagonal tau factors
+// ===========================================================================
+namespace setup {
+
+static double cmul(int m) { return m == 0 ? 2.0 : 1.0; }
+
+// Factors of the tau system rows 0..P-2 of (th0 D^2 - th1) a = f with wall
+// rows (Dirichlet weights 1, Neumann weights n^2).  Equation n >= 2 of each
+// parity (spectral integration of the tau rows):
+//   s_n a_{n-2} + d_n a_n + u_n a_{n+2} = g_n
+//   s_n = -c_{n-2} th1 / (4n(n-1)),  d_n = th0 + [n<=P-2] th1 / (2(n^2-1)),
+//   u_n = -[n+2<=P-2] th1 / (4n(n+1)).
+// Eliminated from the top: a_n = alpha_n a_{n-2} + beta_n.  W_n carries the
+// wall row: sum_n w_n a_n = SA a_par + sum_{n>=par+2} W_n beta_n.
+struct Helm {
+    int P;
+    double th0, th1;
+    bool neumann;
+    std::vector<double> alpha, invden, W;
+    double SA[2];
+    double w(int n) const { return neumann ? (double)n * n : 1.0; }
+    double eq_s(int n) const { return -cmul(n - 2) * th1 / (4.0 * n * (n - 1)); }
+    double eq_d(int n) const { return th0 + (n <= P - 2 ? th1 / (2.0 * ((double)n * n - 1.0)) : 0.0); }
+    double eq_u(int n) const { return (n + 2 <= P - 2) ? -th1 / (4.0 * n * (n + 1)) : 0.0; }
+    void init(int P_, double t0, double t1, bool neum) {
+        P = P_; th0 = t0; th1 = t1; neumann = neum;
+        alpha.assign(P + 1, 0.0); invden.assign(P + 1, 0.0); W.assign(P + 1, 0.0);
+        for (int par = 0; par < 2; ++par) {
+            const int top = ((P & 1) == par) ? P : P - 1;
+            double anext = 0.0;
+            for (int n = top; n >= par + 2; n -= 2) {
+                double den = eq_d(n) + eq_u(n) * anext;
+                invden[n] = 1.0 / den;
+                alpha[n] = -eq_s(n) / den;
+                anext = alpha[n];
+            }
+            double Wn = 0.0;
+            for (int n = top; n >= par + 2; n -= 2) {
+                Wn = (n == top) ? w(n) : w(n) + alpha[n + 2] * Wn;
+                W[n] = Wn;
+            }
+            SA[par] = w(par) + (top >= par + 2 ? alpha[par + 2] * W[par + 2] : 0.0);
+        }
+    }
+    // sequential solve (same algebra as the device scans)
+    void solve(const double* f, double bp, double bm, double* a) const {
+        double bc[2];
+        if (!neumann) { bc[0] = 0.5 * (bp + bm); bc[1] = 0.5 * (bp - bm); }
+        else { bc[0] = 0.5 * (bp - bm); bc[1] = 0.5 * (bp + bm); }
+        std::vector<double> beta(P + 3, 0.0);
+        for (int par = 0; par < 2; ++par) {
+            const int top = ((P & 1) == par) ? P : P - 1;
+            double bnext = 0.0, sw = 0.0;
+            for (int n = top; n >= par + 2; n -= 2) {
+                double g = cmul(n - 2) * f[n - 2] / (4.0 * n * (n - 1));
+                if (n <= P - 2) g -= f[n] / (2.0 * ((double)n * n - 1.0));
+                if (n + 2 <= P - 2) g += f[n + 2] / (4.0 * n * (n + 1));
+                beta[n] = (g - eq_u(n) * bnext) * invden[n];
+                bnext = beta[n];
+                sw += W[n] * beta[n];
+            }
+            double prev = (bc[par] - sw) / SA[par];
+            a[par] = prev;
+            for (int n = par + 2; n <= top; n += 2) {
+                prev = alpha[n] * prev + beta[n];
+                a[n] = prev;
+            }
+        }
+    }
+};
+
+static void diff(const double* a, double* b, int P) {
+    std::vector<double> t(P + 1);
+    t[P] = 0.0;
+    if (P >= 1) t[P - 1] = 2.0 * P * a[P];
+    for (int n = P - 2; n >= 0; --n) t[n] = t[n + 2] + 2.0 * (n + 1) * a[n + 1];
+    t[0] *= 0.5;
+    for (int n = 0; n <= P; ++n) b[n] = t[n];
+}
+static double wallderiv(const double* a, int P, bool right) {
+    double s = 0.0;
+    for (int n = 1; n <= P; ++n) {
+        double w = (double)n * n;
+        if (!right && (n % 2 == 0)) w = -w;
+        s += w * a[n];
+    }
+    return s;
+}
+static double bulkmean(const double* a, int P) {
+    double v = a[0];
+    for (int n = 2; n <= P; n += 2) v += a[n] / (1.0 - (double)n * n);
+    return v;
+}
+
+// Chebyshev coefficients of values at y_j = cos(pi j/P) (chebcoeffs): DCT-I
+// evaluated directly in long double, divided by P, endpoints halved.
+static void chebcoeffs(const double* vals, double* coef, int P) {
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k <= P; ++k) {
+        long double s = 0.5L * vals[0] + 0.5L * ((k % 2) ? -1.0L : 1.0L) * vals[P];
+        for (int n = 1; n < P; ++n) s += (long double)vals[n] * cosl(pi * (long double)((long long)n * k % (2 * P)) / P);
+        long double c = 2.0L * s / P;
+        if (k == 0 || k == P) c *= 0.5L;
+        coef[k] = (double)c;
+    }
+}
+
+template <class F>
+static void parallel_for(long n, F f) {
+    unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (n < 64) nt = 1;
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t)
+        th.emplace_back([=, &f] {
+            for (long i = (long)t; i < n; i += nt) f(i);
+        });
+    for (auto& x : th) x.join();
+}
+
+}  // namespace setup
+
+// ===========================================================================
+// Engine
+// ===========================================================================
+struct DevBank {
+    double *fac_p = nullptr, *fac_v = nullptr, *resp = nullptr, *colsc = nullptr, *sa = nullptr, *meanc = nullptr;
+    double meanc_mean = 0.0, nu = 0.0, lambda = 0.0;
+    bool ready = false;
+    BankDev view() const {
+        BankDev b;
+        b.fac_p = fac_p; b.fac_v = fac_v; b.resp = resp; b.colsc = colsc; b.sa = sa; b.meanc = meanc;
+        b.meanc_mean = meanc_mean;
+        return b;
+    }
+};
+
+struct cf_engine {
+    int Nx, Ny, Nz, Nxh, Nxp, Nzp, P;
+    long B, nr, nq;
+    double Lx, Lz, nu, dt;
+    int cmode;
+    double c1, c2;  // as given (total bulk targets when cmode == 1)
+    double basemean;
+    std::vector<double> base, basecurv;
+    int tkz;
+    // device
+    cudaStream_t stream = nullptr;
+    zd *U[3] = {}, *Pf = nullptr, *Q[3] = {}, *nod[6] = {}, *zp[6] = {};
+    zd *tmpU = nullptr, *tmpP = nullptr;
+    double *d_base = nullptr, *d_basecurv = nullptr, *d_grad = nullptr;
+    zd *d_twP = nullptr, *d_twZ = nullptr, *d_twX = nullptr, *d_cs = nullptr;
+    FftPlan plP, plZ, plX;
+    DevBank bank[3], proj, neum;
+    bool nodal_valid = false;
+    cudaGraphExec_t graph = nullptr;
+    int last_launches = 0;
+    std::vector<void*> allocs;
+};
+
+static const double CA[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+static const double CB[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+static const double CC[3] = {1.0 / 6.0, 5.0 / 24.0, 1.0 / 8.0};
+
+static int dalloc(cf_engine* h, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return fail(CF_E_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    h->allocs.push_back(*p);
+    return CF_OK;
+}
+
+static std::vector<int> fft_radices(int n) {
+    std::vector<int> r;
+    while (n % 8 == 0) { r.push_back(8); n /= 8; }
+    while (n % 4 == 0) { r.push_back(4); n /= 4; }
+    while (n % 2 == 0) { r.push_back(2); n /= 2; }
+    while (n % 3 == 0) { r.push_back(3); n /= 3; }
+    while (n % 5 == 0) { r.push_back(5); n /= 5; }
+    for (int p = 7; p <= n; p += 2)
+        while (n % p == 0) { r.push_back(p); n /= p; }
+    return r;
+}
+
+// per-pass register check: ceil(nb*L/R / nth) * R <= maxe
+static bool plan_fits(const std::vector<int>& rad, int L, int nb, int nth, int maxe) {
+    for (int R : rad) {
+        if (R > 31) return false;
+        long bf = (long)nb * (L / R);
+        long per = (bf + nth - 1) / nth;
+        if (per * R > maxe) return false;
+    }
+    return true;
+}
+
+static int make_plan(cf_engine* h, int L, FftPlan& pl, zd** dtw) {
+    std::vector<int> rad = fft_radices(L);
+    if (rad.size() > CF_FFT_MAXPASS) return fail(CF_E_UNSUPPORTED, "FFT length has too many factors");
+    pl.L = L;
+    pl.np = (int)rad.size();
+    for (int i = 0; i < pl.np; ++i) pl.R[i] = rad[i];
+    std::vector<zd> tw(L);
+    const long double twopi = 6.283185307179586476925286766559005768L;
+    for (int k = 0; k < L; ++k) {
+        long double a = -twopi * (long double)k / (long double)L;
+        tw[k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    int rc = dalloc(h, (void**)dtw, sizeof(zd) * L);
+    if (rc) return rc;
+    CU(cudaMemcpy(*dtw, tw.data(), sizeof(zd) * L, cudaMemcpyHostToDevice));
+    pl.tw = *dtw;
+    return CF_OK;
+}
+
+static double kx_of(const cf_engine* h, int ix) { return 2 * M_PI / h->Lx * ix; }
+static double lz_of(const cf_engine* h, int iz) { return 2 * M_PI / h->Lz * (iz <= (h->Nz >> 1) ? iz : iz - h->Nz); }
+
+// Stokes bank for (nu, lambda): batchedinfluence.jl:45-98, meanmode.jl:205-227
+static int build_bank(cf_engine* h, DevBank& bk, double nu, double lambda) {
+    const int P = h->P, Ny = h->Ny;
+    const long B = h->B;
+    std::vector<double> fac_p((size_t)B * 3 * Ny), fac_v((size_t)B * 3 * Ny), resp((size_t)B * 6 * Ny);
+    std::vector<double> colsc((size_t)B * 8, 0.0), sa((size_t)B * 4, 0.0);
+    std::vector<char> bad(B, 0);
+    setup::parallel_for(B, [&](long c) {
+        const int ix = (int)(c % h->Nxh), iz = (int)(c / h->Nxh);
+        const double k = kx_of(h, ix), l = lz_of(h, iz);
+        const double kap2 = k * k + l * l;
+        const double kp = kap2 == 0.0 ? 1.0 : kap2;  // zero-mode placeholder
+        const double shift = lambda + nu * kap2;
+        setup::Helm ph, vh;
+        ph.init(P, 1.0, kp, false);
+        vh.init(P, nu, shift, false);
+        std::vector<double> zero(Ny, 0.0), work(Ny), pp(Ny), pm(Ny), vp(Ny), vm(Ny), p0(Ny), v0(Ny);
+        ph.solve(zero.data(), 1.0, 0.0, pp.data());
+        setup::diff(pp.data(), work.data(), P);
+        vh.solve(work.data(), 0.0, 0.0, vp.data());
+        ph.solve(zero.data(), 0.0, 1.0, pm.data());
+        setup::diff(pm.data(), work.data(), P);
+        vh.solve(work.data(), 0.0, 0.0, vm.data());
+        double a = setup::wallderiv(vp.data(), P, true), b = setup::wallderiv(vm.data(), P, true);
+        double cc = setup::wallderiv(vp.data(), P, false), d = setup::wallderiv(vm.data(), P, false);
+        double scale = std::max(std::max(std::fabs(a), std::fabs(b)), std::max(std::fabs(cc), std::fabs(d)));
+        double inv[4] = {0, 0, 0, 0};
+        if (!(std::isfinite(scale) && scale > 0)) {
+            bad[c] = 1;
+        } else {
+            a /= scale; b /= scale; cc /= scale; d /= scale;
+            double det = a * d - b * cc;
+            if (!(std::isfinite(det) && std::fabs(det) > 2.220446049250313e-16 * std::max(std::fabs(a * d), std::fabs(b * cc)))) {
+                bad[c] = 1;
+            } else {
+                inv[0] = d / (det * scale); inv[1] = -b / (det * scale);
+                inv[2] = -cc / (det * scale); inv[3] = a / (det * scale);
+            }
+        }
+        // auxiliary tau problem with source (T_{P-1} + T_P)'
+        std::vector<double> src(Ny, 0.0), forcing(Ny);
+        src[P - 1] = 1.0; src[P] = 1.0;
+        setup::diff(src.data(), forcing.data(), P);
+        ph.solve(forcing.data(), 0.0, 0.0, p0.data());
+        setup::diff(p0.data(), forcing.data(), P);
+        vh.solve(forcing.data(), 0.0, 0.0, v0.data());
+        {
+            double up = 0, lo = 0;
+            for (int n = 1; n <= P; ++n) {
+                double t = (double)n * n * v0[n];
+                up -= t;
+                lo -= (n % 2 == 1 ? 1.0 : -1.0) * t;
+            }
+            double dp = inv[0] * up + inv[1] * lo, dm = inv[2] * up + inv[3] * lo;
+            for (int n = 0; n <= P; ++n) {
+                p0[n] += dp * pp[n] + dm * pm[n];
+                v0[n] += dp * vp[n] + dm * vm[n];
+            }
+        }
+        setup::diff(p0.data(), forcing.data(), P);
+        double* csc = &colsc[(size_t)c * 8];
+        for (int i = 0; i < 4; ++i) csc[i] = inv[i];
+        csc[4] = shift * v0[P - 1] + forcing[P - 1];
+        csc[5] = shift * v0[P];
+        csc[6] = shift;
+        csc[7] = kp;
+        double* fp = &fac_p[(size_t)c * 3 * Ny];
+        double* fv = &fac_v[(size_t)c * 3 * Ny];
+        for (int n = 0; n < Ny; ++n) {
+            fp[n] = ph.alpha[n]; fp[Ny + n] = ph.invden[n]; fp[2 * Ny + n] = ph.W[n];
+            fv[n] = vh.alpha[n]; fv[Ny + n] = vh.invden[n]; fv[2 * Ny + n] = vh.W[n];
+        }
+        double* s4 = &sa[(size_t)c * 4];
+        s4[0] = ph.SA[0]; s4[1] = ph.SA[1]; s4[2] = vh.SA[0]; s4[3] = vh.SA[1];
+        double* rs = &resp[(size_t)c * 6 * Ny];
+        const std::vector<double>* v6[6] = {&pp, &pm, &vp, &vm, &p0, &v0};
+        for (int i = 0; i < 6; ++i) std::memcpy(rs + (size_t)i * Ny, v6[i]->data(), sizeof(double) * Ny);
+    });
+    for (long c = 0; c < B; ++c)
+        if (bad[c]) return fail(CF_E_SINGULAR, "singular influence matrix for system " + std::to_string(c + 1));
+    // mean mode (nu D^2 - lambda) c = 1, c(+-1) = 0
+    if (!(std::isfinite(nu) && nu > 0 && std::isfinite(lambda) && lambda >= 0))
+        return fail(CF_E_ARG, "nu must be finite and positive, lambda finite and nonnegative");
+    setup::Helm mh;
+    mh.init(P, nu, lambda, false);
+    std::vector<double> e0(Ny, 0.0), mc(Ny);
+    e0[0] = 1.0;
+    mh.solve(e0.data(), 0.0, 0.0, mc.data());
+    bk.meanc_mean = setup::bulkmean(mc.data(), P);
+    if (!(std::isfinite(bk.meanc_mean) && bk.meanc_mean != 0.0))
+        return fail(CF_E_ARG, "the uniform-gradient response has no finite nonzero bulk mean");
+    int rc;
+    if (!bk.fac_p) {
+        if ((rc = dalloc(h, (void**)&bk.fac_p, fac_p.size() * 8))) return rc;
+        if ((rc = dalloc(h, (void**)&bk.fac_v, fac_v.size() * 8))) return rc;
+        if ((rc = dalloc(h, (void**)&bk.resp, resp.size() * 8))) return rc;
+        if ((rc = dalloc(h, (void**)&bk.colsc, colsc.size() * 8))) return rc;
+        if ((rc = dalloc(h, (void**)&bk.sa, sa.size() * 8))) return rc;
+        if ((rc = dalloc(h, (void**)&bk.meanc, Ny * 8))) return rc;
+    }
+    CU(cudaMemcpy(bk.fac_p, fac_p.data(), fac_p.size() * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(bk.fac_v, fac_v.data(), fac_v.size() * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(bk.resp, resp.data(), resp.size() * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(bk.colsc, colsc.data(), colsc.size() * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(bk.sa, sa.data(), sa.size() * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(bk.meanc, mc.data(), Ny * 8, cudaMemcpyHostToDevice));
+    bk.nu = nu;
+    bk.lambda = lambda;
+    bk.ready = true;
+    return CF_OK;
+}
+
+// Neumann pressure factors (pressure.jl:131-177): th0 = 1, th1 = kappa^2
+static int build_neumann(cf_engine* h) {
+    DevBank& bk = h->neum;
+    if (bk.ready) return CF_OK;
+    const int P = h->P, Ny = h->Ny;
+    const long B = h->B;
+    std::vector<double> fac((size_t)B * 3 * Ny, 0.0), sa((size_t)B * 4, 1.0);
+    setup::parallel_for(B, [&](long c) {
+        const int ix = (int)(c % h->Nxh), iz = (int)(c / h->Nxh);
+        const double k = kx_of(h, ix), l = lz_of(h, iz);
+        const double kap2 = k * k + l * l;
+        if (kap2 == 0.0) return;
+        setup::Helm hn;
+        hn.init(P, 1.0, kap2, true);
+        double* f = &fac[(size_t)c * 3 * Ny];
+        for (int n = 0; n < Ny; ++n) { f[n] = hn.alpha[n]; f[Ny + n] = hn.invden[n]; f[2 * Ny + n] = hn.W[n]; }
+        sa[(size_t)c * 4 + 0] = hn.SA[0];
+        sa[(size_t)c * 4 + 1] = hn.SA[1];
+    });
+    int rc;
+    if ((rc = dalloc(h, (void**)&bk.fac_p, fac.size() * 8))) return rc;
+    if ((rc = dalloc(h, (void**)&bk.sa, sa.size() * 8))) return rc;
+    CU(cudaMemcpy(bk.fac_p, fac.data(), fac.size() * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(bk.sa, sa.data(), sa.size() * 8, cudaMemcpyHostToDevice));
+    bk.ready = true;
+    return CF_OK;
+}
+
+static size_t col_smem(const cf_engine* h) { return (size_t)7 * CF_NCOL * (h->Ny + 1) * sizeof(zd); }
+
+static ColParams col_params(const cf_engine* h) {
+    ColParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.Nx = h->Nx; p.Nz = h->Nz; p.Nxh = h->Nxh; p.Ny = h->Ny; p.P = h->P; p.B = (int)h->B;
+    p.ax = 2 * M_PI / h->Lx; p.bz = 2 * M_PI / h->Lz;
+    p.nu = h->nu;
+    for (int i = 0; i < 3; ++i) { p.U[i] = h->U[i]; p.Q[i] = h->Q[i]; p.Nn[i] = h->nod[i]; p.Nout[i] = nullptr; }
+    p.Pf = h->Pf;
+    for (int i = 0; i < 6; ++i) p.nod[i] = h->nod[i];
+    p.base = h->d_base; p.basecurv = h->d_basecurv;
+    double bmc = setup::bulkmean(h->basecurv.data(), h->P);
+    p.nu_bm_curv = h->nu * bmc;
+    p.cmode = h->cmode;
+    if (h->cmode == 1) { p.c1 = h->c1 - h->basemean; p.c2 = h->c2; }
+    else { p.c1 = h->c1; p.c2 = h->c2; }
+    p.grad_out = h->d_grad;
+    p.plP = h->plP;
+    p.cs = h->d_cs;
+    p.fnorm = 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1));
+    return p;
+}
+
+static FftParams fft_params(const cf_engine* h) {
+    FftParams f;
+    f.Nx = h->Nx; f.Nz = h->Nz; f.Nxh = h->Nxh; f.Ny = h->Ny; f.Nzp = h->Nzp; f.Nxp = h->Nxp;
+    f.tkz = h->tkz;
+    for (int i = 0; i < 6; ++i) { f.nod[i] = h->nod[i]; f.zp[i] = h->zp[i]; }
+    f.plZ = h->plZ; f.plX = h->plX;
+    return f;
+}
+
+// nonlinear periodic transforms: nodal (6) -> nonlinear term at nodes (nod[0..2])
+static int launch_periodic(cf_engine* h, int* count) {
+    FftParams f = fft_params(h);
+    const size_t smz = (size_t)h->tkz * h->Nzp * sizeof(zd);
+    const size_t smx = (size_t)6 * h->Nxp * sizeof(zd);
+    dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
+    k_zinv<<<gz, 256, smz, h->stream>>>(f);
+    dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
+    k_xpass<<<gx, 256, smx, h->stream>>>(f);
+    dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
+    k_zfwd<<<gz3, 256, smz, h->stream>>>(f);
+    if (count) *count += 3;
+    CU(cudaGetLastError());
+    return CF_OK;
+}
+
+static unsigned col_blocks(const cf_engine* h) { return (unsigned)((h->B + CF_NCOL - 1) / CF_NCOL); }
+
+static int launch_prep(cf_engine* h, zd* const Usrc[3], int* count) {
+    ColParams p = col_params(h);
+    for (int i = 0; i < 3; ++i) p.U[i] = Usrc[i];
+    k_column_prep<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+    if (count) *count += 1;
+    CU(cudaGetLastError());
+    return CF_OK;
+}
+
+static int launch_stage(cf_engine* h, int j, int* count) {
+    int rc = launch_periodic(h, count);
+    if (rc) return rc;
+    ColParams p = col_params(h);
+    p.lambda = 1.0 / (CC[j] * h->dt);
+    p.weight = CB[j] / CC[j];
+    p.Acoef = CA[j];
+    p.stage = j;
+    p.store_q = (j < 2) ? 1 : 0;
+    p.bank = h->bank[j].view();
+    k_column_stage<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+    if (count) *count += 1;
+    CU(cudaGetLastError());
+    return CF_OK;
+}
+
+// Same launches as one step, with events around every kernel class (zinv,
+// xpass, zfwd, column) recorded on the handle's stream.
+static int launch_step_profiled(cf_engine* h, cudaEvent_t* ev, double* acc) {
+    FftParams f = fft_params(h);
+    const size_t smz = (size_t)h->tkz * h->Nzp * sizeof(zd);
+    const size_t smx = (size_t)6 * h->Nxp * sizeof(zd);
+    dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
+    dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
+    dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
+    for (int j = 0; j < 3; ++j) {
+        ColParams p = col_params(h);
+        p.lambda = 1.0 / (CC[j] * h->dt);
+        p.weight = CB[j] / CC[j];
+        p.Acoef = CA[j];
+        p.stage = j;
+        p.store_q = (j < 2) ? 1 : 0;
+        p.bank = h->bank[j].view();
+        CU(cudaEventRecord(ev[0], h->stream));
+        k_zinv<<<gz, 256, smz, h->stream>>>(f);
+        CU(cudaEventRecord(ev[1], h->stream));
+        k_xpass<<<gx, 256, smx, h->stream>>>(f);
+        CU(cudaEventRecord(ev[2], h->stream));
+        k_zfwd<<<gz3, 256, smz, h->stream>>>(f);
+        CU(cudaEventRecord(ev[3], h->stream));
+        k_column_stage<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+        CU(cudaEventRecord(ev[4], h->stream));
+        CU(cudaGetLastError());
+        CU(cudaEventSynchronize(ev[4]));
+        for (int k = 0; k < 4; ++k) {
+            float ms = 0.f;
+            CU(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            acc[k] += ms;
+        }
+    }
+    return CF_OK;
+}
+
+static int ensure_banks(cf_engine* h) {
+    for (int j = 0; j < 3; ++j)
+        if (!h->bank[j].ready) {
+            int rc = build_bank(h, h->bank[j], h->nu, 1.0 / (CC[j] * h->dt));
+            if (rc) return rc;
+        }
+    return CF_OK;
+}
+
+static void drop_graph(cf_engine* h) {
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+}
+
+static int build_graph(cf_engine* h) {
+    if (h->graph) return CF_OK;
+    cudaGraph_t g;
+    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int cnt = 0, rc = CF_OK;
+    for (int j = 0; j < 3 && rc == CF_OK; ++j) rc = launch_stage(h, j, &cnt);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(CF_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(CF_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return CF_OK;
+}
+
+static int set_attrs(cf_engine* h) {
+    const int maxsm = 227 * 1024;
+    size_t need[3] = {col_smem(h), (size_t)h->tkz * h->Nzp * sizeof(zd), (size_t)6 * h->Nxp * sizeof(zd)};
+    for (size_t x : need)
+        if (x > (size_t)maxsm) return fail(CF_E_UNSUPPORTED, "grid too large for the shared-memory tiles");
+    CU(cudaFuncSetAttribute(k_column_stage<CF_NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
+    CU(cudaFuncSetAttribute(k_column_prep<CF_NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
+    CU(cudaFuncSetAttribute(k_column_nlout<CF_NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
+    CU(cudaFuncSetAttribute(k_column_project<CF_NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
+    CU(cudaFuncSetAttribute(k_column_pressure<CF_NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
+    CU(cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[1]));
+    CU(cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[1]));
+    CU(cudaFuncSetAttribute(k_xpass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[2]));
+    return CF_OK;
+}
+
+static int validate_and_size(cf_engine* h, const cf_config* c) {
+    if (!(c->Ny >= 5 && c->Ny % 2 == 1)) return fail(CF_E_ARG, "Gibson's tau correction requires odd Ny >= 5");
+    if (!(c->Nx > 0 && c->Nz > 0)) return fail(CF_E_ARG, "Nx and Nz must be positive");
+    if (!(std::isfinite(c->Lx) && std::isfinite(c->Lz) && c->Lx > 0 && c->Lz > 0))
+        return fail(CF_E_ARG, "Lx and Lz must be finite and positive");
+    if (!(std::isfinite(c->dt) && c->dt > 0)) return fail(CF_E_ARG, "dt must be finite and positive");
+    if (!(std::isfinite(c->nu) && c->nu > 0)) return fail(CF_E_ARG, "nu must be finite and positive");
+    if (c->constraint != 0 && c->constraint != 1) return fail(CF_E_ARG, "unknown constraint kind");
+    if (!(std::isfinite(c->c1) && std::isfinite(c->c2))) return fail(CF_E_ARG, "mean-flow constraint values must be finite");
+    h->Nx = c->Nx; h->Ny = c->Ny; h->Nz = c->Nz; h->Lx = c->Lx; h->Lz = c->Lz;
+    h->nu = c->nu; h->dt = c->dt; h->cmode = c->constraint; h->c1 = c->c1; h->c2 = c->c2;
+    h->P = h->Ny - 1;
+    h->Nxh = h->Nx / 2 + 1;
+    h->Nxp = (3 * h->Nx + 1) / 2;
+    h->Nzp = (3 * h->Nz + 1) / 2;
+    h->B = (long)h->Nxh * h->Nz;
+    h->nr = h->B * h->Ny;
+    h->nq = (long)h->Nxh * h->Nzp * h->Ny;
+    if (h->P > 2 * 32 * CF_HELM_MAXR - 2) return fail(CF_E_UNSUPPORTED, "Ny too large for the column kernel");
+    std::vector<int> rP = fft_radices(h->P), rZ = fft_radices(h->Nzp), rX = fft_radices(h->Nxp);
+    if (!plan_fits(rP, h->P, 1, 32, CF_WARP_FFT_MAXE))
+        return fail(CF_E_UNSUPPORTED, "Chebyshev transform length not supported (prime factors <= 31, length <= 512)");
+    if (!plan_fits(rX, h->Nxp, 6, 256, CF_BLOCK_FFT_MAXE))
+        return fail(CF_E_UNSUPPORTED, "padded x length not supported");
+    h->tkz = 0;
+    for (int t : {8, 4, 2, 1})
+        if (plan_fits(rZ, h->Nzp, t, 256, CF_BLOCK_FFT_MAXE) && (size_t)t * h->Nzp * 16 <= 100 * 1024) { h->tkz = t; break; }
+    if (!h->tkz) return fail(CF_E_UNSUPPORTED, "padded z length not supported");
+    return CF_OK;
+}
+
+static void host_synth(const cf_engine* h, uint64_t seed, double amp, int shape, double rho, std::vector<std::complex<double>>& U);
+
+extern "C" {
+
+const char* cf_last_error(void) { return g_err.c_str(); }
+
+void cf_destroy(cf_handle* h) {
+    if (!h) return;
+    drop_graph(h);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int cf_create(const cf_config* cfg, cf_handle** out) {
+    if (!cfg || !out) return fail(CF_E_ARG, "null argument");
+    *out = nullptr;
+    cf_engine* h = new cf_engine();
+    int rc = validate_and_size(h, cfg);
+    if (rc) { delete h; return rc; }
+    // base profile (problem.jl:92, cnrk2.jl:494-495)
+    std::vector<double> vals(h->Ny);
+    for (int j = 0; j < h->Ny; ++j) {
+        double y = (2 * j == h->P) ? 0.0 : std::cos(M_PI * j / h->P);
+        if (cfg->profile == CF_PROFILE_COUETTE) vals[j] = y;
+        else if (cfg->profile == CF_PROFILE_POISEUILLE) vals[j] = 1 - y * y;
+        else if (cfg->profile == CF_PROFILE_VALUES && cfg->base_values) vals[j] = cfg->base_values[j];
+        else { delete h; return fail(CF_E_ARG, "unknown base profile"); }
+    }
+    h->base.resize(h->Ny); h->basecurv.resize(h->Ny);
+    setup::chebcoeffs(vals.data(), h->base.data(), h->P);
+    std::vector<double> d1(h->Ny);
+    setup::diff(h->base.data(), d1.data(), h->P);
+    setup::diff(d1.data(), h->basecurv.data(), h->P);
+    h->basemean = setup::bulkmean(h->base.data(), h->P);
+
+    auto bail = [&](int code) { cf_destroy(h); return code; };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(CF_E_CUDA, "cannot create stream (no CUDA device?)"));
+    const size_t fr = sizeof(zd) * h->nr, fq = sizeof(zd) * h->nq;
+    for (int i = 0; i < 3; ++i) {
+        if ((rc = dalloc(h, (void**)&h->U[i], fr))) return bail(rc);
+        if ((rc = dalloc(h, (void**)&h->Q[i], fr))) return bail(rc);
+    }
+    if ((rc = dalloc(h, (void**)&h->Pf, fr))) return bail(rc);
+    for (int i = 0; i < 6; ++i) {
+        if ((rc = dalloc(h, (void**)&h->nod[i], fr))) return bail(rc);
+        if ((rc = dalloc(h, (void**)&h->zp[i], fq))) return bail(rc);
+    }
+    if ((rc = dalloc(h, (void**)&h->d_base, 8 * h->Ny))) return bail(rc);
+    if ((rc = dalloc(h, (void**)&h->d_basecurv, 8 * h->Ny))) return bail(rc);
+    if ((rc = dalloc(h, (void**)&h->d_grad, 8 * 2))) return bail(rc);
+    if (cudaMemcpy(h->d_base, h->base.data(), 8 * h->Ny, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->d_basecurv, h->basecurv.data(), 8 * h->Ny, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(CF_E_CUDA, "upload failed"));
+    for (int i = 0; i < 3; ++i) cudaMemset(h->U[i], 0, fr), cudaMemset(h->Q[i], 0, fr);
+    cudaMemset(h->Pf, 0, fr);
+    cudaMemset(h->d_grad, 0, 16);
+    if ((rc = make_plan(h, h->P, h->plP, &h->d_twP))) return bail(rc);
+    if ((rc = make_plan(h, h->Nzp, h->plZ, &h->d_twZ))) return bail(rc);
+    if ((rc = make_plan(h, h->Nxp, h->plX, &h->d_twX))) return bail(rc);
+    {
+        std::vector<zd> cs(h->P + 1);
+        const long double pi = 3.141592653589793238462643383279502884L;
+        for (int n = 0; n <= h->P; ++n) {
+            long double a = pi * (long double)n / (long double)h->P;
+            cs[n] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+        if ((rc = dalloc(h, (void**)&h->d_cs, sizeof(zd) * (h->P + 1)))) return bail(rc);
+        cudaMemcpy(h->d_cs, cs.data(), sizeof(zd) * (h->P + 1), cudaMemcpyHostToDevice);
+    }
+    if ((rc = set_attrs(h))) return bail(rc);
+    if ((rc = ensure_banks(h))) return bail(rc);
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(CF_E_CUDA, "set-up failed"));
+    *out = h;
+    return CF_OK;
+}
+
+int cf_set_constraint(cf_handle* h, int kind, double c1, double c2) {
+    if (!h) return fail(CF_E_ARG, "null handle");
+    if (kind != 0 && kind != 1) return fail(CF_E_ARG, "unknown constraint kind");
+    if (!(std::isfinite(c1) && std::isfinite(c2))) return fail(CF_E_ARG, "mean-flow constraint values must be finite");
+    h->cmode = kind; h->c1 = c1; h->c2 = c2;
+    drop_graph(h);
+    return CF_OK;
+}
+
+int cf_set_state(cf_handle* h, const double* U, const double* P) {
+    if (!h || !U || !P) return fail(CF_E_ARG, "null argument");
+    const size_t fr = sizeof(zd) * h->nr;
+    for (int i = 0; i < 3; ++i) CU(cudaMemcpyAsync(h->U[i], U + 2 * i * h->nr, fr, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(h->Pf, P, fr, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    h->nodal_valid = false;
+    return CF_OK;
+}
+int cf_get_state(cf_handle* h, double* U, double* P) {
+    if (!h || !U) return fail(CF_E_ARG, "null argument");
+    const size_t fr = sizeof(zd) * h->nr;
+    for (int i = 0; i < 3; ++i) CU(cudaMemcpyAsync(U + 2 * i * h->nr, h->U[i], fr, cudaMemcpyDeviceToHost, h->stream));
+    if (P) CU(cudaMemcpyAsync(P, h->Pf, fr, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return CF_OK;
+}
+int cf_set_state_device(cf_handle* h, const void* U, const void* P) {
+    if (!h || !U || !P) return fail(CF_E_ARG, "null argument");
+    const size_t fr = sizeof(zd) * h->nr;
+    for (int i = 0; i < 3; ++i)
+        CU(cudaMemcpyAsync(h->U[i], (const char*)U + i * fr, fr, cudaMemcpyDeviceToDevice, h->stream));
+    CU(cudaMemcpyAsync(h->Pf, P, fr, cudaMemcpyDeviceToDevice, h->stream));
+    h->nodal_valid = false;
+    return CF_OK;
+}
+int cf_get_state_device(cf_handle* h, void* U, void* P) {
+    if (!h || !U) return fail(CF_E_ARG, "null argument");
+    const size_t fr = sizeof(zd) * h->nr;
+    for (int i = 0; i < 3; ++i)
+        CU(cudaMemcpyAsync((char*)U + i * fr, h->U[i], fr, cudaMemcpyDeviceToDevice, h->stream));
+    if (P) CU(cudaMemcpyAsync(P, h->Pf, fr, cudaMemcpyDeviceToDevice, h->stream));
+    return CF_OK;
+}
+
+int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out) {
+    if (!h) return fail(CF_E_ARG, "null handle");
+    if (nsteps < 0) return fail(CF_E_ARG, "nsteps must be nonnegative");
+    int rc, cnt = 0;
+    if (!h->nodal_valid) {
+        if ((rc = launch_prep(h, h->U, &cnt))) return rc;
+        h->nodal_valid = true;
+    }
+    if ((rc = build_graph(h))) return rc;
+    for (int s = 0; s < nsteps; ++s) CU(cudaGraphLaunch(h->graph, h->stream));
+    cnt += 12 * nsteps;
+    h->last_launches = cnt;
+    if (t_out) *t_out = t + nsteps * h->dt;
+    if (grads_out) {
+        double g[2];
+        CU(cudaMemcpyAsync(g, h->d_grad, 16, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        grads_out[0] = g[0];
+        grads_out[1] = g[1];
+    }
+    return CF_OK;
+}
+
+static int ensure_tmp(cf_engine* h) {
+    int rc;
+    if (!h->tmpU) {
+        if ((rc = dalloc(h, (void**)&h->tmpU, sizeof(zd) * h->nr * 3))) return rc;
+        if ((rc = dalloc(h, (void**)&h->tmpP, sizeof(zd) * h->nr))) return rc;
+    }
+    return CF_OK;
+}
+
+int cf_nonlinear(cf_handle* h, const double* U, double* N) {
+    if (!h || !U || !N) return fail(CF_E_ARG, "null argument");
+    int rc = ensure_tmp(h);
+    if (rc) return rc;
+    const size_t fr = sizeof(zd) * h->nr;
+    CU(cudaMemcpyAsync(h->tmpU, U, 3 * fr, cudaMemcpyHostToDevice, h->stream));
+    zd* Us[3] = {h->tmpU, h->tmpU + h->nr, h->tmpU + 2 * h->nr};
+    if ((rc = launch_prep(h, Us, nullptr))) return rc;
+    if ((rc = launch_periodic(h, nullptr))) return rc;
+    ColParams p = col_params(h);
+    for (int i = 0; i < 3; ++i) p.Nout[i] = Us[i];
+    k_column_nlout<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(N, h->tmpU, 3 * fr, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    h->nodal_valid = false;
+    return CF_OK;
+}
+
+static int project_dev(cf_engine* h, zd* const Ud[3]) {
+    int rc;
+    if (!h->proj.ready && (rc = build_bank(h, h->proj, 1.0, 0.0))) return rc;
+    ColParams p = col_params(h);
+    for (int i = 0; i < 3; ++i) p.U[i] = Ud[i];
+    p.bank = h->proj.view();
+    if (h->cmode == 1) { p.cmode = 1; p.c1 = h->c1 - h->basemean; p.c2 = h->c2; }
+    else { p.cmode = 0; p.c1 = 0.0; p.c2 = 0.0; }
+    double* gtmp = h->d_grad;
+    p.grad_out = gtmp;
+    k_column_project<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+    CU(cudaGetLastError());
+    return CF_OK;
+}
+
+static int pressure_dev(cf_engine* h, zd* const Ud[3], zd* Pout) {
+    int rc;
+    if ((rc = build_neumann(h))) return rc;
+    if ((rc = launch_prep(h, Ud, nullptr))) return rc;
+    if ((rc = launch_periodic(h, nullptr))) return rc;
+    ColParams p = col_params(h);
+    for (int i = 0; i < 3; ++i) p.U[i] = Ud[i];
+    p.Pf = Pout;
+    p.bank = h->neum.view();
+    k_column_pressure<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+    CU(cudaGetLastError());
+    h->nodal_valid = false;
+    return CF_OK;
+}
+
+int cf_project(cf_handle* h, double* U) {
+    if (!h || !U) return fail(CF_E_ARG, "null argument");
+    int rc = ensure_tmp(h);
+    if (rc) return rc;
+    const size_t fr = sizeof(zd) * h->nr;
+    CU(cudaMemcpyAsync(h->tmpU, U, 3 * fr, cudaMemcpyHostToDevice, h->stream));
+    zd* Us[3] = {h->tmpU, h->tmpU + h->nr, h->tmpU + 2 * h->nr};
+    if ((rc = project_dev(h, Us))) return rc;
+    CU(cudaMemcpyAsync(U, h->tmpU, 3 * fr, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return CF_OK;
+}
+
+int cf_pressure(cf_handle* h, const double* U, double* P) {
+    if (!h || !U || !P) return fail(CF_E_ARG, "null argument");
+    int rc = ensure_tmp(h);
+    if (rc) return rc;
+    const size_t fr = sizeof(zd) * h->nr;
+    CU(cudaMemcpyAsync(h->tmpU, U, 3 * fr, cudaMemcpyHostToDevice, h->stream));
+    zd* Us[3] = {h->tmpU, h->tmpU + h->nr, h->tmpU + 2 * h->nr};
+    if ((rc = pressure_dev(h, Us, h->tmpP))) return rc;
+    CU(cudaMemcpyAsync(P, h->tmpP, fr, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return CF_OK;
+}
+
+int cf_random_state(cf_handle* h, unsigned long long seed, double amp, int shape, double rho) {
+    if (!h) return fail(CF_E_ARG, "null handle");
+    if (!(amp >= 0)) return fail(CF_E_ARG, "epsilon must be non-negative");
+    std::vector<std::complex<double>> U;
+    host_synth(h, seed, amp, shape, rho, U);
+    const size_t fr = sizeof(zd) * h->nr;
+    for (int i = 0; i < 3; ++i) CU(cudaMemcpyAsync(h->U[i], U.data() + i * h->nr, fr, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    int rc;
+    if ((rc = project_dev(h, h->U))) return rc;
+    if ((rc = pressure_dev(h, h->U, h->Pf))) return rc;
+    CU(cudaStreamSynchronize(h->stream));
+    h->nodal_valid = false;
+    return CF_OK;
+}
+
+int cf_diagnostics(cf_handle* h, double* out) {
+    if (!h || !out) return fail(CF_E_ARG, "null argument");
+    std::vector<std::complex<double>> U((size_t)3 * h->nr);
+    int rc = cf_get_state(h, reinterpret_cast<double*>(U.data()), nullptr);
+    if (rc) return rc;
+    const int Ny = h->Ny, P = h->P;
+    const long S = h->B;
+    auto moment = [](int n) { return (n % 2 == 0) ? 1.0 / (1.0 - (double)n * n) : 0.0; };
+    std::vector<double> M((size_t)Ny * Ny);
+    for (int m = 0; m < Ny; ++m)
+        for (int n = 0; n < Ny; ++n) M[(size_t)m * Ny + n] = (moment(m + n) + moment(std::abs(m - n))) / 2;
+    auto nyq = [&](int ix, int iz) { return ((h->Nx % 2 == 0) && ix == h->Nx / 2) || ((h->Nz % 2 == 0) && iz == h->Nz / 2); };
+    auto dotc = [&](const std::complex<double>* a, const std::complex<double>* b) {
+        double r = 0;
+        std::vector<std::complex<double>> w(Ny);
+        for (long c = 0; c < S; ++c) {
+            int ix = c % h->Nxh, iz = c / h->Nxh;
+            if (nyq(ix, iz)) continue;
+            std::complex<double> d = 0;
+            for (int m = 0; m < Ny; ++m) {
+                std::complex<double> s = 0;
+                for (int n = 0; n < Ny; ++n) s += M[(size_t)m * Ny + n] * b[c + n * S];
+                d += std::conj(a[c + m * S]) * s;
+            }
+            r += (ix == 0 ? 1.0 : 2.0) * d.real();
+        }
+        return r;
+    };
+    const std::complex<double>* u[3] = {U.data(), U.data() + h->nr, U.data() + 2 * h->nr};
+    double e = 0;
+    for (int i = 0; i < 3; ++i) e += dotc(u[i], u[i]);
+    // curl and divergence on the host (diagnostic only)
+    std::vector<std::complex<double>> om((size_t)3 * h->nr), dv(h->nr);
+    std::vector<std::complex<double>> col(Ny), dcol(Ny);
+    const std::complex<double> I(0, 1);
+    double mxdiv = 0;
+    for (long c = 0; c < S; ++c) {
+        int ix = c % h->Nxh, iz = c / h->Nxh;
+        double k = kx_of(h, ix), l = lz_of(h, iz);
+        std::vector<double> re(Ny), im(Ny), dre(Ny), dim(Ny);
+        auto dy = [&](const std::complex<double>* f, std::complex<double>* out) {
+            for (int n = 0; n < Ny; ++n) { re[n] = f[c + n * S].real(); im[n] = f[c + n * S].imag(); }
+            setup::diff(re.data(), dre.data(), P);
+            setup::diff(im.data(), dim.data(), P);
+            for (int n = 0; n < Ny; ++n) out[n] = std::complex<double>(dre[n], dim[n]);
+        };
+        std::vector<std::complex<double>> dw(Ny), du(Ny), dvv(Ny);
+        dy(u[2], dw.data());
+        dy(u[0], du.data());
+        dy(u[1], dvv.data());
+        for (int n = 0; n < Ny; ++n) {
+            om[c + n * S] = dw[n] - I * l * u[1][c + n * S];
+            om[h->nr + c + n * S] = I * (l * u[0][c + n * S] - k * u[2][c + n * S]);
+            om[2 * h->nr + c + n * S] = I * k * u[1][c + n * S] - du[n];
+            std::complex<double> d = I * k * u[0][c + n * S] + dvv[n] + I * l * u[2][c + n * S];
+            mxdiv = std::max(mxdiv, std::abs(d));
+        }
+    }
+    double d = 0;
+    for (int i = 0; i < 3; ++i) d += dotc(om.data() + i * h->nr, om.data() + i * h->nr);
+    std::vector<double> m0(Ny);
+    for (int n = 0; n < Ny; ++n) m0[n] = u[0][n * S].real();
+    out[0] = e / 2;
+    out[1] = h->nu * d;
+    out[2] = mxdiv;
+    out[3] = h->nu * setup::wallderiv(m0.data(), P, true);
+    out[4] = h->nu * setup::wallderiv(m0.data(), P, false);
+    return CF_OK;
+}
+
+int cf_step_profiled(cf_handle* h, double t, int nsteps, double* t_out, double* kernel_ms) {
+    if (!h || !kernel_ms) return fail(CF_E_ARG, "null argument");
+    int rc, cnt = 0;
+    if (!h->nodal_valid) {
+        if ((rc = launch_prep(h, h->U, &cnt))) return rc;
+        h->nodal_valid = true;
+    }
+    cudaEvent_t ev[5];
+    for (int k = 0; k < 5; ++k) CU(cudaEventCreate(&ev[k]));
+    for (int k = 0; k < 4; ++k) kernel_ms[k] = 0.0;
+    for (int s = 0; s < nsteps && rc == CF_OK; ++s) rc = launch_step_profiled(h, ev, kernel_ms);
+    for (int k = 0; k < 5; ++k) cudaEventDestroy(ev[k]);
+    if (rc) return rc;
+    h->last_launches = cnt + 12 * nsteps;
+    if (t_out) *t_out = t + nsteps * h->dt;
+    return CF_OK;
+}
+
+int cf_sync(cf_handle* h) {
+    if (!h) return fail(CF_E_ARG, "null handle");
+    CU(cudaStreamSynchronize(h->stream));
+    return CF_OK;
+}
+int cf_last_launch_count(cf_handle* h) { return h ? h->last_launches : 0; }
+void* cf_stream(cf_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+}  // extern "C"
+
+// Seeded synthetic coefficients: splitmix64 hash of (seed, component, ix, iz,
+// n) -> two uniforms -> Box-Muller; amplitude shaped in (k, l, n).
+static inline uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ULL;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    return x ^ (x >> 31);
+}
+static inline double unit01(uint64_t v) { return ((v >> 11) + 0.5) * (1.0 / 9007199254740992.0); }
+static void host_synth(const cf_engine* h, uint64_t seed, double amp, int shape, double rho,
+                       std::vector<std::complex<double>>& U) {
+    const long S = h->B;
+    U.assign((size_t)3 * h->nr, 0.0);
+    for (int c = 0; c < 3; ++c)
+        for (int n = 0; n < h->Ny; ++n)
+            for (int iz = 0; iz < h->Nz; ++iz) {
+                int l = iz <= (h->Nz >> 1) ? iz : iz - h->Nz;
+                for (int ix = 0; ix < h->Nxh; ++ix) {
+                    bool nyq = ((h->Nx % 2 == 0) && ix == h->Nx / 2) || ((h->Nz % 2 == 0) && iz == h->Nz / 2);
+                    double s, r;
+                    if (shape == 0) { s = std::exp(-(std::abs(ix) + std::abs(l)) / 4.0); r = std::exp(-n / 4.0); }
+                    else { s = 1.0 / (1.0 + (double)ix * ix + (double)l * l); r = std::pow(rho, n); }
+                    std::complex<double> v = 0;
+                    if (!nyq) {
+                        uint64_t key = splitmix64(seed ^ splitmix64(((uint64_t)c << 56) ^ ((uint64_t)ix << 36) ^
+                                                                   ((uint64_t)iz << 16) ^ (uint64_t)n));
+                        double a = unit01(splitmix64(key)), b = unit01(splitmix64(key ^ 0xD1B54A32D192ED03ULL));
+                        double rr = std::sqrt(-2.0 * std::log(a));
+                        v = amp * s * r * std::complex<double>(rr * std::cos(2 * M_PI * b), rr * std::sin(2 * M_PI * b));
+                    }
+                    U[(size_t)c * h->nr + n * S + (long)iz * h->Nxh + ix] = v;
+                }
+            }
+    for (int c = 0; c < 3; ++c)
+        for (int n = 0; n < h->Ny; ++n) {
+            std::complex<double>* col = U.data() + (size_t)c * h->nr + n * S;
+            col[0] = col[0].real();
+            for (int iz = (h->Nz >> 1) + 1; iz < h->Nz; ++iz) col[(long)iz * h->Nxh] = std::conj(col[(long)(h->Nz - iz) * h->Nxh]);
+        }
+}

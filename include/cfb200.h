@@ -1,0 +1,112 @@
+/*
+ * cfb200.h -- C ABI of the B200 CNRK2 engine for ChannelFlow.jl's time step.
+ *
+ * The engine replaces the device path of the reference's CNRK2 `step!`
+ * (src/timesteppers/cnrk2.jl:567-625) with the rotational nonlinear term
+ * (src/nonlinear.jl:173-193), the batched influence/tau Stokes solve
+ * (src/solvers/stokes.jl:391-418, batchedinfluence.jl:129-160, meanmode.jl:263-310)
+ * and the padded Fourier-Chebyshev transforms (src/ffts.jl:189-290).  The
+ * reference reaches that path through Julia dispatch on CuArray storage
+ * (ext/ChannelFlowCUDAExt.jl:7-32); a Julia host calls these functions with
+ * `ccall` instead.  All functions return 0 on success and a negative
+ * CF_E_* code on failure; cf_last_error() describes the last failure of the
+ * calling thread.
+ *
+ * Field layout (identical to Julia's ComplexF64 arrays of size (Nx/2+1, Nz, Ny)):
+ * complex128 interleaved (re, im), k fastest, then l (FFT order), then the
+ * Chebyshev degree n.  A velocity is three such fields back to back.
+ * One handle owns its device memory and one CUDA stream; it is not reentrant
+ * (the reference's caches "must not be used concurrently", cnrk2.jl:565).
+ */
+#ifndef CFB200_H
+#define CFB200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CF_OK 0
+#define CF_E_ARG -1       /* invalid argument: even or small Ny, sizes, dt, nu (cnrk2.jl:478, stokes.jl:345-348) */
+#define CF_E_SINGULAR -2  /* singular influence matrix (batchedinfluence.jl:75-76) */
+#define CF_E_NOMEM -3     /* device allocation failed */
+#define CF_E_CUDA -4      /* CUDA runtime error */
+#define CF_E_UNSUPPORTED -5 /* size outside the engine's transform limits */
+#define CF_E_NONFINITE -6 /* non-finite value detected in the state */
+
+#define CF_PROFILE_COUETTE 0    /* Ub(y) = y        (problem.jl:122-123) */
+#define CF_PROFILE_POISEUILLE 1 /* Ub(y) = 1 - y^2  (problem.jl:137-144) */
+#define CF_PROFILE_VALUES 2     /* Ub given at the Ny Lobatto points y_j = cos(pi j/(Ny-1)) */
+
+#define CF_CONSTRAINT_PRESSUREGRADIENT 0 /* (dPdx, dPdz) prescribed */
+#define CF_CONSTRAINT_BULKVELOCITY 1     /* total bulk velocities (Ubulk, Wbulk) prescribed */
+
+typedef struct cf_config {
+    int Nx, Ny, Nz;      /* Grid(Nx, Ny, Nz, Lx, Lz): grids.jl:27-30 */
+    double Lx, Lz;
+    double nu, dt;       /* CNRK2(grid, baseflow, nu, dt): cnrk2.jl:476 */
+    int profile;         /* CF_PROFILE_* */
+    const double* base_values; /* Ny values when profile == CF_PROFILE_VALUES */
+    int constraint;      /* CF_CONSTRAINT_* (problem.jl:81-87) */
+    double c1, c2;       /* gradients or bulk velocities */
+} cf_config;
+
+typedef struct cf_engine cf_handle;
+
+/* ChannelFlowProblem(grid, profile, nu, dt; constraint) + adapt(CuArray, problem)
+ * (problem.jl:69-107, ext/ChannelFlowCUDAExt.jl:18-32). */
+int cf_create(const cf_config* cfg, cf_handle** out);
+void cf_destroy(cf_handle* h);
+
+/* Replace the constraint used by later steps (step! keywords, cnrk2.jl:572-576). */
+int cf_set_constraint(cf_handle* h, int kind, double c1, double c2);
+
+/* adapt(CuArray, state) / Array(...) (src/adapt.jl:6-39): host buffers of
+ * 3*Nr and Nr complex128 values, Nr = (Nx/2+1)*Nz*Ny.  P may be NULL in get. */
+int cf_set_state(cf_handle* h, const double* U, const double* P);
+int cf_get_state(cf_handle* h, double* U, double* P);
+/* The same with device pointers (no host copy). */
+int cf_set_state_device(cf_handle* h, const void* U, const void* P);
+int cf_get_state_device(cf_handle* h, void* U, void* P);
+
+/* step!(scheme, nlterm, U, P, t; constraint...) repeated nsteps times on the
+ * engine state (cnrk2.jl:567-625).  *t_out = t + nsteps*dt; grads_out
+ * (may be NULL) receives the last stage's (dPdx, dPdz) (stokes.jl:417).
+ * Only NoForcing is supported (forcing.jl:9-11). */
+int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out);
+
+/* NonLinearTerm{RotatingForm}(t, U, N) on host buffers (nonlinear.jl:173-193). */
+int cf_nonlinear(cf_handle* h, const double* U, double* N);
+
+/* project!(U, problem) on a host velocity, in place (pressure.jl:36-54). */
+int cf_project(cf_handle* h, double* U);
+/* pressure(U, problem) (pressure.jl:95-104): modified pressure of U. */
+int cf_pressure(cf_handle* h, const double* U, double* P);
+
+/* random_state(problem, epsilon) analogue: seeded spectral Gaussian
+ * perturbation with amplitude amp and spectrum `shape` (0: exp(-(|k|+|l|)/4)
+ * exp(-n/4); 1: (1+k^2+l^2)^-1 rho^n), conjugate symmetric on k = 0, then
+ * project! and pressure (initialization.jl:176-195).  Sets the engine state. */
+int cf_random_state(cf_handle* h, unsigned long long seed, double amp, int shape, double rho);
+
+/* Diagnostics of the engine's perturbation velocity (postprocessing.jl:80-95):
+ * out[0] kinetic energy, out[1] dissipation nu<|curl u|^2>, out[2] max |div u|
+ * coefficient, out[3] nu du/dy(+1) and out[4] nu du/dy(-1) of the (0,0) mode. */
+int cf_diagnostics(cf_handle* h, double* out);
+
+/* step! like cf_step without the CUDA graph, with CUDA events around every
+ * kernel class; kernel_ms[0..3] receives the summed device time of the
+ * z-inverse, x-pass, z-forward and column kernels over the nsteps steps. */
+int cf_step_profiled(cf_handle* h, double t, int nsteps, double* t_out, double* kernel_ms);
+
+/* Block until the handle's stream is idle. */
+int cf_sync(cf_handle* h);
+/* Number of kernel launches issued by the most recent cf_step call. */
+int cf_last_launch_count(cf_handle* h);
+/* Device stream of the handle (cudaStream_t), for callers that time on it. */
+void* cf_stream(cf_handle* h);
+
+const char* cf_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -218,6 +218,11 @@ static void cheb_coeffs(const double* vals, double* coef, int Ny) {
 // Tau Helmholtz solver: rows 0..P-2 of (th0*D^2 - th1) a = f, plus wall rows.
 // Dirichlet: a(+1) = bp, a(-1) = bm.  Neumann: a'(+1) = bp, a'(-1) = bm.
 // ---------------------------------------------------------------------------
+// Timing samples only: when > 1, every independent loop of a stage (columns,
+// planes, rows, points) runs over 1/g_sample_div of its range, so a bounded
+// fraction of one stage can be timed.  Results are then not meaningful.
+static long g_sample_div = 1;
+static inline long sampled(long n) { return g_sample_div > 1 ? std::max(1L, n / g_sample_div) : n; }
 static int g_helm_method = 0;       // 0 auto, 1 dense, 2 quasi-tridiagonal
 static int g_dense_max_ny = 65;     // auto: dense LU up to this Ny
 
@@ -616,7 +621,7 @@ static void inverse_transform(const OGrid& g, const cd* U, double* u) {
     {
         std::vector<cd> col(Ny), buf(2 * P + 2), work(2 * P + 2);
 #pragma omp for schedule(static)
-        for (long c = 0; c < (long)Nz * Nxh; ++c) {
+        for (long c = 0; c < sampled((long)Nz * Nxh); ++c) {
             int iz = c / Nxh, ix = c % Nxh;
             for (int n = 0; n < Ny; ++n) col[n] = U[((long)n * Nz + iz) * Nxh + ix];
             col[0] *= 2.0;
@@ -631,14 +636,14 @@ static void inverse_transform(const OGrid& g, const cd* U, double* u) {
     {
         std::vector<cd> line(std::max(Nzp, Nxp)), work(std::max(Nzp, Nxp));
 #pragma omp for schedule(static)
-        for (long c = 0; c < (long)Ny * Nxh; ++c) {  // z backward c2c
+        for (long c = 0; c < sampled((long)Ny * Nxh); ++c) {  // z backward c2c
             int n = c / Nxh, ix = c % Nxh;
             for (int z = 0; z < Nzp; ++z) line[z] = pad[((size_t)n * Nzp + z) * Nxhp + ix];
             fft_inplace(line.data(), work.data(), Nzp, +1);
             for (int z = 0; z < Nzp; ++z) pad[((size_t)n * Nzp + z) * Nxhp + ix] = line[z];
         }
 #pragma omp for schedule(static)
-        for (long c = 0; c < (long)Ny * Nzp; ++c) {  // x c2r
+        for (long c = 0; c < sampled((long)Ny * Nzp); ++c) {  // x c2r
             const cd* X = &pad[(size_t)c * Nxhp];
             line[0] = X[0].real();
             for (int k = 1; k < Nxhp; ++k) {
@@ -660,13 +665,13 @@ static void forward_transform(const OGrid& g, const double* u, cd* U) {
     {
         std::vector<cd> line(std::max(Nzp, Nxp)), work(std::max(Nzp, Nxp));
 #pragma omp for schedule(static)
-        for (long c = 0; c < (long)Ny * Nzp; ++c) {  // x r2c
+        for (long c = 0; c < sampled((long)Ny * Nzp); ++c) {  // x r2c
             for (int j = 0; j < Nxp; ++j) line[j] = u[(size_t)c * Nxp + j];
             fft_inplace(line.data(), work.data(), Nxp, -1);
             for (int k = 0; k < Nxhp; ++k) pad[(size_t)c * Nxhp + k] = line[k];
         }
 #pragma omp for schedule(static)
-        for (long c = 0; c < (long)Ny * Nxh; ++c) {  // z forward c2c
+        for (long c = 0; c < sampled((long)Ny * Nxh); ++c) {  // z forward c2c
             int n = c / Nxh, ix = c % Nxh;
             for (int z = 0; z < Nzp; ++z) line[z] = pad[((size_t)n * Nzp + z) * Nxhp + ix];
             fft_inplace(line.data(), work.data(), Nzp, -1);
@@ -678,7 +683,7 @@ static void forward_transform(const OGrid& g, const double* u, cd* U) {
     {
         std::vector<cd> col(Ny), buf(2 * P + 2), work(2 * P + 2);
 #pragma omp for schedule(static)
-        for (long c = 0; c < (long)Nz * Nxh; ++c) {
+        for (long c = 0; c < sampled((long)Nz * Nxh); ++c) {
             int iz = c / Nxh, ix = c % Nxh;
             int izp = g.zpad(iz);
             for (int n = 0; n < Ny; ++n) col[n] = pad[((size_t)n * Nzp + izp) * Nxhp + ix];
@@ -794,7 +799,7 @@ struct Stokes {
                double basemean, double* grads) const {
         const long S = (long)g.Nxh * g.Nz;
 #pragma omp parallel for schedule(dynamic, 16)
-        for (long c = 0; c < S; ++c) {
+        for (long c = 0; c < sampled(S); ++c) {
             if (c == 0) continue;
             modes[c].solve(U[0] + c, U[1] + c, U[2] + c, Pf + c, R[0] + c, R[1] + c, R[2] + c, S);
         }
@@ -845,7 +850,7 @@ static void nonlinear(Problem& pb, const cd* const U[3], cd* const Nout[3]) {
     const double *w1 = pb.wphys[0].data(), *w2 = pb.wphys[1].data(), *w3 = pb.wphys[2].data();
     double *n1 = pb.nphys[0].data(), *n2 = pb.nphys[1].data(), *n3 = pb.nphys[2].data();
 #pragma omp parallel for schedule(static)
-    for (long i = 0; i < np; ++i) {
+    for (long i = 0; i < sampled(np); ++i) {
         n1[i] = u2[i] * w3[i] - u3[i] * w2[i];
         n2[i] = u3[i] * w1[i] - u1[i] * w3[i];
         n3[i] = u1[i] * w2[i] - u2[i] * w1[i];
@@ -861,46 +866,49 @@ static bool problem_stokes(Problem& pb) {
     return true;
 }
 
-// step! (cnrk2.jl:567-625).  Returns the last stage's gradients in grads.
-static void cnrk2_step(Problem& pb, cd* const U[3], cd* Pf, double* grads) {
+// One CNRK2 stage j (cnrk2.jl:588-622); gradients carries the previous
+// stage's uniform gradients in and this stage's out.
+static void cnrk2_stage(Problem& pb, cd* const U[3], cd* Pf, int j, double* gradients) {
     const OGrid& g = pb.g;
     const long nr = g.nr(), S = (long)g.Nxh * g.Nz;
-    double gradients[2] = {pb.cmode == 0 ? pb.c1 : 0.0, pb.cmode == 0 ? pb.c2 : 0.0};
     cd* Nf[3] = {pb.N[0].data(), pb.N[1].data(), pb.N[2].data()};
     cd* Rf[3] = {pb.R[0].data(), pb.R[1].data(), pb.R[2].data()};
-    const cd I(0, 1);
-    for (int j = 0; j < 3; ++j) {
-        const cd* Uc[3] = {U[0], U[1], U[2]};
-        nonlinear(pb, Uc, Nf);
-        double old[2] = {gradients[0], gradients[1]};
-        if (pb.cmode == 1) {
-            for (int i = 0; i < 2; ++i) {
-                int comp = i == 0 ? 0 : 2;
-                cd sh = wall_deriv(U[comp], S, g.Ny, true) - wall_deriv(U[comp], S, g.Ny, false);
-                double base = i == 0 ? pb.nu * bulkmean(pb.basecurv.data(), 1, g.Ny) : 0.0;
-                old[i] = pb.nu * sh.real() / 2 + base + bulkmean(Nf[comp], S, g.Ny).real();
-            }
+    const cd* Uc[3] = {U[0], U[1], U[2]};
+    nonlinear(pb, Uc, Nf);
+    double old[2] = {gradients[0], gradients[1]};
+    if (pb.cmode == 1) {
+        for (int i = 0; i < 2; ++i) {
+            int comp = i == 0 ? 0 : 2;
+            cd sh = wall_deriv(U[comp], S, g.Ny, true) - wall_deriv(U[comp], S, g.Ny, false);
+            double base = i == 0 ? pb.nu * bulkmean(pb.basecurv.data(), 1, g.Ny) : 0.0;
+            old[i] = pb.nu * sh.real() / 2 + base + bulkmean(Nf[comp], S, g.Ny).real();
         }
-        for (int i = 0; i < 3; ++i) {
-            cd* Qi = pb.Q[i].data();
-            if (j == 0) std::memcpy(Qi, Nf[i], sizeof(cd) * nr);
-            else for (long x = 0; x < nr; ++x) Qi[x] = CA[j] * Qi[x] + Nf[i][x];
-        }
-        const double lambda = 1.0 / (CC[j] * pb.dt), weight = CB[j] / CC[j];
-        for (int i = 0; i < 3; ++i) {
-            op_laplacian(g, U[i], Rf[i]);
-            if (i == 0) op_ddx1(g, Pf, Nf[i], false);
-            else if (i == 1) op_ddx2(g, Pf, Nf[i], false);
-            else op_ddx3(g, Pf, Nf[i], false);
-            const cd* Qi = pb.Q[i].data();
-            for (long x = 0; x < nr; ++x) Rf[i][x] = lambda * U[i][x] + pb.nu * Rf[i][x] - Nf[i][x] + weight * Qi[x];
-        }
-        for (int n = 0; n < g.Ny; ++n) Rf[0][n * S] += 2 * pb.nu * pb.basecurv[n];
-        Rf[0][0] -= old[0];
-        Rf[2][0] -= old[1];
-        const cd* Rc[3] = {Rf[0], Rf[1], Rf[2]};
-        pb.stokes[j].solve(g, U, Pf, Rc, pb.cmode, pb.c1, pb.c2, pb.basemean, gradients);
     }
+    for (int i = 0; i < 3; ++i) {
+        cd* Qi = pb.Q[i].data();
+        if (j == 0) std::memcpy(Qi, Nf[i], sizeof(cd) * nr);
+        else for (long x = 0; x < nr; ++x) Qi[x] = CA[j] * Qi[x] + Nf[i][x];
+    }
+    const double lambda = 1.0 / (CC[j] * pb.dt), weight = CB[j] / CC[j];
+    for (int i = 0; i < 3; ++i) {
+        op_laplacian(g, U[i], Rf[i]);
+        if (i == 0) op_ddx1(g, Pf, Nf[i], false);
+        else if (i == 1) op_ddx2(g, Pf, Nf[i], false);
+        else op_ddx3(g, Pf, Nf[i], false);
+        const cd* Qi = pb.Q[i].data();
+        for (long x = 0; x < nr; ++x) Rf[i][x] = lambda * U[i][x] + pb.nu * Rf[i][x] - Nf[i][x] + weight * Qi[x];
+    }
+    for (int n = 0; n < g.Ny; ++n) Rf[0][n * S] += 2 * pb.nu * pb.basecurv[n];
+    Rf[0][0] -= old[0];
+    Rf[2][0] -= old[1];
+    const cd* Rc[3] = {Rf[0], Rf[1], Rf[2]};
+    pb.stokes[j].solve(g, U, Pf, Rc, pb.cmode, pb.c1, pb.c2, pb.basemean, gradients);
+}
+
+// step! (cnrk2.jl:567-625).  Returns the last stage's gradients in grads.
+static void cnrk2_step(Problem& pb, cd* const U[3], cd* Pf, double* grads) {
+    double gradients[2] = {pb.cmode == 0 ? pb.c1 : 0.0, pb.cmode == 0 ? pb.c2 : 0.0};
+    for (int j = 0; j < 3; ++j) cnrk2_stage(pb, U, Pf, j, gradients);
     grads[0] = gradients[0];
     grads[1] = gradients[1];
 }
@@ -1061,6 +1069,7 @@ void or_set_threads(int n) {
 #endif
 }
 int or_get_threads() { return nthreads(); }
+void or_set_sample_div(long d) { g_sample_div = d > 1 ? d : 1; }
 void or_set_helmholtz_method(int method, int dense_max_ny) {
     g_helm_method = method;
     if (dense_max_ny > 0) g_dense_max_ny = dense_max_ny;
@@ -1163,6 +1172,17 @@ int or_step(void* h, double* U, double* P, int nsteps, double* grads) {
     cd* Uc = reinterpret_cast<cd*>(U);
     cd* Uf[3] = {Uc, Uc + nr, Uc + 2 * nr};
     for (int s = 0; s < nsteps; ++s) cnrk2_step(*pb, Uf, reinterpret_cast<cd*>(P), grads);
+    return 0;
+}
+// one stage j of a step (a bounded sample of the step's work)
+int or_stage(void* h, double* U, double* P, int j) {
+    auto* pb = static_cast<Problem*>(h);
+    if (!problem_stokes(*pb)) { set_error("singular influence matrix"); return -2; }
+    const long nr = pb->g.nr();
+    cd* Uc = reinterpret_cast<cd*>(U);
+    cd* Uf[3] = {Uc, Uc + nr, Uc + 2 * nr};
+    double gr[2] = {pb->cmode == 0 ? pb->c1 : 0.0, pb->cmode == 0 ? pb->c2 : 0.0};
+    cnrk2_stage(*pb, Uf, reinterpret_cast<cd*>(P), j, gr);
     return 0;
 }
 void or_nonlinear(void* h, const double* U, double* N) {

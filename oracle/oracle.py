@@ -43,6 +43,7 @@ def lib():
             getattr(L, name).argtypes = [ctypes.c_void_p]
         L.or_step.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int, _D]
         L.or_nonlinear.argtypes = [ctypes.c_void_p, _D, _D]
+        L.or_stage.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int]
         L.or_inverse.argtypes = [ctypes.c_void_p, _D, _D]
         L.or_forward.argtypes = [ctypes.c_void_p, _D, _D]
         L.or_operator.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, ctypes.c_int]
@@ -67,6 +68,7 @@ def lib():
         L.or_mean_solve.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_double, ctypes.c_double] + [_D] * 8
         L.or_set_threads.argtypes = [ctypes.c_int]
+        L.or_set_sample_div.argtypes = [ctypes.c_long]
         L.or_get_threads.restype = ctypes.c_int
         L.or_set_helmholtz_method.argtypes = [ctypes.c_int, ctypes.c_int]
         _lib = L
@@ -88,6 +90,11 @@ def set_threads(n):
 
 def get_threads():
     return lib().or_get_threads()
+
+
+def set_sample_div(d):
+    """Timing only: every independent loop of a stage runs over 1/d of its range."""
+    lib().or_set_sample_div(int(d))
 
 
 def set_helmholtz_method(method, dense_max_ny=0):
@@ -225,6 +232,12 @@ class OracleProblem:
         if rc != 0:
             raise ValueError(_err())
         return tuple(g)
+
+    def stage(self, U, P, j):
+        """One CNRK2 stage j in place (a bounded sample of a step's work)."""
+        rc = lib().or_stage(self._h, _p(U.view(np.float64)), _p(P.view(np.float64)), int(j))
+        if rc != 0:
+            raise ValueError(_err())
 
     def nonlinear(self, U):
         U = np.ascontiguousarray(U, dtype=np.complex128)

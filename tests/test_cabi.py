@@ -1,0 +1,39 @@
+"""C-ABI checks that need no GPU: the library loads, every function declared
+in include/cfb200.h is exported, and calls fail cleanly without a device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import cfb200
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    src = open(os.path.join(ROOT, "include", "cfb200.h")).read()
+    return sorted(set(re.findall(r"\b(cf_[a-z_]+)\s*\(", src)))
+
+
+def test_header_matches_python_binding():
+    assert sorted(cfb200.EXPORTS) == [n for n in declared() if n in cfb200.EXPORTS]
+    assert set(declared()) <= set(cfb200.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    L = cfb200.lib()
+    for name in declared():
+        assert hasattr(L, name), name
+
+
+def test_errors_are_reported_not_crashed():
+    # argument validation happens before any device work (cnrk2.jl:478, stokes.jl:345)
+    with pytest.raises(cfb200.CFError) as e:
+        cfb200.CouetteFlow(cfb200.Grid(8, 10, 8, 6.28, 6.28), 0.01, 0.01)
+    assert e.value.code == -1 and "odd Ny" in str(e.value)
+    with pytest.raises(cfb200.CFError):
+        cfb200.CouetteFlow(cfb200.Grid(8, 9, 8, 6.28, 6.28), 0.01, 0.0)
+    with pytest.raises(ValueError):
+        cfb200.ChannelFlowProblem(cfb200.Grid(8, 9, 8, 6.28, 6.28), "couette", 0.01, 0.01,
+                                  pressuregradient=(0, 0), bulkvelocity=(0, 0))
