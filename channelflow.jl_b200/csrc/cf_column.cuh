@@ -1,6 +1,9 @@
 // cf_column.cuh -- per-column (one Fourier pair (k,l), all Chebyshev degrees)
-// device building blocks.  One warp owns one column; the column's vectors
-// live in shared memory.  All routines are warp-synchronous.
+// device building blocks.  A team of two warps owns one column: warp q holds
+// the degrees of parity q.  A column vector lives in shared memory split by
+// parity, degree n at position (n & 1) * hs + (n >> 1) with hs = P/2 + 1, so
+// each parity is a contiguous half and the recurrences below (which couple
+// degrees of one parity only) run inside one warp.
 //
 // Reference arithmetic restated here:
 //  * Chebyshev derivative recurrence b_n = b_{n+2} + 2(n+1) a_{n+1}, b_0
@@ -10,185 +13,302 @@
 //    (docs/src/spatial.md:448-475), in its quasi-tridiagonal (spectral
 //    integration) form: for n >= 2 of each parity
 //       s_n a_{n-2} + d_n a_n + u_n a_{n+2} = g_n,
-//    eliminated from the top degree downwards.  The two linear sweeps are
-//    parallel prefix scans of affine maps; the wall row is reduced with the
-//    precomputed weights W (see cf_setup.cpp).
+//    eliminated from the top degree downwards (a_n = alpha_n a_{n-2} + beta_n);
+//    the two linear sweeps are prefix scans of affine maps and the wall row is
+//    reduced with precomputed weights W_n (factors from the engine set-up).
 //  * DCT-I (FFTW REDFT00, src/transforms/chebyshev.jl:481-502) of a complex
 //    column of length P+1 through one complex FFT of length P.
+//
+// Chains of one parity are scanned in runs: each lane takes E consecutive
+// chain elements (E odd, so the stride-E shared-memory accesses of a warp hit
+// distinct bank groups) and the runs are combined by a warp scan.
 #pragma once
 #include "cf_common.cuh"
 #include "cf_fft.cuh"
 
-#define CF_WARP_FFT_MAXE 16
-#define CF_HELM_MAXR 8  // chain rounds of 32: supports P <= 510
+#define CF_TEAM 64  // threads per column
 
-// b = D a  (b != a), column of Ny = P+1 complex coefficients
-CF_DEV void col_diff(const zd* a, zd* b, int P, int lane) {
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        const int top = ((P & 1) == q) ? P : P - 1;
-        const int cnt = (top - q) / 2 + 1;  // m = top, top-2, ..., q
-        zd carry = zzero();
-        for (int base = 0; base < cnt; base += 32) {
-            const int i = base + lane;
-            const int m = top - 2 * i;
-            zd val = zzero();
-            if (i < cnt && m >= 1) val = zscale(a[m], (double)m);
-            zd s = zadd(warp_scan_z(val, lane), carry);
-            if (i < cnt && m >= 1) b[m - 1] = (m == 1) ? s : zscale(s, 2.0);
-            carry = shfl_z(s, 31);
+// The two warps of one column.  Every routine below is called by all 64
+// threads of the team and ends with the team's barrier, after which all of its
+// outputs are visible to both warps.
+struct Team {
+    int q;     // parity owned by this warp (warp index in the team)
+    int lane;  // lane in the warp
+    int tid;   // 0..63
+    int bar;   // named barrier of the team (1 or 2)
+    int P;     // highest degree (even)
+    int hs;    // half stride: P/2 + 1
+    zd* xch;   // two complex of team scratch in shared memory
+};
+
+// Team barrier.  The ids are literal (a run-time id makes the compiler reserve
+// all sixteen barriers of the block, which limits blocks per SM).
+CF_DEV void tsync(const Team& t) {
+    if (t.bar == 1) asm volatile("bar.sync 1, 64;" ::: "memory");
+    else asm volatile("bar.sync 2, 64;" ::: "memory");
+}
+// shared-memory position of degree (or node) n
+CF_DEV int ppos(int n, int hs) { return (n & 1) * hs + (n >> 1); }
+// number of degrees of parity q in 0..P (P even)
+CF_DEV int pcount(int q, int P) { return q ? (P >> 1) : (P >> 1) + 1; }
+
+// Both warps obtain the warp-uniform value v of each warp: a from warp 0, b
+// from warp 1.
+CF_DEV void team_xchg(const Team& t, zd v, zd& a, zd& b) {
+    if (t.lane == 0) t.xch[t.q] = v;
+    tsync(t);
+    a = t.xch[0];
+    b = t.xch[1];
+    tsync(t);
+}
+
+// Exclusive form of an inclusive warp scan result.
+CF_DEV zd warp_excl_z(zd inc, int lane) {
+    zd o = shfl_up_z(inc, 1);
+    return lane == 0 ? zzero() : o;
+}
+
+// b = D a  (b != a).  Warp q writes the degrees of parity q of b from the
+// degrees of parity 1-q of a; b_P = 0.
+CF_DEV void col_diff(const zd* a, zd* b, const Team& t) {
+    const int P = t.P, hs = t.hs, q = t.q, lane = t.lane;
+    const int pin = 1 - q;                 // parity of the input chain
+    const int top = pin ? P - 1 : P;       // m = top, top-2, ..., pin
+    const int cnt = (top - pin) / 2 + 1;
+    const zd* ah = a + pin * hs;           // a_m at ah[m >> 1]
+    zd* bh = b + q * hs;                   // b_n at bh[n >> 1]
+    const int E = ((cnt + 31) >> 5) | 1;
+    const int i0 = lane * E;
+    zd tot = zzero();
+    for (int s = 0; s < E; ++s) {
+        const int i = i0 + s;
+        const int m = top - 2 * i;
+        if (i < cnt && m >= 1) tot = zaxpy(tot, (double)m, ah[m >> 1]);
+    }
+    zd run = warp_excl_z(warp_scan_z(tot, lane), lane);
+    for (int s = 0; s < E; ++s) {
+        const int i = i0 + s;
+        const int m = top - 2 * i;
+        if (i < cnt && m >= 1) {
+            run = zaxpy(run, (double)m, ah[m >> 1]);
+            bh[(m - 1) >> 1] = (m == 1) ? run : zscale(run, 2.0);
         }
     }
-    if (lane == 0) b[P] = zzero();
+    if (q == 0 && lane == 0) bh[P >> 1] = zzero();
+    tsync(t);
+}
+
+// Warp q copies the parity-q entries of `rows` rows of Ny doubles (global,
+// natural order, row stride Ny) into shared memory in the parity layout (row
+// stride 2*hs).  Only warp q reads them afterwards, so a warp barrier suffices.
+CF_DEV void col_stage_rows(double* dst, const double* __restrict__ src, int rows, const Team& t) {
+    const int P = t.P, Ny = P + 1, hs = t.hs, q = t.q;
+    const int nq = pcount(q, P);
+    for (int r = 0; r < rows; ++r) {
+        double v[8];
+        for (int base = t.lane; base < nq; base += 8 * 32) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int j = base + 32 * u;
+                v[u] = j < nq ? __ldg(src + (long)r * Ny + 2 * j + q) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int j = base + 32 * u;
+                if (j < nq) dst[r * 2 * hs + q * hs + j] = v[u];
+            }
+        }
+    }
     __syncwarp();
 }
 
-// In-place tau Helmholtz solve on x (input f, output a).  fac points at the
-// column's factors: alpha[Ny], invden[Ny], W[Ny]; SA0/SA1 are the wall-row
-// sums of the even/odd parity; bc0/bc1 the parity wall data.
-CF_DEV void col_helm(zd* x, const double* __restrict__ fac, double SA0, double SA1, double th1, int P, zd bc0,
-                     zd bc1, int lane) {
-    const int Ny = P + 1;
-    const double* alpha = fac;
-    const double* invden = fac + Ny;
-    const double* W = fac + 2 * Ny;
-#pragma unroll 1
-    for (int par = 0; par < 2; ++par) {
-        const int top = ((P & 1) == par) ? P : P - 1;
-        const int cnt = (top - par) / 2;  // chain n = top, top-2, ..., par+2
-        // g_n from f (all values read before any write)
-        zd g[CF_HELM_MAXR];
-#pragma unroll
-        for (int r = 0; r < CF_HELM_MAXR; ++r) {
-            const int i = r * 32 + lane;
-            g[r] = zzero();
-            if (i < cnt) {
-                const int n = top - 2 * i;
-                const double cm = (n - 2 == 0) ? 2.0 : 1.0;
-                zd v = zscale(x[n - 2], cm / (4.0 * n * (n - 1)));
-                if (n <= P - 2) v = zaxpy(v, -1.0 / (2.0 * ((double)n * n - 1.0)), x[n]);
-                if (n + 2 <= P - 2) v = zaxpy(v, 1.0 / (4.0 * n * (n + 1)), x[n + 2]);
-                g[r] = v;
-            }
-        }
-        __syncwarp();
-        // backward sweep beta_n = invden_n (g_n - u_n beta_{n+2}), u_n = -th1/(4n(n+1))
-        zd carry = zzero();
-        zd sw = zzero();
-#pragma unroll
-        for (int r = 0; r < CF_HELM_MAXR; ++r) {
-            const int base = r * 32;
-            if (base >= cnt) break;
-            const int i = base + lane;
-            double M = 1.0;
-            zd G = zzero();
-            int n = 0;
-            if (i < cnt) {
-                n = top - 2 * i;
-                const double id = __ldg(invden + n);
-                G = zscale(g[r], id);
-                M = (n + 2 <= P - 2) ? th1 / (4.0 * n * (n + 1)) * id : 0.0;
-            }
-            warp_scan_affine(M, G, lane);
-            zd beta = zaxpy(G, M, carry);
-            if (i < cnt) {
-                x[n] = beta;
-                sw = zaxpy(sw, __ldg(W + n), beta);
-            }
-            carry = shfl_z(beta, 31);
-        }
-        sw = warp_sum_z(sw);
-        const double SA = par ? SA1 : SA0;
-        const zd bc = par ? bc1 : bc0;
-        const zd a0 = zscale(zsub(bc, sw), 1.0 / SA);
-        __syncwarp();
-        // forward sweep a_n = alpha_n a_{n-2} + beta_n
-        carry = a0;
-#pragma unroll
-        for (int r = 0; r < CF_HELM_MAXR; ++r) {
-            const int base = r * 32;
-            if (base >= cnt) break;
-            const int j = base + lane;
-            double M = 1.0;
-            zd G = zzero();
-            int n = 0;
-            if (j < cnt) {
-                n = par + 2 + 2 * j;
-                M = __ldg(alpha + n);
-                G = x[n];
-            }
-            warp_scan_affine(M, G, lane);
-            zd a = zaxpy(G, M, carry);
-            __syncwarp();
-            if (j < cnt) x[n] = a;
-            carry = shfl_z(a, 31);
-        }
-        if (lane == 0) x[par] = a0;
-        __syncwarp();
-    }
+// g_n of the integrated tau equation (n >= 2) from the right-hand side f
+// (parity half fh, f_m at fh[m >> 1]).  gt holds the degree-only coefficients:
+//   gt[n] = c_{n-2}/(4n(n-1)),  gt[Ny+n] = -[n<=P-2]/(2(n^2-1)),
+//   gt[2Ny+n] = [n+2<=P-2]/(4n(n+1))   (c_0 = 2, c_m = 1 otherwise).
+CF_DEV zd helm_g(const zd* fh, const double* __restrict__ gt, int n, int P) {
+    const int Ny = P + 1, j = n >> 1;
+    zd v = zscale(fh[j - 1], __ldg(gt + n));
+    if (n <= P - 2) v = zaxpy(v, __ldg(gt + Ny + n), fh[j]);
+    if (n + 2 <= P - 2) v = zaxpy(v, __ldg(gt + 2 * Ny + n), fh[j + 1]);
+    return v;
 }
 
-// DCT-I (REDFT00, unnormalised) of complex x[0..P] in place; z is P complex
-// of scratch.  X_k = x_0 + (-1)^k x_P + 2 sum_{n=1}^{P-1} x_n cos(pi n k/P).
-// With z_n = (x_n + x_{P-n})/2 - sin(pi n/P)(x_n - x_{P-n}) and Z = FFT_P(z):
+// Tau Helmholtz solve: x holds f on entry and a on exit; scr (distinct) holds
+// the intermediate beta.  alpha, invden, W are the column's elimination
+// factors in the parity layout (shared memory, staged by col_stage_rows);
+// SA0/SA1 and bc0/bc1 are the wall-row sums and data of the two parities.
+// Warp q solves the parity-q system alone.
+CF_DEV void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
+                     const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
+                     const Team& t) {
+    const int P = t.P, Ny = P + 1, q = t.q, lane = t.lane, hs = t.hs;
+    const int top = q ? P - 1 : P;
+    const int cnt = (top - q) / 2;  // backward chain n = top, top-2, ..., q+2
+    const int E = ((cnt + 31) >> 5) | 1;
+    const int i0 = lane * E;
+    zd* xh = x + q * hs;
+    zd* sh = scr + q * hs;
+    const double* ah = alpha + q * hs;
+    const double* ih = invden + q * hs;
+    const double* wh = W + q * hs;
+    // backward sweep beta_n = invden_n (g_n - u_n beta_{n+2}) as maps G + M x
+    double Mc = 1.0;
+    zd Gc = zzero();
+    for (int s = 0; s < E; ++s) {
+        const int i = i0 + s;
+        if (i < cnt) {
+            const int n = top - 2 * i;
+            const double id = ih[n >> 1];
+            const double M = th1 * __ldg(gt + 2 * Ny + n) * id;
+            Gc = zaxpy(zscale(helm_g(xh, gt, n, P), id), M, Gc);
+            Mc *= M;
+        }
+    }
+    warp_scan_affine(Mc, Gc, lane);
+    zd xv = warp_excl_z(Gc, lane);
+    zd sw = zzero();
+    for (int s = 0; s < E; ++s) {
+        const int i = i0 + s;
+        if (i < cnt) {
+            const int n = top - 2 * i;
+            const double id = ih[n >> 1];
+            const double M = th1 * __ldg(gt + 2 * Ny + n) * id;
+            xv = zaxpy(zscale(helm_g(xh, gt, n, P), id), M, xv);
+            sh[n >> 1] = xv;
+            sw = zaxpy(sw, wh[n >> 1], xv);
+        }
+    }
+    sw = warp_sum_z(sw);
+    const zd a0 = zscale(zsub(q ? bc1 : bc0, sw), 1.0 / (q ? SA1 : SA0));
+    __syncwarp();
+    // forward sweep a_n = alpha_n a_{n-2} + beta_n, chain n = q+2, q+4, ..., top
+    Mc = 1.0;
+    Gc = zzero();
+    for (int s = 0; s < E; ++s) {
+        const int jj = i0 + s;
+        if (jj < cnt) {
+            const int j = jj + 1;  // n = q + 2 j
+            const double M = ah[j];
+            Gc = zaxpy(sh[j], M, Gc);
+            Mc *= M;
+        }
+    }
+    warp_scan_affine(Mc, Gc, lane);
+    const double Me = __shfl_up_sync(0xffffffffu, Mc, 1);
+    const zd Ge = warp_excl_z(Gc, lane);
+    xv = (lane == 0) ? a0 : zaxpy(Ge, Me, a0);
+    for (int s = 0; s < E; ++s) {
+        const int jj = i0 + s;
+        if (jj < cnt) {
+            const int j = jj + 1;
+            xv = zaxpy(sh[j], ah[j], xv);
+            xh[j] = xv;
+        }
+    }
+    if (lane == 0) xh[0] = a0;
+    tsync(t);
+}
+
+// DCT-I (REDFT00) of complex x[0..P] in place (parity layout).  z and z2 are
+// transform buffers of round_up(P, 8) complex (swizzled positions).
+// X_k = x_0 + (-1)^k x_P + 2 sum_{n=1}^{P-1} x_n cos(pi n k/P).  With
+// z_n = (x_n + x_{P-n})/2 - sin(pi n/P)(x_n - x_{P-n}) and Z = FFT_P(z):
 //   X_{2m} = Z_m + Z_{P-m},  X_1 = x_0 - x_P + 2 sum_{n=1}^{P-1} x_n cos(pi n/P),
 //   X_{2m+1} = X_{2m-1} + i (Z_m - Z_{P-m}).
-// cs[n] = (cos(pi n/P), sin(pi n/P)), n = 0..P.  P must be even.
-CF_DEV void col_redft00(zd* x, zd* z, const zd* __restrict__ cs, const FftPlan& pl, int P, int lane) {
-    const int H = P >> 1;
+// cs[n] = (cos(pi n/P), sin(pi n/P)), n = 0..P.  P must be even.  After the
+// FFT, warp 0 writes the even outputs and warp 1 scans the odd ones.
+// MODE 1 (forward transform of nodal values, ffts.jl:189-206 with
+// normalize_forward! :378-393): every output times `scale`, X_0 and X_P also
+// halved.  MODE 2 (inverse, icheb with doubled endpoints and the 1/2 of
+// copy_to_padded!, ffts.jl:282-287): 0.5 * DCT of x with x_0, x_P doubled.
+// Both are folded into the z staging (the transform is linear).
+#define CF_DCT_FWD 1
+#define CF_DCT_INV 2
+template <int PL, int MODE>
+CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const FftPlan& pl, double scale,
+                        const Team& t) {
+    const int P = t.P, H = P >> 1, hs = t.hs;
+    // weights of the end terms (n = 0) and of the interior terms
+    const double we = (MODE == CF_DCT_FWD) ? scale : 1.0;
+    const double wi = (MODE == CF_DCT_FWD) ? scale : (MODE == CF_DCT_INV ? 0.5 : 1.0);
     zd x1 = zzero();
-    for (int n = lane; n <= H; n += 32) {
+    for (int n = t.tid; n <= H; n += CF_TEAM) {
         if (n == 0) {
-            zd a = x[0], b = x[P];
-            z[0] = zscale(zadd(a, b), 0.5);
-            x1 = zadd(x1, zsub(a, b));
+            zd a = x[0], b = x[ppos(P, hs)];
+            z[swz(0)] = zscale(zadd(a, b), 0.5 * we);
+            x1 = zaxpy(x1, we, zsub(a, b));
         } else if (n == H) {
-            z[H] = x[H];
+            z[swz(H)] = zscale(x[ppos(H, hs)], wi);
         } else {
-            zd a = x[n], b = x[P - n];
+            zd a = x[ppos(n, hs)], b = x[ppos(P - n, hs)];
             zd c = __ldg(cs + n);
-            zd h = zscale(zadd(a, b), 0.5), d = zsub(a, b);
-            z[n] = zaxpy(h, -c.y, d);
-            z[P - n] = zaxpy(h, c.y, d);
+            zd h = zscale(zadd(a, b), 0.5 * wi), d = zscale(zsub(a, b), wi);
+            z[swz(n)] = zaxpy(h, -c.y, d);
+            z[swz(P - n)] = zaxpy(h, c.y, d);
             x1 = zaxpy(x1, 2.0 * c.x, d);
         }
     }
     x1 = warp_sum_z(x1);
-    __syncwarp();
-    group_fft<false, CF_WARP_FFT_MAXE>(z, 1, P, pl, -1, lane, 32);
-    // odd outputs: prefix sums of i (Z_m - Z_{P-m}), m = 1..H-1
-    zd carry = x1;
-    for (int base = 0; base < H; base += 32) {
-        const int m = base + lane;
-        zd o = zzero();
-        if (m >= 1 && m < H) o = zmuli(zsub(z[m], z[P - m]));
-        zd s = zadd(warp_scan_z(o, lane), carry);
-        if (m < H) x[2 * m + 1] = s;
-        carry = shfl_z(s, 31);
+    if (t.lane == 0) t.xch[t.q] = x1;
+    tsync(t);
+    x1 = zadd(t.xch[0], t.xch[1]);
+    const zd* Z = group_fft_L<true, PL>(z, z2, 1, (P + 7) & ~7, pl, -1, t.tid, CF_TEAM, t.bar);
+    if (t.q == 1) {
+        // odd outputs X_{2m+1}, m = 0..H-1: X_1 plus prefix sums of
+        // i (Z_m - Z_{P-m}), in runs of E (odd) consecutive m per lane
+        const int lane = t.lane;
+        const int E = ((H + 31) >> 5) | 1;
+        const int m0 = lane * E;
+        zd tot = zzero();
+        for (int s = 0; s < E; ++s) {
+            const int m = m0 + s;
+            if (m >= 1 && m < H) tot = zadd(tot, zmuli(zsub(Z[swz(m)], Z[swz(P - m)])));
+        }
+        zd run = zadd(x1, warp_excl_z(warp_scan_z(tot, lane), lane));
+        zd* xo = x + hs;  // X_{2m+1} at xo[m]
+        for (int s = 0; s < E; ++s) {
+            const int m = m0 + s;
+            if (m < H) {
+                if (m >= 1) run = zadd(run, zmuli(zsub(Z[swz(m)], Z[swz(P - m)])));
+                xo[m] = run;
+            }
+        }
+    } else {
+        for (int m = t.lane; m <= H; m += 32)
+            x[m] = (m == 0 || m == H) ? zscale(Z[swz(m)], MODE == CF_DCT_FWD ? 1.0 : 2.0)
+                                      : zadd(Z[swz(m)], Z[swz(P - m)]);
     }
-    for (int m = lane; m <= H; m += 32) {
-        x[2 * m] = (m == 0 || m == H) ? zscale(z[m], 2.0) : zadd(z[m], z[P - m]);
-    }
-    __syncwarp();
+    tsync(t);
 }
 
-// Mean over y (meanmode.jl:173-179): a0 + sum_{even n >= 2} a_n / (1 - n^2)
-CF_DEV zd col_bulkmean(const zd* a, int P, int lane) {
+// Mean over y (meanmode.jl:173-179): a0 + sum_{even n >= 2} a_n / (1 - n^2),
+// returned to both warps.
+CF_DEV zd col_bulkmean(const zd* a, const Team& t) {
     zd s = zzero();
-    for (int n = lane; n <= P; n += 32) {
-        if (n == 0) s = zadd(s, a[0]);
-        else if ((n & 1) == 0) s = zaxpy(s, 1.0 / (1.0 - (double)n * n), a[n]);
+    if (t.q == 0) {
+        for (int j = t.lane; j <= (t.P >> 1); j += 32) {
+            const double n = 2.0 * j;
+            s = (j == 0) ? zadd(s, a[0]) : zaxpy(s, 1.0 / (1.0 - n * n), a[j]);
+        }
+        s = warp_sum_z(s);
     }
-    return warp_sum_z(s);
+    zd m0, m1;
+    team_xchg(t, s, m0, m1);
+    return m0;
 }
-// a'(+1) = sum n^2 a_n ; a'(-1) = sum (-1)^(n+1) n^2 a_n
-CF_DEV void col_wallderiv(const zd* a, int P, int lane, zd& right, zd& left) {
-    zd r = zzero(), l = zzero();
-    for (int n = lane; n <= P; n += 32) {
-        double w = (double)n * n;
-        r = zaxpy(r, w, a[n]);
-        l = zaxpy(l, (n & 1) ? w : -w, a[n]);
+// a'(+1) = sum n^2 a_n ; a'(-1) = sum (-1)^(n+1) n^2 a_n, returned to both warps
+CF_DEV void col_wallderiv(const zd* a, const Team& t, zd& right, zd& left) {
+    const int q = t.q, nq = pcount(q, t.P);
+    const zd* ah = a + q * t.hs;
+    zd s = zzero();
+    for (int j = t.lane; j < nq; j += 32) {
+        const double n = 2.0 * j + q;
+        s = zaxpy(s, n * n, ah[j]);
     }
-    right = warp_sum_z(r);
-    left = warp_sum_z(l);
+    s = warp_sum_z(s);
+    zd s0, s1;
+    team_xchg(t, s, s0, s1);
+    right = zadd(s0, s1);
+    left = zsub(s1, s0);
 }

@@ -22,6 +22,15 @@ CF_DEV zd zmulis(zd a, double s) { return make_double2(-a.y * s, a.x * s); }
 CF_DEV zd zaxpy(zd a, double s, zd b) { return make_double2(fma(s, b.x, a.x), fma(s, b.y, a.y)); }
 CF_DEV zd zzero() { return make_double2(0.0, 0.0); }
 
+// ----------------------------------------------------------- L2 prefetch
+// Bring [p, p+bytes) into L2 (one request per 128-byte line, spread over the
+// calling threads) so that later dependent loads see L2 rather than HBM latency.
+CF_DEV void prefetch_l2(const void* p, long bytes, int tid, int nth) {
+    const char* c = (const char*)p;
+    for (long off = (long)tid * 128; off < bytes; off += (long)nth * 128)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(c + off));
+}
+
 // ------------------------------------------------------------- warp utils
 CF_DEV double shfl_up_d(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 CF_DEV double shfl_d(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }

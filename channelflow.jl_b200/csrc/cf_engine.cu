@@ -17,7 +17,56 @@
 #include "cf_fftkernels.cuh"
 #include "cf_kernels.cuh"
 
-#define CF_NCOL 4
+#define CF_NCOL 2
+static_assert(CF_NCOL == 1 || CF_NCOL == 2, "column teams use named barriers 1 and 2");
+
+// Kernel instantiations by size: the Chebyshev length P of the column kernels
+// and the padded lengths Nzp, Nxp of the periodic transforms have
+// compile-time versions for the grids of the supported workloads (index
+// arithmetic by constants, unrolled runs); other sizes use the run-time-sized
+// instantiation (template argument 0).
+typedef void (*ColKernel)(ColParams);
+typedef void (*FftKernel)(FftParams);
+enum { KC_STAGE, KC_PREP, KC_NLOUT, KC_PROJECT, KC_PRESSURE, KC_COUNT };
+enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_COUNT };
+#define CF_COL_LENGTHS(X) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384)
+
+template <int PT>
+static ColKernel col_kernel_t(int which) {
+    switch (which) {
+        case KC_STAGE: return k_column_stage<CF_NCOL, PT>;
+        case KC_PREP: return k_column_prep<CF_NCOL, PT>;
+        case KC_NLOUT: return k_column_nlout<CF_NCOL, PT>;
+        case KC_PROJECT: return k_column_project<CF_NCOL, PT>;
+        default: return k_column_pressure<CF_NCOL, PT>;
+    }
+}
+static ColKernel col_kernel(int which, int P) {
+    switch (P) {
+#define CF_CASE(N) \
+    case N: return col_kernel_t<N>(which);
+        CF_COL_LENGTHS(CF_CASE)
+#undef CF_CASE
+        default: return col_kernel_t<0>(which);
+    }
+}
+template <int L>
+static FftKernel fft_kernel_t(int which) {
+    switch (which) {
+        case KF_ZINV: return k_zinv<L>;
+        case KF_ZFWD: return k_zfwd<L>;
+        default: return k_xpass<L>;
+    }
+}
+static FftKernel fft_kernel(int which, int L) {
+    switch (L) {
+#define CF_CASE(N) \
+    case N: return fft_kernel_t<N>(which);
+        CF_STATIC_FFT_LENGTHS(CF_CASE)
+#undef CF_CASE
+        default: return fft_kernel_t<0>(which);
+    }
+}
 
 static thread_local std::string g_err;
 static int fail(int code, const std::string& msg) {
@@ -185,6 +234,7 @@ struct cf_engine {
     zd *tmpU = nullptr, *tmpP = nullptr;
     double *d_base = nullptr, *d_basecurv = nullptr, *d_grad = nullptr;
     zd *d_twP = nullptr, *d_twZ = nullptr, *d_twX = nullptr, *d_cs = nullptr;
+    double* d_helmtab = nullptr;
     FftPlan plP, plZ, plX;
     DevBank bank[3], proj, neum;
     bool nodal_valid = false;
@@ -216,14 +266,12 @@ static std::vector<int> fft_radices(int n) {
     return r;
 }
 
-// per-pass register check: ceil(nb*L/R / nth) * R <= maxe
-static bool plan_fits(const std::vector<int>& rad, int L, int nb, int nth, int maxe) {
-    for (int R : rad) {
+static int rup8(int x) { return (x + 7) & ~7; }
+
+// radices above 31 do not fit the packed plan (5 bits per pass)
+static bool radices_ok(const std::vector<int>& rad) {
+    for (int R : rad)
         if (R > 31) return false;
-        long bf = (long)nb * (L / R);
-        long per = (bf + nth - 1) / nth;
-        if (per * R > maxe) return false;
-    }
     return true;
 }
 
@@ -232,7 +280,8 @@ static int make_plan(cf_engine* h, int L, FftPlan& pl, zd** dtw) {
     if (rad.size() > CF_FFT_MAXPASS) return fail(CF_E_UNSUPPORTED, "FFT length has too many factors");
     pl.L = L;
     pl.np = (int)rad.size();
-    for (int i = 0; i < pl.np; ++i) pl.R[i] = rad[i];
+    pl.rcode = 0;
+    for (int i = 0; i < pl.np; ++i) pl.rcode |= (unsigned long long)rad[i] << (5 * i);
     std::vector<zd> tw(L);
     const long double twopi = 6.283185307179586476925286766559005768L;
     for (int k = 0; k < L; ++k) {
@@ -389,12 +438,19 @@ static int build_neumann(cf_engine* h) {
     return CF_OK;
 }
 
-static size_t col_smem(const cf_engine* h) { return (size_t)7 * CF_NCOL * (h->Ny + 1) * sizeof(zd); }
+// column stride (complex) in shared memory: a parity-split vector (2 (P/2 + 1)
+// entries) and a round_up(P, 8) transform buffer both fit
+static int col_stride(const cf_engine* h) { return std::max(h->P + 2, rup8(h->P)); }
+// 8 regions per column plus 2 complex of team scratch per column
+static size_t col_smem(const cf_engine* h) {
+    return ((size_t)8 * CF_NCOL * col_stride(h) + 2 * CF_NCOL) * sizeof(zd);
+}
 
 static ColParams col_params(const cf_engine* h) {
     ColParams p;
     std::memset(&p, 0, sizeof(p));
     p.Nx = h->Nx; p.Nz = h->Nz; p.Nxh = h->Nxh; p.Ny = h->Ny; p.P = h->P; p.B = (int)h->B;
+    p.cs = col_stride(h);
     p.ax = 2 * M_PI / h->Lx; p.bz = 2 * M_PI / h->Lz;
     p.nu = h->nu;
     for (int i = 0; i < 3; ++i) { p.U[i] = h->U[i]; p.Q[i] = h->Q[i]; p.Nn[i] = h->nod[i]; p.Nout[i] = nullptr; }
@@ -408,7 +464,8 @@ static ColParams col_params(const cf_engine* h) {
     else { p.c1 = h->c1; p.c2 = h->c2; }
     p.grad_out = h->d_grad;
     p.plP = h->plP;
-    p.cs = h->d_cs;
+    p.cs_tab = h->d_cs;
+    p.helm_tab = h->d_helmtab;
     p.fnorm = 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1));
     return p;
 }
@@ -417,7 +474,10 @@ static FftParams fft_params(const cf_engine* h) {
     FftParams f;
     f.Nx = h->Nx; f.Nz = h->Nz; f.Nxh = h->Nxh; f.Ny = h->Ny; f.Nzp = h->Nzp; f.Nxp = h->Nxp;
     f.tkz = h->tkz;
-    for (int i = 0; i < 6; ++i) { f.nod[i] = h->nod[i]; f.zp[i] = h->zp[i]; }
+    f.bsz = rup8(h->Nzp);
+    f.bsx = rup8(h->Nxp);
+    f.nod0 = h->nod[0]; f.nod1 = h->nod[1]; f.nod2 = h->nod[2]; f.nod3 = h->nod[3]; f.nod4 = h->nod[4]; f.nod5 = h->nod[5];
+    f.zp0 = h->zp[0]; f.zp1 = h->zp[1]; f.zp2 = h->zp[2]; f.zp3 = h->zp[3]; f.zp4 = h->zp[4]; f.zp5 = h->zp[5];
     f.plZ = h->plZ; f.plX = h->plX;
     return f;
 }
@@ -425,14 +485,14 @@ static FftParams fft_params(const cf_engine* h) {
 // nonlinear periodic transforms: nodal (6) -> nonlinear term at nodes (nod[0..2])
 static int launch_periodic(cf_engine* h, int* count) {
     FftParams f = fft_params(h);
-    const size_t smz = (size_t)h->tkz * h->Nzp * sizeof(zd);
-    const size_t smx = (size_t)6 * h->Nxp * sizeof(zd);
+    const size_t smz = (size_t)2 * h->tkz * rup8(h->Nzp) * sizeof(zd);
+    const size_t smx = (size_t)12 * rup8(h->Nxp) * sizeof(zd);
     dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
-    k_zinv<<<gz, 256, smz, h->stream>>>(f);
+    fft_kernel(KF_ZINV, h->Nzp)<<<gz, 256, smz, h->stream>>>(f);
     dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
-    k_xpass<<<gx, 256, smx, h->stream>>>(f);
+    fft_kernel(KF_XPASS, h->Nxp)<<<gx, 256, smx, h->stream>>>(f);
     dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
-    k_zfwd<<<gz3, 256, smz, h->stream>>>(f);
+    fft_kernel(KF_ZFWD, h->Nzp)<<<gz3, 256, smz, h->stream>>>(f);
     if (count) *count += 3;
     CU(cudaGetLastError());
     return CF_OK;
@@ -443,7 +503,7 @@ static unsigned col_blocks(const cf_engine* h) { return (unsigned)((h->B + CF_NC
 static int launch_prep(cf_engine* h, zd* const Usrc[3], int* count) {
     ColParams p = col_params(h);
     for (int i = 0; i < 3; ++i) p.U[i] = Usrc[i];
-    k_column_prep<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+    col_kernel(KC_PREP, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return CF_OK;
@@ -459,7 +519,7 @@ static int launch_stage(cf_engine* h, int j, int* count) {
     p.stage = j;
     p.store_q = (j < 2) ? 1 : 0;
     p.bank = h->bank[j].view();
-    k_column_stage<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+    col_kernel(KC_STAGE, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return CF_OK;
@@ -469,8 +529,8 @@ static int launch_stage(cf_engine* h, int j, int* count) {
 // xpass, zfwd, column) recorded on the handle's stream.
 static int launch_step_profiled(cf_engine* h, cudaEvent_t* ev, double* acc) {
     FftParams f = fft_params(h);
-    const size_t smz = (size_t)h->tkz * h->Nzp * sizeof(zd);
-    const size_t smx = (size_t)6 * h->Nxp * sizeof(zd);
+    const size_t smz = (size_t)2 * h->tkz * rup8(h->Nzp) * sizeof(zd);
+    const size_t smx = (size_t)12 * rup8(h->Nxp) * sizeof(zd);
     dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
     dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
     dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
@@ -483,13 +543,13 @@ static int launch_step_profiled(cf_engine* h, cudaEvent_t* ev, double* acc) {
         p.store_q = (j < 2) ? 1 : 0;
         p.bank = h->bank[j].view();
         CU(cudaEventRecord(ev[0], h->stream));
-        k_zinv<<<gz, 256, smz, h->stream>>>(f);
+        fft_kernel(KF_ZINV, h->Nzp)<<<gz, 256, smz, h->stream>>>(f);
         CU(cudaEventRecord(ev[1], h->stream));
-        k_xpass<<<gx, 256, smx, h->stream>>>(f);
+        fft_kernel(KF_XPASS, h->Nxp)<<<gx, 256, smx, h->stream>>>(f);
         CU(cudaEventRecord(ev[2], h->stream));
-        k_zfwd<<<gz3, 256, smz, h->stream>>>(f);
+        fft_kernel(KF_ZFWD, h->Nzp)<<<gz3, 256, smz, h->stream>>>(f);
         CU(cudaEventRecord(ev[3], h->stream));
-        k_column_stage<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+        col_kernel(KC_STAGE, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
         CU(cudaEventRecord(ev[4], h->stream));
         CU(cudaGetLastError());
         CU(cudaEventSynchronize(ev[4]));
@@ -535,17 +595,14 @@ static int build_graph(cf_engine* h) {
 
 static int set_attrs(cf_engine* h) {
     const int maxsm = 227 * 1024;
-    size_t need[3] = {col_smem(h), (size_t)h->tkz * h->Nzp * sizeof(zd), (size_t)6 * h->Nxp * sizeof(zd)};
+    size_t need[3] = {col_smem(h), (size_t)2 * h->tkz * rup8(h->Nzp) * sizeof(zd), (size_t)12 * rup8(h->Nxp) * sizeof(zd)};
     for (size_t x : need)
         if (x > (size_t)maxsm) return fail(CF_E_UNSUPPORTED, "grid too large for the shared-memory tiles");
-    CU(cudaFuncSetAttribute(k_column_stage<CF_NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
-    CU(cudaFuncSetAttribute(k_column_prep<CF_NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
-    CU(cudaFuncSetAttribute(k_column_nlout<CF_NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
-    CU(cudaFuncSetAttribute(k_column_project<CF_NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
-    CU(cudaFuncSetAttribute(k_column_pressure<CF_NCOL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
-    CU(cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[1]));
-    CU(cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[1]));
-    CU(cudaFuncSetAttribute(k_xpass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[2]));
+    for (int w = 0; w < KC_COUNT; ++w)
+        CU(cudaFuncSetAttribute(col_kernel(w, h->P), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
+    CU(cudaFuncSetAttribute(fft_kernel(KF_ZINV, h->Nzp), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[1]));
+    CU(cudaFuncSetAttribute(fft_kernel(KF_ZFWD, h->Nzp), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[1]));
+    CU(cudaFuncSetAttribute(fft_kernel(KF_XPASS, h->Nxp), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[2]));
     return CF_OK;
 }
 
@@ -567,16 +624,19 @@ static int validate_and_size(cf_engine* h, const cf_config* c) {
     h->B = (long)h->Nxh * h->Nz;
     h->nr = h->B * h->Ny;
     h->nq = (long)h->Nxh * h->Nzp * h->Ny;
-    if (h->P > 2 * 32 * CF_HELM_MAXR - 2) return fail(CF_E_UNSUPPORTED, "Ny too large for the column kernel");
+    if (col_smem(h) > (size_t)227 * 1024) return fail(CF_E_UNSUPPORTED, "Ny too large for the column kernel");
     std::vector<int> rP = fft_radices(h->P), rZ = fft_radices(h->Nzp), rX = fft_radices(h->Nxp);
-    if (!plan_fits(rP, h->P, 1, 32, CF_WARP_FFT_MAXE))
-        return fail(CF_E_UNSUPPORTED, "Chebyshev transform length not supported (prime factors <= 31, length <= 512)");
-    if (!plan_fits(rX, h->Nxp, 6, 256, CF_BLOCK_FFT_MAXE))
+    if (!radices_ok(rP) || rP.size() > CF_FFT_MAXPASS)
+        return fail(CF_E_UNSUPPORTED, "Chebyshev transform length not supported (prime factors <= 31)");
+    if (!radices_ok(rX) || rX.size() > CF_FFT_MAXPASS || (size_t)12 * rup8(h->Nxp) * 16 > 227 * 1024)
         return fail(CF_E_UNSUPPORTED, "padded x length not supported");
+    if (!radices_ok(rZ) || rZ.size() > CF_FFT_MAXPASS)
+        return fail(CF_E_UNSUPPORTED, "padded z length not supported");
+    // z kernels: two tkz x Nzp buffers; keep them near 74 KB (three blocks per SM)
     h->tkz = 0;
     for (int t : {8, 4, 2, 1})
-        if (plan_fits(rZ, h->Nzp, t, 256, CF_BLOCK_FFT_MAXE) && (size_t)t * h->Nzp * 16 <= 100 * 1024) { h->tkz = t; break; }
-    if (!h->tkz) return fail(CF_E_UNSUPPORTED, "padded z length not supported");
+        if ((size_t)2 * t * rup8(h->Nzp) * 16 <= 74 * 1024 || t == 1) { h->tkz = t; break; }
+    if ((size_t)2 * h->tkz * rup8(h->Nzp) * 16 > 227 * 1024) return fail(CF_E_UNSUPPORTED, "padded z length not supported");
     return CF_OK;
 }
 
@@ -651,6 +711,16 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
         }
         if ((rc = dalloc(h, (void**)&h->d_cs, sizeof(zd) * (h->P + 1)))) return bail(rc);
         cudaMemcpy(h->d_cs, cs.data(), sizeof(zd) * (h->P + 1), cudaMemcpyHostToDevice);
+        // degree coefficients of the integrated tau rows (see helm_g)
+        const int P = h->P, Ny = h->Ny;
+        std::vector<double> gt((size_t)3 * Ny, 0.0);
+        for (int n = 2; n <= P; ++n) {
+            gt[n] = (n == 2 ? 2.0 : 1.0) / (4.0 * n * (n - 1));
+            gt[Ny + n] = (n <= P - 2) ? -1.0 / (2.0 * ((double)n * n - 1.0)) : 0.0;
+            gt[2 * Ny + n] = (n + 2 <= P - 2) ? 1.0 / (4.0 * n * (n + 1)) : 0.0;
+        }
+        if ((rc = dalloc(h, (void**)&h->d_helmtab, sizeof(double) * gt.size()))) return bail(rc);
+        cudaMemcpy(h->d_helmtab, gt.data(), sizeof(double) * gt.size(), cudaMemcpyHostToDevice);
     }
     if ((rc = set_attrs(h))) return bail(rc);
     if ((rc = ensure_banks(h))) return bail(rc);
@@ -746,7 +816,7 @@ int cf_nonlinear(cf_handle* h, const double* U, double* N) {
     if ((rc = launch_periodic(h, nullptr))) return rc;
     ColParams p = col_params(h);
     for (int i = 0; i < 3; ++i) p.Nout[i] = Us[i];
-    k_column_nlout<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+    col_kernel(KC_NLOUT, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(N, h->tmpU, 3 * fr, cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
@@ -764,7 +834,7 @@ static int project_dev(cf_engine* h, zd* const Ud[3]) {
     else { p.cmode = 0; p.c1 = 0.0; p.c2 = 0.0; }
     double* gtmp = h->d_grad;
     p.grad_out = gtmp;
-    k_column_project<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+    col_kernel(KC_PROJECT, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     CU(cudaGetLastError());
     return CF_OK;
 }
@@ -778,7 +848,7 @@ static int pressure_dev(cf_engine* h, zd* const Ud[3], zd* Pout) {
     for (int i = 0; i < 3; ++i) p.U[i] = Ud[i];
     p.Pf = Pout;
     p.bank = h->neum.view();
-    k_column_pressure<CF_NCOL><<<col_blocks(h), CF_NCOL * 32, col_smem(h), h->stream>>>(p);
+    col_kernel(KC_PRESSURE, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     CU(cudaGetLastError());
     h->nodal_valid = false;
     return CF_OK;

@@ -5,26 +5,39 @@
 //   in  x[j + r*L/R]           (j in [0, L/R), r in [0, R))
 //   out y[(j/Ns)*Ns*R + j%Ns + r*Ns] = DFT_R(w^(r*(j%Ns)*L/(Ns*R)) x[...])_r
 // and after all passes the buffer holds the DFT in natural order.  Each pass
-// is done in place: every thread first loads the inputs of all butterflies
-// it owns into registers, the group synchronises, then results are stored.
+// ping-pongs between two shared-memory buffers.
 // tw[k] = exp(-2 pi i k / L); sgn = -1 forward, +1 backward (unnormalised).
 #pragma once
 #include "cf_common.cuh"
 
-#define CF_FFT_MAXPASS 16
+#define CF_FFT_MAXPASS 12
 
+// radices packed 5 bits each (pass p: (rcode >> 5p) & 31), so kernels never
+// index a parameter array at run time
 struct FftPlan {
     int L;
     int np;
-    int R[CF_FFT_MAXPASS];
+    unsigned long long rcode;
     const zd* tw;
 };
 
+// Barrier of the thread group: a warp, the whole block (bar == 0), or a
+// 64-thread team on named barrier 1 or 2 (literal ids: a run-time id makes the
+// compiler reserve all sixteen barriers of the block).
 template <bool BLOCK>
-CF_DEV void group_sync() {
-    if (BLOCK) __syncthreads();
-    else __syncwarp();
+CF_DEV void group_sync(int bar, int) {
+    if (!BLOCK) __syncwarp();
+    else if (bar == 1) asm volatile("bar.sync 1, 64;" ::: "memory");
+    else if (bar == 2) asm volatile("bar.sync 2, 64;" ::: "memory");
+    else __syncthreads();
 }
+
+// Shared-memory position of element e of a transform buffer.  The low three
+// bits are XOR-ed with bits 3-5 and 6-8, so the stride-R stores of a Stockham
+// pass (and the strided loads of the scans) spread over all eight 16-byte bank
+// groups.  A transform buffer must hold round_up(L, 8) elements (the swizzle
+// stays inside each aligned block of eight).
+CF_DEV int swz(int e) { return e ^ (((e >> 3) ^ (e >> 6)) & 7); }
 
 CF_DEV zd tw_get(const zd* tw, int k, int sgn) {
     zd w = __ldg(tw + k);
@@ -98,99 +111,215 @@ CF_DEV void dft_small<8>(zd* v, int sgn) {
     v[7] = zsub(e[3], w3o);
 }
 
-// One in-place pass of compile-time radix R over nb transforms of length L
-// (transform b starts at buf + b*bs).  MAXE bounds the complex registers per
-// thread: the caller guarantees ceil(nb*L/R / nth) * R <= MAXE.
-template <bool BLOCK, int R, int MAXE>
-CF_DEV void fft_pass_t(zd* buf, int nb, int bs, int L, int Ns, const zd* tw, int sgn, int tid, int nth) {
-    constexpr int MB = MAXE / R;
+// a * (c + i sgn s): multiply by exp(sgn i theta) given (cos theta, sin theta)
+CF_DEV zd zrot(zd a, double c, double s, int sgn) {
+    const double ss = sgn * s;
+    return zmake(a.x * c - a.y * ss, a.x * ss + a.y * c);
+}
+
+// radix 9 as 3 x 3: X[k1 + 3 k2] = sum_n2 w3^(n2 k2) w9^(n2 k1) sum_n1 x[3 n1 + n2] w3^(n1 k1)
+template <>
+CF_DEV void dft_small<9>(zd* v, int sgn) {
+    // cos, sin of 2 pi m / 9 for m = 1, 2, 4
+    const double c1 = 0.76604444311897803520, s1 = 0.64278760968653932632;
+    const double c2 = 0.17364817766693034885, s2 = 0.98480775301220805936;
+    const double c4 = -0.93969262078590838405, s4 = 0.34202014332566873304;
+    zd y[3][3];
+#pragma unroll
+    for (int n2 = 0; n2 < 3; ++n2) {
+        zd t[3] = {v[n2], v[3 + n2], v[6 + n2]};
+        dft_small<3>(t, sgn);
+        y[n2][0] = t[0];
+        y[n2][1] = t[1];
+        y[n2][2] = t[2];
+    }
+    // twiddles exp(sgn 2 pi i m / 9), m = n2 k1: (1,1) m=1, (1,2) m=2, (2,1) m=2, (2,2) m=4
+    y[1][1] = zrot(y[1][1], c1, s1, sgn);
+    y[1][2] = zrot(y[1][2], c2, s2, sgn);
+    y[2][1] = zrot(y[2][1], c2, s2, sgn);
+    y[2][2] = zrot(y[2][2], c4, s4, sgn);
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+        zd t[3] = {y[0][k1], y[1][k1], y[2][k1]};
+        dft_small<3>(t, sgn);
+        v[k1] = t[0];
+        v[k1 + 3] = t[1];
+        v[k1 + 6] = t[2];
+    }
+}
+
+// radix 16 as 4 x 4: X[k1 + 4 k2] = sum_n2 w4^(n2 k2) w16^(n2 k1) sum_n1 x[4 n1 + n2] w4^(n1 k1)
+template <>
+CF_DEV void dft_small<16>(zd* v, int sgn) {
+    // cos, sin of 2 pi m / 16 for m = 1, 2, 3
+    const double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;
+    const double c2 = 0.70710678118654752440, s2 = 0.70710678118654752440;
+    const double c3 = 0.38268343236508977173, s3 = 0.92387953251128675613;
+    zd y[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+        zd t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+        dft_small<4>(t, sgn);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) y[n2][k1] = t[k1];
+    }
+    // twiddles exp(sgn 2 pi i m / 16), m = n2 k1 in 1..9
+    y[1][1] = zrot(y[1][1], c1, s1, sgn);
+    y[1][2] = zrot(y[1][2], c2, s2, sgn);
+    y[1][3] = zrot(y[1][3], c3, s3, sgn);
+    y[2][1] = zrot(y[2][1], c2, s2, sgn);
+    y[2][2] = zscale(zmuli(y[2][2]), (double)sgn);  // m = 4: exp(sgn i pi/2)
+    y[2][3] = zrot(y[2][3], -c2, s2, sgn);          // m = 6: (cos, sin)(3pi/4) = (-c2, s2)
+    y[3][1] = zrot(y[3][1], c3, s3, sgn);
+    y[3][2] = zrot(y[3][2], -c2, s2, sgn);          // m = 6
+    y[3][3] = zrot(y[3][3], -c1, -s1, sgn);         // m = 9: (cos, sin)(9pi/8) = (-c1, -s1)
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        zd t[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+        dft_small<4>(t, sgn);
+        v[k1] = t[0];
+        v[k1 + 4] = t[1];
+        v[k1 + 8] = t[2];
+        v[k1 + 12] = t[3];
+    }
+}
+
+// One out-of-place Stockham pass of compile-time radix R over nb transforms of
+// length L (transform b at src + b*bs, written to dst + b*bs).  A thread keeps
+// one butterfly in registers at a time.
+template <bool BLOCK, int R>
+CF_DEV void fft_pass_pp(const zd* __restrict__ src, zd* __restrict__ dst, int nb, int bs, int L, int Ns,
+                        const zd* __restrict__ tw, int sgn, int tid, int nth, int bar) {
     const int NBf = L / R;
     const int total = nb * NBf;
     const int step = L / (Ns * R);
-    zd v[MB > 0 ? MB : 1][R];
+#pragma unroll 2
+    for (int q = tid; q < total; q += nth) {
+        const int b = q / NBf, j = q - b * NBf;
+        const int k = j % Ns;
+        const zd* s = src + (long)b * bs;
+        zd v[R];
 #pragma unroll
-    for (int t = 0; t < MB; ++t) {
-        int q = tid + t * nth;
-        if (q < total) {
-            int b = q / NBf, j = q - b * NBf;
-            int k = j % Ns;
-            const zd* src = buf + (long)b * bs;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                zd x = src[j + r * NBf];
-                v[t][r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
-            }
+        for (int r = 0; r < R; ++r) {
+            zd x = s[swz(j + r * NBf)];
+            v[r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
         }
-    }
-    group_sync<BLOCK>();
+        dft_small<R>(v, sgn);
+        zd* d = dst + (long)b * bs;
+        const int o = (j / Ns) * Ns * R + k;
 #pragma unroll
-    for (int t = 0; t < MB; ++t) {
-        int q = tid + t * nth;
-        if (q < total) {
-            int b = q / NBf, j = q - b * NBf;
-            int k = j % Ns;
-            dft_small<R>(v[t], sgn);
-            zd* dst = buf + (long)b * bs + (j / Ns) * Ns * R + k;
-#pragma unroll
-            for (int r = 0; r < R; ++r) dst[r * Ns] = v[t][r];
-        }
+        for (int r = 0; r < R; ++r) d[swz(o + r * Ns)] = v[r];
     }
-    group_sync<BLOCK>();
+    group_sync<BLOCK>(bar, nth);
 }
 
-// Generic odd prime radix (R <= 31): direct DFT; used only for sizes with
-// uncommon prime factors.  Same in-place protocol, registers in local memory.
-template <bool BLOCK, int MAXE>
-CF_DEV void fft_pass_generic(zd* buf, int nb, int bs, int L, int R, int Ns, const zd* tw, int sgn, int tid,
-                             int nth) {
+// Generic prime radix (R <= 31) by a direct DFT; only sizes with uncommon
+// prime factors take this path.
+template <bool BLOCK>
+CF_DEV void fft_pass_pp_generic(const zd* __restrict__ src, zd* __restrict__ dst, int nb, int bs, int L, int R,
+                                int Ns, const zd* __restrict__ tw, int sgn, int tid, int nth, int bar) {
     const int NBf = L / R;
     const int total = nb * NBf;
     const int step = L / (Ns * R);
-    const int mb = (total + nth - 1) / nth;
-    zd v[MAXE];
-    for (int t = 0; t < mb; ++t) {
-        int q = tid + t * nth;
-        if (q < total) {
-            int b = q / NBf, j = q - b * NBf;
-            int k = j % Ns;
-            const zd* src = buf + (long)b * bs;
+    for (int q = tid; q < total; q += nth) {
+        const int b = q / NBf, j = q - b * NBf;
+        const int k = j % Ns;
+        const zd* s = src + (long)b * bs;
+        zd* d = dst + (long)b * bs;
+        const int ob = (j / Ns) * Ns * R + k;
+        for (int o = 0; o < R; ++o) {
+            zd acc = zzero();
             for (int r = 0; r < R; ++r) {
-                zd x = src[j + r * NBf];
-                v[t * R + r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
+                zd x = s[swz(j + r * NBf)];
+                if (r != 0 && k != 0) x = zmul(x, tw_get(tw, k * r * step, sgn));
+                acc = zadd(acc, (r == 0) ? x : zmul(x, tw_get(tw, ((o * r) % R) * NBf, sgn)));
             }
+            d[swz(ob + o * Ns)] = acc;
         }
     }
-    group_sync<BLOCK>();
-    for (int t = 0; t < mb; ++t) {
-        int q = tid + t * nth;
-        if (q < total) {
-            int b = q / NBf, j = q - b * NBf;
-            int k = j % Ns;
-            zd* dst = buf + (long)b * bs + (j / Ns) * Ns * R + k;
-            for (int s = 0; s < R; ++s) {
-                zd acc = v[t * R];
-                for (int r = 1; r < R; ++r) acc = zadd(acc, zmul(v[t * R + r], tw_get(tw, ((s * r) % R) * NBf, sgn)));
-                dst[s * Ns] = acc;
-            }
-        }
-    }
-    group_sync<BLOCK>();
+    group_sync<BLOCK>(bar, nth);
 }
 
-// Full transform of nb batched sequences (length pl.L, batch stride bs).
-template <bool BLOCK, int MAXE>
-CF_DEV void group_fft(zd* buf, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth) {
+// Compile-time-sized pass: L, Ns and R are constants, so the batch/butterfly
+// index split and the twiddle indices need no run-time division.
+template <bool BLOCK, int L, int Ns, int R>
+CF_DEV void fft_pass_static(const zd* __restrict__ src, zd* __restrict__ dst, int nb, int bs,
+                            const zd* __restrict__ tw, int sgn, int tid, int nth, int bar) {
+    constexpr int NBf = L / R;
+    constexpr int step = L / (Ns * R);
+    const int total = nb * NBf;
+#pragma unroll 2
+    for (int q = tid; q < total; q += nth) {
+        const int b = q / NBf, j = q - b * NBf;
+        const int k = j % Ns;
+        const zd* s = src + (long)b * bs;
+        zd v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            zd x = s[swz(j + r * NBf)];
+            v[r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
+        }
+        dft_small<R>(v, sgn);
+        zd* d = dst + (long)b * bs;
+        const int o = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[swz(o + r * Ns)] = v[r];
+    }
+    group_sync<BLOCK>(bar, nth);
+}
+template <bool BLOCK, int L, int Ns, int R, int... Rest>
+CF_DEV zd* fft_static(zd* src, zd* dst, int nb, int bs, const zd* tw, int sgn, int tid, int nth, int bar) {
+    fft_pass_static<BLOCK, L, Ns, R>(src, dst, nb, bs, tw, sgn, tid, nth, bar);
+    if constexpr (sizeof...(Rest) == 0) {
+        return dst;
+    } else {
+        return fft_static<BLOCK, L, Ns * R, Rest...>(dst, src, nb, bs, tw, sgn, tid, nth, bar);
+    }
+}
+
+// Full transform of nb sequences (length pl.L, batch stride bs, a multiple of
+// 8, elements at swizzled positions b*bs + swz(e)) held in a; b is a scratch
+// buffer of the same size.  Returns the buffer with the result.
+template <bool BLOCK>
+CF_DEV zd* group_fft(zd* a, zd* b, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
     int Ns = 1;
+    zd* src = a;
+    zd* dst = b;
     for (int p = 0; p < pl.np; ++p) {
-        const int R = pl.R[p];
-        switch (R) {
-            case 2: fft_pass_t<BLOCK, 2, MAXE>(buf, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth); break;
-            case 3: fft_pass_t<BLOCK, 3, MAXE>(buf, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth); break;
-            case 4: fft_pass_t<BLOCK, 4, MAXE>(buf, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth); break;
-            case 5: fft_pass_t<BLOCK, 5, MAXE>(buf, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth); break;
-            case 8: fft_pass_t<BLOCK, 8, MAXE>(buf, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth); break;
-            default: fft_pass_generic<BLOCK, MAXE>(buf, nb, bs, pl.L, R, Ns, pl.tw, sgn, tid, nth); break;
-        }
+        const int R = (int)((pl.rcode >> (5 * p)) & 31ull);
+        if (R == 8) fft_pass_pp<BLOCK, 8>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
+        else if (R == 4) fft_pass_pp<BLOCK, 4>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
+        else if (R == 2) fft_pass_pp<BLOCK, 2>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
+        else if (R == 3) fft_pass_pp<BLOCK, 3>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
+        else if (R == 5) fft_pass_pp<BLOCK, 5>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
+        else fft_pass_pp_generic<BLOCK>(src, dst, nb, bs, pl.L, R, Ns, pl.tw, sgn, tid, nth, bar);
         Ns *= R;
+        zd* t = src;
+        src = dst;
+        dst = t;
     }
+    return src;
 }
+
+// Transform of compile-time length L (the sizes of the supported grids);
+// L == 0 selects the run-time plan.  The radix order of a static size need not
+// match pl.R: any factorisation indexes the same twiddle table.
+template <bool BLOCK, int L>
+CF_DEV zd* group_fft_L(zd* a, zd* b, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
+    if constexpr (L == 32) return fft_static<BLOCK, 32, 1, 8, 4>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 48) return fft_static<BLOCK, 48, 1, 8, 2, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 64) return fft_static<BLOCK, 64, 1, 8, 8>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 72) return fft_static<BLOCK, 72, 1, 8, 9>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 96) return fft_static<BLOCK, 96, 1, 8, 4, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 128) return fft_static<BLOCK, 128, 1, 8, 8, 2>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 192) return fft_static<BLOCK, 192, 1, 8, 8, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 256) return fft_static<BLOCK, 256, 1, 8, 8, 4>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 384) return fft_static<BLOCK, 384, 1, 8, 8, 2, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 512) return fft_static<BLOCK, 512, 1, 8, 8, 8>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 576) return fft_static<BLOCK, 576, 1, 8, 8, 9>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 768) return fft_static<BLOCK, 768, 1, 8, 8, 4, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else return group_fft<BLOCK>(a, b, nb, bs, pl, sgn, tid, nth, bar);
+}
+
+// Lengths with a compile-time instantiation (others run the generic plan).
+#define CF_STATIC_FFT_LENGTHS(X) X(32) X(48) X(64) X(72) X(96) X(128) X(192) X(256) X(384) X(512) X(576) X(768)

@@ -8,6 +8,11 @@
 //             corrections, mean mode, flux constraint), curl and inverse DCT
 //             of the new velocity and vorticity for the next stage.
 // Field storage: complex (Ny, Nz, Nxh), k fastest; z-padded (Ny, Nzp, Nxh).
+//
+// Column kernels: a block holds NCOL columns, one team of two warps each
+// (cf_column.cuh).  Shared memory: 8 regions x NCOL columns x cs complex (the
+// parity layout, cs >= max(P + 2, round_up(P, 8))), then 2 complex of team
+// scratch per column.
 #pragma once
 #include "cf_column.cuh"
 
@@ -24,6 +29,7 @@ struct BankDev {
 
 struct ColParams {
     int Nx, Nz, Nxh, Ny, P, B;
+    int cs;  // column stride in shared memory (complex)
     double ax, bz;  // 2 pi / Lx, 2 pi / Lz
     double nu;
     // stage constants
@@ -46,26 +52,92 @@ struct ColParams {
     double* grad_out;        // [2]
     double* status;          // [4] diagnostics scratch (unused by the hot path)
     FftPlan plP;
-    const zd* cs;  // (cos, sin)(pi n / P)
+    const zd* cs_tab;  // (cos, sin)(pi n / P)
+    const double* helm_tab;  // [3][Ny] degree coefficients of the integrated tau rows
     double fnorm;  // 1 / (Nxp Nzp (Ny-1))
 };
 
+// one of three pointers without indexing an array at run time
+template <class T>
+CF_DEV T* sel3(T* a, T* b, T* c, int i) {
+    return i == 0 ? a : (i == 1 ? b : c);
+}
+
+// Blocks per SM the column kernels are compiled for (bounds their registers):
+// at P >= 256 shared memory allows 6 columns per SM, so 168 registers; the
+// smaller sizes are held to 128 registers (8 or more columns per SM).
+template <int NCOL, int PL>
+constexpr int col_minblocks() {
+    return (PL == 0 || PL >= 256) ? 6 / NCOL : 8 / NCOL;
+}
+
+// Common set-up of a column kernel: the calling thread's team and column.
+template <int NCOL, int PL>
+struct ColCtx {
+    Team t;
+    int c0, c, ix, iz;
+    bool valid;
+    zd* smem;
+    int cs;
+    CF_DEV ColCtx(zd* sm, const ColParams& p) {
+        smem = sm;
+        cs = p.cs;
+        const int tm = threadIdx.x / CF_TEAM;
+        t.tid = threadIdx.x - tm * CF_TEAM;
+        t.q = t.tid >> 5;
+        t.lane = t.tid & 31;
+        t.bar = 1 + tm;
+        t.P = PL ? PL : p.P;
+        t.hs = (t.P >> 1) + 1;
+        t.xch = sm + (long)8 * NCOL * cs + 2 * tm;
+        c0 = blockIdx.x * NCOL;
+        c = c0 + tm;
+        valid = c < p.B;
+        ix = c % p.Nxh;
+        iz = c / p.Nxh;
+    }
+    // region r of the whole block / of this column
+    CF_DEV zd* reg(int r) const { return smem + (long)r * NCOL * cs; }
+    CF_DEV zd* col(int r) const { return smem + (long)(r * NCOL + (threadIdx.x / CF_TEAM)) * cs; }
+};
+
+// Tile of NCOL adjacent columns x Ny degrees into shared memory (column t at
+// sm + t*cs, parity layout).  Each thread issues up to 8 loads before storing
+// any of them, so the block keeps many requests in flight.
 template <int NCOL>
-CF_DEV void tile_load(zd* sm, int cs, const zd* __restrict__ g, int c0, const ColParams& p) {
+CF_DEV void tile_load(zd* sm, int cs, int hs, const zd* g, int c0, const ColParams& p) {
+    constexpr int NT = NCOL * CF_TEAM, K = 8;
     const int tot = p.Ny * NCOL;
-    for (int e = threadIdx.x; e < tot; e += NCOL * 32) {
-        const int n = e / NCOL, t = e - n * NCOL;
-        const int c = c0 + t;
-        sm[t * cs + n] = (c < p.B) ? g[(long)n * p.B + c] : zzero();
+    for (int base = threadIdx.x; base < tot; base += NT * K) {
+        zd v[K];
+#pragma unroll
+        for (int u = 0; u < K; ++u) {
+            const int e = base + u * NT;
+            const int n = e / NCOL, t = e - n * NCOL;
+            const int c = c0 + t;
+            v[u] = (e < tot && c < p.B) ? g[(long)n * p.B + c] : zzero();
+        }
+#pragma unroll
+        for (int u = 0; u < K; ++u) {
+            const int e = base + u * NT;
+            const int n = e / NCOL, t = e - n * NCOL;
+            if (e < tot) sm[t * cs + ppos(n, hs)] = v[u];
+        }
     }
 }
+// L2 prefetch of a tile's rows (one 32-byte row segment per degree)
 template <int NCOL>
-CF_DEV void tile_store(const zd* sm, int cs, zd* __restrict__ g, int c0, const ColParams& p) {
+CF_DEV void tile_prefetch(const zd* g, int c0, const ColParams& p) {
+    for (int n = threadIdx.x; n < p.Ny; n += NCOL * CF_TEAM)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(g + (long)n * p.B + c0));
+}
+template <int NCOL>
+CF_DEV void tile_store(const zd* sm, int cs, int hs, zd* __restrict__ g, int c0, const ColParams& p) {
     const int tot = p.Ny * NCOL;
-    for (int e = threadIdx.x; e < tot; e += NCOL * 32) {
+    for (int e = threadIdx.x; e < tot; e += NCOL * CF_TEAM) {
         const int n = e / NCOL, t = e - n * NCOL;
         const int c = c0 + t;
-        if (c < p.B) g[(long)n * p.B + c] = sm[t * cs + n];
+        if (c < p.B) g[(long)n * p.B + c] = sm[t * cs + ppos(n, hs)];
     }
 }
 
@@ -73,35 +145,38 @@ CF_DEV bool col_nyquist(const ColParams& p, int ix, int iz) {
     return ((p.Nx % 2 == 0) && ix == p.Nx / 2) || ((p.Nz % 2 == 0) && iz == p.Nz / 2);
 }
 
-// forward DCT of nodal values in x, normalisation, endpoint weights and
+// zero the column vector x (both parities)
+CF_DEV void col_zero(zd* x, const Team& t) {
+    for (int n = t.tid; n < 2 * t.hs; n += CF_TEAM) x[n] = zzero();
+}
+
+// forward DCT of nodal values in x with normalisation, endpoint weights and
 // Nyquist filter (ffts.jl:189-206, normalize_forward! :378-393)
-CF_DEV void col_forward_y(zd* x, zd* z, const ColParams& p, bool nyq, int lane) {
-    col_redft00(x, z, p.cs, p.plP, p.P, lane);
-    for (int n = lane; n <= p.P; n += 32) {
-        const double e = (n == 0 || n == p.P) ? 0.5 : 1.0;
-        x[n] = nyq ? zzero() : zscale(x[n], p.fnorm * e);
+template <int PL>
+CF_DEV void col_forward_y(zd* x, zd* z, zd* z2, const ColParams& p, bool nyq, const Team& t) {
+    if (nyq) {
+        col_zero(x, t);
+        tsync(t);
+    } else {
+        col_redft00<PL, CF_DCT_FWD>(x, z, z2, p.cs_tab, p.plP, p.fnorm, t);
     }
-    __syncwarp();
 }
 // inverse DCT: nodal values of the series (icheb with doubled endpoints, the
 // 1/2 of copy_to_padded!, ffts.jl:282-287)
-CF_DEV void col_inverse_y(zd* x, zd* z, const ColParams& p, int lane) {
-    if (lane == 0) {
-        x[0] = zscale(x[0], 2.0);
-        x[p.P] = zscale(x[p.P], 2.0);
-    }
-    __syncwarp();
-    col_redft00(x, z, p.cs, p.plP, p.P, lane);
-    for (int n = lane; n <= p.P; n += 32) x[n] = zscale(x[n], 0.5);
-    __syncwarp();
+template <int PL>
+CF_DEV void col_inverse_y(zd* x, zd* z, zd* z2, const ColParams& p, const Team& t) {
+    col_redft00<PL, CF_DCT_INV>(x, z, z2, p.cs_tab, p.plP, 1.0, t);
 }
 
 // Solve the Stokes problem of one column.  In: R0,R1,R2 (= Rx,Ry,Rz).
-// Out: u in R0, v in V, w in R2, p in PT.  A is scratch.  Returns the mean
-// gradients for the (0,0) column.
-CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, const ColParams& p, int c, int ix, int iz,
-                       int lane, double* gout) {
-    const int P = p.P, Ny = p.Ny;
+// Out: u in R0, v in V, w in R2, p in PT.  A is scratch; F0, F1 hold the
+// staged elimination factors.  Returns the mean gradients for the (0,0) column.
+template <int PL>
+CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd* F1, const ColParams& p, int c,
+                       int ix, int iz, const Team& t, double* gout) {
+    const int P = t.P, Ny = P + 1, q = t.q, lane = t.lane, hs = t.hs;
+    const int nq = pcount(q, P);
+    const int qo = q * hs;  // offset of this warp's half
     const BankDev& bk = p.bank;
     const double k = p.ax * ix;
     const double l = p.bz * (iz <= (p.Nz >> 1) ? iz : iz - p.Nz);
@@ -109,88 +184,111 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, const ColPa
     const double* sa = bk.sa + (long)c * 4;
     const double shift = __ldg(csc + 6);
     const double* fv = bk.fac_v + (long)c * 3 * Ny;
+    // elimination factors staged in shared memory (parity layout): alpha,
+    // invden in F0, W in F1
+    double* fa = reinterpret_cast<double*>(F0);
+    double* fi = fa + 2 * hs;
+    double* fw = reinterpret_cast<double*>(F1);
     if (c != 0) {
-        // r = D Ry + i k Rx + i l Rz ; pressure with zero wall values
-        col_diff(R1, PT, P, lane);
-        for (int n = lane; n <= P; n += 32) PT[n] = zadd(PT[n], zadd(zmulis(R0[n], k), zmulis(R2[n], l)));
-        __syncwarp();
-        col_helm(PT, bk.fac_p + (long)c * 3 * Ny, __ldg(sa + 0), __ldg(sa + 1), __ldg(csc + 7), P, zzero(), zzero(),
-                 lane);
-        // q = D p - Ry ; normal velocity
-        col_diff(PT, V, P, lane);
-        for (int n = lane; n <= P; n += 32) V[n] = zsub(V[n], R1[n]);
-        __syncwarp();
-        col_helm(V, fv, __ldg(sa + 2), __ldg(sa + 3), shift, P, zzero(), zzero(), lane);
-        // influence correction (batchedinfluence.jl:101-120)
-        zd up = zzero(), lo = zzero();
-        for (int n = lane; n <= P; n += 32) {
-            double t = (double)n * n;
-            up = zaxpy(up, -t, V[n]);
-            lo = zaxpy(lo, (n & 1) ? -t : t, V[n]);
+        // it = 0: pressure with zero wall values, (D^2 - kappa^2) p = D Ry + i k Rx + i l Rz
+        // it = 1: normal velocity, (nu D^2 - shift) v = D p - Ry
+#pragma unroll 1
+        for (int it = 0; it < 2; ++it) {
+            const double* fsrc = it ? fv : bk.fac_p + (long)c * 3 * Ny;
+            zd* x = it ? V : PT;
+            col_stage_rows(fa, fsrc, 2, t);
+            col_stage_rows(fw, fsrc + 2 * Ny, 1, t);
+            col_diff(it ? PT : R1, x, t);
+            for (int j = lane; j < nq; j += 32) {
+                const int o = qo + j;
+                x[o] = it ? zsub(x[o], R1[o]) : zadd(x[o], zadd(zmulis(R0[o], k), zmulis(R2[o], l)));
+            }
+            __syncwarp();
+            col_helm(x, A, fa, fi, fw, p.helm_tab, __ldg(sa + 2 * it), __ldg(sa + 2 * it + 1),
+                     it ? shift : __ldg(csc + 7), zzero(), zzero(), t);
         }
-        up = warp_sum_z(up);
-        lo = warp_sum_z(lo);
+        // influence correction (batchedinfluence.jl:101-120)
+        zd s = zzero();
+        for (int j = lane; j < nq; j += 32) {
+            const double n = 2.0 * j + q;
+            s = zaxpy(s, n * n, V[qo + j]);
+        }
+        zd s0, s1;
+        team_xchg(t, warp_sum_z(s), s0, s1);
+        // upper = -sum n^2 v_n, lower = sum (-1)^n n^2 v_n
+        const zd up = zscale(zadd(s0, s1), -1.0), lo = zsub(s0, s1);
         const double i00 = __ldg(csc + 0), i01 = __ldg(csc + 1), i10 = __ldg(csc + 2), i11 = __ldg(csc + 3);
         const zd dp = zaxpy(zscale(up, i00), i01, lo);
         const zd dm = zaxpy(zscale(up, i10), i11, lo);
         const double* rs = bk.resp + (long)c * 6 * Ny;
-        for (int n = lane; n <= P; n += 32) {
-            PT[n] = zaxpy(zaxpy(PT[n], __ldg(rs + n), dp), __ldg(rs + Ny + n), dm);
-            V[n] = zaxpy(zaxpy(V[n], __ldg(rs + 2 * Ny + n), dp), __ldg(rs + 3 * Ny + n), dm);
+        for (int j = lane; j < nq; j += 32) {
+            const int n = 2 * j + q, o = qo + j;
+            PT[o] = zaxpy(zaxpy(PT[o], __ldg(rs + n), dp), __ldg(rs + Ny + n), dm);
+            V[o] = zaxpy(zaxpy(V[o], __ldg(rs + 2 * Ny + n), dp), __ldg(rs + 3 * Ny + n), dm);
         }
-        __syncwarp();
+        tsync(t);
         // tau correction (batchedinfluence.jl:148-160); (Dp)_{P-1} = 2P p_P, (Dp)_P = 0
-        const zd s1 = zscale(zsub(zaxpy(zscale(V[P - 1], shift), 2.0 * P, PT[P]), R1[P - 1]),
-                             1.0 / (1.0 - __ldg(csc + 4)));
-        const zd s2 = zscale(zsub(zscale(V[P], shift), R1[P]), 1.0 / (1.0 - __ldg(csc + 5)));
-        __syncwarp();
-        for (int n = lane; n <= P; n += 32) {
-            const bool ev = (n & 1) == 0;
-            PT[n] = zadd(PT[n], zscale(ev ? s1 : s2, __ldg(rs + 4 * Ny + n)));
-            V[n] = zadd(V[n], zscale(ev ? s2 : s1, __ldg(rs + 5 * Ny + n)));
+        const zd vP1 = V[ppos(P - 1, hs)], vP = V[ppos(P, hs)], pP = PT[ppos(P, hs)];
+        const zd rP1 = R1[ppos(P - 1, hs)], rP = R1[ppos(P, hs)];
+        const zd ts1 = zscale(zsub(zaxpy(zscale(vP1, shift), 2.0 * P, pP), rP1), 1.0 / (1.0 - __ldg(csc + 4)));
+        const zd ts2 = zscale(zsub(zscale(vP, shift), rP), 1.0 / (1.0 - __ldg(csc + 5)));
+        tsync(t);
+        const zd sp = q ? ts2 : ts1, sv = q ? ts1 : ts2;
+        for (int j = lane; j < nq; j += 32) {
+            const int n = 2 * j + q, o = qo + j;
+            PT[o] = zaxpy(PT[o], __ldg(rs + 4 * Ny + n), sp);
+            V[o] = zaxpy(V[o], __ldg(rs + 5 * Ny + n), sv);
         }
-        __syncwarp();
+        tsync(t);
     } else {
         // mean mode (meanmode.jl:278-288): integrate Ry through degree P-1, gauge
-        for (int n = lane; n <= P; n += 32) {
+        for (int j = lane; j < nq; j += 32) {
+            const int n = 2 * j + q, o = qo + j;
             zd v = zzero();
             if (n >= 1) {
-                zd lower = (n == 1) ? R1[0] : zscale(R1[n - 1], 0.5);
-                zd upper = (n + 1 < P) ? zscale(R1[n + 1], 0.5) : zzero();
+                zd lower = (n == 1) ? R1[0] : zscale(R1[ppos(n - 1, hs)], 0.5);
+                zd upper = (n + 1 < P) ? zscale(R1[ppos(n + 1, hs)], 0.5) : zzero();
                 v = zscale(zsub(lower, upper), 1.0 / n);
             }
-            PT[n] = v;
-            V[n] = zzero();
+            PT[o] = v;
+            V[o] = zzero();
         }
-        __syncwarp();
-        zd m = col_bulkmean(PT, P, lane);  // PT[0] is zero here
-        if (lane == 0) PT[0] = zscale(m, -1.0);
-        __syncwarp();
+        tsync(t);
+        zd m = col_bulkmean(PT, t);  // PT[0] is zero here
+        if (t.tid == 0) PT[0] = zscale(m, -1.0);
+        tsync(t);
     }
     // tangential velocities: (nu D^2 - shift) u = i k p - Rx, likewise w
-    for (int n = lane; n <= P; n += 32) {
-        R0[n] = zsub(zmulis(PT[n], k), R0[n]);
-        R2[n] = zsub(zmulis(PT[n], l), R2[n]);
+    for (int j = lane; j < nq; j += 32) {
+        const int o = qo + j;
+        R0[o] = zsub(zmulis(PT[o], k), R0[o]);
+        R2[o] = zsub(zmulis(PT[o], l), R2[o]);
     }
     __syncwarp();
-    col_helm(R0, fv, __ldg(sa + 2), __ldg(sa + 3), shift, P, zzero(), zzero(), lane);
-    col_helm(R2, fv, __ldg(sa + 2), __ldg(sa + 3), shift, P, zzero(), zzero(), lane);
+    if (c == 0) {
+        col_stage_rows(fa, fv, 2, t);
+        col_stage_rows(fw, fv + 2 * Ny, 1, t);
+    }
+#pragma unroll 1
+    for (int j = 0; j < 2; ++j)
+        col_helm(j ? R2 : R0, A, fa, fi, fw, p.helm_tab, __ldg(sa + 2), __ldg(sa + 3), shift, zzero(), zzero(), t);
     if (c == 0) {
         double gx, gz;
         if (p.cmode == 1) {
-            zd mu = col_bulkmean(R0, P, lane), mw = col_bulkmean(R2, P, lane);
+            zd mu = col_bulkmean(R0, t), mw = col_bulkmean(R2, t);
             gx = (p.c1 - mu.x) / bk.meanc_mean;
             gz = (p.c2 - mw.x) / bk.meanc_mean;
         } else {
             gx = p.c1;
             gz = p.c2;
         }
-        for (int n = lane; n <= P; n += 32) {
-            const double r = __ldg(bk.meanc + n);
-            R0[n] = zadd(R0[n], zmake(gx * r, 0.0));
-            R2[n] = zadd(R2[n], zmake(gz * r, 0.0));
+        for (int j = lane; j < nq; j += 32) {
+            const int o = qo + j;
+            const double r = __ldg(bk.meanc + 2 * j + q);
+            R0[o] = zadd(R0[o], zmake(gx * r, 0.0));
+            R2[o] = zadd(R2[o], zmake(gz * r, 0.0));
         }
-        __syncwarp();
+        tsync(t);
         gout[0] = gx;
         gout[1] = gz;
     }
@@ -198,313 +296,336 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, const ColPa
 
 // curl of the total velocity and inverse DCT of all six fields to the nodal
 // buffers (nonlinear.jl:179-185, operators.jl:380-398).  u, v, w in U0, U1, U2
-// (modified); W0, W1, W2, Z scratch.
-template <int NCOL>
-CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z, const ColParams& p, int c, int ix,
-                           int iz, int lane, int c0, int cs) {
-    const int P = p.P;
+// (modified); W0, W1, W2 receive the vorticity; Z, Z2 are transform buffers.
+template <int PL>
+CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z, zd* Z2, const ColParams& p, int c,
+                           int ix, int iz, const Team& t) {
+    const int q = t.q, lane = t.lane, qo = q * t.hs, nq = pcount(q, t.P);
     const double k = p.ax * ix;
     const double l = p.bz * (iz <= (p.Nz >> 1) ? iz : iz - p.Nz);
-    if (c == 0)
-        for (int n = lane; n <= P; n += 32) U0[n] = zadd(U0[n], zmake(__ldg(p.base + n), 0.0));
-    __syncwarp();
-    col_diff(U2, W0, P, lane);  // omega_x = D w - i l v
-    col_diff(U0, W2, P, lane);  // omega_z = i k v - D u
-    for (int n = lane; n <= P; n += 32) {
-        W0[n] = zsub(W0[n], zmulis(U1[n], l));
-        W1[n] = zmuli(zsub(zscale(U0[n], l), zscale(U2[n], k)));
-        W2[n] = zsub(zmulis(U1[n], k), W2[n]);
+    if (c == 0) {
+        for (int j = lane; j < nq; j += 32) U0[qo + j] = zadd(U0[qo + j], zmake(__ldg(p.base + 2 * j + q), 0.0));
+        tsync(t);
     }
-    __syncwarp();
-    zd* f[6] = {U0, U1, U2, W0, W1, W2};
+    col_diff(U2, W0, t);  // omega_x = D w - i l v
+    col_diff(U0, W2, t);  // omega_z = i k v - D u
+    for (int j = lane; j < nq; j += 32) {
+        const int o = qo + j;
+        W0[o] = zsub(W0[o], zmulis(U1[o], l));
+        W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
+        W2[o] = zsub(zmulis(U1[o], k), W2[o]);
+    }
+    tsync(t);
 #pragma unroll 1
-    for (int i = 0; i < 6; ++i) col_inverse_y(f[i], Z, p, lane);
+    for (int i = 0; i < 6; ++i) {
+        zd* x = i < 3 ? sel3(U0, U1, U2, i) : sel3(W0, W1, W2, i - 3);
+        col_inverse_y<PL>(x, Z, Z2, p, t);
+    }
 }
 
-// Full CNRK2 stage for NCOL columns per block (one warp per column).
-// SMEM per column: 7 vectors of CS complex.
-template <int NCOL>
-__global__ void __launch_bounds__(NCOL * 32) k_column_stage(ColParams p) {
+// Full CNRK2 stage for NCOL columns per block (one team per column).
+// Regions: 0 R0, 1 R1, 2 R2, 3 PT, 4 A, 5 Bw, 6 Z, 7 Z2 (6, 7: transform buffers).
+template <int NCOL, int PL>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_stage(ColParams p) {
     extern __shared__ zd smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cs = p.Ny + 1;  // column stride (complex)
-    const int c0 = blockIdx.x * NCOL;
-    const int c = c0 + warp;
-    const bool valid = c < p.B;
-    const int ix = c % p.Nxh, iz = c / p.Nxh;
-    // regions: 0 R0, 1 R1, 2 R2, 3 PT, 4 A, 5 Bw, 6 Z
-    zd* reg[7];
-#pragma unroll
-    for (int r = 0; r < 7; ++r) reg[r] = smem + (long)r * NCOL * cs;
-    auto col = [&](int r) { return reg[r] + warp * cs; };
-    const bool nyq = valid ? col_nyquist(p, ix, iz) : true;
-    const double k = p.ax * ix;
-    const double l = p.bz * (iz <= (p.Nz >> 1) ? iz : iz - p.Nz);
+    const ColCtx<NCOL, PL> X(smem, p);
+    const Team& t = X.t;
+    const int cs = X.cs, hs = t.hs, c0 = X.c0, c = X.c, q = t.q, lane = t.lane;
+    const int qo = q * hs, nq = pcount(q, t.P);
+    const bool valid = X.valid;
+    const bool nyq = valid ? col_nyquist(p, X.ix, X.iz) : true;
+    const double k = p.ax * X.ix;
+    const double l = p.bz * (X.iz <= (p.Nz >> 1) ? X.iz : X.iz - p.Nz);
     const double kap2 = k * k + l * l;
-    const int P = p.P;
 
+    // Every input of this block is requested from L2 up front: the rows of
+    // the tiles read below and the columns' Stokes factors and responses
+    // (column-contiguous), so the dependent loads later see L2 latency.
+    {
+        constexpr int NT = NCOL * CF_TEAM;
+        tile_prefetch<NCOL>(p.Pf, c0, p);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            tile_prefetch<NCOL>(p.Nn[i], c0, p);
+            tile_prefetch<NCOL>(p.U[i], c0, p);
+            if (p.stage > 0) tile_prefetch<NCOL>(p.Q[i], c0, p);
+        }
+        const int ncol = min(NCOL, p.B - c0);
+        prefetch_l2(p.bank.fac_p + (long)c0 * 3 * p.Ny, (long)ncol * 3 * p.Ny * 8, threadIdx.x, NT);
+        prefetch_l2(p.bank.fac_v + (long)c0 * 3 * p.Ny, (long)ncol * 3 * p.Ny * 8, threadIdx.x, NT);
+        prefetch_l2(p.bank.resp + (long)c0 * 6 * p.Ny, (long)ncol * 6 * p.Ny * 8, threadIdx.x, NT);
+    }
     // ---------------- Phase A: nonlinear term, history, right-hand side
-    tile_load<NCOL>(reg[3], cs, p.Pf, c0, p);
+    // The three components run through one copy of the loop body (pointers
+    // selected, not indexed): the kernel's issue rate is limited by its
+    // instruction footprint, so the body is not unrolled.
+    tile_load<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p);
     double gold[2] = {p.c1, p.c2};
-    zd bulkN[3], wallR[3], wallL[3];
+    zd bulkN0 = zzero(), bulkN2 = zzero(), wR0 = zzero(), wL0 = zzero(), wR2 = zzero(), wL2 = zzero();
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        tile_load<NCOL>(reg[4], cs, p.Nn[i], c0, p);
+        const zd* Nn_i = sel3(p.Nn[0], p.Nn[1], p.Nn[2], i);
+        zd* Q_i = sel3(p.Q[0], p.Q[1], p.Q[2], i);
+        zd* U_i = sel3(p.U[0], p.U[1], p.U[2], i);
+        tile_load<NCOL>(X.reg(4), cs, hs, Nn_i, c0, p);
+        if (p.stage > 0) tile_load<NCOL>(X.reg(5), cs, hs, Q_i, c0, p);
         __syncthreads();
         if (valid) {
-            col_forward_y(col(4), col(6), p, nyq, lane);
-            if (c == 0) bulkN[i] = col_bulkmean(col(4), P, lane);
-        }
-        __syncthreads();
-        if (p.stage > 0) tile_load<NCOL>(reg[5], cs, p.Q[i], c0, p);
-        __syncthreads();
-        if (valid && p.stage > 0) {
-            zd* A = col(4);
-            const zd* Qo = col(5);
-            for (int n = lane; n <= P; n += 32) A[n] = zaxpy(A[n], p.Acoef, Qo[n]);
-        }
-        __syncthreads();
-        if (p.store_q) tile_store<NCOL>(reg[4], cs, p.Q[i], c0, p);
-        tile_load<NCOL>(reg[5], cs, p.U[i], c0, p);
-        __syncthreads();
-        if (valid) {
-            zd* U = col(5);
-            zd* Qn = col(4);
-            zd* Z = col(6);
-            zd* R = col(i);
-            if (c == 0) col_wallderiv(U, P, lane, wallR[i], wallL[i]);
-            col_diff(U, Z, P, lane);
-            col_diff(Z, R, P, lane);
-            // R = lambda U + nu (D^2 U - kappa^2 U) - d_i P + (B/C) Q
-            if (i == 1) col_diff(col(3), Z, P, lane);
-            const zd* PT = col(3);
-            for (int n = lane; n <= P; n += 32) {
-                zd lap = zaxpy(R[n], -kap2, U[n]);
-                zd r = zaxpy(zscale(U[n], p.lambda), p.nu, lap);
-                zd dP = (i == 0) ? zmulis(PT[n], k) : (i == 1 ? Z[n] : zmulis(PT[n], l));
-                r = zsub(r, dP);
-                r = zaxpy(r, p.weight, Qn[n]);
-                R[n] = r;
+            col_forward_y<PL>(X.col(4), X.col(6), X.col(7), p, nyq, t);
+            if (c == 0) {
+                const zd bm = col_bulkmean(X.col(4), t);
+                if (i == 0) bulkN0 = bm;
+                if (i == 2) bulkN2 = bm;
             }
-            __syncwarp();
+            if (p.stage > 0) {
+                zd* A = X.col(4);
+                const zd* Qo = X.col(5);
+                for (int j = lane; j < nq; j += 32) A[qo + j] = zaxpy(A[qo + j], p.Acoef, Qo[qo + j]);
+            }
+        }
+        __syncthreads();
+        if (p.store_q) tile_store<NCOL>(X.reg(4), cs, hs, Q_i, c0, p);
+        tile_load<NCOL>(X.reg(5), cs, hs, U_i, c0, p);
+        __syncthreads();
+        if (valid) {
+            zd* U = X.col(5);
+            zd* Qn = X.col(4);
+            zd* Z = X.col(6);
+            zd* R = X.col(i);
+            if (c == 0) {
+                zd wr, wl;
+                col_wallderiv(U, t, wr, wl);
+                if (i == 0) {
+                    wR0 = wr;
+                    wL0 = wl;
+                }
+                if (i == 2) {
+                    wR2 = wr;
+                    wL2 = wl;
+                }
+            }
+            col_diff(U, Z, t);
+            col_diff(Z, R, t);
+            // R = lambda U + nu (D^2 U - kappa^2 U) - d_i P + (B/C) Q
+            if (i == 1) col_diff(X.col(3), Z, t);
+            const zd* PT = X.col(3);
+            const double kl = (i == 0) ? k : l;
+            for (int j = lane; j < nq; j += 32) {
+                const int o = qo + j;
+                zd lap = zaxpy(R[o], -kap2, U[o]);
+                zd r = zaxpy(zscale(U[o], p.lambda), p.nu, lap);
+                zd dP = (i == 1) ? Z[o] : zmulis(PT[o], kl);
+                r = zsub(r, dP);
+                r = zaxpy(r, p.weight, Qn[o]);
+                R[o] = r;
+            }
         }
         __syncthreads();
     }
     if (valid && c == 0) {
-        zd* R0 = col(0);
+        zd* R0 = X.col(0);
         if (p.cmode == 1) {
-            gold[0] = p.nu * (wallR[0].x - wallL[0].x) / 2 + p.nu_bm_curv + bulkN[0].x;
-            gold[1] = p.nu * (wallR[2].x - wallL[2].x) / 2 + bulkN[2].x;
+            gold[0] = p.nu * (wR0.x - wL0.x) / 2 + p.nu_bm_curv + bulkN0.x;
+            gold[1] = p.nu * (wR2.x - wL2.x) / 2 + bulkN2.x;
         }
-        for (int n = lane; n <= P; n += 32) R0[n] = zadd(R0[n], zmake(2.0 * p.nu * __ldg(p.basecurv + n), 0.0));
-        __syncwarp();
-        if (lane == 0) {
+        for (int j = lane; j < nq; j += 32)
+            R0[qo + j] = zadd(R0[qo + j], zmake(2.0 * p.nu * __ldg(p.basecurv + 2 * j + q), 0.0));
+        tsync(t);
+        if (t.tid == 0) {
             R0[0].x -= gold[0];
-            zd* R2 = col(2);
+            zd* R2 = X.col(2);
             R2[0].x -= gold[1];
         }
-        __syncwarp();
+        tsync(t);
     }
     // ---------------- Phase B: Stokes solve
     if (valid) {
         if (nyq) {
-            for (int r = 0; r < 6; ++r) {
-                if (r == 1) continue;
-                zd* x = col(r);
-                for (int n = lane; n <= P; n += 32) x[n] = zzero();
-            }
-            __syncwarp();
+            for (int r = 0; r < 6; ++r)
+                if (r != 1) col_zero(X.col(r), t);
+            tsync(t);
         } else {
             double g2[2];
-            col_stokes(col(0), col(1), col(2), col(3), col(4), col(5), p, c, ix, iz, lane, g2);
-            if (c == 0 && lane == 0) {
+            col_stokes<PL>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7), p, c,
+                           X.ix, X.iz, t, g2);
+            if (c == 0 && t.tid == 0) {
                 p.grad_out[0] = g2[0];
                 p.grad_out[1] = g2[1];
             }
         }
     }
     __syncthreads();
-    tile_store<NCOL>(reg[0], cs, p.U[0], c0, p);
-    tile_store<NCOL>(reg[4], cs, p.U[1], c0, p);
-    tile_store<NCOL>(reg[2], cs, p.U[2], c0, p);
-    tile_store<NCOL>(reg[3], cs, p.Pf, c0, p);
+    tile_store<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p);
+    tile_store<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p);
+    tile_store<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p);
+    tile_store<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p);
     __syncthreads();
     // ---------------- Phase C: total velocity, vorticity, nodal values
-    if (valid) col_prep_nodal<NCOL>(col(0), col(4), col(2), col(1), col(3), col(5), col(6), p, c, ix, iz, lane, c0, cs);
+    if (valid)
+        col_prep_nodal<PL>(X.col(0), X.col(4), X.col(2), X.col(1), X.col(3), X.col(5), X.col(6), X.col(7), p, c, X.ix,
+                           X.iz, t);
     __syncthreads();
-    tile_store<NCOL>(reg[0], cs, p.nod[0], c0, p);
-    tile_store<NCOL>(reg[4], cs, p.nod[1], c0, p);
-    tile_store<NCOL>(reg[2], cs, p.nod[2], c0, p);
-    tile_store<NCOL>(reg[1], cs, p.nod[3], c0, p);
-    tile_store<NCOL>(reg[3], cs, p.nod[4], c0, p);
-    tile_store<NCOL>(reg[5], cs, p.nod[5], c0, p);
+    tile_store<NCOL>(X.reg(0), cs, hs, p.nod[0], c0, p);
+    tile_store<NCOL>(X.reg(4), cs, hs, p.nod[1], c0, p);
+    tile_store<NCOL>(X.reg(2), cs, hs, p.nod[2], c0, p);
+    tile_store<NCOL>(X.reg(1), cs, hs, p.nod[3], c0, p);
+    tile_store<NCOL>(X.reg(3), cs, hs, p.nod[4], c0, p);
+    tile_store<NCOL>(X.reg(5), cs, hs, p.nod[5], c0, p);
 }
 
 // Nodal velocity and vorticity from the state U (used after set_state).
-template <int NCOL>
-__global__ void __launch_bounds__(NCOL * 32) k_column_prep(ColParams p) {
+template <int NCOL, int PL>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_prep(ColParams p) {
     extern __shared__ zd smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cs = p.Ny + 1;
-    const int c0 = blockIdx.x * NCOL;
-    const int c = c0 + warp;
-    zd* reg[7];
-#pragma unroll
-    for (int r = 0; r < 7; ++r) reg[r] = smem + (long)r * NCOL * cs;
-    auto col = [&](int r) { return reg[r] + warp * cs; };
-    tile_load<NCOL>(reg[0], cs, p.U[0], c0, p);
-    tile_load<NCOL>(reg[1], cs, p.U[1], c0, p);
-    tile_load<NCOL>(reg[2], cs, p.U[2], c0, p);
+    const ColCtx<NCOL, PL> X(smem, p);
+    const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
+    tile_load<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p);
+    tile_load<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p);
+    tile_load<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p);
     __syncthreads();
-    if (c < p.B)
-        col_prep_nodal<NCOL>(col(0), col(1), col(2), col(3), col(4), col(5), col(6), p, c, c % p.Nxh, c / p.Nxh,
-                             lane, c0, cs);
+    if (X.valid)
+        col_prep_nodal<PL>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7), p, X.c, X.ix,
+                           X.iz, X.t);
     __syncthreads();
-    for (int i = 0; i < 6; ++i) tile_store<NCOL>(reg[i], cs, p.nod[i], c0, p);
+    tile_store<NCOL>(X.reg(0), cs, hs, p.nod[0], c0, p);
+    tile_store<NCOL>(X.reg(1), cs, hs, p.nod[1], c0, p);
+    tile_store<NCOL>(X.reg(2), cs, hs, p.nod[2], c0, p);
+    tile_store<NCOL>(X.reg(3), cs, hs, p.nod[3], c0, p);
+    tile_store<NCOL>(X.reg(4), cs, hs, p.nod[4], c0, p);
+    tile_store<NCOL>(X.reg(5), cs, hs, p.nod[5], c0, p);
 }
 
 // Forward DCT of the nonlinear term only: coefficients into p.Nout.
-template <int NCOL>
-__global__ void __launch_bounds__(NCOL * 32) k_column_nlout(ColParams p) {
+template <int NCOL, int PL>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_nlout(ColParams p) {
     extern __shared__ zd smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cs = p.Ny + 1;
-    const int c0 = blockIdx.x * NCOL;
-    const int c = c0 + warp;
-    zd* reg[2] = {smem, smem + NCOL * cs};
+    const ColCtx<NCOL, PL> X(smem, p);
+    const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
+    const bool nyq = X.valid ? col_nyquist(p, X.ix, X.iz) : true;
+#pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        tile_load<NCOL>(reg[0], cs, p.Nn[i], c0, p);
+        tile_load<NCOL>(X.reg(0), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p);
         __syncthreads();
-        if (c < p.B) col_forward_y(reg[0] + warp * cs, reg[1] + warp * cs, p, col_nyquist(p, c % p.Nxh, c / p.Nxh), lane);
+        if (X.valid) col_forward_y<PL>(X.col(0), X.col(1), X.col(2), p, nyq, X.t);
         __syncthreads();
-        tile_store<NCOL>(reg[0], cs, p.Nout[i], c0, p);
+        tile_store<NCOL>(X.reg(0), cs, hs, sel3(p.Nout[0], p.Nout[1], p.Nout[2], i), c0, p);
         __syncthreads();
     }
 }
 
 // Stokes projection (pressure.jl:36-54): R = -Laplacian(U), solve with the
 // (nu = 1, lambda = 0) bank, velocity overwritten.
-template <int NCOL>
-__global__ void __launch_bounds__(NCOL * 32) k_column_project(ColParams p) {
+template <int NCOL, int PL>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_project(ColParams p) {
     extern __shared__ zd smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cs = p.Ny + 1;
-    const int c0 = blockIdx.x * NCOL;
-    const int c = c0 + warp;
-    const bool valid = c < p.B;
-    const int ix = c % p.Nxh, iz = c / p.Nxh;
-    zd* reg[7];
-#pragma unroll
-    for (int r = 0; r < 7; ++r) reg[r] = smem + (long)r * NCOL * cs;
-    auto col = [&](int r) { return reg[r] + warp * cs; };
-    const double k = p.ax * ix;
-    const double l = p.bz * (iz <= (p.Nz >> 1) ? iz : iz - p.Nz);
+    const ColCtx<NCOL, PL> X(smem, p);
+    const Team& t = X.t;
+    const int cs = X.cs, hs = t.hs, c0 = X.c0, qo = t.q * hs, nq = pcount(t.q, t.P);
+    const double k = p.ax * X.ix;
+    const double l = p.bz * (X.iz <= (p.Nz >> 1) ? X.iz : X.iz - p.Nz);
     const double kap2 = k * k + l * l;
+#pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        tile_load<NCOL>(reg[5], cs, p.U[i], c0, p);
+        tile_load<NCOL>(X.reg(5), cs, hs, sel3(p.U[0], p.U[1], p.U[2], i), c0, p);
         __syncthreads();
-        if (valid) {
-            zd* U = col(5);
-            zd* Z = col(6);
-            zd* R = col(i);
-            col_diff(U, Z, p.P, lane);
-            col_diff(Z, R, p.P, lane);
-            for (int n = lane; n <= p.P; n += 32) R[n] = zscale(zaxpy(R[n], -kap2, U[n]), -1.0);
-            __syncwarp();
+        if (X.valid) {
+            zd* U = X.col(5);
+            zd* Z = X.col(6);
+            zd* R = X.col(i);
+            col_diff(U, Z, t);
+            col_diff(Z, R, t);
+            for (int j = t.lane; j < nq; j += 32) R[qo + j] = zscale(zaxpy(R[qo + j], -kap2, U[qo + j]), -1.0);
         }
         __syncthreads();
     }
-    if (valid) {
-        if (col_nyquist(p, ix, iz)) {
-            for (int r = 0; r < 6; ++r) {
-                zd* x = col(r);
-                for (int n = lane; n <= p.P; n += 32) x[n] = zzero();
-            }
-            __syncwarp();
+    if (X.valid) {
+        if (col_nyquist(p, X.ix, X.iz)) {
+            for (int r = 0; r < 6; ++r) col_zero(X.col(r), t);
+            tsync(t);
         } else {
             double g2[2];
-            col_stokes(col(0), col(1), col(2), col(3), col(4), col(5), p, c, ix, iz, lane, g2);
+            col_stokes<PL>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7), p, X.c,
+                           X.ix, X.iz, t, g2);
         }
     }
     __syncthreads();
-    tile_store<NCOL>(reg[0], cs, p.U[0], c0, p);
-    tile_store<NCOL>(reg[4], cs, p.U[1], c0, p);
-    tile_store<NCOL>(reg[2], cs, p.U[2], c0, p);
+    tile_store<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p);
+    tile_store<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p);
+    tile_store<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p);
 }
 
 // Pressure reconstruction (pressure.jl:115-204) from the nonlinear term at
 // the nodes (p.Nn) and the normal velocity U[1]: Neumann Helmholtz per mode
 // with the factors in p.bank.fac_p / sa[0..1] (Neumann weights).
-template <int NCOL>
-__global__ void __launch_bounds__(NCOL * 32) k_column_pressure(ColParams p) {
+template <int NCOL, int PL>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_pressure(ColParams p) {
     extern __shared__ zd smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cs = p.Ny + 1;
-    const int c0 = blockIdx.x * NCOL;
-    const int c = c0 + warp;
-    const bool valid = c < p.B;
-    const int ix = c % p.Nxh, iz = c / p.Nxh;
-    const int P = p.P;
-    zd* reg[7];
-#pragma unroll
-    for (int r = 0; r < 7; ++r) reg[r] = smem + (long)r * NCOL * cs;
-    auto col = [&](int r) { return reg[r] + warp * cs; };
-    const bool nyq = valid ? col_nyquist(p, ix, iz) : true;
+    const ColCtx<NCOL, PL> X(smem, p);
+    const Team& t = X.t;
+    const int cs = X.cs, hs = t.hs, c0 = X.c0, c = X.c, q = t.q, lane = t.lane;
+    const int P = t.P, qo = q * hs, nq = pcount(q, P);
+    const bool nyq = X.valid ? col_nyquist(p, X.ix, X.iz) : true;
+#pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        tile_load<NCOL>(reg[i], cs, p.Nn[i], c0, p);
+        tile_load<NCOL>(X.reg(i), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p);
         __syncthreads();
-        if (valid) col_forward_y(col(i), col(6), p, nyq, lane);
+        if (X.valid) col_forward_y<PL>(X.col(i), X.col(6), X.col(7), p, nyq, t);
         __syncthreads();
     }
-    tile_load<NCOL>(reg[4], cs, p.U[1], c0, p);
+    tile_load<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p);
     __syncthreads();
-    if (valid) {
-        const double k = p.ax * ix;
-        const double l = p.bz * (iz <= (p.Nz >> 1) ? iz : iz - p.Nz);
-        zd* A0 = col(0);
-        zd* A1 = col(1);
-        zd* A2 = col(2);
-        zd* PT = col(3);
-        zd* V = col(4);
+    if (X.valid) {
+        const double k = p.ax * X.ix;
+        const double l = p.bz * (X.iz <= (p.Nz >> 1) ? X.iz : X.iz - p.Nz);
+        zd* A0 = X.col(0);
+        zd* A1 = X.col(1);
+        zd* A2 = X.col(2);
+        zd* PT = X.col(3);
+        zd* V = X.col(4);
         if (nyq) {
-            for (int n = lane; n <= P; n += 32) PT[n] = zzero();
-            __syncwarp();
+            col_zero(PT, t);
+            tsync(t);
         } else if (c == 0) {
-            for (int n = lane; n <= P; n += 32) {
+            for (int j = lane; j < nq; j += 32) {
+                const int n = 2 * j + q;
                 zd v = zzero();
                 if (n >= 1) {
-                    zd lower = (n == 1) ? A1[0] : zscale(A1[n - 1], 0.5);
-                    zd upper = (n + 1 < P) ? zscale(A1[n + 1], 0.5) : zzero();
+                    zd lower = (n == 1) ? A1[0] : zscale(A1[ppos(n - 1, hs)], 0.5);
+                    zd upper = (n + 1 < P) ? zscale(A1[ppos(n + 1, hs)], 0.5) : zzero();
                     v = zscale(zsub(lower, upper), 1.0 / n);
                 }
-                PT[n] = v;
+                PT[qo + j] = v;
             }
-            __syncwarp();
-            zd m = col_bulkmean(PT, P, lane);
-            if (lane == 0) PT[0] = zscale(m, -1.0);
-            __syncwarp();
+            tsync(t);
+            zd m = col_bulkmean(PT, t);
+            if (t.tid == 0) PT[0] = zscale(m, -1.0);
+            tsync(t);
         } else {
-            col_diff(A1, PT, P, lane);
-            for (int n = lane; n <= P; n += 32) PT[n] = zadd(PT[n], zadd(zmulis(A0[n], k), zmulis(A2[n], l)));
-            zd up = zzero(), lo = zzero();
-            for (int n = lane; n <= P; n += 32) {
-                up = zadd(up, A1[n]);
-                lo = zaxpy(lo, (n & 1) ? -1.0 : 1.0, A1[n]);
+            col_diff(A1, PT, t);
+            zd su = zzero();
+            for (int j = lane; j < nq; j += 32) {
+                const int n = 2 * j + q, o = qo + j;
+                PT[o] = zadd(PT[o], zadd(zmulis(A0[o], k), zmulis(A2[o], l)));
+                su = zadd(su, A1[o]);
                 if (n >= 2) {
-                    const double wn = p.nu * ((double)n * n * ((double)n * n - 1.0) / 3.0);
-                    up = zaxpy(up, wn, V[n]);
-                    lo = zaxpy(lo, (n & 1) ? -wn : wn, V[n]);
+                    const double dn = (double)n;
+                    su = zaxpy(su, p.nu * (dn * dn * (dn * dn - 1.0) / 3.0), V[o]);
                 }
             }
-            up = warp_sum_z(up);
-            lo = warp_sum_z(lo);
-            __syncwarp();
+            zd s0, s1;
+            team_xchg(t, warp_sum_z(su), s0, s1);
+            const zd up = zadd(s0, s1), lo = zsub(s0, s1);
             const double* sa = p.bank.sa + (long)c * 4;
             // Neumann parity data: even rows (up - lo)/2, odd rows (up + lo)/2
-            col_helm(PT, p.bank.fac_p + (long)c * 3 * p.Ny, __ldg(sa + 0), __ldg(sa + 1), k * k + l * l, P,
-                     zscale(zsub(up, lo), 0.5), zscale(zadd(up, lo), 0.5), lane);
+            const double* fpn = p.bank.fac_p + (long)c * 3 * p.Ny;
+            double* fa = reinterpret_cast<double*>(X.col(6));
+            double* fw = reinterpret_cast<double*>(X.col(7));
+            col_stage_rows(fa, fpn, 2, t);
+            col_stage_rows(fw, fpn + 2 * p.Ny, 1, t);
+            col_helm(PT, X.col(5), fa, fa + 2 * hs, fw, p.helm_tab, __ldg(sa + 0), __ldg(sa + 1), k * k + l * l,
+                     zscale(zsub(up, lo), 0.5), zscale(zadd(up, lo), 0.5), t);
         }
     }
     __syncthreads();
-    tile_store<NCOL>(reg[3], cs, p.Pf, c0, p);
+    tile_store<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p);
 }

@@ -701,22 +701,20 @@ static void forward_transform(const OGrid& g, const double* u, cd* U) {
 // Operators (src/fields/operators.jl)
 // ---------------------------------------------------------------------------
 static void op_ddx1(const OGrid& g, const cd* U, cd* O, bool add) {
-    for (int n = 0; n < g.Ny; ++n)
-        for (int iz = 0; iz < g.Nz; ++iz)
-            for (int ix = 0; ix < g.Nxh; ++ix) {
-                long i = ((long)n * g.Nz + iz) * g.Nxh + ix;
-                cd v = cd(0, g.kx(ix)) * U[i];
-                O[i] = add ? O[i] + v : v;
-            }
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < sampled(g.nr()); ++i) {
+        const int ix = (int)(i % g.Nxh);
+        cd v = cd(0, g.kx(ix)) * U[i];
+        O[i] = add ? O[i] + v : v;
+    }
 }
 static void op_ddx3(const OGrid& g, const cd* U, cd* O, bool add) {
-    for (int n = 0; n < g.Ny; ++n)
-        for (int iz = 0; iz < g.Nz; ++iz)
-            for (int ix = 0; ix < g.Nxh; ++ix) {
-                long i = ((long)n * g.Nz + iz) * g.Nxh + ix;
-                cd v = cd(0, g.lz(iz)) * U[i];
-                O[i] = add ? O[i] + v : v;
-            }
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < sampled(g.nr()); ++i) {
+        const int iz = (int)((i / g.Nxh) % g.Nz);
+        cd v = cd(0, g.lz(iz)) * U[i];
+        O[i] = add ? O[i] + v : v;
+    }
 }
 static void op_ddx2(const OGrid& g, const cd* U, cd* O, bool add) {
     const long S = (long)g.Nz * g.Nxh;
@@ -724,7 +722,7 @@ static void op_ddx2(const OGrid& g, const cd* U, cd* O, bool add) {
     {
         std::vector<cd> tmp(g.Ny);
 #pragma omp for
-        for (long c = 0; c < S; ++c) {
+        for (long c = 0; c < sampled(S); ++c) {
             cheb_diff(U + c, S, tmp.data(), 1, g.Ny);
             for (int n = 0; n < g.Ny; ++n) O[c + n * S] = add ? O[c + n * S] + tmp[n] : tmp[n];
         }
@@ -736,40 +734,41 @@ static void op_laplacian(const OGrid& g, const cd* a, cd* b) {
     const double al2 = std::pow(2 * M_PI / g.Lx, 2), be2 = std::pow(2 * M_PI / g.Lz, 2);
     auto A = [&](int j, int iz, int ix) { return a[((long)(j - 1) * Nz + iz) * Nxh + ix]; };
     auto Bv = [&](int j, int iz, int ix) -> cd& { return b[((long)(j - 1) * Nz + iz) * Nxh + ix]; };
-    for (int j = Ny; j >= 1; --j)
-        for (int iz = 0; iz < Nz; ++iz) {
-            int l = iz <= (Nz >> 1) ? iz : iz - Nz;
-            for (int ix = 0; ix < Nxh; ++ix) {
-                double k2 = al2 * (double)ix * ix + be2 * (double)l * l;
-                cd d2 = 0;
-                if (j + 2 <= Ny)
-                    d2 = (4.0 * j * (j + 1)) * A(j + 2, iz, ix) +
-                         (2.0 * (j + 1) / (j + 2)) * (Bv(j + 2, iz, ix) + k2 * A(j + 2, iz, ix));
-                if (j + 4 <= Ny) d2 -= ((double)j / (j + 2)) * (Bv(j + 4, iz, ix) + k2 * A(j + 4, iz, ix));
-                Bv(j, iz, ix) = (j == 1 ? d2 / 2.0 : d2) - k2 * A(j, iz, ix);
-            }
+    // columns are independent; the recurrence runs down each column
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < sampled((long)Nz * Nxh); ++c) {
+        const int iz = (int)(c / Nxh), ix = (int)(c % Nxh);
+        const int l = iz <= (Nz >> 1) ? iz : iz - Nz;
+        const double k2 = al2 * (double)ix * ix + be2 * (double)l * l;
+        for (int j = Ny; j >= 1; --j) {
+            cd d2 = 0;
+            if (j + 2 <= Ny)
+                d2 = (4.0 * j * (j + 1)) * A(j + 2, iz, ix) +
+                     (2.0 * (j + 1) / (j + 2)) * (Bv(j + 2, iz, ix) + k2 * A(j + 2, iz, ix));
+            if (j + 4 <= Ny) d2 -= ((double)j / (j + 2)) * (Bv(j + 4, iz, ix) + k2 * A(j + 4, iz, ix));
+            Bv(j, iz, ix) = (j == 1 ? d2 / 2.0 : d2) - k2 * A(j, iz, ix);
         }
+    }
 }
 // curl! (operators.jl:380-398)
 static void op_curl(const OGrid& g, const cd* const U[3], cd* const O[3]) {
     op_ddx2(g, U[2], O[0], false);
     op_ddx2(g, U[0], O[2], false);
     const cd I(0, 1);
-    for (int n = 0; n < g.Ny; ++n)
-        for (int iz = 0; iz < g.Nz; ++iz)
-            for (int ix = 0; ix < g.Nxh; ++ix) {
-                long i = ((long)n * g.Nz + iz) * g.Nxh + ix;
-                double k = g.kx(ix), l = g.lz(iz);
-                O[0][i] -= I * l * U[1][i];
-                O[1][i] = I * (l * U[0][i] - k * U[2][i]);
-                O[2][i] = I * k * U[1][i] - O[2][i];
-            }
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < sampled(g.nr()); ++i) {
+        const int ix = (int)(i % g.Nxh), iz = (int)((i / g.Nxh) % g.Nz);
+        double k = g.kx(ix), l = g.lz(iz);
+        O[0][i] -= I * l * U[1][i];
+        O[1][i] = I * (l * U[0][i] - k * U[2][i]);
+        O[2][i] = I * k * U[1][i] - O[2][i];
+    }
 }
 static void zero_nyquist(const OGrid& g, cd* U) {
-    for (int n = 0; n < g.Ny; ++n)
-        for (int iz = 0; iz < g.Nz; ++iz)
-            for (int ix = 0; ix < g.Nxh; ++ix)
-                if (g.nyquist(ix, iz)) U[((long)n * g.Nz + iz) * g.Nxh + ix] = 0;
+    for (int iz = 0; iz < g.Nz; ++iz)
+        for (int ix = 0; ix < g.Nxh; ++ix)
+            if (g.nyquist(ix, iz))
+                for (int n = 0; n < g.Ny; ++n) U[((long)n * g.Nz + iz) * g.Nxh + ix] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -836,7 +835,12 @@ struct Problem {
 static void nonlinear(Problem& pb, const cd* const U[3], cd* const Nout[3]) {
     const OGrid& g = pb.g;
     const long nr = g.nr(), S = (long)g.Nxh * g.Nz;
-    for (int i = 0; i < 3; ++i) std::memcpy(pb.TMP[i].data(), U[i], sizeof(cd) * nr);
+    for (int i = 0; i < 3; ++i) {
+        cd* dst = pb.TMP[i].data();
+        const cd* src = U[i];
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < sampled(nr); ++x) dst[x] = src[x];
+    }
     for (int n = 0; n < g.Ny; ++n) pb.TMP[0][n * S] += pb.base[n];
     const cd* T[3] = {pb.TMP[0].data(), pb.TMP[1].data(), pb.TMP[2].data()};
     cd* O[3] = {pb.OM[0].data(), pb.OM[1].data(), pb.OM[2].data()};
@@ -886,8 +890,10 @@ static void cnrk2_stage(Problem& pb, cd* const U[3], cd* Pf, int j, double* grad
     }
     for (int i = 0; i < 3; ++i) {
         cd* Qi = pb.Q[i].data();
-        if (j == 0) std::memcpy(Qi, Nf[i], sizeof(cd) * nr);
-        else for (long x = 0; x < nr; ++x) Qi[x] = CA[j] * Qi[x] + Nf[i][x];
+        const cd* Ni = Nf[i];
+        const double a = CA[j];
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < sampled(nr); ++x) Qi[x] = (j == 0) ? Ni[x] : a * Qi[x] + Ni[x];
     }
     const double lambda = 1.0 / (CC[j] * pb.dt), weight = CB[j] / CC[j];
     for (int i = 0; i < 3; ++i) {
@@ -896,7 +902,11 @@ static void cnrk2_stage(Problem& pb, cd* const U[3], cd* Pf, int j, double* grad
         else if (i == 1) op_ddx2(g, Pf, Nf[i], false);
         else op_ddx3(g, Pf, Nf[i], false);
         const cd* Qi = pb.Q[i].data();
-        for (long x = 0; x < nr; ++x) Rf[i][x] = lambda * U[i][x] + pb.nu * Rf[i][x] - Nf[i][x] + weight * Qi[x];
+        cd* Ri = Rf[i];
+        const cd *Ui = U[i], *Ni = Nf[i];
+        const double nu = pb.nu;
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < sampled(nr); ++x) Ri[x] = lambda * Ui[x] + nu * Ri[x] - Ni[x] + weight * Qi[x];
     }
     for (int n = 0; n < g.Ny; ++n) Rf[0][n * S] += 2 * pb.nu * pb.basecurv[n];
     Rf[0][0] -= old[0];
