@@ -42,7 +42,7 @@ class _Config(ctypes.Structure):
 EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_get_state",
            "cf_set_state_device", "cf_get_state_device", "cf_step", "cf_nonlinear", "cf_project",
            "cf_pressure", "cf_random_state", "cf_diagnostics", "cf_sync", "cf_last_launch_count",
-           "cf_stream", "cf_last_error", "cf_step_profiled"]
+           "cf_stream", "cf_last_error", "cf_step_profiled", "cf_nonlinear_noalloc"]
 
 
 def lib():
@@ -64,6 +64,7 @@ def lib():
         L.cf_get_state_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.cf_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _D, _D]
         L.cf_nonlinear.argtypes = [ctypes.c_void_p, _D, _D]
+        L.cf_nonlinear_noalloc.argtypes = [ctypes.c_void_p, _D, _D]
         L.cf_project.argtypes = [ctypes.c_void_p, _D]
         L.cf_pressure.argtypes = [ctypes.c_void_p, _D, _D]
         L.cf_random_state.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_double, ctypes.c_int,
@@ -232,6 +233,14 @@ class ChannelFlowProblem:
         U = np.ascontiguousarray(U, dtype=np.complex128)
         N = np.zeros_like(U)
         _check(lib().cf_nonlinear(self._h, _ptr(U.view(np.float64)), _ptr(N.view(np.float64))))
+        return N
+
+    def nonlinear_noalloc(self, U):
+        """nonlinear() staged in the library's fixed device scratch (allocates
+        nothing; grids with 3 * Nr * 16 bytes <= 16 MiB)."""
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        N = np.zeros_like(U)
+        _check(lib().cf_nonlinear_noalloc(self._h, _ptr(U.view(np.float64)), _ptr(N.view(np.float64))))
         return N
 
     def diagnostics(self):

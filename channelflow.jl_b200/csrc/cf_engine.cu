@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -819,6 +820,51 @@ int cf_nonlinear(cf_handle* h, const double* U, double* N) {
     col_kernel(KC_NLOUT, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(N, h->tmpU, 3 * fr, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    h->nodal_valid = false;
+    return CF_OK;
+}
+
+// Fixed scratch of cf_nonlinear_noalloc: one array per device (module scope),
+// its address looked up once per device with that device current.
+#define CF_MAX_DEVICES 64
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CF_NOALLOC_SCRATCH_BYTES];
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[CF_MAX_DEVICES] = {};
+
+static int noalloc_scratch(void** out) {
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= CF_MAX_DEVICES) return fail(CF_E_UNSUPPORTED, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return fail(CF_E_CUDA, std::string("scratch address: ") + cudaGetErrorString(e));
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return CF_OK;
+}
+
+int cf_nonlinear_noalloc(cf_handle* h, const double* U, double* N) {
+    if (!h || !U || !N) return fail(CF_E_ARG, "null argument");
+    const size_t fr = sizeof(zd) * h->nr;
+    if (3 * fr > (size_t)CF_NOALLOC_SCRATCH_BYTES)
+        return fail(CF_E_ARG, "grid too large for the fixed scratch (3 * Nr * 16 bytes > 16 MiB)");
+    void* scr = nullptr;
+    int rc = noalloc_scratch(&scr);
+    if (rc) return rc;
+    zd* base = static_cast<zd*>(scr);
+    zd* Us[3] = {base, base + h->nr, base + 2 * h->nr};
+    CU(cudaMemcpyAsync(base, U, 3 * fr, cudaMemcpyHostToDevice, h->stream));
+    if ((rc = launch_prep(h, Us, nullptr))) return rc;
+    if ((rc = launch_periodic(h, nullptr))) return rc;
+    ColParams p = col_params(h);
+    for (int i = 0; i < 3; ++i) p.Nout[i] = Us[i];
+    col_kernel(KC_NLOUT, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(N, base, 3 * fr, cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     h->nodal_valid = false;
     return CF_OK;

@@ -76,6 +76,18 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
 /* NonLinearTerm{RotatingForm}(t, U, N) on host buffers (nonlinear.jl:173-193). */
 int cf_nonlinear(cf_handle* h, const double* U, double* N);
 
+/* cf_nonlinear that allocates no device memory: U and N are staged in a fixed
+ * module-scope device array of CF_NOALLOC_SCRATCH_BYTES (16 MiB) instead of
+ * buffers allocated on first use.  No reference counterpart (an addition of
+ * this library, for callers that must not allocate).  Limit: 3 * Nr * 16 bytes
+ * <= 16 MiB, Nr = (Nx/2+1) * Nz * Ny <= 349525; larger grids return CF_E_ARG.
+ * The array is one per device for the whole process: calls through different
+ * handles (or streams) on one device must not overlap; the caller serialises
+ * them.  The first call on a device looks the array's address up and must not
+ * be made while a stream of that device is being captured. */
+#define CF_NOALLOC_SCRATCH_BYTES (16u << 20)
+int cf_nonlinear_noalloc(cf_handle* h, const double* U, double* N);
+
 /* project!(U, problem) on a host velocity, in place (pressure.jl:36-54). */
 int cf_project(cf_handle* h, double* U);
 /* pressure(U, problem) (pressure.jl:95-104): modified pressure of U. */
