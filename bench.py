@@ -45,6 +45,10 @@ CONFIGS = {
     # Re_tau~590-sized Poiseuille at constant flux, Re_bulk=10900 (headline grid)
     "c3": dict(Nx=384, Ny=257, Nz=384, Lx=2 * math.pi, Lz=math.pi, nu=(2 / 3) / 10900, dt=0.002,
                profile="poiseuille", constraint=(2 / 3, 0.0), amp=0.1, shape=1, rho=0.8),
+    # ensemble of 256 plane Couette instances on uneven grids (one graph per step)
+    "c4": dict(ensemble=[((32, 33, 32), 128), ((48, 49, 48), 96), ((64, 65, 64), 32)],
+               Lx=2 * math.pi / 1.14, Lz=2 * math.pi / 2.5, Re=(300.0, 500.0), amp=(0.05, 0.15), dt=0.01,
+               profile="couette", constraint=None, shape=0, rho=0.8),
     # large grid 512x385x512 (plain FP64 here)
     "c5": dict(Nx=512, Ny=385, Nz=512, Lx=2 * math.pi, Lz=math.pi, nu=(2 / 3) / 10900, dt=0.0015,
                profile="poiseuille", constraint=(2 / 3, 0.0), amp=0.1, shape=1, rho=0.8),
@@ -191,6 +195,17 @@ def run_reference(args, cfg, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    if "ensemble" in cfg:
+        members = ensemble_members(cfg, 0)
+        cb = ensemble_cpu(cfg, members, threads)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "steps/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": len(members) / cb["value"] * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": "c4", "instances": len(members)},
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
     from oracle import oracle as O
 
     O.set_threads(threads)
@@ -232,6 +247,166 @@ def workload_desc(cfg):
             "l2": "state larger than L2 (no flush needed)"}
 
 
+def ensemble_members(cfg, rank):
+    """Members of the ensemble workload: (Nx, Ny, Nz, nu, amplitude, seed),
+    Re and amplitude drawn uniformly from the workload's ranges."""
+    rng = np.random.default_rng(4 + rank)
+    out, i = [], 0
+    for (Nx, Ny, Nz), count in cfg["ensemble"]:
+        for _ in range(count):
+            Re = rng.uniform(*cfg["Re"])
+            amp = rng.uniform(*cfg["amp"])
+            out.append((Nx, Ny, Nz, 1.0 / Re, amp, 5000 + 1000 * rank + i))
+            i += 1
+    return out
+
+
+def ensemble_model_bytes(cfg, members):
+    tot = 0.0
+    for Nx, Ny, Nz, *_ in members:
+        c = dict(cfg, Nx=Nx, Ny=Ny, Nz=Nz)
+        tot += 3 * sum(model_bytes(c).values())
+    return tot
+
+
+def run_ensemble(args, cfg, rank, world, local, torch, dist):
+    """Ensemble workload: value = aggregate steps/s of all instances advanced
+    together (cf_step_batch); the same instances stepped one after another,
+    each through its own CUDA-graph step, give the sequential figure."""
+    import cfb200
+
+    members = ensemble_members(cfg, rank)
+    ens = cfb200.Ensemble([dict(grid=cfb200.Grid(Nx, Ny, Nz, cfg["Lx"], cfg["Lz"]), profile="couette", nu=nu,
+                                dt=cfg["dt"]) for Nx, Ny, Nz, nu, _, _ in members])
+    for inst, (_, _, _, _, amp, seed) in zip(ens.instances, members):
+        cfb200.lib().cf_random_state(inst.handle, seed, amp, cfg["shape"], cfg["rho"])
+    n = len(members)
+    stream = torch.cuda.ExternalStream(ens.stream_ptr())
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ens.step(args.warmup)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    launches = ens.launches()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    ms_per_step = ms / args.steps
+    value = world * n * args.steps / (ms / 1e3)
+
+    # the same instances one after another, each with its own graph step
+    seq_ms = 0.0
+    kseq = max(2, min(args.steps, 5))
+    for inst in ens.instances:
+        s_i = torch.cuda.ExternalStream(inst.stream_ptr())
+        inst.advance(0.0, 1)
+        inst.sync()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(s_i)
+        inst.advance(0.0, kseq)
+        a1.record(s_i)
+        a1.synchronize()
+        seq_ms += a0.elapsed_time(a1) / kseq
+    seq_ms = max_over_ranks(seq_ms)
+    seq_value = world * n / (seq_ms / 1e3)
+
+    # end to end through the host-buffer C ABI: every instance's state is
+    # uploaded from pinned memory and downloaded after each ensemble step
+    hb = []
+    for inst in ens.instances:
+        Uc, Pc = inst.get_state()
+        Uh = torch.empty(Uc.shape + (2,), dtype=torch.float64, pin_memory=True).numpy()
+        Ph = torch.empty(Pc.shape + (2,), dtype=torch.float64, pin_memory=True).numpy()
+        Uh[...] = Uc.view(np.float64).reshape(Uh.shape)
+        Ph[...] = Pc.view(np.float64).reshape(Ph.shape)
+        hb.append((Uh.view(np.complex128).reshape(Uc.shape), Ph.view(np.complex128).reshape(Pc.shape)))
+    ke = max(2, min(args.steps, 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        for inst, (Uv, Pv) in zip(ens.instances, hb):
+            inst.set_state(Uv, Pv)
+        ens.step(1)
+        for inst, (Uv, Pv) in zip(ens.instances, hb):
+            U2, P2 = inst.get_state()
+            Uv[...] = U2
+            Pv[...] = P2
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    state_bytes = sum(4 * 16 * (Nx // 2 + 1) * Nz * Ny for Nx, Ny, Nz, *_ in members)
+
+    peak, peak_kind = peaks()
+    mbytes = ensemble_model_bytes(cfg, members)
+    achieved = mbytes / (ms_per_step * 1e-3) / 1e9
+    energies = [inst.diagnostics()[0] for inst in ens.instances[:: max(1, n // 8)]]
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "c4", "instances": n,
+                   "grids": [f"{c}x({g[0]},{g[1]},{g[2]})" for g, c in cfg["ensemble"]],
+                   "Re": list(cfg["Re"]), "amp": list(cfg["amp"]), "dt": cfg["dt"], "profile": "couette",
+                   "form": "rotational", "precision": "fp64 plain",
+                   "l2": "ensemble state (~1.3 GB) larger than L2 (no flush needed)",
+                   "parallelism": f"replicas x{world}"},
+        "aggregate": "value = instance-steps/s of the whole ensemble (cf_step_batch, one CUDA graph per step)",
+        "sequential": {"value": seq_value, "unit": "steps/s",
+                       "how": "the same instances one after another, each through its own CUDA-graph step "
+                              "(sum of per-instance event-timed step times)"},
+        "speedup_vs_sequential": value / seq_value,
+        "e2e": {"value": world * n * ke / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes},
+        "roofline": {"bound": "hbm", "kernel": "ensemble step (all kernels, byte model summed over instances)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": None, "step_model_bytes": mbytes},
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "diagnostics": {"kinetic_energy_sample": energies},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = ensemble_cpu(cfg, members, os.cpu_count() or 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ens.close()
+
+
+def ensemble_cpu(cfg, members, threads):
+    """Oracle port: one full step of one instance per grid, times the number
+    of instances on that grid, summed (instances one after another)."""
+    from oracle import oracle as O
+
+    O.set_threads(threads)
+    O.set_helmholtz_method("quasitri")
+    total = 0.0
+    for (Nx, Ny, Nz), count in cfg["ensemble"]:
+        nu = next(m[3] for m in members if m[:3] == (Nx, Ny, Nz))
+        pb = O.couette(Nx, Ny, Nz, cfg["Lx"], cfg["Lz"], nu, cfg["dt"])
+        U, P = pb.random_state(seed=1, amp=0.1)
+        pb.step(U, P, 1)
+        t0 = time.perf_counter()
+        pb.step(U, P, 2)
+        total += count * (time.perf_counter() - t0) / 2
+    return {"value": len(members) / total, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": "one instance per grid stepped twice on the oracle; ensemble time = sum over grids of "
+                      "count x step time; value = instance-steps/s"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -260,6 +435,12 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if "ensemble" in cfg:
+        run_ensemble(args, cfg, rank, world, local, torch, dist)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     import cfb200
 
     g = cfb200.Grid(cfg["Nx"], cfg["Ny"], cfg["Nz"], cfg["Lx"], cfg["Lz"])

@@ -42,7 +42,9 @@ class _Config(ctypes.Structure):
 EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_get_state",
            "cf_set_state_device", "cf_get_state_device", "cf_step", "cf_nonlinear", "cf_project",
            "cf_pressure", "cf_random_state", "cf_diagnostics", "cf_sync", "cf_last_launch_count",
-           "cf_stream", "cf_last_error", "cf_step_profiled", "cf_nonlinear_noalloc"]
+           "cf_stream", "cf_last_error", "cf_step_profiled", "cf_nonlinear_noalloc", "cf_create_batch",
+           "cf_destroy_batch", "cf_batch_size", "cf_batch_instance", "cf_step_batch",
+           "cf_batch_last_launch_count", "cf_batch_stream"]
 
 
 def lib():
@@ -65,6 +67,16 @@ def lib():
         L.cf_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _D, _D]
         L.cf_nonlinear.argtypes = [ctypes.c_void_p, _D, _D]
         L.cf_nonlinear_noalloc.argtypes = [ctypes.c_void_p, _D, _D]
+        L.cf_create_batch.argtypes = [ctypes.POINTER(_Config), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.cf_destroy_batch.argtypes = [ctypes.c_void_p]
+        L.cf_destroy_batch.restype = None
+        L.cf_batch_size.argtypes = [ctypes.c_void_p]
+        L.cf_batch_instance.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.cf_batch_instance.restype = ctypes.c_void_p
+        L.cf_step_batch.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.cf_batch_last_launch_count.argtypes = [ctypes.c_void_p]
+        L.cf_batch_stream.argtypes = [ctypes.c_void_p]
+        L.cf_batch_stream.restype = ctypes.c_void_p
         L.cf_project.argtypes = [ctypes.c_void_p, _D]
         L.cf_pressure.argtypes = [ctypes.c_void_p, _D, _D]
         L.cf_random_state.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_double, ctypes.c_int,
@@ -138,6 +150,37 @@ def zero_state(grid):
     return State(np.zeros((3,) + grid.spectralsize, np.complex128), np.zeros(grid.spectralsize, np.complex128))
 
 
+def _make_config(grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None, forcing=None, form=None):
+    """cf_config of ChannelFlowProblem(grid, profile, nu, dt; ...); returns
+    (config, base-profile array kept alive for the call, constraint)."""
+    if pressuregradient is not None and bulkvelocity is not None:
+        raise ValueError("specify either pressuregradient or bulkvelocity")
+    if forcing is not None:
+        raise ValueError("only NoForcing is accelerated by the engine")
+    if form not in (None, "rotational"):
+        raise ValueError("only the rotational nonlinear form is accelerated by the engine")
+    if bulkvelocity is not None:
+        constraint = ("bulkvelocity", tuple(float(v) for v in bulkvelocity))
+    else:
+        pg = (0.0, 0.0) if pressuregradient is None else pressuregradient
+        constraint = ("pressuregradient", tuple(float(v) for v in pg))
+    cfg = _Config()
+    cfg.Nx, cfg.Ny, cfg.Nz = grid.Nx, grid.Ny, grid.Nz
+    cfg.Lx, cfg.Lz, cfg.nu, cfg.dt = grid.Lx, grid.Lz, float(nu), float(dt)
+    base = None
+    if profile == "couette":
+        cfg.profile = 0
+    elif profile == "poiseuille":
+        cfg.profile = 1
+    else:
+        cfg.profile = 2
+        base = np.ascontiguousarray([float(profile(v)) for v in grid.y], dtype=np.float64)
+        cfg.base_values = _ptr(base)
+    cfg.constraint = 1 if constraint[0] == "bulkvelocity" else 0
+    cfg.c1, cfg.c2 = constraint[1]
+    return cfg, base, constraint
+
+
 class ChannelFlowProblem:
     """ChannelFlowProblem(grid, profile, nu, dt; pressuregradient | bulkvelocity)
     (src/problem.jl:69-107) with the rotational form and NoForcing, on the B200.
@@ -146,41 +189,29 @@ class ChannelFlowProblem:
     """
 
     def __init__(self, grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None, forcing=None, form=None):
-        if pressuregradient is not None and bulkvelocity is not None:
-            raise ValueError("specify either pressuregradient or bulkvelocity")
-        if forcing is not None:
-            raise ValueError("only NoForcing is accelerated by the engine")
-        if form not in (None, "rotational"):
-            raise ValueError("only the rotational nonlinear form is accelerated by the engine")
+        cfg, self._base, self.constraint = _make_config(grid, profile, nu, dt, pressuregradient, bulkvelocity,
+                                                        forcing, form)
         self.grid = grid
         self.nu, self.dt = float(nu), float(dt)
-        if bulkvelocity is not None:
-            self.constraint = ("bulkvelocity", tuple(float(v) for v in bulkvelocity))
-        else:
-            pg = (0.0, 0.0) if pressuregradient is None else pressuregradient
-            self.constraint = ("pressuregradient", tuple(float(v) for v in pg))
-        kind = 1 if self.constraint[0] == "bulkvelocity" else 0
-        cfg = _Config()
-        cfg.Nx, cfg.Ny, cfg.Nz = grid.Nx, grid.Ny, grid.Nz
-        cfg.Lx, cfg.Lz, cfg.nu, cfg.dt = grid.Lx, grid.Lz, self.nu, self.dt
-        self._base = None
-        if profile == "couette":
-            cfg.profile = 0
-        elif profile == "poiseuille":
-            cfg.profile = 1
-        else:
-            cfg.profile = 2
-            self._base = np.ascontiguousarray([float(profile(v)) for v in grid.y], dtype=np.float64)
-            cfg.base_values = _ptr(self._base)
-        cfg.constraint = kind
-        cfg.c1, cfg.c2 = self.constraint[1]
         h = ctypes.c_void_p()
         _check(lib().cf_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
+        self._owned = True
+
+    @classmethod
+    def _borrow(cls, handle, grid, nu, dt, constraint):
+        """View of a handle owned elsewhere (an ensemble instance)."""
+        self = cls.__new__(cls)
+        self.grid, self.nu, self.dt, self.constraint = grid, float(nu), float(dt), constraint
+        self._base = None
+        self._h = ctypes.c_void_p(handle)
+        self._owned = False
+        return self
 
     def close(self):
         if getattr(self, "_h", None) and _lib is not None:
-            _lib.cf_destroy(self._h)
+            if getattr(self, "_owned", True):
+                _lib.cf_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -247,6 +278,58 @@ class ChannelFlowProblem:
         out = np.zeros(5)
         _check(lib().cf_diagnostics(self._h, _ptr(out)))
         return out
+
+
+class Ensemble:
+    """Many independent channels advanced together (cf_create_batch): each
+    member is given as (grid, profile, nu, dt, constraint keywords) and is
+    reachable as an ordinary problem through ``instances``; ``step`` advances
+    all of them with one graph per step, every kernel launched once per size
+    class."""
+
+    def __init__(self, members):
+        members = list(members)
+        n = len(members)
+        cfgs = (_Config * n)()
+        self._keep = []
+        specs = []
+        for i, m in enumerate(members):
+            kw = dict(m)
+            grid, profile, nu, dt = kw.pop("grid"), kw.pop("profile"), kw.pop("nu"), kw.pop("dt")
+            cfg, base, constraint = _make_config(grid, profile, nu, dt, **kw)
+            cfgs[i] = cfg
+            self._keep.append(base)
+            specs.append((grid, nu, dt, constraint))
+        h = ctypes.c_void_p()
+        _check(lib().cf_create_batch(cfgs, n, ctypes.byref(h)))
+        self._h = h
+        self.instances = []
+        for i, (grid, nu, dt, constraint) in enumerate(specs):
+            ih = lib().cf_batch_instance(self._h, i)
+            self.instances.append(ChannelFlowProblem._borrow(ih, grid, nu, dt, constraint))
+
+    def __len__(self):
+        return len(self.instances)
+
+    def step(self, nsteps=1):
+        """nsteps CNRK2 steps of every member (asynchronous on the ensemble's stream)."""
+        _check(lib().cf_step_batch(self._h, int(nsteps)))
+
+    def stream_ptr(self):
+        return lib().cf_batch_stream(self._h)
+
+    def launches(self):
+        return lib().cf_batch_last_launch_count(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            for p in self.instances:
+                p._h = None
+            _lib.cf_destroy_batch(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def CouetteFlow(grid, nu, dt, **kw):

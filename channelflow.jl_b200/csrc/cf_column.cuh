@@ -211,7 +211,7 @@ CF_DEV void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, 
 }
 
 // DCT-I (REDFT00) of complex x[0..P] in place (parity layout).  z and z2 are
-// transform buffers of round_up(P, 8) complex (swizzled positions).
+// transform buffers of fft_bufsz(P) complex (padded positions fpos).
 // X_k = x_0 + (-1)^k x_P + 2 sum_{n=1}^{P-1} x_n cos(pi n k/P).  With
 // z_n = (x_n + x_{P-n})/2 - sin(pi n/P)(x_n - x_{P-n}) and Z = FFT_P(z):
 //   X_{2m} = Z_m + Z_{P-m},  X_1 = x_0 - x_P + 2 sum_{n=1}^{P-1} x_n cos(pi n/P),
@@ -236,16 +236,16 @@ CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const F
     for (int n = t.tid; n <= H; n += CF_TEAM) {
         if (n == 0) {
             zd a = x[0], b = x[ppos(P, hs)];
-            z[swz(0)] = zscale(zadd(a, b), 0.5 * we);
+            z[fpos(0)] = zscale(zadd(a, b), 0.5 * we);
             x1 = zaxpy(x1, we, zsub(a, b));
         } else if (n == H) {
-            z[swz(H)] = zscale(x[ppos(H, hs)], wi);
+            z[fpos(H)] = zscale(x[ppos(H, hs)], wi);
         } else {
             zd a = x[ppos(n, hs)], b = x[ppos(P - n, hs)];
             zd c = __ldg(cs + n);
             zd h = zscale(zadd(a, b), 0.5 * wi), d = zscale(zsub(a, b), wi);
-            z[swz(n)] = zaxpy(h, -c.y, d);
-            z[swz(P - n)] = zaxpy(h, c.y, d);
+            z[fpos(n)] = zaxpy(h, -c.y, d);
+            z[fpos(P - n)] = zaxpy(h, c.y, d);
             x1 = zaxpy(x1, 2.0 * c.x, d);
         }
     }
@@ -253,7 +253,7 @@ CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const F
     if (t.lane == 0) t.xch[t.q] = x1;
     tsync(t);
     x1 = zadd(t.xch[0], t.xch[1]);
-    const zd* Z = group_fft_L<true, PL>(z, z2, 1, (P + 7) & ~7, pl, -1, t.tid, CF_TEAM, t.bar);
+    const zd* Z = group_fft_L<true, PL>(z, z2, 1, fft_bufsz(P), pl, -1, t.tid, CF_TEAM, t.bar);
     if (t.q == 1) {
         // odd outputs X_{2m+1}, m = 0..H-1: X_1 plus prefix sums of
         // i (Z_m - Z_{P-m}), in runs of E (odd) consecutive m per lane
@@ -263,21 +263,21 @@ CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const F
         zd tot = zzero();
         for (int s = 0; s < E; ++s) {
             const int m = m0 + s;
-            if (m >= 1 && m < H) tot = zadd(tot, zmuli(zsub(Z[swz(m)], Z[swz(P - m)])));
+            if (m >= 1 && m < H) tot = zadd(tot, zmuli(zsub(Z[fpos(m)], Z[fpos(P - m)])));
         }
         zd run = zadd(x1, warp_excl_z(warp_scan_z(tot, lane), lane));
         zd* xo = x + hs;  // X_{2m+1} at xo[m]
         for (int s = 0; s < E; ++s) {
             const int m = m0 + s;
             if (m < H) {
-                if (m >= 1) run = zadd(run, zmuli(zsub(Z[swz(m)], Z[swz(P - m)])));
+                if (m >= 1) run = zadd(run, zmuli(zsub(Z[fpos(m)], Z[fpos(P - m)])));
                 xo[m] = run;
             }
         }
     } else {
         for (int m = t.lane; m <= H; m += 32)
-            x[m] = (m == 0 || m == H) ? zscale(Z[swz(m)], MODE == CF_DCT_FWD ? 1.0 : 2.0)
-                                      : zadd(Z[swz(m)], Z[swz(P - m)]);
+            x[m] = (m == 0 || m == H) ? zscale(Z[fpos(m)], MODE == CF_DCT_FWD ? 1.0 : 2.0)
+                                      : zadd(Z[fpos(m)], Z[fpos(P - m)]);
     }
     tsync(t);
 }

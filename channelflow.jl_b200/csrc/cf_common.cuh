@@ -31,6 +31,17 @@ CF_DEV void prefetch_l2(const void* p, long bytes, int tid, int nth) {
         asm volatile("prefetch.global.L2 [%0];" ::"l"(c + off));
 }
 
+// Copy of one instance's parameters into shared memory (batched launches:
+// the block's instance is picked by a grid coordinate).
+template <class T>
+CF_DEV void stage_params(T* dst, const T* __restrict__ src) {
+    static_assert(sizeof(T) % 8 == 0, "parameter blocks are copied as 8-byte words");
+    const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(T) / 8); i += blockDim.x) d[i] = s[i];
+    __syncthreads();
+}
+
 // ------------------------------------------------------------- warp utils
 CF_DEV double shfl_up_d(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
 CF_DEV double shfl_d(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }

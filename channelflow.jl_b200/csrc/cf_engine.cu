@@ -79,7 +79,8 @@ static int fail(int code, const std::string& msg) {
         cudaError_t e_ = (call);                                                          \
         if (e_ != cudaSuccess) {                                                          \
             return fail(e_ == cudaErrorMemoryAllocation ? CF_E_NOMEM : CF_E_CUDA,         \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
+                        std::string(#call) + " (cf_engine.cu:" + std::to_string(__LINE__) + \
+                            "): " + cudaGetErrorString(e_));                              \
         }                                                                                 \
     } while (0)
 
@@ -268,6 +269,16 @@ static std::vector<int> fft_radices(int n) {
 }
 
 static int rup8(int x) { return (x + 7) & ~7; }
+// transform-buffer strides and shared memory of the periodic FFT kernels
+static int zbs(const cf_engine* h) { return fft_bufsz(h->Nzp) + 1; }
+static int xbs(const cf_engine* h) { return fft_bufsz(h->Nxp); }
+static size_t zsmem(const cf_engine* h) { return (size_t)2 * h->tkz * zbs(h) * sizeof(zd); }
+static size_t xsmem(const cf_engine* h) { return (size_t)12 * xbs(h) * sizeof(zd); }
+static int ilog2(int v) {
+    int r = 0;
+    while ((1 << (r + 1)) <= v) ++r;
+    return r;
+}
 
 // radices above 31 do not fit the packed plan (5 bits per pass)
 static bool radices_ok(const std::vector<int>& rad) {
@@ -439,12 +450,13 @@ static int build_neumann(cf_engine* h) {
     return CF_OK;
 }
 
-// column stride (complex) in shared memory: a parity-split vector (2 (P/2 + 1)
-// entries) and a round_up(P, 8) transform buffer both fit
-static int col_stride(const cf_engine* h) { return std::max(h->P + 2, rup8(h->P)); }
-// 8 regions per column plus 2 complex of team scratch per column
+// column strides (complex) in shared memory: regions 0-5 hold parity-split
+// vectors (2 (P/2 + 1) entries), regions 6-7 transform buffers (fft_bufsz(P))
+static int col_stride(const cf_engine* h) { return h->P + 2; }
+static int col_zstride(const cf_engine* h) { return std::max(h->P + 2, fft_bufsz(h->P)); }
+// per column: 6 vectors, 2 transform buffers and 2 complex of team scratch
 static size_t col_smem(const cf_engine* h) {
-    return ((size_t)8 * CF_NCOL * col_stride(h) + 2 * CF_NCOL) * sizeof(zd);
+    return ((size_t)CF_NCOL * (6 * col_stride(h) + 2 * col_zstride(h)) + 2 * CF_NCOL) * sizeof(zd);
 }
 
 static ColParams col_params(const cf_engine* h) {
@@ -452,6 +464,7 @@ static ColParams col_params(const cf_engine* h) {
     std::memset(&p, 0, sizeof(p));
     p.Nx = h->Nx; p.Nz = h->Nz; p.Nxh = h->Nxh; p.Ny = h->Ny; p.P = h->P; p.B = (int)h->B;
     p.cs = col_stride(h);
+    p.zs = col_zstride(h);
     p.ax = 2 * M_PI / h->Lx; p.bz = 2 * M_PI / h->Lz;
     p.nu = h->nu;
     for (int i = 0; i < 3; ++i) { p.U[i] = h->U[i]; p.Q[i] = h->Q[i]; p.Nn[i] = h->nod[i]; p.Nout[i] = nullptr; }
@@ -474,9 +487,9 @@ static ColParams col_params(const cf_engine* h) {
 static FftParams fft_params(const cf_engine* h) {
     FftParams f;
     f.Nx = h->Nx; f.Nz = h->Nz; f.Nxh = h->Nxh; f.Ny = h->Ny; f.Nzp = h->Nzp; f.Nxp = h->Nxp;
-    f.tkz = h->tkz;
-    f.bsz = rup8(h->Nzp);
-    f.bsx = rup8(h->Nxp);
+    f.tks = ilog2(h->tkz);
+    f.bsz = zbs(h);
+    f.bsx = xbs(h);
     f.nod0 = h->nod[0]; f.nod1 = h->nod[1]; f.nod2 = h->nod[2]; f.nod3 = h->nod[3]; f.nod4 = h->nod[4]; f.nod5 = h->nod[5];
     f.zp0 = h->zp[0]; f.zp1 = h->zp[1]; f.zp2 = h->zp[2]; f.zp3 = h->zp[3]; f.zp4 = h->zp[4]; f.zp5 = h->zp[5];
     f.plZ = h->plZ; f.plX = h->plX;
@@ -486,8 +499,7 @@ static FftParams fft_params(const cf_engine* h) {
 // nonlinear periodic transforms: nodal (6) -> nonlinear term at nodes (nod[0..2])
 static int launch_periodic(cf_engine* h, int* count) {
     FftParams f = fft_params(h);
-    const size_t smz = (size_t)2 * h->tkz * rup8(h->Nzp) * sizeof(zd);
-    const size_t smx = (size_t)12 * rup8(h->Nxp) * sizeof(zd);
+    const size_t smz = zsmem(h), smx = xsmem(h);
     dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
     fft_kernel(KF_ZINV, h->Nzp)<<<gz, 256, smz, h->stream>>>(f);
     dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
@@ -510,9 +522,8 @@ static int launch_prep(cf_engine* h, zd* const Usrc[3], int* count) {
     return CF_OK;
 }
 
-static int launch_stage(cf_engine* h, int j, int* count) {
-    int rc = launch_periodic(h, count);
-    if (rc) return rc;
+// column-kernel parameters of CNRK2 stage j (cnrk2.jl:588-623)
+static ColParams stage_col_params(const cf_engine* h, int j) {
     ColParams p = col_params(h);
     p.lambda = 1.0 / (CC[j] * h->dt);
     p.weight = CB[j] / CC[j];
@@ -520,6 +531,12 @@ static int launch_stage(cf_engine* h, int j, int* count) {
     p.stage = j;
     p.store_q = (j < 2) ? 1 : 0;
     p.bank = h->bank[j].view();
+    return p;
+}
+static int launch_stage(cf_engine* h, int j, int* count) {
+    int rc = launch_periodic(h, count);
+    if (rc) return rc;
+    ColParams p = stage_col_params(h, j);
     col_kernel(KC_STAGE, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
@@ -530,8 +547,7 @@ static int launch_stage(cf_engine* h, int j, int* count) {
 // xpass, zfwd, column) recorded on the handle's stream.
 static int launch_step_profiled(cf_engine* h, cudaEvent_t* ev, double* acc) {
     FftParams f = fft_params(h);
-    const size_t smz = (size_t)2 * h->tkz * rup8(h->Nzp) * sizeof(zd);
-    const size_t smx = (size_t)12 * rup8(h->Nxp) * sizeof(zd);
+    const size_t smz = zsmem(h), smx = xsmem(h);
     dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
     dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
     dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
@@ -594,16 +610,31 @@ static int build_graph(cf_engine* h) {
     return CF_OK;
 }
 
+// Raise a kernel's dynamic shared-memory limit to at least `need`.  The limit
+// belongs to the kernel, not to a handle: handles of different grids share the
+// run-time-sized instantiations, so it is only ever raised.
+static std::mutex g_attr_mu;
+template <class K>
+static int raise_smem_limit(K* fn, size_t need) {
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    cudaFuncAttributes a;
+    CU(cudaFuncGetAttributes(&a, (const void*)fn));
+    if ((size_t)a.maxDynamicSharedSizeBytes < need)
+        CU(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    return CF_OK;
+}
+
 static int set_attrs(cf_engine* h) {
     const int maxsm = 227 * 1024;
-    size_t need[3] = {col_smem(h), (size_t)2 * h->tkz * rup8(h->Nzp) * sizeof(zd), (size_t)12 * rup8(h->Nxp) * sizeof(zd)};
+    size_t need[3] = {col_smem(h), zsmem(h), xsmem(h)};
     for (size_t x : need)
         if (x > (size_t)maxsm) return fail(CF_E_UNSUPPORTED, "grid too large for the shared-memory tiles");
+    int rc;
     for (int w = 0; w < KC_COUNT; ++w)
-        CU(cudaFuncSetAttribute(col_kernel(w, h->P), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[0]));
-    CU(cudaFuncSetAttribute(fft_kernel(KF_ZINV, h->Nzp), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[1]));
-    CU(cudaFuncSetAttribute(fft_kernel(KF_ZFWD, h->Nzp), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[1]));
-    CU(cudaFuncSetAttribute(fft_kernel(KF_XPASS, h->Nxp), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need[2]));
+        if ((rc = raise_smem_limit(col_kernel(w, h->P), need[0]))) return rc;
+    if ((rc = raise_smem_limit(fft_kernel(KF_ZINV, h->Nzp), need[1]))) return rc;
+    if ((rc = raise_smem_limit(fft_kernel(KF_ZFWD, h->Nzp), need[1]))) return rc;
+    if ((rc = raise_smem_limit(fft_kernel(KF_XPASS, h->Nxp), need[2]))) return rc;
     return CF_OK;
 }
 
@@ -629,15 +660,15 @@ static int validate_and_size(cf_engine* h, const cf_config* c) {
     std::vector<int> rP = fft_radices(h->P), rZ = fft_radices(h->Nzp), rX = fft_radices(h->Nxp);
     if (!radices_ok(rP) || rP.size() > CF_FFT_MAXPASS)
         return fail(CF_E_UNSUPPORTED, "Chebyshev transform length not supported (prime factors <= 31)");
-    if (!radices_ok(rX) || rX.size() > CF_FFT_MAXPASS || (size_t)12 * rup8(h->Nxp) * 16 > 227 * 1024)
+    if (!radices_ok(rX) || rX.size() > CF_FFT_MAXPASS || (size_t)12 * fft_bufsz(h->Nxp) * 16 > 227 * 1024)
         return fail(CF_E_UNSUPPORTED, "padded x length not supported");
     if (!radices_ok(rZ) || rZ.size() > CF_FFT_MAXPASS)
         return fail(CF_E_UNSUPPORTED, "padded z length not supported");
     // z kernels: two tkz x Nzp buffers; keep them near 74 KB (three blocks per SM)
     h->tkz = 0;
     for (int t : {8, 4, 2, 1})
-        if ((size_t)2 * t * rup8(h->Nzp) * 16 <= 74 * 1024 || t == 1) { h->tkz = t; break; }
-    if ((size_t)2 * h->tkz * rup8(h->Nzp) * 16 > 227 * 1024) return fail(CF_E_UNSUPPORTED, "padded z length not supported");
+        if ((size_t)2 * t * (fft_bufsz(h->Nzp) + 1) * 16 <= 74 * 1024 || t == 1) { h->tkz = t; break; }
+    if (zsmem(h) > (size_t)227 * 1024) return fail(CF_E_UNSUPPORTED, "padded z length not supported");
     return CF_OK;
 }
 
@@ -1080,3 +1111,242 @@ static void host_synth(const cf_engine* h, uint64_t seed, double amp, int shape,
             for (int iz = (h->Nz >> 1) + 1; iz < h->Nz; ++iz) col[(long)iz * h->Nxh] = std::conj(col[(long)(h->Nz - iz) * h->Nxh]);
         }
 }
+
+// ---------------------------------------------------------------------------
+// Ensembles: independent channels (grids, Re, seeds) advanced together.
+// Instances with the same grid form a size class.  Every stage launches each
+// of the four kernels once per class over all of its instances (a grid
+// coordinate selects the instance, whose parameters the block stages in
+// shared memory), and the classes run as parallel branches of one CUDA graph
+// per step: 12 launches per class per step, whatever the instance count.
+// ---------------------------------------------------------------------------
+typedef void (*ColBatchKernel)(const ColParams*);
+typedef void (*FftBatchKernel)(const FftParams*);
+
+static ColBatchKernel col_batch_kernel(int P) {
+    switch (P) {
+#define CF_CASE(N) \
+    case N: return k_column_stage_batch<CF_NCOL, N>;
+        CF_COL_LENGTHS(CF_CASE)
+#undef CF_CASE
+        default: return k_column_stage_batch<CF_NCOL, 0>;
+    }
+}
+template <int L>
+static FftBatchKernel fft_batch_kernel_t(int which) {
+    switch (which) {
+        case KF_ZINV: return k_zinv_batch<L>;
+        case KF_ZFWD: return k_zfwd_batch<L>;
+        default: return k_xpass_batch<L>;
+    }
+}
+static FftBatchKernel fft_batch_kernel(int which, int L) {
+    switch (L) {
+#define CF_CASE(N) \
+    case N: return fft_batch_kernel_t<N>(which);
+        CF_STATIC_FFT_LENGTHS(CF_CASE)
+#undef CF_CASE
+        default: return fft_batch_kernel_t<0>(which);
+    }
+}
+
+struct BatchClass {
+    int Nx = 0, Ny = 0, Nz = 0;
+    std::vector<int> members;
+    FftParams* d_fft = nullptr;
+    ColParams* d_col[3] = {nullptr, nullptr, nullptr};
+    std::vector<FftParams> h_fft;
+    std::vector<ColParams> h_col[3];
+    cudaStream_t side = nullptr;
+    cudaEvent_t join = nullptr;
+};
+
+struct cf_batch {
+    std::vector<cf_engine*> inst;
+    std::vector<BatchClass> cls;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, done = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    std::vector<void*> allocs;
+    int last_launches = 0;
+};
+
+void cf_destroy_batch(cf_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (BatchClass& c : b->cls) {
+        if (c.side) cudaStreamDestroy(c.side);
+        if (c.join) cudaEventDestroy(c.join);
+    }
+    for (void* p : b->allocs) cudaFree(p);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    for (cf_engine* h : b->inst) cf_destroy(h);
+    delete b;
+}
+
+static int batch_alloc(cf_batch* b, void** p, size_t bytes) {
+    if (cudaMalloc(p, bytes) != cudaSuccess) return fail(CF_E_NOMEM, "device allocation failed");
+    b->allocs.push_back(*p);
+    return CF_OK;
+}
+
+// Parameters of every instance (host copies refreshed from the instances,
+// so constraint changes made through an instance handle take effect).
+static int batch_upload(cf_batch* b) {
+    for (BatchClass& c : b->cls) {
+        for (size_t k = 0; k < c.members.size(); ++k) {
+            cf_engine* h = b->inst[c.members[k]];
+            c.h_fft[k] = fft_params(h);
+            for (int j = 0; j < 3; ++j) c.h_col[j][k] = stage_col_params(h, j);
+        }
+        CU(cudaMemcpyAsync(c.d_fft, c.h_fft.data(), sizeof(FftParams) * c.h_fft.size(), cudaMemcpyHostToDevice,
+                           b->stream));
+        for (int j = 0; j < 3; ++j)
+            CU(cudaMemcpyAsync(c.d_col[j], c.h_col[j].data(), sizeof(ColParams) * c.h_col[j].size(),
+                               cudaMemcpyHostToDevice, b->stream));
+    }
+    CU(cudaStreamSynchronize(b->stream));
+    return CF_OK;
+}
+
+int cf_create_batch(const cf_config* cfgs, int n, cf_batch** out) {
+    if (!cfgs || n <= 0 || !out) return fail(CF_E_ARG, "null argument or empty ensemble");
+    *out = nullptr;
+    cf_batch* b = new cf_batch();
+    auto bail = [&](int code) {
+        cf_destroy_batch(b);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(CF_E_CUDA, "cannot create stream (no CUDA device?)"));
+    for (int i = 0; i < n; ++i) {
+        cf_handle* h = nullptr;
+        int rc = cf_create(cfgs + i, &h);
+        if (rc) return bail(rc);
+        b->inst.push_back(h);
+    }
+    for (int i = 0; i < n; ++i) {
+        cf_engine* h = b->inst[i];
+        BatchClass* c = nullptr;
+        for (BatchClass& x : b->cls)
+            if (x.Nx == h->Nx && x.Ny == h->Ny && x.Nz == h->Nz) c = &x;
+        if (!c) {
+            b->cls.emplace_back();
+            c = &b->cls.back();
+            c->Nx = h->Nx;
+            c->Ny = h->Ny;
+            c->Nz = h->Nz;
+        }
+        c->members.push_back(i);
+    }
+    for (BatchClass& c : b->cls) {
+        const int m = (int)c.members.size();
+        cf_engine* r = b->inst[c.members[0]];
+        if (6L * m > 65535) return bail(fail(CF_E_UNSUPPORTED, "more than 10922 instances of one grid"));
+        if (col_smem(r) + sizeof(ColParams) > (size_t)227 * 1024)
+            return bail(fail(CF_E_UNSUPPORTED, "Ny too large for the batched column kernel"));
+        c.h_fft.resize(m);
+        int rc;
+        if ((rc = batch_alloc(b, (void**)&c.d_fft, sizeof(FftParams) * m))) return bail(rc);
+        for (int j = 0; j < 3; ++j) {
+            c.h_col[j].resize(m);
+            if ((rc = batch_alloc(b, (void**)&c.d_col[j], sizeof(ColParams) * m))) return bail(rc);
+        }
+        const size_t smz = zsmem(r), smx = xsmem(r);
+        if ((rc = raise_smem_limit(col_batch_kernel(r->P), col_smem(r))) ||
+            (rc = raise_smem_limit(fft_batch_kernel(KF_ZINV, r->Nzp), smz)) ||
+            (rc = raise_smem_limit(fft_batch_kernel(KF_ZFWD, r->Nzp), smz)) ||
+            (rc = raise_smem_limit(fft_batch_kernel(KF_XPASS, r->Nxp), smx)))
+            return bail(rc);
+        if (cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c.join, cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(CF_E_CUDA, "cannot create stream"));
+    }
+    int rc = batch_upload(b);
+    if (rc) return bail(rc);
+    *out = b;
+    return CF_OK;
+}
+
+// The four launches of stage j for one size class on stream s.
+static int launch_class_stage(const cf_batch* b, const BatchClass& c, int j, cudaStream_t s) {
+    const cf_engine* r = b->inst[c.members[0]];
+    const unsigned m = (unsigned)c.members.size();
+    const size_t smz = zsmem(r), smx = xsmem(r);
+    const unsigned gzx = (unsigned)((r->Nxh + r->tkz - 1) / r->tkz);
+    fft_batch_kernel(KF_ZINV, r->Nzp)<<<dim3(gzx, r->Ny, 6 * m), 256, smz, s>>>(c.d_fft);
+    fft_batch_kernel(KF_XPASS, r->Nxp)<<<dim3((r->Nzp + 1) / 2, r->Ny, m), 256, smx, s>>>(c.d_fft);
+    fft_batch_kernel(KF_ZFWD, r->Nzp)<<<dim3(gzx, r->Ny, 3 * m), 256, smz, s>>>(c.d_fft);
+    col_batch_kernel(r->P)<<<dim3(col_blocks(r), m), CF_NCOL * CF_TEAM, col_smem(r), s>>>(c.d_col[j]);
+    CU(cudaGetLastError());
+    return CF_OK;
+}
+
+static int build_batch_graph(cf_batch* b) {
+    if (b->graph) return CF_OK;
+    cudaGraph_t g;
+    CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = CF_OK;
+    if (cudaEventRecord(b->fork, b->stream) != cudaSuccess) rc = fail(CF_E_CUDA, "event record");
+    for (BatchClass& c : b->cls)
+        if (!rc && cudaStreamWaitEvent(c.side, b->fork, 0) != cudaSuccess) rc = fail(CF_E_CUDA, "stream wait");
+    for (int j = 0; j < 3 && !rc; ++j)
+        for (BatchClass& c : b->cls)
+            if (!rc) rc = launch_class_stage(b, c, j, c.side);
+    for (BatchClass& c : b->cls) {
+        if (!rc && cudaEventRecord(c.join, c.side) != cudaSuccess) rc = fail(CF_E_CUDA, "event record");
+        if (!rc && cudaStreamWaitEvent(b->stream, c.join, 0) != cudaSuccess) rc = fail(CF_E_CUDA, "stream wait");
+    }
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) {
+        if (e == cudaSuccess) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(CF_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(CF_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return CF_OK;
+}
+
+int cf_batch_size(cf_batch* b) { return b ? (int)b->inst.size() : 0; }
+
+cf_handle* cf_batch_instance(cf_batch* b, int i) {
+    if (!b || i < 0 || i >= (int)b->inst.size()) {
+        fail(CF_E_ARG, "instance index out of range");
+        return nullptr;
+    }
+    return b->inst[i];
+}
+
+int cf_step_batch(cf_batch* b, int nsteps) {
+    if (!b) return fail(CF_E_ARG, "null ensemble");
+    if (nsteps < 0) return fail(CF_E_ARG, "nsteps must be nonnegative");
+    int rc, cnt = 0;
+    // instance streams: work queued through instance handles finishes first;
+    // nodal fields of instances whose state was set are rebuilt
+    for (cf_engine* h : b->inst) {
+        if (!h->nodal_valid) {
+            if ((rc = launch_prep(h, h->U, &cnt))) return rc;
+            h->nodal_valid = true;
+        }
+        CU(cudaStreamSynchronize(h->stream));
+    }
+    if ((rc = batch_upload(b))) return rc;
+    if ((rc = build_batch_graph(b))) return rc;
+    for (int s = 0; s < nsteps; ++s) CU(cudaGraphLaunch(b->graph, b->stream));
+    cnt += 12 * (int)b->cls.size() * nsteps;
+    b->last_launches = cnt;
+    // later work through an instance handle waits for the ensemble's steps
+    CU(cudaEventRecord(b->done, b->stream));
+    for (cf_engine* h : b->inst) CU(cudaStreamWaitEvent(h->stream, b->done, 0));
+    return CF_OK;
+}
+
+int cf_batch_last_launch_count(cf_batch* b) { return b ? b->last_launches : 0; }
+void* cf_batch_stream(cf_batch* b) { return b ? (void*)b->stream : nullptr; }

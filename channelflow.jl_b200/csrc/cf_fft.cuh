@@ -32,12 +32,14 @@ CF_DEV void group_sync(int bar, int) {
     else __syncthreads();
 }
 
-// Shared-memory position of element e of a transform buffer.  The low three
-// bits are XOR-ed with bits 3-5 and 6-8, so the stride-R stores of a Stockham
-// pass (and the strided loads of the scans) spread over all eight 16-byte bank
-// groups.  A transform buffer must hold round_up(L, 8) elements (the swizzle
-// stays inside each aligned block of eight).
-CF_DEV int swz(int e) { return e ^ (((e >> 3) ^ (e >> 6)) & 7); }
+// Shared-memory position of element e of a transform buffer: one pad slot
+// after every 8 elements.  The stride-R stores of a Stockham pass then spread
+// over the eight 16-byte bank groups, and an offset that is a multiple of 8
+// elements is a constant position offset (9/8 of it), so the strided
+// addresses of a butterfly cost one position computation.
+CF_DEV int fpos(int e) { return e + (e >> 3); }
+// complex slots a transform buffer of length L occupies (multiple of 8)
+__host__ __device__ constexpr int fft_bufsz(int L) { return ((L + (L >> 3) + 1) + 7) & ~7; }
 
 CF_DEV zd tw_get(const zd* tw, int k, int sgn) {
     zd w = __ldg(tw + k);
@@ -201,14 +203,14 @@ CF_DEV void fft_pass_pp(const zd* __restrict__ src, zd* __restrict__ dst, int nb
         zd v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            zd x = s[swz(j + r * NBf)];
+            zd x = s[fpos(j + r * NBf)];
             v[r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
         }
         dft_small<R>(v, sgn);
         zd* d = dst + (long)b * bs;
         const int o = (j / Ns) * Ns * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) d[swz(o + r * Ns)] = v[r];
+        for (int r = 0; r < R; ++r) d[fpos(o + r * Ns)] = v[r];
     }
     group_sync<BLOCK>(bar, nth);
 }
@@ -230,40 +232,48 @@ CF_DEV void fft_pass_pp_generic(const zd* __restrict__ src, zd* __restrict__ dst
         for (int o = 0; o < R; ++o) {
             zd acc = zzero();
             for (int r = 0; r < R; ++r) {
-                zd x = s[swz(j + r * NBf)];
+                zd x = s[fpos(j + r * NBf)];
                 if (r != 0 && k != 0) x = zmul(x, tw_get(tw, k * r * step, sgn));
                 acc = zadd(acc, (r == 0) ? x : zmul(x, tw_get(tw, ((o * r) % R) * NBf, sgn)));
             }
-            d[swz(ob + o * Ns)] = acc;
+            d[fpos(ob + o * Ns)] = acc;
         }
     }
     group_sync<BLOCK>(bar, nth);
 }
 
 // Compile-time-sized pass: L, Ns and R are constants, so the batch/butterfly
-// index split and the twiddle indices need no run-time division.
+// index split and the twiddle indices need no run-time division, and the R
+// strided positions are one fpos() plus constant offsets where the stride is a
+// multiple of 8 (or the R outputs stay inside one group of 8).
 template <bool BLOCK, int L, int Ns, int R>
 CF_DEV void fft_pass_static(const zd* __restrict__ src, zd* __restrict__ dst, int nb, int bs,
                             const zd* __restrict__ tw, int sgn, int tid, int nth, int bar) {
     constexpr int NBf = L / R;
     constexpr int step = L / (Ns * R);
+    constexpr bool LIN_LD = (NBf % 8) == 0;
+    constexpr bool LIN_ST = (Ns % 8) == 0 || (Ns == 1 && 8 % R == 0);
+    constexpr int DLD = NBf + NBf / 8;
+    constexpr int DST = (Ns == 1) ? 1 : Ns + Ns / 8;
     const int total = nb * NBf;
 #pragma unroll 2
     for (int q = tid; q < total; q += nth) {
         const int b = q / NBf, j = q - b * NBf;
         const int k = j % Ns;
         const zd* s = src + (long)b * bs;
+        const int pj = fpos(j);
         zd v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            zd x = s[swz(j + r * NBf)];
+            zd x = s[LIN_LD ? pj + r * DLD : fpos(j + r * NBf)];
             v[r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
         }
         dft_small<R>(v, sgn);
         zd* d = dst + (long)b * bs;
         const int o = (j / Ns) * Ns * R + k;
+        const int po = fpos(o);
 #pragma unroll
-        for (int r = 0; r < R; ++r) d[swz(o + r * Ns)] = v[r];
+        for (int r = 0; r < R; ++r) d[LIN_ST ? po + r * DST : fpos(o + r * Ns)] = v[r];
     }
     group_sync<BLOCK>(bar, nth);
 }
@@ -277,9 +287,9 @@ CF_DEV zd* fft_static(zd* src, zd* dst, int nb, int bs, const zd* tw, int sgn, i
     }
 }
 
-// Full transform of nb sequences (length pl.L, batch stride bs, a multiple of
-// 8, elements at swizzled positions b*bs + swz(e)) held in a; b is a scratch
-// buffer of the same size.  Returns the buffer with the result.
+// Full transform of nb sequences (length pl.L, batch stride bs >=
+// fft_bufsz(L), element e of sequence b at b*bs + fpos(e)) held in a; b is a
+// scratch buffer of the same size.  Returns the buffer with the result.
 template <bool BLOCK>
 CF_DEV zd* group_fft(zd* a, zd* b, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
     int Ns = 1;

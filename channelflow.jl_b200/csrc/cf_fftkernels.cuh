@@ -6,14 +6,14 @@
 // k_xpass: backward x c2r of the six rows (pairs packed as one complex FFT),
 //          n = u x omega at the padded points, forward x r2c, x truncation
 // k_zfwd : forward z FFT of the three products, z truncation (copy_from_padded!)
-// Shared-memory transform buffers use the swizzled positions of cf_fft.cuh.
+// Shared-memory transform buffers use the padded positions (fpos) of cf_fft.cuh.
 #pragma once
 #include "cf_fft.cuh"
 
 struct FftParams {
     int Nx, Nz, Nxh, Ny, Nzp, Nxp;
-    int tkz;       // columns per block in the z kernels
-    int bsz, bsx;  // transform buffer strides: Nzp, Nxp rounded up to 8
+    int tks;       // log2 of the columns per block in the z kernels
+    int bsz, bsx;  // transform buffer strides: fft_bufsz(Nzp) + 1 (odd), fft_bufsz(Nxp)
     zd *nod0, *nod1, *nod2, *nod3, *nod4, *nod5;  // nodal fields
     zd *zp0, *zp1, *zp2, *zp3, *zp4, *zp5;        // z-padded fields
     FftPlan plZ, plX;
@@ -34,75 +34,77 @@ CF_DEV zd* zp_of(const FftParams& p, int i) { return sel6(p.zp0, p.zp1, p.zp2, p
 
 CF_DEV int zpad_index(int iz, int Nz, int Nzp) { return iz <= (Nz >> 1) ? iz : Nzp - (Nz - iz); }
 
-// grid: (ceil(Nxh/tkz), Ny, nfields); block 256; smem 2*tkz*bsz complex
+// grid: (ceil(Nxh/tkz), Ny, nfields); block 256; smem 2*tkz*bsz complex.
+// Column t of the block's tkz columns is transform t (stride bsz, odd, so the
+// column-interleaved staging stores hit distinct bank groups).
 template <int LZ>
-__global__ void __launch_bounds__(256) k_zinv(FftParams p) {
+CF_DEV void zinv_body(const FftParams& p, int bx, int n, int f) {
     extern __shared__ zd sm[];
-    const int f = blockIdx.z, n = blockIdx.y, k0 = blockIdx.x * p.tkz;
-    const int tkz = p.tkz, Nz = p.Nz, Nzp = p.Nzp, Nxh = p.Nxh, bs = p.bsz;
+    const int tks = p.tks, tkz = 1 << tks, tm = tkz - 1;
+    const int k0 = bx << tks;
+    const int Nz = p.Nz, Nzp = LZ ? LZ : p.Nzp, Nxh = p.Nxh, bs = p.bsz;
     zd* bufB = sm + tkz * bs;
     const zd* src = nod_of(p, f) + (long)n * Nz * Nxh;
     zd* dst = zp_of(p, f) + (long)n * Nzp * Nxh;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1, znyq = (Nz % 2 == 0) ? Nz / 2 : -1;
     // zero the padding gap
     const int gap0 = (Nz >> 1) + 1, gap1 = Nzp - (Nz - gap0);
-    for (int e = threadIdx.x; e < tkz * (gap1 - gap0); e += blockDim.x) {
-        int t = e % tkz, z = gap0 + e / tkz;
-        sm[t * bs + swz(z)] = zzero();
-    }
+    for (int e = threadIdx.x; e < ((gap1 - gap0) << tks); e += blockDim.x)
+        sm[(e & tm) * bs + fpos(gap0 + (e >> tks))] = zzero();
     // loads batched 8 per thread before their stores (requests in flight)
-    for (int base = threadIdx.x; base < tkz * Nz; base += 8 * 256) {
+    const int ntot = Nz << tks;
+    for (int base = threadIdx.x; base < ntot; base += 8 * 256) {
         zd v[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int e = base + u * 256;
-            const int t = e % tkz, iz = e / tkz, k = k0 + t;
-            const bool nyq = ((p.Nz % 2 == 0) && iz == Nz / 2) || ((p.Nx % 2 == 0) && k == p.Nx / 2);
-            v[u] = (e < tkz * Nz && k < Nxh && !nyq) ? src[(long)iz * Nxh + k] : zzero();
+            const int iz = e >> tks, k = k0 + (e & tm);
+            v[u] = (e < ntot && k < Nxh && iz != znyq && k != xnyq) ? src[(long)iz * Nxh + k] : zzero();
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int e = base + u * 256;
-            if (e < tkz * Nz) sm[(e % tkz) * bs + swz(zpad_index(e / tkz, Nz, Nzp))] = v[u];
+            if (e < ntot) sm[(e & tm) * bs + fpos(zpad_index(e >> tks, Nz, Nzp))] = v[u];
         }
     }
     __syncthreads();
     const zd* res = group_fft_L<true, LZ>(sm, bufB, tkz, bs, p.plZ, +1, threadIdx.x, blockDim.x, 0);
-    for (int e = threadIdx.x; e < tkz * Nzp; e += blockDim.x) {
-        int t = e % tkz, z = e / tkz;
-        int k = k0 + t;
-        if (k < Nxh) dst[(long)z * Nxh + k] = res[t * bs + swz(z)];
+    for (int e = threadIdx.x; e < (Nzp << tks); e += blockDim.x) {
+        const int t = e & tm, z = e >> tks, k = k0 + t;
+        if (k < Nxh) dst[(long)z * Nxh + k] = res[t * bs + fpos(z)];
     }
 }
 
 // grid: (ceil(Nxh/tkz), Ny, 3); forward z FFT and truncation to Nz
 template <int LZ>
-__global__ void __launch_bounds__(256) k_zfwd(FftParams p) {
+CF_DEV void zfwd_body(const FftParams& p, int bx, int n, int f) {
     extern __shared__ zd sm[];
-    const int f = blockIdx.z, n = blockIdx.y, k0 = blockIdx.x * p.tkz;
-    const int tkz = p.tkz, Nz = p.Nz, Nzp = p.Nzp, Nxh = p.Nxh, bs = p.bsz;
+    const int tks = p.tks, tkz = 1 << tks, tm = tkz - 1;
+    const int k0 = bx << tks;
+    const int Nz = p.Nz, Nzp = LZ ? LZ : p.Nzp, Nxh = p.Nxh, bs = p.bsz;
     zd* bufB = sm + tkz * bs;
     const zd* src = zp_of(p, f) + (long)n * Nzp * Nxh;
     zd* dst = nod_of(p, f) + (long)n * Nz * Nxh;
-    for (int base = threadIdx.x; base < tkz * Nzp; base += 8 * 256) {
+    const int ntot = Nzp << tks;
+    for (int base = threadIdx.x; base < ntot; base += 8 * 256) {
         zd v[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int e = base + u * 256;
-            const int k = k0 + e % tkz;
-            v[u] = (e < tkz * Nzp && k < Nxh) ? src[(long)(e / tkz) * Nxh + k] : zzero();
+            const int k = k0 + (e & tm);
+            v[u] = (e < ntot && k < Nxh) ? src[(long)(e >> tks) * Nxh + k] : zzero();
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int e = base + u * 256;
-            if (e < tkz * Nzp) sm[(e % tkz) * bs + swz(e / tkz)] = v[u];
+            if (e < ntot) sm[(e & tm) * bs + fpos(e >> tks)] = v[u];
         }
     }
     __syncthreads();
     const zd* res = group_fft_L<true, LZ>(sm, bufB, tkz, bs, p.plZ, -1, threadIdx.x, blockDim.x, 0);
-    for (int e = threadIdx.x; e < tkz * Nz; e += blockDim.x) {
-        int t = e % tkz, iz = e / tkz;
-        int k = k0 + t;
-        if (k < Nxh) dst[(long)iz * Nxh + k] = res[t * bs + swz(zpad_index(iz, Nz, Nzp))];
+    for (int e = threadIdx.x; e < (Nz << tks); e += blockDim.x) {
+        const int t = e & tm, iz = e >> tks, k = k0 + t;
+        if (k < Nxh) dst[(long)iz * Nxh + k] = res[t * bs + fpos(zpad_index(iz, Nz, Nzp))];
     }
 }
 
@@ -110,12 +112,11 @@ __global__ void __launch_bounds__(256) k_zfwd(FftParams p) {
 // Rows zA = 2*bx and zB = 2*bx+1 of plane n.  Slots 0..5 hold
 // (u0+iu1, u2+iw0, w1+iw2) of row A at 0,2,4 and of row B at 1,3,5.
 template <int LX>
-__global__ void __launch_bounds__(256) k_xpass(FftParams p) {
+CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
     extern __shared__ zd sm[];
-    const int n = blockIdx.y;
-    const int zA = 2 * blockIdx.x, zB = zA + 1;
+    const int zA = 2 * bx, zB = zA + 1;
     const bool hasB = zB < p.Nzp;
-    const int Nxp = p.Nxp, Nxh = p.Nxh, bs = p.bsx;
+    const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsx;
     const int Nxhp = Nxp / 2 + 1;
     const long rowA = ((long)n * p.Nzp + zA) * Nxh;
     const long rowB = ((long)n * p.Nzp + zB) * Nxh;
@@ -147,12 +148,12 @@ __global__ void __launch_bounds__(256) k_xpass(FftParams p) {
             const int slot = e / Nxhp, k = e - slot * Nxhp;
             zd* s = sm + slot * bs;
             if (k == 0) {
-                s[swz(0)] = zmake(X[u].x, Y[u].x);
+                s[fpos(0)] = zmake(X[u].x, Y[u].x);
             } else if (2 * k == Nxp) {
-                s[swz(k)] = zmake(X[u].x, Y[u].x);
+                s[fpos(k)] = zmake(X[u].x, Y[u].x);
             } else {
-                s[swz(k)] = zmake(X[u].x - Y[u].y, X[u].y + Y[u].x);
-                s[swz(Nxp - k)] = zmake(X[u].x + Y[u].y, Y[u].x - X[u].y);
+                s[fpos(k)] = zmake(X[u].x - Y[u].y, X[u].y + Y[u].x);
+                s[fpos(Nxp - k)] = zmake(X[u].x + Y[u].y, Y[u].x - X[u].y);
             }
         }
     }
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(256) k_xpass(FftParams p) {
     zd* Bf = (A == sm) ? scr : sm;
     // rotational product n = u x omega at every padded x point of both rows
     for (int j = threadIdx.x; j < Nxp; j += blockDim.x) {
-        const int sj = swz(j);
+        const int sj = fpos(j);
         zd a0 = A[0 * bs + sj], a1 = A[2 * bs + sj], a2 = A[4 * bs + sj];
         zd b0 = A[1 * bs + sj], b1 = A[3 * bs + sj], b2 = A[5 * bs + sj];
         // row A: u=(a0.x,a0.y,a1.x), w=(a1.y,a2.x,a2.y)
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(256) k_xpass(FftParams p) {
     for (int e = threadIdx.x; e < 3 * Nxh; e += blockDim.x) {
         const int slot = e / Nxh, k = e - slot * Nxh;
         const zd* s = F + slot * bs;
-        zd Zk = s[swz(k)], Zm = s[swz((Nxp - k) % Nxp)];
+        zd Zk = s[fpos(k)], Zm = s[fpos((Nxp - k) % Nxp)];
         // X = (Z_k + conj Z_-k)/2 ; Y = (Z_k - conj Z_-k)/(2i)
         zd X = zmake(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y));
         zd Y = zmake(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x));
@@ -198,4 +199,42 @@ __global__ void __launch_bounds__(256) k_xpass(FftParams p) {
             if (hasB) p.zp2[rowB + k] = Y;
         }
     }
+}
+
+// Single-instance kernels and their batched forms (one launch per size class;
+// blockIdx.z also selects the instance).
+template <int LZ>
+__global__ void __launch_bounds__(256) k_zinv(FftParams p) {
+    zinv_body<LZ>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <int LZ>
+__global__ void __launch_bounds__(256) k_zfwd(FftParams p) {
+    zfwd_body<LZ>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <int LX>
+__global__ void __launch_bounds__(256) k_xpass(FftParams p) {
+    xpass_body<LX>(p, blockIdx.x, blockIdx.y);
+}
+// grid z = 6 * instances
+template <int LZ>
+__global__ void __launch_bounds__(256) k_zinv_batch(const FftParams* __restrict__ pl) {
+    __shared__ FftParams ps;
+    const int inst = blockIdx.z / 6;
+    stage_params(&ps, pl + inst);
+    zinv_body<LZ>(ps, blockIdx.x, blockIdx.y, blockIdx.z - 6 * inst);
+}
+// grid z = 3 * instances
+template <int LZ>
+__global__ void __launch_bounds__(256) k_zfwd_batch(const FftParams* __restrict__ pl) {
+    __shared__ FftParams ps;
+    const int inst = blockIdx.z / 3;
+    stage_params(&ps, pl + inst);
+    zfwd_body<LZ>(ps, blockIdx.x, blockIdx.y, blockIdx.z - 3 * inst);
+}
+// grid z = instances
+template <int LX>
+__global__ void __launch_bounds__(256) k_xpass_batch(const FftParams* __restrict__ pl) {
+    __shared__ FftParams ps;
+    stage_params(&ps, pl + blockIdx.z);
+    xpass_body<LX>(ps, blockIdx.x, blockIdx.y);
 }

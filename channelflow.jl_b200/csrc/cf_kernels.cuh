@@ -10,9 +10,9 @@
 // Field storage: complex (Ny, Nz, Nxh), k fastest; z-padded (Ny, Nzp, Nxh).
 //
 // Column kernels: a block holds NCOL columns, one team of two warps each
-// (cf_column.cuh).  Shared memory: 8 regions x NCOL columns x cs complex (the
-// parity layout, cs >= max(P + 2, round_up(P, 8))), then 2 complex of team
-// scratch per column.
+// (cf_column.cuh).  Shared memory: 6 vector regions x NCOL columns x cs
+// complex (parity layout, cs = P + 2), 2 transform-buffer regions x NCOL x zs
+// complex (zs >= fft_bufsz(P)), then 2 complex of team scratch per column.
 #pragma once
 #include "cf_column.cuh"
 
@@ -29,7 +29,8 @@ struct BankDev {
 
 struct ColParams {
     int Nx, Nz, Nxh, Ny, P, B;
-    int cs;  // column stride in shared memory (complex)
+    int cs;  // stride of the vector regions 0-5 in shared memory (complex)
+    int zs;  // stride of the transform-buffer regions 6-7 (>= fft_bufsz(P))
     double ax, bz;  // 2 pi / Lx, 2 pi / Lz
     double nu;
     // stage constants
@@ -78,10 +79,11 @@ struct ColCtx {
     int c0, c, ix, iz;
     bool valid;
     zd* smem;
-    int cs;
-    CF_DEV ColCtx(zd* sm, const ColParams& p) {
+    int cs, zs;
+    CF_DEV ColCtx(zd* sm, const ColParams& p, int bx) {
         smem = sm;
         cs = p.cs;
+        zs = p.zs;
         const int tm = threadIdx.x / CF_TEAM;
         t.tid = threadIdx.x - tm * CF_TEAM;
         t.q = t.tid >> 5;
@@ -89,16 +91,18 @@ struct ColCtx {
         t.bar = 1 + tm;
         t.P = PL ? PL : p.P;
         t.hs = (t.P >> 1) + 1;
-        t.xch = sm + (long)8 * NCOL * cs + 2 * tm;
-        c0 = blockIdx.x * NCOL;
+        t.xch = sm + (long)NCOL * (6 * cs + 2 * zs) + 2 * tm;
+        c0 = bx * NCOL;
         c = c0 + tm;
         valid = c < p.B;
         ix = c % p.Nxh;
         iz = c / p.Nxh;
     }
     // region r of the whole block / of this column
-    CF_DEV zd* reg(int r) const { return smem + (long)r * NCOL * cs; }
-    CF_DEV zd* col(int r) const { return smem + (long)(r * NCOL + (threadIdx.x / CF_TEAM)) * cs; }
+    CF_DEV zd* reg(int r) const {
+        return r < 6 ? smem + (long)r * NCOL * cs : smem + (long)NCOL * (6 * cs + (r - 6) * zs);
+    }
+    CF_DEV zd* col(int r) const { return reg(r) + (threadIdx.x / CF_TEAM) * (r < 6 ? cs : zs); }
 };
 
 // Tile of NCOL adjacent columns x Ny degrees into shared memory (column t at
@@ -323,12 +327,13 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
     }
 }
 
-// Full CNRK2 stage for NCOL columns per block (one team per column).
+// Full CNRK2 stage for NCOL columns per block (one team per column); bx is
+// the block's index among the instance's column blocks.
 // Regions: 0 R0, 1 R1, 2 R2, 3 PT, 4 A, 5 Bw, 6 Z, 7 Z2 (6, 7: transform buffers).
 template <int NCOL, int PL>
-__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_stage(ColParams p) {
+CF_DEV void column_stage_body(const ColParams& p, int bx) {
     extern __shared__ zd smem[];
-    const ColCtx<NCOL, PL> X(smem, p);
+    const ColCtx<NCOL, PL> X(smem, p, bx);
     const Team& t = X.t;
     const int cs = X.cs, hs = t.hs, c0 = X.c0, c = X.c, q = t.q, lane = t.lane;
     const int qo = q * hs, nq = pcount(q, t.P);
@@ -473,11 +478,25 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     tile_store<NCOL>(X.reg(5), cs, hs, p.nod[5], c0, p);
 }
 
+template <int NCOL, int PL>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_stage(ColParams p) {
+    column_stage_body<NCOL, PL>(p, blockIdx.x);
+}
+// Batched stage: blockIdx.y selects the instance of a size class, whose
+// parameters are staged in shared memory.
+template <int NCOL, int PL>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>()))
+    k_column_stage_batch(const ColParams* __restrict__ pl) {
+    __shared__ ColParams ps;
+    stage_params(&ps, pl + blockIdx.y);
+    column_stage_body<NCOL, PL>(ps, blockIdx.x);
+}
+
 // Nodal velocity and vorticity from the state U (used after set_state).
 template <int NCOL, int PL>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_prep(ColParams p) {
     extern __shared__ zd smem[];
-    const ColCtx<NCOL, PL> X(smem, p);
+    const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
     const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
     tile_load<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p);
     tile_load<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p);
@@ -499,14 +518,14 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
 template <int NCOL, int PL>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_nlout(ColParams p) {
     extern __shared__ zd smem[];
-    const ColCtx<NCOL, PL> X(smem, p);
+    const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
     const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
     const bool nyq = X.valid ? col_nyquist(p, X.ix, X.iz) : true;
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
         tile_load<NCOL>(X.reg(0), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p);
         __syncthreads();
-        if (X.valid) col_forward_y<PL>(X.col(0), X.col(1), X.col(2), p, nyq, X.t);
+        if (X.valid) col_forward_y<PL>(X.col(0), X.col(6), X.col(7), p, nyq, X.t);
         __syncthreads();
         tile_store<NCOL>(X.reg(0), cs, hs, sel3(p.Nout[0], p.Nout[1], p.Nout[2], i), c0, p);
         __syncthreads();
@@ -518,7 +537,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
 template <int NCOL, int PL>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_project(ColParams p) {
     extern __shared__ zd smem[];
-    const ColCtx<NCOL, PL> X(smem, p);
+    const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
     const Team& t = X.t;
     const int cs = X.cs, hs = t.hs, c0 = X.c0, qo = t.q * hs, nq = pcount(t.q, t.P);
     const double k = p.ax * X.ix;
@@ -560,7 +579,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
 template <int NCOL, int PL>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_pressure(ColParams p) {
     extern __shared__ zd smem[];
-    const ColCtx<NCOL, PL> X(smem, p);
+    const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
     const Team& t = X.t;
     const int cs = X.cs, hs = t.hs, c0 = X.c0, c = X.c, q = t.q, lane = t.lane;
     const int P = t.P, qo = q * hs, nq = pcount(q, P);

@@ -76,6 +76,28 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
 /* NonLinearTerm{RotatingForm}(t, U, N) on host buffers (nonlinear.jl:173-193). */
 int cf_nonlinear(cf_handle* h, const double* U, double* N);
 
+/* ---- Ensembles: many independent channels advanced together ----------------
+ * The reference advances one channel per step! call; an ensemble of N
+ * instances (each its own grid, nu, dt, constraint and state) is stepped here
+ * with one CUDA graph per step in which every kernel is launched once per size
+ * class (instances with equal Nx, Ny, Nz) over all of its instances.  The
+ * instances are ordinary handles owned by the ensemble: set and read their
+ * state, random_state, diagnostics and (one at a time) cf_step through
+ * cf_batch_instance().  Work queued through an instance handle completes
+ * before the next cf_step_batch; later instance calls wait for the ensemble. */
+typedef struct cf_batch cf_batch;
+int cf_create_batch(const cf_config* cfgs, int n, cf_batch** out);
+void cf_destroy_batch(cf_batch* b);
+int cf_batch_size(cf_batch* b);
+/* borrowed handle of instance i (owned by the ensemble; NULL if out of range) */
+cf_handle* cf_batch_instance(cf_batch* b, int i);
+/* nsteps CNRK2 steps of every instance (step! per instance, cnrk2.jl:567-625); asynchronous */
+int cf_step_batch(cf_batch* b, int nsteps);
+/* kernel launches issued by the last cf_step_batch */
+int cf_batch_last_launch_count(cf_batch* b);
+/* the ensemble's CUDA stream (cudaStream_t) */
+void* cf_batch_stream(cf_batch* b);
+
 /* cf_nonlinear that allocates no device memory: U and N are staged in a fixed
  * module-scope device array of CF_NOALLOC_SCRATCH_BYTES (16 MiB) instead of
  * buffers allocated on first use.  No reference counterpart (an addition of

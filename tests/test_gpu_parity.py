@@ -172,3 +172,20 @@ def test_step_interface_host_buffers():
     ref.step(U, P, 3)
     assert abs(t - 0.28) < 1e-14
     assert rel(Uh, U) < 1e-12
+
+
+def test_handles_of_different_grids_coexist():
+    # 16x17x16 and 24x25x20 share the run-time-sized kernel instantiations;
+    # creating the smaller handle last must not restrict the larger one
+    big, ref_big = pair(24, 25, 20, 2 * np.pi, np.pi, 1 / 1000, 0.005, profile="poiseuille",
+                        bulkvelocity=(2 / 3, 0.0))
+    small, _ = pair(16, 17, 16, 5.3, 7.1, 1 / 300, 0.01)
+    U, P = ref_big.random_state(seed=12, amp=0.1)
+    big.set_state(U, P)
+    big.advance(0.0, 3)
+    ref_big.step(U, P, 3)
+    Ug, _ = big.get_state()
+    assert rel(Ug, U) <= 1e-12
+    cfb200.random_state(small, 0.1, seed=1)
+    big.close()
+    small.close()
