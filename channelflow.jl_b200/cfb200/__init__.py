@@ -44,7 +44,7 @@ EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_g
            "cf_pressure", "cf_random_state", "cf_diagnostics", "cf_sync", "cf_last_launch_count",
            "cf_stream", "cf_last_error", "cf_step_profiled", "cf_nonlinear_noalloc", "cf_create_batch",
            "cf_destroy_batch", "cf_batch_size", "cf_batch_instance", "cf_step_batch",
-           "cf_batch_last_launch_count", "cf_batch_stream"]
+           "cf_batch_last_launch_count", "cf_batch_stream", "cf_cheb_transform"]
 
 
 def lib():
@@ -67,6 +67,8 @@ def lib():
         L.cf_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _D, _D]
         L.cf_nonlinear.argtypes = [ctypes.c_void_p, _D, _D]
         L.cf_nonlinear_noalloc.argtypes = [ctypes.c_void_p, _D, _D]
+        L.cf_cheb_transform.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.c_int,
+                                        ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_double]
         L.cf_create_batch.argtypes = [ctypes.POINTER(_Config), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
         L.cf_destroy_batch.argtypes = [ctypes.c_void_p]
         L.cf_destroy_batch.restype = None
@@ -330,6 +332,19 @@ class Ensemble:
 
     def __del__(self):
         self.close()
+
+
+def cheb_transform(X, inverse, scale=1.0):
+    """Chebyshev transform along axis 1 of float32 X (fields, Ny, C) on the
+    tensor cores: inverse -> values at the Lobatto nodes; forward -> scaled
+    coefficients with halved end coefficients."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    nf, Ny, C = X.shape
+    Y = np.zeros_like(X)
+    fp = ctypes.POINTER(ctypes.c_float)
+    _check(lib().cf_cheb_transform(X.ctypes.data_as(fp), Y.ctypes.data_as(fp), Ny, C, nf, 1 if inverse else 0,
+                                   float(scale)))
+    return Y
 
 
 def CouetteFlow(grid, nu, dt, **kw):

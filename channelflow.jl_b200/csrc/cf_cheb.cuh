@@ -1,0 +1,224 @@
+// cf_cheb.cuh -- Chebyshev transforms of many columns as tensor-core
+// contractions (tcgen05, TF32 inputs, FP32 accumulation in tensor memory).
+//
+//   Y[f][n][c] = sum_k T[n][k] X[f][k][c],   n, k in [0, Ny), c in [0, C)
+//
+// for the fields f of one launch; X and Y are FP32 arrays (Ny rows of C
+// floats: a complex (Ny, Nz, Nxh) field read as C = 2 Nxh Nz real columns, T
+// being real).  T is the DCT-I of the forward transform (nodal values ->
+// coefficients, with the reference's normalisation, ffts.jl:189-206 and
+// :378-393) or of the inverse one (coefficients -> nodal values, ffts.jl:
+// 282-287), built by the engine.
+//
+// The contraction is computed transposed, D = X^T T^T: M = 128 columns of X per
+// block (TMEM lane m = column), N = the output degrees (MMAs of at most 256),
+// K = the input degrees in tiles of 32.  Both operands are K-major in shared
+// memory, in the canonical no-swizzle layout of the tensor cores (core
+// matrices of 8 rows x 16 bytes, rows 16 bytes apart, 8-row groups 128 bytes
+// apart, 4-element K chunks LBO bytes apart):
+//   A (X^T): element (m, k) of a K-tile at ((k/4)*128 + m)*16 + (k%4)*4 bytes
+//            (LBO 2048 B); each thread stages one column m, four rows at a time,
+//   B (T^T): element (n, k) at ((k/4)*NP + n)*16 + (k%4)*4 bytes (LBO NP*16 B),
+//            NP = Ny rounded up to 16; the engine stores T^T in global memory
+//            in exactly these K-tile images.
+// TF32 keeps 10 mantissa bits, so each operand is split into a TF32 head and
+// the TF32 rounding of its remainder; hi*hi + hi*lo + lo*hi restores ~FP32
+// accuracy (the three products accumulate in the same FP32 tensor memory).
+#pragma once
+#include "cf_common.cuh"
+
+#define CF_CHEB_MT 128   // columns per block (MMA M)
+#define CF_CHEB_KT 32    // input degrees per K-tile
+#define CF_CHEB_MAXF 6   // fields per launch
+
+struct ChebParams {
+    int Ny, NP, nkt;   // degrees, output degrees rounded up to 16, K-tiles
+    long C;            // real columns per field
+    const float* X[CF_CHEB_MAXF];
+    float* Y[CF_CHEB_MAXF];
+    const float* Bhi;  // [nkt][NP*128 bytes] K-tile images of T^T (TF32 heads)
+    const float* Blo;  // remainders
+    int* err;          // set to 1 when a wait gives up
+};
+
+// ---- PTX wrappers --------------------------------------------------------------
+CF_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+CF_DEV float tf32_round(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// shared-memory matrix descriptor, no swizzle (layout type 0), descriptor
+// version 1; addresses and byte offsets in 16-byte units
+CF_DEV uint64_t umma_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo_bytes >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo_bytes >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+// instruction descriptor: D F32, A and B TF32, both K-major, M x N
+CF_DEV uint32_t umma_idesc_tf32(int M, int N) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+CF_DEV void umma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+CF_DEV void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+CF_DEV void mbar_init(uint32_t mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+}
+// bounded wait for the completion of phase `parity`; false when it gave up
+CF_DEV bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (long it = 0; it < (1L << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+CF_DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+CF_DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+CF_DEV void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 16 consecutive TMEM columns of this warp's 32 lanes, one lane per thread
+CF_DEV void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---- the kernel ------------------------------------------------------------------
+// grid (ceil(C / 128), fields); 128 threads; dynamic shared memory
+// 2 * 16 KB (A heads, remainders) + 2 * NP * 128 B (B images) + 64 B.
+__global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
+    extern __shared__ __align__(1024) unsigned char csm[];
+    const int f = blockIdx.y, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long c0 = (long)blockIdx.x * CF_CHEB_MT;
+    const int NP = p.NP;
+    float* Ahi = reinterpret_cast<float*>(csm);
+    float* Alo = Ahi + CF_CHEB_MT * CF_CHEB_KT;
+    float* Bhi = Alo + CF_CHEB_MT * CF_CHEB_KT;
+    float* Blo = Bhi + NP * CF_CHEB_KT;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + NP * CF_CHEB_KT);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+    // TMEM columns: a power of two >= NP (and >= 32)
+    const int ncols = NP <= 32 ? 32 : (NP <= 64 ? 64 : (NP <= 128 ? 128 : (NP <= 256 ? 256 : 512)));
+    const float* X = p.X[f];
+    float* Y = p.Y[f];
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) mbar_init(smem_u32(mbar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    bool ok = true;
+
+    for (int kt = 0; kt < p.nkt; ++kt) {
+        const int k0 = kt * CF_CHEB_KT;
+        // A: thread tid stages column m = tid: rows k0 + 4j .. 4j+3 form one
+        // 16-byte core-matrix row (the warp's loads of one row are 128
+        // contiguous bytes; its stores are consecutive 16-byte rows)
+        {
+            const long c = c0 + tid;
+            const bool cin = c < p.C;
+#pragma unroll 2
+            for (int j = 0; j < CF_CHEB_KT / 4; ++j) {
+                float x[4];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int k = k0 + 4 * j + r;
+                    x[r] = (cin && k < p.Ny) ? __ldg(X + (long)k * p.C + c) : 0.0f;
+                }
+                float4 h = make_float4(tf32_round(x[0]), tf32_round(x[1]), tf32_round(x[2]), tf32_round(x[3]));
+                float4 l = make_float4(tf32_round(x[0] - h.x), tf32_round(x[1] - h.y), tf32_round(x[2] - h.z),
+                                       tf32_round(x[3] - h.w));
+                const int o = (j * CF_CHEB_MT + tid) * 4;  // floats
+                *reinterpret_cast<float4*>(Ahi + o) = h;
+                *reinterpret_cast<float4*>(Alo + o) = l;
+            }
+        }
+        // B: straight copy of this K-tile's images
+        const float4* bh = reinterpret_cast<const float4*>(p.Bhi + (long)kt * NP * CF_CHEB_KT);
+        const float4* bl = reinterpret_cast<const float4*>(p.Blo + (long)kt * NP * CF_CHEB_KT);
+        for (int i = tid; i < NP * CF_CHEB_KT / 4; i += 128) {
+            reinterpret_cast<float4*>(Bhi)[i] = __ldg(bh + i);
+            reinterpret_cast<float4*>(Blo)[i] = __ldg(bl + i);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const int ksteps = min(CF_CHEB_KT, p.Ny - k0 + 7) / 8;  // 8-degree steps holding data
+            for (int ks = 0; ks < ksteps; ++ks) {
+                const uint32_t aoff = ks * 2 * CF_CHEB_MT * 16, boff = ks * 2 * NP * 16;
+                for (int n0 = 0; n0 < NP; n0 += 256) {
+                    const int N = min(256, NP - n0);
+                    const uint32_t idesc = umma_idesc_tf32(CF_CHEB_MT, N);
+                    const uint32_t d = tmem + (uint32_t)n0;
+                    const uint32_t bo = boff + (n0 / 8) * 128;
+                    const uint64_t ah = umma_desc(smem_u32(Ahi) + aoff, CF_CHEB_MT * 16, 128);
+                    const uint64_t al = umma_desc(smem_u32(Alo) + aoff, CF_CHEB_MT * 16, 128);
+                    const uint64_t bhd = umma_desc(smem_u32(Bhi) + bo, NP * 16, 128);
+                    const uint64_t bld = umma_desc(smem_u32(Blo) + bo, NP * 16, 128);
+                    const uint32_t acc0 = (kt > 0 || ks > 0) ? 1u : 0u;
+                    umma_tf32(d, ah, bhd, idesc, acc0);
+                    umma_tf32(d, ah, bld, idesc, 1u);
+                    umma_tf32(d, al, bhd, idesc, 1u);
+                }
+            }
+            umma_commit(smem_u32(mbar));
+        }
+        // the tiles are overwritten next: wait for the MMAs that read them
+        if (!mbar_wait(smem_u32(mbar), (uint32_t)(kt & 1))) {
+            ok = false;
+            break;
+        }
+        tc_fence_after();
+        __syncthreads();
+    }
+    if (!ok) {
+        if (lane == 0) atomicExch(p.err, 1);
+    } else {
+        // epilogue: lane m of warp w holds column c0 + 32 w + m
+        const long c = c0 + 32 * warp + lane;
+        const uint32_t tw = tmem + ((uint32_t)(32 * warp) << 16);
+        for (int n0 = 0; n0 < NP; n0 += 16) {
+            float v[16];
+            tmem_ld16(tw + (uint32_t)n0, v);
+            if (c < p.C) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    if (n0 + i < p.Ny) Y[(long)(n0 + i) * p.C + c] = v[i];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}

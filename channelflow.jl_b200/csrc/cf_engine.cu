@@ -17,6 +17,7 @@
 #include "../../include/cfb200.h"
 #include "cf_fftkernels.cuh"
 #include "cf_kernels.cuh"
+#include "cf_cheb.cuh"
 
 #define CF_NCOL 2
 static_assert(CF_NCOL == 1 || CF_NCOL == 2, "column teams use named barriers 1 and 2");
@@ -271,7 +272,7 @@ static std::vector<int> fft_radices(int n) {
 static int rup8(int x) { return (x + 7) & ~7; }
 // transform-buffer strides and shared memory of the periodic FFT kernels
 static int zbs(const cf_engine* h) { return fft_bufsz(h->Nzp) + 1; }
-static int xbs(const cf_engine* h) { return fft_bufsz(h->Nxp); }
+static int xbs(const cf_engine* h) { return rup8(h->Nxp); }
 static size_t zsmem(const cf_engine* h) { return (size_t)2 * h->tkz * zbs(h) * sizeof(zd); }
 static size_t xsmem(const cf_engine* h) { return (size_t)12 * xbs(h) * sizeof(zd); }
 static int ilog2(int v) {
@@ -660,7 +661,7 @@ static int validate_and_size(cf_engine* h, const cf_config* c) {
     std::vector<int> rP = fft_radices(h->P), rZ = fft_radices(h->Nzp), rX = fft_radices(h->Nxp);
     if (!radices_ok(rP) || rP.size() > CF_FFT_MAXPASS)
         return fail(CF_E_UNSUPPORTED, "Chebyshev transform length not supported (prime factors <= 31)");
-    if (!radices_ok(rX) || rX.size() > CF_FFT_MAXPASS || (size_t)12 * fft_bufsz(h->Nxp) * 16 > 227 * 1024)
+    if (!radices_ok(rX) || rX.size() > CF_FFT_MAXPASS || (size_t)12 * rup8(h->Nxp) * 16 > 227 * 1024)
         return fail(CF_E_UNSUPPORTED, "padded x length not supported");
     if (!radices_ok(rZ) || rZ.size() > CF_FFT_MAXPASS)
         return fail(CF_E_UNSUPPORTED, "padded z length not supported");
@@ -1350,3 +1351,123 @@ int cf_step_batch(cf_batch* b, int nsteps) {
 
 int cf_batch_last_launch_count(cf_batch* b) { return b ? b->last_launches : 0; }
 void* cf_batch_stream(cf_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+// ---------------------------------------------------------------------------
+// Chebyshev transforms on the tensor cores (mixed-precision path)
+// ---------------------------------------------------------------------------
+// TF32 rounding of x (to nearest, ties away from zero), as cvt.rna.tf32.f32
+static float host_tf32(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    if ((u & 0x7F800000u) != 0x7F800000u) u = (u + 0x1000u) & ~0x1FFFu;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+// T^T K-tile images (TF32 heads and remainders, see cf_cheb.cuh) of
+//   inverse:  y_n = sum_k a_k cos(pi n k / P)                 (ffts.jl:282-287)
+//   forward:  a_k = scale e_k sum_n w_n x_n cos(pi n k / P)   (ffts.jl:189-206,
+//             e_k = 1/2 at k = 0, P; w_n = 1 at n = 0, P, else 2)
+static void cheb_images(int Ny, int inverse, double scale, std::vector<float>& hi, std::vector<float>& lo, int& NP,
+                        int& nkt) {
+    const int P = Ny - 1;
+    NP = (Ny + 15) & ~15;
+    nkt = (Ny + CF_CHEB_KT - 1) / CF_CHEB_KT;
+    hi.assign((size_t)nkt * NP * CF_CHEB_KT, 0.0f);
+    lo.assign(hi.size(), 0.0f);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int n = 0; n < Ny; ++n)        // output degree / node
+        for (int k = 0; k < Ny; ++k) {  // input node / degree
+            const long m = ((long)n * k) % (2L * P);
+            const double c = (double)cosl(pi * (long double)m / (long double)P);
+            double t;
+            if (inverse) {
+                t = c;
+            } else {
+                const double e = (n == 0 || n == P) ? 0.5 : 1.0, w = (k == 0 || k == P) ? 1.0 : 2.0;
+                t = scale * e * w * c;
+            }
+            const float th = host_tf32((float)t);
+            const float tl = host_tf32((float)(t - (double)th));
+            const int kt = k / CF_CHEB_KT, kl = k % CF_CHEB_KT;
+            const size_t idx = (size_t)kt * NP * CF_CHEB_KT + ((size_t)(kl / 4) * NP + n) * 4 + (kl % 4);
+            hi[idx] = th;
+            lo[idx] = tl;
+        }
+}
+
+// Dynamic shared memory of k_cheb_mma: its tiles, padded so that the blocks
+// that fit on an SM (228 KB, 1 KB reserved per block) also fit in its 512 TMEM
+// columns, and no block ever waits in the TMEM allocation.
+static size_t cheb_smem(int NP) {
+    const size_t tiles = (size_t)2 * CF_CHEB_MT * CF_CHEB_KT * 4 + (size_t)2 * NP * CF_CHEB_KT * 4 + 64;
+    const int ncols = NP <= 32 ? 32 : (NP <= 64 ? 64 : (NP <= 128 ? 128 : (NP <= 256 ? 256 : 512)));
+    const size_t per_sm = 233472, maxb = 512 / ncols;
+    const size_t floor_b = per_sm / (maxb + 1) - 1024 + 16;  // maxb + 1 blocks no longer fit
+    return std::max(tiles, floor_b);
+}
+
+int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int inverse, double scale) {
+    if (!X || !Y) return fail(CF_E_ARG, "null argument");
+    if (Ny < 2 || Ny > 512) return fail(CF_E_UNSUPPORTED, "Chebyshev transform needs 2 <= Ny <= 512");
+    if (C < 1 || nfields < 1 || nfields > CF_CHEB_MAXF) return fail(CF_E_ARG, "need C >= 1 and 1..6 fields");
+    std::vector<float> hi, lo;
+    int NP, nkt;
+    cheb_images(Ny, inverse, scale, hi, lo, NP, nkt);
+    const size_t fb = sizeof(float) * (size_t)Ny * C;
+    float *dX = nullptr, *dY = nullptr, *dB = nullptr;
+    int* derr = nullptr;
+    int rc = CF_OK;
+    auto cleanup = [&]() {
+        cudaFree(dX);
+        cudaFree(dY);
+        cudaFree(dB);
+        cudaFree(derr);
+    };
+    if (cudaMalloc(&dX, fb * nfields) != cudaSuccess || cudaMalloc(&dY, fb * nfields) != cudaSuccess ||
+        cudaMalloc(&dB, sizeof(float) * hi.size() * 2) != cudaSuccess || cudaMalloc(&derr, sizeof(int)) != cudaSuccess) {
+        cleanup();
+        return fail(CF_E_NOMEM, "device allocation failed");
+    }
+    do {
+        if (cudaMemcpy(dX, X, fb * nfields, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dB, hi.data(), sizeof(float) * hi.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dB + hi.size(), lo.data(), sizeof(float) * lo.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(derr, 0, sizeof(int)) != cudaSuccess || cudaMemset(dY, 0, fb * nfields) != cudaSuccess) {
+            rc = fail(CF_E_CUDA, "upload failed");
+            break;
+        }
+        if ((rc = raise_smem_limit(k_cheb_mma, cheb_smem(NP)))) break;
+        ChebParams p;
+        std::memset(&p, 0, sizeof(p));
+        p.Ny = Ny;
+        p.NP = NP;
+        p.nkt = nkt;
+        p.C = C;
+        for (int f = 0; f < nfields; ++f) {
+            p.X[f] = dX + (size_t)f * Ny * C;
+            p.Y[f] = dY + (size_t)f * Ny * C;
+        }
+        p.Bhi = dB;
+        p.Blo = dB + hi.size();
+        p.err = derr;
+        dim3 grid((unsigned)((C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nfields);
+        k_cheb_mma<<<grid, 128, cheb_smem(NP)>>>(p);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            rc = fail(CF_E_CUDA, std::string("Chebyshev transform kernel: ") + cudaGetErrorString(e));
+            break;
+        }
+        int herr = 0;
+        cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+        if (herr) {
+            rc = fail(CF_E_CUDA, "Chebyshev transform kernel: a tensor-core wait timed out");
+            break;
+        }
+        if (cudaMemcpy(Y, dY, fb * nfields, cudaMemcpyDeviceToHost) != cudaSuccess) rc = fail(CF_E_CUDA, "download failed");
+    } while (0);
+    cleanup();
+    return rc;
+}

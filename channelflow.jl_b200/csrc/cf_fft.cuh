@@ -40,6 +40,16 @@ CF_DEV void group_sync(int bar, int) {
 CF_DEV int fpos(int e) { return e + (e >> 3); }
 // complex slots a transform buffer of length L occupies (multiple of 8)
 __host__ __device__ constexpr int fft_bufsz(int L) { return ((L + (L >> 3) + 1) + 7) & ~7; }
+// Alternative layout without padding (buffers of round_up(L, 8) elements, for
+// kernels whose shared memory is at an occupancy limit): the low three bits of
+// e are XOR-ed with bits 3-5 and 6-8, spreading the strided stores over the
+// bank groups as well, at a few more integer operations per access.
+CF_DEV int swz(int e) { return e ^ (((e >> 3) ^ (e >> 6)) & 7); }
+// position of element e in a buffer of layout POS (0 padded, 1 XOR-swizzled)
+template <int POS>
+CF_DEV int bpos(int e) {
+    return POS ? swz(e) : fpos(e);
+}
 
 CF_DEV zd tw_get(const zd* tw, int k, int sgn) {
     zd w = __ldg(tw + k);
@@ -189,7 +199,7 @@ CF_DEV void dft_small<16>(zd* v, int sgn) {
 // One out-of-place Stockham pass of compile-time radix R over nb transforms of
 // length L (transform b at src + b*bs, written to dst + b*bs).  A thread keeps
 // one butterfly in registers at a time.
-template <bool BLOCK, int R>
+template <bool BLOCK, int POS, int R>
 CF_DEV void fft_pass_pp(const zd* __restrict__ src, zd* __restrict__ dst, int nb, int bs, int L, int Ns,
                         const zd* __restrict__ tw, int sgn, int tid, int nth, int bar) {
     const int NBf = L / R;
@@ -203,21 +213,21 @@ CF_DEV void fft_pass_pp(const zd* __restrict__ src, zd* __restrict__ dst, int nb
         zd v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            zd x = s[fpos(j + r * NBf)];
+            zd x = s[bpos<POS>(j + r * NBf)];
             v[r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
         }
         dft_small<R>(v, sgn);
         zd* d = dst + (long)b * bs;
         const int o = (j / Ns) * Ns * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) d[fpos(o + r * Ns)] = v[r];
+        for (int r = 0; r < R; ++r) d[bpos<POS>(o + r * Ns)] = v[r];
     }
     group_sync<BLOCK>(bar, nth);
 }
 
 // Generic prime radix (R <= 31) by a direct DFT; only sizes with uncommon
 // prime factors take this path.
-template <bool BLOCK>
+template <bool BLOCK, int POS>
 CF_DEV void fft_pass_pp_generic(const zd* __restrict__ src, zd* __restrict__ dst, int nb, int bs, int L, int R,
                                 int Ns, const zd* __restrict__ tw, int sgn, int tid, int nth, int bar) {
     const int NBf = L / R;
@@ -232,11 +242,11 @@ CF_DEV void fft_pass_pp_generic(const zd* __restrict__ src, zd* __restrict__ dst
         for (int o = 0; o < R; ++o) {
             zd acc = zzero();
             for (int r = 0; r < R; ++r) {
-                zd x = s[fpos(j + r * NBf)];
+                zd x = s[bpos<POS>(j + r * NBf)];
                 if (r != 0 && k != 0) x = zmul(x, tw_get(tw, k * r * step, sgn));
                 acc = zadd(acc, (r == 0) ? x : zmul(x, tw_get(tw, ((o * r) % R) * NBf, sgn)));
             }
-            d[fpos(ob + o * Ns)] = acc;
+            d[bpos<POS>(ob + o * Ns)] = acc;
         }
     }
     group_sync<BLOCK>(bar, nth);
@@ -246,13 +256,13 @@ CF_DEV void fft_pass_pp_generic(const zd* __restrict__ src, zd* __restrict__ dst
 // index split and the twiddle indices need no run-time division, and the R
 // strided positions are one fpos() plus constant offsets where the stride is a
 // multiple of 8 (or the R outputs stay inside one group of 8).
-template <bool BLOCK, int L, int Ns, int R>
+template <bool BLOCK, int POS, int L, int Ns, int R>
 CF_DEV void fft_pass_static(const zd* __restrict__ src, zd* __restrict__ dst, int nb, int bs,
                             const zd* __restrict__ tw, int sgn, int tid, int nth, int bar) {
     constexpr int NBf = L / R;
     constexpr int step = L / (Ns * R);
-    constexpr bool LIN_LD = (NBf % 8) == 0;
-    constexpr bool LIN_ST = (Ns % 8) == 0 || (Ns == 1 && 8 % R == 0);
+    constexpr bool LIN_LD = POS == 0 && (NBf % 8) == 0;
+    constexpr bool LIN_ST = POS == 0 && ((Ns % 8) == 0 || (Ns == 1 && 8 % R == 0));
     constexpr int DLD = NBf + NBf / 8;
     constexpr int DST = (Ns == 1) ? 1 : Ns + Ns / 8;
     const int total = nb * NBf;
@@ -261,48 +271,49 @@ CF_DEV void fft_pass_static(const zd* __restrict__ src, zd* __restrict__ dst, in
         const int b = q / NBf, j = q - b * NBf;
         const int k = j % Ns;
         const zd* s = src + (long)b * bs;
-        const int pj = fpos(j);
+        const int pj = bpos<POS>(j);
         zd v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            zd x = s[LIN_LD ? pj + r * DLD : fpos(j + r * NBf)];
+            zd x = s[LIN_LD ? pj + r * DLD : bpos<POS>(j + r * NBf)];
             v[r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
         }
         dft_small<R>(v, sgn);
         zd* d = dst + (long)b * bs;
         const int o = (j / Ns) * Ns * R + k;
-        const int po = fpos(o);
+        const int po = bpos<POS>(o);
 #pragma unroll
-        for (int r = 0; r < R; ++r) d[LIN_ST ? po + r * DST : fpos(o + r * Ns)] = v[r];
+        for (int r = 0; r < R; ++r) d[LIN_ST ? po + r * DST : bpos<POS>(o + r * Ns)] = v[r];
     }
     group_sync<BLOCK>(bar, nth);
 }
-template <bool BLOCK, int L, int Ns, int R, int... Rest>
+template <bool BLOCK, int POS, int L, int Ns, int R, int... Rest>
 CF_DEV zd* fft_static(zd* src, zd* dst, int nb, int bs, const zd* tw, int sgn, int tid, int nth, int bar) {
-    fft_pass_static<BLOCK, L, Ns, R>(src, dst, nb, bs, tw, sgn, tid, nth, bar);
+    fft_pass_static<BLOCK, POS, L, Ns, R>(src, dst, nb, bs, tw, sgn, tid, nth, bar);
     if constexpr (sizeof...(Rest) == 0) {
         return dst;
     } else {
-        return fft_static<BLOCK, L, Ns * R, Rest...>(dst, src, nb, bs, tw, sgn, tid, nth, bar);
+        return fft_static<BLOCK, POS, L, Ns * R, Rest...>(dst, src, nb, bs, tw, sgn, tid, nth, bar);
     }
 }
 
-// Full transform of nb sequences (length pl.L, batch stride bs >=
-// fft_bufsz(L), element e of sequence b at b*bs + fpos(e)) held in a; b is a
-// scratch buffer of the same size.  Returns the buffer with the result.
-template <bool BLOCK>
+// Full transform of nb sequences (length pl.L, element e of sequence b at
+// b*bs + bpos<POS>(e), bs >= fft_bufsz(L) for the padded layout, >=
+// round_up(L, 8) for the XOR layout) held in a; b is a scratch buffer of the
+// same size.  Returns the buffer with the result.
+template <bool BLOCK, int POS>
 CF_DEV zd* group_fft(zd* a, zd* b, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
     int Ns = 1;
     zd* src = a;
     zd* dst = b;
     for (int p = 0; p < pl.np; ++p) {
         const int R = (int)((pl.rcode >> (5 * p)) & 31ull);
-        if (R == 8) fft_pass_pp<BLOCK, 8>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
-        else if (R == 4) fft_pass_pp<BLOCK, 4>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
-        else if (R == 2) fft_pass_pp<BLOCK, 2>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
-        else if (R == 3) fft_pass_pp<BLOCK, 3>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
-        else if (R == 5) fft_pass_pp<BLOCK, 5>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
-        else fft_pass_pp_generic<BLOCK>(src, dst, nb, bs, pl.L, R, Ns, pl.tw, sgn, tid, nth, bar);
+        if (R == 8) fft_pass_pp<BLOCK, POS, 8>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
+        else if (R == 4) fft_pass_pp<BLOCK, POS, 4>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
+        else if (R == 2) fft_pass_pp<BLOCK, POS, 2>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
+        else if (R == 3) fft_pass_pp<BLOCK, POS, 3>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
+        else if (R == 5) fft_pass_pp<BLOCK, POS, 5>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
+        else fft_pass_pp_generic<BLOCK, POS>(src, dst, nb, bs, pl.L, R, Ns, pl.tw, sgn, tid, nth, bar);
         Ns *= R;
         zd* t = src;
         src = dst;
@@ -314,21 +325,21 @@ CF_DEV zd* group_fft(zd* a, zd* b, int nb, int bs, const FftPlan& pl, int sgn, i
 // Transform of compile-time length L (the sizes of the supported grids);
 // L == 0 selects the run-time plan.  The radix order of a static size need not
 // match pl.R: any factorisation indexes the same twiddle table.
-template <bool BLOCK, int L>
+template <bool BLOCK, int L, int POS = 0>
 CF_DEV zd* group_fft_L(zd* a, zd* b, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
-    if constexpr (L == 32) return fft_static<BLOCK, 32, 1, 8, 4>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 48) return fft_static<BLOCK, 48, 1, 8, 2, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 64) return fft_static<BLOCK, 64, 1, 8, 8>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 72) return fft_static<BLOCK, 72, 1, 8, 9>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 96) return fft_static<BLOCK, 96, 1, 8, 4, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 128) return fft_static<BLOCK, 128, 1, 8, 8, 2>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 192) return fft_static<BLOCK, 192, 1, 8, 8, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 256) return fft_static<BLOCK, 256, 1, 8, 8, 4>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 384) return fft_static<BLOCK, 384, 1, 8, 8, 2, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 512) return fft_static<BLOCK, 512, 1, 8, 8, 8>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 576) return fft_static<BLOCK, 576, 1, 8, 8, 9>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 768) return fft_static<BLOCK, 768, 1, 8, 8, 4, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else return group_fft<BLOCK>(a, b, nb, bs, pl, sgn, tid, nth, bar);
+    if constexpr (L == 32) return fft_static<BLOCK, POS, 32, 1, 8, 4>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 48) return fft_static<BLOCK, POS, 48, 1, 8, 2, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 64) return fft_static<BLOCK, POS, 64, 1, 8, 8>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 72) return fft_static<BLOCK, POS, 72, 1, 8, 9>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 96) return fft_static<BLOCK, POS, 96, 1, 8, 4, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 128) return fft_static<BLOCK, POS, 128, 1, 8, 8, 2>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 192) return fft_static<BLOCK, POS, 192, 1, 8, 8, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 256) return fft_static<BLOCK, POS, 256, 1, 8, 8, 4>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 384) return fft_static<BLOCK, POS, 384, 1, 8, 8, 2, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 512) return fft_static<BLOCK, POS, 512, 1, 8, 8, 8>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 576) return fft_static<BLOCK, POS, 576, 1, 8, 8, 9>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else if constexpr (L == 768) return fft_static<BLOCK, POS, 768, 1, 8, 8, 4, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+    else return group_fft<BLOCK, POS>(a, b, nb, bs, pl, sgn, tid, nth, bar);
 }
 
 // Lengths with a compile-time instantiation (others run the generic plan).

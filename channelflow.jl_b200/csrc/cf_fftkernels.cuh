@@ -13,7 +13,8 @@
 struct FftParams {
     int Nx, Nz, Nxh, Ny, Nzp, Nxp;
     int tks;       // log2 of the columns per block in the z kernels
-    int bsz, bsx;  // transform buffer strides: fft_bufsz(Nzp) + 1 (odd), fft_bufsz(Nxp)
+    int bsz, bsx;  // transform buffer strides: fft_bufsz(Nzp) + 1 (odd, padded layout),
+                   // round_up(Nxp, 8) (XOR-swizzled layout: 12 buffers of the x-pass)
     zd *nod0, *nod1, *nod2, *nod3, *nod4, *nod5;  // nodal fields
     zd *zp0, *zp1, *zp2, *zp3, *zp4, *zp5;        // z-padded fields
     FftPlan plZ, plX;
@@ -148,21 +149,21 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
             const int slot = e / Nxhp, k = e - slot * Nxhp;
             zd* s = sm + slot * bs;
             if (k == 0) {
-                s[fpos(0)] = zmake(X[u].x, Y[u].x);
+                s[swz(0)] = zmake(X[u].x, Y[u].x);
             } else if (2 * k == Nxp) {
-                s[fpos(k)] = zmake(X[u].x, Y[u].x);
+                s[swz(k)] = zmake(X[u].x, Y[u].x);
             } else {
-                s[fpos(k)] = zmake(X[u].x - Y[u].y, X[u].y + Y[u].x);
-                s[fpos(Nxp - k)] = zmake(X[u].x + Y[u].y, Y[u].x - X[u].y);
+                s[swz(k)] = zmake(X[u].x - Y[u].y, X[u].y + Y[u].x);
+                s[swz(Nxp - k)] = zmake(X[u].x + Y[u].y, Y[u].x - X[u].y);
             }
         }
     }
     __syncthreads();
-    zd* A = group_fft_L<true, LX>(sm, scr, 6, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
+    zd* A = group_fft_L<true, LX, 1>(sm, scr, 6, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
     zd* Bf = (A == sm) ? scr : sm;
     // rotational product n = u x omega at every padded x point of both rows
     for (int j = threadIdx.x; j < Nxp; j += blockDim.x) {
-        const int sj = fpos(j);
+        const int sj = swz(j);
         zd a0 = A[0 * bs + sj], a1 = A[2 * bs + sj], a2 = A[4 * bs + sj];
         zd b0 = A[1 * bs + sj], b1 = A[3 * bs + sj], b2 = A[5 * bs + sj];
         // row A: u=(a0.x,a0.y,a1.x), w=(a1.y,a2.x,a2.y)
@@ -177,12 +178,12 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
         Bf[2 * bs + sj] = zmake(nA2, nB2);
     }
     __syncthreads();
-    const zd* F = group_fft_L<true, LX>(Bf, A, 3, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
+    const zd* F = group_fft_L<true, LX, 1>(Bf, A, 3, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
     // separate the packed real transforms and keep k < Nxh
     for (int e = threadIdx.x; e < 3 * Nxh; e += blockDim.x) {
         const int slot = e / Nxh, k = e - slot * Nxh;
         const zd* s = F + slot * bs;
-        zd Zk = s[fpos(k)], Zm = s[fpos((Nxp - k) % Nxp)];
+        zd Zk = s[swz(k)], Zm = s[swz((Nxp - k) % Nxp)];
         // X = (Z_k + conj Z_-k)/2 ; Y = (Z_k - conj Z_-k)/(2i)
         zd X = zmake(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y));
         zd Y = zmake(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x));

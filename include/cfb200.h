@@ -76,6 +76,16 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
 /* NonLinearTerm{RotatingForm}(t, U, N) on host buffers (nonlinear.jl:173-193). */
 int cf_nonlinear(cf_handle* h, const double* U, double* N);
 
+/* Chebyshev transform of many FP32 columns on the tensor cores (the kernel of
+ * the mixed-precision path), on host buffers: X and Y hold nfields arrays of
+ * Ny rows of C floats (a complex field read as real columns).  inverse != 0:
+ * coefficients -> values at the Lobatto nodes (the inverse transform of
+ * ffts.jl:282-287); inverse == 0: nodal values -> coefficients times `scale`
+ * with the endpoint halving (ffts.jl:189-206, normalize_forward!
+ * ffts.jl:378-393).  TF32 operands split in heads and remainders (three
+ * products), FP32 accumulation: ~FP32 accuracy.  2 <= Ny <= 512, nfields <= 6. */
+int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int inverse, double scale);
+
 /* ---- Ensembles: many independent channels advanced together ----------------
  * The reference advances one channel per step! call; an ensemble of N
  * instances (each its own grid, nu, dt, constraint and state) is stepped here
