@@ -407,6 +407,80 @@ def ensemble_cpu(cfg, members, threads):
                       "count x step time; value = instance-steps/s"}
 
 
+def make_problem(cfb200, g, cfg, precision):
+    if cfg["profile"] == "couette":
+        return cfb200.CouetteFlow(g, cfg["nu"], cfg["dt"], precision=precision)
+    return cfb200.PoiseuilleFlow(g, cfg["nu"], cfg["dt"], bulkvelocity=cfg["constraint"], precision=precision)
+
+
+def measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, nerr=100):
+    """The mixed-precision step on the same workload: steps/s (device-resident
+    state, CUDA-graph step, CUDA events), per-kernel event timing, and the
+    error against the FP64 step after nerr steps from the same initial state."""
+    import cfb200
+
+    mx = make_problem(cfb200, g, cfg, "mixed")
+    mx.set_state(U0, P0)
+    stream = torch.cuda.ExternalStream(mx.stream_ptr())
+    mx.advance(0.0, args.warmup)
+    mx.sync()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    mx.advance(0.0, args.steps)
+    launches = mx.launches()
+    e1.record(stream)
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    _, kms = mx.advance_profiled(0.0, args.steps)
+    nl = 3 * args.steps
+    kavg = {"zinv": kms[0] / nl, "xpass": kms[1] / nl, "zfwd": kms[2] / nl, "column": kms[3] / nl,
+            "cheb_fwd": kms[4] / nl, "cheb_inv": kms[5] / nl}
+    Nr, _ = sizes(cfg)
+    Ny, C = cfg["Ny"], 2 * Nr // cfg["Ny"]
+    peak, peak_kind = peaks()
+    tc_peak = peaks_tensor()
+    # tensor-core transform: algorithmic FLOPs of one contraction (2 Ny^2 C per
+    # field) and bytes (FP32 in and out); the TF32 split issues 3x the FLOPs
+    cheb = {}
+    for key, nf in (("cheb_fwd", 3), ("cheb_inv", 6)):
+        t = kavg[key] * 1e-3
+        flops, byts = 2.0 * Ny * Ny * C * nf, 8.0 * Ny * C * nf
+        cheb[key] = {"ms": kavg[key], "algorithmic_TFLOPs": flops / t / 1e12,
+                     "issued_TFLOPs_3xTF32": 3 * flops / t / 1e12, "GBs": byts / t / 1e9,
+                     "hbm_frac": byts / t / 1e9 / peak,
+                     "tensor_frac_of_bf16_peak": (3 * flops / t / 1e12) / tc_peak if tc_peak else None}
+    # error against the FP64 step
+    ref = make_problem(cfb200, g, cfg, "fp64")
+    ref.set_state(U0, P0)
+    mx.set_state(U0, P0)
+    ref.advance(0.0, nerr)
+    mx.advance(0.0, nerr)
+    Ur, _ = ref.get_state()
+    Um, _ = mx.get_state()
+    dr, dm = ref.diagnostics(), mx.diagnostics()
+    out = {"value": args.steps / (ms / 1e3), "unit": "steps/s", "ms_per_step": ms / args.steps,
+           "kernel_ms_per_launch": kavg, "tensor_core_transforms": cheb, "gpu_launches": launches,
+           "error_vs_fp64": {"steps": nerr,
+                             "velocity_rel_l2": float(np.linalg.norm(Um - Ur) / np.linalg.norm(Ur)),
+                             "energy_rel": float(abs(dm[0] - dr[0]) / abs(dr[0])),
+                             "dissipation_rel": float(abs(dm[1] - dr[1]) / abs(dr[1])),
+                             "max_div_mixed": float(dm[2])},
+           "precision": "FP32 periodic transforms and products; tensor-core Chebyshev transforms "
+                        "(TF32 heads and remainders, FP32 accumulation); FP64 Stokes solve and state"}
+    mx.close()
+    ref.close()
+    return out
+
+
+def peaks_tensor():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d.get("bf16_tflops") or 0) or None
+    except Exception:
+        return None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -415,6 +489,7 @@ def main():
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     rank = int(os.environ.get("RANK", "0"))
@@ -449,6 +524,7 @@ def main():
     else:
         pb = cfb200.PoiseuilleFlow(g, cfg["nu"], cfg["dt"], bulkvelocity=cfg["constraint"])
     cfb200.lib().cf_random_state(pb.handle, 1000 + rank, cfg["amp"], cfg["shape"], cfg["rho"])
+    U0, P0 = pb.get_state()
     stream = torch.cuda.ExternalStream(pb.stream_ptr())
 
     def barrier():
@@ -539,6 +615,10 @@ def main():
         "gpu_launches": launches,
         "diagnostics": {"kinetic_energy": diag[0], "dissipation": diag[1], "max_div": diag[2]},
     }
+    if not args.no_mixed:
+        mixed = measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks)
+        mixed["speedup_vs_fp64_plain"] = mixed["value"] / (value / world)
+        line["mixed"] = mixed
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         div = SAMPLE_DIV[args.config]

@@ -36,7 +36,10 @@ class _Config(ctypes.Structure):
                 ("Lx", ctypes.c_double), ("Lz", ctypes.c_double),
                 ("nu", ctypes.c_double), ("dt", ctypes.c_double),
                 ("profile", ctypes.c_int), ("base_values", _D),
-                ("constraint", ctypes.c_int), ("c1", ctypes.c_double), ("c2", ctypes.c_double)]
+                ("constraint", ctypes.c_int), ("c1", ctypes.c_double), ("c2", ctypes.c_double),
+                ("precision", ctypes.c_int)]
+
+PRECISIONS = {"fp64": 0, "mixed": 1}
 
 
 EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_get_state",
@@ -152,7 +155,8 @@ def zero_state(grid):
     return State(np.zeros((3,) + grid.spectralsize, np.complex128), np.zeros(grid.spectralsize, np.complex128))
 
 
-def _make_config(grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None, forcing=None, form=None):
+def _make_config(grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None, forcing=None, form=None,
+                 precision="fp64"):
     """cf_config of ChannelFlowProblem(grid, profile, nu, dt; ...); returns
     (config, base-profile array kept alive for the call, constraint)."""
     if pressuregradient is not None and bulkvelocity is not None:
@@ -180,6 +184,9 @@ def _make_config(grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None
         cfg.base_values = _ptr(base)
     cfg.constraint = 1 if constraint[0] == "bulkvelocity" else 0
     cfg.c1, cfg.c2 = constraint[1]
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+    cfg.precision = PRECISIONS[precision]
     return cfg, base, constraint
 
 
@@ -190,9 +197,11 @@ class ChannelFlowProblem:
     ``profile`` is "couette", "poiseuille" or a callable Ub(y).
     """
 
-    def __init__(self, grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None, forcing=None, form=None):
+    def __init__(self, grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None, forcing=None, form=None,
+                 precision="fp64"):
         cfg, self._base, self.constraint = _make_config(grid, profile, nu, dt, pressuregradient, bulkvelocity,
-                                                        forcing, form)
+                                                        forcing, form, precision)
+        self.precision = precision
         self.grid = grid
         self.nu, self.dt = float(nu), float(dt)
         h = ctypes.c_void_p()
@@ -206,6 +215,7 @@ class ChannelFlowProblem:
         self = cls.__new__(cls)
         self.grid, self.nu, self.dt, self.constraint = grid, float(nu), float(dt), constraint
         self._base = None
+        self.precision = "fp64"
         self._h = ctypes.c_void_p(handle)
         self._owned = False
         return self
@@ -245,9 +255,10 @@ class ChannelFlowProblem:
 
     def advance_profiled(self, t, nsteps=1):
         """As advance() without the graph; returns (t_out, ms per kernel class
-        [z-inverse, x-pass, z-forward, column] summed over the steps)."""
+        [z-inverse, x-pass, z-forward, column, forward and inverse tensor-core
+        Chebyshev transforms (mixed precision)] summed over the steps)."""
         tout = ctypes.c_double()
-        ms = np.zeros(4)
+        ms = np.zeros(6)
         _check(lib().cf_step_profiled(self._h, float(t), int(nsteps), ctypes.byref(tout), _ptr(ms)))
         return tout.value, ms
 

@@ -33,6 +33,7 @@
 
 struct ChebParams {
     int Ny, NP, nkt;   // degrees, output degrees rounded up to 16, K-tiles
+    int nst;           // shared-memory stages (1 or 2)
     long C;            // real columns per field
     const float* X[CF_CHEB_MAXF];
     float* Y[CF_CHEB_MAXF];
@@ -108,19 +109,20 @@ CF_DEV void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 // ---- the kernel ------------------------------------------------------------------
-// grid (ceil(C / 128), fields); 128 threads; dynamic shared memory
-// 2 * 16 KB (A heads, remainders) + 2 * NP * 128 B (B images) + 64 B.
+// grid (ceil(C / 128), fields); 128 threads.  Dynamic shared memory: nst
+// stages of [A heads, A remainders (16 KB each), B heads, B remainders
+// (NP * 128 B each)], then two mbarriers and the TMEM address.  With two
+// stages the loads of K-tile kt overlap the MMAs of K-tile kt - 1.
+CF_DEV uint32_t cheb_stage_bytes(int NP) { return 2u * CF_CHEB_MT * CF_CHEB_KT * 4 + 2u * NP * CF_CHEB_KT * 4; }
+
 __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
     extern __shared__ __align__(1024) unsigned char csm[];
     const int f = blockIdx.y, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long c0 = (long)blockIdx.x * CF_CHEB_MT;
-    const int NP = p.NP;
-    float* Ahi = reinterpret_cast<float*>(csm);
-    float* Alo = Ahi + CF_CHEB_MT * CF_CHEB_KT;
-    float* Bhi = Alo + CF_CHEB_MT * CF_CHEB_KT;
-    float* Blo = Bhi + NP * CF_CHEB_KT;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + NP * CF_CHEB_KT);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+    const int NP = p.NP, nst = p.nst;
+    const uint32_t sb = cheb_stage_bytes(NP);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(csm + nst * sb);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
     // TMEM columns: a power of two >= NP (and >= 32)
     const int ncols = NP <= 32 ? 32 : (NP <= 64 ? 64 : (NP <= 128 ? 128 : (NP <= 256 ? 256 : 512)));
     const float* X = p.X[f];
@@ -131,7 +133,10 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
                      "r"(ncols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    if (tid == 0) mbar_init(smem_u32(mbar), 1);
+    if (tid == 0) {
+        mbar_init(smem_u32(mbar), 1);
+        mbar_init(smem_u32(mbar + 1), 1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     tc_fence_before();
     __syncthreads();
@@ -139,7 +144,18 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
     const uint32_t tmem = *tslot;
     bool ok = true;
 
-    for (int kt = 0; kt < p.nkt; ++kt) {
+    for (int kt = 0; kt < p.nkt && ok; ++kt) {
+        const int st = kt % nst;
+        float* Ahi = reinterpret_cast<float*>(csm + st * sb);
+        float* Alo = Ahi + CF_CHEB_MT * CF_CHEB_KT;
+        float* Bhi = Alo + CF_CHEB_MT * CF_CHEB_KT;
+        float* Blo = Bhi + NP * CF_CHEB_KT;
+        // the stage is free once the MMAs of K-tile kt - nst (its last user) are done
+        if (kt >= nst) {
+            ok = mbar_wait(smem_u32(mbar + st), (uint32_t)(((kt - nst) / nst) & 1));
+            tc_fence_after();
+            if (!ok) break;
+        }
         const int k0 = kt * CF_CHEB_KT;
         // A: thread tid stages column m = tid: rows k0 + 4j .. 4j+3 form one
         // 16-byte core-matrix row (the warp's loads of one row are 128
@@ -147,17 +163,18 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
         {
             const long c = c0 + tid;
             const bool cin = c < p.C;
-#pragma unroll 2
-            for (int j = 0; j < CF_CHEB_KT / 4; ++j) {
-                float x[4];
+            float x[CF_CHEB_KT];
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int k = k0 + 4 * j + r;
-                    x[r] = (cin && k < p.Ny) ? __ldg(X + (long)k * p.C + c) : 0.0f;
-                }
-                float4 h = make_float4(tf32_round(x[0]), tf32_round(x[1]), tf32_round(x[2]), tf32_round(x[3]));
-                float4 l = make_float4(tf32_round(x[0] - h.x), tf32_round(x[1] - h.y), tf32_round(x[2] - h.z),
-                                       tf32_round(x[3] - h.w));
+            for (int r = 0; r < CF_CHEB_KT; ++r) {
+                const int k = k0 + r;
+                x[r] = (cin && k < p.Ny) ? __ldg(X + (long)k * p.C + c) : 0.0f;
+            }
+#pragma unroll
+            for (int j = 0; j < CF_CHEB_KT / 4; ++j) {
+                float4 h = make_float4(tf32_round(x[4 * j]), tf32_round(x[4 * j + 1]), tf32_round(x[4 * j + 2]),
+                                       tf32_round(x[4 * j + 3]));
+                float4 l = make_float4(tf32_round(x[4 * j] - h.x), tf32_round(x[4 * j + 1] - h.y),
+                                       tf32_round(x[4 * j + 2] - h.z), tf32_round(x[4 * j + 3] - h.w));
                 const int o = (j * CF_CHEB_MT + tid) * 4;  // floats
                 *reinterpret_cast<float4*>(Ahi + o) = h;
                 *reinterpret_cast<float4*>(Alo + o) = l;
@@ -167,8 +184,9 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
         const float4* bh = reinterpret_cast<const float4*>(p.Bhi + (long)kt * NP * CF_CHEB_KT);
         const float4* bl = reinterpret_cast<const float4*>(p.Blo + (long)kt * NP * CF_CHEB_KT);
         for (int i = tid; i < NP * CF_CHEB_KT / 4; i += 128) {
-            reinterpret_cast<float4*>(Bhi)[i] = __ldg(bh + i);
-            reinterpret_cast<float4*>(Blo)[i] = __ldg(bl + i);
+            const float4 vh = __ldg(bh + i), vl = __ldg(bl + i);
+            reinterpret_cast<float4*>(Bhi)[i] = vh;
+            reinterpret_cast<float4*>(Blo)[i] = vl;
         }
         fence_async_smem();
         __syncthreads();
@@ -192,16 +210,15 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
                     umma_tf32(d, al, bhd, idesc, 1u);
                 }
             }
-            umma_commit(smem_u32(mbar));
+            umma_commit(smem_u32(mbar + st));
         }
-        // the tiles are overwritten next: wait for the MMAs that read them
-        if (!mbar_wait(smem_u32(mbar), (uint32_t)(kt & 1))) {
-            ok = false;
-            break;
-        }
-        tc_fence_after();
-        __syncthreads();
     }
+    // drain: the last commit of every stage in use
+    for (int kt = max(0, p.nkt - nst); kt < p.nkt && ok; ++kt) {
+        ok = mbar_wait(smem_u32(mbar + (kt % nst)), (uint32_t)((kt / nst) & 1));
+        tc_fence_after();
+    }
+    __syncthreads();
     if (!ok) {
         if (lane == 0) atomicExch(p.err, 1);
     } else {

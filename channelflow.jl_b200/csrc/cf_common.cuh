@@ -22,6 +22,36 @@ CF_DEV zd zmulis(zd a, double s) { return make_double2(-a.y * s, a.x * s); }
 CF_DEV zd zaxpy(zd a, double s, zd b) { return make_double2(fma(s, b.x, a.x), fma(s, b.y, a.y)); }
 CF_DEV zd zzero() { return make_double2(0.0, 0.0); }
 
+// The same operations on single-precision complex values (the FP32 transforms
+// of the mixed-precision path); real factors are rounded to float once.
+typedef float2 zf;
+CF_DEV zf zadd(zf a, zf b) { return make_float2(a.x + b.x, a.y + b.y); }
+CF_DEV zf zsub(zf a, zf b) { return make_float2(a.x - b.x, a.y - b.y); }
+CF_DEV zf zscale(zf a, double s) {
+    const float f = (float)s;
+    return make_float2(a.x * f, a.y * f);
+}
+CF_DEV zf zmul(zf a, zf b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+CF_DEV zf zconj(zf a) { return make_float2(a.x, -a.y); }
+CF_DEV zf zmuli(zf a) { return make_float2(-a.y, a.x); }
+CF_DEV zf zaxpy(zf a, double s, zf b) {
+    const float f = (float)s;
+    return make_float2(fmaf(f, b.x, a.x), fmaf(f, b.y, a.y));
+}
+// complex value of type Z (zd or zf) from real and imaginary parts
+template <class Z>
+CF_DEV Z cmake(double r, double i);
+template <>
+CF_DEV zd cmake<zd>(double r, double i) { return make_double2(r, i); }
+template <>
+CF_DEV zf cmake<zf>(double r, double i) { return make_float2((float)r, (float)i); }
+template <class Z>
+CF_DEV Z czero() { return cmake<Z>(0.0, 0.0); }
+// conversions between the two precisions
+CF_DEV zd to_zd(zd a) { return a; }
+CF_DEV zd to_zd(zf a) { return make_double2((double)a.x, (double)a.y); }
+CF_DEV zf to_zf(zd a) { return make_float2((float)a.x, (float)a.y); }
+
 // ----------------------------------------------------------- L2 prefetch
 // Bring [p, p+bytes) into L2 (one request per 128-byte line, spread over the
 // calling threads) so that later dependent loads see L2 rather than HBM latency.

@@ -29,7 +29,7 @@ static_assert(CF_NCOL == 1 || CF_NCOL == 2, "column teams use named barriers 1 a
 // instantiation (template argument 0).
 typedef void (*ColKernel)(ColParams);
 typedef void (*FftKernel)(FftParams);
-enum { KC_STAGE, KC_PREP, KC_NLOUT, KC_PROJECT, KC_PRESSURE, KC_COUNT };
+enum { KC_STAGE, KC_PREP, KC_NLOUT, KC_PROJECT, KC_PRESSURE, KC_STAGE_MX, KC_PREP_MX, KC_COUNT };
 enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_COUNT };
 #define CF_COL_LENGTHS(X) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384)
 
@@ -40,6 +40,8 @@ static ColKernel col_kernel_t(int which) {
         case KC_PREP: return k_column_prep<CF_NCOL, PT>;
         case KC_NLOUT: return k_column_nlout<CF_NCOL, PT>;
         case KC_PROJECT: return k_column_project<CF_NCOL, PT>;
+        case KC_STAGE_MX: return k_column_stage_mx<CF_NCOL, PT>;
+        case KC_PREP_MX: return k_column_prep<CF_NCOL, PT, true>;
         default: return k_column_pressure<CF_NCOL, PT>;
     }
 }
@@ -53,20 +55,21 @@ static ColKernel col_kernel(int which, int P) {
     }
 }
 template <int L>
-static FftKernel fft_kernel_t(int which) {
+static FftKernel fft_kernel_t(int which, bool f32) {
     switch (which) {
-        case KF_ZINV: return k_zinv<L>;
-        case KF_ZFWD: return k_zfwd<L>;
-        default: return k_xpass<L>;
+        case KF_ZINV: return f32 ? k_zinv<L, zf> : k_zinv<L, zd>;
+        case KF_ZFWD: return f32 ? k_zfwd<L, zf> : k_zfwd<L, zd>;
+        default: return f32 ? k_xpass<L, zf> : k_xpass<L, zd>;
     }
 }
-static FftKernel fft_kernel(int which, int L) {
+// f32: the FP32 transforms of the mixed-precision form
+static FftKernel fft_kernel(int which, int L, bool f32 = false) {
     switch (L) {
 #define CF_CASE(N) \
-    case N: return fft_kernel_t<N>(which);
+    case N: return fft_kernel_t<N>(which, f32);
         CF_STATIC_FFT_LENGTHS(CF_CASE)
 #undef CF_CASE
-        default: return fft_kernel_t<0>(which);
+        default: return fft_kernel_t<0>(which, f32);
     }
 }
 
@@ -241,6 +244,14 @@ struct cf_engine {
     FftPlan plP, plZ, plX;
     DevBank bank[3], proj, neum;
     bool nodal_valid = false;
+    // mixed-precision form (CF_PRECISION_MIXED): FP32 nodal and z-padded
+    // fields, FP32 twiddles, tensor-core Chebyshev transform images
+    int mixed = 0;
+    void *nod32[6] = {}, *zp32[6] = {};
+    zf *d_twZf = nullptr, *d_twXf = nullptr;
+    float *d_chebF = nullptr, *d_chebI = nullptr;  // [heads | remainders]
+    int chebNP = 0, chebKT = 0;
+    int* d_cheberr = nullptr;
     cudaGraphExec_t graph = nullptr;
     int last_launches = 0;
     std::vector<void*> allocs;
@@ -288,7 +299,7 @@ static bool radices_ok(const std::vector<int>& rad) {
     return true;
 }
 
-static int make_plan(cf_engine* h, int L, FftPlan& pl, zd** dtw) {
+static int make_plan(cf_engine* h, int L, FftPlan& pl, zd** dtw, zf** dtwf = nullptr) {
     std::vector<int> rad = fft_radices(L);
     if (rad.size() > CF_FFT_MAXPASS) return fail(CF_E_UNSUPPORTED, "FFT length has too many factors");
     pl.L = L;
@@ -305,6 +316,14 @@ static int make_plan(cf_engine* h, int L, FftPlan& pl, zd** dtw) {
     if (rc) return rc;
     CU(cudaMemcpy(*dtw, tw.data(), sizeof(zd) * L, cudaMemcpyHostToDevice));
     pl.tw = *dtw;
+    pl.twf = nullptr;
+    if (dtwf) {
+        std::vector<zf> twf(L);
+        for (int k = 0; k < L; ++k) twf[k] = make_float2((float)tw[k].x, (float)tw[k].y);
+        if ((rc = dalloc(h, (void**)dtwf, sizeof(zf) * L))) return rc;
+        CU(cudaMemcpy(*dtwf, twf.data(), sizeof(zf) * L, cudaMemcpyHostToDevice));
+        pl.twf = *dtwf;
+    }
     return CF_OK;
 }
 
@@ -596,12 +615,150 @@ static void drop_graph(cf_engine* h) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed-precision form (CF_PRECISION_MIXED).  Per stage: FP32 z-inverse,
+// x-pass (products in FP32) and z-forward transforms of the nonlinear term;
+// the forward Chebyshev transform of N on the tensor cores; the FP64 column
+// kernel without its DCTs (right-hand side, Stokes, influence and tau
+// corrections, mean mode and flux constraint, curl in coefficient space); the
+// inverse Chebyshev transform of the six fields on the tensor cores, in place.
+// ---------------------------------------------------------------------------
+static void cheb_images(int Ny, int inverse, double scale, std::vector<float>& hi, std::vector<float>& lo, int& NP,
+                        int& nkt);
+static size_t cheb_smem(int NP);
+static int cheb_stages(int NP);
+
+static FftParams fft_params32(const cf_engine* h) {
+    FftParams f = fft_params(h);
+    f.nod0 = h->nod32[0]; f.nod1 = h->nod32[1]; f.nod2 = h->nod32[2];
+    f.nod3 = h->nod32[3]; f.nod4 = h->nod32[4]; f.nod5 = h->nod32[5];
+    f.zp0 = h->zp32[0]; f.zp1 = h->zp32[1]; f.zp2 = h->zp32[2];
+    f.zp3 = h->zp32[3]; f.zp4 = h->zp32[4]; f.zp5 = h->zp32[5];
+    return f;
+}
+static int launch_periodic32(cf_engine* h, int* count) {
+    FftParams f = fft_params32(h);
+    const size_t smz = zsmem(h) / 2, smx = xsmem(h) / 2;  // complex float buffers
+    dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
+    fft_kernel(KF_ZINV, h->Nzp, true)<<<gz, 256, smz, h->stream>>>(f);
+    dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
+    fft_kernel(KF_XPASS, h->Nxp, true)<<<gx, 256, smx, h->stream>>>(f);
+    dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
+    fft_kernel(KF_ZFWD, h->Nzp, true)<<<gz3, 256, smz, h->stream>>>(f);
+    if (count) *count += 3;
+    CU(cudaGetLastError());
+    return CF_OK;
+}
+// Chebyshev transform of the first nf FP32 fields in place (forward: N at the
+// nodes -> normalised coefficients; inverse: coefficients -> nodal values)
+static int launch_cheb(cf_engine* h, int nf, bool inverse, int* count) {
+    ChebParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.Ny = h->Ny;
+    p.NP = h->chebNP;
+    p.nkt = h->chebKT;
+    p.nst = cheb_stages(h->chebNP);
+    p.C = 2 * h->B;
+    for (int f = 0; f < nf; ++f) {
+        p.X[f] = static_cast<const float*>(h->nod32[f]);
+        p.Y[f] = static_cast<float*>(h->nod32[f]);
+    }
+    const float* img = inverse ? h->d_chebI : h->d_chebF;
+    p.Bhi = img;
+    p.Blo = img + (size_t)h->chebKT * h->chebNP * CF_CHEB_KT;
+    p.err = h->d_cheberr;
+    dim3 grid((unsigned)((p.C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nf);
+    k_cheb_mma<<<grid, 128, cheb_smem(h->chebNP), h->stream>>>(p);
+    if (count) *count += 1;
+    CU(cudaGetLastError());
+    return CF_OK;
+}
+static int launch_stage_mx(cf_engine* h, int j, int* count) {
+    int rc;
+    if ((rc = launch_periodic32(h, count))) return rc;
+    if ((rc = launch_cheb(h, 3, false, count))) return rc;
+    ColParams p = stage_col_params(h, j);
+    for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->nod32[i]);
+    for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
+    col_kernel(KC_STAGE_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    if (count) *count += 1;
+    CU(cudaGetLastError());
+    return launch_cheb(h, 6, true, count);
+}
+static int launch_prep_mx(cf_engine* h, int* count) {
+    ColParams p = col_params(h);
+    for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
+    col_kernel(KC_PREP_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    if (count) *count += 1;
+    CU(cudaGetLastError());
+    return launch_cheb(h, 6, true, count);
+}
+static int check_cheb_err(cf_engine* h) {
+    int herr = 0;
+    CU(cudaMemcpyAsync(&herr, h->d_cheberr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if (herr) return fail(CF_E_CUDA, "Chebyshev transform kernel: a tensor-core wait timed out");
+    return CF_OK;
+}
+// mixed step with per-kernel event timing: kernel_ms = [z-inverse, x-pass,
+// z-forward, column, forward Chebyshev, inverse Chebyshev] summed over steps
+static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, double* kernel_ms) {
+    int rc = CF_OK, cnt = 0;
+    if (!h->nodal_valid) {
+        if ((rc = launch_prep_mx(h, &cnt))) return rc;
+        h->nodal_valid = true;
+    }
+    cudaEvent_t ev[7];
+    for (int k = 0; k < 7; ++k) CU(cudaEventCreate(&ev[k]));
+    for (int k = 0; k < 6; ++k) kernel_ms[k] = 0.0;
+    FftParams f = fft_params32(h);
+    const size_t smz = zsmem(h) / 2, smx = xsmem(h) / 2;
+    dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
+    dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
+    dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
+    const int order[6] = {0, 1, 2, 4, 3, 5};  // launch order -> kernel_ms slot
+    for (int s = 0; s < nsteps && rc == CF_OK; ++s)
+        for (int j = 0; j < 3 && rc == CF_OK; ++j) {
+            ColParams p = stage_col_params(h, j);
+            for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->nod32[i]);
+            for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
+            cudaEventRecord(ev[0], h->stream);
+            fft_kernel(KF_ZINV, h->Nzp, true)<<<gz, 256, smz, h->stream>>>(f);
+            cudaEventRecord(ev[1], h->stream);
+            fft_kernel(KF_XPASS, h->Nxp, true)<<<gx, 256, smx, h->stream>>>(f);
+            cudaEventRecord(ev[2], h->stream);
+            fft_kernel(KF_ZFWD, h->Nzp, true)<<<gz3, 256, smz, h->stream>>>(f);
+            cudaEventRecord(ev[3], h->stream);
+            if ((rc = launch_cheb(h, 3, false, nullptr))) break;
+            cudaEventRecord(ev[4], h->stream);
+            col_kernel(KC_STAGE_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+            cudaEventRecord(ev[5], h->stream);
+            if ((rc = launch_cheb(h, 6, true, nullptr))) break;
+            cudaEventRecord(ev[6], h->stream);
+            if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(ev[6]) != cudaSuccess) {
+                rc = fail(CF_E_CUDA, "mixed step failed");
+                break;
+            }
+            for (int k = 0; k < 6; ++k) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+                kernel_ms[order[k]] += ms;
+            }
+        }
+    for (int k = 0; k < 7; ++k) cudaEventDestroy(ev[k]);
+    if (rc) return rc;
+    if ((rc = check_cheb_err(h))) return rc;
+    h->last_launches = cnt + 18 * nsteps;
+    if (t_out) *t_out = t + nsteps * h->dt;
+    return CF_OK;
+}
+
 static int build_graph(cf_engine* h) {
     if (h->graph) return CF_OK;
     cudaGraph_t g;
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int cnt = 0, rc = CF_OK;
-    for (int j = 0; j < 3 && rc == CF_OK; ++j) rc = launch_stage(h, j, &cnt);
+    for (int j = 0; j < 3 && rc == CF_OK; ++j) rc = h->mixed ? launch_stage_mx(h, j, &cnt) : launch_stage(h, j, &cnt);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (rc) return rc;
     if (e != cudaSuccess) return fail(CF_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -636,6 +793,12 @@ static int set_attrs(cf_engine* h) {
     if ((rc = raise_smem_limit(fft_kernel(KF_ZINV, h->Nzp), need[1]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_ZFWD, h->Nzp), need[1]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS, h->Nxp), need[2]))) return rc;
+    if (h->mixed) {
+        if ((rc = raise_smem_limit(fft_kernel(KF_ZINV, h->Nzp, true), need[1] / 2))) return rc;
+        if ((rc = raise_smem_limit(fft_kernel(KF_ZFWD, h->Nzp, true), need[1] / 2))) return rc;
+        if ((rc = raise_smem_limit(fft_kernel(KF_XPASS, h->Nxp, true), need[2] / 2))) return rc;
+        if ((rc = raise_smem_limit(k_cheb_mma, cheb_smem(h->chebNP)))) return rc;
+    }
     return CF_OK;
 }
 
@@ -647,6 +810,11 @@ static int validate_and_size(cf_engine* h, const cf_config* c) {
     if (!(std::isfinite(c->dt) && c->dt > 0)) return fail(CF_E_ARG, "dt must be finite and positive");
     if (!(std::isfinite(c->nu) && c->nu > 0)) return fail(CF_E_ARG, "nu must be finite and positive");
     if (c->constraint != 0 && c->constraint != 1) return fail(CF_E_ARG, "unknown constraint kind");
+    if (c->precision != CF_PRECISION_FP64 && c->precision != CF_PRECISION_MIXED)
+        return fail(CF_E_ARG, "unknown precision mode");
+    if (c->precision == CF_PRECISION_MIXED && c->Ny > 512)
+        return fail(CF_E_UNSUPPORTED, "the mixed-precision form supports Ny <= 512");
+    h->mixed = c->precision == CF_PRECISION_MIXED;
     if (!(std::isfinite(c->c1) && std::isfinite(c->c2))) return fail(CF_E_ARG, "mean-flow constraint values must be finite");
     h->Nx = c->Nx; h->Ny = c->Ny; h->Nz = c->Nz; h->Lx = c->Lx; h->Lz = c->Lz;
     h->nu = c->nu; h->dt = c->dt; h->cmode = c->constraint; h->c1 = c->c1; h->c2 = c->c2;
@@ -733,8 +901,28 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
     cudaMemset(h->Pf, 0, fr);
     cudaMemset(h->d_grad, 0, 16);
     if ((rc = make_plan(h, h->P, h->plP, &h->d_twP))) return bail(rc);
-    if ((rc = make_plan(h, h->Nzp, h->plZ, &h->d_twZ))) return bail(rc);
-    if ((rc = make_plan(h, h->Nxp, h->plX, &h->d_twX))) return bail(rc);
+    if ((rc = make_plan(h, h->Nzp, h->plZ, &h->d_twZ, h->mixed ? &h->d_twZf : nullptr))) return bail(rc);
+    if ((rc = make_plan(h, h->Nxp, h->plX, &h->d_twX, h->mixed ? &h->d_twXf : nullptr))) return bail(rc);
+    if (h->mixed) {
+        // FP32 work fields and the two transform-matrix images
+        for (int i = 0; i < 6; ++i) {
+            if ((rc = dalloc(h, &h->nod32[i], sizeof(zf) * h->nr))) return bail(rc);
+            if ((rc = dalloc(h, &h->zp32[i], sizeof(zf) * h->nq))) return bail(rc);
+        }
+        std::vector<float> fhi, flo, ihi, ilo;
+        cheb_images(h->Ny, 0, 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1)), fhi, flo, h->chebNP, h->chebKT);
+        cheb_images(h->Ny, 1, 1.0, ihi, ilo, h->chebNP, h->chebKT);
+        const size_t nb = sizeof(float) * fhi.size();
+        if ((rc = dalloc(h, (void**)&h->d_chebF, 2 * nb))) return bail(rc);
+        if ((rc = dalloc(h, (void**)&h->d_chebI, 2 * nb))) return bail(rc);
+        if ((rc = dalloc(h, (void**)&h->d_cheberr, sizeof(int)))) return bail(rc);
+        if (cudaMemcpy(h->d_chebF, fhi.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->d_chebF + fhi.size(), flo.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->d_chebI, ihi.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->d_chebI + ihi.size(), ilo.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemset(h->d_cheberr, 0, sizeof(int)) != cudaSuccess)
+            return bail(fail(CF_E_CUDA, "upload failed"));
+    }
     {
         std::vector<zd> cs(h->P + 1);
         const long double pi = 3.141592653589793238462643383279502884L;
@@ -811,14 +999,15 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
     if (nsteps < 0) return fail(CF_E_ARG, "nsteps must be nonnegative");
     int rc, cnt = 0;
     if (!h->nodal_valid) {
-        if ((rc = launch_prep(h, h->U, &cnt))) return rc;
+        if ((rc = h->mixed ? launch_prep_mx(h, &cnt) : launch_prep(h, h->U, &cnt))) return rc;
         h->nodal_valid = true;
     }
     if ((rc = build_graph(h))) return rc;
     for (int s = 0; s < nsteps; ++s) CU(cudaGraphLaunch(h->graph, h->stream));
-    cnt += 12 * nsteps;
+    cnt += (h->mixed ? 18 : 12) * nsteps;
     h->last_launches = cnt;
     if (t_out) *t_out = t + nsteps * h->dt;
+    if (grads_out && h->mixed && (rc = check_cheb_err(h))) return rc;
     if (grads_out) {
         double g[2];
         CU(cudaMemcpyAsync(g, h->d_grad, 16, cudaMemcpyDeviceToHost, h->stream));
@@ -1046,14 +1235,15 @@ int cf_diagnostics(cf_handle* h, double* out) {
 
 int cf_step_profiled(cf_handle* h, double t, int nsteps, double* t_out, double* kernel_ms) {
     if (!h || !kernel_ms) return fail(CF_E_ARG, "null argument");
-    int rc, cnt = 0;
+    if (h->mixed) return step_profiled_mx(h, t, nsteps, t_out, kernel_ms);
+    int rc = CF_OK, cnt = 0;
     if (!h->nodal_valid) {
         if ((rc = launch_prep(h, h->U, &cnt))) return rc;
         h->nodal_valid = true;
     }
     cudaEvent_t ev[5];
     for (int k = 0; k < 5; ++k) CU(cudaEventCreate(&ev[k]));
-    for (int k = 0; k < 4; ++k) kernel_ms[k] = 0.0;
+    for (int k = 0; k < 6; ++k) kernel_ms[k] = 0.0;
     for (int s = 0; s < nsteps && rc == CF_OK; ++s) rc = launch_step_profiled(h, ev, kernel_ms);
     for (int k = 0; k < 5; ++k) cudaEventDestroy(ev[k]);
     if (rc) return rc;
@@ -1230,6 +1420,7 @@ int cf_create_batch(const cf_config* cfgs, int n, cf_batch** out) {
         int rc = cf_create(cfgs + i, &h);
         if (rc) return bail(rc);
         b->inst.push_back(h);
+        if (h->mixed) return bail(fail(CF_E_UNSUPPORTED, "ensembles run the FP64 plain form"));
     }
     for (int i = 0; i < n; ++i) {
         cf_engine* h = b->inst[i];
@@ -1397,11 +1588,17 @@ static void cheb_images(int Ny, int inverse, double scale, std::vector<float>& h
         }
 }
 
-// Dynamic shared memory of k_cheb_mma: its tiles, padded so that the blocks
-// that fit on an SM (228 KB, 1 KB reserved per block) also fit in its 512 TMEM
-// columns, and no block ever waits in the TMEM allocation.
+// Shared-memory stages of k_cheb_mma (two when they fit) and its dynamic
+// shared memory, padded so that the blocks that fit on an SM (228 KB, 1 KB
+// reserved per block) also fit in its 512 TMEM columns, so no block ever waits
+// in the TMEM allocation.
+static int cheb_stages(int NP) {
+    const size_t stage = (size_t)2 * CF_CHEB_MT * CF_CHEB_KT * 4 + (size_t)2 * NP * CF_CHEB_KT * 4;
+    return 2 * stage + 64 <= (size_t)220 * 1024 ? 2 : 1;
+}
 static size_t cheb_smem(int NP) {
-    const size_t tiles = (size_t)2 * CF_CHEB_MT * CF_CHEB_KT * 4 + (size_t)2 * NP * CF_CHEB_KT * 4 + 64;
+    const size_t stage = (size_t)2 * CF_CHEB_MT * CF_CHEB_KT * 4 + (size_t)2 * NP * CF_CHEB_KT * 4;
+    const size_t tiles = cheb_stages(NP) * stage + 64;
     const int ncols = NP <= 32 ? 32 : (NP <= 64 ? 64 : (NP <= 128 ? 128 : (NP <= 256 ? 256 : 512)));
     const size_t per_sm = 233472, maxb = 512 / ncols;
     const size_t floor_b = per_sm / (maxb + 1) - 1024 + 16;  // maxb + 1 blocks no longer fit
@@ -1444,6 +1641,7 @@ int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int
         p.Ny = Ny;
         p.NP = NP;
         p.nkt = nkt;
+        p.nst = cheb_stages(NP);
         p.C = C;
         for (int f = 0; f < nfields; ++f) {
             p.X[f] = dX + (size_t)f * Ny * C;

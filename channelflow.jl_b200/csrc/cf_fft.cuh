@@ -18,8 +18,15 @@ struct FftPlan {
     int L;
     int np;
     unsigned long long rcode;
-    const zd* tw;
+    const zd* tw;   // FP64 twiddles
+    const zf* twf;  // FP32 twiddles (mixed-precision transforms)
 };
+template <class Z>
+CF_DEV const Z* plan_tw(const FftPlan& pl);
+template <>
+CF_DEV const zd* plan_tw<zd>(const FftPlan& pl) { return pl.tw; }
+template <>
+CF_DEV const zf* plan_tw<zf>(const FftPlan& pl) { return pl.twf; }
 
 // Barrier of the thread group: a warp, the whole block (bar == 0), or a
 // 64-thread team on named barrier 1 or 2 (literal ids: a run-time id makes the
@@ -51,157 +58,144 @@ CF_DEV int bpos(int e) {
     return POS ? swz(e) : fpos(e);
 }
 
-CF_DEV zd tw_get(const zd* tw, int k, int sgn) {
-    zd w = __ldg(tw + k);
+template <class Z>
+CF_DEV Z tw_get(const Z* tw, int k, int sgn) {
+    Z w = __ldg(tw + k);
     return sgn > 0 ? zconj(w) : w;
 }
 
-// radix-R DFT of v[0..R) in registers; sgn selects the exponent sign
-template <int R>
-CF_DEV void dft_small(zd* v, int sgn);
-
-template <>
-CF_DEV void dft_small<2>(zd* v, int) {
-    zd a = v[0], b = v[1];
-    v[0] = zadd(a, b);
-    v[1] = zsub(a, b);
-}
-template <>
-CF_DEV void dft_small<3>(zd* v, int sgn) {
-    const double h = 0.86602540378443864676;  // sqrt(3)/2
-    zd a = v[0], t1 = zadd(v[1], v[2]);
-    zd t2 = zaxpy(a, -0.5, t1);
-    zd t3 = zscale(zmuli(zsub(v[1], v[2])), h * sgn);
-    v[0] = zadd(a, t1);
-    v[1] = zadd(t2, t3);
-    v[2] = zsub(t2, t3);
-}
-template <>
-CF_DEV void dft_small<4>(zd* v, int sgn) {
-    zd a0 = zadd(v[0], v[2]), a1 = zsub(v[0], v[2]);
-    zd a2 = zadd(v[1], v[3]), a3 = zscale(zmuli(zsub(v[1], v[3])), (double)sgn);
-    v[0] = zadd(a0, a2);
-    v[2] = zsub(a0, a2);
-    v[1] = zadd(a1, a3);
-    v[3] = zsub(a1, a3);
-}
-template <>
-CF_DEV void dft_small<5>(zd* v, int sgn) {
-    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
-    const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
-    zd a0 = v[0];
-    zd p14 = zadd(v[1], v[4]), m14 = zsub(v[1], v[4]);
-    zd p23 = zadd(v[2], v[3]), m23 = zsub(v[2], v[3]);
-    zd r1 = zaxpy(zaxpy(a0, c1, p14), c2, p23);
-    zd r2 = zaxpy(zaxpy(a0, c2, p14), c1, p23);
-    zd i1 = zscale(zmuli(zaxpy(zscale(m14, s1), s2, m23)), (double)sgn);
-    zd i2 = zscale(zmuli(zaxpy(zscale(m14, s2), -s1, m23)), (double)sgn);
-    v[0] = zadd(a0, zadd(p14, p23));
-    v[1] = zadd(r1, i1);
-    v[4] = zsub(r1, i1);
-    v[2] = zadd(r2, i2);
-    v[3] = zsub(r2, i2);
-}
-template <>
-CF_DEV void dft_small<8>(zd* v, int sgn) {
-    const double h = 0.70710678118654752440;
-    zd e[4] = {v[0], v[2], v[4], v[6]};
-    zd o[4] = {v[1], v[3], v[5], v[7]};
-    dft_small<4>(e, sgn);
-    dft_small<4>(o, sgn);
-    // w = exp(sgn i pi/4)
-    zd w1o = zmake(h * (o[1].x - sgn * o[1].y), h * (o[1].y + sgn * o[1].x));
-    zd w2o = zscale(zmuli(o[2]), (double)sgn);
-    zd w3o = zmake(h * (-o[3].x - sgn * o[3].y), h * (-o[3].y + sgn * o[3].x));
-    v[0] = zadd(e[0], o[0]);
-    v[4] = zsub(e[0], o[0]);
-    v[1] = zadd(e[1], w1o);
-    v[5] = zsub(e[1], w1o);
-    v[2] = zadd(e[2], w2o);
-    v[6] = zsub(e[2], w2o);
-    v[3] = zadd(e[3], w3o);
-    v[7] = zsub(e[3], w3o);
-}
-
 // a * (c + i sgn s): multiply by exp(sgn i theta) given (cos theta, sin theta)
-CF_DEV zd zrot(zd a, double c, double s, int sgn) {
+template <class Z>
+CF_DEV Z zrot(Z a, double c, double s, int sgn) {
     const double ss = sgn * s;
-    return zmake(a.x * c - a.y * ss, a.x * ss + a.y * c);
+    return cmake<Z>(a.x * c - a.y * ss, a.x * ss + a.y * c);
 }
 
-// radix 9 as 3 x 3: X[k1 + 3 k2] = sum_n2 w3^(n2 k2) w9^(n2 k1) sum_n1 x[3 n1 + n2] w3^(n1 k1)
-template <>
-CF_DEV void dft_small<9>(zd* v, int sgn) {
-    // cos, sin of 2 pi m / 9 for m = 1, 2, 4
-    const double c1 = 0.76604444311897803520, s1 = 0.64278760968653932632;
-    const double c2 = 0.17364817766693034885, s2 = 0.98480775301220805936;
-    const double c4 = -0.93969262078590838405, s4 = 0.34202014332566873304;
-    zd y[3][3];
+// radix-R DFT of v[0..R) in registers (complex type Z); sgn selects the
+// exponent sign.  R = 9 is computed as 3 x 3 and R = 16 as 4 x 4:
+//   X[k1 + r1 k2] = sum_n2 w_r2^(n2 k2) w_R^(n2 k1) sum_n1 x[r2 n1 + n2] w_r1^(n1 k1)
+template <int R, class Z>
+CF_DEV void dft_small(Z* v, int sgn) {
+    if constexpr (R == 2) {
+        Z a = v[0], b = v[1];
+        v[0] = zadd(a, b);
+        v[1] = zsub(a, b);
+    } else if constexpr (R == 3) {
+        const double h = 0.86602540378443864676;  // sqrt(3)/2
+        Z a = v[0], t1 = zadd(v[1], v[2]);
+        Z t2 = zaxpy(a, -0.5, t1);
+        Z t3 = zscale(zmuli(zsub(v[1], v[2])), h * sgn);
+        v[0] = zadd(a, t1);
+        v[1] = zadd(t2, t3);
+        v[2] = zsub(t2, t3);
+    } else if constexpr (R == 4) {
+        Z a0 = zadd(v[0], v[2]), a1 = zsub(v[0], v[2]);
+        Z a2 = zadd(v[1], v[3]), a3 = zscale(zmuli(zsub(v[1], v[3])), (double)sgn);
+        v[0] = zadd(a0, a2);
+        v[2] = zsub(a0, a2);
+        v[1] = zadd(a1, a3);
+        v[3] = zsub(a1, a3);
+    } else if constexpr (R == 5) {
+        const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+        const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+        Z a0 = v[0];
+        Z p14 = zadd(v[1], v[4]), m14 = zsub(v[1], v[4]);
+        Z p23 = zadd(v[2], v[3]), m23 = zsub(v[2], v[3]);
+        Z r1 = zaxpy(zaxpy(a0, c1, p14), c2, p23);
+        Z r2 = zaxpy(zaxpy(a0, c2, p14), c1, p23);
+        Z i1 = zscale(zmuli(zaxpy(zscale(m14, s1), s2, m23)), (double)sgn);
+        Z i2 = zscale(zmuli(zaxpy(zscale(m14, s2), -s1, m23)), (double)sgn);
+        v[0] = zadd(a0, zadd(p14, p23));
+        v[1] = zadd(r1, i1);
+        v[4] = zsub(r1, i1);
+        v[2] = zadd(r2, i2);
+        v[3] = zsub(r2, i2);
+    } else if constexpr (R == 8) {
+        const double h = 0.70710678118654752440;
+        Z e[4] = {v[0], v[2], v[4], v[6]};
+        Z o[4] = {v[1], v[3], v[5], v[7]};
+        dft_small<4>(e, sgn);
+        dft_small<4>(o, sgn);
+        // w = exp(sgn i pi/4)
+        Z w1o = cmake<Z>(h * (o[1].x - sgn * o[1].y), h * (o[1].y + sgn * o[1].x));
+        Z w2o = zscale(zmuli(o[2]), (double)sgn);
+        Z w3o = cmake<Z>(h * (-o[3].x - sgn * o[3].y), h * (-o[3].y + sgn * o[3].x));
+        v[0] = zadd(e[0], o[0]);
+        v[4] = zsub(e[0], o[0]);
+        v[1] = zadd(e[1], w1o);
+        v[5] = zsub(e[1], w1o);
+        v[2] = zadd(e[2], w2o);
+        v[6] = zsub(e[2], w2o);
+        v[3] = zadd(e[3], w3o);
+        v[7] = zsub(e[3], w3o);
+    } else if constexpr (R == 9) {
+        // cos, sin of 2 pi m / 9 for m = 1, 2, 4
+        const double c1 = 0.76604444311897803520, s1 = 0.64278760968653932632;
+        const double c2 = 0.17364817766693034885, s2 = 0.98480775301220805936;
+        const double c4 = -0.93969262078590838405, s4 = 0.34202014332566873304;
+        Z y[3][3];
 #pragma unroll
-    for (int n2 = 0; n2 < 3; ++n2) {
-        zd t[3] = {v[n2], v[3 + n2], v[6 + n2]};
-        dft_small<3>(t, sgn);
-        y[n2][0] = t[0];
-        y[n2][1] = t[1];
-        y[n2][2] = t[2];
-    }
-    // twiddles exp(sgn 2 pi i m / 9), m = n2 k1: (1,1) m=1, (1,2) m=2, (2,1) m=2, (2,2) m=4
-    y[1][1] = zrot(y[1][1], c1, s1, sgn);
-    y[1][2] = zrot(y[1][2], c2, s2, sgn);
-    y[2][1] = zrot(y[2][1], c2, s2, sgn);
-    y[2][2] = zrot(y[2][2], c4, s4, sgn);
+        for (int n2 = 0; n2 < 3; ++n2) {
+            Z t[3] = {v[n2], v[3 + n2], v[6 + n2]};
+            dft_small<3>(t, sgn);
+            y[n2][0] = t[0];
+            y[n2][1] = t[1];
+            y[n2][2] = t[2];
+        }
+        // twiddles exp(sgn 2 pi i m / 9), m = n2 k1: (1,1) m=1, (1,2) m=2, (2,1) m=2, (2,2) m=4
+        y[1][1] = zrot(y[1][1], c1, s1, sgn);
+        y[1][2] = zrot(y[1][2], c2, s2, sgn);
+        y[2][1] = zrot(y[2][1], c2, s2, sgn);
+        y[2][2] = zrot(y[2][2], c4, s4, sgn);
 #pragma unroll
-    for (int k1 = 0; k1 < 3; ++k1) {
-        zd t[3] = {y[0][k1], y[1][k1], y[2][k1]};
-        dft_small<3>(t, sgn);
-        v[k1] = t[0];
-        v[k1 + 3] = t[1];
-        v[k1 + 6] = t[2];
-    }
-}
-
-// radix 16 as 4 x 4: X[k1 + 4 k2] = sum_n2 w4^(n2 k2) w16^(n2 k1) sum_n1 x[4 n1 + n2] w4^(n1 k1)
-template <>
-CF_DEV void dft_small<16>(zd* v, int sgn) {
-    // cos, sin of 2 pi m / 16 for m = 1, 2, 3
-    const double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;
-    const double c2 = 0.70710678118654752440, s2 = 0.70710678118654752440;
-    const double c3 = 0.38268343236508977173, s3 = 0.92387953251128675613;
-    zd y[4][4];
+        for (int k1 = 0; k1 < 3; ++k1) {
+            Z t[3] = {y[0][k1], y[1][k1], y[2][k1]};
+            dft_small<3>(t, sgn);
+            v[k1] = t[0];
+            v[k1 + 3] = t[1];
+            v[k1 + 6] = t[2];
+        }
+    } else if constexpr (R == 16) {
+        // cos, sin of 2 pi m / 16 for m = 1, 2, 3
+        const double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;
+        const double c2 = 0.70710678118654752440, s2 = 0.70710678118654752440;
+        const double c3 = 0.38268343236508977173, s3 = 0.92387953251128675613;
+        Z y[4][4];
 #pragma unroll
-    for (int n2 = 0; n2 < 4; ++n2) {
-        zd t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
-        dft_small<4>(t, sgn);
+        for (int n2 = 0; n2 < 4; ++n2) {
+            Z t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+            dft_small<4>(t, sgn);
 #pragma unroll
-        for (int k1 = 0; k1 < 4; ++k1) y[n2][k1] = t[k1];
-    }
-    // twiddles exp(sgn 2 pi i m / 16), m = n2 k1 in 1..9
-    y[1][1] = zrot(y[1][1], c1, s1, sgn);
-    y[1][2] = zrot(y[1][2], c2, s2, sgn);
-    y[1][3] = zrot(y[1][3], c3, s3, sgn);
-    y[2][1] = zrot(y[2][1], c2, s2, sgn);
-    y[2][2] = zscale(zmuli(y[2][2]), (double)sgn);  // m = 4: exp(sgn i pi/2)
-    y[2][3] = zrot(y[2][3], -c2, s2, sgn);          // m = 6: (cos, sin)(3pi/4) = (-c2, s2)
-    y[3][1] = zrot(y[3][1], c3, s3, sgn);
-    y[3][2] = zrot(y[3][2], -c2, s2, sgn);          // m = 6
-    y[3][3] = zrot(y[3][3], -c1, -s1, sgn);         // m = 9: (cos, sin)(9pi/8) = (-c1, -s1)
+            for (int k1 = 0; k1 < 4; ++k1) y[n2][k1] = t[k1];
+        }
+        // twiddles exp(sgn 2 pi i m / 16), m = n2 k1 in 1..9
+        y[1][1] = zrot(y[1][1], c1, s1, sgn);
+        y[1][2] = zrot(y[1][2], c2, s2, sgn);
+        y[1][3] = zrot(y[1][3], c3, s3, sgn);
+        y[2][1] = zrot(y[2][1], c2, s2, sgn);
+        y[2][2] = zscale(zmuli(y[2][2]), (double)sgn);  // m = 4: exp(sgn i pi/2)
+        y[2][3] = zrot(y[2][3], -c2, s2, sgn);          // m = 6: (cos, sin)(3pi/4) = (-c2, s2)
+        y[3][1] = zrot(y[3][1], c3, s3, sgn);
+        y[3][2] = zrot(y[3][2], -c2, s2, sgn);          // m = 6
+        y[3][3] = zrot(y[3][3], -c1, -s1, sgn);         // m = 9: (cos, sin)(9pi/8) = (-c1, -s1)
 #pragma unroll
-    for (int k1 = 0; k1 < 4; ++k1) {
-        zd t[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
-        dft_small<4>(t, sgn);
-        v[k1] = t[0];
-        v[k1 + 4] = t[1];
-        v[k1 + 8] = t[2];
-        v[k1 + 12] = t[3];
+        for (int k1 = 0; k1 < 4; ++k1) {
+            Z t[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+            dft_small<4>(t, sgn);
+            v[k1] = t[0];
+            v[k1 + 4] = t[1];
+            v[k1 + 8] = t[2];
+            v[k1 + 12] = t[3];
+        }
     }
 }
 
 // One out-of-place Stockham pass of compile-time radix R over nb transforms of
 // length L (transform b at src + b*bs, written to dst + b*bs).  A thread keeps
 // one butterfly in registers at a time.
-template <bool BLOCK, int POS, int R>
-CF_DEV void fft_pass_pp(const zd* __restrict__ src, zd* __restrict__ dst, int nb, int bs, int L, int Ns,
-                        const zd* __restrict__ tw, int sgn, int tid, int nth, int bar) {
+template <bool BLOCK, int POS, int R, class Z>
+CF_DEV void fft_pass_pp(const Z* __restrict__ src, Z* __restrict__ dst, int nb, int bs, int L, int Ns,
+                        const Z* __restrict__ tw, int sgn, int tid, int nth, int bar) {
     const int NBf = L / R;
     const int total = nb * NBf;
     const int step = L / (Ns * R);
@@ -209,15 +203,15 @@ CF_DEV void fft_pass_pp(const zd* __restrict__ src, zd* __restrict__ dst, int nb
     for (int q = tid; q < total; q += nth) {
         const int b = q / NBf, j = q - b * NBf;
         const int k = j % Ns;
-        const zd* s = src + (long)b * bs;
-        zd v[R];
+        const Z* s = src + (long)b * bs;
+        Z v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            zd x = s[bpos<POS>(j + r * NBf)];
+            Z x = s[bpos<POS>(j + r * NBf)];
             v[r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
         }
         dft_small<R>(v, sgn);
-        zd* d = dst + (long)b * bs;
+        Z* d = dst + (long)b * bs;
         const int o = (j / Ns) * Ns * R + k;
 #pragma unroll
         for (int r = 0; r < R; ++r) d[bpos<POS>(o + r * Ns)] = v[r];
@@ -227,22 +221,22 @@ CF_DEV void fft_pass_pp(const zd* __restrict__ src, zd* __restrict__ dst, int nb
 
 // Generic prime radix (R <= 31) by a direct DFT; only sizes with uncommon
 // prime factors take this path.
-template <bool BLOCK, int POS>
-CF_DEV void fft_pass_pp_generic(const zd* __restrict__ src, zd* __restrict__ dst, int nb, int bs, int L, int R,
-                                int Ns, const zd* __restrict__ tw, int sgn, int tid, int nth, int bar) {
+template <bool BLOCK, int POS, class Z>
+CF_DEV void fft_pass_pp_generic(const Z* __restrict__ src, Z* __restrict__ dst, int nb, int bs, int L, int R,
+                                int Ns, const Z* __restrict__ tw, int sgn, int tid, int nth, int bar) {
     const int NBf = L / R;
     const int total = nb * NBf;
     const int step = L / (Ns * R);
     for (int q = tid; q < total; q += nth) {
         const int b = q / NBf, j = q - b * NBf;
         const int k = j % Ns;
-        const zd* s = src + (long)b * bs;
-        zd* d = dst + (long)b * bs;
+        const Z* s = src + (long)b * bs;
+        Z* d = dst + (long)b * bs;
         const int ob = (j / Ns) * Ns * R + k;
         for (int o = 0; o < R; ++o) {
-            zd acc = zzero();
+            Z acc = czero<Z>();
             for (int r = 0; r < R; ++r) {
-                zd x = s[bpos<POS>(j + r * NBf)];
+                Z x = s[bpos<POS>(j + r * NBf)];
                 if (r != 0 && k != 0) x = zmul(x, tw_get(tw, k * r * step, sgn));
                 acc = zadd(acc, (r == 0) ? x : zmul(x, tw_get(tw, ((o * r) % R) * NBf, sgn)));
             }
@@ -256,9 +250,9 @@ CF_DEV void fft_pass_pp_generic(const zd* __restrict__ src, zd* __restrict__ dst
 // index split and the twiddle indices need no run-time division, and the R
 // strided positions are one fpos() plus constant offsets where the stride is a
 // multiple of 8 (or the R outputs stay inside one group of 8).
-template <bool BLOCK, int POS, int L, int Ns, int R>
-CF_DEV void fft_pass_static(const zd* __restrict__ src, zd* __restrict__ dst, int nb, int bs,
-                            const zd* __restrict__ tw, int sgn, int tid, int nth, int bar) {
+template <bool BLOCK, int POS, int L, int Ns, int R, class Z>
+CF_DEV void fft_pass_static(const Z* __restrict__ src, Z* __restrict__ dst, int nb, int bs,
+                            const Z* __restrict__ tw, int sgn, int tid, int nth, int bar) {
     constexpr int NBf = L / R;
     constexpr int step = L / (Ns * R);
     constexpr bool LIN_LD = POS == 0 && (NBf % 8) == 0;
@@ -270,16 +264,16 @@ CF_DEV void fft_pass_static(const zd* __restrict__ src, zd* __restrict__ dst, in
     for (int q = tid; q < total; q += nth) {
         const int b = q / NBf, j = q - b * NBf;
         const int k = j % Ns;
-        const zd* s = src + (long)b * bs;
+        const Z* s = src + (long)b * bs;
         const int pj = bpos<POS>(j);
-        zd v[R];
+        Z v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            zd x = s[LIN_LD ? pj + r * DLD : bpos<POS>(j + r * NBf)];
+            Z x = s[LIN_LD ? pj + r * DLD : bpos<POS>(j + r * NBf)];
             v[r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
         }
         dft_small<R>(v, sgn);
-        zd* d = dst + (long)b * bs;
+        Z* d = dst + (long)b * bs;
         const int o = (j / Ns) * Ns * R + k;
         const int po = bpos<POS>(o);
 #pragma unroll
@@ -287,13 +281,13 @@ CF_DEV void fft_pass_static(const zd* __restrict__ src, zd* __restrict__ dst, in
     }
     group_sync<BLOCK>(bar, nth);
 }
-template <bool BLOCK, int POS, int L, int Ns, int R, int... Rest>
-CF_DEV zd* fft_static(zd* src, zd* dst, int nb, int bs, const zd* tw, int sgn, int tid, int nth, int bar) {
+template <class Z, bool BLOCK, int POS, int L, int Ns, int R, int... Rest>
+CF_DEV Z* fft_static(Z* src, Z* dst, int nb, int bs, const Z* tw, int sgn, int tid, int nth, int bar) {
     fft_pass_static<BLOCK, POS, L, Ns, R>(src, dst, nb, bs, tw, sgn, tid, nth, bar);
     if constexpr (sizeof...(Rest) == 0) {
         return dst;
     } else {
-        return fft_static<BLOCK, POS, L, Ns * R, Rest...>(dst, src, nb, bs, tw, sgn, tid, nth, bar);
+        return fft_static<Z, BLOCK, POS, L, Ns * R, Rest...>(dst, src, nb, bs, tw, sgn, tid, nth, bar);
     }
 }
 
@@ -301,21 +295,22 @@ CF_DEV zd* fft_static(zd* src, zd* dst, int nb, int bs, const zd* tw, int sgn, i
 // b*bs + bpos<POS>(e), bs >= fft_bufsz(L) for the padded layout, >=
 // round_up(L, 8) for the XOR layout) held in a; b is a scratch buffer of the
 // same size.  Returns the buffer with the result.
-template <bool BLOCK, int POS>
-CF_DEV zd* group_fft(zd* a, zd* b, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
+template <bool BLOCK, int POS, class Z>
+CF_DEV Z* group_fft(Z* a, Z* b, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
     int Ns = 1;
-    zd* src = a;
-    zd* dst = b;
+    Z* src = a;
+    Z* dst = b;
+    const Z* tw = plan_tw<Z>(pl);
     for (int p = 0; p < pl.np; ++p) {
         const int R = (int)((pl.rcode >> (5 * p)) & 31ull);
-        if (R == 8) fft_pass_pp<BLOCK, POS, 8>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
-        else if (R == 4) fft_pass_pp<BLOCK, POS, 4>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
-        else if (R == 2) fft_pass_pp<BLOCK, POS, 2>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
-        else if (R == 3) fft_pass_pp<BLOCK, POS, 3>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
-        else if (R == 5) fft_pass_pp<BLOCK, POS, 5>(src, dst, nb, bs, pl.L, Ns, pl.tw, sgn, tid, nth, bar);
-        else fft_pass_pp_generic<BLOCK, POS>(src, dst, nb, bs, pl.L, R, Ns, pl.tw, sgn, tid, nth, bar);
+        if (R == 8) fft_pass_pp<BLOCK, POS, 8>(src, dst, nb, bs, pl.L, Ns, tw, sgn, tid, nth, bar);
+        else if (R == 4) fft_pass_pp<BLOCK, POS, 4>(src, dst, nb, bs, pl.L, Ns, tw, sgn, tid, nth, bar);
+        else if (R == 2) fft_pass_pp<BLOCK, POS, 2>(src, dst, nb, bs, pl.L, Ns, tw, sgn, tid, nth, bar);
+        else if (R == 3) fft_pass_pp<BLOCK, POS, 3>(src, dst, nb, bs, pl.L, Ns, tw, sgn, tid, nth, bar);
+        else if (R == 5) fft_pass_pp<BLOCK, POS, 5>(src, dst, nb, bs, pl.L, Ns, tw, sgn, tid, nth, bar);
+        else fft_pass_pp_generic<BLOCK, POS>(src, dst, nb, bs, pl.L, R, Ns, tw, sgn, tid, nth, bar);
         Ns *= R;
-        zd* t = src;
+        Z* t = src;
         src = dst;
         dst = t;
     }
@@ -325,20 +320,21 @@ CF_DEV zd* group_fft(zd* a, zd* b, int nb, int bs, const FftPlan& pl, int sgn, i
 // Transform of compile-time length L (the sizes of the supported grids);
 // L == 0 selects the run-time plan.  The radix order of a static size need not
 // match pl.R: any factorisation indexes the same twiddle table.
-template <bool BLOCK, int L, int POS = 0>
-CF_DEV zd* group_fft_L(zd* a, zd* b, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
-    if constexpr (L == 32) return fft_static<BLOCK, POS, 32, 1, 8, 4>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 48) return fft_static<BLOCK, POS, 48, 1, 8, 2, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 64) return fft_static<BLOCK, POS, 64, 1, 8, 8>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 72) return fft_static<BLOCK, POS, 72, 1, 8, 9>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 96) return fft_static<BLOCK, POS, 96, 1, 8, 4, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 128) return fft_static<BLOCK, POS, 128, 1, 8, 8, 2>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 192) return fft_static<BLOCK, POS, 192, 1, 8, 8, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 256) return fft_static<BLOCK, POS, 256, 1, 8, 8, 4>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 384) return fft_static<BLOCK, POS, 384, 1, 8, 8, 2, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 512) return fft_static<BLOCK, POS, 512, 1, 8, 8, 8>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 576) return fft_static<BLOCK, POS, 576, 1, 8, 8, 9>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
-    else if constexpr (L == 768) return fft_static<BLOCK, POS, 768, 1, 8, 8, 4, 3>(a, b, nb, bs, pl.tw, sgn, tid, nth, bar);
+template <bool BLOCK, int L, int POS = 0, class Z>
+CF_DEV Z* group_fft_L(Z* a, Z* b, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
+    const Z* tw = plan_tw<Z>(pl);
+    if constexpr (L == 32) return fft_static<Z, BLOCK, POS, 32, 1, 8, 4>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 48) return fft_static<Z, BLOCK, POS, 48, 1, 8, 2, 3>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 64) return fft_static<Z, BLOCK, POS, 64, 1, 8, 8>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 72) return fft_static<Z, BLOCK, POS, 72, 1, 8, 9>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 96) return fft_static<Z, BLOCK, POS, 96, 1, 8, 4, 3>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 128) return fft_static<Z, BLOCK, POS, 128, 1, 8, 8, 2>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 192) return fft_static<Z, BLOCK, POS, 192, 1, 8, 8, 3>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 256) return fft_static<Z, BLOCK, POS, 256, 1, 8, 8, 4>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 384) return fft_static<Z, BLOCK, POS, 384, 1, 8, 8, 2, 3>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 512) return fft_static<Z, BLOCK, POS, 512, 1, 8, 8, 8>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 576) return fft_static<Z, BLOCK, POS, 576, 1, 8, 8, 9>(a, b, nb, bs, tw, sgn, tid, nth, bar);
+    else if constexpr (L == 768) return fft_static<Z, BLOCK, POS, 768, 1, 8, 8, 4, 3>(a, b, nb, bs, tw, sgn, tid, nth, bar);
     else return group_fft<BLOCK, POS>(a, b, nb, bs, pl, sgn, tid, nth, bar);
 }
 

@@ -108,8 +108,16 @@ struct ColCtx {
 // Tile of NCOL adjacent columns x Ny degrees into shared memory (column t at
 // sm + t*cs, parity layout).  Each thread issues up to 8 loads before storing
 // any of them, so the block keeps many requests in flight.
-template <int NCOL>
-CF_DEV void tile_load(zd* sm, int cs, int hs, const zd* g, int c0, const ColParams& p) {
+// global element of type G (zd, or zf for the mixed-precision coefficients)
+template <class G>
+CF_DEV G from_zd(zd a);
+template <>
+CF_DEV zd from_zd<zd>(zd a) { return a; }
+template <>
+CF_DEV zf from_zd<zf>(zd a) { return to_zf(a); }
+
+template <int NCOL, class G>
+CF_DEV void tile_load(zd* sm, int cs, int hs, const G* g, int c0, const ColParams& p) {
     constexpr int NT = NCOL * CF_TEAM, K = 8;
     const int tot = p.Ny * NCOL;
     for (int base = threadIdx.x; base < tot; base += NT * K) {
@@ -119,7 +127,7 @@ CF_DEV void tile_load(zd* sm, int cs, int hs, const zd* g, int c0, const ColPara
             const int e = base + u * NT;
             const int n = e / NCOL, t = e - n * NCOL;
             const int c = c0 + t;
-            v[u] = (e < tot && c < p.B) ? g[(long)n * p.B + c] : zzero();
+            v[u] = (e < tot && c < p.B) ? to_zd(g[(long)n * p.B + c]) : zzero();
         }
 #pragma unroll
         for (int u = 0; u < K; ++u) {
@@ -130,18 +138,18 @@ CF_DEV void tile_load(zd* sm, int cs, int hs, const zd* g, int c0, const ColPara
     }
 }
 // L2 prefetch of a tile's rows (one 32-byte row segment per degree)
-template <int NCOL>
-CF_DEV void tile_prefetch(const zd* g, int c0, const ColParams& p) {
+template <int NCOL, class G>
+CF_DEV void tile_prefetch(const G* g, int c0, const ColParams& p) {
     for (int n = threadIdx.x; n < p.Ny; n += NCOL * CF_TEAM)
         asm volatile("prefetch.global.L2 [%0];" ::"l"(g + (long)n * p.B + c0));
 }
-template <int NCOL>
-CF_DEV void tile_store(const zd* sm, int cs, int hs, zd* __restrict__ g, int c0, const ColParams& p) {
+template <int NCOL, class G>
+CF_DEV void tile_store(const zd* sm, int cs, int hs, G* __restrict__ g, int c0, const ColParams& p) {
     const int tot = p.Ny * NCOL;
     for (int e = threadIdx.x; e < tot; e += NCOL * CF_TEAM) {
         const int n = e / NCOL, t = e - n * NCOL;
         const int c = c0 + t;
-        if (c < p.B) g[(long)n * p.B + c] = sm[t * cs + ppos(n, hs)];
+        if (c < p.B) g[(long)n * p.B + c] = from_zd<G>(sm[t * cs + ppos(n, hs)]);
     }
 }
 
@@ -301,7 +309,9 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
 // curl of the total velocity and inverse DCT of all six fields to the nodal
 // buffers (nonlinear.jl:179-185, operators.jl:380-398).  u, v, w in U0, U1, U2
 // (modified); W0, W1, W2 receive the vorticity; Z, Z2 are transform buffers.
-template <int PL>
+// MX (mixed precision): the six fields stay coefficients (the tensor-core
+// transform takes them to the nodes).
+template <int PL, bool MX = false>
 CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z, zd* Z2, const ColParams& p, int c,
                            int ix, int iz, const Team& t) {
     const int q = t.q, lane = t.lane, qo = q * t.hs, nq = pcount(q, t.P);
@@ -320,6 +330,7 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
         W2[o] = zsub(zmulis(U1[o], k), W2[o]);
     }
     tsync(t);
+    if (MX) return;
 #pragma unroll 1
     for (int i = 0; i < 6; ++i) {
         zd* x = i < 3 ? sel3(U0, U1, U2, i) : sel3(W0, W1, W2, i - 3);
@@ -330,7 +341,24 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
 // Full CNRK2 stage for NCOL columns per block (one team per column); bx is
 // the block's index among the instance's column blocks.
 // Regions: 0 R0, 1 R1, 2 R2, 3 PT, 4 A, 5 Bw, 6 Z, 7 Z2 (6, 7: transform buffers).
-template <int NCOL, int PL>
+// The six nodal (or, MX, coefficient) fields u, v, w, omega from regions
+// r0..r5 to p.nod.
+template <int NCOL, bool MX, class Ctx>
+CF_DEV void store_six(const Ctx& X, const ColParams& p, int r0, int r1, int r2, int r3, int r4, int r5) {
+    const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
+    const int rr[6] = {r0, r1, r2, r3, r4, r5};
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        if (MX) tile_store<NCOL>(X.reg(rr[i]), cs, hs, reinterpret_cast<zf*>(p.nod[i]), c0, p);
+        else tile_store<NCOL>(X.reg(rr[i]), cs, hs, p.nod[i], c0, p);
+    }
+}
+
+// MX: mixed-precision form.  The nonlinear term arrives as FP32 Chebyshev
+// coefficients (normalised by the tensor-core transform; p.Nn holds zf
+// arrays) and the new velocity and vorticity leave as FP32 coefficients in
+// p.nod; the arithmetic of the stage stays FP64.
+template <int NCOL, int PL, bool MX = false>
 CF_DEV void column_stage_body(const ColParams& p, int bx) {
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, bx);
@@ -351,7 +379,8 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         tile_prefetch<NCOL>(p.Pf, c0, p);
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            tile_prefetch<NCOL>(p.Nn[i], c0, p);
+            if (MX) tile_prefetch<NCOL>(reinterpret_cast<const zf*>(p.Nn[i]), c0, p);
+            else tile_prefetch<NCOL>(p.Nn[i], c0, p);
             tile_prefetch<NCOL>(p.U[i], c0, p);
             if (p.stage > 0) tile_prefetch<NCOL>(p.Q[i], c0, p);
         }
@@ -372,11 +401,17 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         const zd* Nn_i = sel3(p.Nn[0], p.Nn[1], p.Nn[2], i);
         zd* Q_i = sel3(p.Q[0], p.Q[1], p.Q[2], i);
         zd* U_i = sel3(p.U[0], p.U[1], p.U[2], i);
-        tile_load<NCOL>(X.reg(4), cs, hs, Nn_i, c0, p);
+        if (MX) tile_load<NCOL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p);
+        else tile_load<NCOL>(X.reg(4), cs, hs, Nn_i, c0, p);
         if (p.stage > 0) tile_load<NCOL>(X.reg(5), cs, hs, Q_i, c0, p);
         __syncthreads();
         if (valid) {
-            col_forward_y<PL>(X.col(4), X.col(6), X.col(7), p, nyq, t);
+            if (!MX) {
+                col_forward_y<PL>(X.col(4), X.col(6), X.col(7), p, nyq, t);
+            } else if (nyq) {
+                col_zero(X.col(4), t);
+                tsync(t);
+            }
             if (c == 0) {
                 const zd bm = col_bulkmean(X.col(4), t);
                 if (i == 0) bulkN0 = bm;
@@ -467,15 +502,10 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     __syncthreads();
     // ---------------- Phase C: total velocity, vorticity, nodal values
     if (valid)
-        col_prep_nodal<PL>(X.col(0), X.col(4), X.col(2), X.col(1), X.col(3), X.col(5), X.col(6), X.col(7), p, c, X.ix,
-                           X.iz, t);
+        col_prep_nodal<PL, MX>(X.col(0), X.col(4), X.col(2), X.col(1), X.col(3), X.col(5), X.col(6), X.col(7), p, c,
+                               X.ix, X.iz, t);
     __syncthreads();
-    tile_store<NCOL>(X.reg(0), cs, hs, p.nod[0], c0, p);
-    tile_store<NCOL>(X.reg(4), cs, hs, p.nod[1], c0, p);
-    tile_store<NCOL>(X.reg(2), cs, hs, p.nod[2], c0, p);
-    tile_store<NCOL>(X.reg(1), cs, hs, p.nod[3], c0, p);
-    tile_store<NCOL>(X.reg(3), cs, hs, p.nod[4], c0, p);
-    tile_store<NCOL>(X.reg(5), cs, hs, p.nod[5], c0, p);
+    store_six<NCOL, MX>(X, p, 0, 4, 2, 1, 3, 5);
 }
 
 template <int NCOL, int PL>
@@ -492,8 +522,15 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>()))
     column_stage_body<NCOL, PL>(ps, blockIdx.x);
 }
 
-// Nodal velocity and vorticity from the state U (used after set_state).
+// Mixed-precision stage (see column_stage_body).
 template <int NCOL, int PL>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_stage_mx(ColParams p) {
+    column_stage_body<NCOL, PL, true>(p, blockIdx.x);
+}
+
+// Nodal velocity and vorticity from the state U (used after set_state); MX:
+// their FP32 Chebyshev coefficients instead.
+template <int NCOL, int PL, bool MX = false>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_prep(ColParams p) {
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
@@ -503,15 +540,10 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     tile_load<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p);
     __syncthreads();
     if (X.valid)
-        col_prep_nodal<PL>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7), p, X.c, X.ix,
-                           X.iz, X.t);
+        col_prep_nodal<PL, MX>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7), p, X.c,
+                               X.ix, X.iz, X.t);
     __syncthreads();
-    tile_store<NCOL>(X.reg(0), cs, hs, p.nod[0], c0, p);
-    tile_store<NCOL>(X.reg(1), cs, hs, p.nod[1], c0, p);
-    tile_store<NCOL>(X.reg(2), cs, hs, p.nod[2], c0, p);
-    tile_store<NCOL>(X.reg(3), cs, hs, p.nod[3], c0, p);
-    tile_store<NCOL>(X.reg(4), cs, hs, p.nod[4], c0, p);
-    tile_store<NCOL>(X.reg(5), cs, hs, p.nod[5], c0, p);
+    store_six<NCOL, MX>(X, p, 0, 1, 2, 3, 4, 5);
 }
 
 // Forward DCT of the nonlinear term only: coefficients into p.Nout.

@@ -39,6 +39,15 @@ extern "C" {
 #define CF_CONSTRAINT_PRESSUREGRADIENT 0 /* (dPdx, dPdz) prescribed */
 #define CF_CONSTRAINT_BULKVELOCITY 1     /* total bulk velocities (Ubulk, Wbulk) prescribed */
 
+/* Precision of the step.  FP64: the plain form, every operation in double
+ * precision (parity with the reference's step!).  MIXED: the nonlinear term's
+ * periodic transforms and products in FP32 and the Chebyshev transforms as
+ * tensor-core contractions (TF32 heads and remainders, FP32 accumulation);
+ * right-hand side, tau Helmholtz solves, influence-matrix and tau corrections,
+ * mean mode and flux constraint stay FP64, as does the state. */
+#define CF_PRECISION_FP64 0
+#define CF_PRECISION_MIXED 1
+
 typedef struct cf_config {
     int Nx, Ny, Nz;      /* Grid(Nx, Ny, Nz, Lx, Lz): grids.jl:27-30 */
     double Lx, Lz;
@@ -47,6 +56,7 @@ typedef struct cf_config {
     const double* base_values; /* Ny values when profile == CF_PROFILE_VALUES */
     int constraint;      /* CF_CONSTRAINT_* (problem.jl:81-87) */
     double c1, c2;       /* gradients or bulk velocities */
+    int precision;       /* CF_PRECISION_* (0: FP64 plain form) */
 } cf_config;
 
 typedef struct cf_engine cf_handle;
@@ -137,8 +147,9 @@ int cf_random_state(cf_handle* h, unsigned long long seed, double amp, int shape
 int cf_diagnostics(cf_handle* h, double* out);
 
 /* step! like cf_step without the CUDA graph, with CUDA events around every
- * kernel class; kernel_ms[0..3] receives the summed device time of the
- * z-inverse, x-pass, z-forward and column kernels over the nsteps steps. */
+ * kernel class; kernel_ms[0..5] receives the summed device time of the
+ * z-inverse, x-pass, z-forward and column kernels and (mixed precision) the
+ * forward and inverse tensor-core Chebyshev transforms over the nsteps steps. */
 int cf_step_profiled(cf_handle* h, double t, int nsteps, double* t_out, double* kernel_ms);
 
 /* Block until the handle's stream is idle. */

@@ -1,0 +1,88 @@
+"""GPU: the mixed-precision step (FP32 periodic transforms and products,
+tensor-core Chebyshev transforms with TF32 heads and remainders, FP64
+Stokes solve) against the FP64 step of the oracle and of the engine.
+
+The nonlinear term carries FP32 rounding (~1e-7 relative), which the step
+passes to the velocity through dt * N; the tolerances below (1e-5 relative L2
+on the velocity, 1e-6 on the kinetic energy) bound that, and the divergence
+and the constant-flux constraint must hold as in the FP64 form (they are
+imposed by the FP64 Stokes solve).
+"""
+import numpy as np
+import pytest
+
+import cfb200
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+C1 = dict(Nx=32, Ny=33, Nz=32, Lx=2 * np.pi / 1.14, Lz=2 * np.pi / 2.5)
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_mixed_couette_matches_oracle():
+    c = C1
+    g = cfb200.Grid(c["Nx"], c["Ny"], c["Nz"], c["Lx"], c["Lz"])
+    mx = cfb200.CouetteFlow(g, 1 / 400, 0.01, precision="mixed")
+    ref = O.couette(c["Nx"], c["Ny"], c["Nz"], c["Lx"], c["Lz"], 1 / 400, 0.01)
+    U, P = ref.random_state(seed=1, amp=0.1)
+    mx.set_state(U, P)
+    Ur, Pr = U.copy(), P.copy()
+    ref.step(Ur, Pr, 10)
+    mx.advance(0.0, 10)
+    Um, _ = mx.get_state()
+    assert np.all(np.isfinite(Um))
+    e10 = rel(Um, Ur)
+    assert e10 <= 1e-5, e10
+    ref.step(Ur, Pr, 90)
+    mx.advance(0.0, 90)
+    Um, _ = mx.get_state()
+    e100 = rel(Um, Ur)
+    assert e100 <= 1e-5, e100
+    dm, dr = mx.diagnostics(), ref.diagnostics(Ur)
+    assert abs(dm[0] - dr[0]) <= 1e-6 * abs(dr[0])
+    assert dm[2] <= 1e-10  # divergence
+    mx.close()
+
+
+def test_mixed_poiseuille_flux_matches_fp64_engine():
+    g = cfb200.Grid(24, 25, 20, 2 * np.pi, np.pi)
+    kw = dict(bulkvelocity=(2 / 3, 0.0))
+    f64 = cfb200.PoiseuilleFlow(g, 1 / 1500, 0.005, **kw)
+    mx = cfb200.PoiseuilleFlow(g, 1 / 1500, 0.005, precision="mixed", **kw)
+    st = cfb200.random_state(f64, 0.1, seed=4)
+    mx.set_state(st.U, st.P)
+    _, g64 = f64.advance(0.0, 20)
+    _, gmx = mx.advance(0.0, 20)
+    U64, _ = f64.get_state()
+    Umx, _ = mx.get_state()
+    assert rel(Umx, U64) <= 1e-5
+    # the mean gradient carries the FP32 rounding of the bulk mean of N_x
+    # (order 0.1 here) in absolute terms; the gradient itself is ~3e-4
+    assert abs(gmx[0] - g64[0]) <= 1e-6
+    # the perturbation's bulk velocity stays at its target (the FP64 constraint)
+    ny = g.Ny
+    n = np.arange(ny)
+    w = np.where(n % 2 == 0, 1.0 / (1.0 - n * n), 0.0)
+    w[0] = 1.0
+    assert abs(np.dot(w, Umx[0, :, 0, 0].real) - np.dot(w, U64[0, :, 0, 0].real)) <= 1e-9
+    f64.close()
+    mx.close()
+
+
+@pytest.mark.parametrize("dims", [(9, 17, 7), (16, 17, 16), (48, 33, 40)])
+def test_mixed_one_step_sizes(dims):
+    Nx, Ny, Nz = dims
+    g = cfb200.Grid(Nx, Ny, Nz, 5.3, 7.1)
+    ref = O.couette(Nx, Ny, Nz, 5.3, 7.1, 1 / 300, 0.01)
+    mx = cfb200.CouetteFlow(g, 1 / 300, 0.01, precision="mixed")
+    U, P = ref.random_state(seed=3, amp=0.2)
+    mx.set_state(U, P)
+    ref.step(U, P, 2)
+    mx.advance(0.0, 2)
+    Um, _ = mx.get_state()
+    assert rel(Um, U) <= 1e-5
+    mx.close()
