@@ -12,15 +12,19 @@
 //
 // The contraction is computed transposed, D = X^T T^T: M = 128 columns of X per
 // block (TMEM lane m = column), N = the output degrees (MMAs of at most 256),
-// K = the input degrees in tiles of 32.  Both operands are K-major in shared
+// K = the input degrees in tiles of 16.  For more than 256 output degrees
+// the degrees are split over two blocks (grid z), so that every block holds at
+// most 256 TMEM columns and two blocks fit on an SM.  Both operands are K-major in shared
 // memory, in the canonical no-swizzle layout of the tensor cores (core
 // matrices of 8 rows x 16 bytes, rows 16 bytes apart, 8-row groups 128 bytes
 // apart, 4-element K chunks LBO bytes apart):
 //   A (X^T): element (m, k) of a K-tile at ((k/4)*128 + m)*16 + (k%4)*4 bytes
 //            (LBO 2048 B); each thread stages one column m, four rows at a time,
-//   B (T^T): element (n, k) at ((k/4)*NP + n)*16 + (k%4)*4 bytes (LBO NP*16 B),
-//            NP = Ny rounded up to 16; the engine stores T^T in global memory
-//            in exactly these K-tile images.
+//   B (T^T): element (n, k) of the block's output range at ((k/4)*NPs + n)*16
+//            + (k%4)*4 bytes (LBO NPs*16 B), NPs = the range's size (a multiple
+//            of 16); the engine stores T^T in global memory as K-tile images
+//            [4-k chunk][NP rows][4 floats], NP = nsplit * NPs, from which a
+//            block copies its NPs rows of each chunk.
 // TF32 keeps 10 mantissa bits, so each operand is split into a TF32 head and
 // the TF32 rounding of its remainder; hi*hi + hi*lo + lo*hi restores ~FP32
 // accuracy (the three products accumulate in the same FP32 tensor memory).
@@ -28,16 +32,17 @@
 #include "cf_common.cuh"
 
 #define CF_CHEB_MT 128   // columns per block (MMA M)
-#define CF_CHEB_KT 32    // input degrees per K-tile
+#define CF_CHEB_KT 16    // input degrees per K-tile
 #define CF_CHEB_MAXF 6   // fields per launch
 
 struct ChebParams {
-    int Ny, NP, nkt;   // degrees, output degrees rounded up to 16, K-tiles
+    int Ny, NP, nkt;   // degrees, output rows of the images (nsplit * NPs), K-tiles
+    int NPs;           // output rows per block (a multiple of 16, <= 256)
     int nst;           // shared-memory stages (1 or 2)
     long C;            // real columns per field
     const float* X[CF_CHEB_MAXF];
     float* Y[CF_CHEB_MAXF];
-    const float* Bhi;  // [nkt][NP*128 bytes] K-tile images of T^T (TF32 heads)
+    const float* Bhi;  // [nkt][4 chunks][NP rows][4 floats] K-tile images of T^T (TF32 heads)
     const float* Blo;  // remainders
     int* err;          // set to 1 when a wait gives up
 };
@@ -109,22 +114,23 @@ CF_DEV void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 // ---- the kernel ------------------------------------------------------------------
-// grid (ceil(C / 128), fields); 128 threads.  Dynamic shared memory: nst
-// stages of [A heads, A remainders (16 KB each), B heads, B remainders
-// (NP * 128 B each)], then two mbarriers and the TMEM address.  With two
+// grid (ceil(C / 128), fields, nsplit); 128 threads.  Dynamic shared memory:
+// nst stages of [A heads, A remainders (8 KB each), B heads, B remainders
+// (NPs * 64 B each)], then two mbarriers and the TMEM address.  With two
 // stages the loads of K-tile kt overlap the MMAs of K-tile kt - 1.
-CF_DEV uint32_t cheb_stage_bytes(int NP) { return 2u * CF_CHEB_MT * CF_CHEB_KT * 4 + 2u * NP * CF_CHEB_KT * 4; }
+CF_DEV uint32_t cheb_stage_bytes(int NPs) { return 2u * CF_CHEB_MT * CF_CHEB_KT * 4 + 2u * NPs * CF_CHEB_KT * 4; }
 
 __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
     extern __shared__ __align__(1024) unsigned char csm[];
     const int f = blockIdx.y, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long c0 = (long)blockIdx.x * CF_CHEB_MT;
-    const int NP = p.NP, nst = p.nst;
-    const uint32_t sb = cheb_stage_bytes(NP);
+    const int NP = p.NP, NPs = p.NPs, nst = p.nst;
+    const int nlo = blockIdx.z * NPs;  // first output row of this block
+    const uint32_t sb = cheb_stage_bytes(NPs);
     uint64_t* mbar = reinterpret_cast<uint64_t*>(csm + nst * sb);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
     // TMEM columns: a power of two >= NP (and >= 32)
-    const int ncols = NP <= 32 ? 32 : (NP <= 64 ? 64 : (NP <= 128 ? 128 : (NP <= 256 ? 256 : 512)));
+    const int ncols = NPs <= 32 ? 32 : (NPs <= 64 ? 64 : (NPs <= 128 ? 128 : 256));
     const float* X = p.X[f];
     float* Y = p.Y[f];
 
@@ -144,49 +150,79 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
     const uint32_t tmem = *tslot;
     bool ok = true;
 
+    // Software pipeline: the X values of K-tile kt + 1 are requested into
+    // registers before K-tile kt is written to shared memory and multiplied,
+    // so their memory latency overlaps the staging and the MMAs.
+    const long cm = c0 + tid;  // the column this thread stages
+    const bool cin = cm < p.C;
+    float xc[CF_CHEB_KT], xn[CF_CHEB_KT];
+#pragma unroll
+    for (int r = 0; r < CF_CHEB_KT; ++r) xc[r] = (cin && r < p.Ny) ? __ldg(X + (long)r * p.C + cm) : 0.0f;
+    constexpr int BQ = 5;  // float4 of one image part per thread (NPs * 4 <= 5 * 128 for NPs <= 160)
     for (int kt = 0; kt < p.nkt && ok; ++kt) {
         const int st = kt % nst;
         float* Ahi = reinterpret_cast<float*>(csm + st * sb);
         float* Alo = Ahi + CF_CHEB_MT * CF_CHEB_KT;
         float* Bhi = Alo + CF_CHEB_MT * CF_CHEB_KT;
-        float* Blo = Bhi + NP * CF_CHEB_KT;
+        float* Blo = Bhi + NPs * CF_CHEB_KT;
+        const int k0 = kt * CF_CHEB_KT;
+        // requests: X of the next K-tile, and this K-tile's rows of the images
+        // (chunk ch, row n of the block's range; i = ch * NPs + n)
+        if (kt + 1 < p.nkt) {
+#pragma unroll
+            for (int r = 0; r < CF_CHEB_KT; ++r) {
+                const int k = k0 + CF_CHEB_KT + r;
+                xn[r] = (cin && k < p.Ny) ? __ldg(X + (long)k * p.C + cm) : 0.0f;
+            }
+        }
+        const float4* bh = reinterpret_cast<const float4*>(p.Bhi + (long)kt * NP * CF_CHEB_KT);
+        const float4* bl = reinterpret_cast<const float4*>(p.Blo + (long)kt * NP * CF_CHEB_KT);
+        const int nb4 = NPs * CF_CHEB_KT / 4;
+        float4 vh[BQ], vl[BQ];
+        if (nb4 <= BQ * 128) {
+#pragma unroll
+            for (int u = 0; u < BQ; ++u) {
+                const int i = tid + 128 * u;
+                if (i < nb4) {
+                    const int ch = i / NPs, g = ch * NP + nlo + (i - ch * NPs);
+                    vh[u] = __ldg(bh + g);
+                    vl[u] = __ldg(bl + g);
+                }
+            }
+        }
         // the stage is free once the MMAs of K-tile kt - nst (its last user) are done
         if (kt >= nst) {
             ok = mbar_wait(smem_u32(mbar + st), (uint32_t)(((kt - nst) / nst) & 1));
             tc_fence_after();
             if (!ok) break;
         }
-        const int k0 = kt * CF_CHEB_KT;
-        // A: thread tid stages column m = tid: rows k0 + 4j .. 4j+3 form one
-        // 16-byte core-matrix row (the warp's loads of one row are 128
-        // contiguous bytes; its stores are consecutive 16-byte rows)
-        {
-            const long c = c0 + tid;
-            const bool cin = c < p.C;
-            float x[CF_CHEB_KT];
+        // A: column cm, rows k0 + 4j .. 4j+3 form one 16-byte core-matrix row
 #pragma unroll
-            for (int r = 0; r < CF_CHEB_KT; ++r) {
-                const int k = k0 + r;
-                x[r] = (cin && k < p.Ny) ? __ldg(X + (long)k * p.C + c) : 0.0f;
-            }
-#pragma unroll
-            for (int j = 0; j < CF_CHEB_KT / 4; ++j) {
-                float4 h = make_float4(tf32_round(x[4 * j]), tf32_round(x[4 * j + 1]), tf32_round(x[4 * j + 2]),
-                                       tf32_round(x[4 * j + 3]));
-                float4 l = make_float4(tf32_round(x[4 * j] - h.x), tf32_round(x[4 * j + 1] - h.y),
-                                       tf32_round(x[4 * j + 2] - h.z), tf32_round(x[4 * j + 3] - h.w));
-                const int o = (j * CF_CHEB_MT + tid) * 4;  // floats
-                *reinterpret_cast<float4*>(Ahi + o) = h;
-                *reinterpret_cast<float4*>(Alo + o) = l;
-            }
+        for (int j = 0; j < CF_CHEB_KT / 4; ++j) {
+            float4 h = make_float4(tf32_round(xc[4 * j]), tf32_round(xc[4 * j + 1]), tf32_round(xc[4 * j + 2]),
+                                   tf32_round(xc[4 * j + 3]));
+            float4 l = make_float4(tf32_round(xc[4 * j] - h.x), tf32_round(xc[4 * j + 1] - h.y),
+                                   tf32_round(xc[4 * j + 2] - h.z), tf32_round(xc[4 * j + 3] - h.w));
+            const int o = (j * CF_CHEB_MT + tid) * 4;  // floats
+            *reinterpret_cast<float4*>(Ahi + o) = h;
+            *reinterpret_cast<float4*>(Alo + o) = l;
         }
-        // B: straight copy of this K-tile's images
-        const float4* bh = reinterpret_cast<const float4*>(p.Bhi + (long)kt * NP * CF_CHEB_KT);
-        const float4* bl = reinterpret_cast<const float4*>(p.Blo + (long)kt * NP * CF_CHEB_KT);
-        for (int i = tid; i < NP * CF_CHEB_KT / 4; i += 128) {
-            const float4 vh = __ldg(bh + i), vl = __ldg(bl + i);
-            reinterpret_cast<float4*>(Bhi)[i] = vh;
-            reinterpret_cast<float4*>(Blo)[i] = vl;
+        // B: this block's NPs rows of each 4-k chunk of the K-tile's images
+        if (nb4 <= BQ * 128) {
+#pragma unroll
+            for (int u = 0; u < BQ; ++u) {
+                const int i = tid + 128 * u;
+                if (i < nb4) {
+                    reinterpret_cast<float4*>(Bhi)[i] = vh[u];
+                    reinterpret_cast<float4*>(Blo)[i] = vl[u];
+                }
+            }
+        } else {
+            for (int i = tid; i < nb4; i += 128) {
+                const int ch = i / NPs, g = ch * NP + nlo + (i - ch * NPs);
+                reinterpret_cast<float4*>(Bhi)[i] = __ldg(bh + g);
+                reinterpret_cast<float4*>(Blo)[i] = __ldg(bl + g);
+            }
         }
         fence_async_smem();
         __syncthreads();
@@ -194,16 +230,16 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
             tc_fence_after();
             const int ksteps = min(CF_CHEB_KT, p.Ny - k0 + 7) / 8;  // 8-degree steps holding data
             for (int ks = 0; ks < ksteps; ++ks) {
-                const uint32_t aoff = ks * 2 * CF_CHEB_MT * 16, boff = ks * 2 * NP * 16;
-                for (int n0 = 0; n0 < NP; n0 += 256) {
-                    const int N = min(256, NP - n0);
+                const uint32_t aoff = ks * 2 * CF_CHEB_MT * 16, boff = ks * 2 * NPs * 16;
+                for (int n0 = 0; n0 < NPs; n0 += 256) {
+                    const int N = min(256, NPs - n0);
                     const uint32_t idesc = umma_idesc_tf32(CF_CHEB_MT, N);
                     const uint32_t d = tmem + (uint32_t)n0;
                     const uint32_t bo = boff + (n0 / 8) * 128;
                     const uint64_t ah = umma_desc(smem_u32(Ahi) + aoff, CF_CHEB_MT * 16, 128);
                     const uint64_t al = umma_desc(smem_u32(Alo) + aoff, CF_CHEB_MT * 16, 128);
-                    const uint64_t bhd = umma_desc(smem_u32(Bhi) + bo, NP * 16, 128);
-                    const uint64_t bld = umma_desc(smem_u32(Blo) + bo, NP * 16, 128);
+                    const uint64_t bhd = umma_desc(smem_u32(Bhi) + bo, NPs * 16, 128);
+                    const uint64_t bld = umma_desc(smem_u32(Blo) + bo, NPs * 16, 128);
                     const uint32_t acc0 = (kt > 0 || ks > 0) ? 1u : 0u;
                     umma_tf32(d, ah, bhd, idesc, acc0);
                     umma_tf32(d, ah, bld, idesc, 1u);
@@ -212,6 +248,8 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
             }
             umma_commit(smem_u32(mbar + st));
         }
+#pragma unroll
+        for (int r = 0; r < CF_CHEB_KT; ++r) xc[r] = xn[r];
     }
     // drain: the last commit of every stage in use
     for (int kt = max(0, p.nkt - nst); kt < p.nkt && ok; ++kt) {
@@ -225,13 +263,13 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
         // epilogue: lane m of warp w holds column c0 + 32 w + m
         const long c = c0 + 32 * warp + lane;
         const uint32_t tw = tmem + ((uint32_t)(32 * warp) << 16);
-        for (int n0 = 0; n0 < NP; n0 += 16) {
+        for (int n0 = 0; n0 < NPs; n0 += 16) {
             float v[16];
             tmem_ld16(tw + (uint32_t)n0, v);
             if (c < p.C) {
 #pragma unroll
                 for (int i = 0; i < 16; ++i)
-                    if (n0 + i < p.Ny) Y[(long)(n0 + i) * p.C + c] = v[i];
+                    if (nlo + n0 + i < p.Ny) Y[(long)(nlo + n0 + i) * p.C + c] = v[i];
             }
         }
     }

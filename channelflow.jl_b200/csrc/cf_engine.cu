@@ -248,6 +248,7 @@ struct cf_engine {
     // fields, FP32 twiddles, tensor-core Chebyshev transform images
     int mixed = 0;
     void *nod32[6] = {}, *zp32[6] = {};
+    void* coef32[6] = {};  // FP32 Chebyshev coefficients (the transforms run out of place)
     zf *d_twZf = nullptr, *d_twXf = nullptr;
     float *d_chebF = nullptr, *d_chebI = nullptr;  // [heads | remainders]
     int chebNP = 0, chebKT = 0;
@@ -625,8 +626,9 @@ static void drop_graph(cf_engine* h) {
 // ---------------------------------------------------------------------------
 static void cheb_images(int Ny, int inverse, double scale, std::vector<float>& hi, std::vector<float>& lo, int& NP,
                         int& nkt);
-static size_t cheb_smem(int NP);
-static int cheb_stages(int NP);
+static size_t cheb_smem(int NPs);
+static int cheb_stages(int NPs);
+static void cheb_dims(int Ny, int& NPs, int& nsplit, int& NP);
 
 static FftParams fft_params32(const cf_engine* h) {
     FftParams f = fft_params(h);
@@ -649,26 +651,31 @@ static int launch_periodic32(cf_engine* h, int* count) {
     CU(cudaGetLastError());
     return CF_OK;
 }
-// Chebyshev transform of the first nf FP32 fields in place (forward: N at the
-// nodes -> normalised coefficients; inverse: coefficients -> nodal values)
+// Chebyshev transform of the first nf FP32 fields (forward: N at the nodes,
+// nod32 -> normalised coefficients, coef32; inverse: coefficients, coef32 ->
+// nodal values, nod32).  Out of place: the two blocks that share a column tile
+// when the output degrees are split both read all of its input rows.
 static int launch_cheb(cf_engine* h, int nf, bool inverse, int* count) {
     ChebParams p;
     std::memset(&p, 0, sizeof(p));
     p.Ny = h->Ny;
     p.NP = h->chebNP;
     p.nkt = h->chebKT;
-    p.nst = cheb_stages(h->chebNP);
+    int NPs, nsplit, NPt;
+    cheb_dims(h->Ny, NPs, nsplit, NPt);
+    p.NPs = NPs;
+    p.nst = cheb_stages(NPs);
     p.C = 2 * h->B;
     for (int f = 0; f < nf; ++f) {
-        p.X[f] = static_cast<const float*>(h->nod32[f]);
-        p.Y[f] = static_cast<float*>(h->nod32[f]);
+        p.X[f] = static_cast<const float*>(inverse ? h->coef32[f] : h->nod32[f]);
+        p.Y[f] = static_cast<float*>(inverse ? h->nod32[f] : h->coef32[f]);
     }
     const float* img = inverse ? h->d_chebI : h->d_chebF;
     p.Bhi = img;
     p.Blo = img + (size_t)h->chebKT * h->chebNP * CF_CHEB_KT;
     p.err = h->d_cheberr;
-    dim3 grid((unsigned)((p.C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nf);
-    k_cheb_mma<<<grid, 128, cheb_smem(h->chebNP), h->stream>>>(p);
+    dim3 grid((unsigned)((p.C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nf, (unsigned)nsplit);
+    k_cheb_mma<<<grid, 128, cheb_smem(NPs), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return CF_OK;
@@ -678,8 +685,8 @@ static int launch_stage_mx(cf_engine* h, int j, int* count) {
     if ((rc = launch_periodic32(h, count))) return rc;
     if ((rc = launch_cheb(h, 3, false, count))) return rc;
     ColParams p = stage_col_params(h, j);
-    for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->nod32[i]);
-    for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
+    for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->coef32[i]);
+    for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->coef32[i]);
     col_kernel(KC_STAGE_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
@@ -687,7 +694,7 @@ static int launch_stage_mx(cf_engine* h, int j, int* count) {
 }
 static int launch_prep_mx(cf_engine* h, int* count) {
     ColParams p = col_params(h);
-    for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
+    for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->coef32[i]);
     col_kernel(KC_PREP_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
@@ -720,8 +727,8 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
     for (int s = 0; s < nsteps && rc == CF_OK; ++s)
         for (int j = 0; j < 3 && rc == CF_OK; ++j) {
             ColParams p = stage_col_params(h, j);
-            for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->nod32[i]);
-            for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
+            for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->coef32[i]);
+            for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->coef32[i]);
             cudaEventRecord(ev[0], h->stream);
             fft_kernel(KF_ZINV, h->Nzp, true)<<<gz, 256, smz, h->stream>>>(f);
             cudaEventRecord(ev[1], h->stream);
@@ -797,7 +804,9 @@ static int set_attrs(cf_engine* h) {
         if ((rc = raise_smem_limit(fft_kernel(KF_ZINV, h->Nzp, true), need[1] / 2))) return rc;
         if ((rc = raise_smem_limit(fft_kernel(KF_ZFWD, h->Nzp, true), need[1] / 2))) return rc;
         if ((rc = raise_smem_limit(fft_kernel(KF_XPASS, h->Nxp, true), need[2] / 2))) return rc;
-        if ((rc = raise_smem_limit(k_cheb_mma, cheb_smem(h->chebNP)))) return rc;
+        int NPs, nsplit, NPt;
+        cheb_dims(h->Ny, NPs, nsplit, NPt);
+        if ((rc = raise_smem_limit(k_cheb_mma, cheb_smem(NPs)))) return rc;
     }
     return CF_OK;
 }
@@ -908,6 +917,7 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
         for (int i = 0; i < 6; ++i) {
             if ((rc = dalloc(h, &h->nod32[i], sizeof(zf) * h->nr))) return bail(rc);
             if ((rc = dalloc(h, &h->zp32[i], sizeof(zf) * h->nq))) return bail(rc);
+            if ((rc = dalloc(h, &h->coef32[i], sizeof(zf) * h->nr))) return bail(rc);
         }
         std::vector<float> fhi, flo, ihi, ilo;
         cheb_images(h->Ny, 0, 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1)), fhi, flo, h->chebNP, h->chebKT);
@@ -1560,10 +1570,19 @@ static float host_tf32(float x) {
 //   inverse:  y_n = sum_k a_k cos(pi n k / P)                 (ffts.jl:282-287)
 //   forward:  a_k = scale e_k sum_n w_n x_n cos(pi n k / P)   (ffts.jl:189-206,
 //             e_k = 1/2 at k = 0, P; w_n = 1 at n = 0, P, else 2)
+// Output rows per block: all of them (rounded up to 16) when at most 256,
+// else split over two blocks so that each holds <= 256 TMEM columns.
+static void cheb_dims(int Ny, int& NPs, int& nsplit, int& NP) {
+    const int n16 = (Ny + 15) & ~15;
+    nsplit = n16 <= 256 ? 1 : 2;
+    NPs = nsplit == 1 ? n16 : (((n16 + 1) / 2 + 15) & ~15);
+    NP = nsplit * NPs;
+}
 static void cheb_images(int Ny, int inverse, double scale, std::vector<float>& hi, std::vector<float>& lo, int& NP,
                         int& nkt) {
     const int P = Ny - 1;
-    NP = (Ny + 15) & ~15;
+    int NPs, nsplit;
+    cheb_dims(Ny, NPs, nsplit, NP);
     nkt = (Ny + CF_CHEB_KT - 1) / CF_CHEB_KT;
     hi.assign((size_t)nkt * NP * CF_CHEB_KT, 0.0f);
     lo.assign(hi.size(), 0.0f);
@@ -1592,14 +1611,14 @@ static void cheb_images(int Ny, int inverse, double scale, std::vector<float>& h
 // shared memory, padded so that the blocks that fit on an SM (228 KB, 1 KB
 // reserved per block) also fit in its 512 TMEM columns, so no block ever waits
 // in the TMEM allocation.
-static int cheb_stages(int NP) {
-    const size_t stage = (size_t)2 * CF_CHEB_MT * CF_CHEB_KT * 4 + (size_t)2 * NP * CF_CHEB_KT * 4;
+static int cheb_stages(int NPs) {
+    const size_t stage = (size_t)2 * CF_CHEB_MT * CF_CHEB_KT * 4 + (size_t)2 * NPs * CF_CHEB_KT * 4;
     return 2 * stage + 64 <= (size_t)220 * 1024 ? 2 : 1;
 }
-static size_t cheb_smem(int NP) {
-    const size_t stage = (size_t)2 * CF_CHEB_MT * CF_CHEB_KT * 4 + (size_t)2 * NP * CF_CHEB_KT * 4;
-    const size_t tiles = cheb_stages(NP) * stage + 64;
-    const int ncols = NP <= 32 ? 32 : (NP <= 64 ? 64 : (NP <= 128 ? 128 : (NP <= 256 ? 256 : 512)));
+static size_t cheb_smem(int NPs) {
+    const size_t stage = (size_t)2 * CF_CHEB_MT * CF_CHEB_KT * 4 + (size_t)2 * NPs * CF_CHEB_KT * 4;
+    const size_t tiles = cheb_stages(NPs) * stage + 64;
+    const int ncols = NPs <= 32 ? 32 : (NPs <= 64 ? 64 : (NPs <= 128 ? 128 : 256));
     const size_t per_sm = 233472, maxb = 512 / ncols;
     const size_t floor_b = per_sm / (maxb + 1) - 1024 + 16;  // maxb + 1 blocks no longer fit
     return std::max(tiles, floor_b);
@@ -1635,13 +1654,16 @@ int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int
             rc = fail(CF_E_CUDA, "upload failed");
             break;
         }
-        if ((rc = raise_smem_limit(k_cheb_mma, cheb_smem(NP)))) break;
+        int NPs, nsplit, NPt;
+        cheb_dims(Ny, NPs, nsplit, NPt);
+        if ((rc = raise_smem_limit(k_cheb_mma, cheb_smem(NPs)))) break;
         ChebParams p;
         std::memset(&p, 0, sizeof(p));
         p.Ny = Ny;
         p.NP = NP;
         p.nkt = nkt;
-        p.nst = cheb_stages(NP);
+        p.NPs = NPs;
+        p.nst = cheb_stages(NPs);
         p.C = C;
         for (int f = 0; f < nfields; ++f) {
             p.X[f] = dX + (size_t)f * Ny * C;
@@ -1650,8 +1672,8 @@ int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int
         p.Bhi = dB;
         p.Blo = dB + hi.size();
         p.err = derr;
-        dim3 grid((unsigned)((C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nfields);
-        k_cheb_mma<<<grid, 128, cheb_smem(NP)>>>(p);
+        dim3 grid((unsigned)((C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nfields, (unsigned)nsplit);
+        k_cheb_mma<<<grid, 128, cheb_smem(NPs)>>>(p);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) {

@@ -73,7 +73,7 @@ def test_mixed_poiseuille_flux_matches_fp64_engine():
     mx.close()
 
 
-@pytest.mark.parametrize("dims", [(9, 17, 7), (16, 17, 16), (48, 33, 40)])
+@pytest.mark.parametrize("dims", [(9, 17, 7), (16, 17, 16), (48, 33, 40), (8, 257, 6)])
 def test_mixed_one_step_sizes(dims):
     Nx, Ny, Nz = dims
     g = cfb200.Grid(Nx, Ny, Nz, 5.3, 7.1)
