@@ -574,7 +574,9 @@ def main():
     roofline = {"bound": "hbm", "kernel": {"zinv": "k_zinv", "xpass": "k_xpass", "zfwd": "k_zfwd",
                                            "column": "k_column_stage"}[dom],
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "traffic": traffic_from_profiles(dom, args.config),
+                "peak_source": peak_kind,
+                "traffic": traffic_from_profiles({"zinv": "k_zinv", "xpass": "k_xpass", "zfwd": "k_zfwd",
+                                                  "column": "k_column_stage"}[dom], args.config),
                 "algorithmic_bytes_per_launch": mb[dom],
                 "kernel_ms_per_launch": kavg,
                 "step_model_bytes": 3 * sum(mb.values()),

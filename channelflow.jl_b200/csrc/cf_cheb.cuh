@@ -159,7 +159,8 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
 #pragma unroll
     for (int r = 0; r < CF_CHEB_KT; ++r) xc[r] = (cin && r < p.Ny) ? __ldg(X + (long)r * p.C + cm) : 0.0f;
     constexpr int BQ = 5;  // float4 of one image part per thread (NPs * 4 <= 5 * 128 for NPs <= 160)
-    for (int kt = 0; kt < p.nkt && ok; ++kt) {
+    int done = p.nkt;  // K-tiles whose MMAs were committed
+    for (int kt = 0; kt < p.nkt; ++kt) {
         const int st = kt % nst;
         float* Ahi = reinterpret_cast<float*>(csm + st * sb);
         float* Alo = Ahi + CF_CHEB_MT * CF_CHEB_KT;
@@ -194,7 +195,6 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
         if (kt >= nst) {
             ok = mbar_wait(smem_u32(mbar + st), (uint32_t)(((kt - nst) / nst) & 1));
             tc_fence_after();
-            if (!ok) break;
         }
         // A: column cm, rows k0 + 4j .. 4j+3 form one 16-byte core-matrix row
 #pragma unroll
@@ -225,7 +225,12 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
             }
         }
         fence_async_smem();
-        __syncthreads();
+        // every thread stops here together if any wait gave up
+        if (!__syncthreads_and(ok)) {
+            ok = false;
+            done = kt;
+            break;
+        }
         if (tid == 0) {
             tc_fence_after();
             const int ksteps = min(CF_CHEB_KT, p.Ny - k0 + 7) / 8;  // 8-degree steps holding data
@@ -251,12 +256,13 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
 #pragma unroll
         for (int r = 0; r < CF_CHEB_KT; ++r) xc[r] = xn[r];
     }
-    // drain: the last commit of every stage in use
-    for (int kt = max(0, p.nkt - nst); kt < p.nkt && ok; ++kt) {
-        ok = mbar_wait(smem_u32(mbar + (kt % nst)), (uint32_t)((kt / nst) & 1));
+    // drain: the last commit of every stage in use (also after a failed wait,
+    // so no MMA is left running when TMEM is freed; all waits bounded)
+    for (int kt = max(0, done - nst); kt < done; ++kt) {
+        ok = mbar_wait(smem_u32(mbar + (kt % nst)), (uint32_t)((kt / nst) & 1)) && ok;
         tc_fence_after();
     }
-    __syncthreads();
+    ok = __syncthreads_and(ok) != 0;
     if (!ok) {
         if (lane == 0) atomicExch(p.err, 1);
     } else {

