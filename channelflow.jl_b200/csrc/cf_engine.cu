@@ -253,6 +253,7 @@ struct cf_engine {
     float *d_chebF = nullptr, *d_chebI = nullptr;  // [heads | remainders]
     int chebNP = 0, chebKT = 0;
     int* d_cheberr = nullptr;
+    double* d_diag = nullptr;  // diagnostics accumulators
     cudaGraphExec_t graph = nullptr;
     int last_launches = 0;
     std::vector<void*> allocs;
@@ -1173,73 +1174,38 @@ int cf_random_state(cf_handle* h, unsigned long long seed, double amp, int shape
     return CF_OK;
 }
 
+typedef void (*DiagKernel)(ColParams, double*);
+static DiagKernel diag_kernel(int P) {
+    switch (P) {
+#define CF_CASE(N) \
+    case N: return k_column_diag<CF_NCOL, N>;
+        CF_COL_LENGTHS(CF_CASE)
+#undef CF_CASE
+        default: return k_column_diag<CF_NCOL, 0>;
+    }
+}
+
+// Diagnostics on the device: one column team per Fourier column (see
+// k_column_diag); five doubles come back to the host.
 int cf_diagnostics(cf_handle* h, double* out) {
     if (!h || !out) return fail(CF_E_ARG, "null argument");
-    std::vector<std::complex<double>> U((size_t)3 * h->nr);
-    int rc = cf_get_state(h, reinterpret_cast<double*>(U.data()), nullptr);
-    if (rc) return rc;
-    const int Ny = h->Ny, P = h->P;
-    const long S = h->B;
-    auto moment = [](int n) { return (n % 2 == 0) ? 1.0 / (1.0 - (double)n * n) : 0.0; };
-    std::vector<double> M((size_t)Ny * Ny);
-    for (int m = 0; m < Ny; ++m)
-        for (int n = 0; n < Ny; ++n) M[(size_t)m * Ny + n] = (moment(m + n) + moment(std::abs(m - n))) / 2;
-    auto nyq = [&](int ix, int iz) { return ((h->Nx % 2 == 0) && ix == h->Nx / 2) || ((h->Nz % 2 == 0) && iz == h->Nz / 2); };
-    auto dotc = [&](const std::complex<double>* a, const std::complex<double>* b) {
-        double r = 0;
-        std::vector<std::complex<double>> w(Ny);
-        for (long c = 0; c < S; ++c) {
-            int ix = c % h->Nxh, iz = c / h->Nxh;
-            if (nyq(ix, iz)) continue;
-            std::complex<double> d = 0;
-            for (int m = 0; m < Ny; ++m) {
-                std::complex<double> s = 0;
-                for (int n = 0; n < Ny; ++n) s += M[(size_t)m * Ny + n] * b[c + n * S];
-                d += std::conj(a[c + m * S]) * s;
-            }
-            r += (ix == 0 ? 1.0 : 2.0) * d.real();
-        }
-        return r;
-    };
-    const std::complex<double>* u[3] = {U.data(), U.data() + h->nr, U.data() + 2 * h->nr};
-    double e = 0;
-    for (int i = 0; i < 3; ++i) e += dotc(u[i], u[i]);
-    // curl and divergence on the host (diagnostic only)
-    std::vector<std::complex<double>> om((size_t)3 * h->nr), dv(h->nr);
-    std::vector<std::complex<double>> col(Ny), dcol(Ny);
-    const std::complex<double> I(0, 1);
-    double mxdiv = 0;
-    for (long c = 0; c < S; ++c) {
-        int ix = c % h->Nxh, iz = c / h->Nxh;
-        double k = kx_of(h, ix), l = lz_of(h, iz);
-        std::vector<double> re(Ny), im(Ny), dre(Ny), dim(Ny);
-        auto dy = [&](const std::complex<double>* f, std::complex<double>* out) {
-            for (int n = 0; n < Ny; ++n) { re[n] = f[c + n * S].real(); im[n] = f[c + n * S].imag(); }
-            setup::diff(re.data(), dre.data(), P);
-            setup::diff(im.data(), dim.data(), P);
-            for (int n = 0; n < Ny; ++n) out[n] = std::complex<double>(dre[n], dim[n]);
-        };
-        std::vector<std::complex<double>> dw(Ny), du(Ny), dvv(Ny);
-        dy(u[2], dw.data());
-        dy(u[0], du.data());
-        dy(u[1], dvv.data());
-        for (int n = 0; n < Ny; ++n) {
-            om[c + n * S] = dw[n] - I * l * u[1][c + n * S];
-            om[h->nr + c + n * S] = I * (l * u[0][c + n * S] - k * u[2][c + n * S]);
-            om[2 * h->nr + c + n * S] = I * k * u[1][c + n * S] - du[n];
-            std::complex<double> d = I * k * u[0][c + n * S] + dvv[n] + I * l * u[2][c + n * S];
-            mxdiv = std::max(mxdiv, std::abs(d));
-        }
+    int rc;
+    if (!h->d_diag) {
+        if ((rc = dalloc(h, (void**)&h->d_diag, 8 * sizeof(double)))) return rc;
+        if ((rc = raise_smem_limit(diag_kernel(h->P), col_smem(h)))) return rc;
     }
-    double d = 0;
-    for (int i = 0; i < 3; ++i) d += dotc(om.data() + i * h->nr, om.data() + i * h->nr);
-    std::vector<double> m0(Ny);
-    for (int n = 0; n < Ny; ++n) m0[n] = u[0][n * S].real();
-    out[0] = e / 2;
-    out[1] = h->nu * d;
-    out[2] = mxdiv;
-    out[3] = h->nu * setup::wallderiv(m0.data(), P, true);
-    out[4] = h->nu * setup::wallderiv(m0.data(), P, false);
+    CU(cudaMemsetAsync(h->d_diag, 0, 8 * sizeof(double), h->stream));
+    ColParams p = col_params(h);
+    diag_kernel(h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p, h->d_diag);
+    CU(cudaGetLastError());
+    double acc[5];
+    CU(cudaMemcpyAsync(acc, h->d_diag, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    out[0] = acc[0] / 2;
+    out[1] = h->nu * acc[1];
+    out[2] = acc[2];  // bits of a non-negative double, stored by atomicMax
+    out[3] = h->nu * acc[3];
+    out[4] = h->nu * acc[4];
     return CF_OK;
 }
 

@@ -680,3 +680,93 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     __syncthreads();
     tile_store<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p);
 }
+
+// Diagnostics of the perturbation velocity on the device (postprocessing.jl:
+// 80-95): acc[0] += sum over columns of <u_i, u_i>, acc[1] += <omega_i,
+// omega_i>, acc[2] = max |div u| coefficient (as the bits of a non-negative
+// double, ordered like the value), acc[3], acc[4] = u'(+1), u'(-1) of the
+// (0,0) mode.  <a, b> = sum_{m,n} conj(a_m) b_n M_mn with M_mn = (mom(m+n) +
+// mom(|m-n|))/2, mom(j) = 1/(1-j^2) for even j, 0 for odd j (the Chebyshev
+// inner product on [-1, 1] divided by 2), weighted 1 for kx = 0 and 2
+// otherwise; Nyquist columns are skipped.  M couples degrees of equal parity
+// only, so warp q sums the parity-q part.  Regions: 0-2 u, v, w; 3-5 omega;
+// 6 the moment table (block); 7 D v.
+CF_DEV double diag_form(const zd* a, const double* mom, const Team& t) {
+    const int q = t.q, qo = q * t.hs, nq = pcount(q, t.P);
+    double s = 0.0;
+    for (int j = t.lane; j < nq; j += 32) {
+        const int m = 2 * j + q;
+        zd acc = zzero();
+        for (int i = 0; i < nq; ++i) {
+            const int n = 2 * i + q;
+            const double M = 0.5 * (mom[m + n] + mom[m > n ? m - n : n - m]);
+            acc = zaxpy(acc, M, a[qo + i]);
+        }
+        const zd am = a[qo + j];
+        s += am.x * acc.x + am.y * acc.y;  // Re(conj(a_m) acc)
+    }
+    return warp_sum_d(s);
+}
+
+template <int NCOL, int PL>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_diag(ColParams p,
+                                                                                             double* acc) {
+    extern __shared__ zd smem[];
+    const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
+    const Team& t = X.t;
+    const int cs = X.cs, hs = t.hs, c0 = X.c0, q = t.q, lane = t.lane, P = t.P;
+    const int qo = q * hs, nq = pcount(q, P);
+    tile_load<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p);
+    tile_load<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p);
+    tile_load<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p);
+    double* mom = reinterpret_cast<double*>(X.reg(6));
+    for (int j = threadIdx.x; j <= 2 * P; j += NCOL * CF_TEAM)
+        mom[j] = (j & 1) ? 0.0 : 1.0 / (1.0 - (double)j * j);
+    __syncthreads();
+    if (!X.valid) return;
+    const bool nyq = col_nyquist(p, X.ix, X.iz);
+    const double k = p.ax * X.ix;
+    const double l = p.bz * (X.iz <= (p.Nz >> 1) ? X.iz : X.iz - p.Nz);
+    zd* U0 = X.col(0);
+    zd* U1 = X.col(1);
+    zd* U2 = X.col(2);
+    zd* W0 = X.col(3);
+    zd* W1 = X.col(4);
+    zd* W2 = X.col(5);
+    zd* DV = X.col(7);
+    col_diff(U2, W0, t);
+    col_diff(U0, W2, t);
+    col_diff(U1, DV, t);
+    double dmax = 0.0;
+    for (int j = lane; j < nq; j += 32) {
+        const int o = qo + j;
+        W0[o] = zsub(W0[o], zmulis(U1[o], l));
+        W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
+        W2[o] = zsub(zmulis(U1[o], k), W2[o]);
+        const zd d = zadd(zadd(zmulis(U0[o], k), DV[o]), zmulis(U2[o], l));
+        dmax = fmax(dmax, sqrt(d.x * d.x + d.y * d.y));
+    }
+    tsync(t);
+    if (X.c == 0) {
+        zd wr, wl;
+        col_wallderiv(U0, t, wr, wl);
+        if (t.tid == 0) {
+            acc[3] = wr.x;
+            acc[4] = wl.x;
+        }
+    }
+    for (int m = 16; m >= 1; m >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
+    if (lane == 0) atomicMax(reinterpret_cast<unsigned long long*>(acc + 2), (unsigned long long)__double_as_longlong(dmax));
+    if (nyq) return;
+    const double w = X.ix == 0 ? 1.0 : 2.0;
+    double e = 0.0, dis = 0.0;
+#pragma unroll 1
+    for (int f = 0; f < 3; ++f) {
+        e += diag_form(sel3(U0, U1, U2, f), mom, t);
+        dis += diag_form(sel3(W0, W1, W2, f), mom, t);
+    }
+    if (lane == 0) {
+        atomicAdd(acc + 0, w * e);
+        atomicAdd(acc + 1, w * dis);
+    }
+}

@@ -141,9 +141,11 @@ int cf_pressure(cf_handle* h, const double* U, double* P);
  * project! and pressure (initialization.jl:176-195).  Sets the engine state. */
 int cf_random_state(cf_handle* h, unsigned long long seed, double amp, int shape, double rho);
 
-/* Diagnostics of the engine's perturbation velocity (postprocessing.jl:80-95):
- * out[0] kinetic energy, out[1] dissipation nu<|curl u|^2>, out[2] max |div u|
- * coefficient, out[3] nu du/dy(+1) and out[4] nu du/dy(-1) of the (0,0) mode. */
+/* Diagnostics of the engine's perturbation velocity (postprocessing.jl:80-95),
+ * computed on the device (one column team per Fourier mode; five doubles come
+ * back): out[0] kinetic energy, out[1] dissipation nu<|curl u|^2>, out[2] max
+ * |div u| coefficient, out[3] nu du/dy(+1) and out[4] nu du/dy(-1) of the
+ * (0,0) mode. */
 int cf_diagnostics(cf_handle* h, double* out);
 
 /* step! like cf_step without the CUDA graph, with CUDA events around every

@@ -189,3 +189,20 @@ def test_handles_of_different_grids_coexist():
     cfb200.random_state(small, 0.1, seed=1)
     big.close()
     small.close()
+
+
+@pytest.mark.parametrize("dims,profile", [((16, 17, 16), "couette"), ((9, 17, 7), "couette"),
+                                          ((24, 25, 20), "poiseuille")])
+def test_device_diagnostics_match_oracle(dims, profile):
+    Nx, Ny, Nz = dims
+    kw = {"bulkvelocity": (2 / 3, 0.0)} if profile == "poiseuille" else {}
+    gpu, ref = pair(Nx, Ny, Nz, 5.3, 7.1, 1 / 300, 0.01, profile=profile, **kw)
+    U, P = ref.random_state(seed=21, amp=0.3)
+    gpu.set_state(U, P)
+    dg, do = gpu.diagnostics(), ref.diagnostics(U)
+    for i in (0, 1):  # kinetic energy, dissipation
+        assert abs(dg[i] - do[i]) <= 1e-12 * abs(do[i])
+    assert abs(dg[2] - do[2]) <= 1e-12 + 1e-9 * abs(do[2])  # max |div|
+    for i in (3, 4):  # wall shear of the mean mode
+        assert abs(dg[i] - do[i]) <= 1e-12 * max(1.0, abs(do[i]))
+    gpu.close()
