@@ -37,9 +37,11 @@ class _Config(ctypes.Structure):
                 ("nu", ctypes.c_double), ("dt", ctypes.c_double),
                 ("profile", ctypes.c_int), ("base_values", _D),
                 ("constraint", ctypes.c_int), ("c1", ctypes.c_double), ("c2", ctypes.c_double),
-                ("precision", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("form", ctypes.c_int)]
 
 PRECISIONS = {"fp64": 0, "mixed": 1}
+# NonLinearTerm forms (src/nonlinear.jl:10-17): CF_FORM_* of cfb200.h
+FORMS = {"rotational": 0, "convective": 1, "divergence": 2}
 
 
 EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_get_state",
@@ -47,7 +49,7 @@ EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_g
            "cf_pressure", "cf_random_state", "cf_diagnostics", "cf_sync", "cf_last_launch_count",
            "cf_stream", "cf_last_error", "cf_step_profiled", "cf_nonlinear_noalloc", "cf_create_batch",
            "cf_destroy_batch", "cf_batch_size", "cf_batch_instance", "cf_step_batch",
-           "cf_batch_last_launch_count", "cf_batch_stream", "cf_cheb_transform"]
+           "cf_batch_last_launch_count", "cf_batch_stream", "cf_cheb_transform", "cf_step_dt"]
 
 
 def lib():
@@ -68,6 +70,7 @@ def lib():
         L.cf_set_state_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.cf_get_state_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.cf_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _D, _D]
+        L.cf_step_dt.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D, _D]
         L.cf_nonlinear.argtypes = [ctypes.c_void_p, _D, _D]
         L.cf_nonlinear_noalloc.argtypes = [ctypes.c_void_p, _D, _D]
         L.cf_cheb_transform.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.c_int,
@@ -163,8 +166,9 @@ def _make_config(grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None
         raise ValueError("specify either pressuregradient or bulkvelocity")
     if forcing is not None:
         raise ValueError("only NoForcing is accelerated by the engine")
-    if form not in (None, "rotational"):
-        raise ValueError("only the rotational nonlinear form is accelerated by the engine")
+    form = "rotational" if form is None else form
+    if form not in FORMS:
+        raise ValueError(f"form must be one of {sorted(FORMS)}")
     if bulkvelocity is not None:
         constraint = ("bulkvelocity", tuple(float(v) for v in bulkvelocity))
     else:
@@ -187,14 +191,17 @@ def _make_config(grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
     cfg.precision = PRECISIONS[precision]
+    cfg.form = FORMS[form]
     return cfg, base, constraint
 
 
 class ChannelFlowProblem:
-    """ChannelFlowProblem(grid, profile, nu, dt; pressuregradient | bulkvelocity)
-    (src/problem.jl:69-107) with the rotational form and NoForcing, on the B200.
+    """ChannelFlowProblem(grid, profile, nu, dt; pressuregradient | bulkvelocity,
+    form) (src/problem.jl:69-107) with NoForcing, on the B200.
 
-    ``profile`` is "couette", "poiseuille" or a callable Ub(y).
+    ``profile`` is "couette", "poiseuille" or a callable Ub(y); ``form`` is the
+    nonlinear form, "rotational" (default), "convective" or "divergence"
+    (src/nonlinear.jl:10-17).
     """
 
     def __init__(self, grid, profile, nu, dt, pressuregradient=None, bulkvelocity=None, forcing=None, form=None,
@@ -202,6 +209,7 @@ class ChannelFlowProblem:
         cfg, self._base, self.constraint = _make_config(grid, profile, nu, dt, pressuregradient, bulkvelocity,
                                                         forcing, form, precision)
         self.precision = precision
+        self.form = "rotational" if form is None else form
         self.grid = grid
         self.nu, self.dt = float(nu), float(dt)
         h = ctypes.c_void_p()
@@ -216,6 +224,7 @@ class ChannelFlowProblem:
         self.grid, self.nu, self.dt, self.constraint = grid, float(nu), float(dt), constraint
         self._base = None
         self.precision = "fp64"
+        self.form = "rotational"
         self._h = ctypes.c_void_p(handle)
         self._owned = False
         return self
@@ -253,6 +262,15 @@ class ChannelFlowProblem:
         _check(lib().cf_step(self._h, float(t), int(nsteps), ctypes.byref(tout), _ptr(g)))
         return tout.value, tuple(g)
 
+    def advance_dt(self, t, dt):
+        """One step of duration dt (the Flows adapter's step,
+        ext/ChannelFlowFlowsExt.jl:36-52; factors for a dt other than the
+        nominal one are built on first use and kept); returns (t + dt, gradients)."""
+        tout = ctypes.c_double()
+        g = np.zeros(2)
+        _check(lib().cf_step_dt(self._h, float(t), float(dt), ctypes.byref(tout), _ptr(g)))
+        return tout.value, tuple(g)
+
     def advance_profiled(self, t, nsteps=1):
         """As advance() without the graph; returns (t_out, ms per kernel class
         [z-inverse, x-pass, z-forward, column, forward and inverse tensor-core
@@ -273,7 +291,7 @@ class ChannelFlowProblem:
 
     # ------------------------------------------------ operators
     def nonlinear(self, U):
-        """NonLinearTerm{RotatingForm}(t, U, N) (src/nonlinear.jl:173-193)."""
+        """NonLinearTerm(t, U, N) of the problem's form (src/nonlinear.jl:113-193)."""
         U = np.ascontiguousarray(U, dtype=np.complex128)
         N = np.zeros_like(U)
         _check(lib().cf_nonlinear(self._h, _ptr(U.view(np.float64)), _ptr(N.view(np.float64))))
@@ -379,7 +397,8 @@ def project_(U, problem):
 
 
 def pressure(U, problem):
-    """pressure(U, problem) (src/pressure.jl:95-104): modified pressure for the rotational form."""
+    """pressure(U, problem) (src/pressure.jl:95-104): the modified pressure for
+    the rotational form, the ordinary pressure for the other two."""
     U = np.ascontiguousarray(U, dtype=np.complex128)
     P = np.zeros(problem.grid.spectralsize, np.complex128)
     _check(lib().cf_pressure(problem.handle, _ptr(U.view(np.float64)), _ptr(P.view(np.float64))))
@@ -410,6 +429,37 @@ def step_(problem, U, P, t, nsteps=1):
     U[...] = U2
     P[...] = P2
     return t2
+
+
+def flow(problem):
+    """Flows.flow(problem) (ext/ChannelFlowFlowsExt.jl:28-29): a callable
+    (state, (t0, t1)) -> state advancing a host State in place from t0 to t1
+    with the nominal step and a final step shortened to end on t1 (run with
+    its own factors, cf_step_dt; test/test_timestepping.jl:31-41).  A
+    remainder below 1e-10 of the nominal step is not stepped."""
+
+    def run(state, span):
+        t0, t1 = float(span[0]), float(span[1])
+        if not t1 >= t0:
+            raise ValueError("the interval must not run backwards")
+        if state.U.shape != (3,) + problem.grid.spectralsize or state.P.shape != problem.grid.spectralsize:
+            raise ValueError("the state does not belong to the problem's grid")
+        dt = problem.dt
+        problem.set_state(state.U, state.P)
+        nfull = int(np.floor((t1 - t0) / dt * (1 + 1e-12)))
+        t = t0
+        if nfull:
+            t, _ = problem.advance(t, nfull)
+            t = t0 + nfull * dt
+        rest = t1 - t
+        if rest > 1e-10 * dt:
+            t, _ = problem.advance_dt(t, rest)
+        U, P = problem.get_state()
+        state.U[...] = U
+        state.P[...] = P
+        return state
+
+    return run
 
 
 def kinetic_energy_of(problem):

@@ -5,6 +5,10 @@
 
 #define CF_DEV __device__ __forceinline__
 
+// Nonlinear forms of NonLinearTerm (src/nonlinear.jl:10-17); the values of
+// cf_config.form.
+enum NlForm { NL_ROT = 0, NL_CONV = 1, NL_DIV = 2 };
+
 // ----------------------------------------------------------------- complex
 typedef double2 zd;
 

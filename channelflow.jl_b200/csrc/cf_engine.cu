@@ -29,8 +29,13 @@ static_assert(CF_NCOL == 1 || CF_NCOL == 2, "column teams use named barriers 1 a
 // instantiation (template argument 0).
 typedef void (*ColKernel)(ColParams);
 typedef void (*FftKernel)(FftParams);
-enum { KC_STAGE, KC_PREP, KC_NLOUT, KC_PROJECT, KC_PRESSURE, KC_STAGE_MX, KC_PREP_MX, KC_COUNT };
-enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_COUNT };
+enum {
+    KC_STAGE, KC_PREP, KC_NLOUT, KC_PROJECT, KC_PRESSURE, KC_STAGE_MX, KC_PREP_MX,
+    KC_STAGE_CONV, KC_PREP_CONV, KC_STAGE_DIV, KC_PREP_DIV, KC_DIV, KC_PRESSURE_COEF, KC_COUNT
+};
+enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_XPASS_CONV, KF_XPASS_DIV, KF_COUNT };
+static_assert(CF_FORM_ROTATIONAL == NL_ROT && CF_FORM_CONVECTIVE == NL_CONV && CF_FORM_DIVERGENCE == NL_DIV,
+              "cf_config.form values are the device form tags");
 #define CF_COL_LENGTHS(X) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384)
 
 template <int PT>
@@ -42,6 +47,12 @@ static ColKernel col_kernel_t(int which) {
         case KC_PROJECT: return k_column_project<CF_NCOL, PT>;
         case KC_STAGE_MX: return k_column_stage_mx<CF_NCOL, PT>;
         case KC_PREP_MX: return k_column_prep<CF_NCOL, PT, true>;
+        case KC_STAGE_CONV: return k_column_stage<CF_NCOL, PT, NL_CONV>;
+        case KC_PREP_CONV: return k_column_prep<CF_NCOL, PT, false, NL_CONV>;
+        case KC_STAGE_DIV: return k_column_stage<CF_NCOL, PT, NL_DIV>;
+        case KC_PREP_DIV: return k_column_prep<CF_NCOL, PT, false, NL_DIV>;
+        case KC_DIV: return k_column_div<CF_NCOL, PT>;
+        case KC_PRESSURE_COEF: return k_column_pressure<CF_NCOL, PT, true>;
         default: return k_column_pressure<CF_NCOL, PT>;
     }
 }
@@ -59,6 +70,8 @@ static FftKernel fft_kernel_t(int which, bool f32) {
     switch (which) {
         case KF_ZINV: return f32 ? k_zinv<L, zf> : k_zinv<L, zd>;
         case KF_ZFWD: return f32 ? k_zfwd<L, zf> : k_zfwd<L, zd>;
+        case KF_XPASS_CONV: return k_xpass_conv<L>;
+        case KF_XPASS_DIV: return k_xpass_div<L>;
         default: return f32 ? k_xpass<L, zf> : k_xpass<L, zd>;
     }
 }
@@ -236,13 +249,19 @@ struct cf_engine {
     int tkz;
     // device
     cudaStream_t stream = nullptr;
-    zd *U[3] = {}, *Pf = nullptr, *Q[3] = {}, *nod[6] = {}, *zp[6] = {};
+    int form = NL_ROT;  // nonlinear form (CF_FORM_*)
+    // z-padded work fields: 6 (rotational, divergence) or 9 (convective)
+    zd *U[3] = {}, *Pf = nullptr, *Q[3] = {}, *nod[6] = {}, *zp[9] = {};
     zd *tmpU = nullptr, *tmpP = nullptr;
     double *d_base = nullptr, *d_basecurv = nullptr, *d_grad = nullptr;
     zd *d_twP = nullptr, *d_twZ = nullptr, *d_twX = nullptr, *d_cs = nullptr;
     double* d_helmtab = nullptr;
     FftPlan plP, plZ, plX;
     DevBank bank[3], proj, neum;
+    // factors of a step of another duration (the shortened final step of a
+    // Flows interval): built on first use for tdt, kept for repeated calls
+    DevBank tbank[3];
+    double tdt = 0.0;
     bool nodal_valid = false;
     // mixed-precision form (CF_PRECISION_MIXED): FP32 nodal and z-padded
     // fields, FP32 twiddles, tensor-core Chebyshev transform images
@@ -512,33 +531,66 @@ static FftParams fft_params(const cf_engine* h) {
     f.tks = ilog2(h->tkz);
     f.bsz = zbs(h);
     f.bsx = xbs(h);
+    f.ax = 2 * M_PI / h->Lx; f.bz = 2 * M_PI / h->Lz;
     f.nod0 = h->nod[0]; f.nod1 = h->nod[1]; f.nod2 = h->nod[2]; f.nod3 = h->nod[3]; f.nod4 = h->nod[4]; f.nod5 = h->nod[5];
     f.zp0 = h->zp[0]; f.zp1 = h->zp[1]; f.zp2 = h->zp[2]; f.zp3 = h->zp[3]; f.zp4 = h->zp[4]; f.zp5 = h->zp[5];
+    f.zp6 = h->zp[6]; f.zp7 = h->zp[7]; f.zp8 = h->zp[8];
     f.plZ = h->plZ; f.plX = h->plX;
     return f;
 }
 
-// nonlinear periodic transforms: nodal (6) -> nonlinear term at nodes (nod[0..2])
-static int launch_periodic(cf_engine* h, int* count) {
+// Launch shapes of the periodic transforms of the handle's nonlinear form:
+// fields through the z-inverse and the z-forward, the x-pass kernel and its
+// rows per block.
+struct PeriodicShape {
+    int nzinv, nzfwd, xkind, xrows;
+};
+static PeriodicShape periodic_shape(const cf_engine* h) {
+    if (h->form == NL_CONV) return {9, 3, KF_XPASS_CONV, 1};
+    if (h->form == NL_DIV) return {3, 6, KF_XPASS_DIV, 2};
+    return {6, 3, KF_XPASS, 2};
+}
+static int launch_periodic_kernels(cf_engine* h, cudaEvent_t* ev) {
     FftParams f = fft_params(h);
+    const PeriodicShape s = periodic_shape(h);
     const size_t smz = zsmem(h), smx = xsmem(h);
-    dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
-    fft_kernel(KF_ZINV, h->Nzp)<<<gz, 256, smz, h->stream>>>(f);
-    dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
-    fft_kernel(KF_XPASS, h->Nxp)<<<gx, 256, smx, h->stream>>>(f);
-    dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
-    fft_kernel(KF_ZFWD, h->Nzp)<<<gz3, 256, smz, h->stream>>>(f);
-    if (count) *count += 3;
+    const unsigned gzx = (unsigned)((h->Nxh + h->tkz - 1) / h->tkz);
+    fft_kernel(KF_ZINV, h->Nzp)<<<dim3(gzx, (unsigned)h->Ny, s.nzinv), 256, smz, h->stream>>>(f);
+    if (ev) CU(cudaEventRecord(ev[0], h->stream));
+    const dim3 gx((unsigned)((h->Nzp + s.xrows - 1) / s.xrows), (unsigned)h->Ny);
+    fft_kernel(s.xkind, h->Nxp)<<<gx, 256, smx, h->stream>>>(f);
+    if (ev) CU(cudaEventRecord(ev[1], h->stream));
+    fft_kernel(KF_ZFWD, h->Nzp)<<<dim3(gzx, (unsigned)h->Ny, s.nzfwd), 256, smz, h->stream>>>(f);
     CU(cudaGetLastError());
     return CF_OK;
 }
 
 static unsigned col_blocks(const cf_engine* h) { return (unsigned)((h->B + CF_NCOL - 1) / CF_NCOL); }
 
+// Nonlinear periodic transforms: nodal fields -> the nonlinear term at the
+// nodes (nod[0..2]); for the divergence form the six products at the nodes,
+// then k_column_div: N as coefficients into Nout (nod[0..2] when null).
+static int launch_periodic(cf_engine* h, int* count, zd* const* Nout = nullptr) {
+    int rc = launch_periodic_kernels(h, nullptr);
+    if (rc) return rc;
+    if (count) *count += 3;
+    if (h->form == NL_DIV) {
+        ColParams p = col_params(h);
+        for (int i = 0; i < 3; ++i) p.Nout[i] = Nout ? Nout[i] : h->nod[i];
+        col_kernel(KC_DIV, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+        if (count) *count += 1;
+        CU(cudaGetLastError());
+    }
+    return CF_OK;
+}
+// kernel launches of one CNRK2 step (FP64 forms)
+static int step_launches(const cf_engine* h) { return h->form == NL_DIV ? 15 : 12; }
+
 static int launch_prep(cf_engine* h, zd* const Usrc[3], int* count) {
     ColParams p = col_params(h);
     for (int i = 0; i < 3; ++i) p.U[i] = Usrc[i];
-    col_kernel(KC_PREP, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    const int kc = h->form == NL_CONV ? KC_PREP_CONV : (h->form == NL_DIV ? KC_PREP_DIV : KC_PREP);
+    col_kernel(kc, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return CF_OK;
@@ -555,40 +607,35 @@ static ColParams stage_col_params(const cf_engine* h, int j) {
     p.bank = h->bank[j].view();
     return p;
 }
+static int stage_kernel_kind(const cf_engine* h) {
+    return h->form == NL_CONV ? KC_STAGE_CONV : (h->form == NL_DIV ? KC_STAGE_DIV : KC_STAGE);
+}
 static int launch_stage(cf_engine* h, int j, int* count) {
     int rc = launch_periodic(h, count);
     if (rc) return rc;
     ColParams p = stage_col_params(h, j);
-    col_kernel(KC_STAGE, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    col_kernel(stage_kernel_kind(h), h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return CF_OK;
 }
 
 // Same launches as one step, with events around every kernel class (zinv,
-// xpass, zfwd, column) recorded on the handle's stream.
+// xpass, zfwd, column; the divergence form's k_column_div counts with the
+// column kernel) recorded on the handle's stream.
 static int launch_step_profiled(cf_engine* h, cudaEvent_t* ev, double* acc) {
-    FftParams f = fft_params(h);
-    const size_t smz = zsmem(h), smx = xsmem(h);
-    dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
-    dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
-    dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
     for (int j = 0; j < 3; ++j) {
-        ColParams p = col_params(h);
-        p.lambda = 1.0 / (CC[j] * h->dt);
-        p.weight = CB[j] / CC[j];
-        p.Acoef = CA[j];
-        p.stage = j;
-        p.store_q = (j < 2) ? 1 : 0;
-        p.bank = h->bank[j].view();
+        ColParams p = stage_col_params(h, j);
         CU(cudaEventRecord(ev[0], h->stream));
-        fft_kernel(KF_ZINV, h->Nzp)<<<gz, 256, smz, h->stream>>>(f);
-        CU(cudaEventRecord(ev[1], h->stream));
-        fft_kernel(KF_XPASS, h->Nxp)<<<gx, 256, smx, h->stream>>>(f);
-        CU(cudaEventRecord(ev[2], h->stream));
-        fft_kernel(KF_ZFWD, h->Nzp)<<<gz3, 256, smz, h->stream>>>(f);
+        int rc = launch_periodic_kernels(h, ev + 1);
+        if (rc) return rc;
         CU(cudaEventRecord(ev[3], h->stream));
-        col_kernel(KC_STAGE, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+        if (h->form == NL_DIV) {
+            ColParams pd = col_params(h);
+            for (int i = 0; i < 3; ++i) pd.Nout[i] = h->nod[i];
+            col_kernel(KC_DIV, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(pd);
+        }
+        col_kernel(stage_kernel_kind(h), h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
         CU(cudaEventRecord(ev[4], h->stream));
         CU(cudaGetLastError());
         CU(cudaEventSynchronize(ev[4]));
@@ -801,6 +848,8 @@ static int set_attrs(cf_engine* h) {
     if ((rc = raise_smem_limit(fft_kernel(KF_ZINV, h->Nzp), need[1]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_ZFWD, h->Nzp), need[1]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS, h->Nxp), need[2]))) return rc;
+    if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_CONV, h->Nxp), need[2]))) return rc;
+    if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_DIV, h->Nxp), need[2]))) return rc;
     if (h->mixed) {
         if ((rc = raise_smem_limit(fft_kernel(KF_ZINV, h->Nzp, true), need[1] / 2))) return rc;
         if ((rc = raise_smem_limit(fft_kernel(KF_ZFWD, h->Nzp, true), need[1] / 2))) return rc;
@@ -825,6 +874,11 @@ static int validate_and_size(cf_engine* h, const cf_config* c) {
     if (c->precision == CF_PRECISION_MIXED && c->Ny > 512)
         return fail(CF_E_UNSUPPORTED, "the mixed-precision form supports Ny <= 512");
     h->mixed = c->precision == CF_PRECISION_MIXED;
+    if (c->form != CF_FORM_ROTATIONAL && c->form != CF_FORM_CONVECTIVE && c->form != CF_FORM_DIVERGENCE)
+        return fail(CF_E_ARG, "unknown nonlinear form");
+    if (h->mixed && c->form != CF_FORM_ROTATIONAL)
+        return fail(CF_E_UNSUPPORTED, "the mixed-precision form runs the rotational nonlinear term");
+    h->form = c->form;
     if (!(std::isfinite(c->c1) && std::isfinite(c->c2))) return fail(CF_E_ARG, "mean-flow constraint values must be finite");
     h->Nx = c->Nx; h->Ny = c->Ny; h->Nz = c->Nz; h->Lx = c->Lx; h->Lz = c->Lz;
     h->nu = c->nu; h->dt = c->dt; h->cmode = c->constraint; h->c1 = c->c1; h->c2 = c->c2;
@@ -897,10 +951,10 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
         if ((rc = dalloc(h, (void**)&h->Q[i], fr))) return bail(rc);
     }
     if ((rc = dalloc(h, (void**)&h->Pf, fr))) return bail(rc);
-    for (int i = 0; i < 6; ++i) {
+    for (int i = 0; i < 6; ++i)
         if ((rc = dalloc(h, (void**)&h->nod[i], fr))) return bail(rc);
+    for (int i = 0; i < periodic_shape(h).nzinv || i < 6; ++i)
         if ((rc = dalloc(h, (void**)&h->zp[i], fq))) return bail(rc);
-    }
     if ((rc = dalloc(h, (void**)&h->d_base, 8 * h->Ny))) return bail(rc);
     if ((rc = dalloc(h, (void**)&h->d_basecurv, 8 * h->Ny))) return bail(rc);
     if ((rc = dalloc(h, (void**)&h->d_grad, 8 * 2))) return bail(rc);
@@ -1015,9 +1069,50 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
     }
     if ((rc = build_graph(h))) return rc;
     for (int s = 0; s < nsteps; ++s) CU(cudaGraphLaunch(h->graph, h->stream));
-    cnt += (h->mixed ? 18 : 12) * nsteps;
+    cnt += (h->mixed ? 18 : step_launches(h)) * nsteps;
     h->last_launches = cnt;
     if (t_out) *t_out = t + nsteps * h->dt;
+    if (grads_out && h->mixed && (rc = check_cheb_err(h))) return rc;
+    if (grads_out) {
+        double g[2];
+        CU(cudaMemcpyAsync(g, h->d_grad, 16, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        grads_out[0] = g[0];
+        grads_out[1] = g[1];
+    }
+    return CF_OK;
+}
+
+int cf_step_dt(cf_handle* h, double t, double dt, double* t_out, double* grads_out) {
+    if (!h) return fail(CF_E_ARG, "null handle");
+    if (!(std::isfinite(dt) && dt > 0)) return fail(CF_E_ARG, "dt must be finite and positive");
+    if (dt == h->dt) return cf_step(h, t, 1, t_out, grads_out);
+    int rc, cnt = 0;
+    if (h->tdt != dt) {
+        // the factors may still be read by an earlier step of this kind
+        CU(cudaStreamSynchronize(h->stream));
+        h->tdt = 0.0;
+        for (int j = 0; j < 3; ++j)
+            if ((rc = build_bank(h, h->tbank[j], h->nu, 1.0 / (CC[j] * dt)))) return rc;
+        h->tdt = dt;
+    }
+    if (!h->nodal_valid) {
+        if ((rc = h->mixed ? launch_prep_mx(h, &cnt) : launch_prep(h, h->U, &cnt))) return rc;
+        h->nodal_valid = true;
+    }
+    // the stage launches read dt and the banks from the handle: swap the
+    // temporary ones in for three eager stages (the nominal step's graph holds
+    // its own parameters)
+    std::swap(h->bank, h->tbank);
+    const double dt0 = h->dt;
+    h->dt = dt;
+    rc = CF_OK;
+    for (int j = 0; j < 3 && rc == CF_OK; ++j) rc = h->mixed ? launch_stage_mx(h, j, &cnt) : launch_stage(h, j, &cnt);
+    h->dt = dt0;
+    std::swap(h->bank, h->tbank);
+    if (rc) return rc;
+    h->last_launches = cnt;
+    if (t_out) *t_out = t + dt;
     if (grads_out && h->mixed && (rc = check_cheb_err(h))) return rc;
     if (grads_out) {
         double g[2];
@@ -1038,6 +1133,20 @@ static int ensure_tmp(cf_engine* h) {
     return CF_OK;
 }
 
+// The nonlinear term of the velocity in Us as coefficients, overwriting Us
+// (the velocity is consumed by the preparation kernel first).
+static int launch_nonlinear(cf_engine* h, zd* const Us[3]) {
+    int rc;
+    if ((rc = launch_prep(h, Us, nullptr))) return rc;
+    if (h->form == NL_DIV) return launch_periodic(h, nullptr, Us);
+    if ((rc = launch_periodic(h, nullptr))) return rc;
+    ColParams p = col_params(h);
+    for (int i = 0; i < 3; ++i) p.Nout[i] = Us[i];
+    col_kernel(KC_NLOUT, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    CU(cudaGetLastError());
+    return CF_OK;
+}
+
 int cf_nonlinear(cf_handle* h, const double* U, double* N) {
     if (!h || !U || !N) return fail(CF_E_ARG, "null argument");
     int rc = ensure_tmp(h);
@@ -1045,12 +1154,7 @@ int cf_nonlinear(cf_handle* h, const double* U, double* N) {
     const size_t fr = sizeof(zd) * h->nr;
     CU(cudaMemcpyAsync(h->tmpU, U, 3 * fr, cudaMemcpyHostToDevice, h->stream));
     zd* Us[3] = {h->tmpU, h->tmpU + h->nr, h->tmpU + 2 * h->nr};
-    if ((rc = launch_prep(h, Us, nullptr))) return rc;
-    if ((rc = launch_periodic(h, nullptr))) return rc;
-    ColParams p = col_params(h);
-    for (int i = 0; i < 3; ++i) p.Nout[i] = Us[i];
-    col_kernel(KC_NLOUT, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
-    CU(cudaGetLastError());
+    if ((rc = launch_nonlinear(h, Us))) return rc;
     CU(cudaMemcpyAsync(N, h->tmpU, 3 * fr, cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     h->nodal_valid = false;
@@ -1090,12 +1194,7 @@ int cf_nonlinear_noalloc(cf_handle* h, const double* U, double* N) {
     zd* base = static_cast<zd*>(scr);
     zd* Us[3] = {base, base + h->nr, base + 2 * h->nr};
     CU(cudaMemcpyAsync(base, U, 3 * fr, cudaMemcpyHostToDevice, h->stream));
-    if ((rc = launch_prep(h, Us, nullptr))) return rc;
-    if ((rc = launch_periodic(h, nullptr))) return rc;
-    ColParams p = col_params(h);
-    for (int i = 0; i < 3; ++i) p.Nout[i] = Us[i];
-    col_kernel(KC_NLOUT, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
-    CU(cudaGetLastError());
+    if ((rc = launch_nonlinear(h, Us))) return rc;
     CU(cudaMemcpyAsync(N, base, 3 * fr, cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     h->nodal_valid = false;
@@ -1126,7 +1225,9 @@ static int pressure_dev(cf_engine* h, zd* const Ud[3], zd* Pout) {
     for (int i = 0; i < 3; ++i) p.U[i] = Ud[i];
     p.Pf = Pout;
     p.bank = h->neum.view();
-    col_kernel(KC_PRESSURE, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    // the divergence form's term arrives in nod[0..2] as coefficients
+    col_kernel(h->form == NL_DIV ? KC_PRESSURE_COEF : KC_PRESSURE, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM,
+                                                                          col_smem(h), h->stream>>>(p);
     CU(cudaGetLastError());
     h->nodal_valid = false;
     return CF_OK;
@@ -1223,7 +1324,7 @@ int cf_step_profiled(cf_handle* h, double t, int nsteps, double* t_out, double* 
     for (int s = 0; s < nsteps && rc == CF_OK; ++s) rc = launch_step_profiled(h, ev, kernel_ms);
     for (int k = 0; k < 5; ++k) cudaEventDestroy(ev[k]);
     if (rc) return rc;
-    h->last_launches = cnt + 12 * nsteps;
+    h->last_launches = cnt + step_launches(h) * nsteps;
     if (t_out) *t_out = t + nsteps * h->dt;
     return CF_OK;
 }
@@ -1397,6 +1498,7 @@ int cf_create_batch(const cf_config* cfgs, int n, cf_batch** out) {
         if (rc) return bail(rc);
         b->inst.push_back(h);
         if (h->mixed) return bail(fail(CF_E_UNSUPPORTED, "ensembles run the FP64 plain form"));
+        if (h->form != NL_ROT) return bail(fail(CF_E_UNSUPPORTED, "ensembles run the rotational nonlinear form"));
     }
     for (int i = 0; i < n; ++i) {
         cf_engine* h = b->inst[i];

@@ -1,12 +1,19 @@
-// cf_fftkernels.cuh -- periodic-direction transforms of the rotational
-// nonlinear term (src/ffts.jl:189-206 and 275-290, src/nonlinear.jl:184-191).
+// cf_fftkernels.cuh -- periodic-direction transforms of the nonlinear term
+// (src/ffts.jl:189-206 and 275-290, src/nonlinear.jl:113-191).
 //
 // k_zinv : nodal (Ny,Nz,Nxh) -> z-padded spectrum (copy_to_padded!, Nyquist
 //          filter) -> backward z FFT of length Nzp   (Ny,Nzp,Nxh)
-// k_xpass: backward x c2r of the six rows (pairs packed as one complex FFT),
-//          n = u x omega at the padded points, forward x r2c, x truncation
-// k_zfwd : forward z FFT of the three products, z truncation (copy_from_padded!)
+// k_xpass: backward x c2r of the rows (pairs packed as one complex FFT), the
+//          product of the nonlinear form at the padded points, forward x r2c,
+//          x truncation
+// k_zfwd : forward z FFT of the products, z truncation (copy_from_padded!)
 // Shared-memory transform buffers use the padded positions (fpos) of cf_fft.cuh.
+//
+// Fields per form (NlForm):
+//   rotational  nodal u, omega (6) -> z-padded 0-5 -> n = u x omega (3)
+//   convective  nodal u, du/dy (6) -> z-padded 0-5 and du/dz (6-8, made by
+//               k_zinv) -> n = -(u.grad)u (3; du/dx made by k_xpass)
+//   divergence  nodal u (3) -> z-padded 0-2 -> -u_i u_j (6: 00 01 02 11 12 22)
 #pragma once
 #include "cf_fft.cuh"
 
@@ -15,37 +22,59 @@ struct FftParams {
     int tks;       // log2 of the columns per block in the z kernels
     int bsz, bsx;  // transform buffer strides: fft_bufsz(Nzp) + 1 (odd, padded layout),
                    // round_up(Nxp, 8) (XOR-swizzled layout: 12 buffers of the x-pass)
+    double ax, bz;  // 2 pi / Lx, 2 pi / Lz (derivatives of the convective form)
     // nodal and z-padded fields: complex double (FP64 path) or complex float
     // (FP32 transforms of the mixed-precision path)
     void *nod0, *nod1, *nod2, *nod3, *nod4, *nod5;
-    void *zp0, *zp1, *zp2, *zp3, *zp4, *zp5;
+    void *zp0, *zp1, *zp2, *zp3, *zp4, *zp5, *zp6, *zp7, *zp8;
     FftPlan plZ, plX;
 };
 
-CF_DEV void* sel6(void* a0, void* a1, void* a2, void* a3, void* a4, void* a5, int i) {
-    switch (i) {
-        case 0: return a0;
-        case 1: return a1;
-        case 2: return a2;
-        case 3: return a3;
-        case 4: return a4;
-        default: return a5;
-    }
-}
+// field i of the parameter block without indexing an array at run time
 template <class Z>
 CF_DEV Z* nod_of(const FftParams& p, int i) {
-    return static_cast<Z*>(sel6(p.nod0, p.nod1, p.nod2, p.nod3, p.nod4, p.nod5, i));
+    void* a;
+    switch (i) {
+        case 0: a = p.nod0; break;
+        case 1: a = p.nod1; break;
+        case 2: a = p.nod2; break;
+        case 3: a = p.nod3; break;
+        case 4: a = p.nod4; break;
+        default: a = p.nod5; break;
+    }
+    return static_cast<Z*>(a);
 }
 template <class Z>
 CF_DEV Z* zp_of(const FftParams& p, int i) {
-    return static_cast<Z*>(sel6(p.zp0, p.zp1, p.zp2, p.zp3, p.zp4, p.zp5, i));
+    void* a;
+    switch (i) {
+        case 0: a = p.zp0; break;
+        case 1: a = p.zp1; break;
+        case 2: a = p.zp2; break;
+        case 3: a = p.zp3; break;
+        case 4: a = p.zp4; break;
+        case 5: a = p.zp5; break;
+        case 6: a = p.zp6; break;
+        case 7: a = p.zp7; break;
+        default: a = p.zp8; break;
+    }
+    return static_cast<Z*>(a);
+}
+
+// i s a
+template <class Z>
+CF_DEV Z cmuli(Z a, double s) {
+    return cmake<Z>(-s * a.y, s * a.x);
 }
 
 CF_DEV int zpad_index(int iz, int Nz, int Nzp) { return iz <= (Nz >> 1) ? iz : Nzp - (Nz - iz); }
 
 // grid: (ceil(Nxh/tkz), Ny, nfields); block 256; smem 2*tkz*bsz complex.
 // Column t of the block's tkz columns is transform t (stride bsz, odd, so the
-// column-interleaved staging stores hit distinct bank groups).
+// column-interleaved staging stores hit distinct bank groups).  Fields 6-8
+// (convective form) are d/dz of nodal fields 0-2: i bz l times the nodal
+// values (ddx3!, operators.jl:14-23, applied after the Chebyshev transform,
+// with which it commutes).
 template <int LZ, class Z>
 CF_DEV void zinv_body(const FftParams& p, int bx, int n, int f) {
     extern __shared__ __align__(16) unsigned char fsm_raw[];
@@ -54,7 +83,8 @@ CF_DEV void zinv_body(const FftParams& p, int bx, int n, int f) {
     const int k0 = bx << tks;
     const int Nz = p.Nz, Nzp = LZ ? LZ : p.Nzp, Nxh = p.Nxh, bs = p.bsz;
     Z* bufB = sm + tkz * bs;
-    const Z* src = nod_of<Z>(p, f) + (long)n * Nz * Nxh;
+    const bool dz = f >= 6;
+    const Z* src = nod_of<Z>(p, dz ? f - 6 : f) + (long)n * Nz * Nxh;
     Z* dst = zp_of<Z>(p, f) + (long)n * Nzp * Nxh;
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1, znyq = (Nz % 2 == 0) ? Nz / 2 : -1;
     // zero the padding gap
@@ -70,6 +100,7 @@ CF_DEV void zinv_body(const FftParams& p, int bx, int n, int f) {
             const int e = base + u * 256;
             const int iz = e >> tks, k = k0 + (e & tm);
             v[u] = (e < ntot && k < Nxh && iz != znyq && k != xnyq) ? src[(long)iz * Nxh + k] : czero<Z>();
+            if (dz) v[u] = cmuli(v[u], p.bz * (double)(iz <= (Nz >> 1) ? iz : iz - Nz));
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
@@ -119,44 +150,27 @@ CF_DEV void zfwd_body(const FftParams& p, int bx, int n, int f) {
     }
 }
 
-// grid: (ceil(Nzp/2), Ny); block 256; smem 12*bsx complex (6 slots + scratch).
-// Rows zA = 2*bx and zB = 2*bx+1 of plane n.  Slots 0..5 hold
-// (u0+iu1, u2+iw0, w1+iw2) of row A at 0,2,4 and of row B at 1,3,5.
-template <int LX, class Z>
-CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
-    extern __shared__ __align__(16) unsigned char fsm_raw[];
-    Z* sm = reinterpret_cast<Z*>(fsm_raw);
-    const int zA = 2 * bx, zB = zA + 1;
-    const bool hasB = zB < p.Nzp;
-    const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsx;
-    const int Nxhp = Nxp / 2 + 1;
-    const long rowA = ((long)n * p.Nzp + zA) * Nxh;
-    const long rowB = ((long)n * p.Nzp + zB) * Nxh;
-    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
-    Z* scr = sm + 6 * bs;
-    // pack Hermitian pairs: Z_k = X_k + i Y_k, Z_{Nxp-k} = conj(X_k) + i conj(Y_k);
-    // every position 0..Nxp-1 of the six slots is written (zeros for a missing
-    // row B and for k >= Nxh)
-    for (int base = threadIdx.x; base < 6 * Nxhp; base += 4 * 256) {
+// Pack nslots transform slots from pairs of real rows given by their half
+// spectra X, Y (get(slot, k, X, Y) for k < Nxh, Nyquist excluded; zero
+// elsewhere): Z_k = X_k + i Y_k, Z_{Nxp-k} = conj(X_k) + i conj(Y_k).  Every
+// position 0..Nxp-1 of the slots is written.  Block of 256 threads.
+template <class Z, class Get>
+CF_DEV void xpack(Z* sm, int bs, int nslots, int Nxh, int Nxp, int xnyq, const Get& get) {
+    const int Nxhp = Nxp / 2 + 1, tot = nslots * Nxhp;
+    for (int base = threadIdx.x; base < tot; base += 4 * 256) {
         Z X[4], Y[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int e = base + u * 256;
             const int slot = e / Nxhp, k = e - slot * Nxhp;
-            const int pair = slot >> 1;
-            const bool isB = slot & 1;
-            const long row = isB ? rowB : rowA;
             X[u] = czero<Z>();
             Y[u] = czero<Z>();
-            if (e < 6 * Nxhp && !(isB && !hasB) && k < Nxh && k != xnyq) {
-                X[u] = zp_of<Z>(p, 2 * pair)[row + k];
-                Y[u] = zp_of<Z>(p, 2 * pair + 1)[row + k];
-            }
+            if (e < tot && k < Nxh && k != xnyq) get(slot, k, X[u], Y[u]);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int e = base + u * 256;
-            if (e >= 6 * Nxhp) continue;
+            if (e >= tot) continue;
             const int slot = e / Nxhp, k = e - slot * Nxhp;
             Z* s = sm + slot * bs;
             if (k == 0) {
@@ -169,6 +183,45 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
             }
         }
     }
+}
+
+// Separate nslots forward-transformed slots into the half spectra of their
+// two real rows, X = (Z_k + conj Z_-k)/2, Y = (Z_k - conj Z_-k)/(2i), and
+// hand them to put(slot, k, X, Y) for k < Nxh (the x truncation).
+template <class Z, class Put>
+CF_DEV void xunpack(const Z* F, int bs, int nslots, int Nxh, int Nxp, const Put& put) {
+    for (int e = threadIdx.x; e < nslots * Nxh; e += blockDim.x) {
+        const int slot = e / Nxh, k = e - slot * Nxh;
+        const Z* s = F + slot * bs;
+        Z Zk = s[swz(k)], Zm = s[swz((Nxp - k) % Nxp)];
+        put(slot, k, cmake<Z>(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y)),
+            cmake<Z>(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x)));
+    }
+}
+
+// Rotational form.  grid: (ceil(Nzp/2), Ny); block 256; smem 12*bsx complex
+// (6 slots + scratch).  Rows zA = 2*bx and zB = 2*bx+1 of plane n.  Slots
+// 0..5 hold (u0+iu1, u2+iw0, w1+iw2) of row A at 0,2,4 and of row B at 1,3,5.
+template <int LX, class Z>
+CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
+    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    Z* sm = reinterpret_cast<Z*>(fsm_raw);
+    const int zA = 2 * bx, zB = zA + 1;
+    const bool hasB = zB < p.Nzp;
+    const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsx;
+    const long rowA = ((long)n * p.Nzp + zA) * Nxh;
+    const long rowB = ((long)n * p.Nzp + zB) * Nxh;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
+    Z* scr = sm + 6 * bs;
+    // zeros for a missing row B
+    xpack(sm, bs, 6, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+        const int pair = slot >> 1;
+        const bool isB = slot & 1;
+        if (isB && !hasB) return;
+        const long row = isB ? rowB : rowA;
+        X = zp_of<Z>(p, 2 * pair)[row + k];
+        Y = zp_of<Z>(p, 2 * pair + 1)[row + k];
+    });
     __syncthreads();
     Z* A = group_fft_L<true, LX, 1>(sm, scr, 6, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
     Z* Bf = (A == sm) ? scr : sm;
@@ -190,14 +243,7 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
     }
     __syncthreads();
     const Z* F = group_fft_L<true, LX, 1>(Bf, A, 3, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    // separate the packed real transforms and keep k < Nxh
-    for (int e = threadIdx.x; e < 3 * Nxh; e += blockDim.x) {
-        const int slot = e / Nxh, k = e - slot * Nxh;
-        const Z* s = F + slot * bs;
-        Z Zk = s[swz(k)], Zm = s[swz((Nxp - k) % Nxp)];
-        // X = (Z_k + conj Z_-k)/2 ; Y = (Z_k - conj Z_-k)/(2i)
-        Z X = cmake<Z>(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y));
-        Z Y = cmake<Z>(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x));
+    xunpack(F, bs, 3, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
         if (slot == 0) {
             zp_of<Z>(p, 0)[rowA + k] = X;
             zp_of<Z>(p, 1)[rowA + k] = Y;
@@ -210,7 +256,104 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
             zp_of<Z>(p, 2)[rowA + k] = X;
             if (hasB) zp_of<Z>(p, 2)[rowB + k] = Y;
         }
+    });
+}
+
+// Convective form (nonlinear.jl:113-140, dot! operators.jl:247-254).  grid:
+// (Nzp, Ny); block 256; smem 12*bsx complex.  One row z = bx of plane n, twelve
+// real rows packed in six slots: field codes 0-2 u (z-padded 0-2), 3-5 du/dx
+// (i ax k times fields 0-2, ddx1!), 6-8 du/dy (z-padded 3-5), 9-11 du/dz
+// (z-padded 6-8); slot s holds codes 2s, 2s+1.  Product n_i = -(u0 du_i/dx +
+// u1 du_i/dy + u2 du_i/dz) (the sign of _store_rhs!, nonlinear.jl:139), in
+// slots (n0 + i n1, n2), written to z-padded 0-2.
+template <int LX, class Z>
+CF_DEV void xpass_conv_body(const FftParams& p, int z, int n) {
+    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    Z* sm = reinterpret_cast<Z*>(fsm_raw);
+    const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsx;
+    const long row = ((long)n * p.Nzp + z) * Nxh;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
+    Z* scr = sm + 6 * bs;
+    auto fetch = [&](int code, int k) -> Z {
+        if (code < 3) return zp_of<Z>(p, code)[row + k];
+        if (code < 6) return cmuli(zp_of<Z>(p, code - 3)[row + k], p.ax * k);
+        return zp_of<Z>(p, code - 3)[row + k];
+    };
+    xpack(sm, bs, 6, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+        X = fetch(2 * slot, k);
+        Y = fetch(2 * slot + 1, k);
+    });
+    __syncthreads();
+    Z* A = group_fft_L<true, LX, 1>(sm, scr, 6, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
+    Z* Bf = (A == sm) ? scr : sm;
+    for (int j = threadIdx.x; j < Nxp; j += blockDim.x) {
+        const int sj = swz(j);
+        const Z s0 = A[0 * bs + sj], s1 = A[1 * bs + sj], s2 = A[2 * bs + sj];
+        const Z s3 = A[3 * bs + sj], s4 = A[4 * bs + sj], s5 = A[5 * bs + sj];
+        const double u0 = s0.x, u1 = s0.y, u2 = s1.x;
+        const double gx0 = s1.y, gx1 = s2.x, gx2 = s2.y;
+        const double gy0 = s3.x, gy1 = s3.y, gy2 = s4.x;
+        const double gz0 = s4.y, gz1 = s5.x, gz2 = s5.y;
+        const double n0 = -(u0 * gx0 + u1 * gy0 + u2 * gz0);
+        const double n1 = -(u0 * gx1 + u1 * gy1 + u2 * gz1);
+        const double n2 = -(u0 * gx2 + u1 * gy2 + u2 * gz2);
+        Bf[0 * bs + sj] = cmake<Z>(n0, n1);
+        Bf[1 * bs + sj] = cmake<Z>(n2, 0.0);
     }
+    __syncthreads();
+    const Z* F = group_fft_L<true, LX, 1>(Bf, A, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
+    xunpack(F, bs, 2, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+        if (slot == 0) {
+            zp_of<Z>(p, 0)[row + k] = X;
+            zp_of<Z>(p, 1)[row + k] = Y;
+        } else {
+            zp_of<Z>(p, 2)[row + k] = X;
+        }
+    });
+}
+
+// Divergence form (nonlinear.jl:146-167, outer! operators.jl:227-234).  grid:
+// (ceil(Nzp/2), Ny); block 256; smem 12*bsx complex.  Rows zA = 2*bx, zB =
+// 2*bx+1 of plane n; slot f holds (u_f row A) + i (u_f row B).  The six
+// distinct products (u_i u_j = u_j u_i exactly) are negated (the sign of
+// _store_rhs!, nonlinear.jl:166, moved ahead of the linear transforms and
+// div!) into slots m = 00 01 02 11 12 22 and written to z-padded 0-5.
+template <int LX, class Z>
+CF_DEV void xpass_div_body(const FftParams& p, int bx, int n) {
+    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    Z* sm = reinterpret_cast<Z*>(fsm_raw);
+    const int zA = 2 * bx, zB = zA + 1;
+    const bool hasB = zB < p.Nzp;
+    const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsx;
+    const long rowA = ((long)n * p.Nzp + zA) * Nxh;
+    const long rowB = ((long)n * p.Nzp + zB) * Nxh;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
+    Z* scr = sm + 6 * bs;
+    xpack(sm, bs, 3, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+        const Z* src = zp_of<Z>(p, slot);
+        X = src[rowA + k];
+        if (hasB) Y = src[rowB + k];
+    });
+    __syncthreads();
+    Z* A = group_fft_L<true, LX, 1>(sm, scr, 3, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
+    Z* Bf = (A == sm) ? scr : sm;
+    for (int j = threadIdx.x; j < Nxp; j += blockDim.x) {
+        const int sj = swz(j);
+        const Z a0 = A[0 * bs + sj], a1 = A[1 * bs + sj], a2 = A[2 * bs + sj];
+        Bf[0 * bs + sj] = cmake<Z>(-(a0.x * a0.x), -(a0.y * a0.y));
+        Bf[1 * bs + sj] = cmake<Z>(-(a0.x * a1.x), -(a0.y * a1.y));
+        Bf[2 * bs + sj] = cmake<Z>(-(a0.x * a2.x), -(a0.y * a2.y));
+        Bf[3 * bs + sj] = cmake<Z>(-(a1.x * a1.x), -(a1.y * a1.y));
+        Bf[4 * bs + sj] = cmake<Z>(-(a1.x * a2.x), -(a1.y * a2.y));
+        Bf[5 * bs + sj] = cmake<Z>(-(a2.x * a2.x), -(a2.y * a2.y));
+    }
+    __syncthreads();
+    const Z* F = group_fft_L<true, LX, 1>(Bf, A, 6, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
+    xunpack(F, bs, 6, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+        Z* dst = zp_of<Z>(p, slot);
+        dst[rowA + k] = X;
+        if (hasB) dst[rowB + k] = Y;
+    });
 }
 
 // Single-instance kernels and their batched forms (one launch per size class;
@@ -226,6 +369,14 @@ __global__ void __launch_bounds__(256) k_zfwd(FftParams p) {
 template <int LX, class Z = zd>
 __global__ void __launch_bounds__(256) k_xpass(FftParams p) {
     xpass_body<LX, Z>(p, blockIdx.x, blockIdx.y);
+}
+template <int LX>
+__global__ void __launch_bounds__(256) k_xpass_conv(FftParams p) {
+    xpass_conv_body<LX, zd>(p, blockIdx.x, blockIdx.y);
+}
+template <int LX>
+__global__ void __launch_bounds__(256) k_xpass_div(FftParams p) {
+    xpass_div_body<LX, zd>(p, blockIdx.x, blockIdx.y);
 }
 // grid z = 6 * instances
 template <int LZ>

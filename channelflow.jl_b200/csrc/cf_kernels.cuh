@@ -7,6 +7,9 @@
 //   k_column  forward DCT of n, Q update, RHS, Stokes solve (influence and tau
 //             corrections, mean mode, flux constraint), curl and inverse DCT
 //             of the new velocity and vorticity for the next stage.
+// (rotational form; the convective form sends u and du/dy to the nodes and the
+// divergence form u alone, and the latter's products pass through
+// k_column_div, which returns N as coefficients, before k_column.)
 // Field storage: complex (Ny, Nz, Nxh), k fastest; z-padded (Ny, Nzp, Nxh).
 //
 // Column kernels: a block holds NCOL columns, one team of two warps each
@@ -306,12 +309,17 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
     }
 }
 
-// curl of the total velocity and inverse DCT of all six fields to the nodal
-// buffers (nonlinear.jl:179-185, operators.jl:380-398).  u, v, w in U0, U1, U2
-// (modified); W0, W1, W2 receive the vorticity; Z, Z2 are transform buffers.
-// MX (mixed precision): the six fields stay coefficients (the tensor-core
-// transform takes them to the nodes).
-template <int PL, bool MX = false>
+// Total velocity (the base profile added to mode (0,0) of u) and the fields
+// the nonlinear form needs at the nodes, inverse DCT to the nodal buffers.
+// u, v, w in U0, U1, U2 (modified); Z, Z2 are transform buffers.
+//   NL_ROT  W0, W1, W2 receive the vorticity (nonlinear.jl:179-185,
+//           operators.jl:380-398); six nodal fields
+//   NL_CONV W0, W1, W2 receive du_i/dy (grad!, operators.jl:206-214; the x and
+//           z derivatives are formed by the periodic transforms); six fields
+//   NL_DIV  u, v, w alone (nonlinear.jl:153-156); three fields
+// MX (mixed precision, rotational form): the six fields stay coefficients
+// (the tensor-core transform takes them to the nodes).
+template <int PL, bool MX = false, int FORM = NL_ROT>
 CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z, zd* Z2, const ColParams& p, int c,
                            int ix, int iz, const Team& t) {
     const int q = t.q, lane = t.lane, qo = q * t.hs, nq = pcount(q, t.P);
@@ -321,18 +329,24 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
         for (int j = lane; j < nq; j += 32) U0[qo + j] = zadd(U0[qo + j], zmake(__ldg(p.base + 2 * j + q), 0.0));
         tsync(t);
     }
-    col_diff(U2, W0, t);  // omega_x = D w - i l v
-    col_diff(U0, W2, t);  // omega_z = i k v - D u
-    for (int j = lane; j < nq; j += 32) {
-        const int o = qo + j;
-        W0[o] = zsub(W0[o], zmulis(U1[o], l));
-        W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
-        W2[o] = zsub(zmulis(U1[o], k), W2[o]);
-    }
-    tsync(t);
-    if (MX) return;
+    if (FORM == NL_ROT) {
+        col_diff(U2, W0, t);  // omega_x = D w - i l v
+        col_diff(U0, W2, t);  // omega_z = i k v - D u
+        for (int j = lane; j < nq; j += 32) {
+            const int o = qo + j;
+            W0[o] = zsub(W0[o], zmulis(U1[o], l));
+            W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
+            W2[o] = zsub(zmulis(U1[o], k), W2[o]);
+        }
+        tsync(t);
+    } else if (FORM == NL_CONV) {
 #pragma unroll 1
-    for (int i = 0; i < 6; ++i) {
+        for (int i = 0; i < 3; ++i) col_diff(sel3(U0, U1, U2, i), sel3(W0, W1, W2, i), t);
+    }
+    if (MX) return;
+    constexpr int NF = FORM == NL_DIV ? 3 : 6;
+#pragma unroll 1
+    for (int i = 0; i < NF; ++i) {
         zd* x = i < 3 ? sel3(U0, U1, U2, i) : sel3(W0, W1, W2, i - 3);
         col_inverse_y<PL>(x, Z, Z2, p, t);
     }
@@ -354,12 +368,23 @@ CF_DEV void store_six(const Ctx& X, const ColParams& p, int r0, int r1, int r2, 
     }
 }
 
+// the three nodal fields u, v, w from regions r0..r2 to p.nod (divergence form)
+template <int NCOL, class Ctx>
+CF_DEV void store_three(const Ctx& X, const ColParams& p, int r0, int r1, int r2) {
+    tile_store<NCOL>(X.reg(r0), X.cs, X.t.hs, p.nod[0], X.c0, p);
+    tile_store<NCOL>(X.reg(r1), X.cs, X.t.hs, p.nod[1], X.c0, p);
+    tile_store<NCOL>(X.reg(r2), X.cs, X.t.hs, p.nod[2], X.c0, p);
+}
+
 // MX: mixed-precision form.  The nonlinear term arrives as FP32 Chebyshev
 // coefficients (normalised by the tensor-core transform; p.Nn holds zf
 // arrays) and the new velocity and vorticity leave as FP32 coefficients in
 // p.nod; the arithmetic of the stage stays FP64.
-template <int NCOL, int PL, bool MX = false>
+// FORM: the nonlinear form; the divergence form's term arrives as FP64
+// coefficients (from k_column_div), the others' at the nodes.
+template <int NCOL, int PL, bool MX = false, int FORM = NL_ROT>
 CF_DEV void column_stage_body(const ColParams& p, int bx) {
+    constexpr bool NCOEF = MX || FORM == NL_DIV;  // N arrives as coefficients
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, bx);
     const Team& t = X.t;
@@ -406,7 +431,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         if (p.stage > 0) tile_load<NCOL>(X.reg(5), cs, hs, Q_i, c0, p);
         __syncthreads();
         if (valid) {
-            if (!MX) {
+            if (!NCOEF) {
                 col_forward_y<PL>(X.col(4), X.col(6), X.col(7), p, nyq, t);
             } else if (nyq) {
                 col_zero(X.col(4), t);
@@ -502,15 +527,16 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     __syncthreads();
     // ---------------- Phase C: total velocity, vorticity, nodal values
     if (valid)
-        col_prep_nodal<PL, MX>(X.col(0), X.col(4), X.col(2), X.col(1), X.col(3), X.col(5), X.col(6), X.col(7), p, c,
-                               X.ix, X.iz, t);
+        col_prep_nodal<PL, MX, FORM>(X.col(0), X.col(4), X.col(2), X.col(1), X.col(3), X.col(5), X.col(6), X.col(7),
+                                     p, c, X.ix, X.iz, t);
     __syncthreads();
-    store_six<NCOL, MX>(X, p, 0, 4, 2, 1, 3, 5);
+    if (FORM == NL_DIV) store_three<NCOL>(X, p, 0, 4, 2);
+    else store_six<NCOL, MX>(X, p, 0, 4, 2, 1, 3, 5);
 }
 
-template <int NCOL, int PL>
+template <int NCOL, int PL, int FORM = NL_ROT>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_stage(ColParams p) {
-    column_stage_body<NCOL, PL>(p, blockIdx.x);
+    column_stage_body<NCOL, PL, false, FORM>(p, blockIdx.x);
 }
 // Batched stage: blockIdx.y selects the instance of a size class, whose
 // parameters are staged in shared memory.
@@ -528,9 +554,10 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     column_stage_body<NCOL, PL, true>(p, blockIdx.x);
 }
 
-// Nodal velocity and vorticity from the state U (used after set_state); MX:
-// their FP32 Chebyshev coefficients instead.
-template <int NCOL, int PL, bool MX = false>
+// Nodal fields of the nonlinear form (velocity and vorticity for the
+// rotational form) from the state U (used after set_state); MX: their FP32
+// Chebyshev coefficients instead.
+template <int NCOL, int PL, bool MX = false, int FORM = NL_ROT>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_prep(ColParams p) {
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
@@ -540,10 +567,56 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     tile_load<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p);
     __syncthreads();
     if (X.valid)
-        col_prep_nodal<PL, MX>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7), p, X.c,
-                               X.ix, X.iz, X.t);
+        col_prep_nodal<PL, MX, FORM>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7),
+                                     p, X.c, X.ix, X.iz, X.t);
     __syncthreads();
-    store_six<NCOL, MX>(X, p, 0, 1, 2, 3, 4, 5);
+    if (FORM == NL_DIV) store_three<NCOL>(X, p, 0, 1, 2);
+    else store_six<NCOL, MX>(X, p, 0, 1, 2, 3, 4, 5);
+}
+
+// Divergence form, after the periodic transforms: forward DCT of the six
+// negated products -u_i u_j at the nodes (p.nod, order 00 01 02 11 12 22) and
+// div! of the rows in coefficient space (operators.jl:270-294):
+//   N_i = i k (-uu_i0) + D (-uu_i1) + i l (-uu_i2)
+// written as FP64 coefficients to p.Nout.  Regions 0-5 hold the six products,
+// 6 and 7 the transform buffers (region 6 then takes the derivative).
+template <int NCOL, int PL>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_div(ColParams p) {
+    extern __shared__ zd smem[];
+    const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
+    const Team& t = X.t;
+    const int cs = X.cs, hs = t.hs, c0 = X.c0, qo = t.q * hs, nq = pcount(t.q, t.P);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) tile_load<NCOL>(X.reg(m), cs, hs, p.nod[m], c0, p);
+    __syncthreads();
+    if (X.valid) {
+        const bool nyq = col_nyquist(p, X.ix, X.iz);
+#pragma unroll 1
+        for (int m = 0; m < 6; ++m) col_forward_y<PL>(X.col(m), X.col(6), X.col(7), p, nyq, t);
+        const double k = p.ax * X.ix;
+        const double l = p.bz * (X.iz <= (p.Nz >> 1) ? X.iz : X.iz - p.Nz);
+        // row i: (x, y, z) entries in regions (a, b, c), result into region a
+        // of a product no later row reads: N2 -> 5 (02, 12, 22), N1 -> 3
+        // (01, 11, 12), N0 -> 0 (00, 01, 02)
+        const int ra[3] = {2, 1, 0}, rb[3] = {4, 3, 1}, rc[3] = {5, 4, 2}, ro[3] = {5, 3, 0};
+        zd* D = X.col(6);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            col_diff(X.col(rb[r]), D, t);
+            const zd* a = X.col(ra[r]);
+            const zd* cz = X.col(rc[r]);
+            zd* o = X.col(ro[r]);
+            for (int j = t.lane; j < nq; j += 32) {
+                const int e = qo + j;
+                o[e] = zadd(zadd(zmulis(a[e], k), D[e]), zmulis(cz[e], l));
+            }
+            tsync(t);
+        }
+    }
+    __syncthreads();
+    tile_store<NCOL>(X.reg(0), cs, hs, p.Nout[0], c0, p);
+    tile_store<NCOL>(X.reg(3), cs, hs, p.Nout[1], c0, p);
+    tile_store<NCOL>(X.reg(5), cs, hs, p.Nout[2], c0, p);
 }
 
 // Forward DCT of the nonlinear term only: coefficients into p.Nout.
@@ -606,9 +679,10 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
 }
 
 // Pressure reconstruction (pressure.jl:115-204) from the nonlinear term at
-// the nodes (p.Nn) and the normal velocity U[1]: Neumann Helmholtz per mode
-// with the factors in p.bank.fac_p / sa[0..1] (Neumann weights).
-template <int NCOL, int PL>
+// the nodes (p.Nn; NCOEF: as coefficients) and the normal velocity U[1]:
+// Neumann Helmholtz per mode with the factors in p.bank.fac_p / sa[0..1]
+// (Neumann weights).
+template <int NCOL, int PL, bool NCOEF = false>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_pressure(ColParams p) {
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
@@ -620,7 +694,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     for (int i = 0; i < 3; ++i) {
         tile_load<NCOL>(X.reg(i), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p);
         __syncthreads();
-        if (X.valid) col_forward_y<PL>(X.col(i), X.col(6), X.col(7), p, nyq, t);
+        if (X.valid && !NCOEF) col_forward_y<PL>(X.col(i), X.col(6), X.col(7), p, nyq, t);
         __syncthreads();
     }
     tile_load<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p);

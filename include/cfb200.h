@@ -2,8 +2,8 @@
  * cfb200.h -- C ABI of the B200 CNRK2 engine for ChannelFlow.jl's time step.
  *
  * The engine replaces the device path of the reference's CNRK2 `step!`
- * (src/timesteppers/cnrk2.jl:567-625) with the rotational nonlinear term
- * (src/nonlinear.jl:173-193), the batched influence/tau Stokes solve
+ * (src/timesteppers/cnrk2.jl:567-625) with the nonlinear term in any of its
+ * three forms (src/nonlinear.jl:113-193), the batched influence/tau Stokes solve
  * (src/solvers/stokes.jl:391-418, batchedinfluence.jl:129-160, meanmode.jl:263-310)
  * and the padded Fourier-Chebyshev transforms (src/ffts.jl:189-290).  The
  * reference reaches that path through Julia dispatch on CuArray storage
@@ -48,6 +48,15 @@ extern "C" {
 #define CF_PRECISION_FP64 0
 #define CF_PRECISION_MIXED 1
 
+/* Nonlinear form of NonLinearTerm(...; form) (src/nonlinear.jl:10-17, 113-193).
+ * ROTATIONAL: u x curl(u) with the modified pressure (the default);
+ * CONVECTIVE: -(u.grad)u; DIVERGENCE: -div(u u).  The last two carry the
+ * ordinary pressure (pressure.jl:86-92).  The mixed precision and ensembles
+ * run the rotational form only. */
+#define CF_FORM_ROTATIONAL 0
+#define CF_FORM_CONVECTIVE 1
+#define CF_FORM_DIVERGENCE 2
+
 typedef struct cf_config {
     int Nx, Ny, Nz;      /* Grid(Nx, Ny, Nz, Lx, Lz): grids.jl:27-30 */
     double Lx, Lz;
@@ -57,6 +66,7 @@ typedef struct cf_config {
     int constraint;      /* CF_CONSTRAINT_* (problem.jl:81-87) */
     double c1, c2;       /* gradients or bulk velocities */
     int precision;       /* CF_PRECISION_* (0: FP64 plain form) */
+    int form;            /* CF_FORM_* (0: rotational) */
 } cf_config;
 
 typedef struct cf_engine cf_handle;
@@ -83,7 +93,16 @@ int cf_get_state_device(cf_handle* h, void* U, void* P);
  * Only NoForcing is supported (forcing.jl:9-11). */
 int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out);
 
-/* NonLinearTerm{RotatingForm}(t, U, N) on host buffers (nonlinear.jl:173-193). */
+/* One step! of duration dt from t: the Flows adapter's step
+ * (ext/ChannelFlowFlowsExt.jl:36-52), which Flows calls with a shortened dt to
+ * end an interval between nominal steps.  dt equal to the nominal step is
+ * cf_step(h, t, 1, ...); any other dt runs with Stokes factors built for it
+ * (the adapter's temporary CNRK2, :46) on the first call with that dt and kept
+ * for repeated calls, while the nominal factors stay in place.
+ * *t_out = t + dt. */
+int cf_step_dt(cf_handle* h, double t, double dt, double* t_out, double* grads_out);
+
+/* NonLinearTerm(t, U, N) of the handle's form on host buffers (nonlinear.jl:113-193). */
 int cf_nonlinear(cf_handle* h, const double* U, double* N);
 
 /* Chebyshev transform of many FP32 columns on the tensor cores (the kernel of

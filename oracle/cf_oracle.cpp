@@ -11,7 +11,8 @@
 //   transforms           src/ffts.jl:156-206, 245-290, 366-436
 //   DCT-I (REDFT00)      src/transforms/chebyshev.jl:481-502
 //   operators            src/fields/operators.jl:14-190, 478-484
-//   nonlinear (rot.)     src/nonlinear.jl:173-193
+//   nonlinear terms      src/nonlinear.jl:113-193 (rotational, convective,
+//                        divergence forms)
 //   influence solver     src/solvers/influence.jl:60-316
 //   batched bank         src/solvers/batchedinfluence.jl:32-160
 //   mean mode            src/solvers/meanmode.jl:13-150
@@ -832,6 +833,12 @@ struct Problem {
     std::vector<cd> Q[3], N[3], R[3];
     std::vector<cd> TMP[3], OM[3];
     std::vector<double> uphys[3], wphys[3], nphys[3];
+    // nonlinear form (nonlinear.jl:10-17): 0 rotational, 1 convective, 2 divergence
+    int form = 0;
+    std::vector<cd> GR[9];          // convective: spectral gradient (i, j) at 3 i + j
+    std::vector<double> gphys[9];   // convective: its padded physical values
+    std::vector<cd> UU[6];          // divergence: spectral products 00 01 02 11 12 22
+    std::vector<double> uuphys[6];  // divergence: physical products
 
     long nr() const { return g.nr(); }
     void alloc_nl() {
@@ -842,8 +849,9 @@ struct Problem {
     }
 };
 
-// NonLinearTerm{RotatingForm} (nonlinear.jl:173-193); overwrites Nout.
-static void nonlinear(Problem& pb, const cd* const U[3], cd* const Nout[3]) {
+// total velocity: TMP = U with the base profile added to mode (0,0) of u
+// (nonlinear.jl:123-124, 153-154, 179-180)
+static void total_velocity(Problem& pb, const cd* const U[3]) {
     const OGrid& g = pb.g;
     const long nr = g.nr(), S = (long)g.Nxh * g.Nz;
     for (int i = 0; i < 3; ++i) {
@@ -853,6 +861,86 @@ static void nonlinear(Problem& pb, const cd* const U[3], cd* const Nout[3]) {
         for (long x = 0; x < sampled(nr); ++x) dst[x] = src[x];
     }
     for (int n = 0; n < g.Ny; ++n) pb.TMP[0][n * S] += pb.base[n];
+}
+
+// _store_rhs! with sign -1 (nonlinear.jl:200-210)
+static void negate(const OGrid& g, cd* const N[3]) {
+    for (int i = 0; i < 3; ++i) {
+        cd* x = N[i];
+#pragma omp parallel for schedule(static)
+        for (long j = 0; j < g.nr(); ++j) x[j] = -x[j];
+    }
+}
+
+// NonLinearTerm{ConvectiveForm} (nonlinear.jl:113-140): grad! of the total
+// velocity (operators.jl:206-214), 12 inverse transforms, dot! (operators.jl:
+// 247-254), 3 forward transforms, sign -1.
+static void nonlinear_convective(Problem& pb, const cd* const U[3], cd* const Nout[3]) {
+    const OGrid& g = pb.g;
+    total_velocity(pb, U);
+    for (int i = 0; i < 3; ++i) {
+        const cd* T = pb.TMP[i].data();
+        op_ddx1(g, T, pb.GR[3 * i + 0].data(), false);
+        op_ddx2(g, T, pb.GR[3 * i + 1].data(), false);
+        op_ddx3(g, T, pb.GR[3 * i + 2].data(), false);
+    }
+    for (int i = 0; i < 3; ++i) inverse_transform(g, pb.TMP[i].data(), pb.uphys[i].data());
+    for (int m = 0; m < 9; ++m) inverse_transform(g, pb.GR[m].data(), pb.gphys[m].data());
+    const long np = g.nphys();
+    const double *u1 = pb.uphys[0].data(), *u2 = pb.uphys[1].data(), *u3 = pb.uphys[2].data();
+    for (int i = 0; i < 3; ++i) {
+        const double *g1 = pb.gphys[3 * i].data(), *g2 = pb.gphys[3 * i + 1].data(), *g3 = pb.gphys[3 * i + 2].data();
+        double* n = pb.nphys[i].data();
+#pragma omp parallel for schedule(static)
+        for (long x = 0; x < sampled(np); ++x) n[x] = u1[x] * g1[x] + u2[x] * g2[x] + u3[x] * g3[x];
+    }
+    for (int i = 0; i < 3; ++i) forward_transform(g, pb.nphys[i].data(), Nout[i]);
+    negate(g, Nout);
+}
+
+// index of the product u_i u_j among the six distinct ones (00 01 02 11 12 22)
+static int sym6(int i, int j) {
+    if (i > j) std::swap(i, j);
+    return i == 0 ? j : (i == 1 ? 2 + j : 5);
+}
+
+// NonLinearTerm{DivergenceForm} (nonlinear.jl:146-167): 3 inverse transforms,
+// outer! (operators.jl:227-234; u_i u_j = u_j u_i exactly, so the six distinct
+// products are transformed), forward transforms, div! of the rows
+// (operators.jl:270-294), sign -1.
+static void nonlinear_divergence(Problem& pb, const cd* const U[3], cd* const Nout[3]) {
+    const OGrid& g = pb.g;
+    total_velocity(pb, U);
+    for (int i = 0; i < 3; ++i) inverse_transform(g, pb.TMP[i].data(), pb.uphys[i].data());
+    const long np = g.nphys();
+    for (int i = 0; i < 3; ++i)
+        for (int j = i; j < 3; ++j) {
+            const double *a = pb.uphys[i].data(), *b = pb.uphys[j].data();
+            double* o = pb.uuphys[sym6(i, j)].data();
+#pragma omp parallel for schedule(static)
+            for (long x = 0; x < sampled(np); ++x) o[x] = a[x] * b[x];
+        }
+    for (int m = 0; m < 6; ++m) forward_transform(g, pb.uuphys[m].data(), pb.UU[m].data());
+    for (int i = 0; i < 3; ++i) {
+        op_ddx1(g, pb.UU[sym6(i, 0)].data(), Nout[i], false);
+        op_ddx2(g, pb.UU[sym6(i, 1)].data(), Nout[i], true);
+        op_ddx3(g, pb.UU[sym6(i, 2)].data(), Nout[i], true);
+    }
+    negate(g, Nout);
+}
+
+static void nonlinear_rotational(Problem& pb, const cd* const U[3], cd* const Nout[3]);
+// NonLinearTerm call of the problem's form; overwrites Nout.
+static void nonlinear(Problem& pb, const cd* const U[3], cd* const Nout[3]) {
+    if (pb.form == 1) nonlinear_convective(pb, U, Nout);
+    else if (pb.form == 2) nonlinear_divergence(pb, U, Nout);
+    else nonlinear_rotational(pb, U, Nout);
+}
+
+// NonLinearTerm{RotatingForm} (nonlinear.jl:173-193); overwrites Nout.
+static void nonlinear_rotational(Problem& pb, const cd* const U[3], cd* const Nout[3]) {
+    const OGrid& g = pb.g;
+    total_velocity(pb, U);
     const cd* T[3] = {pb.TMP[0].data(), pb.TMP[1].data(), pb.TMP[2].data()};
     cd* O[3] = {pb.OM[0].data(), pb.OM[1].data(), pb.OM[2].data()};
     op_curl(g, T, O);
@@ -881,9 +969,10 @@ static bool problem_stokes(Problem& pb) {
     return true;
 }
 
-// One CNRK2 stage j (cnrk2.jl:588-622); gradients carries the previous
-// stage's uniform gradients in and this stage's out.
-static void cnrk2_stage(Problem& pb, cd* const U[3], cd* Pf, int j, double* gradients) {
+// One CNRK2 stage j (cnrk2.jl:588-622) of a step of duration dt with the
+// Stokes solvers st (the problem's own for its nominal dt); gradients carries
+// the previous stage's uniform gradients in and this stage's out.
+static void cnrk2_stage(Problem& pb, cd* const U[3], cd* Pf, int j, double* gradients, double dt, const Stokes* st) {
     const OGrid& g = pb.g;
     const long nr = g.nr(), S = (long)g.Nxh * g.Nz;
     cd* Nf[3] = {pb.N[0].data(), pb.N[1].data(), pb.N[2].data()};
@@ -906,7 +995,7 @@ static void cnrk2_stage(Problem& pb, cd* const U[3], cd* Pf, int j, double* grad
 #pragma omp parallel for schedule(static)
         for (long x = 0; x < sampled(nr); ++x) Qi[x] = (j == 0) ? Ni[x] : a * Qi[x] + Ni[x];
     }
-    const double lambda = 1.0 / (CC[j] * pb.dt), weight = CB[j] / CC[j];
+    const double lambda = 1.0 / (CC[j] * dt), weight = CB[j] / CC[j];
     for (int i = 0; i < 3; ++i) {
         op_laplacian(g, U[i], Rf[i]);
         if (i == 0) op_ddx1(g, Pf, Nf[i], false);
@@ -923,13 +1012,13 @@ static void cnrk2_stage(Problem& pb, cd* const U[3], cd* Pf, int j, double* grad
     Rf[0][0] -= old[0];
     Rf[2][0] -= old[1];
     const cd* Rc[3] = {Rf[0], Rf[1], Rf[2]};
-    pb.stokes[j].solve(g, U, Pf, Rc, pb.cmode, pb.c1, pb.c2, pb.basemean, gradients);
+    st[j].solve(g, U, Pf, Rc, pb.cmode, pb.c1, pb.c2, pb.basemean, gradients);
 }
 
 // step! (cnrk2.jl:567-625).  Returns the last stage's gradients in grads.
-static void cnrk2_step(Problem& pb, cd* const U[3], cd* Pf, double* grads) {
+static void cnrk2_step(Problem& pb, cd* const U[3], cd* Pf, double* grads, double dt, const Stokes* st) {
     double gradients[2] = {pb.cmode == 0 ? pb.c1 : 0.0, pb.cmode == 0 ? pb.c2 : 0.0};
-    for (int j = 0; j < 3; ++j) cnrk2_stage(pb, U, Pf, j, gradients);
+    for (int j = 0; j < 3; ++j) cnrk2_stage(pb, U, Pf, j, gradients, dt, st);
     grads[0] = gradients[0];
     grads[1] = gradients[1];
 }
@@ -1174,6 +1263,19 @@ void* or_create(int Nx, int Ny, int Nz, double Lx, double Lz, double nu, double 
     pb->alloc_nl();
     return pb;
 }
+// nonlinear form of the problem (NonLinearTerm(...; form), nonlinear.jl:55-70):
+// 0 RotatingForm, 1 ConvectiveForm, 2 DivergenceForm
+int or_set_form(void* h, int form) {
+    auto* pb = static_cast<Problem*>(h);
+    if (form < 0 || form > 2) { set_error("unknown nonlinear form"); return -1; }
+    pb->form = form;
+    const long nr = pb->g.nr(), np = pb->g.nphys();
+    if (form == 1 && pb->GR[0].empty())
+        for (int m = 0; m < 9; ++m) { pb->GR[m].assign(nr, 0); pb->gphys[m].assign(np, 0); }
+    if (form == 2 && pb->UU[0].empty())
+        for (int m = 0; m < 6; ++m) { pb->UU[m].assign(nr, 0); pb->uuphys[m].assign(np, 0); }
+    return 0;
+}
 void or_destroy(void* h) { delete static_cast<Problem*>(h); }
 void or_get_base(void* h, double* base, double* curv) {
     auto* pb = static_cast<Problem*>(h);
@@ -1192,7 +1294,22 @@ int or_step(void* h, double* U, double* P, int nsteps, double* grads) {
     const long nr = pb->g.nr();
     cd* Uc = reinterpret_cast<cd*>(U);
     cd* Uf[3] = {Uc, Uc + nr, Uc + 2 * nr};
-    for (int s = 0; s < nsteps; ++s) cnrk2_step(*pb, Uf, reinterpret_cast<cd*>(P), grads);
+    for (int s = 0; s < nsteps; ++s) cnrk2_step(*pb, Uf, reinterpret_cast<cd*>(P), grads, pb->dt, pb->stokes);
+    return 0;
+}
+// One step of duration dt with Stokes solvers built for it (the Flows
+// adapter's temporary CNRK2 for a shortened final step,
+// ext/ChannelFlowFlowsExt.jl:45-50); the problem's own solvers are untouched.
+int or_step_dt(void* h, double* U, double* P, double dt, double* grads) {
+    auto* pb = static_cast<Problem*>(h);
+    if (!(std::isfinite(dt) && dt > 0)) { set_error("dt must be finite and positive"); return -1; }
+    Stokes st[3];
+    for (int j = 0; j < 3; ++j)
+        if (!st[j].init(pb->g, pb->nu, 1.0 / (CC[j] * dt))) { set_error("singular influence matrix"); return -2; }
+    const long nr = pb->g.nr();
+    cd* Uc = reinterpret_cast<cd*>(U);
+    cd* Uf[3] = {Uc, Uc + nr, Uc + 2 * nr};
+    cnrk2_step(*pb, Uf, reinterpret_cast<cd*>(P), grads, dt, st);
     return 0;
 }
 // one stage j of a step (a bounded sample of the step's work)
@@ -1203,7 +1320,7 @@ int or_stage(void* h, double* U, double* P, int j) {
     cd* Uc = reinterpret_cast<cd*>(U);
     cd* Uf[3] = {Uc, Uc + nr, Uc + 2 * nr};
     double gr[2] = {pb->cmode == 0 ? pb->c1 : 0.0, pb->cmode == 0 ? pb->c2 : 0.0};
-    cnrk2_stage(*pb, Uf, reinterpret_cast<cd*>(P), j, gr);
+    cnrk2_stage(*pb, Uf, reinterpret_cast<cd*>(P), j, gr, pb->dt, pb->stokes);
     return 0;
 }
 void or_nonlinear(void* h, const double* U, double* N) {

@@ -21,6 +21,9 @@ _lib = None
 
 _D = ctypes.POINTER(ctypes.c_double)
 
+# NonLinearTerm forms (src/nonlinear.jl:10-17)
+FORMS = {"rotational": 0, "convective": 1, "divergence": 2}
+
 
 def build():
     """Compile the oracle library (idempotent)."""
@@ -39,9 +42,11 @@ def lib():
         L.or_create.restype = ctypes.c_void_p
         L.or_create.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 4 + [_D, ctypes.c_int] + [ctypes.c_double] * 2
         L.or_destroy.argtypes = [ctypes.c_void_p]
+        L.or_set_form.argtypes = [ctypes.c_void_p, ctypes.c_int]
         for name in ("or_prepare",):
             getattr(L, name).argtypes = [ctypes.c_void_p]
         L.or_step.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int, _D]
+        L.or_step_dt.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_double, _D]
         L.or_nonlinear.argtypes = [ctypes.c_void_p, _D, _D]
         L.or_stage.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int]
         L.or_inverse.argtypes = [ctypes.c_void_p, _D, _D]
@@ -174,12 +179,15 @@ def mean_solve(Ny, nu, lam, Rx, Ry, Rz, pressuregradient=None, bulkvelocity=None
 
 # ------------------------------------------------------------------ problem
 class OracleProblem:
-    """CPU restatement of ChannelFlowProblem + CNRK2 + NonLinearTerm{RotatingForm}.
+    """CPU restatement of ChannelFlowProblem + CNRK2 + NonLinearTerm.
 
     ``constraint`` is ("pressuregradient", (gx, gz)) or ("bulkvelocity", (ub, wb)).
+    ``form`` is the nonlinear form (src/nonlinear.jl:10-17): "rotational"
+    (default), "convective" or "divergence".
     """
 
-    def __init__(self, Nx, Ny, Nz, Lx, Lz, nu, dt, profile, constraint=("pressuregradient", (0.0, 0.0))):
+    def __init__(self, Nx, Ny, Nz, Lx, Lz, nu, dt, profile, constraint=("pressuregradient", (0.0, 0.0)),
+                 form="rotational"):
         self.Nx, self.Ny, self.Nz, self.Lx, self.Lz = Nx, Ny, Nz, float(Lx), float(Lz)
         self.nu, self.dt = float(nu), float(dt)
         self.Nxh = Nx // 2 + 1
@@ -196,6 +204,11 @@ class OracleProblem:
         if not h:
             raise ValueError(_err())
         self._h = ctypes.c_void_p(h)
+        if form not in FORMS:
+            raise ValueError(f"unknown nonlinear form {form!r}")
+        self.form = form
+        if lib().or_set_form(self._h, FORMS[form]) != 0:
+            raise ValueError(_err())
         self.base = np.zeros(Ny)
         self.basecurv = np.zeros(Ny)
         lib().or_get_base(self._h, _p(self.base), _p(self.basecurv))
@@ -229,6 +242,16 @@ class OracleProblem:
         assert P.dtype == np.complex128 and P.flags["C_CONTIGUOUS"] and P.shape == self.shape
         g = np.zeros(2)
         rc = lib().or_step(self._h, _p(U.view(np.float64)), _p(P.view(np.float64)), int(nsteps), _p(g))
+        if rc != 0:
+            raise ValueError(_err())
+        return tuple(g)
+
+    def step_dt(self, U, P, dt):
+        """One step of duration dt (a shortened final step) in place; returns the gradients."""
+        assert U.dtype == np.complex128 and U.flags["C_CONTIGUOUS"] and U.shape == (3,) + self.shape
+        assert P.dtype == np.complex128 and P.flags["C_CONTIGUOUS"] and P.shape == self.shape
+        g = np.zeros(2)
+        rc = lib().or_step_dt(self._h, _p(U.view(np.float64)), _p(P.view(np.float64)), float(dt), _p(g))
         if rc != 0:
             raise ValueError(_err())
         return tuple(g)
@@ -347,9 +370,9 @@ def couette(Nx, Ny, Nz, Lx, Lz, nu, dt, **kw):
     return OracleProblem(Nx, Ny, Nz, Lx, Lz, nu, dt, lambda y: y, **kw)
 
 
-def poiseuille(Nx, Ny, Nz, Lx, Lz, nu, dt, bulkvelocity=None, pressuregradient=None):
+def poiseuille(Nx, Ny, Nz, Lx, Lz, nu, dt, bulkvelocity=None, pressuregradient=None, form="rotational"):
     if bulkvelocity is not None:
         c = ("bulkvelocity", bulkvelocity)
     else:
         c = ("pressuregradient", pressuregradient if pressuregradient is not None else (-2 * nu, 0.0))
-    return OracleProblem(Nx, Ny, Nz, Lx, Lz, nu, dt, lambda y: 1 - y * y, constraint=c)
+    return OracleProblem(Nx, Ny, Nz, Lx, Lz, nu, dt, lambda y: 1 - y * y, constraint=c, form=form)

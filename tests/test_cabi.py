@@ -37,3 +37,18 @@ def test_errors_are_reported_not_crashed():
     with pytest.raises(ValueError):
         cfb200.ChannelFlowProblem(cfb200.Grid(8, 9, 8, 6.28, 6.28), "couette", 0.01, 0.01,
                                   pressuregradient=(0, 0), bulkvelocity=(0, 0))
+
+
+def test_form_validation_before_device_work():
+    g = cfb200.Grid(8, 9, 8, 6.28, 6.28)
+    with pytest.raises(ValueError):
+        cfb200.CouetteFlow(g, 0.01, 0.01, form="skew-symmetric")
+    # the mixed precision runs the rotational form only (CF_E_UNSUPPORTED)
+    with pytest.raises(cfb200.CFError) as e:
+        cfb200.CouetteFlow(g, 0.01, 0.01, form="divergence", precision="mixed")
+    assert e.value.code == -5
+    # an out-of-range cf_config.form is CF_E_ARG
+    cfg, _, _ = cfb200._make_config(g, "couette", 0.01, 0.01)
+    cfg.form = 7
+    h = ctypes.c_void_p()
+    assert cfb200.lib().cf_create(ctypes.byref(cfg), ctypes.byref(h)) == -1

@@ -111,6 +111,27 @@ def test_analytic_nonlinear_rotational():
     assert np.array_equal(U, saved)
 
 
+@pytest.mark.parametrize("form", ["convective", "divergence"])
+def test_analytic_nonlinear_forms(form):
+    # test_nonlinear.jl:1-38 (convective and divergence forms): the total
+    # velocity (y^2 + y, 1, 0) is divergence-free, so both give -(2y + 1) e_x
+    pb = make(5, 9, 5, 2 * np.pi, 2 * np.pi, profile=lambda y: y, form=form)
+    U = np.stack([pb.spectral(lambda x, y, z: y**2 + 0 * x), pb.spectral(lambda x, y, z: 1.0 + 0 * x),
+                  pb.zeros()])
+    saved = U.copy()
+    for _ in range(2):  # repeated calls reuse the work arrays
+        N = pb.nonlinear(U)
+        assert np.max(np.abs(pb.ifft(N[0]) - pb.sample(lambda x, y, z: -(2 * y + 1) + 0 * x))) < 2e-11
+        assert np.max(np.abs(pb.ifft(N[1]))) < 2e-11
+        assert np.max(np.abs(pb.ifft(N[2]))) < 2e-11
+    assert np.array_equal(U, saved)
+
+
+def test_unknown_form_rejected():
+    with pytest.raises(ValueError):
+        make(5, 9, 5, 2 * np.pi, 2 * np.pi, form="skew")
+
+
 def check_constraints(pb, U):
     # helpers.jl:77-87
     assert np.max(np.abs(pb.div(U))) < 2e-9
@@ -151,11 +172,22 @@ def test_projection_bulk_constraint():
 
 
 def test_laminar_couette_modified_pressure():
-    # test_projection.jl:86-96
+    # test_projection.jl:77-87
     pb = make(5, 9, 5, 2 * np.pi, 2 * np.pi, profile=lambda y: y)
     U = pb.project(pb.zeros(3))
     P = pb.pressure(U)
     assert np.max(np.abs(pb.ifft(P) - pb.sample(lambda x, y, z: y**2 / 2 - 1 / 6 + 0 * x))) < 2e-10
+
+
+@pytest.mark.parametrize("form", ["convective", "divergence"])
+def test_laminar_couette_physical_pressure(form):
+    # pressure.jl:86-92: for the convective and divergence forms P is the
+    # ordinary pressure, which is uniform (zero in the zero-mean gauge) for
+    # laminar Couette flow, where (u.grad)u = 0
+    pb = make(5, 9, 5, 2 * np.pi, 2 * np.pi, profile=lambda y: y, form=form)
+    U = pb.project(pb.zeros(3))
+    P = pb.pressure(U)
+    assert np.max(np.abs(P)) < 2e-12
 
 
 def test_random_state_admissible():
