@@ -67,11 +67,21 @@ def sizes(cfg):
 def model_bytes(cfg, s_nl=16):
     """Algorithmic bytes per kernel launch (fixed byte model of the step).
 
-    per stage: 16*19*Nr (U, P, Q read/write 14; responses and factors 5)
-               + s_nl*(18*Nr + 18*Nq) (N read 3, nodes written 6, z-inverse
-               6->6, x-pass 6->3, z-forward 3->3)
+    per stage (rotational form): 16*19*Nr (U, P, Q read/write 14; responses
+    and factors 5) + s_nl*(18*Nr + 18*Nq) (N read 3, nodes written 6,
+    z-inverse 6->6, x-pass 6->3, z-forward 3->3).  Convective form: z-inverse
+    6->9, x-pass 9->3.  Divergence form: nodes written 3, z-inverse 3->3,
+    x-pass 3->6, z-forward 6->6, and k_column_div (counted with the column
+    kernel) 6->3.
     """
     Nr, Nq = sizes(cfg)
+    form = cfg.get("form", "rotational")
+    if form == "convective":
+        return {"zinv": s_nl * (6 * Nr + 9 * Nq), "xpass": s_nl * (12 * Nq), "zfwd": s_nl * (3 * Nq + 3 * Nr),
+                "column": 16 * 19 * Nr + s_nl * 9 * Nr}
+    if form == "divergence":
+        return {"zinv": s_nl * (3 * Nr + 3 * Nq), "xpass": s_nl * (9 * Nq), "zfwd": s_nl * (6 * Nq + 6 * Nr),
+                "column": 16 * 19 * Nr + s_nl * 15 * Nr}
     return {
         "zinv": s_nl * (6 * Nr + 6 * Nq),
         "xpass": s_nl * (9 * Nq),
@@ -243,7 +253,7 @@ def workload_desc(cfg):
     return {"grid": [cfg["Nx"], cfg["Ny"], cfg["Nz"]], "Lx": cfg["Lx"], "Lz": cfg["Lz"], "nu": cfg["nu"],
             "dt": cfg["dt"], "profile": cfg["profile"],
             "constraint": ("bulkvelocity" if cfg["constraint"] else "pressuregradient(0,0)"),
-            "form": "rotational", "precision": "fp64 plain",
+            "form": cfg.get("form", "rotational"), "precision": "fp64 plain",
             "l2": "state larger than L2 (no flush needed)"}
 
 
@@ -490,8 +500,17 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
+    ap.add_argument("--form", default="rotational", choices=["rotational", "convective", "divergence"],
+                    help="nonlinear form of the FP64 step (the mixed form runs the rotational one)")
+    ap.add_argument("--grid", default=None,
+                    help="Nx,Ny,Nz replacing the configuration's grid (smaller cases for profiling)")
     args = ap.parse_args()
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.grid:
+        cfg["Nx"], cfg["Ny"], cfg["Nz"] = (int(v) for v in args.grid.split(","))
+    cfg["form"] = args.form
+    if args.form != "rotational":
+        args.no_mixed = True
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -520,9 +539,9 @@ def main():
 
     g = cfb200.Grid(cfg["Nx"], cfg["Ny"], cfg["Nz"], cfg["Lx"], cfg["Lz"])
     if cfg["profile"] == "couette":
-        pb = cfb200.CouetteFlow(g, cfg["nu"], cfg["dt"])
+        pb = cfb200.CouetteFlow(g, cfg["nu"], cfg["dt"], form=args.form)
     else:
-        pb = cfb200.PoiseuilleFlow(g, cfg["nu"], cfg["dt"], bulkvelocity=cfg["constraint"])
+        pb = cfb200.PoiseuilleFlow(g, cfg["nu"], cfg["dt"], bulkvelocity=cfg["constraint"], form=args.form)
     cfb200.lib().cf_random_state(pb.handle, 1000 + rank, cfg["amp"], cfg["shape"], cfg["rho"])
     U0, P0 = pb.get_state()
     stream = torch.cuda.ExternalStream(pb.stream_ptr())
@@ -571,12 +590,13 @@ def main():
     dom = max(kavg, key=kavg.get)
     peak, peak_kind = peaks()
     achieved = mb[dom] / (kavg[dom] * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": {"zinv": "k_zinv", "xpass": "k_xpass", "zfwd": "k_zfwd",
-                                           "column": "k_column_stage"}[dom],
+    xname = {"rotational": "k_xpass", "convective": "k_xpass_conv", "divergence": "k_xpass_div"}[args.form]
+    knames = {"zinv": "k_zinv", "xpass": xname, "zfwd": "k_zfwd", "column": "k_column_stage"}
+    roofline = {"bound": "hbm", "kernel": knames[dom],
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_kind,
-                "traffic": traffic_from_profiles({"zinv": "k_zinv", "xpass": "k_xpass", "zfwd": "k_zfwd",
-                                                  "column": "k_column_stage"}[dom], args.config),
+                "traffic": (traffic_from_profiles(knames[dom], args.config)
+                            if not args.grid and args.form == "rotational" else None),
                 "algorithmic_bytes_per_launch": mb[dom],
                 "kernel_ms_per_launch": kavg,
                 "step_model_bytes": 3 * sum(mb.values()),

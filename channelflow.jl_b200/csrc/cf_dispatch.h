@@ -1,0 +1,42 @@
+// cf_dispatch.h -- kernel tables of the engine.  The kernels of one size (the
+// Chebyshev length P of the column kernels, the padded length L of the
+// periodic transforms) are instantiated in their own translation unit
+// (cf_inst_col.cu, cf_inst_fft.cu, compiled once per size with CF_INST_P or
+// CF_INST_L defined), so the library builds in parallel; the host code in
+// cf_engine.cu picks a size's table through these declarations.
+#pragma once
+#include "cf_fftkernels.cuh"
+#include "cf_kernels.cuh"
+
+#define CF_NCOL 2
+static_assert(CF_NCOL == 1 || CF_NCOL == 2, "column teams use named barriers 1 and 2");
+
+// Column-kernel lengths P and periodic lengths L with compile-time
+// instantiations; other sizes use the run-time-sized one (argument 0).
+#define CF_COL_LENGTHS(X) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384)
+
+typedef void (*ColKernel)(ColParams);
+typedef void (*FftKernel)(FftParams);
+typedef void (*DiagKernel)(ColParams, double*);
+typedef void (*ColBatchKernel)(const ColParams*);
+typedef void (*FftBatchKernel)(const FftParams*);
+
+enum {
+    KC_STAGE, KC_PREP, KC_NLOUT, KC_PROJECT, KC_PRESSURE, KC_STAGE_MX, KC_PREP_MX,
+    KC_STAGE_CONV, KC_PREP_CONV, KC_STAGE_DIV, KC_PREP_DIV, KC_DIV, KC_PRESSURE_COEF, KC_COUNT
+};
+enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_XPASS_CONV, KF_XPASS_DIV, KF_COUNT };
+
+// defined for P in CF_COL_LENGTHS and 0 (cf_inst_col.cu)
+template <int P>
+ColKernel col_kernel_for(int which);
+template <int P>
+DiagKernel diag_kernel_for();
+template <int P>
+ColBatchKernel col_batch_kernel_for();
+// defined for L in CF_STATIC_FFT_LENGTHS and 0 (cf_inst_fft.cu); f32: the
+// FP32 transforms of the mixed-precision form
+template <int L>
+FftKernel fft_kernel_for(int which, bool f32);
+template <int L>
+FftBatchKernel fft_batch_kernel_for(int which);

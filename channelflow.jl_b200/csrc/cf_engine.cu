@@ -15,74 +15,31 @@
 #include <vector>
 
 #include "../../include/cfb200.h"
-#include "cf_fftkernels.cuh"
-#include "cf_kernels.cuh"
+#include "cf_dispatch.h"
 #include "cf_cheb.cuh"
 
-#define CF_NCOL 2
-static_assert(CF_NCOL == 1 || CF_NCOL == 2, "column teams use named barriers 1 and 2");
-
-// Kernel instantiations by size: the Chebyshev length P of the column kernels
-// and the padded lengths Nzp, Nxp of the periodic transforms have
-// compile-time versions for the grids of the supported workloads (index
-// arithmetic by constants, unrolled runs); other sizes use the run-time-sized
-// instantiation (template argument 0).
-typedef void (*ColKernel)(ColParams);
-typedef void (*FftKernel)(FftParams);
-enum {
-    KC_STAGE, KC_PREP, KC_NLOUT, KC_PROJECT, KC_PRESSURE, KC_STAGE_MX, KC_PREP_MX,
-    KC_STAGE_CONV, KC_PREP_CONV, KC_STAGE_DIV, KC_PREP_DIV, KC_DIV, KC_PRESSURE_COEF, KC_COUNT
-};
-enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_XPASS_CONV, KF_XPASS_DIV, KF_COUNT };
 static_assert(CF_FORM_ROTATIONAL == NL_ROT && CF_FORM_CONVECTIVE == NL_CONV && CF_FORM_DIVERGENCE == NL_DIV,
               "cf_config.form values are the device form tags");
-#define CF_COL_LENGTHS(X) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384)
 
-template <int PT>
-static ColKernel col_kernel_t(int which) {
-    switch (which) {
-        case KC_STAGE: return k_column_stage<CF_NCOL, PT>;
-        case KC_PREP: return k_column_prep<CF_NCOL, PT>;
-        case KC_NLOUT: return k_column_nlout<CF_NCOL, PT>;
-        case KC_PROJECT: return k_column_project<CF_NCOL, PT>;
-        case KC_STAGE_MX: return k_column_stage_mx<CF_NCOL, PT>;
-        case KC_PREP_MX: return k_column_prep<CF_NCOL, PT, true>;
-        case KC_STAGE_CONV: return k_column_stage<CF_NCOL, PT, NL_CONV>;
-        case KC_PREP_CONV: return k_column_prep<CF_NCOL, PT, false, NL_CONV>;
-        case KC_STAGE_DIV: return k_column_stage<CF_NCOL, PT, NL_DIV>;
-        case KC_PREP_DIV: return k_column_prep<CF_NCOL, PT, false, NL_DIV>;
-        case KC_DIV: return k_column_div<CF_NCOL, PT>;
-        case KC_PRESSURE_COEF: return k_column_pressure<CF_NCOL, PT, true>;
-        default: return k_column_pressure<CF_NCOL, PT>;
-    }
-}
+// Kernel of a size: the compile-time instantiation for the sizes of the
+// supported workloads (index arithmetic by constants, unrolled runs), the
+// run-time-sized one otherwise.
 static ColKernel col_kernel(int which, int P) {
     switch (P) {
 #define CF_CASE(N) \
-    case N: return col_kernel_t<N>(which);
+    case N: return col_kernel_for<N>(which);
         CF_COL_LENGTHS(CF_CASE)
 #undef CF_CASE
-        default: return col_kernel_t<0>(which);
+        default: return col_kernel_for<0>(which);
     }
 }
-template <int L>
-static FftKernel fft_kernel_t(int which, bool f32) {
-    switch (which) {
-        case KF_ZINV: return f32 ? k_zinv<L, zf> : k_zinv<L, zd>;
-        case KF_ZFWD: return f32 ? k_zfwd<L, zf> : k_zfwd<L, zd>;
-        case KF_XPASS_CONV: return k_xpass_conv<L>;
-        case KF_XPASS_DIV: return k_xpass_div<L>;
-        default: return f32 ? k_xpass<L, zf> : k_xpass<L, zd>;
-    }
-}
-// f32: the FP32 transforms of the mixed-precision form
 static FftKernel fft_kernel(int which, int L, bool f32 = false) {
     switch (L) {
 #define CF_CASE(N) \
-    case N: return fft_kernel_t<N>(which, f32);
+    case N: return fft_kernel_for<N>(which, f32);
         CF_STATIC_FFT_LENGTHS(CF_CASE)
 #undef CF_CASE
-        default: return fft_kernel_t<0>(which, f32);
+        default: return fft_kernel_for<0>(which, f32);
     }
 }
 
@@ -306,7 +263,9 @@ static int rup8(int x) { return (x + 7) & ~7; }
 static int zbs(const cf_engine* h) { return fft_bufsz(h->Nzp) + 1; }
 static int xbs(const cf_engine* h) { return rup8(h->Nxp); }
 static size_t zsmem(const cf_engine* h) { return (size_t)2 * h->tkz * zbs(h) * sizeof(zd); }
-static size_t xsmem(const cf_engine* h) { return (size_t)12 * xbs(h) * sizeof(zd); }
+// x-pass shared memory: 12 slots (two rows of the FP32 rotational form, the
+// convective and divergence forms) or 6 (one row of the FP64 rotational form)
+static size_t xsmem(const cf_engine* h, int slots = 12) { return (size_t)slots * xbs(h) * sizeof(zd); }
 static int ilog2(int v) {
     int r = 0;
     while ((1 << (r + 1)) <= v) ++r;
@@ -548,12 +507,12 @@ struct PeriodicShape {
 static PeriodicShape periodic_shape(const cf_engine* h) {
     if (h->form == NL_CONV) return {9, 3, KF_XPASS_CONV, 1};
     if (h->form == NL_DIV) return {3, 6, KF_XPASS_DIV, 2};
-    return {6, 3, KF_XPASS, 2};
+    return {6, 3, KF_XPASS, 1};
 }
 static int launch_periodic_kernels(cf_engine* h, cudaEvent_t* ev) {
     FftParams f = fft_params(h);
     const PeriodicShape s = periodic_shape(h);
-    const size_t smz = zsmem(h), smx = xsmem(h);
+    const size_t smz = zsmem(h), smx = xsmem(h, s.xkind == KF_XPASS ? 6 : 12);
     const unsigned gzx = (unsigned)((h->Nxh + h->tkz - 1) / h->tkz);
     fft_kernel(KF_ZINV, h->Nzp)<<<dim3(gzx, (unsigned)h->Ny, s.nzinv), 256, smz, h->stream>>>(f);
     if (ev) CU(cudaEventRecord(ev[0], h->stream));
@@ -1275,14 +1234,13 @@ int cf_random_state(cf_handle* h, unsigned long long seed, double amp, int shape
     return CF_OK;
 }
 
-typedef void (*DiagKernel)(ColParams, double*);
 static DiagKernel diag_kernel(int P) {
     switch (P) {
 #define CF_CASE(N) \
-    case N: return k_column_diag<CF_NCOL, N>;
+    case N: return diag_kernel_for<N>();
         CF_COL_LENGTHS(CF_CASE)
 #undef CF_CASE
-        default: return k_column_diag<CF_NCOL, 0>;
+        default: return diag_kernel_for<0>();
     }
 }
 
@@ -1388,33 +1346,22 @@ static void host_synth(const cf_engine* h, uint64_t seed, double amp, int shape,
 // shared memory), and the classes run as parallel branches of one CUDA graph
 // per step: 12 launches per class per step, whatever the instance count.
 // ---------------------------------------------------------------------------
-typedef void (*ColBatchKernel)(const ColParams*);
-typedef void (*FftBatchKernel)(const FftParams*);
-
 static ColBatchKernel col_batch_kernel(int P) {
     switch (P) {
 #define CF_CASE(N) \
-    case N: return k_column_stage_batch<CF_NCOL, N>;
+    case N: return col_batch_kernel_for<N>();
         CF_COL_LENGTHS(CF_CASE)
 #undef CF_CASE
-        default: return k_column_stage_batch<CF_NCOL, 0>;
-    }
-}
-template <int L>
-static FftBatchKernel fft_batch_kernel_t(int which) {
-    switch (which) {
-        case KF_ZINV: return k_zinv_batch<L>;
-        case KF_ZFWD: return k_zfwd_batch<L>;
-        default: return k_xpass_batch<L>;
+        default: return col_batch_kernel_for<0>();
     }
 }
 static FftBatchKernel fft_batch_kernel(int which, int L) {
     switch (L) {
 #define CF_CASE(N) \
-    case N: return fft_batch_kernel_t<N>(which);
+    case N: return fft_batch_kernel_for<N>(which);
         CF_STATIC_FFT_LENGTHS(CF_CASE)
 #undef CF_CASE
-        default: return fft_batch_kernel_t<0>(which);
+        default: return fft_batch_kernel_for<0>(which);
     }
 }
 
@@ -1527,7 +1474,7 @@ int cf_create_batch(const cf_config* cfgs, int n, cf_batch** out) {
             c.h_col[j].resize(m);
             if ((rc = batch_alloc(b, (void**)&c.d_col[j], sizeof(ColParams) * m))) return bail(rc);
         }
-        const size_t smz = zsmem(r), smx = xsmem(r);
+        const size_t smz = zsmem(r), smx = xsmem(r, 6);
         if ((rc = raise_smem_limit(col_batch_kernel(r->P), col_smem(r))) ||
             (rc = raise_smem_limit(fft_batch_kernel(KF_ZINV, r->Nzp), smz)) ||
             (rc = raise_smem_limit(fft_batch_kernel(KF_ZFWD, r->Nzp), smz)) ||
@@ -1547,10 +1494,10 @@ int cf_create_batch(const cf_config* cfgs, int n, cf_batch** out) {
 static int launch_class_stage(const cf_batch* b, const BatchClass& c, int j, cudaStream_t s) {
     const cf_engine* r = b->inst[c.members[0]];
     const unsigned m = (unsigned)c.members.size();
-    const size_t smz = zsmem(r), smx = xsmem(r);
+    const size_t smz = zsmem(r), smx = xsmem(r, 6);
     const unsigned gzx = (unsigned)((r->Nxh + r->tkz - 1) / r->tkz);
     fft_batch_kernel(KF_ZINV, r->Nzp)<<<dim3(gzx, r->Ny, 6 * m), 256, smz, s>>>(c.d_fft);
-    fft_batch_kernel(KF_XPASS, r->Nxp)<<<dim3((r->Nzp + 1) / 2, r->Ny, m), 256, smx, s>>>(c.d_fft);
+    fft_batch_kernel(KF_XPASS, r->Nxp)<<<dim3(r->Nzp, r->Ny, m), 256, smx, s>>>(c.d_fft);
     fft_batch_kernel(KF_ZFWD, r->Nzp)<<<dim3(gzx, r->Ny, 3 * m), 256, smz, s>>>(c.d_fft);
     col_batch_kernel(r->P)<<<dim3(col_blocks(r), m), CF_NCOL * CF_TEAM, col_smem(r), s>>>(c.d_col[j]);
     CU(cudaGetLastError());

@@ -199,9 +199,10 @@ CF_DEV void xunpack(const Z* F, int bs, int nslots, int Nxh, int Nxp, const Put&
     }
 }
 
-// Rotational form.  grid: (ceil(Nzp/2), Ny); block 256; smem 12*bsx complex
-// (6 slots + scratch).  Rows zA = 2*bx and zB = 2*bx+1 of plane n.  Slots
-// 0..5 hold (u0+iu1, u2+iw0, w1+iw2) of row A at 0,2,4 and of row B at 1,3,5.
+// Rotational form, two rows per block (the FP32 transforms of the mixed
+// form).  grid: (ceil(Nzp/2), Ny); block 256; smem 12*bsx complex (6 slots +
+// scratch).  Rows zA = 2*bx and zB = 2*bx+1 of plane n.  Slots 0..5 hold
+// (u0+iu1, u2+iw0, w1+iw2) of row A at 0,2,4 and of row B at 1,3,5.
 template <int LX, class Z>
 CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
     extern __shared__ __align__(16) unsigned char fsm_raw[];
@@ -255,6 +256,44 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
         } else {
             zp_of<Z>(p, 2)[rowA + k] = X;
             if (hasB) zp_of<Z>(p, 2)[rowB + k] = Y;
+        }
+    });
+}
+
+// Rotational form, one row per block (the FP64 path: half the shared memory
+// of the two-row form, so more blocks per SM hide the FFT passes' latency).
+// grid: (Nzp, Ny); block 256; smem 6*bsx complex.  Slots 0..2 hold (u0+iu1,
+// u2+iw0, w1+iw2) of row z = bx; the products leave in (n0+in1, n2).
+template <int LX, class Z>
+CF_DEV void xpass_row_body(const FftParams& p, int z, int n) {
+    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    Z* sm = reinterpret_cast<Z*>(fsm_raw);
+    const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsx;
+    const long row = ((long)n * p.Nzp + z) * Nxh;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
+    Z* scr = sm + 3 * bs;
+    xpack(sm, bs, 3, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+        X = zp_of<Z>(p, 2 * slot)[row + k];
+        Y = zp_of<Z>(p, 2 * slot + 1)[row + k];
+    });
+    __syncthreads();
+    Z* A = group_fft_L<true, LX, 1>(sm, scr, 3, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
+    Z* Bf = (A == sm) ? scr : sm;
+    for (int j = threadIdx.x; j < Nxp; j += blockDim.x) {
+        const int sj = swz(j);
+        const Z a0 = A[0 * bs + sj], a1 = A[1 * bs + sj], a2 = A[2 * bs + sj];
+        // u = (a0.x, a0.y, a1.x), omega = (a1.y, a2.x, a2.y)
+        Bf[0 * bs + sj] = cmake<Z>(a0.y * a2.y - a1.x * a2.x, a1.x * a1.y - a0.x * a2.y);
+        Bf[1 * bs + sj] = cmake<Z>(a0.x * a2.x - a0.y * a1.y, 0.0);
+    }
+    __syncthreads();
+    const Z* F = group_fft_L<true, LX, 1>(Bf, A, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
+    xunpack(F, bs, 2, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+        if (slot == 0) {
+            zp_of<Z>(p, 0)[row + k] = X;
+            zp_of<Z>(p, 1)[row + k] = Y;
+        } else {
+            zp_of<Z>(p, 2)[row + k] = X;
         }
     });
 }
@@ -366,9 +405,11 @@ template <int LZ, class Z = zd>
 __global__ void __launch_bounds__(256) k_zfwd(FftParams p) {
     zfwd_body<LZ, Z>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
+// FP64: one row per block; FP32 (mixed form): two rows per block
 template <int LX, class Z = zd>
-__global__ void __launch_bounds__(256) k_xpass(FftParams p) {
-    xpass_body<LX, Z>(p, blockIdx.x, blockIdx.y);
+__global__ void __launch_bounds__(256, (sizeof(Z) == 16 ? 3 : 4)) k_xpass(FftParams p) {
+    if constexpr (sizeof(Z) == 16) xpass_row_body<LX, Z>(p, blockIdx.x, blockIdx.y);
+    else xpass_body<LX, Z>(p, blockIdx.x, blockIdx.y);
 }
 template <int LX>
 __global__ void __launch_bounds__(256) k_xpass_conv(FftParams p) {
@@ -394,10 +435,10 @@ __global__ void __launch_bounds__(256) k_zfwd_batch(const FftParams* __restrict_
     stage_params(&ps, pl + inst);
     zfwd_body<LZ, zd>(ps, blockIdx.x, blockIdx.y, blockIdx.z - 3 * inst);
 }
-// grid z = instances
+// grid (Nzp, Ny, instances)
 template <int LX>
-__global__ void __launch_bounds__(256) k_xpass_batch(const FftParams* __restrict__ pl) {
+__global__ void __launch_bounds__(256, 3) k_xpass_batch(const FftParams* __restrict__ pl) {
     __shared__ FftParams ps;
     stage_params(&ps, pl + blockIdx.z);
-    xpass_body<LX, zd>(ps, blockIdx.x, blockIdx.y);
+    xpass_row_body<LX, zd>(ps, blockIdx.x, blockIdx.y);
 }

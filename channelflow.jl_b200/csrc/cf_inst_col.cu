@@ -1,0 +1,38 @@
+// cf_inst_col.cu -- the column kernels of one Chebyshev length P = CF_INST_P
+// (0: the run-time-sized instantiation); compiled once per length.
+#include "cf_dispatch.h"
+
+#ifndef CF_INST_P
+#error "compile with -DCF_INST_P=<length>"
+#endif
+
+template <int P>
+ColKernel col_kernel_for(int which) {
+    switch (which) {
+        case KC_STAGE: return k_column_stage<CF_NCOL, P>;
+        case KC_PREP: return k_column_prep<CF_NCOL, P>;
+        case KC_NLOUT: return k_column_nlout<CF_NCOL, P>;
+        case KC_PROJECT: return k_column_project<CF_NCOL, P>;
+        case KC_STAGE_MX: return k_column_stage_mx<CF_NCOL, P>;
+        case KC_PREP_MX: return k_column_prep<CF_NCOL, P, true>;
+        case KC_STAGE_CONV: return k_column_stage<CF_NCOL, P, NL_CONV>;
+        case KC_PREP_CONV: return k_column_prep<CF_NCOL, P, false, NL_CONV>;
+        case KC_STAGE_DIV: return k_column_stage<CF_NCOL, P, NL_DIV>;
+        case KC_PREP_DIV: return k_column_prep<CF_NCOL, P, false, NL_DIV>;
+        case KC_DIV: return k_column_div<CF_NCOL, P>;
+        case KC_PRESSURE_COEF: return k_column_pressure<CF_NCOL, P, true>;
+        default: return k_column_pressure<CF_NCOL, P>;
+    }
+}
+template <int P>
+DiagKernel diag_kernel_for() {
+    return k_column_diag<CF_NCOL, P>;
+}
+template <int P>
+ColBatchKernel col_batch_kernel_for() {
+    return k_column_stage_batch<CF_NCOL, P>;
+}
+
+template ColKernel col_kernel_for<CF_INST_P>(int);
+template DiagKernel diag_kernel_for<CF_INST_P>();
+template ColBatchKernel col_batch_kernel_for<CF_INST_P>();

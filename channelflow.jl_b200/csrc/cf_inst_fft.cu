@@ -1,0 +1,29 @@
+// cf_inst_fft.cu -- the periodic-transform kernels of one padded length
+// L = CF_INST_L (0: the run-time-sized instantiation); compiled once per length.
+#include "cf_dispatch.h"
+
+#ifndef CF_INST_L
+#error "compile with -DCF_INST_L=<length>"
+#endif
+
+template <int L>
+FftKernel fft_kernel_for(int which, bool f32) {
+    switch (which) {
+        case KF_ZINV: return f32 ? k_zinv<L, zf> : k_zinv<L, zd>;
+        case KF_ZFWD: return f32 ? k_zfwd<L, zf> : k_zfwd<L, zd>;
+        case KF_XPASS_CONV: return k_xpass_conv<L>;
+        case KF_XPASS_DIV: return k_xpass_div<L>;
+        default: return f32 ? k_xpass<L, zf> : k_xpass<L, zd>;
+    }
+}
+template <int L>
+FftBatchKernel fft_batch_kernel_for(int which) {
+    switch (which) {
+        case KF_ZINV: return k_zinv_batch<L>;
+        case KF_ZFWD: return k_zfwd_batch<L>;
+        default: return k_xpass_batch<L>;
+    }
+}
+
+template FftKernel fft_kernel_for<CF_INST_L>(int, bool);
+template FftBatchKernel fft_batch_kernel_for<CF_INST_L>(int);
