@@ -70,7 +70,7 @@ CF_DEV zd warp_excl_z(zd inc, int lane) {
 
 // b = D a  (b != a).  Warp q writes the degrees of parity q of b from the
 // degrees of parity 1-q of a; b_P = 0.
-CF_DEV void col_diff(const zd* a, zd* b, const Team& t) {
+CF_DEV_NOINLINE void col_diff(const zd* a, zd* b, const Team t) {
     const int P = t.P, hs = t.hs, q = t.q, lane = t.lane;
     const int pin = 1 - q;                 // parity of the input chain
     const int top = pin ? P - 1 : P;       // m = top, top-2, ..., pin
@@ -98,24 +98,31 @@ CF_DEV void col_diff(const zd* a, zd* b, const Team& t) {
     tsync(t);
 }
 
-// Warp q copies the parity-q entries of `rows` rows of Ny doubles (global,
-// natural order, row stride Ny) into shared memory in the parity layout (row
-// stride 2*hs).  Only warp q reads them afterwards, so a warp barrier suffices.
-CF_DEV void col_stage_rows(double* dst, const double* __restrict__ src, int rows, const Team& t) {
+// The three elimination factor rows of a column (alpha, invden, W: src,
+// src + Ny, src + 2 Ny; Ny doubles each, natural order) into shared memory in
+// the parity layout: alpha and invden at fa and fa + 2 hs, W at fw.  Warp q
+// copies its parity; all loads of a lane are issued before its first store
+// (one memory round trip for P <= 318).  Only warp q reads them afterwards,
+// so a warp barrier suffices.
+CF_DEV void col_stage_factors(double* fa, double* fw, const double* __restrict__ src, const Team& t) {
     const int P = t.P, Ny = P + 1, hs = t.hs, q = t.q;
     const int nq = pcount(q, P);
-    for (int r = 0; r < rows; ++r) {
-        double v[8];
-        for (int base = t.lane; base < nq; base += 8 * 32) {
+    for (int base = t.lane; base < nq; base += 5 * 32) {
+        double v[3][5];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int u = 0; u < 5; ++u) {
                 const int j = base + 32 * u;
-                v[u] = j < nq ? __ldg(src + (long)r * Ny + 2 * j + q) : 0.0;
+                v[r][u] = j < nq ? __ldg(src + (long)r * Ny + 2 * j + q) : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int j = base + 32 * u;
-                if (j < nq) dst[r * 2 * hs + q * hs + j] = v[u];
+        for (int u = 0; u < 5; ++u) {
+            const int j = base + 32 * u;
+            if (j < nq) {
+                fa[q * hs + j] = v[0][u];
+                fa[2 * hs + q * hs + j] = v[1][u];
+                fw[q * hs + j] = v[2][u];
             }
         }
     }
@@ -136,12 +143,12 @@ CF_DEV zd helm_g(const zd* fh, const double* __restrict__ gt, int n, int P) {
 
 // Tau Helmholtz solve: x holds f on entry and a on exit; scr (distinct) holds
 // the intermediate beta.  alpha, invden, W are the column's elimination
-// factors in the parity layout (shared memory, staged by col_stage_rows);
+// factors in the parity layout (shared memory, staged by col_stage_factors);
 // SA0/SA1 and bc0/bc1 are the wall-row sums and data of the two parities.
 // Warp q solves the parity-q system alone.
-CF_DEV void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
-                     const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
-                     const Team& t) {
+CF_DEV_NOINLINE void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
+                              const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
+                              const Team t) {
     const int P = t.P, Ny = P + 1, q = t.q, lane = t.lane, hs = t.hs;
     const int top = q ? P - 1 : P;
     const int cnt = (top - q) / 2;  // backward chain n = top, top-2, ..., q+2
@@ -225,6 +232,11 @@ CF_DEV void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, 
 // Both are folded into the z staging (the transform is linear).
 #define CF_DCT_FWD 1
 #define CF_DCT_INV 2
+// the team's complex FFT of length P (shared by both transform modes)
+template <int PL>
+CF_DEV_NOINLINE const zd* col_team_fft(zd* z, zd* z2, const FftPlan pl, const Team t) {
+    return group_fft_L<true, PL>(z, z2, 1, fft_bufsz(t.P), pl, -1, t.tid, CF_TEAM, t.bar);
+}
 template <int PL, int MODE>
 CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const FftPlan& pl, double scale,
                         const Team& t) {
@@ -253,7 +265,7 @@ CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const F
     if (t.lane == 0) t.xch[t.q] = x1;
     tsync(t);
     x1 = zadd(t.xch[0], t.xch[1]);
-    const zd* Z = group_fft_L<true, PL>(z, z2, 1, fft_bufsz(P), pl, -1, t.tid, CF_TEAM, t.bar);
+    const zd* Z = col_team_fft<PL>(z, z2, pl, t);
     if (t.q == 1) {
         // odd outputs X_{2m+1}, m = 0..H-1: X_1 plus prefix sums of
         // i (Z_m - Z_{P-m}), in runs of E (odd) consecutive m per lane

@@ -4,6 +4,11 @@
 #include <stdint.h>
 
 #define CF_DEV __device__ __forceinline__
+// Helpers called from many sites of the column kernels: one out-of-line copy
+// each keeps a kernel's instructions within the instruction caches (inlined at
+// every site, the column stage kernel stalled on instruction fetch).  Static:
+// every translation unit keeps its own copy.
+#define CF_DEV_NOINLINE static __device__ __noinline__
 
 // Nonlinear forms of NonLinearTerm (src/nonlinear.jl:10-17); the values of
 // cf_config.form.

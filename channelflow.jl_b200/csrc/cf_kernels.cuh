@@ -120,9 +120,9 @@ template <>
 CF_DEV zf from_zd<zf>(zd a) { return to_zf(a); }
 
 template <int NCOL, class G>
-CF_DEV void tile_load(zd* sm, int cs, int hs, const G* g, int c0, const ColParams& p) {
+CF_DEV_NOINLINE void tile_load(zd* sm, int cs, int hs, const G* g, int c0, int Ny, int B) {
     constexpr int NT = NCOL * CF_TEAM, K = 8;
-    const int tot = p.Ny * NCOL;
+    const int tot = Ny * NCOL;
     for (int base = threadIdx.x; base < tot; base += NT * K) {
         zd v[K];
 #pragma unroll
@@ -130,7 +130,7 @@ CF_DEV void tile_load(zd* sm, int cs, int hs, const G* g, int c0, const ColParam
             const int e = base + u * NT;
             const int n = e / NCOL, t = e - n * NCOL;
             const int c = c0 + t;
-            v[u] = (e < tot && c < p.B) ? to_zd(g[(long)n * p.B + c]) : zzero();
+            v[u] = (e < tot && c < B) ? to_zd(g[(long)n * B + c]) : zzero();
         }
 #pragma unroll
         for (int u = 0; u < K; ++u) {
@@ -147,12 +147,12 @@ CF_DEV void tile_prefetch(const G* g, int c0, const ColParams& p) {
         asm volatile("prefetch.global.L2 [%0];" ::"l"(g + (long)n * p.B + c0));
 }
 template <int NCOL, class G>
-CF_DEV void tile_store(const zd* sm, int cs, int hs, G* __restrict__ g, int c0, const ColParams& p) {
-    const int tot = p.Ny * NCOL;
+CF_DEV_NOINLINE void tile_store(const zd* sm, int cs, int hs, G* __restrict__ g, int c0, int Ny, int B) {
+    const int tot = Ny * NCOL;
     for (int e = threadIdx.x; e < tot; e += NCOL * CF_TEAM) {
         const int n = e / NCOL, t = e - n * NCOL;
         const int c = c0 + t;
-        if (c < p.B) g[(long)n * p.B + c] = from_zd<G>(sm[t * cs + ppos(n, hs)]);
+        if (c < B) g[(long)n * B + c] = from_zd<G>(sm[t * cs + ppos(n, hs)]);
     }
 }
 
@@ -211,8 +211,7 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         for (int it = 0; it < 2; ++it) {
             const double* fsrc = it ? fv : bk.fac_p + (long)c * 3 * Ny;
             zd* x = it ? V : PT;
-            col_stage_rows(fa, fsrc, 2, t);
-            col_stage_rows(fw, fsrc + 2 * Ny, 1, t);
+            col_stage_factors(fa, fw, fsrc, t);
             col_diff(it ? PT : R1, x, t);
             for (int j = lane; j < nq; j += 32) {
                 const int o = qo + j;
@@ -280,10 +279,7 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         R2[o] = zsub(zmulis(PT[o], l), R2[o]);
     }
     __syncwarp();
-    if (c == 0) {
-        col_stage_rows(fa, fv, 2, t);
-        col_stage_rows(fw, fv + 2 * Ny, 1, t);
-    }
+    if (c == 0) col_stage_factors(fa, fw, fv, t);
 #pragma unroll 1
     for (int j = 0; j < 2; ++j)
         col_helm(j ? R2 : R0, A, fa, fi, fw, p.helm_tab, __ldg(sa + 2), __ldg(sa + 3), shift, zzero(), zzero(), t);
@@ -335,7 +331,7 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
         for (int j = lane; j < nq; j += 32) {
             const int o = qo + j;
             W0[o] = zsub(W0[o], zmulis(U1[o], l));
-            W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
+            if (MX) W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
             W2[o] = zsub(zmulis(U1[o], k), W2[o]);
         }
         tsync(t);
@@ -344,11 +340,21 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
         for (int i = 0; i < 3; ++i) col_diff(sel3(U0, U1, U2, i), sel3(W0, W1, W2, i), t);
     }
     if (MX) return;
+    // omega_y = i (l u - k w) is formed from the nodal u and w below (the
+    // transform is linear): five transforms for the rotational form
     constexpr int NF = FORM == NL_DIV ? 3 : 6;
 #pragma unroll 1
     for (int i = 0; i < NF; ++i) {
+        if (FORM == NL_ROT && i == 4) continue;
         zd* x = i < 3 ? sel3(U0, U1, U2, i) : sel3(W0, W1, W2, i - 3);
         col_inverse_y<PL>(x, Z, Z2, p, t);
+    }
+    if (FORM == NL_ROT) {
+        for (int j = lane; j < nq; j += 32) {
+            const int o = qo + j;
+            W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
+        }
+        tsync(t);
     }
 }
 
@@ -363,17 +369,17 @@ CF_DEV void store_six(const Ctx& X, const ColParams& p, int r0, int r1, int r2, 
     const int rr[6] = {r0, r1, r2, r3, r4, r5};
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        if (MX) tile_store<NCOL>(X.reg(rr[i]), cs, hs, reinterpret_cast<zf*>(p.nod[i]), c0, p);
-        else tile_store<NCOL>(X.reg(rr[i]), cs, hs, p.nod[i], c0, p);
+        if (MX) tile_store<NCOL>(X.reg(rr[i]), cs, hs, reinterpret_cast<zf*>(p.nod[i]), c0, p.Ny, p.B);
+        else tile_store<NCOL>(X.reg(rr[i]), cs, hs, p.nod[i], c0, p.Ny, p.B);
     }
 }
 
 // the three nodal fields u, v, w from regions r0..r2 to p.nod (divergence form)
 template <int NCOL, class Ctx>
 CF_DEV void store_three(const Ctx& X, const ColParams& p, int r0, int r1, int r2) {
-    tile_store<NCOL>(X.reg(r0), X.cs, X.t.hs, p.nod[0], X.c0, p);
-    tile_store<NCOL>(X.reg(r1), X.cs, X.t.hs, p.nod[1], X.c0, p);
-    tile_store<NCOL>(X.reg(r2), X.cs, X.t.hs, p.nod[2], X.c0, p);
+    tile_store<NCOL>(X.reg(r0), X.cs, X.t.hs, p.nod[0], X.c0, p.Ny, p.B);
+    tile_store<NCOL>(X.reg(r1), X.cs, X.t.hs, p.nod[1], X.c0, p.Ny, p.B);
+    tile_store<NCOL>(X.reg(r2), X.cs, X.t.hs, p.nod[2], X.c0, p.Ny, p.B);
 }
 
 // MX: mixed-precision form.  The nonlinear term arrives as FP32 Chebyshev
@@ -418,7 +424,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     // The three components run through one copy of the loop body (pointers
     // selected, not indexed): the kernel's issue rate is limited by its
     // instruction footprint, so the body is not unrolled.
-    tile_load<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p);
+    tile_load<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
     double gold[2] = {p.c1, p.c2};
     zd bulkN0 = zzero(), bulkN2 = zzero(), wR0 = zzero(), wL0 = zzero(), wR2 = zzero(), wL2 = zzero();
 #pragma unroll 1
@@ -426,9 +432,9 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         const zd* Nn_i = sel3(p.Nn[0], p.Nn[1], p.Nn[2], i);
         zd* Q_i = sel3(p.Q[0], p.Q[1], p.Q[2], i);
         zd* U_i = sel3(p.U[0], p.U[1], p.U[2], i);
-        if (MX) tile_load<NCOL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p);
-        else tile_load<NCOL>(X.reg(4), cs, hs, Nn_i, c0, p);
-        if (p.stage > 0) tile_load<NCOL>(X.reg(5), cs, hs, Q_i, c0, p);
+        if (MX) tile_load<NCOL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
+        else tile_load<NCOL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
+        if (p.stage > 0) tile_load<NCOL>(X.reg(5), cs, hs, Q_i, c0, p.Ny, p.B);
         __syncthreads();
         if (valid) {
             if (!NCOEF) {
@@ -449,8 +455,8 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
             }
         }
         __syncthreads();
-        if (p.store_q) tile_store<NCOL>(X.reg(4), cs, hs, Q_i, c0, p);
-        tile_load<NCOL>(X.reg(5), cs, hs, U_i, c0, p);
+        if (p.store_q) tile_store<NCOL>(X.reg(4), cs, hs, Q_i, c0, p.Ny, p.B);
+        tile_load<NCOL>(X.reg(5), cs, hs, U_i, c0, p.Ny, p.B);
         __syncthreads();
         if (valid) {
             zd* U = X.col(5);
@@ -520,10 +526,10 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         }
     }
     __syncthreads();
-    tile_store<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p);
-    tile_store<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p);
-    tile_store<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p);
-    tile_store<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p);
+    tile_store<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+    tile_store<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_store<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+    tile_store<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
     __syncthreads();
     // ---------------- Phase C: total velocity, vorticity, nodal values
     if (valid)
@@ -562,9 +568,9 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
     const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
-    tile_load<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p);
-    tile_load<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p);
-    tile_load<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p);
+    tile_load<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+    tile_load<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_load<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
     __syncthreads();
     if (X.valid)
         col_prep_nodal<PL, MX, FORM>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7),
@@ -587,7 +593,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const Team& t = X.t;
     const int cs = X.cs, hs = t.hs, c0 = X.c0, qo = t.q * hs, nq = pcount(t.q, t.P);
 #pragma unroll
-    for (int m = 0; m < 6; ++m) tile_load<NCOL>(X.reg(m), cs, hs, p.nod[m], c0, p);
+    for (int m = 0; m < 6; ++m) tile_load<NCOL>(X.reg(m), cs, hs, p.nod[m], c0, p.Ny, p.B);
     __syncthreads();
     if (X.valid) {
         const bool nyq = col_nyquist(p, X.ix, X.iz);
@@ -614,9 +620,9 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
         }
     }
     __syncthreads();
-    tile_store<NCOL>(X.reg(0), cs, hs, p.Nout[0], c0, p);
-    tile_store<NCOL>(X.reg(3), cs, hs, p.Nout[1], c0, p);
-    tile_store<NCOL>(X.reg(5), cs, hs, p.Nout[2], c0, p);
+    tile_store<NCOL>(X.reg(0), cs, hs, p.Nout[0], c0, p.Ny, p.B);
+    tile_store<NCOL>(X.reg(3), cs, hs, p.Nout[1], c0, p.Ny, p.B);
+    tile_store<NCOL>(X.reg(5), cs, hs, p.Nout[2], c0, p.Ny, p.B);
 }
 
 // Forward DCT of the nonlinear term only: coefficients into p.Nout.
@@ -628,11 +634,11 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const bool nyq = X.valid ? col_nyquist(p, X.ix, X.iz) : true;
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        tile_load<NCOL>(X.reg(0), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p);
+        tile_load<NCOL>(X.reg(0), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p.Ny, p.B);
         __syncthreads();
         if (X.valid) col_forward_y<PL>(X.col(0), X.col(6), X.col(7), p, nyq, X.t);
         __syncthreads();
-        tile_store<NCOL>(X.reg(0), cs, hs, sel3(p.Nout[0], p.Nout[1], p.Nout[2], i), c0, p);
+        tile_store<NCOL>(X.reg(0), cs, hs, sel3(p.Nout[0], p.Nout[1], p.Nout[2], i), c0, p.Ny, p.B);
         __syncthreads();
     }
 }
@@ -650,7 +656,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const double kap2 = k * k + l * l;
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        tile_load<NCOL>(X.reg(5), cs, hs, sel3(p.U[0], p.U[1], p.U[2], i), c0, p);
+        tile_load<NCOL>(X.reg(5), cs, hs, sel3(p.U[0], p.U[1], p.U[2], i), c0, p.Ny, p.B);
         __syncthreads();
         if (X.valid) {
             zd* U = X.col(5);
@@ -673,9 +679,9 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
         }
     }
     __syncthreads();
-    tile_store<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p);
-    tile_store<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p);
-    tile_store<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p);
+    tile_store<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+    tile_store<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_store<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
 }
 
 // Pressure reconstruction (pressure.jl:115-204) from the nonlinear term at
@@ -692,12 +698,12 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const bool nyq = X.valid ? col_nyquist(p, X.ix, X.iz) : true;
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        tile_load<NCOL>(X.reg(i), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p);
+        tile_load<NCOL>(X.reg(i), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p.Ny, p.B);
         __syncthreads();
         if (X.valid && !NCOEF) col_forward_y<PL>(X.col(i), X.col(6), X.col(7), p, nyq, t);
         __syncthreads();
     }
-    tile_load<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p);
+    tile_load<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
     __syncthreads();
     if (X.valid) {
         const double k = p.ax * X.ix;
@@ -745,14 +751,13 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
             const double* fpn = p.bank.fac_p + (long)c * 3 * p.Ny;
             double* fa = reinterpret_cast<double*>(X.col(6));
             double* fw = reinterpret_cast<double*>(X.col(7));
-            col_stage_rows(fa, fpn, 2, t);
-            col_stage_rows(fw, fpn + 2 * p.Ny, 1, t);
+            col_stage_factors(fa, fw, fpn, t);
             col_helm(PT, X.col(5), fa, fa + 2 * hs, fw, p.helm_tab, __ldg(sa + 0), __ldg(sa + 1), k * k + l * l,
                      zscale(zsub(up, lo), 0.5), zscale(zadd(up, lo), 0.5), t);
         }
     }
     __syncthreads();
-    tile_store<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p);
+    tile_store<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
 }
 
 // Diagnostics of the perturbation velocity on the device (postprocessing.jl:
@@ -790,9 +795,9 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const Team& t = X.t;
     const int cs = X.cs, hs = t.hs, c0 = X.c0, q = t.q, lane = t.lane, P = t.P;
     const int qo = q * hs, nq = pcount(q, P);
-    tile_load<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p);
-    tile_load<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p);
-    tile_load<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p);
+    tile_load<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+    tile_load<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_load<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
     double* mom = reinterpret_cast<double*>(X.reg(6));
     for (int j = threadIdx.x; j <= 2 * P; j += NCOL * CF_TEAM)
         mom[j] = (j & 1) ? 0.0 : 1.0 / (1.0 - (double)j * j);
