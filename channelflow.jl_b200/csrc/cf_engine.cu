@@ -263,9 +263,12 @@ static int rup8(int x) { return (x + 7) & ~7; }
 static int zbs(const cf_engine* h) { return fft_bufsz(h->Nzp) + 1; }
 static int xbs(const cf_engine* h) { return rup8(h->Nxp); }
 static size_t zsmem(const cf_engine* h) { return (size_t)2 * h->tkz * zbs(h) * sizeof(zd); }
-// x-pass shared memory: 12 slots (two rows of the FP32 rotational form, the
-// convective and divergence forms) or 6 (one row of the FP64 rotational form)
-static size_t xsmem(const cf_engine* h, int slots = 12) { return (size_t)slots * xbs(h) * sizeof(zd); }
+// x-pass shared memory: 12 slots of round_up(Nxp, 8) (two rows of the FP32
+// rotational form, the convective and divergence forms), or 6 slots of
+// fft_bufsz(Nxp) (one row of the FP64 rotational form)
+static size_t xsmem(const cf_engine* h, int slots = 12) {
+    return (size_t)slots * (slots == 6 ? fft_bufsz(h->Nxp) : xbs(h)) * sizeof(zd);
+}
 static int ilog2(int v) {
     int r = 0;
     while ((1 << (r + 1)) <= v) ++r;
@@ -490,6 +493,7 @@ static FftParams fft_params(const cf_engine* h) {
     f.tks = ilog2(h->tkz);
     f.bsz = zbs(h);
     f.bsx = xbs(h);
+    f.bsxp = fft_bufsz(h->Nxp);
     f.ax = 2 * M_PI / h->Lx; f.bz = 2 * M_PI / h->Lz;
     f.nod0 = h->nod[0]; f.nod1 = h->nod[1]; f.nod2 = h->nod[2]; f.nod3 = h->nod[3]; f.nod4 = h->nod[4]; f.nod5 = h->nod[5];
     f.zp0 = h->zp[0]; f.zp1 = h->zp[1]; f.zp2 = h->zp[2]; f.zp3 = h->zp[3]; f.zp4 = h->zp[4]; f.zp5 = h->zp[5];
@@ -798,7 +802,7 @@ static int raise_smem_limit(K* fn, size_t need) {
 
 static int set_attrs(cf_engine* h) {
     const int maxsm = 227 * 1024;
-    size_t need[3] = {col_smem(h), zsmem(h), xsmem(h)};
+    size_t need[3] = {col_smem(h), zsmem(h), std::max(xsmem(h), xsmem(h, 6))};
     for (size_t x : need)
         if (x > (size_t)maxsm) return fail(CF_E_UNSUPPORTED, "grid too large for the shared-memory tiles");
     int rc;

@@ -22,6 +22,7 @@ struct FftParams {
     int tks;       // log2 of the columns per block in the z kernels
     int bsz, bsx;  // transform buffer strides: fft_bufsz(Nzp) + 1 (odd, padded layout),
                    // round_up(Nxp, 8) (XOR-swizzled layout: 12 buffers of the x-pass)
+    int bsxp;      // fft_bufsz(Nxp): padded layout of the one-row FP64 x-pass
     double ax, bz;  // 2 pi / Lx, 2 pi / Lz (derivatives of the convective form)
     // nodal and z-padded fields: complex double (FP64 path) or complex float
     // (FP32 transforms of the mixed-precision path)
@@ -153,8 +154,9 @@ CF_DEV void zfwd_body(const FftParams& p, int bx, int n, int f) {
 // Pack nslots transform slots from pairs of real rows given by their half
 // spectra X, Y (get(slot, k, X, Y) for k < Nxh, Nyquist excluded; zero
 // elsewhere): Z_k = X_k + i Y_k, Z_{Nxp-k} = conj(X_k) + i conj(Y_k).  Every
-// position 0..Nxp-1 of the slots is written.  Block of 256 threads.
-template <class Z, class Get>
+// position 0..Nxp-1 of the slots is written.  Block of 256 threads.  POS: the
+// slots' layout (cf_fft.cuh bpos: 0 padded, 1 XOR-swizzled).
+template <class Z, int POS = 1, class Get>
 CF_DEV void xpack(Z* sm, int bs, int nslots, int Nxh, int Nxp, int xnyq, const Get& get) {
     const int Nxhp = Nxp / 2 + 1, tot = nslots * Nxhp;
     for (int base = threadIdx.x; base < tot; base += 4 * 256) {
@@ -174,12 +176,12 @@ CF_DEV void xpack(Z* sm, int bs, int nslots, int Nxh, int Nxp, int xnyq, const G
             const int slot = e / Nxhp, k = e - slot * Nxhp;
             Z* s = sm + slot * bs;
             if (k == 0) {
-                s[swz(0)] = cmake<Z>(X[u].x, Y[u].x);
+                s[bpos<POS>(0)] = cmake<Z>(X[u].x, Y[u].x);
             } else if (2 * k == Nxp) {
-                s[swz(k)] = cmake<Z>(X[u].x, Y[u].x);
+                s[bpos<POS>(k)] = cmake<Z>(X[u].x, Y[u].x);
             } else {
-                s[swz(k)] = cmake<Z>(X[u].x - Y[u].y, X[u].y + Y[u].x);
-                s[swz(Nxp - k)] = cmake<Z>(X[u].x + Y[u].y, Y[u].x - X[u].y);
+                s[bpos<POS>(k)] = cmake<Z>(X[u].x - Y[u].y, X[u].y + Y[u].x);
+                s[bpos<POS>(Nxp - k)] = cmake<Z>(X[u].x + Y[u].y, Y[u].x - X[u].y);
             }
         }
     }
@@ -188,12 +190,12 @@ CF_DEV void xpack(Z* sm, int bs, int nslots, int Nxh, int Nxp, int xnyq, const G
 // Separate nslots forward-transformed slots into the half spectra of their
 // two real rows, X = (Z_k + conj Z_-k)/2, Y = (Z_k - conj Z_-k)/(2i), and
 // hand them to put(slot, k, X, Y) for k < Nxh (the x truncation).
-template <class Z, class Put>
+template <class Z, int POS = 1, class Put>
 CF_DEV void xunpack(const Z* F, int bs, int nslots, int Nxh, int Nxp, const Put& put) {
     for (int e = threadIdx.x; e < nslots * Nxh; e += blockDim.x) {
         const int slot = e / Nxh, k = e - slot * Nxh;
         const Z* s = F + slot * bs;
-        Z Zk = s[swz(k)], Zm = s[swz((Nxp - k) % Nxp)];
+        Z Zk = s[bpos<POS>(k)], Zm = s[bpos<POS>((Nxp - k) % Nxp)];
         put(slot, k, cmake<Z>(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y)),
             cmake<Z>(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x)));
     }
@@ -261,34 +263,35 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
 }
 
 // Rotational form, one row per block (the FP64 path: half the shared memory
-// of the two-row form, so more blocks per SM hide the FFT passes' latency).
-// grid: (Nzp, Ny); block 256; smem 6*bsx complex.  Slots 0..2 hold (u0+iu1,
+// of the two-row form, so more blocks per SM hide the FFT passes' latency, in
+// the padded layout, whose strided butterfly positions are constant offsets).
+// grid: (Nzp, Ny); block 256; smem 6*bsxp complex.  Slots 0..2 hold (u0+iu1,
 // u2+iw0, w1+iw2) of row z = bx; the products leave in (n0+in1, n2).
 template <int LX, class Z>
 CF_DEV void xpass_row_body(const FftParams& p, int z, int n) {
     extern __shared__ __align__(16) unsigned char fsm_raw[];
     Z* sm = reinterpret_cast<Z*>(fsm_raw);
-    const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsx;
+    const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsxp;
     const long row = ((long)n * p.Nzp + z) * Nxh;
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
     Z* scr = sm + 3 * bs;
-    xpack(sm, bs, 3, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+    xpack<Z, 0>(sm, bs, 3, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
         X = zp_of<Z>(p, 2 * slot)[row + k];
         Y = zp_of<Z>(p, 2 * slot + 1)[row + k];
     });
     __syncthreads();
-    Z* A = group_fft_L<true, LX, 1>(sm, scr, 3, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
+    Z* A = group_fft_L<true, LX, 0>(sm, scr, 3, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
     Z* Bf = (A == sm) ? scr : sm;
     for (int j = threadIdx.x; j < Nxp; j += blockDim.x) {
-        const int sj = swz(j);
+        const int sj = fpos(j);
         const Z a0 = A[0 * bs + sj], a1 = A[1 * bs + sj], a2 = A[2 * bs + sj];
         // u = (a0.x, a0.y, a1.x), omega = (a1.y, a2.x, a2.y)
         Bf[0 * bs + sj] = cmake<Z>(a0.y * a2.y - a1.x * a2.x, a1.x * a1.y - a0.x * a2.y);
         Bf[1 * bs + sj] = cmake<Z>(a0.x * a2.x - a0.y * a1.y, 0.0);
     }
     __syncthreads();
-    const Z* F = group_fft_L<true, LX, 1>(Bf, A, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    xunpack(F, bs, 2, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+    const Z* F = group_fft_L<true, LX, 0>(Bf, A, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
+    xunpack<Z, 0>(F, bs, 2, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
         if (slot == 0) {
             zp_of<Z>(p, 0)[row + k] = X;
             zp_of<Z>(p, 1)[row + k] = Y;
