@@ -140,6 +140,28 @@ CF_DEV_NOINLINE void tile_load(zd* sm, int cs, int hs, const G* g, int c0, int N
         }
     }
 }
+// The same tile of FP64 coefficients copied asynchronously (16-byte cp.async
+// per complex, zero fill outside the grid): the call only issues the copies,
+// so several tiles are in flight together; tile_wait() completes all of a
+// thread's issued copies (a __syncthreads must follow before other threads
+// read them).
+template <int NCOL>
+CF_DEV_NOINLINE void tile_load_async(zd* sm, int cs, int hs, const zd* g, int c0, int Ny, int B) {
+    constexpr int NT = NCOL * CF_TEAM;
+    const int tot = Ny * NCOL;
+    for (int e = threadIdx.x; e < tot; e += NT) {
+        const int n = e / NCOL, t = e - n * NCOL;
+        const int c = c0 + t;
+        const bool ok = c < B;
+        const zd* src = ok ? g + (long)n * B + c : g;
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(sm + t * cs + ppos(n, hs));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(ok ? 16 : 0)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+CF_DEV void tile_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // L2 prefetch of a tile's rows (one 32-byte row segment per degree)
 template <int NCOL, class G>
 CF_DEV void tile_prefetch(const G* g, int c0, const ColParams& p) {
@@ -424,7 +446,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     // The three components run through one copy of the loop body (pointers
     // selected, not indexed): the kernel's issue rate is limited by its
     // instruction footprint, so the body is not unrolled.
-    tile_load<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
+    tile_load_async<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);  // completed with N_0
     double gold[2] = {p.c1, p.c2};
     zd bulkN0 = zzero(), bulkN2 = zzero(), wR0 = zzero(), wL0 = zzero(), wR2 = zzero(), wL2 = zzero();
 #pragma unroll 1
@@ -432,9 +454,10 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         const zd* Nn_i = sel3(p.Nn[0], p.Nn[1], p.Nn[2], i);
         zd* Q_i = sel3(p.Q[0], p.Q[1], p.Q[2], i);
         zd* U_i = sel3(p.U[0], p.U[1], p.U[2], i);
+        if (p.stage > 0) tile_load_async<NCOL>(X.reg(5), cs, hs, Q_i, c0, p.Ny, p.B);
         if (MX) tile_load<NCOL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
-        else tile_load<NCOL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
-        if (p.stage > 0) tile_load<NCOL>(X.reg(5), cs, hs, Q_i, c0, p.Ny, p.B);
+        else tile_load_async<NCOL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
+        tile_wait();
         __syncthreads();
         if (valid) {
             if (!NCOEF) {
@@ -456,7 +479,8 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         }
         __syncthreads();
         if (p.store_q) tile_store<NCOL>(X.reg(4), cs, hs, Q_i, c0, p.Ny, p.B);
-        tile_load<NCOL>(X.reg(5), cs, hs, U_i, c0, p.Ny, p.B);
+        tile_load_async<NCOL>(X.reg(5), cs, hs, U_i, c0, p.Ny, p.B);
+        tile_wait();
         __syncthreads();
         if (valid) {
             zd* U = X.col(5);
@@ -568,9 +592,10 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
     const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
-    tile_load<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
-    tile_load<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
-    tile_load<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+    tile_load_async<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+    tile_load_async<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_load_async<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+    tile_wait();
     __syncthreads();
     if (X.valid)
         col_prep_nodal<PL, MX, FORM>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7),
@@ -593,7 +618,8 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const Team& t = X.t;
     const int cs = X.cs, hs = t.hs, c0 = X.c0, qo = t.q * hs, nq = pcount(t.q, t.P);
 #pragma unroll
-    for (int m = 0; m < 6; ++m) tile_load<NCOL>(X.reg(m), cs, hs, p.nod[m], c0, p.Ny, p.B);
+    for (int m = 0; m < 6; ++m) tile_load_async<NCOL>(X.reg(m), cs, hs, p.nod[m], c0, p.Ny, p.B);
+    tile_wait();
     __syncthreads();
     if (X.valid) {
         const bool nyq = col_nyquist(p, X.ix, X.iz);
@@ -795,9 +821,10 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const Team& t = X.t;
     const int cs = X.cs, hs = t.hs, c0 = X.c0, q = t.q, lane = t.lane, P = t.P;
     const int qo = q * hs, nq = pcount(q, P);
-    tile_load<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
-    tile_load<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
-    tile_load<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+    tile_load_async<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+    tile_load_async<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_load_async<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+    tile_wait();
     double* mom = reinterpret_cast<double*>(X.reg(6));
     for (int j = threadIdx.x; j <= 2 * P; j += NCOL * CF_TEAM)
         mom[j] = (j & 1) ? 0.0 : 1.0 / (1.0 - (double)j * j);
