@@ -61,15 +61,6 @@ CF_DEV zd to_zd(zd a) { return a; }
 CF_DEV zd to_zd(zf a) { return make_double2((double)a.x, (double)a.y); }
 CF_DEV zf to_zf(zd a) { return make_float2((float)a.x, (float)a.y); }
 
-// ----------------------------------------------------------- L2 prefetch
-// Bring [p, p+bytes) into L2 (one request per 128-byte line, spread over the
-// calling threads) so that later dependent loads see L2 rather than HBM latency.
-CF_DEV void prefetch_l2(const void* p, long bytes, int tid, int nth) {
-    const char* c = (const char*)p;
-    for (long off = (long)tid * 128; off < bytes; off += (long)nth * 128)
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(c + off));
-}
-
 // Copy of one instance's parameters into shared memory (batched launches:
 // the block's instance is picked by a grid coordinate).
 template <class T>

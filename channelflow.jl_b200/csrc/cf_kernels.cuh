@@ -162,12 +162,6 @@ CF_DEV_NOINLINE void tile_load_async(zd* sm, int cs, int hs, const zd* g, int c0
 }
 CF_DEV void tile_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// L2 prefetch of a tile's rows (one 32-byte row segment per degree)
-template <int NCOL, class G>
-CF_DEV void tile_prefetch(const G* g, int c0, const ColParams& p) {
-    for (int n = threadIdx.x; n < p.Ny; n += NCOL * CF_TEAM)
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(g + (long)n * p.B + c0));
-}
 template <int NCOL, class G>
 CF_DEV_NOINLINE void tile_store(const zd* sm, int cs, int hs, G* __restrict__ g, int c0, int Ny, int B) {
     const int tot = Ny * NCOL;
@@ -424,24 +418,6 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     const double l = p.bz * (X.iz <= (p.Nz >> 1) ? X.iz : X.iz - p.Nz);
     const double kap2 = k * k + l * l;
 
-    // Every input of this block is requested from L2 up front: the rows of
-    // the tiles read below and the columns' Stokes factors and responses
-    // (column-contiguous), so the dependent loads later see L2 latency.
-    {
-        constexpr int NT = NCOL * CF_TEAM;
-        tile_prefetch<NCOL>(p.Pf, c0, p);
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            if (MX) tile_prefetch<NCOL>(reinterpret_cast<const zf*>(p.Nn[i]), c0, p);
-            else tile_prefetch<NCOL>(p.Nn[i], c0, p);
-            tile_prefetch<NCOL>(p.U[i], c0, p);
-            if (p.stage > 0) tile_prefetch<NCOL>(p.Q[i], c0, p);
-        }
-        const int ncol = min(NCOL, p.B - c0);
-        prefetch_l2(p.bank.fac_p + (long)c0 * 3 * p.Ny, (long)ncol * 3 * p.Ny * 8, threadIdx.x, NT);
-        prefetch_l2(p.bank.fac_v + (long)c0 * 3 * p.Ny, (long)ncol * 3 * p.Ny * 8, threadIdx.x, NT);
-        prefetch_l2(p.bank.resp + (long)c0 * 6 * p.Ny, (long)ncol * 6 * p.Ny * 8, threadIdx.x, NT);
-    }
     // ---------------- Phase A: nonlinear term, history, right-hand side
     // The three components run through one copy of the loop body (pointers
     // selected, not indexed): the kernel's issue rate is limited by its
