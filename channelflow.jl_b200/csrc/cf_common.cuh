@@ -61,6 +61,28 @@ CF_DEV zd to_zd(zd a) { return a; }
 CF_DEV zd to_zd(zf a) { return make_double2((double)a.x, (double)a.y); }
 CF_DEV zf to_zf(zd a) { return make_float2((float)a.x, (float)a.y); }
 
+// ------------------------------------------------ asynchronous copies
+// One element (8 or 16 bytes) copied global -> shared without passing through
+// registers (zero fill when !ok; src must still be a valid address).  The
+// copies of a thread complete in commit groups (cp_async_commit), waited for
+// with cp_async_wait<N>() (all but the N most recent groups); a __syncthreads
+// must follow before other threads read the copied data.
+template <int BYTES>
+CF_DEV void cp_async_el(void* sdst, const void* gsrc, bool ok) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gsrc), "r"(ok ? 16 : 0)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(gsrc), "r"(ok ? 8 : 0)
+                     : "memory");
+}
+CF_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+CF_DEV void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Copy of one instance's parameters into shared memory (batched launches:
 // the block's instance is picked by a grid coordinate).
 template <class T>

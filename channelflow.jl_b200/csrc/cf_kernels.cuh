@@ -153,14 +153,11 @@ CF_DEV_NOINLINE void tile_load_async(zd* sm, int cs, int hs, const zd* g, int c0
         const int n = e / NCOL, t = e - n * NCOL;
         const int c = c0 + t;
         const bool ok = c < B;
-        const zd* src = ok ? g + (long)n * B + c : g;
-        const unsigned dst = (unsigned)__cvta_generic_to_shared(sm + t * cs + ppos(n, hs));
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(ok ? 16 : 0)
-                     : "memory");
+        cp_async_el<16>(sm + t * cs + ppos(n, hs), ok ? g + (long)n * B + c : g, ok);
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
+    cp_async_commit();
 }
-CF_DEV void tile_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+CF_DEV void tile_wait() { cp_async_wait<0>(); }
 
 template <int NCOL, class G>
 CF_DEV_NOINLINE void tile_store(const zd* sm, int cs, int hs, G* __restrict__ g, int c0, int Ny, int B) {
