@@ -249,9 +249,18 @@ class ChannelFlowProblem:
         assert U.shape == (3,) + self.grid.spectralsize and P.shape == self.grid.spectralsize
         _check(lib().cf_set_state(self._h, _ptr(U.view(np.float64)), _ptr(P.view(np.float64))))
 
-    def get_state(self):
-        U = np.zeros((3,) + self.grid.spectralsize, np.complex128)
-        P = np.zeros(self.grid.spectralsize, np.complex128)
+    def get_state(self, out=None):
+        """Download the state; out=(U, P) writes into the caller's contiguous
+        complex128 arrays (e.g. pinned buffers) instead of new ones."""
+        if out is None:
+            U = np.zeros((3,) + self.grid.spectralsize, np.complex128)
+            P = np.zeros(self.grid.spectralsize, np.complex128)
+        else:
+            U, P = out
+            if not (U.dtype == np.complex128 and P.dtype == np.complex128 and U.flags["C_CONTIGUOUS"]
+                    and P.flags["C_CONTIGUOUS"] and U.shape == (3,) + self.grid.spectralsize
+                    and P.shape == self.grid.spectralsize):
+                raise ValueError("out must be contiguous complex128 arrays of the state's shapes")
         _check(lib().cf_get_state(self._h, _ptr(U.view(np.float64)), _ptr(P.view(np.float64))))
         return U, P
 
@@ -425,10 +434,19 @@ def step_(problem, U, P, t, nsteps=1):
         raise ValueError("fields must have the resolved spectral size")
     problem.set_state(U, P)
     t2, _ = problem.advance(t, nsteps)
-    U2, P2 = problem.get_state()
-    U[...] = U2
-    P[...] = P2
+    _download_into(problem, U, P)
     return t2
+
+
+def _download_into(problem, U, P):
+    """The engine state into the caller's arrays: directly when they are
+    contiguous complex128 (pinned buffers stay pinned), else through a copy."""
+    if U.dtype == np.complex128 and P.dtype == np.complex128 and U.flags["C_CONTIGUOUS"] and P.flags["C_CONTIGUOUS"]:
+        problem.get_state(out=(U, P))
+    else:
+        U2, P2 = problem.get_state()
+        U[...] = U2
+        P[...] = P2
 
 
 def flow(problem):
@@ -454,9 +472,7 @@ def flow(problem):
         rest = t1 - t
         if rest > 1e-10 * dt:
             t, _ = problem.advance_dt(t, rest)
-        U, P = problem.get_state()
-        state.U[...] = U
-        state.P[...] = P
+        _download_into(problem, state.U, state.P)
         return state
 
     return run

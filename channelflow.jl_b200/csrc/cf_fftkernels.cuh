@@ -151,53 +151,61 @@ CF_DEV void zfwd_body(const FftParams& p, int bx, int n, int f) {
     }
 }
 
-// Pack nslots transform slots from pairs of real rows given by their half
+// Pack NS transform slots from pairs of real rows given by their half
 // spectra X, Y (get(slot, k, X, Y) for k < Nxh, Nyquist excluded; zero
 // elsewhere): Z_k = X_k + i Y_k, Z_{Nxp-k} = conj(X_k) + i conj(Y_k).  Every
-// position 0..Nxp-1 of the slots is written.  Block of 256 threads.  POS: the
-// slots' layout (cf_fft.cuh bpos: 0 padded, 1 XOR-swizzled).
-template <class Z, int POS = 1, class Get>
-CF_DEV void xpack(Z* sm, int bs, int nslots, int Nxh, int Nxp, int xnyq, const Get& get) {
-    const int Nxhp = Nxp / 2 + 1, tot = nslots * Nxhp;
-    for (int base = threadIdx.x; base < tot; base += 4 * 256) {
-        Z X[4], Y[4];
+// position 0..Nxp-1 of the slots is written.  The slot loop is unrolled, so
+// get() sees a constant slot (its source pointer is selected at compile
+// time); each thread issues the loads of all slots (KPT positions each)
+// before its first store.  POS: the slots' layout (cf_fft.cuh bpos: 0 padded,
+// 1 XOR-swizzled).
+template <class Z, int POS, int NS, class Get>
+CF_DEV void xpack(Z* sm, int bs, int Nxh, int Nxp, int xnyq, const Get& get) {
+    constexpr int KPT = NS <= 3 ? 2 : 1;
+    const int Nxhp = Nxp / 2 + 1, NT = blockDim.x;
+    for (int k0 = threadIdx.x; k0 < Nxhp; k0 += KPT * NT) {
+        Z X[NS][KPT], Y[NS][KPT];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int e = base + u * 256;
-            const int slot = e / Nxhp, k = e - slot * Nxhp;
-            X[u] = czero<Z>();
-            Y[u] = czero<Z>();
-            if (e < tot && k < Nxh && k != xnyq) get(slot, k, X[u], Y[u]);
-        }
+        for (int s = 0; s < NS; ++s)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int e = base + u * 256;
-            if (e >= tot) continue;
-            const int slot = e / Nxhp, k = e - slot * Nxhp;
-            Z* s = sm + slot * bs;
-            if (k == 0) {
-                s[bpos<POS>(0)] = cmake<Z>(X[u].x, Y[u].x);
-            } else if (2 * k == Nxp) {
-                s[bpos<POS>(k)] = cmake<Z>(X[u].x, Y[u].x);
-            } else {
-                s[bpos<POS>(k)] = cmake<Z>(X[u].x - Y[u].y, X[u].y + Y[u].x);
-                s[bpos<POS>(Nxp - k)] = cmake<Z>(X[u].x + Y[u].y, Y[u].x - X[u].y);
+            for (int u = 0; u < KPT; ++u) {
+                const int k = k0 + u * NT;
+                X[s][u] = czero<Z>();
+                Y[s][u] = czero<Z>();
+                if (k < Nxh && k != xnyq) get(s, k, X[s][u], Y[s][u]);
             }
-        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s)
+#pragma unroll
+            for (int u = 0; u < KPT; ++u) {
+                const int k = k0 + u * NT;
+                if (k >= Nxhp) continue;
+                Z* o = sm + s * bs;
+                const Z x = X[s][u], y = Y[s][u];
+                if (k == 0 || 2 * k == Nxp) {
+                    o[bpos<POS>(k)] = cmake<Z>(x.x, y.x);
+                } else {
+                    o[bpos<POS>(k)] = cmake<Z>(x.x - y.y, x.y + y.x);
+                    o[bpos<POS>(Nxp - k)] = cmake<Z>(x.x + y.y, y.x - x.y);
+                }
+            }
     }
 }
 
-// Separate nslots forward-transformed slots into the half spectra of their
-// two real rows, X = (Z_k + conj Z_-k)/2, Y = (Z_k - conj Z_-k)/(2i), and
-// hand them to put(slot, k, X, Y) for k < Nxh (the x truncation).
-template <class Z, int POS = 1, class Put>
-CF_DEV void xunpack(const Z* F, int bs, int nslots, int Nxh, int Nxp, const Put& put) {
-    for (int e = threadIdx.x; e < nslots * Nxh; e += blockDim.x) {
-        const int slot = e / Nxh, k = e - slot * Nxh;
-        const Z* s = F + slot * bs;
-        Z Zk = s[bpos<POS>(k)], Zm = s[bpos<POS>((Nxp - k) % Nxp)];
-        put(slot, k, cmake<Z>(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y)),
-            cmake<Z>(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x)));
+// Separate NS forward-transformed slots into the half spectra of their two
+// real rows, X = (Z_k + conj Z_-k)/2, Y = (Z_k - conj Z_-k)/(2i), and hand
+// them to put(slot, k, X, Y) for k < Nxh (the x truncation); constant slot
+// per unrolled iteration.
+template <class Z, int POS, int NS, class Put>
+CF_DEV void xunpack(const Z* F, int bs, int Nxh, int Nxp, const Put& put) {
+    for (int k = threadIdx.x; k < Nxh; k += blockDim.x) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const Z* o = F + s * bs;
+            const Z Zk = o[bpos<POS>(k)], Zm = o[bpos<POS>((Nxp - k) % Nxp)];
+            put(s, k, cmake<Z>(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y)),
+                cmake<Z>(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x)));
+        }
     }
 }
 
@@ -217,7 +225,7 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
     Z* scr = sm + 6 * bs;
     // zeros for a missing row B
-    xpack(sm, bs, 6, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+    xpack<Z, 1, 6>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
         const int pair = slot >> 1;
         const bool isB = slot & 1;
         if (isB && !hasB) return;
@@ -246,7 +254,7 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
     }
     __syncthreads();
     const Z* F = group_fft_L<true, LX, 1>(Bf, A, 3, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    xunpack(F, bs, 3, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+    xunpack<Z, 1, 3>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
         if (slot == 0) {
             zp_of<Z>(p, 0)[rowA + k] = X;
             zp_of<Z>(p, 1)[rowA + k] = Y;
@@ -275,7 +283,7 @@ CF_DEV void xpass_row_body(const FftParams& p, int z, int n) {
     const long row = ((long)n * p.Nzp + z) * Nxh;
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
     Z* scr = sm + 3 * bs;
-    xpack<Z, 0>(sm, bs, 3, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+    xpack<Z, 0, 3>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
         X = zp_of<Z>(p, 2 * slot)[row + k];
         Y = zp_of<Z>(p, 2 * slot + 1)[row + k];
     });
@@ -291,7 +299,7 @@ CF_DEV void xpass_row_body(const FftParams& p, int z, int n) {
     }
     __syncthreads();
     const Z* F = group_fft_L<true, LX, 0>(Bf, A, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    xunpack<Z, 0>(F, bs, 2, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+    xunpack<Z, 0, 2>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
         if (slot == 0) {
             zp_of<Z>(p, 0)[row + k] = X;
             zp_of<Z>(p, 1)[row + k] = Y;
@@ -321,7 +329,7 @@ CF_DEV void xpass_conv_body(const FftParams& p, int z, int n) {
         if (code < 6) return cmuli(zp_of<Z>(p, code - 3)[row + k], p.ax * k);
         return zp_of<Z>(p, code - 3)[row + k];
     };
-    xpack(sm, bs, 6, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+    xpack<Z, 1, 6>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
         X = fetch(2 * slot, k);
         Y = fetch(2 * slot + 1, k);
     });
@@ -344,7 +352,7 @@ CF_DEV void xpass_conv_body(const FftParams& p, int z, int n) {
     }
     __syncthreads();
     const Z* F = group_fft_L<true, LX, 1>(Bf, A, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    xunpack(F, bs, 2, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+    xunpack<Z, 1, 2>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
         if (slot == 0) {
             zp_of<Z>(p, 0)[row + k] = X;
             zp_of<Z>(p, 1)[row + k] = Y;
@@ -371,7 +379,7 @@ CF_DEV void xpass_div_body(const FftParams& p, int bx, int n) {
     const long rowB = ((long)n * p.Nzp + zB) * Nxh;
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
     Z* scr = sm + 6 * bs;
-    xpack(sm, bs, 3, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+    xpack<Z, 1, 3>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
         const Z* src = zp_of<Z>(p, slot);
         X = src[rowA + k];
         if (hasB) Y = src[rowB + k];
@@ -391,7 +399,7 @@ CF_DEV void xpass_div_body(const FftParams& p, int bx, int n) {
     }
     __syncthreads();
     const Z* F = group_fft_L<true, LX, 1>(Bf, A, 6, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    xunpack(F, bs, 6, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+    xunpack<Z, 1, 6>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
         Z* dst = zp_of<Z>(p, slot);
         dst[rowA + k] = X;
         if (hasB) dst[rowB + k] = Y;
