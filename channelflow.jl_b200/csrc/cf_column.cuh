@@ -28,6 +28,15 @@
 
 #define CF_TEAM 64  // threads per column
 
+// The long columns (P >= 192, and the run-time-sized kernels) call the
+// repeated helpers below out of line (one copy each keeps those kernels'
+// instructions within the instruction caches); the short ones inline them
+// (the call costs more there than the fetch).
+template <int PL>
+__host__ __device__ constexpr bool col_ool() {
+    return PL == 0 || PL >= 192;
+}
+
 // The two warps of one column.  Every routine below is called by all 64
 // threads of the team and ends with the team's barrier, after which all of its
 // outputs are visible to both warps.
@@ -70,7 +79,7 @@ CF_DEV zd warp_excl_z(zd inc, int lane) {
 
 // b = D a  (b != a).  Warp q writes the degrees of parity q of b from the
 // degrees of parity 1-q of a; b_P = 0.
-CF_DEV_NOINLINE void col_diff(const zd* a, zd* b, const Team t) {
+CF_DEV void col_diff_body(const zd* a, zd* b, const Team& t) {
     const int P = t.P, hs = t.hs, q = t.q, lane = t.lane;
     const int pin = 1 - q;                 // parity of the input chain
     const int top = pin ? P - 1 : P;       // m = top, top-2, ..., pin
@@ -96,6 +105,12 @@ CF_DEV_NOINLINE void col_diff(const zd* a, zd* b, const Team t) {
     }
     if (q == 0 && lane == 0) bh[P >> 1] = zzero();
     tsync(t);
+}
+CF_DEV_NOINLINE void col_diff_ool(const zd* a, zd* b, const Team t) { col_diff_body(a, b, t); }
+template <int PL>
+CF_DEV void col_diff(const zd* a, zd* b, const Team& t) {
+    if constexpr (col_ool<PL>()) col_diff_ool(a, b, t);
+    else col_diff_body(a, b, t);
 }
 
 // The three elimination factor rows of a column (alpha, invden, W: src,
@@ -146,9 +161,9 @@ CF_DEV zd helm_g(const zd* fh, const double* __restrict__ gt, int n, int P) {
 // factors in the parity layout (shared memory, staged by col_stage_factors);
 // SA0/SA1 and bc0/bc1 are the wall-row sums and data of the two parities.
 // Warp q solves the parity-q system alone.
-CF_DEV_NOINLINE void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
-                              const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
-                              const Team t) {
+CF_DEV void col_helm_body(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
+                          const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
+                          const Team& t) {
     const int P = t.P, Ny = P + 1, q = t.q, lane = t.lane, hs = t.hs;
     const int top = q ? P - 1 : P;
     const int cnt = (top - q) / 2;  // backward chain n = top, top-2, ..., q+2
@@ -216,6 +231,18 @@ CF_DEV_NOINLINE void col_helm(zd* x, zd* scr, const double* alpha, const double*
     if (lane == 0) xh[0] = a0;
     tsync(t);
 }
+CF_DEV_NOINLINE void col_helm_ool(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
+                                  const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0,
+                                  zd bc1, const Team t) {
+    col_helm_body(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
+}
+template <int PL>
+CF_DEV void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
+                     const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
+                     const Team& t) {
+    if constexpr (col_ool<PL>()) col_helm_ool(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
+    else col_helm_body(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
+}
 
 // DCT-I (REDFT00) of complex x[0..P] in place (parity layout).  z and z2 are
 // transform buffers of fft_bufsz(P) complex (padded positions fpos).
@@ -234,8 +261,13 @@ CF_DEV_NOINLINE void col_helm(zd* x, zd* scr, const double* alpha, const double*
 #define CF_DCT_INV 2
 // the team's complex FFT of length P (shared by both transform modes)
 template <int PL>
-CF_DEV_NOINLINE const zd* col_team_fft(zd* z, zd* z2, const FftPlan pl, const Team t) {
+CF_DEV_NOINLINE const zd* col_team_fft_ool(zd* z, zd* z2, const FftPlan pl, const Team t) {
     return group_fft_L<true, PL>(z, z2, 1, fft_bufsz(t.P), pl, -1, t.tid, CF_TEAM, t.bar);
+}
+template <int PL>
+CF_DEV const zd* col_team_fft(zd* z, zd* z2, const FftPlan& pl, const Team& t) {
+    if constexpr (col_ool<PL>()) return col_team_fft_ool<PL>(z, z2, pl, t);
+    else return group_fft_L<true, PL>(z, z2, 1, fft_bufsz(t.P), pl, -1, t.tid, CF_TEAM, t.bar);
 }
 template <int PL, int MODE>
 CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const FftPlan& pl, double scale,

@@ -159,8 +159,38 @@ CF_DEV void zfwd_body(const FftParams& p, int bx, int n, int f) {
 // time); each thread issues the loads of all slots (KPT positions each)
 // before its first store.  POS: the slots' layout (cf_fft.cuh bpos: 0 padded,
 // 1 XOR-swizzled).
-template <class Z, int POS, int NS, class Get>
+// FLAT: the (slot, position) pairs spread over all threads instead, with the
+// slot known at run time (more threads busy when rows are short).
+template <class Z, int POS, int NS, bool FLAT, class Get>
 CF_DEV void xpack(Z* sm, int bs, int Nxh, int Nxp, int xnyq, const Get& get) {
+    if constexpr (FLAT) {
+        const int Nxhp = Nxp / 2 + 1, tot = NS * Nxhp;
+        for (int base = threadIdx.x; base < tot; base += 4 * 256) {
+            Z X[4], Y[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = base + u * 256;
+                const int slot = e / Nxhp, k = e - slot * Nxhp;
+                X[u] = czero<Z>();
+                Y[u] = czero<Z>();
+                if (e < tot && k < Nxh && k != xnyq) get(slot, k, X[u], Y[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = base + u * 256;
+                if (e >= tot) continue;
+                const int slot = e / Nxhp, k = e - slot * Nxhp;
+                Z* o = sm + slot * bs;
+                if (k == 0 || 2 * k == Nxp) {
+                    o[bpos<POS>(k)] = cmake<Z>(X[u].x, Y[u].x);
+                } else {
+                    o[bpos<POS>(k)] = cmake<Z>(X[u].x - Y[u].y, X[u].y + Y[u].x);
+                    o[bpos<POS>(Nxp - k)] = cmake<Z>(X[u].x + Y[u].y, Y[u].x - X[u].y);
+                }
+            }
+        }
+        return;
+    }
     constexpr int KPT = NS <= 3 ? 2 : 1;
     const int Nxhp = Nxp / 2 + 1, NT = blockDim.x;
     for (int k0 = threadIdx.x; k0 < Nxhp; k0 += KPT * NT) {
@@ -196,8 +226,18 @@ CF_DEV void xpack(Z* sm, int bs, int Nxh, int Nxp, int xnyq, const Get& get) {
 // real rows, X = (Z_k + conj Z_-k)/2, Y = (Z_k - conj Z_-k)/(2i), and hand
 // them to put(slot, k, X, Y) for k < Nxh (the x truncation); constant slot
 // per unrolled iteration.
-template <class Z, int POS, int NS, class Put>
+template <class Z, int POS, int NS, bool FLAT, class Put>
 CF_DEV void xunpack(const Z* F, int bs, int Nxh, int Nxp, const Put& put) {
+    if constexpr (FLAT) {
+        for (int e = threadIdx.x; e < NS * Nxh; e += blockDim.x) {
+            const int slot = e / Nxh, k = e - slot * Nxh;
+            const Z* o = F + slot * bs;
+            const Z Zk = o[bpos<POS>(k)], Zm = o[bpos<POS>((Nxp - k) % Nxp)];
+            put(slot, k, cmake<Z>(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y)),
+                cmake<Z>(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x)));
+        }
+        return;
+    }
     for (int k = threadIdx.x; k < Nxh; k += blockDim.x) {
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
@@ -225,7 +265,7 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
     Z* scr = sm + 6 * bs;
     // zeros for a missing row B
-    xpack<Z, 1, 6>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+    xpack<Z, 1, 6, true>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
         const int pair = slot >> 1;
         const bool isB = slot & 1;
         if (isB && !hasB) return;
@@ -254,7 +294,7 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
     }
     __syncthreads();
     const Z* F = group_fft_L<true, LX, 1>(Bf, A, 3, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    xunpack<Z, 1, 3>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+    xunpack<Z, 1, 3, true>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
         if (slot == 0) {
             zp_of<Z>(p, 0)[rowA + k] = X;
             zp_of<Z>(p, 1)[rowA + k] = Y;
@@ -283,7 +323,7 @@ CF_DEV void xpass_row_body(const FftParams& p, int z, int n) {
     const long row = ((long)n * p.Nzp + z) * Nxh;
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
     Z* scr = sm + 3 * bs;
-    xpack<Z, 0, 3>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+    xpack<Z, 0, 3, false>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
         X = zp_of<Z>(p, 2 * slot)[row + k];
         Y = zp_of<Z>(p, 2 * slot + 1)[row + k];
     });
@@ -299,7 +339,7 @@ CF_DEV void xpass_row_body(const FftParams& p, int z, int n) {
     }
     __syncthreads();
     const Z* F = group_fft_L<true, LX, 0>(Bf, A, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    xunpack<Z, 0, 2>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+    xunpack<Z, 0, 2, false>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
         if (slot == 0) {
             zp_of<Z>(p, 0)[row + k] = X;
             zp_of<Z>(p, 1)[row + k] = Y;
@@ -329,7 +369,7 @@ CF_DEV void xpass_conv_body(const FftParams& p, int z, int n) {
         if (code < 6) return cmuli(zp_of<Z>(p, code - 3)[row + k], p.ax * k);
         return zp_of<Z>(p, code - 3)[row + k];
     };
-    xpack<Z, 1, 6>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+    xpack<Z, 1, 6, true>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
         X = fetch(2 * slot, k);
         Y = fetch(2 * slot + 1, k);
     });
@@ -352,7 +392,7 @@ CF_DEV void xpass_conv_body(const FftParams& p, int z, int n) {
     }
     __syncthreads();
     const Z* F = group_fft_L<true, LX, 1>(Bf, A, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    xunpack<Z, 1, 2>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+    xunpack<Z, 1, 2, true>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
         if (slot == 0) {
             zp_of<Z>(p, 0)[row + k] = X;
             zp_of<Z>(p, 1)[row + k] = Y;
@@ -379,7 +419,7 @@ CF_DEV void xpass_div_body(const FftParams& p, int bx, int n) {
     const long rowB = ((long)n * p.Nzp + zB) * Nxh;
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
     Z* scr = sm + 6 * bs;
-    xpack<Z, 1, 3>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+    xpack<Z, 1, 3, true>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, Z& X, Z& Y) {
         const Z* src = zp_of<Z>(p, slot);
         X = src[rowA + k];
         if (hasB) Y = src[rowB + k];
@@ -399,7 +439,7 @@ CF_DEV void xpass_div_body(const FftParams& p, int bx, int n) {
     }
     __syncthreads();
     const Z* F = group_fft_L<true, LX, 1>(Bf, A, 6, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    xunpack<Z, 1, 6>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
+    xunpack<Z, 1, 6, true>(F, bs, Nxh, Nxp, [&](int slot, int k, Z X, Z Y) {
         Z* dst = zp_of<Z>(p, slot);
         dst[rowA + k] = X;
         if (hasB) dst[rowB + k] = Y;
@@ -421,6 +461,12 @@ template <int LX, class Z = zd>
 __global__ void __launch_bounds__(256, (sizeof(Z) == 16 ? 3 : 4)) k_xpass(FftParams p) {
     if constexpr (sizeof(Z) == 16) xpass_row_body<LX, Z>(p, blockIdx.x, blockIdx.y);
     else xpass_body<LX, Z>(p, blockIdx.x, blockIdx.y);
+}
+// FP64, two rows per block (padded lengths up to 256, where one row leaves
+// most of the block idle in the FFT passes)
+template <int LX>
+__global__ void __launch_bounds__(256) k_xpass2(FftParams p) {
+    xpass_body<LX, zd>(p, blockIdx.x, blockIdx.y);
 }
 template <int LX>
 __global__ void __launch_bounds__(256) k_xpass_conv(FftParams p) {
@@ -446,10 +492,11 @@ __global__ void __launch_bounds__(256) k_zfwd_batch(const FftParams* __restrict_
     stage_params(&ps, pl + inst);
     zfwd_body<LZ, zd>(ps, blockIdx.x, blockIdx.y, blockIdx.z - 3 * inst);
 }
-// grid (Nzp, Ny, instances)
+// grid (ceil(Nzp/2), Ny, instances): two rows per block (the ensembles' grids
+// are small)
 template <int LX>
-__global__ void __launch_bounds__(256, 3) k_xpass_batch(const FftParams* __restrict__ pl) {
+__global__ void __launch_bounds__(256) k_xpass_batch(const FftParams* __restrict__ pl) {
     __shared__ FftParams ps;
     stage_params(&ps, pl + blockIdx.z);
-    xpass_row_body<LX, zd>(ps, blockIdx.x, blockIdx.y);
+    xpass_body<LX, zd>(ps, blockIdx.x, blockIdx.y);
 }

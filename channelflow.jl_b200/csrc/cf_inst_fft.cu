@@ -13,6 +13,7 @@ FftKernel fft_kernel_for(int which, bool f32) {
         case KF_ZFWD: return f32 ? k_zfwd<L, zf> : k_zfwd<L, zd>;
         case KF_XPASS_CONV: return k_xpass_conv<L>;
         case KF_XPASS_DIV: return k_xpass_div<L>;
+        case KF_XPASS2: return k_xpass2<L>;
         default: return f32 ? k_xpass<L, zf> : k_xpass<L, zd>;
     }
 }

@@ -120,7 +120,7 @@ template <>
 CF_DEV zf from_zd<zf>(zd a) { return to_zf(a); }
 
 template <int NCOL, class G>
-CF_DEV_NOINLINE void tile_load(zd* sm, int cs, int hs, const G* g, int c0, int Ny, int B) {
+CF_DEV void tile_load_body(zd* sm, int cs, int hs, const G* g, int c0, int Ny, int B) {
     constexpr int NT = NCOL * CF_TEAM, K = 8;
     const int tot = Ny * NCOL;
     for (int base = threadIdx.x; base < tot; base += NT * K) {
@@ -140,13 +140,22 @@ CF_DEV_NOINLINE void tile_load(zd* sm, int cs, int hs, const G* g, int c0, int N
         }
     }
 }
+template <int NCOL, class G>
+CF_DEV_NOINLINE void tile_load_ool(zd* sm, int cs, int hs, const G* g, int c0, int Ny, int B) {
+    tile_load_body<NCOL, G>(sm, cs, hs, g, c0, Ny, B);
+}
+template <int NCOL, int PL, class G>
+CF_DEV void tile_load(zd* sm, int cs, int hs, const G* g, int c0, int Ny, int B) {
+    if constexpr (col_ool<PL>()) tile_load_ool<NCOL, G>(sm, cs, hs, g, c0, Ny, B);
+    else tile_load_body<NCOL, G>(sm, cs, hs, g, c0, Ny, B);
+}
 // The same tile of FP64 coefficients copied asynchronously (16-byte cp.async
 // per complex, zero fill outside the grid): the call only issues the copies,
 // so several tiles are in flight together; tile_wait() completes all of a
 // thread's issued copies (a __syncthreads must follow before other threads
 // read them).
 template <int NCOL>
-CF_DEV_NOINLINE void tile_load_async(zd* sm, int cs, int hs, const zd* g, int c0, int Ny, int B) {
+CF_DEV void tile_load_async_body(zd* sm, int cs, int hs, const zd* g, int c0, int Ny, int B) {
     constexpr int NT = NCOL * CF_TEAM;
     const int tot = Ny * NCOL;
     for (int e = threadIdx.x; e < tot; e += NT) {
@@ -157,16 +166,34 @@ CF_DEV_NOINLINE void tile_load_async(zd* sm, int cs, int hs, const zd* g, int c0
     }
     cp_async_commit();
 }
+template <int NCOL>
+CF_DEV_NOINLINE void tile_load_async_ool(zd* sm, int cs, int hs, const zd* g, int c0, int Ny, int B) {
+    tile_load_async_body<NCOL>(sm, cs, hs, g, c0, Ny, B);
+}
+template <int NCOL, int PL>
+CF_DEV void tile_load_async(zd* sm, int cs, int hs, const zd* g, int c0, int Ny, int B) {
+    if constexpr (col_ool<PL>()) tile_load_async_ool<NCOL>(sm, cs, hs, g, c0, Ny, B);
+    else tile_load_async_body<NCOL>(sm, cs, hs, g, c0, Ny, B);
+}
 CF_DEV void tile_wait() { cp_async_wait<0>(); }
 
 template <int NCOL, class G>
-CF_DEV_NOINLINE void tile_store(const zd* sm, int cs, int hs, G* __restrict__ g, int c0, int Ny, int B) {
+CF_DEV void tile_store_body(const zd* sm, int cs, int hs, G* __restrict__ g, int c0, int Ny, int B) {
     const int tot = Ny * NCOL;
     for (int e = threadIdx.x; e < tot; e += NCOL * CF_TEAM) {
         const int n = e / NCOL, t = e - n * NCOL;
         const int c = c0 + t;
         if (c < B) g[(long)n * B + c] = from_zd<G>(sm[t * cs + ppos(n, hs)]);
     }
+}
+template <int NCOL, class G>
+CF_DEV_NOINLINE void tile_store_ool(const zd* sm, int cs, int hs, G* __restrict__ g, int c0, int Ny, int B) {
+    tile_store_body<NCOL, G>(sm, cs, hs, g, c0, Ny, B);
+}
+template <int NCOL, int PL, class G>
+CF_DEV void tile_store(const zd* sm, int cs, int hs, G* __restrict__ g, int c0, int Ny, int B) {
+    if constexpr (col_ool<PL>()) tile_store_ool<NCOL, G>(sm, cs, hs, g, c0, Ny, B);
+    else tile_store_body<NCOL, G>(sm, cs, hs, g, c0, Ny, B);
 }
 
 CF_DEV bool col_nyquist(const ColParams& p, int ix, int iz) {
@@ -225,13 +252,13 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
             const double* fsrc = it ? fv : bk.fac_p + (long)c * 3 * Ny;
             zd* x = it ? V : PT;
             col_stage_factors(fa, fw, fsrc, t);
-            col_diff(it ? PT : R1, x, t);
+            col_diff<PL>(it ? PT : R1, x, t);
             for (int j = lane; j < nq; j += 32) {
                 const int o = qo + j;
                 x[o] = it ? zsub(x[o], R1[o]) : zadd(x[o], zadd(zmulis(R0[o], k), zmulis(R2[o], l)));
             }
             __syncwarp();
-            col_helm(x, A, fa, fi, fw, p.helm_tab, __ldg(sa + 2 * it), __ldg(sa + 2 * it + 1),
+            col_helm<PL>(x, A, fa, fi, fw, p.helm_tab, __ldg(sa + 2 * it), __ldg(sa + 2 * it + 1),
                      it ? shift : __ldg(csc + 7), zzero(), zzero(), t);
         }
         // influence correction (batchedinfluence.jl:101-120)
@@ -295,7 +322,7 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
     if (c == 0) col_stage_factors(fa, fw, fv, t);
 #pragma unroll 1
     for (int j = 0; j < 2; ++j)
-        col_helm(j ? R2 : R0, A, fa, fi, fw, p.helm_tab, __ldg(sa + 2), __ldg(sa + 3), shift, zzero(), zzero(), t);
+        col_helm<PL>(j ? R2 : R0, A, fa, fi, fw, p.helm_tab, __ldg(sa + 2), __ldg(sa + 3), shift, zzero(), zzero(), t);
     if (c == 0) {
         double gx, gz;
         if (p.cmode == 1) {
@@ -339,8 +366,8 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
         tsync(t);
     }
     if (FORM == NL_ROT) {
-        col_diff(U2, W0, t);  // omega_x = D w - i l v
-        col_diff(U0, W2, t);  // omega_z = i k v - D u
+        col_diff<PL>(U2, W0, t);  // omega_x = D w - i l v
+        col_diff<PL>(U0, W2, t);  // omega_z = i k v - D u
         for (int j = lane; j < nq; j += 32) {
             const int o = qo + j;
             W0[o] = zsub(W0[o], zmulis(U1[o], l));
@@ -350,7 +377,7 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
         tsync(t);
     } else if (FORM == NL_CONV) {
 #pragma unroll 1
-        for (int i = 0; i < 3; ++i) col_diff(sel3(U0, U1, U2, i), sel3(W0, W1, W2, i), t);
+        for (int i = 0; i < 3; ++i) col_diff<PL>(sel3(U0, U1, U2, i), sel3(W0, W1, W2, i), t);
     }
     if (MX) return;
     // omega_y = i (l u - k w) is formed from the nodal u and w below (the
@@ -376,23 +403,23 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
 // Regions: 0 R0, 1 R1, 2 R2, 3 PT, 4 A, 5 Bw, 6 Z, 7 Z2 (6, 7: transform buffers).
 // The six nodal (or, MX, coefficient) fields u, v, w, omega from regions
 // r0..r5 to p.nod.
-template <int NCOL, bool MX, class Ctx>
+template <int NCOL, int PL, bool MX, class Ctx>
 CF_DEV void store_six(const Ctx& X, const ColParams& p, int r0, int r1, int r2, int r3, int r4, int r5) {
     const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
     const int rr[6] = {r0, r1, r2, r3, r4, r5};
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        if (MX) tile_store<NCOL>(X.reg(rr[i]), cs, hs, reinterpret_cast<zf*>(p.nod[i]), c0, p.Ny, p.B);
-        else tile_store<NCOL>(X.reg(rr[i]), cs, hs, p.nod[i], c0, p.Ny, p.B);
+        if (MX) tile_store<NCOL, PL>(X.reg(rr[i]), cs, hs, reinterpret_cast<zf*>(p.nod[i]), c0, p.Ny, p.B);
+        else tile_store<NCOL, PL>(X.reg(rr[i]), cs, hs, p.nod[i], c0, p.Ny, p.B);
     }
 }
 
 // the three nodal fields u, v, w from regions r0..r2 to p.nod (divergence form)
-template <int NCOL, class Ctx>
+template <int NCOL, int PL, class Ctx>
 CF_DEV void store_three(const Ctx& X, const ColParams& p, int r0, int r1, int r2) {
-    tile_store<NCOL>(X.reg(r0), X.cs, X.t.hs, p.nod[0], X.c0, p.Ny, p.B);
-    tile_store<NCOL>(X.reg(r1), X.cs, X.t.hs, p.nod[1], X.c0, p.Ny, p.B);
-    tile_store<NCOL>(X.reg(r2), X.cs, X.t.hs, p.nod[2], X.c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(r0), X.cs, X.t.hs, p.nod[0], X.c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(r1), X.cs, X.t.hs, p.nod[1], X.c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(r2), X.cs, X.t.hs, p.nod[2], X.c0, p.Ny, p.B);
 }
 
 // MX: mixed-precision form.  The nonlinear term arrives as FP32 Chebyshev
@@ -419,7 +446,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     // The three components run through one copy of the loop body (pointers
     // selected, not indexed): the kernel's issue rate is limited by its
     // instruction footprint, so the body is not unrolled.
-    tile_load_async<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);  // completed with N_0
+    tile_load_async<NCOL, PL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);  // completed with N_0
     double gold[2] = {p.c1, p.c2};
     zd bulkN0 = zzero(), bulkN2 = zzero(), wR0 = zzero(), wL0 = zzero(), wR2 = zzero(), wL2 = zzero();
 #pragma unroll 1
@@ -427,9 +454,9 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         const zd* Nn_i = sel3(p.Nn[0], p.Nn[1], p.Nn[2], i);
         zd* Q_i = sel3(p.Q[0], p.Q[1], p.Q[2], i);
         zd* U_i = sel3(p.U[0], p.U[1], p.U[2], i);
-        if (p.stage > 0) tile_load_async<NCOL>(X.reg(5), cs, hs, Q_i, c0, p.Ny, p.B);
-        if (MX) tile_load<NCOL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
-        else tile_load_async<NCOL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
+        if (p.stage > 0) tile_load_async<NCOL, PL>(X.reg(5), cs, hs, Q_i, c0, p.Ny, p.B);
+        if (MX) tile_load<NCOL, PL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
+        else tile_load_async<NCOL, PL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
         tile_wait();
         __syncthreads();
         if (valid) {
@@ -451,8 +478,8 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
             }
         }
         __syncthreads();
-        if (p.store_q) tile_store<NCOL>(X.reg(4), cs, hs, Q_i, c0, p.Ny, p.B);
-        tile_load_async<NCOL>(X.reg(5), cs, hs, U_i, c0, p.Ny, p.B);
+        if (p.store_q) tile_store<NCOL, PL>(X.reg(4), cs, hs, Q_i, c0, p.Ny, p.B);
+        tile_load_async<NCOL, PL>(X.reg(5), cs, hs, U_i, c0, p.Ny, p.B);
         tile_wait();
         __syncthreads();
         if (valid) {
@@ -472,10 +499,10 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
                     wL2 = wl;
                 }
             }
-            col_diff(U, Z, t);
-            col_diff(Z, R, t);
+            col_diff<PL>(U, Z, t);
+            col_diff<PL>(Z, R, t);
             // R = lambda U + nu (D^2 U - kappa^2 U) - d_i P + (B/C) Q
-            if (i == 1) col_diff(X.col(3), Z, t);
+            if (i == 1) col_diff<PL>(X.col(3), Z, t);
             const zd* PT = X.col(3);
             const double kl = (i == 0) ? k : l;
             for (int j = lane; j < nq; j += 32) {
@@ -523,18 +550,18 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         }
     }
     __syncthreads();
-    tile_store<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
-    tile_store<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
-    tile_store<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
-    tile_store<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
     __syncthreads();
     // ---------------- Phase C: total velocity, vorticity, nodal values
     if (valid)
         col_prep_nodal<PL, MX, FORM>(X.col(0), X.col(4), X.col(2), X.col(1), X.col(3), X.col(5), X.col(6), X.col(7),
                                      p, c, X.ix, X.iz, t);
     __syncthreads();
-    if (FORM == NL_DIV) store_three<NCOL>(X, p, 0, 4, 2);
-    else store_six<NCOL, MX>(X, p, 0, 4, 2, 1, 3, 5);
+    if (FORM == NL_DIV) store_three<NCOL, PL>(X, p, 0, 4, 2);
+    else store_six<NCOL, PL, MX>(X, p, 0, 4, 2, 1, 3, 5);
 }
 
 template <int NCOL, int PL, int FORM = NL_ROT>
@@ -565,17 +592,17 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
     const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
-    tile_load_async<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
-    tile_load_async<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
-    tile_load_async<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+    tile_load_async<NCOL, PL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+    tile_load_async<NCOL, PL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_load_async<NCOL, PL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
     tile_wait();
     __syncthreads();
     if (X.valid)
         col_prep_nodal<PL, MX, FORM>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7),
                                      p, X.c, X.ix, X.iz, X.t);
     __syncthreads();
-    if (FORM == NL_DIV) store_three<NCOL>(X, p, 0, 1, 2);
-    else store_six<NCOL, MX>(X, p, 0, 1, 2, 3, 4, 5);
+    if (FORM == NL_DIV) store_three<NCOL, PL>(X, p, 0, 1, 2);
+    else store_six<NCOL, PL, MX>(X, p, 0, 1, 2, 3, 4, 5);
 }
 
 // Divergence form, after the periodic transforms: forward DCT of the six
@@ -591,7 +618,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const Team& t = X.t;
     const int cs = X.cs, hs = t.hs, c0 = X.c0, qo = t.q * hs, nq = pcount(t.q, t.P);
 #pragma unroll
-    for (int m = 0; m < 6; ++m) tile_load_async<NCOL>(X.reg(m), cs, hs, p.nod[m], c0, p.Ny, p.B);
+    for (int m = 0; m < 6; ++m) tile_load_async<NCOL, PL>(X.reg(m), cs, hs, p.nod[m], c0, p.Ny, p.B);
     tile_wait();
     __syncthreads();
     if (X.valid) {
@@ -607,7 +634,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
         zd* D = X.col(6);
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
-            col_diff(X.col(rb[r]), D, t);
+            col_diff<PL>(X.col(rb[r]), D, t);
             const zd* a = X.col(ra[r]);
             const zd* cz = X.col(rc[r]);
             zd* o = X.col(ro[r]);
@@ -619,9 +646,9 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
         }
     }
     __syncthreads();
-    tile_store<NCOL>(X.reg(0), cs, hs, p.Nout[0], c0, p.Ny, p.B);
-    tile_store<NCOL>(X.reg(3), cs, hs, p.Nout[1], c0, p.Ny, p.B);
-    tile_store<NCOL>(X.reg(5), cs, hs, p.Nout[2], c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(0), cs, hs, p.Nout[0], c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(3), cs, hs, p.Nout[1], c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(5), cs, hs, p.Nout[2], c0, p.Ny, p.B);
 }
 
 // Forward DCT of the nonlinear term only: coefficients into p.Nout.
@@ -633,11 +660,11 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const bool nyq = X.valid ? col_nyquist(p, X.ix, X.iz) : true;
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        tile_load<NCOL>(X.reg(0), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p.Ny, p.B);
+        tile_load<NCOL, PL>(X.reg(0), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p.Ny, p.B);
         __syncthreads();
         if (X.valid) col_forward_y<PL>(X.col(0), X.col(6), X.col(7), p, nyq, X.t);
         __syncthreads();
-        tile_store<NCOL>(X.reg(0), cs, hs, sel3(p.Nout[0], p.Nout[1], p.Nout[2], i), c0, p.Ny, p.B);
+        tile_store<NCOL, PL>(X.reg(0), cs, hs, sel3(p.Nout[0], p.Nout[1], p.Nout[2], i), c0, p.Ny, p.B);
         __syncthreads();
     }
 }
@@ -655,14 +682,14 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const double kap2 = k * k + l * l;
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        tile_load<NCOL>(X.reg(5), cs, hs, sel3(p.U[0], p.U[1], p.U[2], i), c0, p.Ny, p.B);
+        tile_load<NCOL, PL>(X.reg(5), cs, hs, sel3(p.U[0], p.U[1], p.U[2], i), c0, p.Ny, p.B);
         __syncthreads();
         if (X.valid) {
             zd* U = X.col(5);
             zd* Z = X.col(6);
             zd* R = X.col(i);
-            col_diff(U, Z, t);
-            col_diff(Z, R, t);
+            col_diff<PL>(U, Z, t);
+            col_diff<PL>(Z, R, t);
             for (int j = t.lane; j < nq; j += 32) R[qo + j] = zscale(zaxpy(R[qo + j], -kap2, U[qo + j]), -1.0);
         }
         __syncthreads();
@@ -678,9 +705,9 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
         }
     }
     __syncthreads();
-    tile_store<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
-    tile_store<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
-    tile_store<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
 }
 
 // Pressure reconstruction (pressure.jl:115-204) from the nonlinear term at
@@ -697,12 +724,12 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const bool nyq = X.valid ? col_nyquist(p, X.ix, X.iz) : true;
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        tile_load<NCOL>(X.reg(i), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p.Ny, p.B);
+        tile_load<NCOL, PL>(X.reg(i), cs, hs, sel3(p.Nn[0], p.Nn[1], p.Nn[2], i), c0, p.Ny, p.B);
         __syncthreads();
         if (X.valid && !NCOEF) col_forward_y<PL>(X.col(i), X.col(6), X.col(7), p, nyq, t);
         __syncthreads();
     }
-    tile_load<NCOL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_load<NCOL, PL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
     __syncthreads();
     if (X.valid) {
         const double k = p.ax * X.ix;
@@ -731,7 +758,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
             if (t.tid == 0) PT[0] = zscale(m, -1.0);
             tsync(t);
         } else {
-            col_diff(A1, PT, t);
+            col_diff<PL>(A1, PT, t);
             zd su = zzero();
             for (int j = lane; j < nq; j += 32) {
                 const int n = 2 * j + q, o = qo + j;
@@ -751,12 +778,12 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
             double* fa = reinterpret_cast<double*>(X.col(6));
             double* fw = reinterpret_cast<double*>(X.col(7));
             col_stage_factors(fa, fw, fpn, t);
-            col_helm(PT, X.col(5), fa, fa + 2 * hs, fw, p.helm_tab, __ldg(sa + 0), __ldg(sa + 1), k * k + l * l,
+            col_helm<PL>(PT, X.col(5), fa, fa + 2 * hs, fw, p.helm_tab, __ldg(sa + 0), __ldg(sa + 1), k * k + l * l,
                      zscale(zsub(up, lo), 0.5), zscale(zadd(up, lo), 0.5), t);
         }
     }
     __syncthreads();
-    tile_store<NCOL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
+    tile_store<NCOL, PL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
 }
 
 // Diagnostics of the perturbation velocity on the device (postprocessing.jl:
@@ -794,9 +821,9 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const Team& t = X.t;
     const int cs = X.cs, hs = t.hs, c0 = X.c0, q = t.q, lane = t.lane, P = t.P;
     const int qo = q * hs, nq = pcount(q, P);
-    tile_load_async<NCOL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
-    tile_load_async<NCOL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
-    tile_load_async<NCOL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+    tile_load_async<NCOL, PL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+    tile_load_async<NCOL, PL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
+    tile_load_async<NCOL, PL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
     tile_wait();
     double* mom = reinterpret_cast<double*>(X.reg(6));
     for (int j = threadIdx.x; j <= 2 * P; j += NCOL * CF_TEAM)
@@ -813,9 +840,9 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     zd* W1 = X.col(4);
     zd* W2 = X.col(5);
     zd* DV = X.col(7);
-    col_diff(U2, W0, t);
-    col_diff(U0, W2, t);
-    col_diff(U1, DV, t);
+    col_diff<PL>(U2, W0, t);
+    col_diff<PL>(U0, W2, t);
+    col_diff<PL>(U1, DV, t);
     double dmax = 0.0;
     for (int j = lane; j < nq; j += 32) {
         const int o = qo + j;
