@@ -64,6 +64,19 @@ CF_DEV Z tw_get(const Z* tw, int k, int sgn) {
     return sgn > 0 ? zconj(w) : w;
 }
 
+// Twiddles w^r, r = 1..R-1, of one butterfly from the single table entry
+// w = tw[t1] by complex products (w^r = w^(r/2) w^(r - r/2), depth <= 3 for
+// R <= 9) instead of R-1 table loads: the loads share the L1/shared-memory
+// pipe with the butterfly data, which bounds the transform kernels, while the
+// FP64 pipe has room.  Each product adds about one rounding (a few 1e-16
+// relative in FP64).
+template <int R, class Z>
+CF_DEV void tw_powers(const Z* tw, int t1, int sgn, Z* w) {
+    w[1] = tw_get(tw, t1, sgn);
+#pragma unroll
+    for (int r = 2; r < R; ++r) w[r] = zmul(w[r >> 1], w[r - (r >> 1)]);
+}
+
 // a * (c + i sgn s): multiply by exp(sgn i theta) given (cos theta, sin theta)
 template <class Z>
 CF_DEV Z zrot(Z a, double c, double s, int sgn) {
@@ -266,11 +279,13 @@ CF_DEV void fft_pass_static(const Z* __restrict__ src, Z* __restrict__ dst, int 
         const int k = j % Ns;
         const Z* s = src + (long)b * bs;
         const int pj = bpos<POS>(j);
-        Z v[R];
+        Z v[R], w[R];
+        if constexpr (Ns > 1) tw_powers<R>(tw, k * step, sgn, w);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             Z x = s[LIN_LD ? pj + r * DLD : bpos<POS>(j + r * NBf)];
-            v[r] = (r == 0 || k == 0) ? x : zmul(x, tw_get(tw, k * r * step, sgn));
+            if constexpr (Ns > 1) v[r] = (r == 0 || k == 0) ? x : zmul(x, w[r]);
+            else v[r] = x;
         }
         dft_small<R>(v, sgn);
         Z* d = dst + (long)b * bs;
