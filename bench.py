@@ -423,13 +423,15 @@ def make_problem(cfb200, g, cfg, precision):
     return cfb200.PoiseuilleFlow(g, cfg["nu"], cfg["dt"], bulkvelocity=cfg["constraint"], precision=precision)
 
 
-def measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, nerr=100):
-    """The mixed-precision step on the same workload: steps/s (device-resident
+def measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, nerr=100, precision="mixed"):
+    """A mixed-precision step on the same workload: steps/s (device-resident
     state, CUDA-graph step, CUDA events), per-kernel event timing, and the
-    error against the FP64 step after nerr steps from the same initial state."""
+    error against the FP64 step after nerr steps from the same initial state.
+    precision "mixed": FP32 periodic transforms, FP64 Chebyshev transforms in
+    the column kernel; "mixed-tc": the Chebyshev transforms on the tensor cores."""
     import cfb200
 
-    mx = make_problem(cfb200, g, cfg, "mixed")
+    mx = make_problem(cfb200, g, cfg, precision)
     mx.set_state(U0, P0)
     stream = torch.cuda.ExternalStream(mx.stream_ptr())
     mx.advance(0.0, args.warmup)
@@ -453,7 +455,7 @@ def measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, nerr=100):
     # tensor-core transform: algorithmic FLOPs of one contraction (2 Ny^2 C per
     # field) and bytes (FP32 in and out); the TF32 split issues 3x the FLOPs
     cheb = {}
-    for key, nf in (("cheb_fwd", 3), ("cheb_inv", 6)):
+    for key, nf in ((("cheb_fwd", 3), ("cheb_inv", 6)) if precision == "mixed-tc" else ()):
         t = kavg[key] * 1e-3
         flops, byts = 2.0 * Ny * Ny * C * nf, 8.0 * Ny * C * nf
         cheb[key] = {"ms": kavg[key], "algorithmic_TFLOPs": flops / t / 1e12,
@@ -470,14 +472,19 @@ def measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, nerr=100):
     Um, _ = mx.get_state()
     dr, dm = ref.diagnostics(), mx.diagnostics()
     out = {"value": args.steps / (ms / 1e3), "unit": "steps/s", "ms_per_step": ms / args.steps,
-           "kernel_ms_per_launch": kavg, "tensor_core_transforms": cheb, "gpu_launches": launches,
+           "kernel_ms_per_launch": kavg, "gpu_launches": launches,
            "error_vs_fp64": {"steps": nerr,
                              "velocity_rel_l2": float(np.linalg.norm(Um - Ur) / np.linalg.norm(Ur)),
                              "energy_rel": float(abs(dm[0] - dr[0]) / abs(dr[0])),
                              "dissipation_rel": float(abs(dm[1] - dr[1]) / abs(dr[1])),
                              "max_div_mixed": float(dm[2])},
-           "precision": "FP32 periodic transforms and products; tensor-core Chebyshev transforms "
-                        "(TF32 heads and remainders, FP32 accumulation); FP64 Stokes solve and state"}
+           "precision": ("FP32 periodic transforms and products; tensor-core Chebyshev transforms "
+                         "(TF32 heads and remainders, FP32 accumulation); FP64 Stokes solve and state"
+                         if precision == "mixed-tc" else
+                         "FP32 periodic transforms and products (FP32 nodal fields); FP64 Chebyshev "
+                         "transforms, Stokes solve and state")}
+    if cheb:
+        out["tensor_core_transforms"] = cheb
     mx.close()
     ref.close()
     return out
@@ -640,6 +647,9 @@ def main():
     if not args.no_mixed:
         mixed = measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks)
         mixed["speedup_vs_fp64_plain"] = mixed["value"] / (value / world)
+        tc = measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, nerr=20, precision="mixed-tc")
+        tc["speedup_vs_fp64_plain"] = tc["value"] / (value / world)
+        mixed["tensor_core_variant"] = tc
         line["mixed"] = mixed
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1

@@ -23,7 +23,8 @@ typedef void (*FftBatchKernel)(const FftParams*);
 
 enum {
     KC_STAGE, KC_PREP, KC_NLOUT, KC_PROJECT, KC_PRESSURE, KC_STAGE_MX, KC_PREP_MX,
-    KC_STAGE_CONV, KC_PREP_CONV, KC_STAGE_DIV, KC_PREP_DIV, KC_DIV, KC_PRESSURE_COEF, KC_COUNT
+    KC_STAGE_CONV, KC_PREP_CONV, KC_STAGE_DIV, KC_PREP_DIV, KC_DIV, KC_PRESSURE_COEF,
+    KC_STAGE_MXD, KC_PREP_MXD, KC_COUNT
 };
 enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_XPASS_CONV, KF_XPASS_DIV, KF_XPASS2, KF_COUNT };
 

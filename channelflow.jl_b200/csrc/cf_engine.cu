@@ -223,6 +223,7 @@ struct cf_engine {
     // mixed-precision form (CF_PRECISION_MIXED): FP32 nodal and z-padded
     // fields, FP32 twiddles, tensor-core Chebyshev transform images
     int mixed = 0;
+    bool tc = false;  // mixed: Chebyshev transforms on the tensor cores (else FP64 in the column kernel)
     void *nod32[6] = {}, *zp32[6] = {};
     void* coef32[6] = {};  // FP32 Chebyshev coefficients (the transforms run out of place)
     zf *d_twZf = nullptr, *d_twXf = nullptr;
@@ -697,6 +698,16 @@ static int launch_cheb(cf_engine* h, int nf, bool inverse, int* count) {
 static int launch_stage_mx(cf_engine* h, int j, int* count) {
     int rc;
     if ((rc = launch_periodic32(h, count))) return rc;
+    if (!h->tc) {
+        // FP32 nodal fields in and out, Chebyshev transforms in the column kernel
+        ColParams p = stage_col_params(h, j);
+        for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->nod32[i]);
+        for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
+        col_kernel(KC_STAGE_MXD, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+        if (count) *count += 1;
+        CU(cudaGetLastError());
+        return CF_OK;
+    }
     if ((rc = launch_cheb(h, 3, false, count))) return rc;
     ColParams p = stage_col_params(h, j);
     for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->coef32[i]);
@@ -708,6 +719,13 @@ static int launch_stage_mx(cf_engine* h, int j, int* count) {
 }
 static int launch_prep_mx(cf_engine* h, int* count) {
     ColParams p = col_params(h);
+    if (!h->tc) {
+        for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
+        col_kernel(KC_PREP_MXD, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+        if (count) *count += 1;
+        CU(cudaGetLastError());
+        return CF_OK;
+    }
     for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->coef32[i]);
     col_kernel(KC_PREP_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
@@ -715,6 +733,7 @@ static int launch_prep_mx(cf_engine* h, int* count) {
     return launch_cheb(h, 6, true, count);
 }
 static int check_cheb_err(cf_engine* h) {
+    if (!h->tc) return CF_OK;
     int herr = 0;
     CU(cudaMemcpyAsync(&herr, h->d_cheberr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
@@ -741,8 +760,9 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
     for (int s = 0; s < nsteps && rc == CF_OK; ++s)
         for (int j = 0; j < 3 && rc == CF_OK; ++j) {
             ColParams p = stage_col_params(h, j);
-            for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->coef32[i]);
-            for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->coef32[i]);
+            void* const* io = h->tc ? h->coef32 : h->nod32;
+            for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(io[i]);
+            for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(io[i]);
             cudaEventRecord(ev[0], h->stream);
             fft_kernel(KF_ZINV, h->Nzp, true)<<<gz, 256, smz, h->stream>>>(f);
             cudaEventRecord(ev[1], h->stream);
@@ -750,11 +770,12 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
             cudaEventRecord(ev[2], h->stream);
             fft_kernel(KF_ZFWD, h->Nzp, true)<<<gz3, 256, smz, h->stream>>>(f);
             cudaEventRecord(ev[3], h->stream);
-            if ((rc = launch_cheb(h, 3, false, nullptr))) break;
+            if (h->tc && (rc = launch_cheb(h, 3, false, nullptr))) break;
             cudaEventRecord(ev[4], h->stream);
-            col_kernel(KC_STAGE_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+            col_kernel(h->tc ? KC_STAGE_MX : KC_STAGE_MXD, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h),
+                                                                  h->stream>>>(p);
             cudaEventRecord(ev[5], h->stream);
-            if ((rc = launch_cheb(h, 6, true, nullptr))) break;
+            if (h->tc && (rc = launch_cheb(h, 6, true, nullptr))) break;
             cudaEventRecord(ev[6], h->stream);
             if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(ev[6]) != cudaSuccess) {
                 rc = fail(CF_E_CUDA, "mixed step failed");
@@ -769,7 +790,7 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
     for (int k = 0; k < 7; ++k) cudaEventDestroy(ev[k]);
     if (rc) return rc;
     if ((rc = check_cheb_err(h))) return rc;
-    h->last_launches = cnt + 18 * nsteps;
+    h->last_launches = cnt + (h->tc ? 18 : 12) * nsteps;
     if (t_out) *t_out = t + nsteps * h->dt;
     return CF_OK;
 }
@@ -821,6 +842,8 @@ static int set_attrs(cf_engine* h) {
         if ((rc = raise_smem_limit(fft_kernel(KF_ZINV, h->Nzp, true), need[1] / 2))) return rc;
         if ((rc = raise_smem_limit(fft_kernel(KF_ZFWD, h->Nzp, true), need[1] / 2))) return rc;
         if ((rc = raise_smem_limit(fft_kernel(KF_XPASS, h->Nxp, true), need[2] / 2))) return rc;
+    }
+    if (h->mixed && h->tc) {
         int NPs, nsplit, NPt;
         cheb_dims(h->Ny, NPs, nsplit, NPt);
         if ((rc = raise_smem_limit(k_cheb_mma, cheb_smem(NPs)))) return rc;
@@ -836,11 +859,13 @@ static int validate_and_size(cf_engine* h, const cf_config* c) {
     if (!(std::isfinite(c->dt) && c->dt > 0)) return fail(CF_E_ARG, "dt must be finite and positive");
     if (!(std::isfinite(c->nu) && c->nu > 0)) return fail(CF_E_ARG, "nu must be finite and positive");
     if (c->constraint != 0 && c->constraint != 1) return fail(CF_E_ARG, "unknown constraint kind");
-    if (c->precision != CF_PRECISION_FP64 && c->precision != CF_PRECISION_MIXED)
+    if (c->precision != CF_PRECISION_FP64 && c->precision != CF_PRECISION_MIXED &&
+        c->precision != CF_PRECISION_MIXED_TC)
         return fail(CF_E_ARG, "unknown precision mode");
-    if (c->precision == CF_PRECISION_MIXED && c->Ny > 512)
-        return fail(CF_E_UNSUPPORTED, "the mixed-precision form supports Ny <= 512");
-    h->mixed = c->precision == CF_PRECISION_MIXED;
+    if (c->precision == CF_PRECISION_MIXED_TC && c->Ny > 512)
+        return fail(CF_E_UNSUPPORTED, "the tensor-core Chebyshev transforms support Ny <= 512");
+    h->mixed = c->precision != CF_PRECISION_FP64;
+    h->tc = c->precision == CF_PRECISION_MIXED_TC;
     if (c->form != CF_FORM_ROTATIONAL && c->form != CF_FORM_CONVECTIVE && c->form != CF_FORM_DIVERGENCE)
         return fail(CF_E_ARG, "unknown nonlinear form");
     if (h->mixed && c->form != CF_FORM_ROTATIONAL)
@@ -935,12 +960,15 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
     if ((rc = make_plan(h, h->Nzp, h->plZ, &h->d_twZ, h->mixed ? &h->d_twZf : nullptr))) return bail(rc);
     if ((rc = make_plan(h, h->Nxp, h->plX, &h->d_twX, h->mixed ? &h->d_twXf : nullptr))) return bail(rc);
     if (h->mixed) {
-        // FP32 work fields and the two transform-matrix images
+        // FP32 work fields and (tensor-core transforms) the coefficient
+        // fields and the two transform-matrix images
         for (int i = 0; i < 6; ++i) {
             if ((rc = dalloc(h, &h->nod32[i], sizeof(zf) * h->nr))) return bail(rc);
             if ((rc = dalloc(h, &h->zp32[i], sizeof(zf) * h->nq))) return bail(rc);
-            if ((rc = dalloc(h, &h->coef32[i], sizeof(zf) * h->nr))) return bail(rc);
+            if (h->tc && (rc = dalloc(h, &h->coef32[i], sizeof(zf) * h->nr))) return bail(rc);
         }
+    }
+    if (h->mixed && h->tc) {
         std::vector<float> fhi, flo, ihi, ilo;
         cheb_images(h->Ny, 0, 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1)), fhi, flo, h->chebNP, h->chebKT);
         cheb_images(h->Ny, 1, 1.0, ihi, ilo, h->chebNP, h->chebKT);
@@ -1036,7 +1064,7 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
     }
     if ((rc = build_graph(h))) return rc;
     for (int s = 0; s < nsteps; ++s) CU(cudaGraphLaunch(h->graph, h->stream));
-    cnt += (h->mixed ? 18 : step_launches(h)) * nsteps;
+    cnt += (h->mixed && h->tc ? 18 : step_launches(h)) * nsteps;
     h->last_launches = cnt;
     if (t_out) *t_out = t + nsteps * h->dt;
     if (grads_out && h->mixed && (rc = check_cheb_err(h))) return rc;

@@ -13,12 +13,14 @@ ColKernel col_kernel_for(int which) {
         case KC_PREP: return k_column_prep<CF_NCOL, P>;
         case KC_NLOUT: return k_column_nlout<CF_NCOL, P>;
         case KC_PROJECT: return k_column_project<CF_NCOL, P>;
-        case KC_STAGE_MX: return k_column_stage_mx<CF_NCOL, P>;
-        case KC_PREP_MX: return k_column_prep<CF_NCOL, P, true>;
+        case KC_STAGE_MX: return k_column_stage_mx<CF_NCOL, P, 1>;
+        case KC_PREP_MX: return k_column_prep<CF_NCOL, P, 1>;
+        case KC_STAGE_MXD: return k_column_stage_mx<CF_NCOL, P, 2>;
+        case KC_PREP_MXD: return k_column_prep<CF_NCOL, P, 2>;
         case KC_STAGE_CONV: return k_column_stage<CF_NCOL, P, NL_CONV>;
-        case KC_PREP_CONV: return k_column_prep<CF_NCOL, P, false, NL_CONV>;
+        case KC_PREP_CONV: return k_column_prep<CF_NCOL, P, 0, NL_CONV>;
         case KC_STAGE_DIV: return k_column_stage<CF_NCOL, P, NL_DIV>;
-        case KC_PREP_DIV: return k_column_prep<CF_NCOL, P, false, NL_DIV>;
+        case KC_PREP_DIV: return k_column_prep<CF_NCOL, P, 0, NL_DIV>;
         case KC_DIV: return k_column_div<CF_NCOL, P>;
         case KC_PRESSURE_COEF: return k_column_pressure<CF_NCOL, P, true>;
         default: return k_column_pressure<CF_NCOL, P>;

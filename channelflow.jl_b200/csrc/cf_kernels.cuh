@@ -401,8 +401,8 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
 // Full CNRK2 stage for NCOL columns per block (one team per column); bx is
 // the block's index among the instance's column blocks.
 // Regions: 0 R0, 1 R1, 2 R2, 3 PT, 4 A, 5 Bw, 6 Z, 7 Z2 (6, 7: transform buffers).
-// The six nodal (or, MX, coefficient) fields u, v, w, omega from regions
-// r0..r5 to p.nod.
+// The six nodal (or coefficient) fields u, v, w, omega from regions r0..r5
+// to p.nod (MX: as complex float).
 template <int NCOL, int PL, bool MX, class Ctx>
 CF_DEV void store_six(const Ctx& X, const ColParams& p, int r0, int r1, int r2, int r3, int r4, int r5) {
     const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
@@ -422,15 +422,18 @@ CF_DEV void store_three(const Ctx& X, const ColParams& p, int r0, int r1, int r2
     tile_store<NCOL, PL>(X.reg(r2), X.cs, X.t.hs, p.nod[2], X.c0, p.Ny, p.B);
 }
 
-// MX: mixed-precision form.  The nonlinear term arrives as FP32 Chebyshev
-// coefficients (normalised by the tensor-core transform; p.Nn holds zf
-// arrays) and the new velocity and vorticity leave as FP32 coefficients in
-// p.nod; the arithmetic of the stage stays FP64.
+// MIX (mixed-precision forms; the arithmetic of the stage stays FP64):
+//   0  FP64: the nonlinear term at the nodes in, nodal fields out (complex double)
+//   1  tensor-core Chebyshev transforms outside: the term arrives as FP32
+//      coefficients (normalised by the transform; p.Nn holds zf arrays) and
+//      the new velocity and vorticity leave as FP32 coefficients in p.nod
+//   2  FP32 nodal fields in and out, Chebyshev transforms here in FP64
 // FORM: the nonlinear form; the divergence form's term arrives as FP64
 // coefficients (from k_column_div), the others' at the nodes.
-template <int NCOL, int PL, bool MX = false, int FORM = NL_ROT>
+template <int NCOL, int PL, int MIX = 0, int FORM = NL_ROT>
 CF_DEV void column_stage_body(const ColParams& p, int bx) {
-    constexpr bool NCOEF = MX || FORM == NL_DIV;  // N arrives as coefficients
+    constexpr bool NCOEF = MIX == 1 || FORM == NL_DIV;  // N arrives as coefficients
+    constexpr bool F32 = MIX != 0;                       // FP32 N in, FP32 fields out
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, bx);
     const Team& t = X.t;
@@ -455,7 +458,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         zd* Q_i = sel3(p.Q[0], p.Q[1], p.Q[2], i);
         zd* U_i = sel3(p.U[0], p.U[1], p.U[2], i);
         if (p.stage > 0) tile_load_async<NCOL, PL>(X.reg(5), cs, hs, Q_i, c0, p.Ny, p.B);
-        if (MX) tile_load<NCOL, PL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
+        if (F32) tile_load<NCOL, PL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
         else tile_load_async<NCOL, PL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
         tile_wait();
         __syncthreads();
@@ -557,16 +560,16 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     __syncthreads();
     // ---------------- Phase C: total velocity, vorticity, nodal values
     if (valid)
-        col_prep_nodal<PL, MX, FORM>(X.col(0), X.col(4), X.col(2), X.col(1), X.col(3), X.col(5), X.col(6), X.col(7),
-                                     p, c, X.ix, X.iz, t);
+        col_prep_nodal<PL, MIX == 1, FORM>(X.col(0), X.col(4), X.col(2), X.col(1), X.col(3), X.col(5), X.col(6),
+                                           X.col(7), p, c, X.ix, X.iz, t);
     __syncthreads();
     if (FORM == NL_DIV) store_three<NCOL, PL>(X, p, 0, 4, 2);
-    else store_six<NCOL, PL, MX>(X, p, 0, 4, 2, 1, 3, 5);
+    else store_six<NCOL, PL, F32>(X, p, 0, 4, 2, 1, 3, 5);
 }
 
 template <int NCOL, int PL, int FORM = NL_ROT>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_stage(ColParams p) {
-    column_stage_body<NCOL, PL, false, FORM>(p, blockIdx.x);
+    column_stage_body<NCOL, PL, 0, FORM>(p, blockIdx.x);
 }
 // Batched stage: blockIdx.y selects the instance of a size class, whose
 // parameters are staged in shared memory.
@@ -578,16 +581,16 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>()))
     column_stage_body<NCOL, PL>(ps, blockIdx.x);
 }
 
-// Mixed-precision stage (see column_stage_body).
-template <int NCOL, int PL>
+// Mixed-precision stages (MIX 1 and 2 of column_stage_body).
+template <int NCOL, int PL, int MIX>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_stage_mx(ColParams p) {
-    column_stage_body<NCOL, PL, true>(p, blockIdx.x);
+    column_stage_body<NCOL, PL, MIX>(p, blockIdx.x);
 }
 
 // Nodal fields of the nonlinear form (velocity and vorticity for the
-// rotational form) from the state U (used after set_state); MX: their FP32
-// Chebyshev coefficients instead.
-template <int NCOL, int PL, bool MX = false, int FORM = NL_ROT>
+// rotational form) from the state U (used after set_state); MIX 1: their FP32
+// Chebyshev coefficients instead; MIX 2: FP32 nodal values.
+template <int NCOL, int PL, int MIX = 0, int FORM = NL_ROT>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_prep(ColParams p) {
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
@@ -598,11 +601,11 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     tile_wait();
     __syncthreads();
     if (X.valid)
-        col_prep_nodal<PL, MX, FORM>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7),
-                                     p, X.c, X.ix, X.iz, X.t);
+        col_prep_nodal<PL, MIX == 1, FORM>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6),
+                                           X.col(7), p, X.c, X.ix, X.iz, X.t);
     __syncthreads();
     if (FORM == NL_DIV) store_three<NCOL, PL>(X, p, 0, 1, 2);
-    else store_six<NCOL, PL, MX>(X, p, 0, 1, 2, 3, 4, 5);
+    else store_six<NCOL, PL, (MIX != 0)>(X, p, 0, 1, 2, 3, 4, 5);
 }
 
 // Divergence form, after the periodic transforms: forward DCT of the six

@@ -41,12 +41,15 @@ extern "C" {
 
 /* Precision of the step.  FP64: the plain form, every operation in double
  * precision (parity with the reference's step!).  MIXED: the nonlinear term's
- * periodic transforms and products in FP32 and the Chebyshev transforms as
- * tensor-core contractions (TF32 heads and remainders, FP32 accumulation);
- * right-hand side, tau Helmholtz solves, influence-matrix and tau corrections,
- * mean mode and flux constraint stay FP64, as does the state. */
+ * periodic transforms and products in FP32 (its nodal fields stored in FP32);
+ * Chebyshev transforms, right-hand side, tau Helmholtz solves,
+ * influence-matrix and tau corrections, mean mode and flux constraint stay
+ * FP64, as does the state.  MIXED_TC: as MIXED with the Chebyshev transforms
+ * as tensor-core contractions (TF32 heads and remainders, FP32 accumulation)
+ * between FP32 coefficient and nodal fields; Ny <= 512. */
 #define CF_PRECISION_FP64 0
 #define CF_PRECISION_MIXED 1
+#define CF_PRECISION_MIXED_TC 2
 
 /* Nonlinear form of NonLinearTerm(...; form) (src/nonlinear.jl:10-17, 113-193).
  * ROTATIONAL: u x curl(u) with the modified pressure (the default);

@@ -23,10 +23,14 @@ def rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-def test_mixed_couette_matches_oracle():
+MIXED = ["mixed", "mixed-tc"]
+
+
+@pytest.mark.parametrize("precision", MIXED)
+def test_mixed_couette_matches_oracle(precision):
     c = C1
     g = cfb200.Grid(c["Nx"], c["Ny"], c["Nz"], c["Lx"], c["Lz"])
-    mx = cfb200.CouetteFlow(g, 1 / 400, 0.01, precision="mixed")
+    mx = cfb200.CouetteFlow(g, 1 / 400, 0.01, precision=precision)
     ref = O.couette(c["Nx"], c["Ny"], c["Nz"], c["Lx"], c["Lz"], 1 / 400, 0.01)
     U, P = ref.random_state(seed=1, amp=0.1)
     mx.set_state(U, P)
@@ -48,11 +52,12 @@ def test_mixed_couette_matches_oracle():
     mx.close()
 
 
-def test_mixed_poiseuille_flux_matches_fp64_engine():
+@pytest.mark.parametrize("precision", MIXED)
+def test_mixed_poiseuille_flux_matches_fp64_engine(precision):
     g = cfb200.Grid(24, 25, 20, 2 * np.pi, np.pi)
     kw = dict(bulkvelocity=(2 / 3, 0.0))
     f64 = cfb200.PoiseuilleFlow(g, 1 / 1500, 0.005, **kw)
-    mx = cfb200.PoiseuilleFlow(g, 1 / 1500, 0.005, precision="mixed", **kw)
+    mx = cfb200.PoiseuilleFlow(g, 1 / 1500, 0.005, precision=precision, **kw)
     st = cfb200.random_state(f64, 0.1, seed=4)
     mx.set_state(st.U, st.P)
     _, g64 = f64.advance(0.0, 20)
@@ -73,16 +78,34 @@ def test_mixed_poiseuille_flux_matches_fp64_engine():
     mx.close()
 
 
+@pytest.mark.parametrize("precision", MIXED)
 @pytest.mark.parametrize("dims", [(9, 17, 7), (16, 17, 16), (48, 33, 40), (8, 257, 6)])
-def test_mixed_one_step_sizes(dims):
+def test_mixed_one_step_sizes(dims, precision):
     Nx, Ny, Nz = dims
     g = cfb200.Grid(Nx, Ny, Nz, 5.3, 7.1)
     ref = O.couette(Nx, Ny, Nz, 5.3, 7.1, 1 / 300, 0.01)
-    mx = cfb200.CouetteFlow(g, 1 / 300, 0.01, precision="mixed")
+    mx = cfb200.CouetteFlow(g, 1 / 300, 0.01, precision=precision)
     U, P = ref.random_state(seed=3, amp=0.2)
     mx.set_state(U, P)
     ref.step(U, P, 2)
     mx.advance(0.0, 2)
+    Um, _ = mx.get_state()
+    assert rel(Um, U) <= 1e-5
+    mx.close()
+
+
+def test_mixed_large_ny_without_tensor_cores():
+    # the in-kernel FP64 Chebyshev transforms have no Ny limit of the
+    # tensor-core images (Ny <= 512)
+    g = cfb200.Grid(8, 577, 6, 5.3, 7.1)
+    with pytest.raises(cfb200.CFError):
+        cfb200.CouetteFlow(g, 1 / 300, 0.01, precision="mixed-tc")
+    ref = O.couette(8, 577, 6, 5.3, 7.1, 1 / 300, 0.01)
+    mx = cfb200.CouetteFlow(g, 1 / 300, 0.01, precision="mixed")
+    U, P = ref.random_state(seed=3, amp=0.2)
+    mx.set_state(U, P)
+    ref.step(U, P, 1)
+    mx.advance(0.0, 1)
     Um, _ = mx.get_state()
     assert rel(Um, U) <= 1e-5
     mx.close()
