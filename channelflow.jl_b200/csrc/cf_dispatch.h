@@ -17,7 +17,7 @@ static_assert(CF_NCOL == 1 || CF_NCOL == 2, "column teams use named barriers 1 a
 
 typedef void (*ColKernel)(ColParams);
 typedef void (*FftKernel)(FftParams);
-typedef void (*DiagKernel)(ColParams, double*);
+typedef void (*DiagKernel)(ColParams, double*, double*);
 typedef void (*ColBatchKernel)(const ColParams*);
 typedef void (*FftBatchKernel)(const FftParams*);
 

@@ -231,6 +231,7 @@ struct cf_engine {
     int chebNP = 0, chebKT = 0;
     int* d_cheberr = nullptr;
     double* d_diag = nullptr;  // diagnostics accumulators
+    double* d_diagpart = nullptr;  // diagnostics block partials (3 per column block)
     cudaGraphExec_t graph = nullptr;
     int last_launches = 0;
     std::vector<void*> allocs;
@@ -1287,18 +1288,20 @@ int cf_diagnostics(cf_handle* h, double* out) {
     int rc;
     if (!h->d_diag) {
         if ((rc = dalloc(h, (void**)&h->d_diag, 8 * sizeof(double)))) return rc;
+        if ((rc = dalloc(h, (void**)&h->d_diagpart, 3 * sizeof(double) * col_blocks(h)))) return rc;
         if ((rc = raise_smem_limit(diag_kernel(h->P), col_smem(h)))) return rc;
     }
     CU(cudaMemsetAsync(h->d_diag, 0, 8 * sizeof(double), h->stream));
     ColParams p = col_params(h);
-    diag_kernel(h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p, h->d_diag);
+    diag_kernel(h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p, h->d_diag, h->d_diagpart);
+    k_diag_reduce<<<1, 1024, 0, h->stream>>>(h->d_diagpart, (int)col_blocks(h), h->d_diag);
     CU(cudaGetLastError());
     double acc[5];
     CU(cudaMemcpyAsync(acc, h->d_diag, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     out[0] = acc[0] / 2;
     out[1] = h->nu * acc[1];
-    out[2] = acc[2];  // bits of a non-negative double, stored by atomicMax
+    out[2] = acc[2];
     out[3] = h->nu * acc[3];
     out[4] = h->nu * acc[4];
     return CF_OK;

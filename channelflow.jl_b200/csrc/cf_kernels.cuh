@@ -790,36 +790,49 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
 }
 
 // Diagnostics of the perturbation velocity on the device (postprocessing.jl:
-// 80-95): acc[0] += sum over columns of <u_i, u_i>, acc[1] += <omega_i,
-// omega_i>, acc[2] = max |div u| coefficient (as the bits of a non-negative
-// double, ordered like the value), acc[3], acc[4] = u'(+1), u'(-1) of the
-// (0,0) mode.  <a, b> = sum_{m,n} conj(a_m) b_n M_mn with M_mn = (mom(m+n) +
-// mom(|m-n|))/2, mom(j) = 1/(1-j^2) for even j, 0 for odd j (the Chebyshev
-// inner product on [-1, 1] divided by 2), weighted 1 for kx = 0 and 2
-// otherwise; Nyquist columns are skipped.  M couples degrees of equal parity
-// only, so warp q sums the parity-q part.  Regions: 0-2 u, v, w; 3-5 omega;
-// 6 the moment table (block); 7 D v.
+// 80-95), per block: part[3 b] = sum over its columns of <u_i, u_i>,
+// part[3 b + 1] = of <omega_i, omega_i>, part[3 b + 2] = max |div u|
+// coefficient (summed by k_diag_reduce into acc[0..2]); acc[3], acc[4] =
+// u'(+1), u'(-1) of the (0,0) mode.  <a, b> = sum_{m,n} conj(a_m) b_n M_mn
+// with M_mn = (mom(m+n) + mom(|m-n|))/2, mom(j) = 1/(1-j^2) for even j, 0 for
+// odd j (the Chebyshev inner product on [-1, 1] divided by 2), weighted 1 for
+// kx = 0 and 2 otherwise; Nyquist columns are skipped.  M couples degrees of
+// equal parity only, so warp q sums the parity-q part, and only the even
+// moments occur (table mom[h] = mom(2h), h = 0..P).  Regions: 0-2 u, v, w;
+// 3-5 omega; 6 the moment table (block); 7 D v.
 CF_DEV double diag_form(const zd* a, const double* mom, const Team& t) {
+    // M is symmetric: the terms n > m count twice, n = m once; four
+    // independent accumulators keep several loads and FMAs in flight.  m and n
+    // have equal parity, so only even moments occur: mom[h] = mom(2h).
     const int q = t.q, qo = q * t.hs, nq = pcount(q, t.P);
     double s = 0.0;
     for (int j = t.lane; j < nq; j += 32) {
         const int m = 2 * j + q;
-        zd acc = zzero();
-        for (int i = 0; i < nq; ++i) {
-            const int n = 2 * i + q;
-            const double M = 0.5 * (mom[m + n] + mom[m > n ? m - n : n - m]);
-            acc = zaxpy(acc, M, a[qo + i]);
-        }
         const zd am = a[qo + j];
-        s += am.x * acc.x + am.y * acc.y;  // Re(conj(a_m) acc)
+        zd acc[4] = {zzero(), zzero(), zzero(), zzero()};
+        int i = j + 1;
+        for (; i + 3 < nq; i += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                // m + n = 2 (j + i + u + q), n - m = 2 (i + u - j)
+                acc[u] = zaxpy(acc[u], mom[j + i + u + q] + mom[i + u - j], a[qo + i + u]);
+            }
+        }
+        for (; i < nq; ++i) acc[0] = zaxpy(acc[0], mom[j + i + q] + mom[i - j], a[qo + i]);
+        const zd off = zadd(zadd(acc[0], acc[1]), zadd(acc[2], acc[3]));
+        // diagonal M_mm = (mom(2m) + mom(0)) / 2; off-diagonal pairs 2 M_mn = mom(m+n) + mom(n-m)
+        const double Mmm = 0.5 * (mom[m] + mom[0]);
+        s += Mmm * (am.x * am.x + am.y * am.y) + (am.x * off.x + am.y * off.y);  // Re(conj(a_m) ...)
     }
     return warp_sum_d(s);
 }
 
 template <int NCOL, int PL>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_diag(ColParams p,
-                                                                                             double* acc) {
+                                                                                             double* acc,
+                                                                                             double* part) {
     extern __shared__ zd smem[];
+    __shared__ double red[3][2 * NCOL];
     const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
     const Team& t = X.t;
     const int cs = X.cs, hs = t.hs, c0 = X.c0, q = t.q, lane = t.lane, P = t.P;
@@ -829,53 +842,101 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     tile_load_async<NCOL, PL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
     tile_wait();
     double* mom = reinterpret_cast<double*>(X.reg(6));
-    for (int j = threadIdx.x; j <= 2 * P; j += NCOL * CF_TEAM)
-        mom[j] = (j & 1) ? 0.0 : 1.0 / (1.0 - (double)j * j);
+    for (int j = threadIdx.x; j <= P; j += NCOL * CF_TEAM) mom[j] = 1.0 / (1.0 - 4.0 * (double)j * j);
     __syncthreads();
-    if (!X.valid) return;
-    const bool nyq = col_nyquist(p, X.ix, X.iz);
-    const double k = p.ax * X.ix;
-    const double l = p.bz * (X.iz <= (p.Nz >> 1) ? X.iz : X.iz - p.Nz);
-    zd* U0 = X.col(0);
-    zd* U1 = X.col(1);
-    zd* U2 = X.col(2);
-    zd* W0 = X.col(3);
-    zd* W1 = X.col(4);
-    zd* W2 = X.col(5);
-    zd* DV = X.col(7);
-    col_diff<PL>(U2, W0, t);
-    col_diff<PL>(U0, W2, t);
-    col_diff<PL>(U1, DV, t);
-    double dmax = 0.0;
-    for (int j = lane; j < nq; j += 32) {
-        const int o = qo + j;
-        W0[o] = zsub(W0[o], zmulis(U1[o], l));
-        W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
-        W2[o] = zsub(zmulis(U1[o], k), W2[o]);
-        const zd d = zadd(zadd(zmulis(U0[o], k), DV[o]), zmulis(U2[o], l));
-        dmax = fmax(dmax, sqrt(d.x * d.x + d.y * d.y));
-    }
-    tsync(t);
-    if (X.c == 0) {
-        zd wr, wl;
-        col_wallderiv(U0, t, wr, wl);
-        if (t.tid == 0) {
-            acc[3] = wr.x;
-            acc[4] = wl.x;
+    double e = 0.0, dis = 0.0, dmax = 0.0;
+    if (X.valid) {
+        const bool nyq = col_nyquist(p, X.ix, X.iz);
+        const double k = p.ax * X.ix;
+        const double l = p.bz * (X.iz <= (p.Nz >> 1) ? X.iz : X.iz - p.Nz);
+        zd* U0 = X.col(0);
+        zd* U1 = X.col(1);
+        zd* U2 = X.col(2);
+        zd* W0 = X.col(3);
+        zd* W1 = X.col(4);
+        zd* W2 = X.col(5);
+        zd* DV = X.col(7);
+        col_diff<PL>(U2, W0, t);
+        col_diff<PL>(U0, W2, t);
+        col_diff<PL>(U1, DV, t);
+        for (int j = lane; j < nq; j += 32) {
+            const int o = qo + j;
+            W0[o] = zsub(W0[o], zmulis(U1[o], l));
+            W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
+            W2[o] = zsub(zmulis(U1[o], k), W2[o]);
+            const zd d = zadd(zadd(zmulis(U0[o], k), DV[o]), zmulis(U2[o], l));
+            dmax = fmax(dmax, sqrt(d.x * d.x + d.y * d.y));
+        }
+        tsync(t);
+        if (X.c == 0) {
+            zd wr, wl;
+            col_wallderiv(U0, t, wr, wl);
+            if (t.tid == 0) {
+                acc[3] = wr.x;
+                acc[4] = wl.x;
+            }
+        }
+        for (int m = 16; m >= 1; m >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
+        if (!nyq) {
+            const double w = X.ix == 0 ? 1.0 : 2.0;
+#pragma unroll 1
+            for (int f = 0; f < 3; ++f) {
+                e += diag_form(sel3(U0, U1, U2, f), mom, t);
+                dis += diag_form(sel3(W0, W1, W2, f), mom, t);
+            }
+            e *= w;
+            dis *= w;
         }
     }
-    for (int m = 16; m >= 1; m >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, m));
-    if (lane == 0) atomicMax(reinterpret_cast<unsigned long long*>(acc + 2), (unsigned long long)__double_as_longlong(dmax));
-    if (nyq) return;
-    const double w = X.ix == 0 ? 1.0 : 2.0;
-    double e = 0.0, dis = 0.0;
-#pragma unroll 1
-    for (int f = 0; f < 3; ++f) {
-        e += diag_form(sel3(U0, U1, U2, f), mom, t);
-        dis += diag_form(sel3(W0, W1, W2, f), mom, t);
-    }
+    // block partials (no same-address atomics: summed by k_diag_reduce)
+    const int wi = threadIdx.x >> 5;
     if (lane == 0) {
-        atomicAdd(acc + 0, w * e);
-        atomicAdd(acc + 1, w * dis);
+        red[0][wi] = e;
+        red[1][wi] = dis;
+        red[2][wi] = dmax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double se = 0.0, sd = 0.0, mx = 0.0;
+        for (int i = 0; i < 2 * NCOL; ++i) {
+            se += red[0][i];
+            sd += red[1][i];
+            mx = fmax(mx, red[2][i]);
+        }
+        part[3 * blockIdx.x + 0] = se;
+        part[3 * blockIdx.x + 1] = sd;
+        part[3 * blockIdx.x + 2] = mx;
+    }
+}
+
+// Sum of the diagnostics' block partials (one block of 1024 threads, fixed
+// order): acc[0], acc[1] sums, acc[2] max.
+static __global__ void __launch_bounds__(1024) k_diag_reduce(const double* __restrict__ part, int nblk, double* acc) {
+    __shared__ double s[3][32];
+    double a = 0.0, b = 0.0, m = 0.0;
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+        a += part[3 * i];
+        b += part[3 * i + 1];
+        m = fmax(m, part[3 * i + 2]);
+    }
+    a = warp_sum_d(a);
+    b = warp_sum_d(b);
+    for (int o = 16; o >= 1; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) {
+        s[0][threadIdx.x >> 5] = a;
+        s[1][threadIdx.x >> 5] = b;
+        s[2][threadIdx.x >> 5] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sa = 0.0, sb = 0.0, sm = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            sa += s[0][w];
+            sb += s[1][w];
+            sm = fmax(sm, s[2][w]);
+        }
+        acc[0] = sa;
+        acc[1] = sb;
+        acc[2] = sm;
     }
 }
