@@ -48,7 +48,6 @@ struct ChebParams {
 };
 
 // ---- PTX wrappers --------------------------------------------------------------
-CF_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 CF_DEV float tf32_round(float x) {
     uint32_t r;
@@ -77,27 +76,8 @@ CF_DEV void umma_commit(uint32_t mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                  : "memory");
 }
-CF_DEV void mbar_init(uint32_t mbar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
-}
-// bounded wait for the completion of phase `parity`; false when it gave up
-CF_DEV bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (long it = 0; it < (1L << 22); ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(mbar), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
 CF_DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 CF_DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-CF_DEV void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // 16 consecutive TMEM columns of this warp's 32 lanes, one lane per thread
 CF_DEV void tmem_ld16(uint32_t taddr, float* v) {

@@ -83,6 +83,53 @@ CF_DEV void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// ------------------------------------------ mbarriers and bulk copies
+CF_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+CF_DEV void mbar_init(uint32_t mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+}
+// bounded wait for the completion of phase `parity`; false when it gave up
+CF_DEV bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (long it = 0; it < (1L << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// generic-proxy shared-memory writes made visible to the async proxy (TMA, tensor cores)
+CF_DEV void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+CF_DEV void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+CF_DEV void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+// TMA tile copies of a 3-D tensor map (no multicast): global -> shared
+// completing on an mbarrier, shared -> global in a bulk group.  The
+// innermost coordinate x times the element size is a multiple of 16 bytes at
+// every call site.
+CF_DEV void tma_load_3d(void* sdst, const void* map, int x, int y, int z, uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(sdst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(mbar)
+        : "memory");
+}
+CF_DEV void tma_store_3d(const void* map, int x, int y, int z, const void* ssrc) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map),
+                 "r"(x), "r"(y), "r"(z), "r"(smem_u32(ssrc))
+                 : "memory");
+}
+CF_DEV void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// until the bulk stores of this thread have read their shared memory (bounded
+// by construction: the copies are in flight and complete)
+CF_DEV void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
 // Copy of one instance's parameters into shared memory (batched launches:
 // the block's instance is picked by a grid coordinate).
 template <class T>

@@ -20,6 +20,7 @@ typedef void (*FftKernel)(FftParams);
 typedef void (*DiagKernel)(ColParams, double*, double*);
 typedef void (*ColBatchKernel)(const ColParams*);
 typedef void (*FftBatchKernel)(const FftParams*);
+typedef void (*FftTmaKernel)(FftParams, FftMaps);
 
 enum {
     KC_STAGE, KC_PREP, KC_NLOUT, KC_PROJECT, KC_PRESSURE, KC_STAGE_MX, KC_PREP_MX,
@@ -41,3 +42,6 @@ template <int L>
 FftKernel fft_kernel_for(int which, bool f32);
 template <int L>
 FftBatchKernel fft_batch_kernel_for(int which);
+// the z kernels with TMA row transfers (which: KF_ZINV or KF_ZFWD)
+template <int L>
+FftTmaKernel fft_tma_kernel_for(int which, bool f32);

@@ -33,6 +33,15 @@ static ColKernel col_kernel(int which, int P) {
         default: return col_kernel_for<0>(which);
     }
 }
+static FftTmaKernel fft_tma_kernel(int which, int L, bool f32) {
+    switch (L) {
+#define CF_CASE(N) \
+    case N: return fft_tma_kernel_for<N>(which, f32);
+        CF_STATIC_FFT_LENGTHS(CF_CASE)
+#undef CF_CASE
+        default: return fft_tma_kernel_for<0>(which, f32);
+    }
+}
 static FftKernel fft_kernel(int which, int L, bool f32 = false) {
     switch (L) {
 #define CF_CASE(N) \
@@ -204,6 +213,11 @@ struct cf_engine {
     double basemean;
     std::vector<double> base, basecurv;
     int tkz;
+    // TMA row transfers of the z kernels (maps of the FP64 and the FP32 fields)
+    FftMaps maps64, maps32;
+    bool tma64 = false, tma32 = false;
+    int zbox = 0, zpbox = 0;  // rows per TMA box (nodal, z-padded)
+    int* d_ffterr = nullptr;
     // device
     cudaStream_t stream = nullptr;
     int form = NL_ROT;  // nonlinear form (CF_FORM_*)
@@ -265,6 +279,13 @@ static int rup8(int x) { return (x + 7) & ~7; }
 static int zbs(const cf_engine* h) { return fft_bufsz(h->Nzp) + 1; }
 static int xbs(const cf_engine* h) { return rup8(h->Nxp); }
 static size_t zsmem(const cf_engine* h) { return (size_t)2 * h->tkz * zbs(h) * sizeof(zd); }
+// TMA z kernels: transform buffers, then (128-aligned) the staging rows of the
+// longer of the nodal and z-padded transfers; es = bytes per complex element
+static size_t zstage_off(const cf_engine* h, size_t es) { return ((zsmem(h) / sizeof(zd)) * es + 127) & ~(size_t)127; }
+static size_t zsmem_tma(const cf_engine* h, size_t es) {
+    const int rz = ((h->Nz + h->zbox - 1) / h->zbox) * h->zbox, rp = ((h->Nzp + h->zpbox - 1) / h->zpbox) * h->zpbox;
+    return zstage_off(h, es) + (size_t)std::max(rz, rp) * h->tkz * es;
+}
 // x-pass shared memory: 12 slots of round_up(Nxp, 8) (two rows of the FP32
 // rotational form, the convective and divergence forms), or 6 slots of
 // fft_bufsz(Nxp) (one row of the FP64 rotational form)
@@ -501,7 +522,21 @@ static FftParams fft_params(const cf_engine* h) {
     f.zp0 = h->zp[0]; f.zp1 = h->zp[1]; f.zp2 = h->zp[2]; f.zp3 = h->zp[3]; f.zp4 = h->zp[4]; f.zp5 = h->zp[5];
     f.zp6 = h->zp[6]; f.zp7 = h->zp[7]; f.zp8 = h->zp[8];
     f.plZ = h->plZ; f.plX = h->plX;
+    f.zbox = h->zbox; f.zpbox = h->zpbox;
+    f.stoff = (int)zstage_off(h, sizeof(zd));
+    f.err = h->d_ffterr;
     return f;
+}
+
+// z-inverse (nf fields) or z-forward of the FP64 (f32 false) or FP32 fields:
+// the TMA kernels when the maps could be encoded, else the gather kernels
+static void launch_z(cf_engine* h, int which, bool f32, int nf, const FftParams& f) {
+    const dim3 g((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, (unsigned)nf);
+    if (f32 ? h->tma32 : h->tma64)
+        fft_tma_kernel(which, h->Nzp, f32)<<<g, 256, zsmem_tma(h, f32 ? sizeof(zf) : sizeof(zd)), h->stream>>>(
+            f, f32 ? h->maps32 : h->maps64);
+    else
+        fft_kernel(which, h->Nzp, f32)<<<g, 256, f32 ? zsmem(h) / 2 : zsmem(h), h->stream>>>(f);
 }
 
 // Launch shapes of the periodic transforms of the handle's nonlinear form:
@@ -521,14 +556,13 @@ static PeriodicShape periodic_shape(const cf_engine* h) {
 static int launch_periodic_kernels(cf_engine* h, cudaEvent_t* ev) {
     FftParams f = fft_params(h);
     const PeriodicShape s = periodic_shape(h);
-    const size_t smz = zsmem(h), smx = xsmem(h, s.xkind == KF_XPASS ? 6 : 12);
-    const unsigned gzx = (unsigned)((h->Nxh + h->tkz - 1) / h->tkz);
-    fft_kernel(KF_ZINV, h->Nzp)<<<dim3(gzx, (unsigned)h->Ny, s.nzinv), 256, smz, h->stream>>>(f);
+    const size_t smx = xsmem(h, s.xkind == KF_XPASS ? 6 : 12);
+    launch_z(h, KF_ZINV, false, s.nzinv, f);
     if (ev) CU(cudaEventRecord(ev[0], h->stream));
     const dim3 gx((unsigned)((h->Nzp + s.xrows - 1) / s.xrows), (unsigned)h->Ny);
     fft_kernel(s.xkind, h->Nxp)<<<gx, 256, smx, h->stream>>>(f);
     if (ev) CU(cudaEventRecord(ev[1], h->stream));
-    fft_kernel(KF_ZFWD, h->Nzp)<<<dim3(gzx, (unsigned)h->Ny, s.nzfwd), 256, smz, h->stream>>>(f);
+    launch_z(h, KF_ZFWD, false, s.nzfwd, f);
     CU(cudaGetLastError());
     return CF_OK;
 }
@@ -652,17 +686,16 @@ static FftParams fft_params32(const cf_engine* h) {
     f.nod3 = h->nod32[3]; f.nod4 = h->nod32[4]; f.nod5 = h->nod32[5];
     f.zp0 = h->zp32[0]; f.zp1 = h->zp32[1]; f.zp2 = h->zp32[2];
     f.zp3 = h->zp32[3]; f.zp4 = h->zp32[4]; f.zp5 = h->zp32[5];
+    f.stoff = (int)zstage_off(h, sizeof(zf));
     return f;
 }
 static int launch_periodic32(cf_engine* h, int* count) {
     FftParams f = fft_params32(h);
-    const size_t smz = zsmem(h) / 2, smx = xsmem(h) / 2;  // complex float buffers
-    dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
-    fft_kernel(KF_ZINV, h->Nzp, true)<<<gz, 256, smz, h->stream>>>(f);
+    const size_t smx = xsmem(h) / 2;  // complex float buffers
+    launch_z(h, KF_ZINV, true, 6, f);
     dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
     fft_kernel(KF_XPASS, h->Nxp, true)<<<gx, 256, smx, h->stream>>>(f);
-    dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
-    fft_kernel(KF_ZFWD, h->Nzp, true)<<<gz3, 256, smz, h->stream>>>(f);
+    launch_z(h, KF_ZFWD, true, 3, f);
     if (count) *count += 3;
     CU(cudaGetLastError());
     return CF_OK;
@@ -734,11 +767,17 @@ static int launch_prep_mx(cf_engine* h, int* count) {
     return launch_cheb(h, 6, true, count);
 }
 static int check_cheb_err(cf_engine* h) {
-    if (!h->tc) return CF_OK;
     int herr = 0;
-    CU(cudaMemcpyAsync(&herr, h->d_cheberr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
-    if (herr) return fail(CF_E_CUDA, "Chebyshev transform kernel: a tensor-core wait timed out");
+    if (h->tc) {
+        CU(cudaMemcpyAsync(&herr, h->d_cheberr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        if (herr) return fail(CF_E_CUDA, "Chebyshev transform kernel: a tensor-core wait timed out");
+    }
+    if (h->tma64 || h->tma32) {
+        CU(cudaMemcpyAsync(&herr, h->d_ffterr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        if (herr) return fail(CF_E_CUDA, "z transform kernel: a TMA wait timed out");
+    }
     return CF_OK;
 }
 // mixed step with per-kernel event timing: kernel_ms = [z-inverse, x-pass,
@@ -753,10 +792,8 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
     for (int k = 0; k < 7; ++k) CU(cudaEventCreate(&ev[k]));
     for (int k = 0; k < 6; ++k) kernel_ms[k] = 0.0;
     FftParams f = fft_params32(h);
-    const size_t smz = zsmem(h) / 2, smx = xsmem(h) / 2;
-    dim3 gz((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 6);
+    const size_t smx = xsmem(h) / 2;
     dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
-    dim3 gz3((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, 3);
     const int order[6] = {0, 1, 2, 4, 3, 5};  // launch order -> kernel_ms slot
     for (int s = 0; s < nsteps && rc == CF_OK; ++s)
         for (int j = 0; j < 3 && rc == CF_OK; ++j) {
@@ -765,11 +802,11 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
             for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(io[i]);
             for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(io[i]);
             cudaEventRecord(ev[0], h->stream);
-            fft_kernel(KF_ZINV, h->Nzp, true)<<<gz, 256, smz, h->stream>>>(f);
+            launch_z(h, KF_ZINV, true, 6, f);
             cudaEventRecord(ev[1], h->stream);
             fft_kernel(KF_XPASS, h->Nxp, true)<<<gx, 256, smx, h->stream>>>(f);
             cudaEventRecord(ev[2], h->stream);
-            fft_kernel(KF_ZFWD, h->Nzp, true)<<<gz3, 256, smz, h->stream>>>(f);
+            launch_z(h, KF_ZFWD, true, 3, f);
             cudaEventRecord(ev[3], h->stream);
             if (h->tc && (rc = launch_cheb(h, 3, false, nullptr))) break;
             cudaEventRecord(ev[4], h->stream);
@@ -811,6 +848,64 @@ static int build_graph(cf_engine* h) {
     return CF_OK;
 }
 
+// Tensor maps of the z kernels' TMA row transfers.  The encoder is the
+// driver's cuTensorMapEncodeTiled, looked up through the runtime (no driver
+// library link).  Returns false (the gather kernels are used) when a map
+// cannot be encoded, e.g. a row stride that is not a multiple of 16 bytes.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+// one field: complex elements (2 scalars) of es bytes, (Nxh, rows, Ny), box (tkz, box rows, 1)
+static bool encode_field(const cf_engine* h, CUtensorMap* m, void* base, int rows, int box, bool f32) {
+    EncodeTiledFn fn = encode_tiled_fn();
+    if (!fn || !base) return false;
+    const size_t sc = f32 ? 4 : 8;
+    const cuuint64_t dims[3] = {(cuuint64_t)2 * h->Nxh, (cuuint64_t)rows, (cuuint64_t)h->Ny};
+    const cuuint64_t strides[2] = {(cuuint64_t)2 * h->Nxh * sc, (cuuint64_t)2 * h->Nxh * rows * sc};
+    const cuuint32_t boxd[3] = {(cuuint32_t)(2 * h->tkz), (cuuint32_t)box, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides,
+              boxd, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+static void encode_maps(cf_engine* h) {
+    std::memset(&h->maps64, 0, sizeof(FftMaps));
+    std::memset(&h->maps32, 0, sizeof(FftMaps));
+    // only for narrow column groups: with tkz >= 4 the gathered row segments
+    // are 64 bytes or more and the plain loads cost less than the staging
+    // (measured: TMA 1.71 against 1.79 ms for the z-inverse at tkz = 2,
+    // 0.119 against 0.091 ms at tkz = 8)
+    bool ok = h->d_ffterr != nullptr && h->tkz <= 2;
+    for (int i = 0; i < 6 && ok; ++i)
+        if (h->nod[i]) ok = encode_field(h, &h->maps64.nod[i], h->nod[i], h->Nz, h->zbox, false);
+    for (int i = 0; i < 9 && ok; ++i)
+        if (h->zp[i]) ok = encode_field(h, &h->maps64.zp[i], h->zp[i], h->Nzp, h->zpbox, false);
+    h->tma64 = ok && zsmem_tma(h, sizeof(zd)) <= (size_t)227 * 1024;
+    if (h->mixed) {
+        ok = h->d_ffterr != nullptr && h->tkz <= 2;
+        for (int i = 0; i < 6 && ok; ++i) ok = encode_field(h, &h->maps32.nod[i], h->nod32[i], h->Nz, h->zbox, true);
+        for (int i = 0; i < 6 && ok; ++i) ok = encode_field(h, &h->maps32.zp[i], h->zp32[i], h->Nzp, h->zpbox, true);
+        h->tma32 = ok && zsmem_tma(h, sizeof(zf)) <= (size_t)227 * 1024;
+    }
+}
+
 // Raise a kernel's dynamic shared-memory limit to at least `need`.  The limit
 // belongs to the kernel, not to a handle: handles of different grids share the
 // run-time-sized instantiations, so it is only ever raised.
@@ -839,6 +934,14 @@ static int set_attrs(cf_engine* h) {
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_CONV, h->Nxp), need[2]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_DIV, h->Nxp), need[2]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS2, h->Nxp), need[2]))) return rc;
+    if (h->tma64) {
+        if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZINV, h->Nzp, false), zsmem_tma(h, sizeof(zd))))) return rc;
+        if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZFWD, h->Nzp, false), zsmem_tma(h, sizeof(zd))))) return rc;
+    }
+    if (h->tma32) {
+        if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZINV, h->Nzp, true), zsmem_tma(h, sizeof(zf))))) return rc;
+        if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZFWD, h->Nzp, true), zsmem_tma(h, sizeof(zf))))) return rc;
+    }
     if (h->mixed) {
         if ((rc = raise_smem_limit(fft_kernel(KF_ZINV, h->Nzp, true), need[1] / 2))) return rc;
         if ((rc = raise_smem_limit(fft_kernel(KF_ZFWD, h->Nzp, true), need[1] / 2))) return rc;
@@ -895,6 +998,14 @@ static int validate_and_size(cf_engine* h, const cf_config* c) {
     for (int t : {8, 4, 2, 1})
         if ((size_t)2 * t * (fft_bufsz(h->Nzp) + 1) * 16 <= 74 * 1024 || t == 1) { h->tkz = t; break; }
     if (zsmem(h) > (size_t)227 * 1024) return fail(CF_E_UNSUPPORTED, "padded z length not supported");
+    // TMA boxes: at most 256 rows, a multiple of 8 rows (128-byte box strides
+    // in the staging buffer for both element sizes)
+    auto box_rows = [](int rows) {
+        const int nb = (rows + 255) / 256;
+        return ((rows + nb - 1) / nb + 7) & ~7;
+    };
+    h->zbox = box_rows(h->Nz);
+    h->zpbox = box_rows(h->Nzp);
     return CF_OK;
 }
 
@@ -1004,6 +1115,9 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
         if ((rc = dalloc(h, (void**)&h->d_helmtab, sizeof(double) * gt.size()))) return bail(rc);
         cudaMemcpy(h->d_helmtab, gt.data(), sizeof(double) * gt.size(), cudaMemcpyHostToDevice);
     }
+    if ((rc = dalloc(h, (void**)&h->d_ffterr, sizeof(int)))) return bail(rc);
+    if (cudaMemset(h->d_ffterr, 0, sizeof(int)) != cudaSuccess) return bail(fail(CF_E_CUDA, "upload failed"));
+    encode_maps(h);
     if ((rc = set_attrs(h))) return bail(rc);
     if ((rc = ensure_banks(h))) return bail(rc);
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(CF_E_CUDA, "set-up failed"));
@@ -1068,7 +1182,7 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
     cnt += (h->mixed && h->tc ? 18 : step_launches(h)) * nsteps;
     h->last_launches = cnt;
     if (t_out) *t_out = t + nsteps * h->dt;
-    if (grads_out && h->mixed && (rc = check_cheb_err(h))) return rc;
+    if (grads_out && (rc = check_cheb_err(h))) return rc;
     if (grads_out) {
         double g[2];
         CU(cudaMemcpyAsync(g, h->d_grad, 16, cudaMemcpyDeviceToHost, h->stream));
@@ -1109,7 +1223,7 @@ int cf_step_dt(cf_handle* h, double t, double dt, double* t_out, double* grads_o
     if (rc) return rc;
     h->last_launches = cnt;
     if (t_out) *t_out = t + dt;
-    if (grads_out && h->mixed && (rc = check_cheb_err(h))) return rc;
+    if (grads_out && (rc = check_cheb_err(h))) return rc;
     if (grads_out) {
         double g[2];
         CU(cudaMemcpyAsync(g, h->d_grad, 16, cudaMemcpyDeviceToHost, h->stream));

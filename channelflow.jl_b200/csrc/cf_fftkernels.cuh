@@ -15,6 +15,8 @@
 //               k_zinv) -> n = -(u.grad)u (3; du/dx made by k_xpass)
 //   divergence  nodal u (3) -> z-padded 0-2 -> -u_i u_j (6: 00 01 02 11 12 22)
 #pragma once
+#include <cuda.h>  // CUtensorMap
+
 #include "cf_fft.cuh"
 
 struct FftParams {
@@ -23,6 +25,9 @@ struct FftParams {
     int bsz, bsx;  // transform buffer strides: fft_bufsz(Nzp) + 1 (odd, padded layout),
                    // round_up(Nxp, 8) (XOR-swizzled layout: 12 buffers of the x-pass)
     int bsxp;      // fft_bufsz(Nxp): padded layout of the one-row FP64 x-pass
+    int zbox, zpbox;  // TMA z kernels: rows per box of the nodal (Nz) and z-padded (Nzp) fields
+    int stoff;     // TMA z kernels: byte offset of the staging buffer in shared memory
+    int* err;      // TMA z kernels: set to 1 when a wait gives up
     double ax, bz;  // 2 pi / Lx, 2 pi / Lz (derivatives of the convective form)
     // nodal and z-padded fields: complex double (FP64 path) or complex float
     // (FP32 transforms of the mixed-precision path)
@@ -62,6 +67,14 @@ CF_DEV Z* zp_of(const FftParams& p, int i) {
     return static_cast<Z*>(a);
 }
 
+// TMA maps of the z kernels' fields, over the scalars of the complex type:
+// nodal (2 Nxh, Nz, Ny) with box (2 tkz, zbox, 1), z-padded (2 Nxh, Nzp, Ny)
+// with box (2 tkz, zpbox, 1).
+struct FftMaps {
+    CUtensorMap nod[6];
+    CUtensorMap zp[9];
+};
+
 // i s a
 template <class Z>
 CF_DEV Z cmuli(Z a, double s) {
@@ -78,7 +91,7 @@ CF_DEV int zpad_index(int iz, int Nz, int Nzp) { return iz <= (Nz >> 1) ? iz : N
 // with which it commutes).
 template <int LZ, class Z>
 CF_DEV void zinv_body(const FftParams& p, int bx, int n, int f) {
-    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
     Z* sm = reinterpret_cast<Z*>(fsm_raw);
     const int tks = p.tks, tkz = 1 << tks, tm = tkz - 1;
     const int k0 = bx << tks;
@@ -117,10 +130,100 @@ CF_DEV void zinv_body(const FftParams& p, int bx, int n, int f) {
     }
 }
 
+// The z kernels with their strided row gathers and scatters done by TMA:
+// tkz columns x all rows of one plane move as boxes of (2 tkz scalars, zbox
+// rows) between the global fields and a dense staging buffer in shared memory
+// (stage[row * tkz + t]), so the strided 32-byte row segments cost no L1
+// wavefronts.  Rows past the end of a box load as zeros and are not stored.
+// smem: the 2*tkz*bsz transform elements, then (at byte p.stoff, 128-aligned)
+// the staging buffer.  One thread issues the copies; every wait is bounded
+// (p.err set, the block returns).
+template <class Z>
+CF_DEV Z* zstage(const FftParams& p) {
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    return reinterpret_cast<Z*>(fsm_raw + p.stoff);
+}
+template <class Z>
+CF_DEV bool zload_tma(const FftParams& p, const CUtensorMap* map, int k0, int rows, int box, int n, Z* stage,
+                      uint64_t* mbar) {
+    const uint32_t mb = smem_u32(mbar);
+    const int tkz = 1 << p.tks, nb = (rows + box - 1) / box;
+    if (threadIdx.x == 0) {
+        mbar_init(mb, 1);
+        fence_mbar_init();
+        mbar_expect_tx(mb, (uint32_t)(nb * box * tkz * sizeof(Z)));
+        for (int b = 0; b < nb; ++b) tma_load_3d(stage + (long)b * box * tkz, map, 2 * k0, b * box, n, mb);
+    }
+    __syncthreads();
+    const bool ok = __syncthreads_and(mbar_wait(mb, 0));
+    if (!ok && threadIdx.x == 0) atomicExch(p.err, 1);
+    return ok;
+}
+template <class Z>
+CF_DEV void zstore_tma(const FftParams& p, const CUtensorMap* map, int k0, int rows, int box, int n,
+                       const Z* stage) {
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int tkz = 1 << p.tks;
+        for (int b = 0; b * box < rows; ++b) tma_store_3d(map, 2 * k0, b * box, n, stage + (long)b * box * tkz);
+        bulk_commit();
+        bulk_wait_read();
+    }
+}
+
+template <int LZ, class Z>
+CF_DEV void zinv_tma_body(const FftParams& p, const FftMaps& m, int bx, int n, int f) {
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    __shared__ __align__(8) uint64_t mbar;
+    Z* sm = reinterpret_cast<Z*>(fsm_raw);
+    Z* stage = zstage<Z>(p);
+    const int tks = p.tks, tkz = 1 << tks, tm = tkz - 1;
+    const int k0 = bx << tks;
+    const int Nz = p.Nz, Nzp = LZ ? LZ : p.Nzp, Nxh = p.Nxh, bs = p.bsz;
+    Z* bufB = sm + tkz * bs;
+    const bool dz = f >= 6;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1, znyq = (Nz % 2 == 0) ? Nz / 2 : -1;
+    // zero the padding gap while the rows arrive
+    const int gap0 = (Nz >> 1) + 1, gap1 = Nzp - (Nz - gap0);
+    for (int e = threadIdx.x; e < ((gap1 - gap0) << tks); e += blockDim.x)
+        sm[(e & tm) * bs + fpos(gap0 + (e >> tks))] = czero<Z>();
+    if (!zload_tma<Z>(p, &m.nod[dz ? f - 6 : f], k0, Nz, p.zbox, n, stage, &mbar)) return;
+    for (int e = threadIdx.x; e < (Nz << tks); e += blockDim.x) {
+        const int iz = e >> tks, k = k0 + (e & tm);
+        Z v = (k < Nxh && iz != znyq && k != xnyq) ? stage[e] : czero<Z>();
+        if (dz) v = cmuli(v, p.bz * (double)(iz <= (Nz >> 1) ? iz : iz - Nz));
+        sm[(e & tm) * bs + fpos(zpad_index(iz, Nz, Nzp))] = v;
+    }
+    __syncthreads();
+    const Z* res = group_fft_L<true, LZ>(sm, bufB, tkz, bs, p.plZ, +1, threadIdx.x, blockDim.x, 0);
+    for (int e = threadIdx.x; e < (Nzp << tks); e += blockDim.x) stage[e] = res[(e & tm) * bs + fpos(e >> tks)];
+    zstore_tma<Z>(p, &m.zp[f], k0, Nzp, p.zpbox, n, stage);
+}
+
+template <int LZ, class Z>
+CF_DEV void zfwd_tma_body(const FftParams& p, const FftMaps& m, int bx, int n, int f) {
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    __shared__ __align__(8) uint64_t mbar;
+    Z* sm = reinterpret_cast<Z*>(fsm_raw);
+    Z* stage = zstage<Z>(p);
+    const int tks = p.tks, tkz = 1 << tks, tm = tkz - 1;
+    const int k0 = bx << tks;
+    const int Nz = p.Nz, Nzp = LZ ? LZ : p.Nzp, bs = p.bsz;
+    Z* bufB = sm + tkz * bs;
+    if (!zload_tma<Z>(p, &m.zp[f], k0, Nzp, p.zpbox, n, stage, &mbar)) return;
+    for (int e = threadIdx.x; e < (Nzp << tks); e += blockDim.x) sm[(e & tm) * bs + fpos(e >> tks)] = stage[e];
+    __syncthreads();
+    const Z* res = group_fft_L<true, LZ>(sm, bufB, tkz, bs, p.plZ, -1, threadIdx.x, blockDim.x, 0);
+    for (int e = threadIdx.x; e < (Nz << tks); e += blockDim.x)
+        stage[e] = res[(e & tm) * bs + fpos(zpad_index(e >> tks, Nz, Nzp))];
+    zstore_tma<Z>(p, &m.nod[f], k0, Nz, p.zbox, n, stage);
+}
+
 // grid: (ceil(Nxh/tkz), Ny, 3); forward z FFT and truncation to Nz
 template <int LZ, class Z>
 CF_DEV void zfwd_body(const FftParams& p, int bx, int n, int f) {
-    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
     Z* sm = reinterpret_cast<Z*>(fsm_raw);
     const int tks = p.tks, tkz = 1 << tks, tm = tkz - 1;
     const int k0 = bx << tks;
@@ -189,36 +292,36 @@ CF_DEV void xpack(Z* sm, int bs, int Nxh, int Nxp, int xnyq, const Get& get) {
                 }
             }
         }
-        return;
-    }
-    constexpr int KPT = NS <= 3 ? 2 : 1;
-    const int Nxhp = Nxp / 2 + 1, NT = blockDim.x;
-    for (int k0 = threadIdx.x; k0 < Nxhp; k0 += KPT * NT) {
-        Z X[NS][KPT], Y[NS][KPT];
+    } else {
+        constexpr int KPT = NS <= 3 ? 2 : 1;
+        const int Nxhp = Nxp / 2 + 1, NT = blockDim.x;
+        for (int k0 = threadIdx.x; k0 < Nxhp; k0 += KPT * NT) {
+            Z X[NS][KPT], Y[NS][KPT];
 #pragma unroll
-        for (int s = 0; s < NS; ++s)
+            for (int s = 0; s < NS; ++s)
 #pragma unroll
-            for (int u = 0; u < KPT; ++u) {
-                const int k = k0 + u * NT;
-                X[s][u] = czero<Z>();
-                Y[s][u] = czero<Z>();
-                if (k < Nxh && k != xnyq) get(s, k, X[s][u], Y[s][u]);
-            }
-#pragma unroll
-        for (int s = 0; s < NS; ++s)
-#pragma unroll
-            for (int u = 0; u < KPT; ++u) {
-                const int k = k0 + u * NT;
-                if (k >= Nxhp) continue;
-                Z* o = sm + s * bs;
-                const Z x = X[s][u], y = Y[s][u];
-                if (k == 0 || 2 * k == Nxp) {
-                    o[bpos<POS>(k)] = cmake<Z>(x.x, y.x);
-                } else {
-                    o[bpos<POS>(k)] = cmake<Z>(x.x - y.y, x.y + y.x);
-                    o[bpos<POS>(Nxp - k)] = cmake<Z>(x.x + y.y, y.x - x.y);
+                for (int u = 0; u < KPT; ++u) {
+                    const int k = k0 + u * NT;
+                    X[s][u] = czero<Z>();
+                    Y[s][u] = czero<Z>();
+                    if (k < Nxh && k != xnyq) get(s, k, X[s][u], Y[s][u]);
                 }
-            }
+#pragma unroll
+            for (int s = 0; s < NS; ++s)
+#pragma unroll
+                for (int u = 0; u < KPT; ++u) {
+                    const int k = k0 + u * NT;
+                    if (k >= Nxhp) continue;
+                    Z* o = sm + s * bs;
+                    const Z x = X[s][u], y = Y[s][u];
+                    if (k == 0 || 2 * k == Nxp) {
+                        o[bpos<POS>(k)] = cmake<Z>(x.x, y.x);
+                    } else {
+                        o[bpos<POS>(k)] = cmake<Z>(x.x - y.y, x.y + y.x);
+                        o[bpos<POS>(Nxp - k)] = cmake<Z>(x.x + y.y, y.x - x.y);
+                    }
+                }
+        }
     }
 }
 
@@ -236,15 +339,15 @@ CF_DEV void xunpack(const Z* F, int bs, int Nxh, int Nxp, const Put& put) {
             put(slot, k, cmake<Z>(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y)),
                 cmake<Z>(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x)));
         }
-        return;
-    }
-    for (int k = threadIdx.x; k < Nxh; k += blockDim.x) {
+    } else {
+        for (int k = threadIdx.x; k < Nxh; k += blockDim.x) {
 #pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const Z* o = F + s * bs;
-            const Z Zk = o[bpos<POS>(k)], Zm = o[bpos<POS>((Nxp - k) % Nxp)];
-            put(s, k, cmake<Z>(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y)),
-                cmake<Z>(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x)));
+            for (int s = 0; s < NS; ++s) {
+                const Z* o = F + s * bs;
+                const Z Zk = o[bpos<POS>(k)], Zm = o[bpos<POS>((Nxp - k) % Nxp)];
+                put(s, k, cmake<Z>(0.5 * (Zk.x + Zm.x), 0.5 * (Zk.y - Zm.y)),
+                    cmake<Z>(0.5 * (Zk.y + Zm.y), 0.5 * (Zm.x - Zk.x)));
+            }
         }
     }
 }
@@ -255,7 +358,7 @@ CF_DEV void xunpack(const Z* F, int bs, int Nxh, int Nxp, const Put& put) {
 // (u0+iu1, u2+iw0, w1+iw2) of row A at 0,2,4 and of row B at 1,3,5.
 template <int LX, class Z>
 CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
-    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
     Z* sm = reinterpret_cast<Z*>(fsm_raw);
     const int zA = 2 * bx, zB = zA + 1;
     const bool hasB = zB < p.Nzp;
@@ -317,7 +420,7 @@ CF_DEV void xpass_body(const FftParams& p, int bx, int n) {
 // u2+iw0, w1+iw2) of row z = bx; the products leave in (n0+in1, n2).
 template <int LX, class Z>
 CF_DEV void xpass_row_body(const FftParams& p, int z, int n) {
-    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
     Z* sm = reinterpret_cast<Z*>(fsm_raw);
     const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsxp;
     const long row = ((long)n * p.Nzp + z) * Nxh;
@@ -358,7 +461,7 @@ CF_DEV void xpass_row_body(const FftParams& p, int z, int n) {
 // slots (n0 + i n1, n2), written to z-padded 0-2.
 template <int LX, class Z>
 CF_DEV void xpass_conv_body(const FftParams& p, int z, int n) {
-    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
     Z* sm = reinterpret_cast<Z*>(fsm_raw);
     const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsx;
     const long row = ((long)n * p.Nzp + z) * Nxh;
@@ -410,7 +513,7 @@ CF_DEV void xpass_conv_body(const FftParams& p, int z, int n) {
 // div!) into slots m = 00 01 02 11 12 22 and written to z-padded 0-5.
 template <int LX, class Z>
 CF_DEV void xpass_div_body(const FftParams& p, int bx, int n) {
-    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
     Z* sm = reinterpret_cast<Z*>(fsm_raw);
     const int zA = 2 * bx, zB = zA + 1;
     const bool hasB = zB < p.Nzp;
@@ -451,6 +554,14 @@ CF_DEV void xpass_div_body(const FftParams& p, int bx, int n) {
 template <int LZ, class Z = zd>
 __global__ void __launch_bounds__(256) k_zinv(FftParams p) {
     zinv_body<LZ, Z>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <int LZ, class Z = zd>
+__global__ void __launch_bounds__(256) k_zinv_tma(FftParams p, const __grid_constant__ FftMaps m) {
+    zinv_tma_body<LZ, Z>(p, m, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <int LZ, class Z = zd>
+__global__ void __launch_bounds__(256) k_zfwd_tma(FftParams p, const __grid_constant__ FftMaps m) {
+    zfwd_tma_body<LZ, Z>(p, m, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int LZ, class Z = zd>
 __global__ void __launch_bounds__(256) k_zfwd(FftParams p) {

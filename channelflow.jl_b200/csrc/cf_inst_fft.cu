@@ -26,5 +26,12 @@ FftBatchKernel fft_batch_kernel_for(int which) {
     }
 }
 
+template <int L>
+FftTmaKernel fft_tma_kernel_for(int which, bool f32) {
+    if (which == KF_ZINV) return f32 ? k_zinv_tma<L, zf> : k_zinv_tma<L, zd>;
+    return f32 ? k_zfwd_tma<L, zf> : k_zfwd_tma<L, zd>;
+}
+
 template FftKernel fft_kernel_for<CF_INST_L>(int, bool);
+template FftTmaKernel fft_tma_kernel_for<CF_INST_L>(int, bool);
 template FftBatchKernel fft_batch_kernel_for<CF_INST_L>(int);
