@@ -49,7 +49,8 @@ EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_g
            "cf_pressure", "cf_random_state", "cf_diagnostics", "cf_sync", "cf_last_launch_count",
            "cf_stream", "cf_last_error", "cf_step_profiled", "cf_nonlinear_noalloc", "cf_create_batch",
            "cf_destroy_batch", "cf_batch_size", "cf_batch_instance", "cf_step_batch",
-           "cf_batch_last_launch_count", "cf_batch_stream", "cf_cheb_transform", "cf_step_dt"]
+           "cf_batch_last_launch_count", "cf_batch_stream", "cf_cheb_transform", "cf_step_dt",
+           "cf_step_host"]
 
 
 def lib():
@@ -71,6 +72,7 @@ def lib():
         L.cf_get_state_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.cf_step.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _D, _D]
         L.cf_step_dt.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _D, _D]
+        L.cf_step_host.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_double, ctypes.c_int, _D, _D]
         L.cf_nonlinear.argtypes = [ctypes.c_void_p, _D, _D]
         L.cf_nonlinear_noalloc.argtypes = [ctypes.c_void_p, _D, _D]
         L.cf_cheb_transform.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), ctypes.c_int,
@@ -428,14 +430,21 @@ def step_(problem, U, P, t, nsteps=1):
     """step!(scheme, nlterm, U, P, t; constraint...) (src/timesteppers/cnrk2.jl:567-625).
 
     Host buffers U, P are advanced in place (upload, nsteps device steps,
-    download) and t + nsteps*dt is returned.
+    download) and t + nsteps*dt is returned.  Contiguous complex128 buffers go
+    through cf_step_host, which overlaps the transfers with the first and last
+    column kernels; others through a contiguous copy.
     """
     if U.shape != (3,) + problem.grid.spectralsize or P.shape != problem.grid.spectralsize:
         raise ValueError("fields must have the resolved spectral size")
-    problem.set_state(U, P)
-    t2, _ = problem.advance(t, nsteps)
-    _download_into(problem, U, P)
-    return t2
+    direct = all(a.dtype == np.complex128 and a.flags["C_CONTIGUOUS"] and a.flags["WRITEABLE"] for a in (U, P))
+    Uc, Pc = (U, P) if direct else (np.ascontiguousarray(U, np.complex128), np.ascontiguousarray(P, np.complex128))
+    tout = ctypes.c_double()
+    _check(lib().cf_step_host(problem._h, _ptr(Uc.view(np.float64)), _ptr(Pc.view(np.float64)), float(t),
+                              int(nsteps), ctypes.byref(tout), None))
+    if not direct:
+        U[...] = Uc
+        P[...] = Pc
+    return tout.value
 
 
 def _download_into(problem, U, P):

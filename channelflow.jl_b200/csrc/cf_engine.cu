@@ -18,6 +18,9 @@
 #include "cf_dispatch.h"
 #include "cf_cheb.cuh"
 
+// kz-plane chunks of the state in a host-buffer step (cf_step_host)
+#define CF_HOST_CHUNKS 8
+
 static_assert(CF_FORM_ROTATIONAL == NL_ROT && CF_FORM_CONVECTIVE == NL_CONV && CF_FORM_DIVERGENCE == NL_DIV,
               "cf_config.form values are the device form tags");
 
@@ -248,6 +251,10 @@ struct cf_engine {
     double* d_diagpart = nullptr;  // diagnostics block partials (3 per column block)
     cudaGraphExec_t graph = nullptr;
     int last_launches = 0;
+    // host-buffer steps (cf_step_host): the copy stream and the events that
+    // order the kz-plane chunks of the state between it and the handle stream
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t hev[2 * CF_HOST_CHUNKS + 2] = {};
     std::vector<void*> allocs;
 };
 
@@ -1009,6 +1016,70 @@ static int validate_and_size(cf_engine* h, const cf_config* c) {
     return CF_OK;
 }
 
+// ---- host-buffer steps: the state crosses PCIe in kz-plane chunks that
+// overlap the column kernels on either side of the step
+//
+// Chunk k holds the kz planes [zb[k], zb[k+1]) of every y plane: columns
+// [zb[k] Nxh, zb[k+1] Nxh) (column c = kz Nxh + kx), whole column blocks when
+// zb[k] Nxh is a multiple of CF_NCOL.  Returns the number of chunks.
+static int host_chunks(const cf_engine* h, int* zb) {
+    const int K = std::min(CF_HOST_CHUNKS, std::max(1, h->Nz / 2));
+    zb[0] = 0;
+    for (int k = 1; k < K; ++k) {
+        int z = (int)((long)k * h->Nz / K);
+        if (((long)z * h->Nxh) % CF_NCOL) z -= 1;  // Nxh odd: an even plane (Nz >= 2K keeps them increasing)
+        zb[k] = z;
+    }
+    zb[K] = h->Nz;
+    return K;
+}
+static unsigned chunk_block(const cf_engine* h, const int* zb, int K, int k) {
+    return k >= K ? col_blocks(h) : (unsigned)(((long)zb[k] * h->Nxh) / CF_NCOL);
+}
+// copy kz planes [z0, z1) of every y plane of one field (pitched: a y plane
+// is B = Nz Nxh complex, the chunk a contiguous run of it)
+static int copy_planes(void* dst, const void* src, const cf_engine* h, int z0, int z1, cudaMemcpyKind kind,
+                       cudaStream_t st) {
+    const size_t pitch = sizeof(zd) * (size_t)h->B, off = sizeof(zd) * (size_t)z0 * h->Nxh;
+    const size_t width = sizeof(zd) * (size_t)(z1 - z0) * h->Nxh;
+    CU(cudaMemcpy2DAsync((char*)dst + off, pitch, (const char*)src + off, pitch, width, (size_t)h->Ny, kind, st));
+    return CF_OK;
+}
+static int ensure_copy_stream(cf_engine* h) {
+    if (h->cstream) return CF_OK;
+    CU(cudaStreamCreateWithFlags(&h->cstream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : h->hev) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return CF_OK;
+}
+// column kernel over the blocks [b0, b1) of the columns
+static int launch_cols(cf_engine* h, int kind, ColParams p, unsigned b0, unsigned b1, int* count) {
+    if (b1 <= b0) return CF_OK;
+    p.bofs = (int)b0;
+    col_kernel(kind, h->P)<<<b1 - b0, CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    if (count) *count += 1;
+    CU(cudaGetLastError());
+    return CF_OK;
+}
+// prep (nodal fields of the state) and stage-j column kernel of the FP64
+// forms and of the mixed form with the Chebyshev transforms in the kernel
+static int host_prep_kind(const cf_engine* h, ColParams& p) {
+    p = col_params(h);
+    if (h->mixed) {
+        for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
+        return KC_PREP_MXD;
+    }
+    return h->form == NL_CONV ? KC_PREP_CONV : (h->form == NL_DIV ? KC_PREP_DIV : KC_PREP);
+}
+static int host_stage_kind(const cf_engine* h, int j, ColParams& p) {
+    p = stage_col_params(h, j);
+    if (h->mixed) {
+        for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->nod32[i]);
+        for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
+        return KC_STAGE_MXD;
+    }
+    return stage_kernel_kind(h);
+}
+
 static void host_synth(const cf_engine* h, uint64_t seed, double amp, int shape, double rho, std::vector<std::complex<double>>& U);
 
 extern "C" {
@@ -1019,7 +1090,11 @@ void cf_destroy(cf_handle* h) {
     if (!h) return;
     drop_graph(h);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->cstream) cudaStreamSynchronize(h->cstream);
     for (void* p : h->allocs) cudaFree(p);
+    for (cudaEvent_t e : h->hev)
+        if (e) cudaEventDestroy(e);
+    if (h->cstream) cudaStreamDestroy(h->cstream);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -1224,6 +1299,104 @@ int cf_step_dt(cf_handle* h, double t, double dt, double* t_out, double* grads_o
     h->last_launches = cnt;
     if (t_out) *t_out = t + dt;
     if (grads_out && (rc = check_cheb_err(h))) return rc;
+    if (grads_out) {
+        double g[2];
+        CU(cudaMemcpyAsync(g, h->d_grad, 16, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        grads_out[0] = g[0];
+        grads_out[1] = g[1];
+    }
+    return CF_OK;
+}
+
+// step! over host arrays (cnrk2.jl:149-207 with CPU fields): upload U and
+// P, advance nsteps, download the new U and P.  The state crosses PCIe in
+// kz-plane chunks on a copy stream: the nodal fields of chunk k are computed
+// while chunk k+1 arrives; the pressure, first read by the first stage's
+// column kernel, arrives during that stage's periodic transforms; the last
+// stage's column kernel runs chunk by chunk, each chunk downloaded while the
+// next is computed.  That kernel leaves out the nodal fields of a following
+// stage (a host step's successor uploads a new state), so afterwards the
+// handle's nodal fields are stale and a following cf_step recomputes them
+// from the state, which gives the same values.
+int cf_step_host(cf_handle* h, double* U, double* P, double t, int nsteps, double* t_out, double* grads_out) {
+    if (!h || !U || !P) return fail(CF_E_ARG, "null argument");
+    if (nsteps < 0) return fail(CF_E_ARG, "nsteps must be nonnegative");
+    int rc;
+    if (nsteps == 0 || (h->mixed && h->tc)) {
+        // the tensor-core form transforms all columns in one launch: no chunks
+        if ((rc = cf_set_state(h, U, P)) || (rc = cf_step(h, t, nsteps, t_out, grads_out))) return rc;
+        return cf_get_state(h, U, P);
+    }
+    if ((rc = ensure_copy_stream(h))) return rc;
+    if (nsteps > 2 && (rc = build_graph(h))) return rc;
+    int zb[CF_HOST_CHUNKS + 1];
+    const int K = host_chunks(h, zb);
+    cudaEvent_t* up = h->hev + 1;                    // velocity chunks 0..K-1, then the pressure
+    cudaEvent_t* dn = h->hev + CF_HOST_CHUNKS + 2;   // last-stage column chunks
+    const size_t fd = 2 * (size_t)h->nr;  // doubles per field
+    zd* dev[4] = {h->U[0], h->U[1], h->U[2], h->Pf};
+    double* host[4] = {U, U + fd, U + 2 * fd, P};
+    // the copies of the state follow the work already queued on the handle
+    CU(cudaEventRecord(h->hev[0], h->stream));
+    CU(cudaStreamWaitEvent(h->cstream, h->hev[0], 0));
+    auto run = [&]() -> int {
+        int r, cnt = 0;
+        for (int k = 0; k < K; ++k) {
+            for (int i = 0; i < 3; ++i)
+                if ((r = copy_planes(dev[i], host[i], h, zb[k], zb[k + 1], cudaMemcpyHostToDevice, h->cstream)))
+                    return r;
+            CU(cudaEventRecord(up[k], h->cstream));
+        }
+        if ((r = copy_planes(dev[3], host[3], h, 0, h->Nz, cudaMemcpyHostToDevice, h->cstream))) return r;
+        CU(cudaEventRecord(up[K], h->cstream));
+        ColParams pp;
+        const int kprep = host_prep_kind(h, pp);
+        for (int k = 0; k < K; ++k) {
+            CU(cudaStreamWaitEvent(h->stream, up[k], 0));
+            if ((r = launch_cols(h, kprep, pp, chunk_block(h, zb, K, k), chunk_block(h, zb, K, k + 1), &cnt)))
+                return r;
+        }
+        h->nodal_valid = true;
+        for (int s = 0; s < nsteps; ++s) {
+            const bool first = s == 0, last = s == nsteps - 1;
+            if (!first && !last) {
+                CU(cudaGraphLaunch(h->graph, h->stream));
+                cnt += step_launches(h);
+                continue;
+            }
+            for (int j = 0; j < 3; ++j) {
+                if ((r = h->mixed ? launch_periodic32(h, &cnt) : launch_periodic(h, &cnt))) return r;
+                if (first && j == 0) CU(cudaStreamWaitEvent(h->stream, up[K], 0));
+                ColParams p;
+                const int kind = host_stage_kind(h, j, p);
+                if (!(last && j == 2)) {
+                    if ((r = launch_cols(h, kind, p, 0, col_blocks(h), &cnt))) return r;
+                    continue;
+                }
+                p.skip_nodal = 1;
+                h->nodal_valid = false;
+                for (int k = 0; k < K; ++k) {
+                    if ((r = launch_cols(h, kind, p, chunk_block(h, zb, K, k), chunk_block(h, zb, K, k + 1), &cnt)))
+                        return r;
+                    CU(cudaEventRecord(dn[k], h->stream));
+                    CU(cudaStreamWaitEvent(h->cstream, dn[k], 0));
+                    for (int i = 0; i < 4; ++i)
+                        if ((r = copy_planes(host[i], dev[i], h, zb[k], zb[k + 1], cudaMemcpyDeviceToHost, h->cstream)))
+                            return r;
+                }
+            }
+        }
+        h->last_launches = cnt;
+        return CF_OK;
+    };
+    rc = run();
+    // no copy into or out of the caller's buffers outlives the call
+    const cudaError_t e = cudaStreamSynchronize(h->cstream);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(CF_E_CUDA, std::string("host step copies: ") + cudaGetErrorString(e));
+    if ((rc = check_cheb_err(h))) return rc;
+    if (t_out) *t_out = t + nsteps * h->dt;
     if (grads_out) {
         double g[2];
         CU(cudaMemcpyAsync(g, h->d_grad, 16, cudaMemcpyDeviceToHost, h->stream));

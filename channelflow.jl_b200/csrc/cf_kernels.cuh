@@ -56,6 +56,8 @@ struct ColParams {
     double* grad_out;        // [2]
     double* status;          // [4] diagnostics scratch (unused by the hot path)
     FftPlan plP;
+    int bofs;        // first column block of the launch (a launch over part of the columns)
+    int skip_nodal;  // stage kernels: end after storing the state (no nodal fields for a next stage)
     const zd* cs_tab;  // (cos, sin)(pi n / P)
     const double* helm_tab;  // [3][Ny] degree coefficients of the integrated tau rows
     double fnorm;  // 1 / (Nxp Nzp (Ny-1))
@@ -95,7 +97,7 @@ struct ColCtx {
         t.P = PL ? PL : p.P;
         t.hs = (t.P >> 1) + 1;
         t.xch = sm + (long)NCOL * (6 * cs + 2 * zs) + 2 * tm;
-        c0 = bx * NCOL;
+        c0 = (bx + p.bofs) * NCOL;
         c = c0 + tm;
         valid = c < p.B;
         ix = c % p.Nxh;
@@ -557,6 +559,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     tile_store<NCOL, PL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
     tile_store<NCOL, PL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
     tile_store<NCOL, PL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
+    if (p.skip_nodal) return;
     __syncthreads();
     // ---------------- Phase C: total velocity, vorticity, nodal values
     if (valid)

@@ -105,6 +105,14 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
  * *t_out = t + dt. */
 int cf_step_dt(cf_handle* h, double t, double dt, double* t_out, double* grads_out);
 
+/* step!(scheme, nlterm, U, P, t; ...) on host fields (CPU arrays of the
+ * layout of cf_set_state; cnrk2.jl:149-207): the engine state becomes U, P,
+ * nsteps steps run, and the new state is written back into U, P.  Equal to
+ * cf_set_state + cf_step + cf_get_state, with the transfers overlapped with
+ * the first and last column kernels (kz-plane chunks on a copy stream).
+ * Pinned buffers give full PCIe bandwidth.  *t_out, grads_out as cf_step. */
+int cf_step_host(cf_handle* h, double* U, double* P, double t, int nsteps, double* t_out, double* grads_out);
+
 /* NonLinearTerm(t, U, N) of the handle's form on host buffers (nonlinear.jl:113-193). */
 int cf_nonlinear(cf_handle* h, const double* U, double* N);
 
