@@ -286,13 +286,18 @@ static int rup8(int x) { return (x + 7) & ~7; }
 static int zbs(const cf_engine* h) { return fft_bufsz(h->Nzp) + 1; }
 static int xbs(const cf_engine* h) { return rup8(h->Nxp); }
 static size_t zsmem(const cf_engine* h) { return (size_t)2 * h->tkz * zbs(h) * sizeof(zd); }
-// TMA z kernels: transform buffers, then (128-aligned) the staging rows of the
-// longer of the nodal and z-padded transfers; es = bytes per complex element
-static size_t zstage_off(const cf_engine* h, size_t es) { return ((zsmem(h) / sizeof(zd)) * es + 127) & ~(size_t)127; }
-static size_t zsmem_tma(const cf_engine* h, size_t es) {
+// TMA z kernels: the first transform buffer, then (128-aligned) the second,
+// which also stages the rows of the nodal and z-padded transfers (boxes
+// rounded up to whole boxes); es = bytes per complex element.  Either buffer
+// stages the stored rows, so the rounded row counts must fit one buffer.
+static int zstage_rows(const cf_engine* h) {
     const int rz = ((h->Nz + h->zbox - 1) / h->zbox) * h->zbox, rp = ((h->Nzp + h->zpbox - 1) / h->zpbox) * h->zpbox;
-    return zstage_off(h, es) + (size_t)std::max(rz, rp) * h->tkz * es;
+    return std::max(rz, rp);
 }
+static size_t zstage_off(const cf_engine* h, size_t es) {
+    return ((size_t)h->tkz * zbs(h) * es + 127) & ~(size_t)127;
+}
+static size_t zsmem_tma(const cf_engine* h, size_t es) { return zstage_off(h, es) + (size_t)h->tkz * zbs(h) * es; }
 // x-pass shared memory: 12 slots of round_up(Nxp, 8) (two rows of the FP32
 // rotational form, the convective and divergence forms), or 6 slots of
 // fft_bufsz(Nxp) (one row of the FP64 rotational form)
@@ -904,12 +909,13 @@ static void encode_maps(cf_engine* h) {
         if (h->nod[i]) ok = encode_field(h, &h->maps64.nod[i], h->nod[i], h->Nz, h->zbox, false);
     for (int i = 0; i < 9 && ok; ++i)
         if (h->zp[i]) ok = encode_field(h, &h->maps64.zp[i], h->zp[i], h->Nzp, h->zpbox, false);
+    ok = ok && zstage_rows(h) <= zbs(h);
     h->tma64 = ok && zsmem_tma(h, sizeof(zd)) <= (size_t)227 * 1024;
     if (h->mixed) {
         ok = h->d_ffterr != nullptr && h->tkz <= 2;
         for (int i = 0; i < 6 && ok; ++i) ok = encode_field(h, &h->maps32.nod[i], h->nod32[i], h->Nz, h->zbox, true);
         for (int i = 0; i < 6 && ok; ++i) ok = encode_field(h, &h->maps32.zp[i], h->zp32[i], h->Nzp, h->zpbox, true);
-        h->tma32 = ok && zsmem_tma(h, sizeof(zf)) <= (size_t)227 * 1024;
+        h->tma32 = ok && zstage_rows(h) <= zbs(h) && zsmem_tma(h, sizeof(zf)) <= (size_t)227 * 1024;
     }
 }
 

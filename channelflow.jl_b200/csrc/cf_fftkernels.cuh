@@ -132,12 +132,15 @@ CF_DEV void zinv_body(const FftParams& p, int bx, int n, int f) {
 
 // The z kernels with their strided row gathers and scatters done by TMA:
 // tkz columns x all rows of one plane move as boxes of (2 tkz scalars, zbox
-// rows) between the global fields and a dense staging buffer in shared memory
+// rows) between the global fields and a dense staging layout in shared memory
 // (stage[row * tkz + t]), so the strided 32-byte row segments cost no L1
 // wavefronts.  Rows past the end of a box load as zeros and are not stored.
-// smem: the 2*tkz*bsz transform elements, then (at byte p.stoff, 128-aligned)
-// the staging buffer.  One thread issues the copies; every wait is bounded
-// (p.err set, the block returns).
+// smem: two transform buffers of tkz*bsz elements, the second at byte p.stoff
+// (128-aligned), which also stages the rows: the loaded rows are unpacked from
+// it before the transform uses it, and the result is packed for the store into
+// whichever buffer the last pass did not write (no third buffer, so four
+// blocks fit per SM at Nzp = 576 in FP64).  One thread issues the copies;
+// every wait is bounded (p.err set, the block returns).
 template <class Z>
 CF_DEV Z* zstage(const FftParams& p) {
     extern __shared__ __align__(128) unsigned char fsm_raw[];
@@ -177,26 +180,26 @@ CF_DEV void zinv_tma_body(const FftParams& p, const FftMaps& m, int bx, int n, i
     extern __shared__ __align__(128) unsigned char fsm_raw[];
     __shared__ __align__(8) uint64_t mbar;
     Z* sm = reinterpret_cast<Z*>(fsm_raw);
-    Z* stage = zstage<Z>(p);
+    Z* const bufB = zstage<Z>(p);
     const int tks = p.tks, tkz = 1 << tks, tm = tkz - 1;
     const int k0 = bx << tks;
     const int Nz = p.Nz, Nzp = LZ ? LZ : p.Nzp, Nxh = p.Nxh, bs = p.bsz;
-    Z* bufB = sm + tkz * bs;
     const bool dz = f >= 6;
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1, znyq = (Nz % 2 == 0) ? Nz / 2 : -1;
     // zero the padding gap while the rows arrive
     const int gap0 = (Nz >> 1) + 1, gap1 = Nzp - (Nz - gap0);
     for (int e = threadIdx.x; e < ((gap1 - gap0) << tks); e += blockDim.x)
         sm[(e & tm) * bs + fpos(gap0 + (e >> tks))] = czero<Z>();
-    if (!zload_tma<Z>(p, &m.nod[dz ? f - 6 : f], k0, Nz, p.zbox, n, stage, &mbar)) return;
+    if (!zload_tma<Z>(p, &m.nod[dz ? f - 6 : f], k0, Nz, p.zbox, n, bufB, &mbar)) return;
     for (int e = threadIdx.x; e < (Nz << tks); e += blockDim.x) {
         const int iz = e >> tks, k = k0 + (e & tm);
-        Z v = (k < Nxh && iz != znyq && k != xnyq) ? stage[e] : czero<Z>();
+        Z v = (k < Nxh && iz != znyq && k != xnyq) ? bufB[e] : czero<Z>();
         if (dz) v = cmuli(v, p.bz * (double)(iz <= (Nz >> 1) ? iz : iz - Nz));
         sm[(e & tm) * bs + fpos(zpad_index(iz, Nz, Nzp))] = v;
     }
     __syncthreads();
     const Z* res = group_fft_L<true, LZ>(sm, bufB, tkz, bs, p.plZ, +1, threadIdx.x, blockDim.x, 0);
+    Z* stage = (res == sm) ? bufB : sm;
     for (int e = threadIdx.x; e < (Nzp << tks); e += blockDim.x) stage[e] = res[(e & tm) * bs + fpos(e >> tks)];
     zstore_tma<Z>(p, &m.zp[f], k0, Nzp, p.zpbox, n, stage);
 }
@@ -206,15 +209,15 @@ CF_DEV void zfwd_tma_body(const FftParams& p, const FftMaps& m, int bx, int n, i
     extern __shared__ __align__(128) unsigned char fsm_raw[];
     __shared__ __align__(8) uint64_t mbar;
     Z* sm = reinterpret_cast<Z*>(fsm_raw);
-    Z* stage = zstage<Z>(p);
+    Z* const bufB = zstage<Z>(p);
     const int tks = p.tks, tkz = 1 << tks, tm = tkz - 1;
     const int k0 = bx << tks;
     const int Nz = p.Nz, Nzp = LZ ? LZ : p.Nzp, bs = p.bsz;
-    Z* bufB = sm + tkz * bs;
-    if (!zload_tma<Z>(p, &m.zp[f], k0, Nzp, p.zpbox, n, stage, &mbar)) return;
-    for (int e = threadIdx.x; e < (Nzp << tks); e += blockDim.x) sm[(e & tm) * bs + fpos(e >> tks)] = stage[e];
+    if (!zload_tma<Z>(p, &m.zp[f], k0, Nzp, p.zpbox, n, bufB, &mbar)) return;
+    for (int e = threadIdx.x; e < (Nzp << tks); e += blockDim.x) sm[(e & tm) * bs + fpos(e >> tks)] = bufB[e];
     __syncthreads();
     const Z* res = group_fft_L<true, LZ>(sm, bufB, tkz, bs, p.plZ, -1, threadIdx.x, blockDim.x, 0);
+    Z* stage = (res == sm) ? bufB : sm;
     for (int e = threadIdx.x; e < (Nz << tks); e += blockDim.x)
         stage[e] = res[(e & tm) * bs + fpos(zpad_index(e >> tks, Nz, Nzp))];
     zstore_tma<Z>(p, &m.nod[f], k0, Nz, p.zbox, n, stage);
@@ -555,12 +558,15 @@ template <int LZ, class Z = zd>
 __global__ void __launch_bounds__(256) k_zinv(FftParams p) {
     zinv_body<LZ, Z>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
+// five blocks per SM (two transform buffers of 2 x 657 complex at Nzp = 576
+// in FP64; the register cap spills a few words, measured faster than four:
+// 1.27 against 1.35 ms for the z-inverse at 384x257x384)
 template <int LZ, class Z = zd>
-__global__ void __launch_bounds__(256) k_zinv_tma(FftParams p, const __grid_constant__ FftMaps m) {
+__global__ void __launch_bounds__(256, 5) k_zinv_tma(FftParams p, const __grid_constant__ FftMaps m) {
     zinv_tma_body<LZ, Z>(p, m, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int LZ, class Z = zd>
-__global__ void __launch_bounds__(256) k_zfwd_tma(FftParams p, const __grid_constant__ FftMaps m) {
+__global__ void __launch_bounds__(256, 5) k_zfwd_tma(FftParams p, const __grid_constant__ FftMaps m) {
     zfwd_tma_body<LZ, Z>(p, m, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int LZ, class Z = zd>
