@@ -558,15 +558,16 @@ template <int LZ, class Z = zd>
 __global__ void __launch_bounds__(256) k_zinv(FftParams p) {
     zinv_body<LZ, Z>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
-// five blocks per SM (two transform buffers of 2 x 657 complex at Nzp = 576
-// in FP64; the register cap spills a few words, measured faster than four:
-// 1.27 against 1.35 ms for the z-inverse at 384x257x384)
+// five blocks per SM in FP64 (two transform buffers of 2 x 657 complex at
+// Nzp = 576; the register cap spills a few words, measured faster than four:
+// 1.27 against 1.35 ms for the z-inverse at 384x257x384), six in FP32 (the
+// register count they take uncapped)
 template <int LZ, class Z = zd>
-__global__ void __launch_bounds__(256, 5) k_zinv_tma(FftParams p, const __grid_constant__ FftMaps m) {
+__global__ void __launch_bounds__(256, (sizeof(Z) == 16 ? 5 : 6)) k_zinv_tma(FftParams p, const __grid_constant__ FftMaps m) {
     zinv_tma_body<LZ, Z>(p, m, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int LZ, class Z = zd>
-__global__ void __launch_bounds__(256, 5) k_zfwd_tma(FftParams p, const __grid_constant__ FftMaps m) {
+__global__ void __launch_bounds__(256, (sizeof(Z) == 16 ? 5 : 6)) k_zfwd_tma(FftParams p, const __grid_constant__ FftMaps m) {
     zfwd_tma_body<LZ, Z>(p, m, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <int LZ, class Z = zd>
