@@ -300,9 +300,10 @@ static size_t zstage_off(const cf_engine* h, size_t es) {
 static size_t zsmem_tma(const cf_engine* h, size_t es) { return zstage_off(h, es) + (size_t)h->tkz * zbs(h) * es; }
 // x-pass shared memory: 12 slots of round_up(Nxp, 8) (two rows of the FP32
 // rotational form, the convective and divergence forms), or 6 slots of
-// fft_bufsz(Nxp) (one row of the FP64 rotational form)
+// fft_bufsz(Nxp) (one row of the FP64 rotational form), 3 with the
+// transforms in place
 static size_t xsmem(const cf_engine* h, int slots = 12) {
-    return (size_t)slots * (slots == 6 ? fft_bufsz(h->Nxp) : xbs(h)) * sizeof(zd);
+    return (size_t)slots * (slots < 12 ? fft_bufsz(h->Nxp) : xbs(h)) * sizeof(zd);
 }
 static int ilog2(int v) {
     int r = 0;
@@ -563,12 +564,15 @@ static PeriodicShape periodic_shape(const cf_engine* h) {
     // one z-row per block from Nxp > 256 (measured: 2.94 against 3.16 ms at
     // Nxp = 576), two below (0.18 against 0.23 ms at Nxp = 192)
     if (h->Nxp <= 256) return {6, 3, KF_XPASS2, 2};
+    // in-place transforms where the butterflies fit the block (half the shared
+    // memory, more blocks per SM)
+    if (h->Nxp == 512 || h->Nxp == 576) return {6, 3, KF_XPASS_IP, 1};
     return {6, 3, KF_XPASS, 1};
 }
 static int launch_periodic_kernels(cf_engine* h, cudaEvent_t* ev) {
     FftParams f = fft_params(h);
     const PeriodicShape s = periodic_shape(h);
-    const size_t smx = xsmem(h, s.xkind == KF_XPASS ? 6 : 12);
+    const size_t smx = s.xkind == KF_XPASS_IP ? xsmem(h, 3) : xsmem(h, s.xkind == KF_XPASS ? 6 : 12);
     launch_z(h, KF_ZINV, false, s.nzinv, f);
     if (ev) CU(cudaEventRecord(ev[0], h->stream));
     const dim3 gx((unsigned)((h->Nzp + s.xrows - 1) / s.xrows), (unsigned)h->Ny);
@@ -947,6 +951,7 @@ static int set_attrs(cf_engine* h) {
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_CONV, h->Nxp), need[2]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_DIV, h->Nxp), need[2]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS2, h->Nxp), need[2]))) return rc;
+    if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_IP, h->Nxp), xsmem(h, 3)))) return rc;
     if (h->tma64) {
         if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZINV, h->Nzp, false), zsmem_tma(h, sizeof(zd))))) return rc;
         if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZFWD, h->Nzp, false), zsmem_tma(h, sizeof(zd))))) return rc;

@@ -306,6 +306,65 @@ CF_DEV Z* fft_static(Z* src, Z* dst, int nb, int bs, const Z* tw, int sgn, int t
     }
 }
 
+// In-place form of fft_pass_static for groups with a thread per butterfly
+// (nb * L / R <= nth): a thread reads its butterfly's R inputs, the group
+// synchronises, and the thread writes its R outputs over the same buffer.
+// One buffer per transform instead of two (twice the transforms per shared
+// memory) for one more barrier per pass.
+template <bool BLOCK, int POS, int L, int Ns, int R, class Z>
+CF_DEV void fft_pass_static_ip(Z* buf, int nb, int bs, const Z* __restrict__ tw, int sgn, int tid, int nth, int bar) {
+    constexpr int NBf = L / R;
+    constexpr int step = L / (Ns * R);
+    constexpr bool LIN_LD = POS == 0 && (NBf % 8) == 0;
+    constexpr bool LIN_ST = POS == 0 && ((Ns % 8) == 0 || (Ns == 1 && 8 % R == 0));
+    constexpr int DLD = NBf + NBf / 8;
+    constexpr int DST = (Ns == 1) ? 1 : Ns + Ns / 8;
+    const bool act = tid < nb * NBf;
+    const int b = act ? tid / NBf : 0, j = tid - b * NBf;
+    const int k = j % Ns;
+    Z v[R];
+    if (act) {
+        const Z* s = buf + (long)b * bs;
+        const int pj = bpos<POS>(j);
+        Z w[R];
+        if constexpr (Ns > 1) tw_powers<R>(tw, k * step, sgn, w);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            Z x = s[LIN_LD ? pj + r * DLD : bpos<POS>(j + r * NBf)];
+            if constexpr (Ns > 1) v[r] = (r == 0 || k == 0) ? x : zmul(x, w[r]);
+            else v[r] = x;
+        }
+        dft_small<R>(v, sgn);
+    }
+    group_sync<BLOCK>(bar, nth);
+    if (act) {
+        Z* d = buf + (long)b * bs;
+        const int o = (j / Ns) * Ns * R + k;
+        const int po = bpos<POS>(o);
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[LIN_ST ? po + r * DST : bpos<POS>(o + r * Ns)] = v[r];
+    }
+    group_sync<BLOCK>(bar, nth);
+}
+template <class Z, bool BLOCK, int POS, int L, int Ns, int R, int... Rest>
+CF_DEV void fft_static_ip(Z* buf, int nb, int bs, const Z* tw, int sgn, int tid, int nth, int bar) {
+    fft_pass_static_ip<BLOCK, POS, L, Ns, R>(buf, nb, bs, tw, sgn, tid, nth, bar);
+    if constexpr (sizeof...(Rest) > 0) fft_static_ip<Z, BLOCK, POS, L, Ns * R, Rest...>(buf, nb, bs, tw, sgn, tid, nth, bar);
+}
+// lengths with an in-place plan, and the most butterflies of one transform's
+// passes (nb times it must not exceed the group's threads)
+template <int L>
+__host__ __device__ constexpr int fft_ip_butterflies() {
+    return L == 512 ? 64 : (L == 576 ? 72 : 0);
+}
+template <bool BLOCK, int L, int POS = 0, class Z>
+CF_DEV void group_fft_ip(Z* a, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
+    static_assert(fft_ip_butterflies<L>() > 0, "no in-place plan for this length");
+    const Z* tw = plan_tw<Z>(pl);
+    if constexpr (L == 512) fft_static_ip<Z, BLOCK, POS, 512, 1, 8, 8, 8>(a, nb, bs, tw, sgn, tid, nth, bar);
+    else fft_static_ip<Z, BLOCK, POS, 576, 1, 8, 8, 9>(a, nb, bs, tw, sgn, tid, nth, bar);
+}
+
 // Full transform of nb sequences (length pl.L, element e of sequence b at
 // b*bs + bpos<POS>(e), bs >= fft_bufsz(L) for the padded layout, >=
 // round_up(L, 8) for the XOR layout) held in a; b is a scratch buffer of the

@@ -19,6 +19,11 @@
 
 #include "cf_fft.cuh"
 
+// blocks per SM of the in-place x-pass (bounds its registers)
+#ifndef CF_XPASS_IP_BLOCKS
+#define CF_XPASS_IP_BLOCKS 4
+#endif
+
 struct FftParams {
     int Nx, Nz, Nxh, Ny, Nzp, Nxp;
     int tks;       // log2 of the columns per block in the z kernels
@@ -455,6 +460,44 @@ CF_DEV void xpass_row_body(const FftParams& p, int z, int n) {
     });
 }
 
+// The same with the transforms in place (lengths with an in-place plan, whose
+// butterflies fit the block's threads: 3 x 72 at Nxp = 576): three slots of
+// fft_bufsz(Nxp), half the shared memory, so more blocks fit per SM.  The
+// product at x point j reads and writes slots 0-2 at j only (one thread per
+// j), so it runs in place without a barrier of its own.
+template <int LX>
+CF_DEV void xpass_row_ip_body(const FftParams& p, int z, int n) {
+    static_assert(3 * fft_ip_butterflies<LX>() <= 256, "one butterfly per thread");
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    zd* sm = reinterpret_cast<zd*>(fsm_raw);
+    const int Nxh = p.Nxh, bs = p.bsxp;
+    const long row = ((long)n * p.Nzp + z) * Nxh;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
+    xpack<zd, 0, 3, false>(sm, bs, Nxh, LX, xnyq, [&](int slot, int k, zd& X, zd& Y) {
+        X = zp_of<zd>(p, 2 * slot)[row + k];
+        Y = zp_of<zd>(p, 2 * slot + 1)[row + k];
+    });
+    __syncthreads();
+    group_fft_ip<true, LX, 0>(sm, 3, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
+    for (int j = threadIdx.x; j < LX; j += blockDim.x) {
+        const int sj = fpos(j);
+        const zd a0 = sm[sj], a1 = sm[bs + sj], a2 = sm[2 * bs + sj];
+        // u = (a0.x, a0.y, a1.x), omega = (a1.y, a2.x, a2.y)
+        sm[sj] = zmake(a0.y * a2.y - a1.x * a2.x, a1.x * a1.y - a0.x * a2.y);
+        sm[bs + sj] = zmake(a0.x * a2.x - a0.y * a1.y, 0.0);
+    }
+    __syncthreads();
+    group_fft_ip<true, LX, 0>(sm, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
+    xunpack<zd, 0, 2, false>(sm, bs, Nxh, LX, [&](int slot, int k, zd X, zd Y) {
+        if (slot == 0) {
+            zp_of<zd>(p, 0)[row + k] = X;
+            zp_of<zd>(p, 1)[row + k] = Y;
+        } else {
+            zp_of<zd>(p, 2)[row + k] = X;
+        }
+    });
+}
+
 // Convective form (nonlinear.jl:113-140, dot! operators.jl:247-254).  grid:
 // (Nzp, Ny); block 256; smem 12*bsx complex.  One row z = bx of plane n, twelve
 // real rows packed in six slots: field codes 0-2 u (z-padded 0-2), 3-5 du/dx
@@ -582,6 +625,12 @@ __global__ void __launch_bounds__(256, (sizeof(Z) == 16 ? 3 : 4)) k_xpass(FftPar
 }
 // FP64, two rows per block (padded lengths up to 256, where one row leaves
 // most of the block idle in the FFT passes)
+// in-place transforms (lengths with an in-place plan; other lengths compile an
+// empty kernel that the engine never selects)
+template <int LX>
+__global__ void __launch_bounds__(256, CF_XPASS_IP_BLOCKS) k_xpass_ip(FftParams p) {
+    if constexpr (fft_ip_butterflies<LX>() > 0) xpass_row_ip_body<LX>(p, blockIdx.x, blockIdx.y);
+}
 template <int LX>
 __global__ void __launch_bounds__(256) k_xpass2(FftParams p) {
     xpass_body<LX, zd>(p, blockIdx.x, blockIdx.y);
