@@ -326,13 +326,14 @@ CF_DEV void fft_pass_static_ip(Z* buf, int nb, int bs, const Z* __restrict__ tw,
     if (act) {
         const Z* s = buf + (long)b * bs;
         const int pj = bpos<POS>(j);
-        Z w[R];
-        if constexpr (Ns > 1) tw_powers<R>(tw, k * step, sgn, w);
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            Z x = s[LIN_LD ? pj + r * DLD : bpos<POS>(j + r * NBf)];
-            if constexpr (Ns > 1) v[r] = (r == 0 || k == 0) ? x : zmul(x, w[r]);
-            else v[r] = x;
+        for (int r = 0; r < R; ++r) v[r] = s[LIN_LD ? pj + r * DLD : bpos<POS>(j + r * NBf)];
+        if constexpr (Ns > 1) {
+            Z w[R];
+            tw_powers<R>(tw, k * step, sgn, w);
+#pragma unroll
+            for (int r = 1; r < R; ++r)
+                if (k != 0) v[r] = zmul(v[r], w[r]);
         }
         dft_small<R>(v, sgn);
     }

@@ -19,9 +19,15 @@
 
 #include "cf_fft.cuh"
 
-// blocks per SM of the in-place x-pass (bounds its registers)
+// blocks per SM of the in-place x-pass (bounds its registers), and the x
+// positions per thread of its row loads: one (measured at 384x257x384: 2.21
+// ms, against 2.28 with two positions, whose loads in flight spill at this
+// register bound, and 2.27 at five blocks per SM)
 #ifndef CF_XPASS_IP_BLOCKS
 #define CF_XPASS_IP_BLOCKS 4
+#endif
+#ifndef CF_XPASS_IP_KPT
+#define CF_XPASS_IP_KPT 1
 #endif
 
 struct FftParams {
@@ -272,7 +278,7 @@ CF_DEV void zfwd_body(const FftParams& p, int bx, int n, int f) {
 // 1 XOR-swizzled).
 // FLAT: the (slot, position) pairs spread over all threads instead, with the
 // slot known at run time (more threads busy when rows are short).
-template <class Z, int POS, int NS, bool FLAT, class Get>
+template <class Z, int POS, int NS, bool FLAT, int KP = 0, class Get>
 CF_DEV void xpack(Z* sm, int bs, int Nxh, int Nxp, int xnyq, const Get& get) {
     if constexpr (FLAT) {
         const int Nxhp = Nxp / 2 + 1, tot = NS * Nxhp;
@@ -301,7 +307,7 @@ CF_DEV void xpack(Z* sm, int bs, int Nxh, int Nxp, int xnyq, const Get& get) {
             }
         }
     } else {
-        constexpr int KPT = NS <= 3 ? 2 : 1;
+        constexpr int KPT = KP ? KP : (NS <= 3 ? 2 : 1);  // positions per thread (loads in flight)
         const int Nxhp = Nxp / 2 + 1, NT = blockDim.x;
         for (int k0 = threadIdx.x; k0 < Nxhp; k0 += KPT * NT) {
             Z X[NS][KPT], Y[NS][KPT];
@@ -473,7 +479,7 @@ CF_DEV void xpass_row_ip_body(const FftParams& p, int z, int n) {
     const int Nxh = p.Nxh, bs = p.bsxp;
     const long row = ((long)n * p.Nzp + z) * Nxh;
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
-    xpack<zd, 0, 3, false>(sm, bs, Nxh, LX, xnyq, [&](int slot, int k, zd& X, zd& Y) {
+    xpack<zd, 0, 3, false, CF_XPASS_IP_KPT>(sm, bs, Nxh, LX, xnyq, [&](int slot, int k, zd& X, zd& Y) {
         X = zp_of<zd>(p, 2 * slot)[row + k];
         Y = zp_of<zd>(p, 2 * slot + 1)[row + k];
     });
