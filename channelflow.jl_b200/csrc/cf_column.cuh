@@ -1,9 +1,10 @@
 // cf_column.cuh -- per-column (one Fourier pair (k,l), all Chebyshev degrees)
 // device building blocks.  A team of two warps owns one column: warp q holds
 // the degrees of parity q.  A column vector lives in shared memory split by
-// parity, degree n at position (n & 1) * hs + (n >> 1) with hs = P/2 + 1, so
-// each parity is a contiguous half and the recurrences below (which couple
-// degrees of one parity only) run inside one warp.
+// parity, degree n at position (n & 1) * hs + (n >> 1) (hs = col_half_stride:
+// P/2 + 1 rounded up to 4 mod 8), so each parity is a contiguous half and the
+// recurrences below (which couple degrees of one parity only) run inside one
+// warp.
 //
 // Reference arithmetic restated here:
 //  * Chebyshev derivative recurrence b_n = b_{n+2} + 2(n+1) a_{n+1}, b_0
@@ -46,7 +47,7 @@ struct Team {
     int tid;   // 0..63
     int bar;   // named barrier of the team (1 or 2)
     int P;     // highest degree (even)
-    int hs;    // half stride: P/2 + 1
+    int hs;    // half stride: col_half_stride(P)
     zd* xch;   // two complex of team scratch in shared memory
 };
 
@@ -55,6 +56,14 @@ struct Team {
 CF_DEV void tsync(const Team& t) {
     if (t.bar == 1) asm volatile("bar.sync 1, 64;" ::: "memory");
     else asm volatile("bar.sync 2, 64;" ::: "memory");
+}
+// Offset of the odd half: P/2 + 1 (the even degrees) rounded up to 4 mod 8
+// complex.  A loop over consecutive degrees puts the 8 threads of a 16-byte
+// access phase on 4 even and 4 odd positions, which then fall in disjoint
+// halves of the eight 16-byte bank groups (the column stride of the tiles,
+// 2 hs + 2, is 2 mod 8 for the same reason with two columns per block).
+__host__ __device__ constexpr int col_half_stride(int P) {
+    return ((P >> 1) + 1) + ((4 - ((P >> 1) + 1)) & 7);
 }
 // shared-memory position of degree (or node) n
 CF_DEV int ppos(int n, int hs) { return (n & 1) * hs + (n >> 1); }

@@ -95,8 +95,8 @@ CF_DEV Z cmuli(Z a, double s) {
 CF_DEV int zpad_index(int iz, int Nz, int Nzp) { return iz <= (Nz >> 1) ? iz : Nzp - (Nz - iz); }
 
 // grid: (ceil(Nxh/tkz), Ny, nfields); block 256; smem 2*tkz*bsz complex.
-// Column t of the block's tkz columns is transform t (stride bsz, odd, so the
-// column-interleaved staging stores hit distinct bank groups).  Fields 6-8
+// Column t of the block's tkz columns is transform t (stride bsz, chosen by
+// the host so that the column-interleaved stores hit distinct bank groups).  Fields 6-8
 // (convective form) are d/dz of nodal fields 0-2: i bz l times the nodal
 // values (ddx3!, operators.jl:14-23, applied after the Chebyshev transform,
 // with which it commutes).

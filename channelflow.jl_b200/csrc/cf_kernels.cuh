@@ -95,7 +95,7 @@ struct ColCtx {
         t.lane = t.tid & 31;
         t.bar = 1 + tm;
         t.P = PL ? PL : p.P;
-        t.hs = (t.P >> 1) + 1;
+        t.hs = col_half_stride(t.P);
         t.xch = sm + (long)NCOL * (6 * cs + 2 * zs) + 2 * tm;
         c0 = (bx + p.bofs) * NCOL;
         c = c0 + tm;
