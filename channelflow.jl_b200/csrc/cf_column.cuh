@@ -48,7 +48,7 @@ struct Team {
     int bar;   // named barrier of the team (1 or 2)
     int P;     // highest degree (even)
     int hs;    // half stride: col_half_stride(P)
-    zd* xch;   // two complex of team scratch in shared memory
+    zd* xch;   // four complex of team scratch in shared memory
 };
 
 // Team barrier.  The ids are literal (a run-time id makes the compiler reserve
@@ -331,6 +331,166 @@ CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const F
         for (int m = t.lane; m <= H; m += 32)
             x[m] = (m == 0 || m == H) ? zscale(Z[fpos(m)], MODE == CF_DCT_FWD ? 1.0 : 2.0)
                                       : zadd(Z[fpos(m)], Z[fpos(P - m)]);
+    }
+    tsync(t);
+}
+
+// ---- two transforms at once: the team's FFT passes in place over both
+// vectors (transform b at z + b*bs), so both fit the two transform buffers
+// and the radix-8 passes keep all 64 threads busy (one butterfly per thread
+// instead of 32 threads for one transform).
+// In-place Stockham pass over NB transforms of length L (radix R, Ns = product
+// of the earlier radices), each thread holding up to BPT butterflies: all
+// reads, a team barrier, all writes, a team barrier.
+template <int L, int Ns, int R, int NB>
+CF_DEV void team_pass_ip(zd* buf, int bs, const zd* __restrict__ tw, int sgn, const Team& t) {
+    constexpr int NBf = L / R, TOT = NB * NBf, BPT = (TOT + CF_TEAM - 1) / CF_TEAM;
+    constexpr int step = L / (Ns * R);
+    constexpr bool LIN_LD = (NBf % 8) == 0;
+    constexpr bool LIN_ST = (Ns % 8) == 0 || (Ns == 1 && 8 % R == 0);
+    constexpr int DLD = NBf + NBf / 8;
+    constexpr int DST = (Ns == 1) ? 1 : Ns + Ns / 8;
+    zd v[BPT][R];
+#pragma unroll
+    for (int u = 0; u < BPT; ++u) {
+        const int q = t.tid + u * CF_TEAM;
+        if (TOT % CF_TEAM == 0 || q < TOT) {
+            const int b = q / NBf, j = q - b * NBf, k = j % Ns;
+            const zd* s = buf + b * bs;
+            const int pj = fpos(j);
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[u][r] = s[LIN_LD ? pj + r * DLD : fpos(j + r * NBf)];
+            if constexpr (Ns > 1) {
+                zd w[R];
+                tw_powers<R>(tw, k * step, sgn, w);
+#pragma unroll
+                for (int r = 1; r < R; ++r)
+                    if (k != 0) v[u][r] = zmul(v[u][r], w[r]);
+            }
+            dft_small<R>(v[u], sgn);
+        }
+    }
+    tsync(t);
+#pragma unroll
+    for (int u = 0; u < BPT; ++u) {
+        const int q = t.tid + u * CF_TEAM;
+        if (TOT % CF_TEAM == 0 || q < TOT) {
+            const int b = q / NBf, j = q - b * NBf, k = j % Ns;
+            zd* d = buf + b * bs;
+            const int o = (j / Ns) * Ns * R + k;
+            const int po = fpos(o);
+#pragma unroll
+            for (int r = 0; r < R; ++r) d[LIN_ST ? po + r * DST : fpos(o + r * Ns)] = v[u][r];
+        }
+    }
+    tsync(t);
+}
+template <int L, int Ns, int NB, int R, int... Rest>
+CF_DEV void team_fft_ip(zd* buf, int bs, const zd* tw, int sgn, const Team& t) {
+    team_pass_ip<L, Ns, R, NB>(buf, bs, tw, sgn, t);
+    if constexpr (sizeof...(Rest) > 0) team_fft_ip<L, Ns * R, NB, Rest...>(buf, bs, tw, sgn, t);
+}
+// forward FFT of length PL of the two transforms at z and z + bs (the
+// factorisations of group_fft_L; PL = 192, 256, 384)
+template <int PL>
+CF_DEV void col_team_fft2_body(zd* z, int bs, const FftPlan& pl, const Team& t) {
+    const zd* tw = pl.tw;
+    if constexpr (PL == 192) team_fft_ip<192, 1, 2, 8, 8, 3>(z, bs, tw, -1, t);
+    else if constexpr (PL == 256) team_fft_ip<256, 1, 2, 8, 8, 4>(z, bs, tw, -1, t);
+    else team_fft_ip<384, 1, 2, 8, 8, 2, 3>(z, bs, tw, -1, t);
+}
+template <int PL>
+CF_DEV_NOINLINE void col_team_fft2_ool(zd* z, int bs, const FftPlan pl, const Team t) {
+    col_team_fft2_body<PL>(z, bs, pl, t);
+}
+// lengths that transform in pairs: the long compile-time lengths (measured:
+// column kernel 6.06 -> 5.95 ms at P = 256; at P = 128, whose kernel is held
+// by registers and whose radix-8 passes have 16 butterflies per transform,
+// 0.399 -> 0.409 ms, so the shorter lengths keep single transforms)
+template <int PL>
+__host__ __device__ constexpr bool col_has_pair() {
+    return PL == 192 || PL == 256 || PL == 384;
+}
+// col_redft00 of two vectors xa, xb (transform buffers z and z + bs): the
+// same staging, transform and output steps, both vectors per step.
+template <int PL, int MODE>
+CF_DEV void col_redft00_pair(zd* xa, zd* xb, zd* z, int bs, const zd* __restrict__ cs, const FftPlan& pl,
+                             double scale, const Team& t) {
+    static_assert(col_has_pair<PL>(), "pair transforms need a compile-time length");
+    const int P = t.P, H = P >> 1, hs = t.hs;
+    const double we = (MODE == CF_DCT_FWD) ? scale : 1.0;
+    const double wi = (MODE == CF_DCT_FWD) ? scale : (MODE == CF_DCT_INV ? 0.5 : 1.0);
+    zd* const zb = z + bs;
+    zd x1a = zzero(), x1b = zzero();
+    for (int n = t.tid; n <= H; n += CF_TEAM) {
+        if (n == 0) {
+            const zd a = xa[0], b = xa[ppos(P, hs)], a2 = xb[0], b2 = xb[ppos(P, hs)];
+            z[fpos(0)] = zscale(zadd(a, b), 0.5 * we);
+            zb[fpos(0)] = zscale(zadd(a2, b2), 0.5 * we);
+            x1a = zaxpy(x1a, we, zsub(a, b));
+            x1b = zaxpy(x1b, we, zsub(a2, b2));
+        } else if (n == H) {
+            z[fpos(H)] = zscale(xa[ppos(H, hs)], wi);
+            zb[fpos(H)] = zscale(xb[ppos(H, hs)], wi);
+        } else {
+            const zd a = xa[ppos(n, hs)], b = xa[ppos(P - n, hs)];
+            const zd a2 = xb[ppos(n, hs)], b2 = xb[ppos(P - n, hs)];
+            const zd c = __ldg(cs + n);
+            const zd h = zscale(zadd(a, b), 0.5 * wi), d = zscale(zsub(a, b), wi);
+            const zd h2 = zscale(zadd(a2, b2), 0.5 * wi), d2 = zscale(zsub(a2, b2), wi);
+            z[fpos(n)] = zaxpy(h, -c.y, d);
+            z[fpos(P - n)] = zaxpy(h, c.y, d);
+            zb[fpos(n)] = zaxpy(h2, -c.y, d2);
+            zb[fpos(P - n)] = zaxpy(h2, c.y, d2);
+            x1a = zaxpy(x1a, 2.0 * c.x, d);
+            x1b = zaxpy(x1b, 2.0 * c.x, d2);
+        }
+    }
+    x1a = warp_sum_z(x1a);
+    x1b = warp_sum_z(x1b);
+    if (t.lane == 0) {
+        t.xch[t.q] = x1a;
+        t.xch[2 + t.q] = x1b;
+    }
+    tsync(t);
+    x1a = zadd(t.xch[0], t.xch[1]);
+    x1b = zadd(t.xch[2], t.xch[3]);
+    if constexpr (col_ool<PL>()) col_team_fft2_ool<PL>(z, bs, pl, t);
+    else col_team_fft2_body<PL>(z, bs, pl, t);
+    if (t.q == 1) {
+        const int lane = t.lane;
+        const int E = ((H + 31) >> 5) | 1;
+        const int m0 = lane * E;
+        zd ta = zzero(), tb = zzero();
+        for (int s = 0; s < E; ++s) {
+            const int m = m0 + s;
+            if (m >= 1 && m < H) {
+                ta = zadd(ta, zmuli(zsub(z[fpos(m)], z[fpos(P - m)])));
+                tb = zadd(tb, zmuli(zsub(zb[fpos(m)], zb[fpos(P - m)])));
+            }
+        }
+        zd ra = zadd(x1a, warp_excl_z(warp_scan_z(ta, lane), lane));
+        zd rb = zadd(x1b, warp_excl_z(warp_scan_z(tb, lane), lane));
+        zd* xoa = xa + hs;
+        zd* xob = xb + hs;
+        for (int s = 0; s < E; ++s) {
+            const int m = m0 + s;
+            if (m < H) {
+                if (m >= 1) {
+                    ra = zadd(ra, zmuli(zsub(z[fpos(m)], z[fpos(P - m)])));
+                    rb = zadd(rb, zmuli(zsub(zb[fpos(m)], zb[fpos(P - m)])));
+                }
+                xoa[m] = ra;
+                xob[m] = rb;
+            }
+        }
+    } else {
+        const double ew = MODE == CF_DCT_FWD ? 1.0 : 2.0;
+        for (int m = t.lane; m <= H; m += 32) {
+            const bool end = m == 0 || m == H;
+            xa[m] = end ? zscale(z[fpos(m)], ew) : zadd(z[fpos(m)], z[fpos(P - m)]);
+            xb[m] = end ? zscale(zb[fpos(m)], ew) : zadd(zb[fpos(m)], zb[fpos(P - m)]);
+        }
     }
     tsync(t);
 }

@@ -96,7 +96,7 @@ struct ColCtx {
         t.bar = 1 + tm;
         t.P = PL ? PL : p.P;
         t.hs = col_half_stride(t.P);
-        t.xch = sm + (long)NCOL * (6 * cs + 2 * zs) + 2 * tm;
+        t.xch = sm + (long)NCOL * (6 * cs + 2 * zs) + 4 * tm;
         c0 = (bx + p.bofs) * NCOL;
         c = c0 + tm;
         valid = c < p.B;
@@ -223,6 +223,11 @@ CF_DEV void col_forward_y(zd* x, zd* z, zd* z2, const ColParams& p, bool nyq, co
 template <int PL>
 CF_DEV void col_inverse_y(zd* x, zd* z, zd* z2, const ColParams& p, const Team& t) {
     col_redft00<PL, CF_DCT_INV>(x, z, z2, p.cs_tab, p.plP, 1.0, t);
+}
+// the same for two vectors at once (transform buffers z and z2, in place)
+template <int PL>
+CF_DEV void col_inverse_y2(zd* xa, zd* xb, zd* z, zd* z2, const ColParams& p, const Team& t) {
+    col_redft00_pair<PL, CF_DCT_INV>(xa, xb, z, (int)(z2 - z), p.cs_tab, p.plP, 1.0, t);
 }
 
 // Solve the Stokes problem of one column.  In: R0,R1,R2 (= Rx,Ry,Rz).
@@ -383,13 +388,25 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
     }
     if (MX) return;
     // omega_y = i (l u - k w) is formed from the nodal u and w below (the
-    // transform is linear): five transforms for the rotational form
-    constexpr int NF = FORM == NL_DIV ? 3 : 6;
+    // transform is linear): five transforms for the rotational form, in pairs
+    // where the length has a pair transform
+    if constexpr (col_has_pair<PL>()) {
+        col_inverse_y2<PL>(U0, U1, Z, Z2, p, t);
+        if (FORM == NL_DIV) {
+            col_inverse_y<PL>(U2, Z, Z2, p, t);
+        } else {
+            col_inverse_y2<PL>(U2, W0, Z, Z2, p, t);
+            if (FORM == NL_ROT) col_inverse_y<PL>(W2, Z, Z2, p, t);
+            else col_inverse_y2<PL>(W1, W2, Z, Z2, p, t);
+        }
+    } else {
+        constexpr int NF = FORM == NL_DIV ? 3 : 6;
 #pragma unroll 1
-    for (int i = 0; i < NF; ++i) {
-        if (FORM == NL_ROT && i == 4) continue;
-        zd* x = i < 3 ? sel3(U0, U1, U2, i) : sel3(W0, W1, W2, i - 3);
-        col_inverse_y<PL>(x, Z, Z2, p, t);
+        for (int i = 0; i < NF; ++i) {
+            if (FORM == NL_ROT && i == 4) continue;
+            zd* x = i < 3 ? sel3(U0, U1, U2, i) : sel3(W0, W1, W2, i - 3);
+            col_inverse_y<PL>(x, Z, Z2, p, t);
+        }
     }
     if (FORM == NL_ROT) {
         for (int j = lane; j < nq; j += 32) {

@@ -206,3 +206,22 @@ def test_device_diagnostics_match_oracle(dims, profile):
     for i in (3, 4):  # wall shear of the mean mode
         assert abs(dg[i] - do[i]) <= 1e-12 * max(1.0, abs(do[i]))
     gpu.close()
+
+
+@pytest.mark.parametrize("form", ["rotational", "convective", "divergence"])
+@pytest.mark.parametrize("dims", [(8, 193, 6), (6, 385, 4)])
+def test_long_columns_all_forms(dims, form):
+    # Chebyshev lengths 192 and 384 (compile-time column kernels whose nodal
+    # outputs are transformed two at a time) against the oracle
+    Nx, Ny, Nz = dims
+    g = cfb200.Grid(Nx, Ny, Nz, 5.3, 7.1)
+    gpu = cfb200.CouetteFlow(g, 1 / 300, 0.01, form=form)
+    ref = O.couette(Nx, Ny, Nz, 5.3, 7.1, 1 / 300, 0.01, form=form)
+    U, P = ref.random_state(seed=7, amp=0.2)
+    gpu.set_state(U, P)
+    gpu.advance(0.0, 2)
+    ref.step(U, P, 2)
+    Ug, Pg = gpu.get_state()
+    assert rel(Ug, U) <= 1e-12
+    assert rel(Pg, P) <= 1e-9
+    gpu.close()
