@@ -467,7 +467,11 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     // ---------------- Phase A: nonlinear term, history, right-hand side
     // The three components run through one copy of the loop body (pointers
     // selected, not indexed): the kernel's issue rate is limited by its
-    // instruction footprint, so the body is not unrolled.
+    // instruction footprint, so the body is not unrolled.  The tiles of
+    // component i (N_i, Q_i, U_i) are requested together: U_i goes to a
+    // right-hand-side region not yet written (1, then 2), and for i = 2, whose
+    // right-hand side takes region 2, Q_2 goes there (consumed before the
+    // right-hand side is formed) and U_2 to region 5.
     tile_load_async<NCOL, PL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);  // completed with N_0
     double gold[2] = {p.c1, p.c2};
     zd bulkN0 = zzero(), bulkN2 = zzero(), wR0 = zzero(), wL0 = zzero(), wR2 = zzero(), wL2 = zzero();
@@ -476,7 +480,9 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         const zd* Nn_i = sel3(p.Nn[0], p.Nn[1], p.Nn[2], i);
         zd* Q_i = sel3(p.Q[0], p.Q[1], p.Q[2], i);
         zd* U_i = sel3(p.U[0], p.U[1], p.U[2], i);
-        if (p.stage > 0) tile_load_async<NCOL, PL>(X.reg(5), cs, hs, Q_i, c0, p.Ny, p.B);
+        const int qreg = (i == 2) ? 2 : 5, ureg = (i == 2) ? 5 : i + 1;
+        if (p.stage > 0) tile_load_async<NCOL, PL>(X.reg(qreg), cs, hs, Q_i, c0, p.Ny, p.B);
+        tile_load_async<NCOL, PL>(X.reg(ureg), cs, hs, U_i, c0, p.Ny, p.B);
         if (F32) tile_load<NCOL, PL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
         else tile_load_async<NCOL, PL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
         tile_wait();
@@ -495,17 +501,14 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
             }
             if (p.stage > 0) {
                 zd* A = X.col(4);
-                const zd* Qo = X.col(5);
+                const zd* Qo = X.col(qreg);
                 for (int j = lane; j < nq; j += 32) A[qo + j] = zaxpy(A[qo + j], p.Acoef, Qo[qo + j]);
             }
         }
         __syncthreads();
         if (p.store_q) tile_store<NCOL, PL>(X.reg(4), cs, hs, Q_i, c0, p.Ny, p.B);
-        tile_load_async<NCOL, PL>(X.reg(5), cs, hs, U_i, c0, p.Ny, p.B);
-        tile_wait();
-        __syncthreads();
         if (valid) {
-            zd* U = X.col(5);
+            zd* U = X.col(ureg);
             zd* Qn = X.col(4);
             zd* Z = X.col(6);
             zd* R = X.col(i);
