@@ -564,27 +564,34 @@ static void launch_z(cf_engine* h, int which, bool f32, int nf, const FftParams&
 // fields through the z-inverse and the z-forward, the x-pass kernel and its
 // rows per block.
 struct PeriodicShape {
-    int nzinv, nzfwd, xkind, xrows;
+    int nzinv, nzfwd, xkind, xrows, xthreads;
 };
 static PeriodicShape periodic_shape(const cf_engine* h) {
-    if (h->form == NL_CONV) return {9, 3, KF_XPASS_CONV, 1};
-    if (h->form == NL_DIV) return {3, 6, KF_XPASS_DIV, 2};
-    // one z-row per block from Nxp > 256 (measured: 2.94 against 3.16 ms at
-    // Nxp = 576), two below (0.18 against 0.23 ms at Nxp = 192)
-    if (h->Nxp <= 256) return {6, 3, KF_XPASS2, 2};
     // in-place transforms where the butterflies fit the block (half the shared
     // memory, more blocks per SM)
-    if (h->Nxp == 512 || h->Nxp == 576) return {6, 3, KF_XPASS_IP, 1};
-    return {6, 3, KF_XPASS, 1};
+    const bool ip = h->Nxp == 512 || h->Nxp == 576;
+    if (h->form == NL_CONV) return ip ? PeriodicShape{9, 3, KF_XPASS_CONV_IP, 1, 512} : PeriodicShape{9, 3, KF_XPASS_CONV, 1, 256};
+    if (h->form == NL_DIV) return {3, 6, KF_XPASS_DIV, 2, 256};
+    // one z-row per block from Nxp > 256 (measured: 2.94 against 3.16 ms at
+    // Nxp = 576), two below (0.18 against 0.23 ms at Nxp = 192)
+    if (h->Nxp <= 256) return {6, 3, KF_XPASS2, 2, 256};
+    if (ip) return {6, 3, KF_XPASS_IP, 1, 256};
+    return {6, 3, KF_XPASS, 1, 256};
+}
+// dynamic shared memory of the x-pass kind
+static size_t xpass_smem(const cf_engine* h, int kind) {
+    if (kind == KF_XPASS_IP) return xsmem(h, 3);
+    if (kind == KF_XPASS || kind == KF_XPASS_CONV_IP) return xsmem(h, 6);
+    return xsmem(h, 12);
 }
 static int launch_periodic_kernels(cf_engine* h, cudaEvent_t* ev) {
     FftParams f = fft_params(h);
     const PeriodicShape s = periodic_shape(h);
-    const size_t smx = s.xkind == KF_XPASS_IP ? xsmem(h, 3) : xsmem(h, s.xkind == KF_XPASS ? 6 : 12);
+    const size_t smx = xpass_smem(h, s.xkind);
     launch_z(h, KF_ZINV, false, s.nzinv, f);
     if (ev) CU(cudaEventRecord(ev[0], h->stream));
     const dim3 gx((unsigned)((h->Nzp + s.xrows - 1) / s.xrows), (unsigned)h->Ny);
-    fft_kernel(s.xkind, h->Nxp)<<<gx, 256, smx, h->stream>>>(f);
+    fft_kernel(s.xkind, h->Nxp)<<<gx, s.xthreads, smx, h->stream>>>(f);
     if (ev) CU(cudaEventRecord(ev[1], h->stream));
     launch_z(h, KF_ZFWD, false, s.nzfwd, f);
     CU(cudaGetLastError());
@@ -960,6 +967,7 @@ static int set_attrs(cf_engine* h) {
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_DIV, h->Nxp), need[2]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS2, h->Nxp), need[2]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_IP, h->Nxp), xsmem(h, 3)))) return rc;
+    if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_CONV_IP, h->Nxp), xsmem(h, 6)))) return rc;
     if (h->tma64) {
         if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZINV, h->Nzp, false), zsmem_tma(h, sizeof(zd))))) return rc;
         if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZFWD, h->Nzp, false), zsmem_tma(h, sizeof(zd))))) return rc;

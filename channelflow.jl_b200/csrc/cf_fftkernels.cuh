@@ -281,12 +281,12 @@ CF_DEV void zfwd_body(const FftParams& p, int bx, int n, int f) {
 template <class Z, int POS, int NS, bool FLAT, int KP = 0, class Get>
 CF_DEV void xpack(Z* sm, int bs, int Nxh, int Nxp, int xnyq, const Get& get) {
     if constexpr (FLAT) {
-        const int Nxhp = Nxp / 2 + 1, tot = NS * Nxhp;
-        for (int base = threadIdx.x; base < tot; base += 4 * 256) {
+        const int Nxhp = Nxp / 2 + 1, tot = NS * Nxhp, NT = blockDim.x;
+        for (int base = threadIdx.x; base < tot; base += 4 * NT) {
             Z X[4], Y[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const int e = base + u * 256;
+                const int e = base + u * NT;
                 const int slot = e / Nxhp, k = e - slot * Nxhp;
                 X[u] = czero<Z>();
                 Y[u] = czero<Z>();
@@ -294,7 +294,7 @@ CF_DEV void xpack(Z* sm, int bs, int Nxh, int Nxp, int xnyq, const Get& get) {
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const int e = base + u * 256;
+                const int e = base + u * NT;
                 if (e >= tot) continue;
                 const int slot = e / Nxhp, k = e - slot * Nxhp;
                 Z* o = sm + slot * bs;
@@ -557,6 +557,53 @@ CF_DEV void xpass_conv_body(const FftParams& p, int z, int n) {
     });
 }
 
+// The convective x-pass with the transforms in place (lengths with an
+// in-place plan; 512 threads, one per butterfly of the six slots: 6 x 72 at
+// Nxp = 576): six slots of fft_bufsz(Nxp), so two blocks of 16 warps fit per
+// SM instead of two of 8.  Same packing, product and truncation as
+// xpass_conv_body; the product at j rewrites slots 0-1 at j in place.
+template <int LX>
+CF_DEV void xpass_conv_ip_body(const FftParams& p, int z, int n) {
+    static_assert(6 * fft_ip_butterflies<LX>() <= 512, "one butterfly per thread");
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    zd* sm = reinterpret_cast<zd*>(fsm_raw);
+    const int Nxh = p.Nxh, bs = p.bsxp;
+    const long row = ((long)n * p.Nzp + z) * Nxh;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
+    auto fetch = [&](int code, int k) -> zd {
+        if (code < 3) return zp_of<zd>(p, code)[row + k];
+        if (code < 6) return cmuli(zp_of<zd>(p, code - 3)[row + k], p.ax * k);
+        return zp_of<zd>(p, code - 3)[row + k];
+    };
+    xpack<zd, 0, 6, true>(sm, bs, Nxh, LX, xnyq, [&](int slot, int k, zd& X, zd& Y) {
+        X = fetch(2 * slot, k);
+        Y = fetch(2 * slot + 1, k);
+    });
+    __syncthreads();
+    group_fft_ip<true, LX, 0>(sm, 6, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
+    for (int j = threadIdx.x; j < LX; j += blockDim.x) {
+        const int sj = fpos(j);
+        const zd s0 = sm[sj], s1 = sm[bs + sj], s2 = sm[2 * bs + sj];
+        const zd s3 = sm[3 * bs + sj], s4 = sm[4 * bs + sj], s5 = sm[5 * bs + sj];
+        const double u0 = s0.x, u1 = s0.y, u2 = s1.x;
+        const double gx0 = s1.y, gx1 = s2.x, gx2 = s2.y;
+        const double gy0 = s3.x, gy1 = s3.y, gy2 = s4.x;
+        const double gz0 = s4.y, gz1 = s5.x, gz2 = s5.y;
+        sm[sj] = zmake(-(u0 * gx0 + u1 * gy0 + u2 * gz0), -(u0 * gx1 + u1 * gy1 + u2 * gz1));
+        sm[bs + sj] = zmake(-(u0 * gx2 + u1 * gy2 + u2 * gz2), 0.0);
+    }
+    __syncthreads();
+    group_fft_ip<true, LX, 0>(sm, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
+    xunpack<zd, 0, 2, true>(sm, bs, Nxh, LX, [&](int slot, int k, zd X, zd Y) {
+        if (slot == 0) {
+            zp_of<zd>(p, 0)[row + k] = X;
+            zp_of<zd>(p, 1)[row + k] = Y;
+        } else {
+            zp_of<zd>(p, 2)[row + k] = X;
+        }
+    });
+}
+
 // Divergence form (nonlinear.jl:146-167, outer! operators.jl:227-234).  grid:
 // (ceil(Nzp/2), Ny); block 256; smem 12*bsx complex.  Rows zA = 2*bx, zB =
 // 2*bx+1 of plane n; slot f holds (u_f row A) + i (u_f row B).  The six
@@ -640,6 +687,12 @@ __global__ void __launch_bounds__(256, CF_XPASS_IP_BLOCKS) k_xpass_ip(FftParams 
 template <int LX>
 __global__ void __launch_bounds__(256) k_xpass2(FftParams p) {
     xpass_body<LX, zd>(p, blockIdx.x, blockIdx.y);
+}
+// in-place convective x-pass, 512 threads (lengths with an in-place plan;
+// other lengths compile an empty kernel that the engine never selects)
+template <int LX>
+__global__ void __launch_bounds__(512, 2) k_xpass_conv_ip(FftParams p) {
+    if constexpr (fft_ip_butterflies<LX>() > 0) xpass_conv_ip_body<LX>(p, blockIdx.x, blockIdx.y);
 }
 template <int LX>
 __global__ void __launch_bounds__(256) k_xpass_conv(FftParams p) {

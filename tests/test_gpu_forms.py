@@ -50,8 +50,9 @@ def test_analytic_nonlinear_forms(form):
 
 
 @pytest.mark.parametrize("form", FORMS)
-@pytest.mark.parametrize("dims", [(16, 17, 16), (9, 17, 7), (6, 13, 10), (48, 33, 40), (8, 81, 1)])
+@pytest.mark.parametrize("dims", [(16, 17, 16), (9, 17, 7), (6, 13, 10), (48, 33, 40), (8, 81, 1), (384, 17, 4)])
 def test_nonlinear_term_forms(form, dims):
+    # (384, 17, 4): padded x length 576, the x-pass with in-place transforms
     Nx, Ny, Nz = dims
     gpu, ref = pair(Nx, Ny, Nz, 5.3, 7.1, 0.01, 0.01, form)
     U = ref.synth(seed=3, amp=0.2)
