@@ -27,7 +27,7 @@ enum {
     KC_STAGE_CONV, KC_PREP_CONV, KC_STAGE_DIV, KC_PREP_DIV, KC_DIV, KC_PRESSURE_COEF,
     KC_STAGE_MXD, KC_PREP_MXD, KC_COUNT
 };
-enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_XPASS_CONV, KF_XPASS_DIV, KF_XPASS2, KF_XPASS_IP, KF_XPASS_CONV_IP, KF_COUNT };
+enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_XPASS_CONV, KF_XPASS_DIV, KF_XPASS2, KF_XPASS_IP, KF_XPASS_CONV_IP, KF_XPASS_DIV_IP, KF_COUNT };
 
 // defined for P in CF_COL_LENGTHS and 0 (cf_inst_col.cu)
 template <int P>

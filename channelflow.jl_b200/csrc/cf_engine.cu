@@ -571,7 +571,7 @@ static PeriodicShape periodic_shape(const cf_engine* h) {
     // memory, more blocks per SM)
     const bool ip = h->Nxp == 512 || h->Nxp == 576;
     if (h->form == NL_CONV) return ip ? PeriodicShape{9, 3, KF_XPASS_CONV_IP, 1, 512} : PeriodicShape{9, 3, KF_XPASS_CONV, 1, 256};
-    if (h->form == NL_DIV) return {3, 6, KF_XPASS_DIV, 2, 256};
+    if (h->form == NL_DIV) return ip ? PeriodicShape{3, 6, KF_XPASS_DIV_IP, 2, 512} : PeriodicShape{3, 6, KF_XPASS_DIV, 2, 256};
     // one z-row per block from Nxp > 256 (measured: 2.94 against 3.16 ms at
     // Nxp = 576), two below (0.18 against 0.23 ms at Nxp = 192)
     if (h->Nxp <= 256) return {6, 3, KF_XPASS2, 2, 256};
@@ -581,7 +581,7 @@ static PeriodicShape periodic_shape(const cf_engine* h) {
 // dynamic shared memory of the x-pass kind
 static size_t xpass_smem(const cf_engine* h, int kind) {
     if (kind == KF_XPASS_IP) return xsmem(h, 3);
-    if (kind == KF_XPASS || kind == KF_XPASS_CONV_IP) return xsmem(h, 6);
+    if (kind == KF_XPASS || kind == KF_XPASS_CONV_IP || kind == KF_XPASS_DIV_IP) return xsmem(h, 6);
     return xsmem(h, 12);
 }
 static int launch_periodic_kernels(cf_engine* h, cudaEvent_t* ev) {
@@ -968,6 +968,7 @@ static int set_attrs(cf_engine* h) {
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS2, h->Nxp), need[2]))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_IP, h->Nxp), xsmem(h, 3)))) return rc;
     if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_CONV_IP, h->Nxp), xsmem(h, 6)))) return rc;
+    if ((rc = raise_smem_limit(fft_kernel(KF_XPASS_DIV_IP, h->Nxp), xsmem(h, 6)))) return rc;
     if (h->tma64) {
         if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZINV, h->Nzp, false), zsmem_tma(h, sizeof(zd))))) return rc;
         if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZFWD, h->Nzp, false), zsmem_tma(h, sizeof(zd))))) return rc;

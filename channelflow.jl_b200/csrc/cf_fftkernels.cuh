@@ -648,6 +648,48 @@ CF_DEV void xpass_div_body(const FftParams& p, int bx, int n) {
     });
 }
 
+// The divergence x-pass with the transforms in place (lengths with an in-place
+// plan; 512 threads, one per butterfly of the six product slots): six slots
+// of fft_bufsz(Nxp).  The three forward transforms run in slots 0-2; the
+// product at j reads slots 0-2 at j and writes slots 0-5 at j (one thread per
+// j, no barrier of its own).
+template <int LX>
+CF_DEV void xpass_div_ip_body(const FftParams& p, int bx, int n) {
+    static_assert(6 * fft_ip_butterflies<LX>() <= 512, "one butterfly per thread");
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    zd* sm = reinterpret_cast<zd*>(fsm_raw);
+    const int zA = 2 * bx, zB = zA + 1;
+    const bool hasB = zB < p.Nzp;
+    const int Nxh = p.Nxh, bs = p.bsxp;
+    const long rowA = ((long)n * p.Nzp + zA) * Nxh;
+    const long rowB = ((long)n * p.Nzp + zB) * Nxh;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
+    xpack<zd, 0, 3, true>(sm, bs, Nxh, LX, xnyq, [&](int slot, int k, zd& X, zd& Y) {
+        const zd* src = zp_of<zd>(p, slot);
+        X = src[rowA + k];
+        if (hasB) Y = src[rowB + k];
+    });
+    __syncthreads();
+    group_fft_ip<true, LX, 0>(sm, 3, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
+    for (int j = threadIdx.x; j < LX; j += blockDim.x) {
+        const int sj = fpos(j);
+        const zd a0 = sm[sj], a1 = sm[bs + sj], a2 = sm[2 * bs + sj];
+        sm[sj] = zmake(-(a0.x * a0.x), -(a0.y * a0.y));
+        sm[bs + sj] = zmake(-(a0.x * a1.x), -(a0.y * a1.y));
+        sm[2 * bs + sj] = zmake(-(a0.x * a2.x), -(a0.y * a2.y));
+        sm[3 * bs + sj] = zmake(-(a1.x * a1.x), -(a1.y * a1.y));
+        sm[4 * bs + sj] = zmake(-(a1.x * a2.x), -(a1.y * a2.y));
+        sm[5 * bs + sj] = zmake(-(a2.x * a2.x), -(a2.y * a2.y));
+    }
+    __syncthreads();
+    group_fft_ip<true, LX, 0>(sm, 6, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
+    xunpack<zd, 0, 6, true>(sm, bs, Nxh, LX, [&](int slot, int k, zd X, zd Y) {
+        zd* dst = zp_of<zd>(p, slot);
+        dst[rowA + k] = X;
+        if (hasB) dst[rowB + k] = Y;
+    });
+}
+
 // Single-instance kernels and their batched forms (one launch per size class;
 // blockIdx.z also selects the instance).
 template <int LZ, class Z = zd>
@@ -697,6 +739,11 @@ __global__ void __launch_bounds__(512, 2) k_xpass_conv_ip(FftParams p) {
 template <int LX>
 __global__ void __launch_bounds__(256) k_xpass_conv(FftParams p) {
     xpass_conv_body<LX, zd>(p, blockIdx.x, blockIdx.y);
+}
+// in-place divergence x-pass, 512 threads (lengths with an in-place plan)
+template <int LX>
+__global__ void __launch_bounds__(512, 2) k_xpass_div_ip(FftParams p) {
+    if constexpr (fft_ip_butterflies<LX>() > 0) xpass_div_ip_body<LX>(p, blockIdx.x, blockIdx.y);
 }
 template <int LX>
 __global__ void __launch_bounds__(256) k_xpass_div(FftParams p) {
