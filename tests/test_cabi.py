@@ -52,3 +52,14 @@ def test_form_validation_before_device_work():
     cfg.form = 7
     h = ctypes.c_void_p()
     assert cfb200.lib().cf_create(ctypes.byref(cfg), ctypes.byref(h)) == -1
+
+
+def test_step_entry_points_reject_null_handles():
+    # every step entry point checks its handle and arguments before any CUDA call
+    L = cfb200.lib()
+    t = ctypes.c_double()
+    buf = (ctypes.c_double * 4)()
+    assert L.cf_step(None, 0.0, 1, ctypes.byref(t), None) == -1
+    assert L.cf_step_dt(None, 0.0, 0.01, ctypes.byref(t), None) == -1
+    assert L.cf_step_host(None, buf, buf, 0.0, 1, ctypes.byref(t), None) == -1
+    assert "null" in L.cf_last_error().decode()
