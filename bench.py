@@ -198,6 +198,50 @@ def cpu_baseline(cfg, threads, div):
     return dt * div
 
 
+# ---- replicas: one process per GPU, no data-path collective; the ranks only
+# meet at the barriers around the timed region and in the max of their times
+def init_ranks(backend="nccl", timeout_s=120):
+    """(rank, world, local rank, torch.distributed or None) from the torchrun
+    environment; with more than one rank, a process group of `backend` whose
+    collectives end with an error after `timeout_s` seconds."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world == 1:
+        return rank, world, local, None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+    return rank, world, local, dist
+
+
+def rank_ops(dist, device="cuda"):
+    """barrier() and max_over_ranks(x) of the run (no-ops with one rank); the
+    maximum is reduced in a float64 tensor on `device`."""
+    import torch
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return barrier, max_over_ranks
+
+
+def finish_ranks(dist):
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_reference(args, cfg, rank):
     """--impl reference: the oracle port (the reference's algorithm restated on
     the CPU) on this host's cores; each step is a bounded sample of one CNRK2
@@ -292,19 +336,12 @@ def run_ensemble(args, cfg, rank, world, local, torch, dist):
         cfb200.lib().cf_random_state(inst.handle, seed, amp, cfg["shape"], cfg["rho"])
     n = len(members)
     stream = torch.cuda.ExternalStream(ens.stream_ptr())
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = rank_ops(dist, "cuda")
 
     ens.step(args.warmup)
     torch.cuda.synchronize()
     sampler = ClockSampler(local)
-    if dist is not None:
-        dist.barrier()
+    barrier()
     torch.cuda.synchronize()
     sampler.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -518,29 +555,18 @@ def main():
     cfg["form"] = args.form
     if args.form != "rotational":
         args.no_mixed = True
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-
     if args.impl == "reference":
-        run_reference(args, cfg, rank)
+        # rank 0 alone times the CPU reference; other ranks exit without work
+        run_reference(args, cfg, int(os.environ.get("RANK", "0")))
         return
 
     import torch
 
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rank, world, local, dist = init_ranks("nccl")
     if "ensemble" in cfg:
         run_ensemble(args, cfg, rank, world, local, torch, dist)
-        if dist is not None:
-            dist.barrier()
-            dist.destroy_process_group()
+        finish_ranks(dist)
         return
     import cfb200
 
@@ -552,17 +578,7 @@ def main():
     cfb200.lib().cf_random_state(pb.handle, 1000 + rank, cfg["amp"], cfg["shape"], cfg["rho"])
     U0, P0 = pb.get_state()
     stream = torch.cuda.ExternalStream(pb.stream_ptr())
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = rank_ops(dist, "cuda")
 
     # warm-up (CUDA-graph step)
     t = 0.0
@@ -661,9 +677,7 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
     pb.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    finish_ranks(dist)
 
 
 if __name__ == "__main__":
