@@ -63,3 +63,27 @@ def test_step_entry_points_reject_null_handles():
     assert L.cf_step_dt(None, 0.0, 0.01, ctypes.byref(t), None) == -1
     assert L.cf_step_host(None, buf, buf, 0.0, 1, ctypes.byref(t), None) == -1
     assert "null" in L.cf_last_error().decode()
+
+
+@pytest.mark.parametrize("dims, field, value, code, words", [
+    ((8, 17, 8), "nu", float("inf"), -1, "nu must be finite"),
+    ((8, 17, 8), "dt", -0.01, -1, "dt must be finite"),
+    ((8, 17, 8), "precision", 7, -1, "unknown precision"),
+    ((8, 577, 6), "precision", 2, -5, "Ny <= 512"),
+    ((74, 17, 8), None, None, -5, "padded x length"),
+    ((8, 17, 74), None, None, -5, "padded z length"),
+    ((8, 1025, 6), None, None, -5, "Ny too large"),
+])
+def test_sizes_and_modes_rejected_before_device_work(dims, field, value, code, words):
+    # cf_create checks the configuration before it creates a stream or
+    # allocates (no GPU needed): 3/2-padded lengths with a prime factor above
+    # 31 (74 -> 111 = 3 x 37), a column too long for the shared memory of the
+    # column kernel, the tensor-core transforms beyond Ny = 512
+    g = cfb200.Grid(*dims, 6.28, 6.28)
+    cfg, _, _ = cfb200._make_config(g, "couette", 0.01, 0.01)
+    if field:
+        setattr(cfg, field, value)
+    h = ctypes.c_void_p()
+    assert cfb200.lib().cf_create(ctypes.byref(cfg), ctypes.byref(h)) == code
+    assert words in cfb200.lib().cf_last_error().decode()
+    assert not h.value
