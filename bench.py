@@ -11,14 +11,17 @@ larger than the 126 MB L2, so no flush is needed between steps.
 
 The JSON line carries: value (steps/s, device-resident state, CUDA-graph step,
 timed with CUDA events on the engine stream, max over ranks), e2e (the same
-metric through the host-buffer C-ABI path: state upload, step, state download
-per step from pinned memory), roofline of the dominant kernel (algorithmic
+metric through the host-buffer C-ABI path, cf_step_host: state upload, step,
+state download per step from and into pinned memory, the transfers overlapped
+with the first and last column kernels), roofline of the dominant kernel (algorithmic
 bytes from the fixed byte model / event-timed kernel time), the CPU baseline
 (the oracle port on this host's cores, a bounded sample of one CNRK2 stage),
 clocks sampled during the timed region, and the kernel-launch count.
 
 N > 1 (torchrun): independent replicas, one per GPU, no data-path collective
-(a single channel does not shard; the ensemble of replicas does).
+(a single channel does not shard; the ensemble of replicas does); the ranks
+meet only at the barriers around the timed region and in the maximum of their
+times.  --impl reference runs on rank 0 alone.
 """
 import argparse
 import json
