@@ -50,7 +50,10 @@ EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_g
            "cf_stream", "cf_last_error", "cf_step_profiled", "cf_nonlinear_noalloc", "cf_create_batch",
            "cf_destroy_batch", "cf_batch_size", "cf_batch_instance", "cf_step_batch",
            "cf_batch_last_launch_count", "cf_batch_stream", "cf_cheb_transform", "cf_step_dt",
-           "cf_step_host"]
+           "cf_step_host", "cf_power_input", "cf_device_bytes", "cf_set_wait_limit"]
+
+# return codes of cfb200.h
+CF_E_ARG, CF_E_SINGULAR, CF_E_NOMEM, CF_E_CUDA, CF_E_UNSUPPORTED, CF_E_NONFINITE = -1, -2, -3, -4, -5, -6
 
 
 def lib():
@@ -97,6 +100,10 @@ def lib():
         L.cf_last_launch_count.argtypes = [ctypes.c_void_p]
         L.cf_stream.argtypes = [ctypes.c_void_p]
         L.cf_stream.restype = ctypes.c_void_p
+        L.cf_power_input.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double, _D]
+        L.cf_device_bytes.argtypes = [ctypes.c_void_p]
+        L.cf_device_bytes.restype = ctypes.c_longlong
+        L.cf_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_long]
         _lib = L
     return _lib
 
@@ -156,7 +163,7 @@ class State:
 
 
 def zero_state(grid):
-    """zero_state(grid) (src/initialization.jl:160)."""
+    """zero_state(grid) (src/initialization.jl:16)."""
     return State(np.zeros((3,) + grid.spectralsize, np.complex128), np.zeros(grid.spectralsize, np.complex128))
 
 
@@ -321,6 +328,23 @@ class ChannelFlowProblem:
         _check(lib().cf_diagnostics(self._h, _ptr(out)))
         return out
 
+    def power_input(self, pressuregradient=(0.0, 0.0), with_base=False):
+        """power_input(U, nu; pressuregradient) (src/postprocessing.jl:113-128) of
+        the engine's velocity; with_base adds the base profile first (total flow)."""
+        out = np.zeros(1)
+        _check(lib().cf_power_input(self._h, 1 if with_base else 0, float(pressuregradient[0]),
+                                    float(pressuregradient[1]), _ptr(out)))
+        return float(out[0])
+
+    def device_bytes(self):
+        """Device memory held by the handle (bytes)."""
+        return int(lib().cf_device_bytes(self._h))
+
+    def set_wait_limit(self, spins):
+        """Test hook: polls after which a kernel's first bounded wait gives up
+        (negative restores the default)."""
+        _check(lib().cf_set_wait_limit(self._h, int(spins)))
+
 
 class Ensemble:
     """Many independent channels advanced together (cf_create_batch): each
@@ -417,7 +441,7 @@ def pressure(U, problem):
 
 
 def random_state(problem, epsilon, seed=1, shape=0, rho=0.8):
-    """random_state(problem, epsilon) (src/initialization.jl:176-195) with a seeded
+    """random_state(problem, epsilon) (src/initialization.jl:32-51) with a seeded
     spectral generator: returns a host State and leaves it resident in the engine."""
     if epsilon < 0:
         raise ValueError("epsilon must be non-negative")
@@ -427,7 +451,7 @@ def random_state(problem, epsilon, seed=1, shape=0, rho=0.8):
 
 
 def step_(problem, U, P, t, nsteps=1):
-    """step!(scheme, nlterm, U, P, t; constraint...) (src/timesteppers/cnrk2.jl:567-625).
+    """step!(scheme, nlterm, U, P, t; constraint...) (src/timesteppers/cnrk2.jl:149-207).
 
     Host buffers U, P are advanced in place (upload, nsteps device steps,
     download) and t + nsteps*dt is returned.  Contiguous complex128 buffers go

@@ -6,9 +6,9 @@
 // for the fields f of one launch; X and Y are FP32 arrays (Ny rows of C
 // floats: a complex (Ny, Nz, Nxh) field read as C = 2 Nxh Nz real columns, T
 // being real).  T is the DCT-I of the forward transform (nodal values ->
-// coefficients, with the reference's normalisation, ffts.jl:189-206 and
-// :378-393) or of the inverse one (coefficients -> nodal values, ffts.jl:
-// 282-287), built by the engine.
+// coefficients, with the reference's normalisation, ffts.jl:65-82 and
+// :254-269) or of the inverse one (coefficients -> nodal values,
+// chebyshev.jl:58-66 and ffts.jl:162), built by the engine.
 //
 // The contraction is computed transposed, D = X^T T^T: M = 128 columns of X per
 // block (TMEM lane m = column), N = the output degrees (MMAs of at most 256),
@@ -45,6 +45,7 @@ struct ChebParams {
     const float* Bhi;  // [nkt][4 chunks][NP rows][4 floats] K-tile images of T^T (TF32 heads)
     const float* Blo;  // remainders
     int* err;          // set to 1 when a wait gives up
+    long spins;        // polls of a wait for a free stage (CF_WAIT_SPINS; shortened only by tests)
 };
 
 // ---- PTX wrappers --------------------------------------------------------------
@@ -173,7 +174,7 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
         }
         // the stage is free once the MMAs of K-tile kt - nst (its last user) are done
         if (kt >= nst) {
-            ok = mbar_wait(smem_u32(mbar + st), (uint32_t)(((kt - nst) / nst) & 1));
+            ok = mbar_wait(smem_u32(mbar + st), (uint32_t)(((kt - nst) / nst) & 1), p.spins);
             tc_fence_after();
         }
         // A: column cm, rows k0 + 4j .. 4j+3 form one 16-byte core-matrix row

@@ -17,7 +17,7 @@
 //    eliminated from the top degree downwards (a_n = alpha_n a_{n-2} + beta_n);
 //    the two linear sweeps are prefix scans of affine maps and the wall row is
 //    reduced with precomputed weights W_n (factors from the engine set-up).
-//  * DCT-I (FFTW REDFT00, src/transforms/chebyshev.jl:481-502) of a complex
+//  * DCT-I (FFTW REDFT00, src/transforms/chebyshev.jl:45-66) of a complex
 //    column of length P+1 through one complex FFT of length P.
 //
 // Chains of one parity are scanned in runs: each lane takes E consecutive
@@ -261,10 +261,10 @@ CF_DEV void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, 
 //   X_{2m+1} = X_{2m-1} + i (Z_m - Z_{P-m}).
 // cs[n] = (cos(pi n/P), sin(pi n/P)), n = 0..P.  P must be even.  After the
 // FFT, warp 0 writes the even outputs and warp 1 scans the odd ones.
-// MODE 1 (forward transform of nodal values, ffts.jl:189-206 with
-// normalize_forward! :378-393): every output times `scale`, X_0 and X_P also
+// MODE 1 (forward transform of nodal values, ffts.jl:65-82 with
+// normalize_forward! :254-269): every output times `scale`, X_0 and X_P also
 // halved.  MODE 2 (inverse, icheb with doubled endpoints and the 1/2 of
-// copy_to_padded!, ffts.jl:282-287): 0.5 * DCT of x with x_0, x_P doubled.
+// copy_to_padded!, chebyshev.jl:58-66, ffts.jl:162): 0.5 * DCT of x with x_0, x_P doubled.
 // Both are folded into the z staging (the transform is linear).
 #define CF_DCT_FWD 1
 #define CF_DCT_INV 2
@@ -495,7 +495,7 @@ CF_DEV void col_redft00_pair(zd* xa, zd* xb, zd* z, int bs, const zd* __restrict
     tsync(t);
 }
 
-// Mean over y (meanmode.jl:173-179): a0 + sum_{even n >= 2} a_n / (1 - n^2),
+// Mean over y (meanmode.jl:13-19): a0 + sum_{even n >= 2} a_n / (1 - n^2),
 // returned to both warps.
 CF_DEV zd col_bulkmean(const zd* a, const Team& t) {
     zd s = zzero();

@@ -88,9 +88,13 @@ CF_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_sha
 CF_DEV void mbar_init(uint32_t mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
 }
-// bounded wait for the completion of phase `parity`; false when it gave up
-CF_DEV bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (long it = 0; it < (1L << 22); ++it) {
+// Bounded wait for the completion of phase `parity`; false when it gave up
+// after `limit` polls.  A kernel whose wait gave up still waits (with the
+// default limit) for its own copies or MMAs in flight before it leaves, so no
+// asynchronous write lands in shared memory that a later block owns.
+#define CF_WAIT_SPINS (1L << 22)
+CF_DEV bool mbar_wait(uint32_t mbar, uint32_t parity, long limit = CF_WAIT_SPINS) {
+    for (long it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

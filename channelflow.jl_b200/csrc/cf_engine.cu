@@ -220,7 +220,14 @@ struct cf_engine {
     FftMaps maps64, maps32;
     bool tma64 = false, tma32 = false;
     int zbox = 0, zpbox = 0;  // rows per TMA box (nodal, z-padded)
+    // status words written by the kernels, read and cleared by check_status:
+    // [0] a TMA wait of a z kernel gave up, [1] a tensor-core wait gave up,
+    // [2] the mean mode went non-finite (d_ffterr, d_cheberr point into it)
+    int* d_status = nullptr;
     int* d_ffterr = nullptr;
+    int device = 0;                  // the CUDA device the handle was created on
+    long wait_spins = CF_WAIT_SPINS;  // polls of a kernel's first bounded wait (cf_set_wait_limit)
+    size_t dev_bytes = 0;            // device memory the handle holds (cf_device_bytes)
     // device
     cudaStream_t stream = nullptr;
     int form = NL_ROT;  // nonlinear form (CF_FORM_*)
@@ -266,8 +273,23 @@ static int dalloc(cf_engine* h, void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) return fail(CF_E_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
     h->allocs.push_back(*p);
+    h->dev_bytes += bytes;
     return CF_OK;
 }
+
+// The handle's device is current for the duration of an entry point; the
+// caller's current device is restored on return.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
 
 static std::vector<int> fft_radices(int n) {
     std::vector<int> r;
@@ -355,7 +377,7 @@ static int make_plan(cf_engine* h, int L, FftPlan& pl, zd** dtw, zf** dtwf = nul
 static double kx_of(const cf_engine* h, int ix) { return 2 * M_PI / h->Lx * ix; }
 static double lz_of(const cf_engine* h, int iz) { return 2 * M_PI / h->Lz * (iz <= (h->Nz >> 1) ? iz : iz - h->Nz); }
 
-// Stokes bank for (nu, lambda): batchedinfluence.jl:45-98, meanmode.jl:205-227
+// Stokes bank for (nu, lambda): batchedinfluence.jl:45-98, meanmode.jl:45-67
 static int build_bank(cf_engine* h, DevBank& bk, double nu, double lambda) {
     const int P = h->P, Ny = h->Ny;
     const long B = h->B;
@@ -528,6 +550,7 @@ static ColParams col_params(const cf_engine* h) {
     p.cs_tab = h->d_cs;
     p.helm_tab = h->d_helmtab;
     p.fnorm = 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1));
+    p.flags = h->d_status + 2;
     return p;
 }
 
@@ -546,6 +569,7 @@ static FftParams fft_params(const cf_engine* h) {
     f.zbox = h->zbox; f.zpbox = h->zpbox;
     f.stoff = (int)zstage_off(h, sizeof(zd));
     f.err = h->d_ffterr;
+    f.spins = h->wait_spins;
     return f;
 }
 
@@ -629,7 +653,7 @@ static int launch_prep(cf_engine* h, zd* const Usrc[3], int* count) {
     return CF_OK;
 }
 
-// column-kernel parameters of CNRK2 stage j (cnrk2.jl:588-623)
+// column-kernel parameters of CNRK2 stage j (cnrk2.jl:170-205)
 static ColParams stage_col_params(const cf_engine* h, int j) {
     ColParams p = col_params(h);
     p.lambda = 1.0 / (CC[j] * h->dt);
@@ -754,6 +778,7 @@ static int launch_cheb(cf_engine* h, int nf, bool inverse, int* count) {
     p.Bhi = img;
     p.Blo = img + (size_t)h->chebKT * h->chebNP * CF_CHEB_KT;
     p.err = h->d_cheberr;
+    p.spins = h->wait_spins;
     dim3 grid((unsigned)((p.C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nf, (unsigned)nsplit);
     k_cheb_mma<<<grid, 128, cheb_smem(NPs), h->stream>>>(p);
     if (count) *count += 1;
@@ -797,19 +822,25 @@ static int launch_prep_mx(cf_engine* h, int* count) {
     CU(cudaGetLastError());
     return launch_cheb(h, 6, true, count);
 }
-static int check_cheb_err(cf_engine* h) {
-    int herr = 0;
-    if (h->tc) {
-        CU(cudaMemcpyAsync(&herr, h->d_cheberr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-        CU(cudaStreamSynchronize(h->stream));
-        if (herr) return fail(CF_E_CUDA, "Chebyshev transform kernel: a tensor-core wait timed out");
-    }
-    if (h->tma64 || h->tma32) {
-        CU(cudaMemcpyAsync(&herr, h->d_ffterr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-        CU(cudaStreamSynchronize(h->stream));
-        if (herr) return fail(CF_E_CUDA, "z transform kernel: a TMA wait timed out");
-    }
-    return CF_OK;
+// Wait for the handle's stream and report what its kernels flagged since the
+// last check (each flag is reported once, then cleared): a bounded wait that
+// gave up (CF_E_CUDA; the output of that launch is not valid) or a non-finite
+// mean mode (CF_E_NONFINITE: a NaN or Inf anywhere in the state reaches the
+// (0,0) mode through the nonlinear term within one stage).
+// The calls that do not step (nonlinear term, projection, pressure,
+// diagnostics) report the wait flags only and leave a non-finite flag of an
+// earlier step for the next step-synchronising call (with_state false).
+static int check_status(cf_engine* h, bool with_state = true) {
+    int st[4];
+    CU(cudaMemcpyAsync(st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    const int n = with_state ? 3 : 2;
+    if (!(st[0] | st[1] | (with_state ? st[2] : 0))) return CF_OK;
+    CU(cudaMemsetAsync(h->d_status, 0, n * sizeof(int), h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if (st[0]) return fail(CF_E_CUDA, "z transform kernel: a TMA wait timed out");
+    if (st[1]) return fail(CF_E_CUDA, "Chebyshev transform kernel: a tensor-core wait timed out");
+    return fail(CF_E_NONFINITE, "the state became non-finite (NaN or Inf in the mean mode)");
 }
 // mixed step with per-kernel event timing: kernel_ms = [z-inverse, x-pass,
 // z-forward, column, forward Chebyshev, inverse Chebyshev] summed over steps
@@ -858,7 +889,7 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
         }
     for (int k = 0; k < 7; ++k) cudaEventDestroy(ev[k]);
     if (rc) return rc;
-    if ((rc = check_cheb_err(h))) return rc;
+    if ((rc = check_status(h))) return rc;
     h->last_launches = cnt + (h->tc ? 18 : 12) * nsteps;
     if (t_out) *t_out = t + nsteps * h->dt;
     return CF_OK;
@@ -1110,12 +1141,39 @@ static int host_stage_kind(const cf_engine* h, int j, ColParams& p) {
 
 static void host_synth(const cf_engine* h, uint64_t seed, double amp, int shape, double rho, std::vector<std::complex<double>>& U);
 
+// Fixed scratch of cf_nonlinear_noalloc: one array per device (module
+// scope, resident from module load until exit).  Host code names
+// g_noalloc_scratch only through the device address that cudaGetSymbolAddress
+// returns for the current device; cf_create looks it up with the handle's
+// device current (every create refreshes it, so a context recreated after a
+// device reset gets its own address; handles of the old context are invalid
+// after such a reset anyway).
+#define CF_MAX_DEVICES 64
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CF_NOALLOC_SCRATCH_BYTES];
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[CF_MAX_DEVICES] = {};
+
+static int noalloc_setup(int dev) {
+    if (dev < 0 || dev >= CF_MAX_DEVICES) return fail(CF_E_UNSUPPORTED, "device ordinal out of range");
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return fail(CF_E_CUDA, std::string("scratch address: ") + cudaGetErrorString(e));
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    g_noalloc_addr[dev] = p;
+    return CF_OK;
+}
+static void* noalloc_scratch(int dev) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    return (dev >= 0 && dev < CF_MAX_DEVICES) ? g_noalloc_addr[dev] : nullptr;
+}
+
 extern "C" {
 
 const char* cf_last_error(void) { return g_err.c_str(); }
 
 void cf_destroy(cf_handle* h) {
     if (!h) return;
+    DeviceGuard dg_(h->device);
     drop_graph(h);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->cstream) cudaStreamSynchronize(h->cstream);
@@ -1133,7 +1191,7 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
     cf_engine* h = new cf_engine();
     int rc = validate_and_size(h, cfg);
     if (rc) { delete h; return rc; }
-    // base profile (problem.jl:92, cnrk2.jl:494-495)
+    // base profile at the nodes (problem.jl:92) and its coefficients (cnrk2.jl:58-82)
     std::vector<double> vals(h->Ny);
     for (int j = 0; j < h->Ny; ++j) {
         double y = (2 * j == h->P) ? 0.0 : std::cos(M_PI * j / h->P);
@@ -1150,8 +1208,14 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
     h->basemean = setup::bulkmean(h->base.data(), h->P);
 
     auto bail = [&](int code) { cf_destroy(h); return code; };
+    if (cudaGetDevice(&h->device) != cudaSuccess) { delete h; return fail(CF_E_CUDA, "no CUDA device"); }
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(CF_E_CUDA, "cannot create stream (no CUDA device?)"));
+    if ((rc = noalloc_setup(h->device))) return bail(rc);
+    if ((rc = dalloc(h, (void**)&h->d_status, 4 * sizeof(int)))) return bail(rc);
+    if (cudaMemset(h->d_status, 0, 4 * sizeof(int)) != cudaSuccess) return bail(fail(CF_E_CUDA, "upload failed"));
+    h->d_ffterr = h->d_status;
+    h->d_cheberr = h->d_status + 1;
     const size_t fr = sizeof(zd) * h->nr, fq = sizeof(zd) * h->nq;
     for (int i = 0; i < 3; ++i) {
         if ((rc = dalloc(h, (void**)&h->U[i], fr))) return bail(rc);
@@ -1190,12 +1254,10 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
         const size_t nb = sizeof(float) * fhi.size();
         if ((rc = dalloc(h, (void**)&h->d_chebF, 2 * nb))) return bail(rc);
         if ((rc = dalloc(h, (void**)&h->d_chebI, 2 * nb))) return bail(rc);
-        if ((rc = dalloc(h, (void**)&h->d_cheberr, sizeof(int)))) return bail(rc);
         if (cudaMemcpy(h->d_chebF, fhi.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->d_chebF + fhi.size(), flo.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemcpy(h->d_chebI, ihi.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->d_chebI + ihi.size(), ilo.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemset(h->d_cheberr, 0, sizeof(int)) != cudaSuccess)
+            cudaMemcpy(h->d_chebI + ihi.size(), ilo.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess)
             return bail(fail(CF_E_CUDA, "upload failed"));
     }
     {
@@ -1218,8 +1280,6 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
         if ((rc = dalloc(h, (void**)&h->d_helmtab, sizeof(double) * gt.size()))) return bail(rc);
         cudaMemcpy(h->d_helmtab, gt.data(), sizeof(double) * gt.size(), cudaMemcpyHostToDevice);
     }
-    if ((rc = dalloc(h, (void**)&h->d_ffterr, sizeof(int)))) return bail(rc);
-    if (cudaMemset(h->d_ffterr, 0, sizeof(int)) != cudaSuccess) return bail(fail(CF_E_CUDA, "upload failed"));
     encode_maps(h);
     if ((rc = set_attrs(h))) return bail(rc);
     if ((rc = ensure_banks(h))) return bail(rc);
@@ -1239,6 +1299,7 @@ int cf_set_constraint(cf_handle* h, int kind, double c1, double c2) {
 
 int cf_set_state(cf_handle* h, const double* U, const double* P) {
     if (!h || !U || !P) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
     const size_t fr = sizeof(zd) * h->nr;
     for (int i = 0; i < 3; ++i) CU(cudaMemcpyAsync(h->U[i], U + 2 * i * h->nr, fr, cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemcpyAsync(h->Pf, P, fr, cudaMemcpyHostToDevice, h->stream));
@@ -1248,6 +1309,7 @@ int cf_set_state(cf_handle* h, const double* U, const double* P) {
 }
 int cf_get_state(cf_handle* h, double* U, double* P) {
     if (!h || !U) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
     const size_t fr = sizeof(zd) * h->nr;
     for (int i = 0; i < 3; ++i) CU(cudaMemcpyAsync(U + 2 * i * h->nr, h->U[i], fr, cudaMemcpyDeviceToHost, h->stream));
     if (P) CU(cudaMemcpyAsync(P, h->Pf, fr, cudaMemcpyDeviceToHost, h->stream));
@@ -1256,6 +1318,7 @@ int cf_get_state(cf_handle* h, double* U, double* P) {
 }
 int cf_set_state_device(cf_handle* h, const void* U, const void* P) {
     if (!h || !U || !P) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
     const size_t fr = sizeof(zd) * h->nr;
     for (int i = 0; i < 3; ++i)
         CU(cudaMemcpyAsync(h->U[i], (const char*)U + i * fr, fr, cudaMemcpyDeviceToDevice, h->stream));
@@ -1265,6 +1328,7 @@ int cf_set_state_device(cf_handle* h, const void* U, const void* P) {
 }
 int cf_get_state_device(cf_handle* h, void* U, void* P) {
     if (!h || !U) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
     const size_t fr = sizeof(zd) * h->nr;
     for (int i = 0; i < 3; ++i)
         CU(cudaMemcpyAsync((char*)U + i * fr, h->U[i], fr, cudaMemcpyDeviceToDevice, h->stream));
@@ -1274,6 +1338,7 @@ int cf_get_state_device(cf_handle* h, void* U, void* P) {
 
 int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out) {
     if (!h) return fail(CF_E_ARG, "null handle");
+    DeviceGuard dg_(h->device);
     if (nsteps < 0) return fail(CF_E_ARG, "nsteps must be nonnegative");
     int rc, cnt = 0;
     if (!h->nodal_valid) {
@@ -1285,7 +1350,7 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
     cnt += (h->mixed && h->tc ? 18 : step_launches(h)) * nsteps;
     h->last_launches = cnt;
     if (t_out) *t_out = t + nsteps * h->dt;
-    if (grads_out && (rc = check_cheb_err(h))) return rc;
+    if (grads_out && (rc = check_status(h))) return rc;
     if (grads_out) {
         double g[2];
         CU(cudaMemcpyAsync(g, h->d_grad, 16, cudaMemcpyDeviceToHost, h->stream));
@@ -1298,6 +1363,7 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
 
 int cf_step_dt(cf_handle* h, double t, double dt, double* t_out, double* grads_out) {
     if (!h) return fail(CF_E_ARG, "null handle");
+    DeviceGuard dg_(h->device);
     if (!(std::isfinite(dt) && dt > 0)) return fail(CF_E_ARG, "dt must be finite and positive");
     if (dt == h->dt) return cf_step(h, t, 1, t_out, grads_out);
     int rc, cnt = 0;
@@ -1326,7 +1392,7 @@ int cf_step_dt(cf_handle* h, double t, double dt, double* t_out, double* grads_o
     if (rc) return rc;
     h->last_launches = cnt;
     if (t_out) *t_out = t + dt;
-    if (grads_out && (rc = check_cheb_err(h))) return rc;
+    if (grads_out && (rc = check_status(h))) return rc;
     if (grads_out) {
         double g[2];
         CU(cudaMemcpyAsync(g, h->d_grad, 16, cudaMemcpyDeviceToHost, h->stream));
@@ -1349,6 +1415,7 @@ int cf_step_dt(cf_handle* h, double t, double dt, double* t_out, double* grads_o
 // from the state, which gives the same values.
 int cf_step_host(cf_handle* h, double* U, double* P, double t, int nsteps, double* t_out, double* grads_out) {
     if (!h || !U || !P) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
     if (nsteps < 0) return fail(CF_E_ARG, "nsteps must be nonnegative");
     int rc;
     if (nsteps == 0 || (h->mixed && h->tc)) {
@@ -1423,7 +1490,7 @@ int cf_step_host(cf_handle* h, double* U, double* P, double t, int nsteps, doubl
     const cudaError_t e = cudaStreamSynchronize(h->cstream);
     if (rc) return rc;
     if (e != cudaSuccess) return fail(CF_E_CUDA, std::string("host step copies: ") + cudaGetErrorString(e));
-    if ((rc = check_cheb_err(h))) return rc;
+    if ((rc = check_status(h))) return rc;
     if (t_out) *t_out = t + nsteps * h->dt;
     if (grads_out) {
         double g[2];
@@ -1460,6 +1527,7 @@ static int launch_nonlinear(cf_engine* h, zd* const Us[3]) {
 
 int cf_nonlinear(cf_handle* h, const double* U, double* N) {
     if (!h || !U || !N) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
     int rc = ensure_tmp(h);
     if (rc) return rc;
     const size_t fr = sizeof(zd) * h->nr;
@@ -1467,47 +1535,26 @@ int cf_nonlinear(cf_handle* h, const double* U, double* N) {
     zd* Us[3] = {h->tmpU, h->tmpU + h->nr, h->tmpU + 2 * h->nr};
     if ((rc = launch_nonlinear(h, Us))) return rc;
     CU(cudaMemcpyAsync(N, h->tmpU, 3 * fr, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
+    if ((rc = check_status(h, false))) return rc;
     h->nodal_valid = false;
-    return CF_OK;
-}
-
-// Fixed scratch of cf_nonlinear_noalloc: one array per device (module scope),
-// its address looked up once per device with that device current.
-#define CF_MAX_DEVICES 64
-static __device__ __align__(256) unsigned char g_noalloc_scratch[CF_NOALLOC_SCRATCH_BYTES];
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_addr[CF_MAX_DEVICES] = {};
-
-static int noalloc_scratch(void** out) {
-    int dev = 0;
-    CU(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= CF_MAX_DEVICES) return fail(CF_E_UNSUPPORTED, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return fail(CF_E_CUDA, std::string("scratch address: ") + cudaGetErrorString(e));
-        g_noalloc_addr[dev] = p;
-    }
-    *out = g_noalloc_addr[dev];
     return CF_OK;
 }
 
 int cf_nonlinear_noalloc(cf_handle* h, const double* U, double* N) {
     if (!h || !U || !N) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
     const size_t fr = sizeof(zd) * h->nr;
     if (3 * fr > (size_t)CF_NOALLOC_SCRATCH_BYTES)
         return fail(CF_E_ARG, "grid too large for the fixed scratch (3 * Nr * 16 bytes > 16 MiB)");
-    void* scr = nullptr;
-    int rc = noalloc_scratch(&scr);
-    if (rc) return rc;
+    void* scr = noalloc_scratch(h->device);
+    if (!scr) return fail(CF_E_CUDA, "fixed scratch address not set up for the handle's device");
+    int rc;
     zd* base = static_cast<zd*>(scr);
     zd* Us[3] = {base, base + h->nr, base + 2 * h->nr};
     CU(cudaMemcpyAsync(base, U, 3 * fr, cudaMemcpyHostToDevice, h->stream));
     if ((rc = launch_nonlinear(h, Us))) return rc;
     CU(cudaMemcpyAsync(N, base, 3 * fr, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
+    if ((rc = check_status(h, false))) return rc;
     h->nodal_valid = false;
     return CF_OK;
 }
@@ -1546,6 +1593,7 @@ static int pressure_dev(cf_engine* h, zd* const Ud[3], zd* Pout) {
 
 int cf_project(cf_handle* h, double* U) {
     if (!h || !U) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
     int rc = ensure_tmp(h);
     if (rc) return rc;
     const size_t fr = sizeof(zd) * h->nr;
@@ -1553,12 +1601,13 @@ int cf_project(cf_handle* h, double* U) {
     zd* Us[3] = {h->tmpU, h->tmpU + h->nr, h->tmpU + 2 * h->nr};
     if ((rc = project_dev(h, Us))) return rc;
     CU(cudaMemcpyAsync(U, h->tmpU, 3 * fr, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
+    if ((rc = check_status(h, false))) return rc;
     return CF_OK;
 }
 
 int cf_pressure(cf_handle* h, const double* U, double* P) {
     if (!h || !U || !P) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
     int rc = ensure_tmp(h);
     if (rc) return rc;
     const size_t fr = sizeof(zd) * h->nr;
@@ -1566,12 +1615,13 @@ int cf_pressure(cf_handle* h, const double* U, double* P) {
     zd* Us[3] = {h->tmpU, h->tmpU + h->nr, h->tmpU + 2 * h->nr};
     if ((rc = pressure_dev(h, Us, h->tmpP))) return rc;
     CU(cudaMemcpyAsync(P, h->tmpP, fr, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
+    if ((rc = check_status(h, false))) return rc;
     return CF_OK;
 }
 
 int cf_random_state(cf_handle* h, unsigned long long seed, double amp, int shape, double rho) {
     if (!h) return fail(CF_E_ARG, "null handle");
+    DeviceGuard dg_(h->device);
     if (!(amp >= 0)) return fail(CF_E_ARG, "epsilon must be non-negative");
     std::vector<std::complex<double>> U;
     host_synth(h, seed, amp, shape, rho, U);
@@ -1581,7 +1631,7 @@ int cf_random_state(cf_handle* h, unsigned long long seed, double amp, int shape
     int rc;
     if ((rc = project_dev(h, h->U))) return rc;
     if ((rc = pressure_dev(h, h->U, h->Pf))) return rc;
-    CU(cudaStreamSynchronize(h->stream));
+    if ((rc = check_status(h, false))) return rc;
     h->nodal_valid = false;
     return CF_OK;
 }
@@ -1596,16 +1646,23 @@ static DiagKernel diag_kernel(int P) {
     }
 }
 
-// Diagnostics on the device: one column team per Fourier column (see
-// k_column_diag); five doubles come back to the host.
-int cf_diagnostics(cf_handle* h, double* out) {
-    if (!h || !out) return fail(CF_E_ARG, "null argument");
+static int ensure_diag(cf_engine* h) {
     int rc;
     if (!h->d_diag) {
         if ((rc = dalloc(h, (void**)&h->d_diag, 8 * sizeof(double)))) return rc;
         if ((rc = dalloc(h, (void**)&h->d_diagpart, 3 * sizeof(double) * col_blocks(h)))) return rc;
         if ((rc = raise_smem_limit(diag_kernel(h->P), col_smem(h)))) return rc;
     }
+    return CF_OK;
+}
+
+// Diagnostics on the device: one column team per Fourier column (see
+// k_column_diag); five doubles come back to the host.
+int cf_diagnostics(cf_handle* h, double* out) {
+    if (!h || !out) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
+    int rc;
+    if ((rc = ensure_diag(h))) return rc;
     CU(cudaMemsetAsync(h->d_diag, 0, 8 * sizeof(double), h->stream));
     ColParams p = col_params(h);
     diag_kernel(h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p, h->d_diag, h->d_diagpart);
@@ -1613,7 +1670,7 @@ int cf_diagnostics(cf_handle* h, double* out) {
     CU(cudaGetLastError());
     double acc[5];
     CU(cudaMemcpyAsync(acc, h->d_diag, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
+    if ((rc = check_status(h, false))) return rc;
     out[0] = acc[0] / 2;
     out[1] = h->nu * acc[1];
     out[2] = acc[2];
@@ -1622,8 +1679,25 @@ int cf_diagnostics(cf_handle* h, double* out) {
     return CF_OK;
 }
 
+// Power input of the engine's mean profile (one warp over the (0,0) column;
+// one double comes back).
+int cf_power_input(cf_handle* h, int with_base, double dPdx, double dPdz, double* out) {
+    if (!h || !out) return fail(CF_E_ARG, "null argument");
+    if (!(std::isfinite(dPdx) && std::isfinite(dPdz))) return fail(CF_E_ARG, "pressure gradient must be finite");
+    DeviceGuard dg_(h->device);
+    int rc;
+    if ((rc = ensure_diag(h))) return rc;
+    k_power_input<<<1, 32, 0, h->stream>>>(h->U[0], h->U[2], with_base ? h->d_base : nullptr, (long)h->Nz * h->Nxh,
+                                           h->Ny, h->nu, dPdx, dPdz, h->d_diag + 6);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(out, h->d_diag + 6, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if ((rc = check_status(h, false))) return rc;
+    return CF_OK;
+}
+
 int cf_step_profiled(cf_handle* h, double t, int nsteps, double* t_out, double* kernel_ms) {
     if (!h || !kernel_ms) return fail(CF_E_ARG, "null argument");
+    DeviceGuard dg_(h->device);
     if (h->mixed) return step_profiled_mx(h, t, nsteps, t_out, kernel_ms);
     int rc = CF_OK, cnt = 0;
     if (!h->nodal_valid) {
@@ -1636,6 +1710,7 @@ int cf_step_profiled(cf_handle* h, double t, int nsteps, double* t_out, double* 
     for (int s = 0; s < nsteps && rc == CF_OK; ++s) rc = launch_step_profiled(h, ev, kernel_ms);
     for (int k = 0; k < 5; ++k) cudaEventDestroy(ev[k]);
     if (rc) return rc;
+    if ((rc = check_status(h))) return rc;
     h->last_launches = cnt + step_launches(h) * nsteps;
     if (t_out) *t_out = t + nsteps * h->dt;
     return CF_OK;
@@ -1643,9 +1718,18 @@ int cf_step_profiled(cf_handle* h, double t, int nsteps, double* t_out, double* 
 
 int cf_sync(cf_handle* h) {
     if (!h) return fail(CF_E_ARG, "null handle");
-    CU(cudaStreamSynchronize(h->stream));
+    DeviceGuard dg_(h->device);
+    int rc;
+    if ((rc = check_status(h))) return rc;
     return CF_OK;
 }
+int cf_set_wait_limit(cf_handle* h, long spins) {
+    if (!h) return fail(CF_E_ARG, "null handle");
+    h->wait_spins = spins < 0 ? CF_WAIT_SPINS : spins;
+    drop_graph(h);  // the step graph holds the launch parameters
+    return CF_OK;
+}
+long long cf_device_bytes(cf_handle* h) { return h ? (long long)h->dev_bytes : 0; }
 int cf_last_launch_count(cf_handle* h) { return h ? h->last_launches : 0; }
 void* cf_stream(cf_handle* h) { return h ? (void*)h->stream : nullptr; }
 
@@ -1936,8 +2020,8 @@ static float host_tf32(float x) {
 }
 
 // T^T K-tile images (TF32 heads and remainders, see cf_cheb.cuh) of
-//   inverse:  y_n = sum_k a_k cos(pi n k / P)                 (ffts.jl:282-287)
-//   forward:  a_k = scale e_k sum_n w_n x_n cos(pi n k / P)   (ffts.jl:189-206,
+//   inverse:  y_n = sum_k a_k cos(pi n k / P)                 (chebyshev.jl:58-66, ffts.jl:162)
+//   forward:  a_k = scale e_k sum_n w_n x_n cos(pi n k / P)   (ffts.jl:65-82,
 //             e_k = 1/2 at k = 0, P; w_n = 1 at n = 0, P, else 2)
 // Output rows per block: all of them (rounded up to 16) when at most 256,
 // else split over two blocks so that each holds <= 256 TMEM columns.
@@ -2041,6 +2125,7 @@ int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int
         p.Bhi = dB;
         p.Blo = dB + hi.size();
         p.err = derr;
+        p.spins = CF_WAIT_SPINS;
         dim3 grid((unsigned)((C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nfields, (unsigned)nsplit);
         k_cheb_mma<<<grid, 128, cheb_smem(NPs)>>>(p);
         cudaError_t e = cudaGetLastError();

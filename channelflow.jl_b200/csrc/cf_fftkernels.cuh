@@ -1,5 +1,5 @@
 // cf_fftkernels.cuh -- periodic-direction transforms of the nonlinear term
-// (src/ffts.jl:189-206 and 275-290, src/nonlinear.jl:113-191).
+// (src/ffts.jl:65-82, 151-166, 242-312; src/nonlinear.jl:113-199).
 //
 // k_zinv : nodal (Ny,Nz,Nxh) -> z-padded spectrum (copy_to_padded!, Nyquist
 //          filter) -> backward z FFT of length Nzp   (Ny,Nzp,Nxh)
@@ -39,6 +39,7 @@ struct FftParams {
     int zbox, zpbox;  // TMA z kernels: rows per box of the nodal (Nz) and z-padded (Nzp) fields
     int stoff;     // TMA z kernels: byte offset of the staging buffer in shared memory
     int* err;      // TMA z kernels: set to 1 when a wait gives up
+    long spins;    // TMA z kernels: polls of the first wait for a tile (CF_WAIT_SPINS; shortened only by tests)
     double ax, bz;  // 2 pi / Lx, 2 pi / Lz (derivatives of the convective form)
     // nodal and z-padded fields: complex double (FP64 path) or complex float
     // (FP32 transforms of the mixed-precision path)
@@ -169,8 +170,13 @@ CF_DEV bool zload_tma(const FftParams& p, const CUtensorMap* map, int k0, int ro
         for (int b = 0; b < nb; ++b) tma_load_3d(stage + (long)b * box * tkz, map, 2 * k0, b * box, n, mb);
     }
     __syncthreads();
-    const bool ok = __syncthreads_and(mbar_wait(mb, 0));
-    if (!ok && threadIdx.x == 0) atomicExch(p.err, 1);
+    const bool ok = __syncthreads_and(mbar_wait(mb, 0, p.spins));
+    if (!ok) {
+        // the boxes still in flight land before the block gives up its shared memory
+        mbar_wait(mb, 0);
+        __syncthreads();
+        if (threadIdx.x == 0) atomicExch(p.err, 1);
+    }
     return ok;
 }
 template <class Z>

@@ -1,6 +1,6 @@
 // cf_kernels.cuh -- the CNRK2 stage kernels.
 //
-// Per stage (src/timesteppers/cnrk2.jl:588-623) the engine launches
+// Per stage (src/timesteppers/cnrk2.jl:170-205) the engine launches
 //   k_zinv    nodal u, omega (6 fields)  -> z-padded, z-inverse FFT
 //   k_xpass   x c2r of 6 rows, n = u x omega, x r2c of 3 rows, truncation
 //   k_zfwd    z-forward FFT + z truncation -> n at Chebyshev nodes
@@ -55,6 +55,7 @@ struct ColParams {
     double c1, c2;           // gradients, or perturbation bulk targets
     double* grad_out;        // [2]
     double* status;          // [4] diagnostics scratch (unused by the hot path)
+    int* flags;              // status word set to 1 when the mean mode goes non-finite
     FftPlan plP;
     int bofs;        // first column block of the launch (a launch over part of the columns)
     int skip_nodal;  // stage kernels: end after storing the state (no nodal fields for a next stage)
@@ -208,7 +209,7 @@ CF_DEV void col_zero(zd* x, const Team& t) {
 }
 
 // forward DCT of nodal values in x with normalisation, endpoint weights and
-// Nyquist filter (ffts.jl:189-206, normalize_forward! :378-393)
+// Nyquist filter (ffts.jl:65-82, normalize_forward! :254-269)
 template <int PL>
 CF_DEV void col_forward_y(zd* x, zd* z, zd* z2, const ColParams& p, bool nyq, const Team& t) {
     if (nyq) {
@@ -219,7 +220,7 @@ CF_DEV void col_forward_y(zd* x, zd* z, zd* z2, const ColParams& p, bool nyq, co
     }
 }
 // inverse DCT: nodal values of the series (icheb with doubled endpoints, the
-// 1/2 of copy_to_padded!, ffts.jl:282-287)
+// 1/2 of copy_to_padded!, chebyshev.jl:58-66, ffts.jl:162)
 template <int PL>
 CF_DEV void col_inverse_y(zd* x, zd* z, zd* z2, const ColParams& p, const Team& t) {
     col_redft00<PL, CF_DCT_INV>(x, z, z2, p.cs_tab, p.plP, 1.0, t);
@@ -302,7 +303,7 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         }
         tsync(t);
     } else {
-        // mean mode (meanmode.jl:278-288): integrate Ry through degree P-1, gauge
+        // mean mode (meanmode.jl:103-150): integrate Ry through degree P-1, gauge
         for (int j = lane; j < nq; j += 32) {
             const int n = 2 * j + q, o = qo + j;
             zd v = zzero();
@@ -356,7 +357,7 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
 // the nonlinear form needs at the nodes, inverse DCT to the nodal buffers.
 // u, v, w in U0, U1, U2 (modified); Z, Z2 are transform buffers.
 //   NL_ROT  W0, W1, W2 receive the vorticity (nonlinear.jl:179-185,
-//           operators.jl:380-398); six nodal fields
+//           operators.jl:172-190); six nodal fields
 //   NL_CONV W0, W1, W2 receive du_i/dy (grad!, operators.jl:206-214; the x and
 //           z derivatives are formed by the periodic transforms); six fields
 //   NL_DIV  u, v, w alone (nonlinear.jl:153-156); three fields
@@ -544,6 +545,12 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     }
     if (valid && c == 0) {
         zd* R0 = X.col(0);
+        // A NaN or Inf anywhere in the state reaches every Fourier mode of the
+        // nonlinear term within one stage (the periodic transforms mix all
+        // modes), so the (0,0) team's bulk means and wall derivatives see it.
+        if (t.tid == 0 && p.flags &&
+            !isfinite(bulkN0.x + bulkN0.y + bulkN2.x + bulkN2.y + wR0.x + wL0.x + wR2.x + wL2.x))
+            atomicExch(p.flags, 1);
         if (p.cmode == 1) {
             gold[0] = p.nu * (wR0.x - wL0.x) / 2 + p.nu_bm_curv + bulkN0.x;
             gold[1] = p.nu * (wR2.x - wL2.x) / 2 + bulkN2.x;
@@ -962,4 +969,39 @@ static __global__ void __launch_bounds__(1024) k_diag_reduce(const double* __res
         acc[1] = sb;
         acc[2] = sm;
     }
+}
+
+// Power input of the mean profile (src/postprocessing.jl:113-128): for the
+// (0,0) columns of u and w (with the base profile's coefficients added to u
+// when base != null), nu/2 [conj(a(+1)) a'(+1) - conj(a(-1)) a'(-1)] -
+// gradient * bulkmean(a), summed over the two components.  One warp; the
+// column (0,0) of the (Ny, Nz, Nxh) layout has stride Nz * Nxh.
+static __global__ void __launch_bounds__(32) k_power_input(const zd* __restrict__ u, const zd* __restrict__ w,
+                                                         const double* __restrict__ base, long stride, int Ny,
+                                                         double nu, double gx, double gz, double* out) {
+    const int lane = threadIdx.x;
+    double tot = 0.0;
+#pragma unroll 1
+    for (int i = 0; i < 2; ++i) {
+        const zd* a = i ? w : u;
+        zd up = zzero(), lo = zzero(), dr = zzero(), dl = zzero(), bm = zzero();
+        for (int n = lane; n < Ny; n += 32) {
+            zd v = a[(long)n * stride];
+            if (i == 0 && base) v.x += base[n];
+            const double sg = (n & 1) ? -1.0 : 1.0, n2 = (double)n * n;
+            up = zadd(up, v);
+            lo = zaxpy(lo, sg, v);
+            dr = zaxpy(dr, n2, v);
+            dl = zaxpy(dl, -sg * n2, v);
+            if (!(n & 1)) bm = (n == 0) ? zadd(bm, v) : zaxpy(bm, 1.0 / (1.0 - n2), v);
+        }
+        up = warp_sum_z(up);
+        lo = warp_sum_z(lo);
+        dr = warp_sum_z(dr);
+        dl = warp_sum_z(dl);
+        bm = warp_sum_z(bm);
+        // real(conj(x) y) = x.re y.re + x.im y.im
+        tot += nu / 2 * ((up.x * dr.x + up.y * dr.y) - (lo.x * dl.x + lo.y * dl.y)) - (i ? gz : gx) * bm.x;
+    }
+    if (lane == 0) *out = tot;
 }

@@ -7,19 +7,19 @@
 //
 // It restates, function by function, the reference algorithm (paths relative
 // to the ChannelFlow.jl repository):
-//   grids / storage      src/grids.jl:22-96, src/indexing.jl:112-124
-//   transforms           src/ffts.jl:156-206, 245-290, 366-436
-//   DCT-I (REDFT00)      src/transforms/chebyshev.jl:481-502
-//   operators            src/fields/operators.jl:14-190, 478-484
+//   grids / storage      src/grids.jl:22-96, src/indexing.jl:14-28
+//   transforms           src/ffts.jl:65-82, 151-166, 242-312
+//   DCT-I (REDFT00)      src/transforms/chebyshev.jl:45-66
+//   operators            src/fields/operators.jl:14-190, 270-294
 //   nonlinear terms      src/nonlinear.jl:113-193 (rotational, convective,
 //                        divergence forms)
 //   influence solver     src/solvers/influence.jl:60-316
 //   batched bank         src/solvers/batchedinfluence.jl:32-160
 //   mean mode            src/solvers/meanmode.jl:13-150
-//   Stokes wrapper       src/solvers/stokes.jl:340-418
-//   CNRK2                src/timesteppers/cnrk2.jl:430-625
+//   Stokes wrapper       src/solvers/stokes.jl:23-108
+//   CNRK2                src/timesteppers/cnrk2.jl:12-207
 //   projection/pressure  src/pressure.jl:36-204
-//   diagnostics          src/postprocessing.jl:235-299
+//   diagnostics          src/postprocessing.jl:21-128
 // The tau Helmholtz solver of the un-vendored dependency
 // ChebyshevHelmoltzSolvers.jl (v0.1.0, git-tree 27b8d9f9...) is restated from
 // its defining tau system (docs/src/spatial.md:448-475): rows 0..P-2 of
@@ -182,7 +182,7 @@ static void cheb_diff(const T* a, long sa, T* b, long sb, int Ny) {
     for (int n = 0; n < Ny; ++n) b[n * sb] = tmp[n];
 }
 
-// Mean over y: a0 + sum_{even n>=2} a_n/(1-n^2)  (meanmode.jl:173-179)
+// Mean over y: a0 + sum_{even n>=2} a_n/(1-n^2)  (meanmode.jl:13-19)
 template <class T>
 static T bulkmean(const T* a, long s, int Ny) {
     T v = a[0];
@@ -528,7 +528,7 @@ struct ModeSolver {
     }
 };
 
-// Mean mode (meanmode.jl:205-310)
+// Mean mode (meanmode.jl:38-150)
 struct MeanSolver {
     int Ny = 0;
     double nu = 0, lambda = 0;
@@ -614,7 +614,7 @@ static int nthreads() {
 #endif
 }
 
-// Inverse transform (ffts.jl:275-290): spectral (Ny,Nz,Nxh) -> padded physical (Ny,Nzp,Nxp)
+// Inverse transform (ffts.jl:151-166): spectral (Ny,Nz,Nxh) -> padded physical (Ny,Nzp,Nxp)
 // Work array of the padded spectrum, shared by the transforms (the oracle is
 // single-caller) and allocated once, so a timed stage pays no allocation.
 static std::vector<cd>& pad_buffer(size_t n) {
@@ -669,7 +669,7 @@ static void inverse_transform(const OGrid& g, const cd* U, double* u) {
     }
 }
 
-// Forward transform (ffts.jl:189-206, normalize_forward! :378-393)
+// Forward transform (ffts.jl:65-82, normalize_forward! :254-269)
 static void forward_transform(const OGrid& g, const double* u, cd* U) {
     const int Ny = g.Ny, P = Ny - 1, Nz = g.Nz, Nxh = g.Nxh, Nzp = g.Nzp, Nxp = g.Nxp, Nxhp = g.Nxhp;
     std::vector<cd>& pad = pad_buffer((size_t)Ny * Nzp * Nxhp);
@@ -740,7 +740,7 @@ static void op_ddx2(const OGrid& g, const cd* U, cd* O, bool add) {
         }
     }
 }
-// laplacian! non-aliased path (operators.jl:312-332)
+// laplacian! non-aliased path (operators.jl:104-124)
 static void op_laplacian(const OGrid& g, const cd* a, cd* b) {
     const int Ny = g.Ny, Nz = g.Nz, Nxh = g.Nxh;
     const double al2 = std::pow(2 * M_PI / g.Lx, 2), be2 = std::pow(2 * M_PI / g.Lz, 2);
@@ -762,7 +762,7 @@ static void op_laplacian(const OGrid& g, const cd* a, cd* b) {
         }
     }
 }
-// curl! (operators.jl:380-398)
+// curl! (operators.jl:172-190)
 static void op_curl(const OGrid& g, const cd* const U[3], cd* const O[3]) {
     op_ddx2(g, U[2], O[0], false);
     op_ddx2(g, U[0], O[2], false);
@@ -805,7 +805,7 @@ struct Stokes {
         }
         return ok;
     }
-    // solve! (stokes.jl:391-418); mode 0 pressure gradient, 1 bulk (total targets)
+    // solve! (stokes.jl:81-108); mode 0 pressure gradient, 1 bulk (total targets)
     void solve(const OGrid& g, cd* const U[3], cd* Pf, const cd* const R[3], int mode, double c1, double c2,
                double basemean, double* grads) const {
         const long S = (long)g.Nxh * g.Nz;
@@ -863,7 +863,7 @@ static void total_velocity(Problem& pb, const cd* const U[3]) {
     for (int n = 0; n < g.Ny; ++n) pb.TMP[0][n * S] += pb.base[n];
 }
 
-// _store_rhs! with sign -1 (nonlinear.jl:200-210)
+// _store_rhs! with sign -1 (nonlinear.jl:200-208)
 static void negate(const OGrid& g, cd* const N[3]) {
     for (int i = 0; i < 3; ++i) {
         cd* x = N[i];
@@ -969,7 +969,7 @@ static bool problem_stokes(Problem& pb) {
     return true;
 }
 
-// One CNRK2 stage j (cnrk2.jl:588-622) of a step of duration dt with the
+// One CNRK2 stage j (cnrk2.jl:170-205) of a step of duration dt with the
 // Stokes solvers st (the problem's own for its nominal dt); gradients carries
 // the previous stage's uniform gradients in and this stage's out.
 static void cnrk2_stage(Problem& pb, cd* const U[3], cd* Pf, int j, double* gradients, double dt, const Stokes* st) {
@@ -1015,7 +1015,7 @@ static void cnrk2_stage(Problem& pb, cd* const U[3], cd* Pf, int j, double* grad
     st[j].solve(g, U, Pf, Rc, pb.cmode, pb.c1, pb.c2, pb.basemean, gradients);
 }
 
-// step! (cnrk2.jl:567-625).  Returns the last stage's gradients in grads.
+// step! (cnrk2.jl:149-207).  Returns the last stage's gradients in grads.
 static void cnrk2_step(Problem& pb, cd* const U[3], cd* Pf, double* grads, double dt, const Stokes* st) {
     double gradients[2] = {pb.cmode == 0 ? pb.c1 : 0.0, pb.cmode == 0 ? pb.c2 : 0.0};
     for (int j = 0; j < 3; ++j) cnrk2_stage(pb, U, Pf, j, gradients, dt, st);
@@ -1099,7 +1099,7 @@ static bool pressure(Problem& pb, const cd* const U[3], cd* Pout) {
     return ok;
 }
 
-// Spectral inner product (postprocessing.jl:235-259)
+// Spectral inner product (postprocessing.jl:31-62)
 static double spectral_dot(const OGrid& g, const cd* U, const cd* V) {
     const int Ny = g.Ny;
     const long S = (long)g.Nxh * g.Nz;

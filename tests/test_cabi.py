@@ -28,7 +28,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_errors_are_reported_not_crashed():
-    # argument validation happens before any device work (cnrk2.jl:478, stokes.jl:345)
+    # argument validation happens before any device work (stokes.jl:35, stokes.jl:36-38)
     with pytest.raises(cfb200.CFError) as e:
         cfb200.CouetteFlow(cfb200.Grid(8, 10, 8, 6.28, 6.28), 0.01, 0.01)
     assert e.value.code == -1 and "odd Ny" in str(e.value)

@@ -29,6 +29,10 @@ def members():
         out.append(dict(grid=g1, profile="couette", nu=nu, dt=0.01))
     for nu in (1 / 1000, 1 / 1500):
         out.append(dict(grid=g2, profile="poiseuille", nu=nu, dt=0.005, bulkvelocity=(2 / 3, 0.0)))
+    # the Chebyshev length of the 48x49x48 ensemble members (P = 48)
+    g3 = cfb200.Grid(12, 49, 10, LX, LZ)
+    for nu in (1 / 350, 1 / 450):
+        out.append(dict(grid=g3, profile="couette", nu=nu, dt=0.01))
     return out
 
 
@@ -40,7 +44,7 @@ def twin(m):
 def test_ensemble_matches_single_instances():
     ms = members()
     ens = cfb200.Ensemble(ms)
-    assert len(ens) == 5
+    assert len(ens) == 7
     twins = []
     for i, (m, inst) in enumerate(zip(ms, ens.instances)):
         cfb200.random_state(inst, 0.1, seed=100 + i)
@@ -51,8 +55,8 @@ def test_ensemble_matches_single_instances():
     nsteps = 15
     ens.step(nsteps)
     ens.step(nsteps)
-    # two size classes, 12 launches per class per step
-    assert ens.launches() == 12 * 2 * nsteps
+    # three size classes, 12 launches per class per step
+    assert ens.launches() == 12 * 3 * nsteps
     for inst, t in zip(ens.instances, twins):
         t.advance(0.0, 2 * nsteps)
         Ue, Pe = inst.get_state()
@@ -64,14 +68,18 @@ def test_ensemble_matches_single_instances():
     ens.close()
 
 
-def test_ensemble_member_matches_oracle():
+@pytest.mark.parametrize("which", [3, 6])
+def test_ensemble_member_matches_oracle(which):
     ms = members()
     ens = cfb200.Ensemble(ms)
-    m = ms[3]
+    m = ms[which]
     g = m["grid"]
-    ref = O.poiseuille(g.Nx, g.Ny, g.Nz, g.Lx, g.Lz, m["nu"], m["dt"], bulkvelocity=m["bulkvelocity"])
+    if m["profile"] == "poiseuille":
+        ref = O.poiseuille(g.Nx, g.Ny, g.Nz, g.Lx, g.Lz, m["nu"], m["dt"], bulkvelocity=m["bulkvelocity"])
+    else:
+        ref = O.couette(g.Nx, g.Ny, g.Nz, g.Lx, g.Lz, m["nu"], m["dt"])
     U, P = ref.random_state(seed=7, amp=0.1)
-    inst = ens.instances[3]
+    inst = ens.instances[which]
     inst.set_state(U, P)
     Ur, Pr = U.copy(), P.copy()
     ref.step(Ur, Pr, 10)

@@ -9,7 +9,7 @@ rounding differences in v are amplified in p.  A pressure error is a pure
 gradient in the next stage's source, which the Stokes solve absorbs into the
 new pressure, so it never reaches the velocity.  The reference's own CPU/GPU
 parity tests allow the same order (rtol 2e-10 after 5 steps at 16^3 and 1e-8
-on 32^3..128^3, test/cuda/runtests.jl:61,173).
+on 32^3..128^3, test/cuda/runtests.jl:61,170).
 """
 import json
 import os
@@ -224,4 +224,53 @@ def test_long_columns_all_forms(dims, form):
     Ug, Pg = gpu.get_state()
     assert rel(Ug, U) <= 1e-12
     assert rel(Pg, P) <= 1e-9
+    gpu.close()
+
+
+# The column kernels are compiled per Chebyshev length (P = 32, 48, 64, 96,
+# 128, 192, 256, 384) and the x-pass per padded length; these grids run the
+# instantiations that the timed workloads use: P = 256 (384x257x384), P = 128
+# (128x129x128), P = 48 (the 48x49x48 ensemble members), and P = 256 together
+# with the 576-point in-place x-pass and with the 576-point z kernels.
+@pytest.mark.parametrize("form", ["rotational", "convective", "divergence"])
+@pytest.mark.parametrize("dims", [(8, 257, 6), (16, 129, 12), (12, 49, 10), (384, 257, 4), (4, 257, 384)])
+def test_timed_lengths_all_forms(dims, form):
+    Nx, Ny, Nz = dims
+    g = cfb200.Grid(Nx, Ny, Nz, 2 * np.pi, np.pi)
+    nu = (2 / 3) / 10900
+    gpu = cfb200.PoiseuilleFlow(g, nu, 0.002, bulkvelocity=(2 / 3, 0.0), form=form)
+    ref = O.poiseuille(Nx, Ny, Nz, 2 * np.pi, np.pi, nu, 0.002, bulkvelocity=(2 / 3, 0.0), form=form)
+    U, P = ref.random_state(seed=31, amp=0.1, shape=1, rho=0.8)
+    gpu.set_state(U, P)
+    _, gg = gpu.advance(0.0, 3)
+    go = ref.step(U, P, 3)
+    Ug, Pg = gpu.get_state()
+    assert rel(Ug, U) <= 1e-12
+    assert rel(Pg, P) <= 1e-9
+    assert abs(gg[0] - go[0]) <= 1e-13 + 1e-9 * abs(go[0])
+    gpu.close()
+
+
+def test_c2_poiseuille_flux_20_steps():
+    # 128x129x128 constant-flux Poiseuille, Re_bulk = 2800, Lx = 4 pi,
+    # Lz = 4 pi / 3, dt = 0.005, amplitude 0.2 with the k^-2 x 0.7^n spectrum:
+    # velocity, energy, dissipation, wall shear and divergence against the oracle
+    nu = (2 / 3) / 2800
+    gpu, ref = pair(128, 129, 128, 4 * np.pi, 4 * np.pi / 3, nu, 0.005, profile="poiseuille",
+                    bulkvelocity=(2 / 3, 0.0))
+    U, P = ref.random_state(seed=2, amp=0.2, shape=1, rho=0.7)
+    gpu.set_state(U, P)
+    t, gg = gpu.advance(0.0, 20)
+    go = ref.step(U, P, 20)
+    Ug, Pg = gpu.get_state()
+    assert abs(t - 0.1) < 1e-12
+    assert rel(Ug, U) <= 1e-11
+    assert rel(Pg, P) <= 1e-8
+    assert abs(gg[0] - go[0]) <= 1e-13 + 1e-9 * abs(go[0])
+    dg, do = gpu.diagnostics(), ref.diagnostics(U)
+    assert abs(dg[0] - do[0]) <= 1e-11 * abs(do[0])  # kinetic energy
+    assert abs(dg[1] - do[1]) <= 1e-11 * abs(do[1])  # dissipation
+    assert dg[2] < 1e-8  # divergence
+    for i in (3, 4):  # wall shear of the mean mode
+        assert abs(dg[i] - do[i]) <= 1e-11 * max(1e-3, abs(do[i]))
     gpu.close()

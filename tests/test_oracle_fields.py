@@ -66,7 +66,7 @@ def test_highest_chebyshev_coefficient(N):
 @pytest.mark.parametrize("Ny", [9, 17])
 @pytest.mark.parametrize("NxNz", [(40, 42), (41, 43)])
 def test_analytic_derivatives(Ny, NxNz):
-    # test_operators.jl:1-184
+    # test_operators.jl:1-95
     Nx, Nz = NxNz
     pb = make(Nx, Ny, Nz, 5.3, 7.1)
     a, b = 2 * np.pi / 5.3, 2 * np.pi / 7.1

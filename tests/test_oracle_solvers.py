@@ -129,7 +129,7 @@ def test_influence_rejects_bad_sizes():
 
 
 def test_mean_mode(method):
-    # test_helmoltz.jl:238-364
+    # test_helmoltz.jl:151-277
     for Ny in (9, 16, 33):
         for lam in (0.0, 2.5):
             nu = 0.03
@@ -169,7 +169,7 @@ def test_mean_mode(method):
     normal = derivative(p) - R[1]
     assert np.max(np.abs(normal[: Ny - 1])) < 2e-11
     assert abs(normal[-1] + R[1][-1]) < 2e-12
-    # golden value: test_helmoltz.jl:357-362
+    # golden value: test_helmoltz.jl:273-275
     small = [np.zeros(5, complex)] * 3
     (u, v, w, p), g = O.mean_solve(5, nu, 0.0, *small, bulkvelocity=(2 / 3, 0))
     assert abs(g[0] + 2 * nu) < 2e-12 and abs(g[1]) < 2e-12
