@@ -167,11 +167,6 @@ def traffic_from_profiles(kernel, cfg_name):
         return None
 
 
-# CPU sample size: each timed CPU "step" runs 1/SAMPLE_DIV of every independent
-# loop of one CNRK2 stage (columns, y-planes, rows, points) of the full grid.
-SAMPLE_DIV = {"c1": 1, "c2": 1, "c3": 16, "c5": 48}
-
-
 def make_oracle(cfg):
     from oracle import oracle as O
 
@@ -181,24 +176,52 @@ def make_oracle(cfg):
     return O.poiseuille(c["Nx"], c["Ny"], c["Nz"], c["Lx"], c["Lz"], c["nu"], c["dt"], bulkvelocity=c["constraint"])
 
 
-def cpu_baseline(cfg, threads, div):
-    """Oracle port timed on this host: 1/div of one CNRK2 stage of the full workload."""
+def time_oracle_stages(cfg, threads, warmup, count):
+    """The oracle port (the reference's algorithm restated in C++) timed on
+    this host: full, unsampled CNRK2 stages of the whole workload, `warmup`
+    untimed ones, then `count` timed ones (stage j = i mod 3 in turn, as a step
+    runs them).  Returns (seconds per step, the stage times): a step is the
+    sum over its three stages of the fastest sample of each (the minimum of
+    the samples after warm-up, as the reference's own benchmark takes the
+    minimum, benchmarks/step.jl:31-53); with fewer than three samples, three
+    times the fastest stage."""
     from oracle import oracle as O
 
     O.set_threads(threads)
     O.set_helmholtz_method("quasitri")
+    O.set_sample_div(1)
     c = cfg
     pb = make_oracle(cfg)
     U = pb.synth(seed=1, amp=c["amp"], shape=c["shape"], rho=c["rho"])
     P = pb.zeros()
     pb.prepare()
-    O.set_sample_div(div)
-    pb.stage(U, P, 0)
-    t0 = time.perf_counter()
-    pb.stage(U, P, 1)
-    dt = time.perf_counter() - t0
-    O.set_sample_div(1)
-    return dt * div
+    for w in range(warmup):
+        pb.stage(U, P, w % 3)
+    times = [[], [], []]
+    for i in range(count):
+        j = (warmup + i) % 3
+        t0 = time.perf_counter()
+        pb.stage(U, P, j)
+        times[j].append(time.perf_counter() - t0)
+    if all(times):
+        step_s = sum(min(t) for t in times)
+    else:
+        step_s = 3 * min(t for ts in times for t in ts)
+    return step_s, times
+
+
+def cpu_baseline(cfg, name):
+    """The CPU baseline of the engine line: one full stage of the workload on
+    all host threads after one warm-up stage, and (for the scaling with
+    cores) three full stages of 128x129x128 on one thread."""
+    threads = os.cpu_count() or 1
+    step_s, times = time_oracle_stages(cfg, threads, 1, 1)
+    one_s, _ = time_oracle_stages(CONFIGS["c2"], 1, 1, 3)
+    return {"value": 1.0 / step_s, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"one full CNRK2 stage of {name} ({times[1][0]:.2f} s, after one warm-up stage) on "
+                      f"{threads} threads; steps/s = 1/(3 x stage time)",
+            "one_thread_c2": {"value": 1.0 / one_s, "unit": "steps/s", "cores": 1,
+                              "sample": "three full stages of 128x129x128 (one of each) after one warm-up stage"}}
 
 
 # ---- replicas: one process per GPU, no data-path collective; the ranks only
@@ -247,8 +270,8 @@ def finish_ranks(dist):
 
 def run_reference(args, cfg, rank):
     """--impl reference: the oracle port (the reference's algorithm restated on
-    the CPU) on this host's cores; each step is a bounded sample of one CNRK2
-    stage of the full workload; steps/s = 1 / (3 x stage time)."""
+    the CPU) on all of this host's cores; each timed step is one full,
+    unsampled CNRK2 stage of the workload (time_oracle_stages)."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
@@ -263,34 +286,18 @@ def run_reference(args, cfg, rank):
                 "e2e": {"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
-    from oracle import oracle as O
-
-    O.set_threads(threads)
-    O.set_helmholtz_method("quasitri")
-    c = cfg
-    div = SAMPLE_DIV[args.config]
-    pb = make_oracle(cfg)
-    U = pb.synth(seed=1, amp=c["amp"], shape=c["shape"], rho=c["rho"])
-    P = pb.zeros()
-    pb.prepare()
-    O.set_sample_div(div)
-    for w in range(args.warmup):
-        pb.stage(U, P, w % 3)
-    t0 = time.perf_counter()
-    for s in range(args.steps):
-        pb.stage(U, P, s % 3)
-    el = time.perf_counter() - t0
-    O.set_sample_div(1)
-    stage_s = div * el / max(args.steps, 1)
-    value = 1.0 / (3 * stage_s)
+    step_s, times = time_oracle_stages(cfg, threads, args.warmup, args.steps)
+    value = 1.0 / step_s
+    timed = sum(t for ts in times for t in ts)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3 * stage_s * 1e3, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.config, **workload_desc(cfg)},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
-                         "sample": f"each timed step runs 1/{div} of every independent loop of one CNRK2 stage of the "
-                                   f"full grid; steps/s = 1/(3 x {div} x sample time)"},
+                         "sample": f"each timed step is one full, unsampled CNRK2 stage of the workload (stages "
+                                   f"0, 1, 2 in turn, {args.warmup} warm-up stages first); steps/s = 1 / (sum over "
+                                   f"the three stages of the fastest sample of each); {timed:.1f} s timed"},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -327,6 +334,13 @@ def ensemble_model_bytes(cfg, members):
 
 
 def run_ensemble(args, cfg, rank, world, local, torch, dist):
+    """--config c4: the ensemble line (measure_ensemble) printed by rank 0."""
+    line = measure_ensemble(args, cfg, rank, world, local, torch, dist)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_ensemble(args, cfg, rank, world, local, torch, dist):
     """Ensemble workload: value = aggregate steps/s of all instances advanced
     together (cf_step_batch); the same instances stepped one after another,
     each through its own CUDA-graph step, give the sequential figure."""
@@ -431,9 +445,8 @@ def run_ensemble(args, cfg, rank, world, local, torch, dist):
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = ensemble_cpu(cfg, members, os.cpu_count() or 1)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     ens.close()
+    return line
 
 
 def ensemble_cpu(cfg, members, threads):
@@ -463,12 +476,38 @@ def make_problem(cfb200, g, cfg, precision):
     return cfb200.PoiseuilleFlow(g, cfg["nu"], cfg["dt"], bulkvelocity=cfg["constraint"], precision=precision)
 
 
-def measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, nerr=100, precision="mixed"):
+MIXED_DESC = {
+    "mixed": "FP32 periodic transforms and products (FP32 nodal fields); FP64 Chebyshev transforms, Stokes solve "
+             "and state",
+    "mixed-tc": "FP32 periodic transforms and products; tensor-core Chebyshev transforms (TF32 heads and "
+                "remainders, three products, FP32 accumulation); FP64 Stokes solve and state",
+    "mixed-bf16": "FP32 periodic transforms and products; tensor-core Chebyshev transforms (three BF16 pieces per "
+                  "operand, six BF16 products, FP32 accumulation); FP64 Stokes solve and state",
+}
+
+
+def fp64_reference_run(cfg, g, U0, P0, nerr):
+    """The FP64 engine's state, diagnostics and last gradients after nerr steps
+    from (U0, P0): the reference of the mixed forms' errors."""
+    import cfb200
+
+    ref = make_problem(cfb200, g, cfg, "fp64")
+    ref.set_state(U0, P0)
+    _, grads = ref.advance(0.0, nerr)
+    Ur, _ = ref.get_state()
+    dr = ref.diagnostics()
+    ref.close()
+    return Ur, dr, grads
+
+
+def measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, fp64, nerr, precision="mixed"):
     """A mixed-precision step on the same workload: steps/s (device-resident
     state, CUDA-graph step, CUDA events), per-kernel event timing, and the
-    error against the FP64 step after nerr steps from the same initial state.
+    error of every reported result against the FP64 step after nerr steps from
+    the same initial state (fp64: fp64_reference_run's result).
     precision "mixed": FP32 periodic transforms, FP64 Chebyshev transforms in
-    the column kernel; "mixed-tc": the Chebyshev transforms on the tensor cores."""
+    the column kernel; "mixed-tc" / "mixed-bf16": the Chebyshev transforms on
+    the tensor cores with the TF32 or the BF16 operand split."""
     import cfb200
 
     mx = make_problem(cfb200, g, cfg, precision)
@@ -494,39 +533,43 @@ def measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, nerr=100, precisi
     tc_peak = peaks_tensor()
     # tensor-core transform: algorithmic FLOPs of one contraction (2 Ny^2 C per
     # field) and bytes (FP32 in and out); the TF32 split issues 3x the FLOPs
+    # (K = 8 per TF32 MMA), the BF16 split 6x (K = 16 at twice the rate)
     cheb = {}
-    for key, nf in ((("cheb_fwd", 3), ("cheb_inv", 6)) if precision == "mixed-tc" else ()):
+    nprod = {"mixed-tc": 3, "mixed-bf16": 6}.get(precision, 0)
+    for key, nf in ((("cheb_fwd", 3), ("cheb_inv", 6)) if nprod else ()):
         t = kavg[key] * 1e-3
         flops, byts = 2.0 * Ny * Ny * C * nf, 8.0 * Ny * C * nf
         cheb[key] = {"ms": kavg[key], "algorithmic_TFLOPs": flops / t / 1e12,
-                     "issued_TFLOPs_3xTF32": 3 * flops / t / 1e12, "GBs": byts / t / 1e9,
+                     "issued_TFLOPs": nprod * flops / t / 1e12, "products": nprod, "GBs": byts / t / 1e9,
                      "hbm_frac": byts / t / 1e9 / peak,
-                     "tensor_frac_of_bf16_peak": (3 * flops / t / 1e12) / tc_peak if tc_peak else None}
+                     # issued rate against the measured dense BF16 peak, halved for
+                     # TF32 operands (the TF32 tensor rate is half the BF16 one)
+                     "tensor_frac_of_type_peak": ((nprod * flops / t / 1e12) / (tc_peak * (0.5 if nprod == 3 else 1.0))
+                                                  if tc_peak else None)}
     # error against the FP64 step
-    ref = make_problem(cfb200, g, cfg, "fp64")
-    ref.set_state(U0, P0)
+    Ur, dr, gr = fp64
     mx.set_state(U0, P0)
-    ref.advance(0.0, nerr)
-    mx.advance(0.0, nerr)
-    Ur, _ = ref.get_state()
+    _, gm = mx.advance(0.0, nerr)
     Um, _ = mx.get_state()
-    dr, dm = ref.diagnostics(), mx.diagnostics()
+    dm = mx.diagnostics()
+
+    def rerr(a, b):
+        return float(abs(a - b) / max(abs(b), 1e-300))
+
     out = {"value": args.steps / (ms / 1e3), "unit": "steps/s", "ms_per_step": ms / args.steps,
            "kernel_ms_per_launch": kavg, "gpu_launches": launches,
            "error_vs_fp64": {"steps": nerr,
                              "velocity_rel_l2": float(np.linalg.norm(Um - Ur) / np.linalg.norm(Ur)),
-                             "energy_rel": float(abs(dm[0] - dr[0]) / abs(dr[0])),
-                             "dissipation_rel": float(abs(dm[1] - dr[1]) / abs(dr[1])),
-                             "max_div_mixed": float(dm[2])},
-           "precision": ("FP32 periodic transforms and products; tensor-core Chebyshev transforms "
-                         "(TF32 heads and remainders, FP32 accumulation); FP64 Stokes solve and state"
-                         if precision == "mixed-tc" else
-                         "FP32 periodic transforms and products (FP32 nodal fields); FP64 Chebyshev "
-                         "transforms, Stokes solve and state")}
+                             "energy_rel": rerr(dm[0], dr[0]),
+                             "dissipation_rel": rerr(dm[1], dr[1]),
+                             "wall_shear_upper_rel": rerr(dm[3], dr[3]),
+                             "wall_shear_lower_rel": rerr(dm[4], dr[4]),
+                             "flux_gradient_rel": rerr(gm[0], gr[0]),
+                             "max_div_mixed": float(dm[2]), "max_div_fp64": float(dr[2])},
+           "precision": MIXED_DESC[precision]}
     if cheb:
         out["tensor_core_transforms"] = cheb
     mx.close()
-    ref.close()
     return out
 
 
@@ -549,6 +592,9 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--form", default="rotational", choices=["rotational", "convective", "divergence"],
                     help="nonlinear form of the FP64 step (the mixed form runs the rotational one)")
+    ap.add_argument("--err-steps", type=int, default=1000,
+                    help="steps after which the mixed forms' errors against FP64 are taken")
+    ap.add_argument("--no-c4", action="store_true", help="skip the ensemble measurement of the default line")
     ap.add_argument("--grid", default=None,
                     help="Nx,Ny,Nz replacing the configuration's grid (smaller cases for profiling)")
     args = ap.parse_args()
@@ -664,19 +710,17 @@ def main():
         "diagnostics": {"kinetic_energy": diag[0], "dissipation": diag[1], "max_div": diag[2]},
     }
     if not args.no_mixed:
-        mixed = measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks)
-        mixed["speedup_vs_fp64_plain"] = mixed["value"] / (value / world)
-        tc = measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, nerr=20, precision="mixed-tc")
-        tc["speedup_vs_fp64_plain"] = tc["value"] / (value / world)
-        mixed["tensor_core_variant"] = tc
-        line["mixed"] = mixed
+        fp64 = fp64_reference_run(cfg, g, U0, P0, args.err_steps)
+        line["mixed"] = {}
+        for prec, key in (("mixed", "default"), ("mixed-tc", "tensor_core_tf32"), ("mixed-bf16", "tensor_core_bf16")):
+            m = measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, fp64, args.err_steps, precision=prec)
+            m["speedup_vs_fp64_plain"] = m["value"] / (value / world)
+            line["mixed"][key] = m
+    if not args.no_c4 and args.config == "c3" and not args.grid:
+        line["c4"] = measure_ensemble(argparse.Namespace(steps=5, warmup=3, no_cpu=True), CONFIGS["c4"], rank,
+                                      world, local, torch, dist)
     if rank == 0 and world == 1 and not args.no_cpu:
-        threads = os.cpu_count() or 1
-        div = SAMPLE_DIV[args.config]
-        stage_s = cpu_baseline(cfg, threads, div)
-        line["cpu_baseline"] = {"value": 1.0 / (3 * stage_s), "unit": "steps/s", "cores": threads, "kind": "port",
-                                "sample": f"1/{div} of every independent loop of one CNRK2 stage of the full grid "
-                                          f"on the oracle; steps/s = 1/(3 x {div} x sample time)"}
+        line["cpu_baseline"] = cpu_baseline(cfg, args.config)
     if rank == 0:
         print(json.dumps(line), flush=True)
     pb.close()

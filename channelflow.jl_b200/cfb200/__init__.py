@@ -39,7 +39,7 @@ class _Config(ctypes.Structure):
                 ("constraint", ctypes.c_int), ("c1", ctypes.c_double), ("c2", ctypes.c_double),
                 ("precision", ctypes.c_int), ("form", ctypes.c_int)]
 
-PRECISIONS = {"fp64": 0, "mixed": 1, "mixed-tc": 2}
+PRECISIONS = {"fp64": 0, "mixed": 1, "mixed-tc": 2, "mixed-bf16": 3}
 # NonLinearTerm forms (src/nonlinear.jl:10-17): CF_FORM_* of cfb200.h
 FORMS = {"rotational": 0, "convective": 1, "divergence": 2}
 
@@ -50,7 +50,7 @@ EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_g
            "cf_stream", "cf_last_error", "cf_step_profiled", "cf_nonlinear_noalloc", "cf_create_batch",
            "cf_destroy_batch", "cf_batch_size", "cf_batch_instance", "cf_step_batch",
            "cf_batch_last_launch_count", "cf_batch_stream", "cf_cheb_transform", "cf_step_dt",
-           "cf_step_host", "cf_power_input", "cf_device_bytes", "cf_set_wait_limit"]
+           "cf_step_host", "cf_power_input", "cf_device_bytes", "cf_set_wait_limit", "cf_cheb_transform_split"]
 
 # return codes of cfb200.h
 CF_E_ARG, CF_E_SINGULAR, CF_E_NOMEM, CF_E_CUDA, CF_E_UNSUPPORTED, CF_E_NONFINITE = -1, -2, -3, -4, -5, -6
@@ -104,6 +104,9 @@ def lib():
         L.cf_device_bytes.argtypes = [ctypes.c_void_p]
         L.cf_device_bytes.restype = ctypes.c_longlong
         L.cf_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_long]
+        L.cf_cheb_transform_split.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                              ctypes.c_int, ctypes.c_long, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_double, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -398,16 +401,18 @@ class Ensemble:
         self.close()
 
 
-def cheb_transform(X, inverse, scale=1.0):
+def cheb_transform(X, inverse, scale=1.0, split="tf32"):
     """Chebyshev transform along axis 1 of float32 X (fields, Ny, C) on the
     tensor cores: inverse -> values at the Lobatto nodes; forward -> scaled
-    coefficients with halved end coefficients."""
+    coefficients with halved end coefficients.  split: "tf32" (heads and
+    remainders) or "bf16" (three BF16 pieces)."""
     X = np.ascontiguousarray(X, dtype=np.float32)
     nf, Ny, C = X.shape
     Y = np.zeros_like(X)
     fp = ctypes.POINTER(ctypes.c_float)
-    _check(lib().cf_cheb_transform(X.ctypes.data_as(fp), Y.ctypes.data_as(fp), Ny, C, nf, 1 if inverse else 0,
-                                   float(scale)))
+    code = {"tf32": 0, "bf16": 1}[split]
+    _check(lib().cf_cheb_transform_split(X.ctypes.data_as(fp), Y.ctypes.data_as(fp), Ny, C, nf,
+                                         1 if inverse else 0, float(scale), code))
     return Y
 
 

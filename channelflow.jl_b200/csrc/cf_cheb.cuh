@@ -28,7 +28,17 @@
 // TF32 keeps 10 mantissa bits, so each operand is split into a TF32 head and
 // the TF32 rounding of its remainder; hi*hi + hi*lo + lo*hi restores ~FP32
 // accuracy (the three products accumulate in the same FP32 tensor memory).
+// The BF16 split (SPLIT 1, kind::f16 with BF16 operands, K = 16 per MMA)
+// writes each operand as three BF16 pieces x = b0 + b1 + b2 (8 significant
+// bits each, 24 in all: the FP32 value), with b1 = bf16(x - b0) and
+// b2 = bf16(x - b0 - b1), both differences exact in FP32, and accumulates the
+// six products b_i c_j with i + j <= 2 (the dropped ones are below 2^-24 of
+// the product): FP32-level accuracy from BF16 tensor cores.  Its chunks of 16
+// bytes hold 8 K values, so a K-tile of 16 is two chunks and one MMA step;
+// the images are [2 chunks][NP rows][8 bf16] per K-tile and piece.
 #pragma once
+#include <cuda_bf16.h>
+
 #include "cf_common.cuh"
 
 #define CF_CHEB_MT 128   // columns per block (MMA M)
@@ -42,8 +52,10 @@ struct ChebParams {
     long C;            // real columns per field
     const float* X[CF_CHEB_MAXF];
     float* Y[CF_CHEB_MAXF];
-    const float* Bhi;  // [nkt][4 chunks][NP rows][4 floats] K-tile images of T^T (TF32 heads)
-    const float* Blo;  // remainders
+    // K-tile images of T^T, one per operand piece: TF32 [nkt][4 chunks][NP
+    // rows][4 floats] (head, remainder); BF16 [nkt][2 chunks][NP rows][8
+    // bf16] (three pieces)
+    const void* B[3];
     int* err;          // set to 1 when a wait gives up
     long spins;        // polls of a wait for a free stage (CF_WAIT_SPINS; shortened only by tests)
 };
@@ -73,6 +85,27 @@ CF_DEV void umma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t i
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
+// instruction descriptor: D F32, A and B BF16 (kind::f16), both K-major, M x N
+CF_DEV uint32_t umma_idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+CF_DEV void umma_f16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+// the three BF16 pieces of x (round to nearest even; the differences are exact)
+CF_DEV void bf16_split3(float x, uint16_t& b0, uint16_t& b1, uint16_t& b2) {
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(h0);
+    const __nv_bfloat16 h1 = __float2bfloat16_rn(r1);
+    const __nv_bfloat16 h2 = __float2bfloat16_rn(r1 - __bfloat162float(h1));
+    b0 = __bfloat16_as_ushort(h0);
+    b1 = __bfloat16_as_ushort(h1);
+    b2 = __bfloat16_as_ushort(h2);
+}
 CF_DEV void umma_commit(uint32_t mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                  : "memory");
@@ -96,18 +129,36 @@ CF_DEV void tmem_ld16(uint32_t taddr, float* v) {
 
 // ---- the kernel ------------------------------------------------------------------
 // grid (ceil(C / 128), fields, nsplit); 128 threads.  Dynamic shared memory:
-// nst stages of [A heads, A remainders (8 KB each), B heads, B remainders
-// (NPs * 64 B each)], then two mbarriers and the TMEM address.  With two
-// stages the loads of K-tile kt overlap the MMAs of K-tile kt - 1.
-CF_DEV uint32_t cheb_stage_bytes(int NPs) { return 2u * CF_CHEB_MT * CF_CHEB_KT * 4 + 2u * NPs * CF_CHEB_KT * 4; }
+// nst stages of [A pieces, B pieces] (TF32: two pieces of 8 KB + NPs * 64 B;
+// BF16: three of 4 KB + NPs * 32 B), then two mbarriers and the TMEM address.
+// With two stages the loads of K-tile kt overlap the MMAs of K-tile kt - 1.
+template <int SPLIT>
+struct ChebSplit;
+template <>
+struct ChebSplit<0> {  // TF32 head and remainder, three products
+    static constexpr int NPC = 2, ES = 4, CPK = 4, BQ = 5;
+};
+template <>
+struct ChebSplit<1> {  // BF16 pieces b0 + b1 + b2, six products
+    static constexpr int NPC = 3, ES = 2, CPK = 2, BQ = 4;
+};
+__host__ __device__ constexpr uint32_t cheb_stage_bytes(int NPs, int split) {
+    return split ? 3u * CF_CHEB_MT * CF_CHEB_KT * 2 + 3u * NPs * CF_CHEB_KT * 2
+                 : 2u * CF_CHEB_MT * CF_CHEB_KT * 4 + 2u * NPs * CF_CHEB_KT * 4;
+}
 
+template <int SPLIT>
 __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
+    using S = ChebSplit<SPLIT>;
+    constexpr int NPC = S::NPC, CPK = S::CPK, BQ = S::BQ;
+    constexpr uint32_t APB = CF_CHEB_MT * CF_CHEB_KT * S::ES;  // bytes of one A piece
     extern __shared__ __align__(1024) unsigned char csm[];
     const int f = blockIdx.y, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long c0 = (long)blockIdx.x * CF_CHEB_MT;
     const int NP = p.NP, NPs = p.NPs, nst = p.nst;
     const int nlo = blockIdx.z * NPs;  // first output row of this block
-    const uint32_t sb = cheb_stage_bytes(NPs);
+    const uint32_t sb = cheb_stage_bytes(NPs, SPLIT);
+    const uint32_t BPB = (uint32_t)NPs * CF_CHEB_KT * S::ES;  // bytes of one B piece
     uint64_t* mbar = reinterpret_cast<uint64_t*>(csm + nst * sb);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
     // TMEM columns: a power of two >= NP (and >= 32)
@@ -139,14 +190,13 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
     float xc[CF_CHEB_KT], xn[CF_CHEB_KT];
 #pragma unroll
     for (int r = 0; r < CF_CHEB_KT; ++r) xc[r] = (cin && r < p.Ny) ? __ldg(X + (long)r * p.C + cm) : 0.0f;
-    constexpr int BQ = 5;  // float4 of one image part per thread (NPs * 4 <= 5 * 128 for NPs <= 160)
+    // 16-byte units of the B pieces per K-tile: NPs rows x CPK chunks
+    const int nbu = NPs * CPK;
     int done = p.nkt;  // K-tiles whose MMAs were committed
     for (int kt = 0; kt < p.nkt; ++kt) {
         const int st = kt % nst;
-        float* Ahi = reinterpret_cast<float*>(csm + st * sb);
-        float* Alo = Ahi + CF_CHEB_MT * CF_CHEB_KT;
-        float* Bhi = Alo + CF_CHEB_MT * CF_CHEB_KT;
-        float* Blo = Bhi + NPs * CF_CHEB_KT;
+        unsigned char* Ast = csm + st * sb;
+        unsigned char* Bst = Ast + NPC * APB;
         const int k0 = kt * CF_CHEB_KT;
         // requests: X of the next K-tile, and this K-tile's rows of the images
         // (chunk ch, row n of the block's range; i = ch * NPs + n)
@@ -157,18 +207,19 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
                 xn[r] = (cin && k < p.Ny) ? __ldg(X + (long)k * p.C + cm) : 0.0f;
             }
         }
-        const float4* bh = reinterpret_cast<const float4*>(p.Bhi + (long)kt * NP * CF_CHEB_KT);
-        const float4* bl = reinterpret_cast<const float4*>(p.Blo + (long)kt * NP * CF_CHEB_KT);
-        const int nb4 = NPs * CF_CHEB_KT / 4;
-        float4 vh[BQ], vl[BQ];
-        if (nb4 <= BQ * 128) {
+        const uint4* bimg[NPC];
+#pragma unroll
+        for (int q = 0; q < NPC; ++q)
+            bimg[q] = reinterpret_cast<const uint4*>(p.B[q]) + (long)kt * NP * CPK;
+        uint4 vb[NPC][BQ];
+        if (nbu <= BQ * 128) {
 #pragma unroll
             for (int u = 0; u < BQ; ++u) {
                 const int i = tid + 128 * u;
-                if (i < nb4) {
+                if (i < nbu) {
                     const int ch = i / NPs, g = ch * NP + nlo + (i - ch * NPs);
-                    vh[u] = __ldg(bh + g);
-                    vl[u] = __ldg(bl + g);
+#pragma unroll
+                    for (int q = 0; q < NPC; ++q) vb[q][u] = __ldg(bimg[q] + g);
                 }
             }
         }
@@ -177,32 +228,52 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
             ok = mbar_wait(smem_u32(mbar + st), (uint32_t)(((kt - nst) / nst) & 1), p.spins);
             tc_fence_after();
         }
-        // A: column cm, rows k0 + 4j .. 4j+3 form one 16-byte core-matrix row
+        // A: column cm; chunk j (16 bytes) of K-tile values at (j * 128 + tid) * 16
+        if constexpr (SPLIT == 0) {
 #pragma unroll
-        for (int j = 0; j < CF_CHEB_KT / 4; ++j) {
-            float4 h = make_float4(tf32_round(xc[4 * j]), tf32_round(xc[4 * j + 1]), tf32_round(xc[4 * j + 2]),
-                                   tf32_round(xc[4 * j + 3]));
-            float4 l = make_float4(tf32_round(xc[4 * j] - h.x), tf32_round(xc[4 * j + 1] - h.y),
-                                   tf32_round(xc[4 * j + 2] - h.z), tf32_round(xc[4 * j + 3] - h.w));
-            const int o = (j * CF_CHEB_MT + tid) * 4;  // floats
-            *reinterpret_cast<float4*>(Ahi + o) = h;
-            *reinterpret_cast<float4*>(Alo + o) = l;
+            for (int j = 0; j < CF_CHEB_KT / 4; ++j) {
+                float4 h = make_float4(tf32_round(xc[4 * j]), tf32_round(xc[4 * j + 1]), tf32_round(xc[4 * j + 2]),
+                                       tf32_round(xc[4 * j + 3]));
+                float4 l = make_float4(tf32_round(xc[4 * j] - h.x), tf32_round(xc[4 * j + 1] - h.y),
+                                       tf32_round(xc[4 * j + 2] - h.z), tf32_round(xc[4 * j + 3] - h.w));
+                const uint32_t o = (j * CF_CHEB_MT + tid) * 16;
+                *reinterpret_cast<float4*>(Ast + o) = h;
+                *reinterpret_cast<float4*>(Ast + APB + o) = l;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < CF_CHEB_KT / 8; ++j) {
+                uint32_t w[3][4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    uint16_t a0, a1, a2, c0b, c1b, c2b;
+                    bf16_split3(xc[8 * j + 2 * e], a0, a1, a2);
+                    bf16_split3(xc[8 * j + 2 * e + 1], c0b, c1b, c2b);
+                    w[0][e] = (uint32_t)a0 | ((uint32_t)c0b << 16);
+                    w[1][e] = (uint32_t)a1 | ((uint32_t)c1b << 16);
+                    w[2][e] = (uint32_t)a2 | ((uint32_t)c2b << 16);
+                }
+                const uint32_t o = (j * CF_CHEB_MT + tid) * 16;
+#pragma unroll
+                for (int q = 0; q < 3; ++q)
+                    *reinterpret_cast<uint4*>(Ast + q * APB + o) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+            }
         }
-        // B: this block's NPs rows of each 4-k chunk of the K-tile's images
-        if (nb4 <= BQ * 128) {
+        // B: this block's NPs rows of each chunk of the K-tile's images
+        if (nbu <= BQ * 128) {
 #pragma unroll
             for (int u = 0; u < BQ; ++u) {
                 const int i = tid + 128 * u;
-                if (i < nb4) {
-                    reinterpret_cast<float4*>(Bhi)[i] = vh[u];
-                    reinterpret_cast<float4*>(Blo)[i] = vl[u];
+                if (i < nbu) {
+#pragma unroll
+                    for (int q = 0; q < NPC; ++q) reinterpret_cast<uint4*>(Bst + q * BPB)[i] = vb[q][u];
                 }
             }
         } else {
-            for (int i = tid; i < nb4; i += 128) {
+            for (int i = tid; i < nbu; i += 128) {
                 const int ch = i / NPs, g = ch * NP + nlo + (i - ch * NPs);
-                reinterpret_cast<float4*>(Bhi)[i] = __ldg(bh + g);
-                reinterpret_cast<float4*>(Blo)[i] = __ldg(bl + g);
+#pragma unroll
+                for (int q = 0; q < NPC; ++q) reinterpret_cast<uint4*>(Bst + q * BPB)[i] = __ldg(bimg[q] + g);
             }
         }
         fence_async_smem();
@@ -214,22 +285,36 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
         }
         if (tid == 0) {
             tc_fence_after();
-            const int ksteps = min(CF_CHEB_KT, p.Ny - k0 + 7) / 8;  // 8-degree steps holding data
+            // MMA steps of K (8 for TF32, 16 for BF16) that hold data
+            const int kstep = SPLIT ? 16 : 8;
+            const int ksteps = min(CF_CHEB_KT, p.Ny - k0 + kstep - 1) / kstep;
             for (int ks = 0; ks < ksteps; ++ks) {
                 const uint32_t aoff = ks * 2 * CF_CHEB_MT * 16, boff = ks * 2 * NPs * 16;
                 for (int n0 = 0; n0 < NPs; n0 += 256) {
                     const int N = min(256, NPs - n0);
-                    const uint32_t idesc = umma_idesc_tf32(CF_CHEB_MT, N);
                     const uint32_t d = tmem + (uint32_t)n0;
                     const uint32_t bo = boff + (n0 / 8) * 128;
-                    const uint64_t ah = umma_desc(smem_u32(Ahi) + aoff, CF_CHEB_MT * 16, 128);
-                    const uint64_t al = umma_desc(smem_u32(Alo) + aoff, CF_CHEB_MT * 16, 128);
-                    const uint64_t bhd = umma_desc(smem_u32(Bhi) + bo, NPs * 16, 128);
-                    const uint64_t bld = umma_desc(smem_u32(Blo) + bo, NPs * 16, 128);
+                    uint64_t ad[NPC], bd[NPC];
+#pragma unroll
+                    for (int q = 0; q < NPC; ++q) {
+                        ad[q] = umma_desc(smem_u32(Ast + q * APB) + aoff, CF_CHEB_MT * 16, 128);
+                        bd[q] = umma_desc(smem_u32(Bst + q * BPB) + bo, NPs * 16, 128);
+                    }
                     const uint32_t acc0 = (kt > 0 || ks > 0) ? 1u : 0u;
-                    umma_tf32(d, ah, bhd, idesc, acc0);
-                    umma_tf32(d, ah, bld, idesc, 1u);
-                    umma_tf32(d, al, bhd, idesc, 1u);
+                    if constexpr (SPLIT == 0) {
+                        const uint32_t idesc = umma_idesc_tf32(CF_CHEB_MT, N);
+                        umma_tf32(d, ad[0], bd[0], idesc, acc0);
+                        umma_tf32(d, ad[0], bd[1], idesc, 1u);
+                        umma_tf32(d, ad[1], bd[0], idesc, 1u);
+                    } else {
+                        const uint32_t idesc = umma_idesc_bf16(CF_CHEB_MT, N);
+                        umma_f16(d, ad[0], bd[0], idesc, acc0);
+                        umma_f16(d, ad[0], bd[1], idesc, 1u);
+                        umma_f16(d, ad[1], bd[0], idesc, 1u);
+                        umma_f16(d, ad[0], bd[2], idesc, 1u);
+                        umma_f16(d, ad[1], bd[1], idesc, 1u);
+                        umma_f16(d, ad[2], bd[0], idesc, 1u);
+                    }
                 }
             }
             umma_commit(smem_u32(mbar + st));

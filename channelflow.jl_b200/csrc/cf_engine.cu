@@ -251,7 +251,8 @@ struct cf_engine {
     void *nod32[6] = {}, *zp32[6] = {};
     void* coef32[6] = {};  // FP32 Chebyshev coefficients (the transforms run out of place)
     zf *d_twZf = nullptr, *d_twXf = nullptr;
-    float *d_chebF = nullptr, *d_chebI = nullptr;  // [heads | remainders]
+    unsigned char *d_chebF = nullptr, *d_chebI = nullptr;  // transform-matrix images, pieces back to back
+    int split = 0;  // tensor-core operand split: 0 TF32 head and remainder, 1 three BF16 pieces
     int chebNP = 0, chebKT = 0;
     int* d_cheberr = nullptr;
     double* d_diag = nullptr;  // diagnostics accumulators
@@ -729,11 +730,15 @@ static void drop_graph(cf_engine* h) {
 // corrections, mean mode and flux constraint, curl in coefficient space); the
 // inverse Chebyshev transform of the six fields on the tensor cores, in place.
 // ---------------------------------------------------------------------------
-static void cheb_images(int Ny, int inverse, double scale, std::vector<float>& hi, std::vector<float>& lo, int& NP,
+typedef void (*ChebKernel)(ChebParams);
+static void cheb_images(int Ny, int inverse, double scale, int split, std::vector<unsigned char>& img, int& NP,
                         int& nkt);
-static size_t cheb_smem(int NPs);
-static int cheb_stages(int NPs);
+static size_t cheb_smem(int NPs, int split);
+static int cheb_stages(int NPs, int split);
 static void cheb_dims(int Ny, int& NPs, int& nsplit, int& NP);
+static int cheb_pieces(int split);
+static size_t cheb_piece_bytes(int Ny, int split);
+static ChebKernel cheb_kernel(int split);
 
 static FftParams fft_params32(const cf_engine* h) {
     FftParams f = fft_params(h);
@@ -768,19 +773,19 @@ static int launch_cheb(cf_engine* h, int nf, bool inverse, int* count) {
     int NPs, nsplit, NPt;
     cheb_dims(h->Ny, NPs, nsplit, NPt);
     p.NPs = NPs;
-    p.nst = cheb_stages(NPs);
+    p.nst = cheb_stages(NPs, h->split);
     p.C = 2 * h->B;
     for (int f = 0; f < nf; ++f) {
         p.X[f] = static_cast<const float*>(inverse ? h->coef32[f] : h->nod32[f]);
         p.Y[f] = static_cast<float*>(inverse ? h->nod32[f] : h->coef32[f]);
     }
-    const float* img = inverse ? h->d_chebI : h->d_chebF;
-    p.Bhi = img;
-    p.Blo = img + (size_t)h->chebKT * h->chebNP * CF_CHEB_KT;
+    const unsigned char* img = inverse ? h->d_chebI : h->d_chebF;
+    const size_t pb = cheb_piece_bytes(h->Ny, h->split);
+    for (int q = 0; q < cheb_pieces(h->split); ++q) p.B[q] = img + q * pb;
     p.err = h->d_cheberr;
     p.spins = h->wait_spins;
     dim3 grid((unsigned)((p.C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nf, (unsigned)nsplit);
-    k_cheb_mma<<<grid, 128, cheb_smem(NPs), h->stream>>>(p);
+    cheb_kernel(h->split)<<<grid, 128, cheb_smem(NPs, h->split), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return CF_OK;
@@ -1016,7 +1021,7 @@ static int set_attrs(cf_engine* h) {
     if (h->mixed && h->tc) {
         int NPs, nsplit, NPt;
         cheb_dims(h->Ny, NPs, nsplit, NPt);
-        if ((rc = raise_smem_limit(k_cheb_mma, cheb_smem(NPs)))) return rc;
+        if ((rc = raise_smem_limit(cheb_kernel(h->split), cheb_smem(NPs, h->split)))) return rc;
     }
     return CF_OK;
 }
@@ -1030,12 +1035,13 @@ static int validate_and_size(cf_engine* h, const cf_config* c) {
     if (!(std::isfinite(c->nu) && c->nu > 0)) return fail(CF_E_ARG, "nu must be finite and positive");
     if (c->constraint != 0 && c->constraint != 1) return fail(CF_E_ARG, "unknown constraint kind");
     if (c->precision != CF_PRECISION_FP64 && c->precision != CF_PRECISION_MIXED &&
-        c->precision != CF_PRECISION_MIXED_TC)
+        c->precision != CF_PRECISION_MIXED_TC && c->precision != CF_PRECISION_MIXED_BF16)
         return fail(CF_E_ARG, "unknown precision mode");
-    if (c->precision == CF_PRECISION_MIXED_TC && c->Ny > 512)
+    if ((c->precision == CF_PRECISION_MIXED_TC || c->precision == CF_PRECISION_MIXED_BF16) && c->Ny > 512)
         return fail(CF_E_UNSUPPORTED, "the tensor-core Chebyshev transforms support Ny <= 512");
     h->mixed = c->precision != CF_PRECISION_FP64;
-    h->tc = c->precision == CF_PRECISION_MIXED_TC;
+    h->tc = c->precision == CF_PRECISION_MIXED_TC || c->precision == CF_PRECISION_MIXED_BF16;
+    h->split = c->precision == CF_PRECISION_MIXED_BF16 ? 1 : 0;
     if (c->form != CF_FORM_ROTATIONAL && c->form != CF_FORM_CONVECTIVE && c->form != CF_FORM_DIVERGENCE)
         return fail(CF_E_ARG, "unknown nonlinear form");
     if (h->mixed && c->form != CF_FORM_ROTATIONAL)
@@ -1248,16 +1254,13 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
         }
     }
     if (h->mixed && h->tc) {
-        std::vector<float> fhi, flo, ihi, ilo;
-        cheb_images(h->Ny, 0, 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1)), fhi, flo, h->chebNP, h->chebKT);
-        cheb_images(h->Ny, 1, 1.0, ihi, ilo, h->chebNP, h->chebKT);
-        const size_t nb = sizeof(float) * fhi.size();
-        if ((rc = dalloc(h, (void**)&h->d_chebF, 2 * nb))) return bail(rc);
-        if ((rc = dalloc(h, (void**)&h->d_chebI, 2 * nb))) return bail(rc);
-        if (cudaMemcpy(h->d_chebF, fhi.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->d_chebF + fhi.size(), flo.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->d_chebI, ihi.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->d_chebI + ihi.size(), ilo.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess)
+        std::vector<unsigned char> fimg, iimg;
+        cheb_images(h->Ny, 0, 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1)), h->split, fimg, h->chebNP, h->chebKT);
+        cheb_images(h->Ny, 1, 1.0, h->split, iimg, h->chebNP, h->chebKT);
+        if ((rc = dalloc(h, (void**)&h->d_chebF, fimg.size()))) return bail(rc);
+        if ((rc = dalloc(h, (void**)&h->d_chebI, iimg.size()))) return bail(rc);
+        if (cudaMemcpy(h->d_chebF, fimg.data(), fimg.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->d_chebI, iimg.data(), iimg.size(), cudaMemcpyHostToDevice) != cudaSuccess)
             return bail(fail(CF_E_CUDA, "upload failed"));
     }
     {
@@ -2031,14 +2034,37 @@ static void cheb_dims(int Ny, int& NPs, int& nsplit, int& NP) {
     NPs = nsplit == 1 ? n16 : (((n16 + 1) / 2 + 15) & ~15);
     NP = nsplit * NPs;
 }
-static void cheb_images(int Ny, int inverse, double scale, std::vector<float>& hi, std::vector<float>& lo, int& NP,
+// BF16 rounding to nearest even of a finite float (the IEEE rule on the
+// upper 16 bits of the FP32 pattern)
+static uint16_t host_bf16(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+static float bf16_value(uint16_t b) {
+    const uint32_t u = (uint32_t)b << 16;
+    float x;
+    std::memcpy(&x, &u, 4);
+    return x;
+}
+// Image bytes per piece and pieces of a split (0: TF32 head and remainder,
+// 1: three BF16 pieces).
+static int cheb_pieces(int split) { return split ? 3 : 2; }
+static size_t cheb_piece_bytes(int Ny, int split) {
+    int NPs, nsplit, NP;
+    cheb_dims(Ny, NPs, nsplit, NP);
+    const int nkt = (Ny + CF_CHEB_KT - 1) / CF_CHEB_KT;
+    return (size_t)nkt * NP * CF_CHEB_KT * (split ? 2 : 4);
+}
+static void cheb_images(int Ny, int inverse, double scale, int split, std::vector<unsigned char>& img, int& NP,
                         int& nkt) {
     const int P = Ny - 1;
     int NPs, nsplit;
     cheb_dims(Ny, NPs, nsplit, NP);
     nkt = (Ny + CF_CHEB_KT - 1) / CF_CHEB_KT;
-    hi.assign((size_t)nkt * NP * CF_CHEB_KT, 0.0f);
-    lo.assign(hi.size(), 0.0f);
+    const size_t pb = cheb_piece_bytes(Ny, split);
+    img.assign(pb * cheb_pieces(split), 0);
     const long double pi = 3.141592653589793238462643383279502884L;
     for (int n = 0; n < Ny; ++n)        // output degree / node
         for (int k = 0; k < Ny; ++k) {  // input node / degree
@@ -2051,12 +2077,24 @@ static void cheb_images(int Ny, int inverse, double scale, std::vector<float>& h
                 const double e = (n == 0 || n == P) ? 0.5 : 1.0, w = (k == 0 || k == P) ? 1.0 : 2.0;
                 t = scale * e * w * c;
             }
-            const float th = host_tf32((float)t);
-            const float tl = host_tf32((float)(t - (double)th));
             const int kt = k / CF_CHEB_KT, kl = k % CF_CHEB_KT;
-            const size_t idx = (size_t)kt * NP * CF_CHEB_KT + ((size_t)(kl / 4) * NP + n) * 4 + (kl % 4);
-            hi[idx] = th;
-            lo[idx] = tl;
+            if (split == 0) {
+                const float th = host_tf32((float)t);
+                const float tl = host_tf32((float)(t - (double)th));
+                const size_t idx = (size_t)kt * NP * CF_CHEB_KT + ((size_t)(kl / 4) * NP + n) * 4 + (kl % 4);
+                std::memcpy(&img[4 * idx], &th, 4);
+                std::memcpy(&img[pb + 4 * idx], &tl, 4);
+            } else {
+                const float tf = (float)t;
+                const uint16_t b0 = host_bf16(tf);
+                const float r1 = tf - bf16_value(b0);
+                const uint16_t b1 = host_bf16(r1);
+                const uint16_t b2 = host_bf16(r1 - bf16_value(b1));
+                const size_t idx = (size_t)kt * NP * CF_CHEB_KT + ((size_t)(kl / 8) * NP + n) * 8 + (kl % 8);
+                std::memcpy(&img[2 * idx], &b0, 2);
+                std::memcpy(&img[pb + 2 * idx], &b1, 2);
+                std::memcpy(&img[2 * pb + 2 * idx], &b2, 2);
+            }
         }
 }
 
@@ -2064,28 +2102,33 @@ static void cheb_images(int Ny, int inverse, double scale, std::vector<float>& h
 // shared memory, padded so that the blocks that fit on an SM (228 KB, 1 KB
 // reserved per block) also fit in its 512 TMEM columns, so no block ever waits
 // in the TMEM allocation.
-static int cheb_stages(int NPs) {
-    const size_t stage = (size_t)2 * CF_CHEB_MT * CF_CHEB_KT * 4 + (size_t)2 * NPs * CF_CHEB_KT * 4;
+static int cheb_stages(int NPs, int split) {
+    const size_t stage = cheb_stage_bytes(NPs, split);
     return 2 * stage + 64 <= (size_t)220 * 1024 ? 2 : 1;
 }
-static size_t cheb_smem(int NPs) {
-    const size_t stage = (size_t)2 * CF_CHEB_MT * CF_CHEB_KT * 4 + (size_t)2 * NPs * CF_CHEB_KT * 4;
-    const size_t tiles = cheb_stages(NPs) * stage + 64;
+static size_t cheb_smem(int NPs, int split) {
+    const size_t stage = cheb_stage_bytes(NPs, split);
+    const size_t tiles = cheb_stages(NPs, split) * stage + 64;
     const int ncols = NPs <= 32 ? 32 : (NPs <= 64 ? 64 : (NPs <= 128 ? 128 : 256));
     const size_t per_sm = 233472, maxb = 512 / ncols;
     const size_t floor_b = per_sm / (maxb + 1) - 1024 + 16;  // maxb + 1 blocks no longer fit
     return std::max(tiles, floor_b);
 }
+static ChebKernel cheb_kernel(int split) { return split ? k_cheb_mma<1> : k_cheb_mma<0>; }
 
-int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int inverse, double scale) {
+int cf_cheb_transform_split(const float* X, float* Y, int Ny, long C, int nfields, int inverse, double scale,
+                            int split) {
     if (!X || !Y) return fail(CF_E_ARG, "null argument");
     if (Ny < 2 || Ny > 512) return fail(CF_E_UNSUPPORTED, "Chebyshev transform needs 2 <= Ny <= 512");
     if (C < 1 || nfields < 1 || nfields > CF_CHEB_MAXF) return fail(CF_E_ARG, "need C >= 1 and 1..6 fields");
-    std::vector<float> hi, lo;
+    if (split != 0 && split != 1) return fail(CF_E_ARG, "split must be 0 (TF32) or 1 (BF16)");
+    std::vector<unsigned char> img;
     int NP, nkt;
-    cheb_images(Ny, inverse, scale, hi, lo, NP, nkt);
+    cheb_images(Ny, inverse, scale, split, img, NP, nkt);
+    const size_t pb = cheb_piece_bytes(Ny, split);
     const size_t fb = sizeof(float) * (size_t)Ny * C;
-    float *dX = nullptr, *dY = nullptr, *dB = nullptr;
+    float *dX = nullptr, *dY = nullptr;
+    unsigned char* dB = nullptr;
     int* derr = nullptr;
     int rc = CF_OK;
     auto cleanup = [&]() {
@@ -2095,39 +2138,37 @@ int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int
         cudaFree(derr);
     };
     if (cudaMalloc(&dX, fb * nfields) != cudaSuccess || cudaMalloc(&dY, fb * nfields) != cudaSuccess ||
-        cudaMalloc(&dB, sizeof(float) * hi.size() * 2) != cudaSuccess || cudaMalloc(&derr, sizeof(int)) != cudaSuccess) {
+        cudaMalloc(&dB, img.size()) != cudaSuccess || cudaMalloc(&derr, sizeof(int)) != cudaSuccess) {
         cleanup();
         return fail(CF_E_NOMEM, "device allocation failed");
     }
     do {
         if (cudaMemcpy(dX, X, fb * nfields, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(dB, hi.data(), sizeof(float) * hi.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(dB + hi.size(), lo.data(), sizeof(float) * lo.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dB, img.data(), img.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
             cudaMemset(derr, 0, sizeof(int)) != cudaSuccess || cudaMemset(dY, 0, fb * nfields) != cudaSuccess) {
             rc = fail(CF_E_CUDA, "upload failed");
             break;
         }
         int NPs, nsplit, NPt;
         cheb_dims(Ny, NPs, nsplit, NPt);
-        if ((rc = raise_smem_limit(k_cheb_mma, cheb_smem(NPs)))) break;
+        if ((rc = raise_smem_limit(cheb_kernel(split), cheb_smem(NPs, split)))) break;
         ChebParams p;
         std::memset(&p, 0, sizeof(p));
         p.Ny = Ny;
         p.NP = NP;
         p.nkt = nkt;
         p.NPs = NPs;
-        p.nst = cheb_stages(NPs);
+        p.nst = cheb_stages(NPs, split);
         p.C = C;
         for (int f = 0; f < nfields; ++f) {
             p.X[f] = dX + (size_t)f * Ny * C;
             p.Y[f] = dY + (size_t)f * Ny * C;
         }
-        p.Bhi = dB;
-        p.Blo = dB + hi.size();
+        for (int q = 0; q < cheb_pieces(split); ++q) p.B[q] = dB + q * pb;
         p.err = derr;
         p.spins = CF_WAIT_SPINS;
         dim3 grid((unsigned)((C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nfields, (unsigned)nsplit);
-        k_cheb_mma<<<grid, 128, cheb_smem(NPs)>>>(p);
+        cheb_kernel(split)<<<grid, 128, cheb_smem(NPs, split)>>>(p);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) {
@@ -2144,4 +2185,7 @@ int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int
     } while (0);
     cleanup();
     return rc;
+}
+int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int inverse, double scale) {
+    return cf_cheb_transform_split(X, Y, Ny, C, nfields, inverse, scale, 0);
 }

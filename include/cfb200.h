@@ -49,10 +49,14 @@ extern "C" {
  * influence-matrix and tau corrections, mean mode and flux constraint stay
  * FP64, as does the state.  MIXED_TC: as MIXED with the Chebyshev transforms
  * as tensor-core contractions (TF32 heads and remainders, FP32 accumulation)
- * between FP32 coefficient and nodal fields; Ny <= 512. */
+ * between FP32 coefficient and nodal fields; Ny <= 512.  MIXED_BF16: as
+ * MIXED_TC with the contractions on the BF16 tensor cores, each operand
+ * split into three BF16 pieces (24 significant bits) and the six products of
+ * order >= 2^-16 accumulated in FP32. */
 #define CF_PRECISION_FP64 0
 #define CF_PRECISION_MIXED 1
 #define CF_PRECISION_MIXED_TC 2
+#define CF_PRECISION_MIXED_BF16 3
 
 /* Nonlinear form of NonLinearTerm(...; form) (src/nonlinear.jl:11-17, 113-199).
  * ROTATIONAL: u x curl(u) with the modified pressure (the default);
@@ -134,6 +138,11 @@ int cf_nonlinear(cf_handle* h, const double* U, double* N);
  * ffts.jl:254-269).  TF32 operands split in heads and remainders (three
  * products), FP32 accumulation: ~FP32 accuracy.  2 <= Ny <= 512, nfields <= 6. */
 int cf_cheb_transform(const float* X, float* Y, int Ny, long C, int nfields, int inverse, double scale);
+/* The same with a chosen operand split: 0 TF32 heads and remainders (as
+ * cf_cheb_transform), 1 three BF16 pieces with six BF16 products; both
+ * accumulate in FP32 and reach ~FP32 accuracy. */
+int cf_cheb_transform_split(const float* X, float* Y, int Ny, long C, int nfields, int inverse, double scale,
+                            int split);
 
 /* ---- Ensembles: many independent channels advanced together ----------------
  * The reference advances one channel per step! call (cnrk2.jl:149-207); an
