@@ -50,7 +50,8 @@ EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_g
            "cf_stream", "cf_last_error", "cf_step_profiled", "cf_nonlinear_noalloc", "cf_create_batch",
            "cf_destroy_batch", "cf_batch_size", "cf_batch_instance", "cf_step_batch",
            "cf_batch_last_launch_count", "cf_batch_stream", "cf_cheb_transform", "cf_step_dt",
-           "cf_step_host", "cf_power_input", "cf_device_bytes", "cf_set_wait_limit", "cf_cheb_transform_split"]
+           "cf_step_host", "cf_power_input", "cf_device_bytes", "cf_set_wait_limit", "cf_cheb_transform_split",
+           "cf_batch_schedule"]
 
 # return codes of cfb200.h
 CF_E_ARG, CF_E_SINGULAR, CF_E_NOMEM, CF_E_CUDA, CF_E_UNSUPPORTED, CF_E_NONFINITE = -1, -2, -3, -4, -5, -6
@@ -90,6 +91,7 @@ def lib():
         L.cf_batch_last_launch_count.argtypes = [ctypes.c_void_p]
         L.cf_batch_stream.argtypes = [ctypes.c_void_p]
         L.cf_batch_stream.restype = ctypes.c_void_p
+        L.cf_batch_schedule.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
         L.cf_project.argtypes = [ctypes.c_void_p, _D]
         L.cf_pressure.argtypes = [ctypes.c_void_p, _D, _D]
         L.cf_random_state.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_double, ctypes.c_int,
@@ -389,6 +391,14 @@ class Ensemble:
 
     def launches(self):
         return lib().cf_batch_last_launch_count(self._h)
+
+    def schedule(self):
+        """The autotuner's choice per size class (and the candidates' timings)."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        n = lib().cf_batch_schedule(self._h, buf, len(buf))
+        if n < 0:
+            _check(n)
+        return buf.value.decode()
 
     def close(self):
         if getattr(self, "_h", None) and _lib is not None:

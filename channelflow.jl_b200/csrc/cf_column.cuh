@@ -86,8 +86,20 @@ CF_DEV zd warp_excl_z(zd inc, int lane) {
     return lane == 0 ? zzero() : o;
 }
 
+// Elements per lane of a chain of cnt elements scanned by one warp (odd),
+// and its largest value for the chains of a compile-time length PL (chains
+// of at most (PL/2 + 1) elements): the loops over a lane's run are unrolled
+// to that bound, so the run's loads issue together and its values stay in
+// registers between the two passes of a scan.
+CF_DEV int run_len(int cnt) { return ((cnt + 31) >> 5) | 1; }
+template <int PL>
+__host__ __device__ constexpr int run_max() {
+    return PL ? ((((PL >> 1) + 1) + 31) >> 5) | 1 : 0;
+}
+
 // b = D a  (b != a).  Warp q writes the degrees of parity q of b from the
 // degrees of parity 1-q of a; b_P = 0.
+template <int PL>
 CF_DEV void col_diff_body(const zd* a, zd* b, const Team& t) {
     const int P = t.P, hs = t.hs, q = t.q, lane = t.lane;
     const int pin = 1 - q;                 // parity of the input chain
@@ -95,31 +107,57 @@ CF_DEV void col_diff_body(const zd* a, zd* b, const Team& t) {
     const int cnt = (top - pin) / 2 + 1;
     const zd* ah = a + pin * hs;           // a_m at ah[m >> 1]
     zd* bh = b + q * hs;                   // b_n at bh[n >> 1]
-    const int E = ((cnt + 31) >> 5) | 1;
+    const int E = run_len(cnt);
     const int i0 = lane * E;
-    zd tot = zzero();
-    for (int s = 0; s < E; ++s) {
-        const int i = i0 + s;
-        const int m = top - 2 * i;
-        if (i < cnt && m >= 1) tot = zaxpy(tot, (double)m, ah[m >> 1]);
-    }
-    zd run = warp_excl_z(warp_scan_z(tot, lane), lane);
-    for (int s = 0; s < E; ++s) {
-        const int i = i0 + s;
-        const int m = top - 2 * i;
-        if (i < cnt && m >= 1) {
-            run = zaxpy(run, (double)m, ah[m >> 1]);
-            bh[(m - 1) >> 1] = (m == 1) ? run : zscale(run, 2.0);
+    if constexpr (PL != 0) {
+        constexpr int EM = run_max<PL>();
+        zd v[EM];
+#pragma unroll
+        for (int s = 0; s < EM; ++s) {
+            const int i = i0 + s, m = top - 2 * i;
+            v[s] = (s < E && i < cnt && m >= 1) ? ah[m >> 1] : zzero();
+        }
+        zd tot = zzero();
+#pragma unroll
+        for (int s = 0; s < EM; ++s) {
+            const int i = i0 + s, m = top - 2 * i;
+            if (s < E && i < cnt && m >= 1) tot = zaxpy(tot, (double)m, v[s]);
+        }
+        zd run = warp_excl_z(warp_scan_z(tot, lane), lane);
+#pragma unroll
+        for (int s = 0; s < EM; ++s) {
+            const int i = i0 + s, m = top - 2 * i;
+            if (s < E && i < cnt && m >= 1) {
+                run = zaxpy(run, (double)m, v[s]);
+                bh[(m - 1) >> 1] = (m == 1) ? run : zscale(run, 2.0);
+            }
+        }
+    } else {
+        zd tot = zzero();
+        for (int s = 0; s < E; ++s) {
+            const int i = i0 + s;
+            const int m = top - 2 * i;
+            if (i < cnt && m >= 1) tot = zaxpy(tot, (double)m, ah[m >> 1]);
+        }
+        zd run = warp_excl_z(warp_scan_z(tot, lane), lane);
+        for (int s = 0; s < E; ++s) {
+            const int i = i0 + s;
+            const int m = top - 2 * i;
+            if (i < cnt && m >= 1) {
+                run = zaxpy(run, (double)m, ah[m >> 1]);
+                bh[(m - 1) >> 1] = (m == 1) ? run : zscale(run, 2.0);
+            }
         }
     }
     if (q == 0 && lane == 0) bh[P >> 1] = zzero();
     tsync(t);
 }
-CF_DEV_NOINLINE void col_diff_ool(const zd* a, zd* b, const Team t) { col_diff_body(a, b, t); }
+template <int PL>
+CF_DEV_NOINLINE void col_diff_ool(const zd* a, zd* b, const Team t) { col_diff_body<PL>(a, b, t); }
 template <int PL>
 CF_DEV void col_diff(const zd* a, zd* b, const Team& t) {
-    if constexpr (col_ool<PL>()) col_diff_ool(a, b, t);
-    else col_diff_body(a, b, t);
+    if constexpr (col_ool<PL>()) col_diff_ool<PL>(a, b, t);
+    else col_diff_body<PL>(a, b, t);
 }
 
 // The three elimination factor rows of a column (alpha, invden, W: src,
@@ -165,19 +203,116 @@ CF_DEV zd helm_g(const zd* fh, const double* __restrict__ gt, int n, int P) {
     return v;
 }
 
+// The tau Helmholtz solve below for a compile-time length: the same
+// arithmetic in the same order, with each lane's run unrolled and its
+// intermediate terms (g_n invden_n and the map factors of the backward sweep,
+// beta and alpha of the forward sweep) kept in registers between the two
+// passes of each sweep instead of being loaded again.
+template <int PL>
+CF_DEV void col_helm_runs(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
+                          const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
+                          const Team& t, int top, int cnt, int E, int i0) {
+    constexpr int EM = run_max<PL>();
+    const int P = t.P, Ny = P + 1, q = t.q, lane = t.lane, hs = t.hs;
+    zd* xh = x + q * hs;
+    zd* sh = scr + q * hs;
+    const double* ah = alpha + q * hs;
+    const double* ih = invden + q * hs;
+    const double* wh = W + q * hs;
+    // backward sweep beta_n = invden_n (g_n - u_n beta_{n+2}) as maps G + M x
+    zd g[EM];
+    double Ms[EM];
+#pragma unroll
+    for (int s = 0; s < EM; ++s) {
+        const int i = i0 + s;
+        g[s] = zzero();
+        Ms[s] = 1.0;
+        if (s < E && i < cnt) {
+            const int n = top - 2 * i;
+            const double id = ih[n >> 1];
+            Ms[s] = th1 * __ldg(gt + 2 * Ny + n) * id;
+            g[s] = zscale(helm_g(xh, gt, n, P), id);
+        }
+    }
+    double Mc = 1.0;
+    zd Gc = zzero();
+#pragma unroll
+    for (int s = 0; s < EM; ++s)
+        if (s < E && i0 + s < cnt) {
+            Gc = zaxpy(g[s], Ms[s], Gc);
+            Mc *= Ms[s];
+        }
+    warp_scan_affine(Mc, Gc, lane);
+    zd xv = warp_excl_z(Gc, lane);
+    zd sw = zzero();
+#pragma unroll
+    for (int s = 0; s < EM; ++s) {
+        const int i = i0 + s;
+        if (s < E && i < cnt) {
+            const int n = top - 2 * i;
+            xv = zaxpy(g[s], Ms[s], xv);
+            sh[n >> 1] = xv;
+            sw = zaxpy(sw, wh[n >> 1], xv);
+        }
+    }
+    sw = warp_sum_z(sw);
+    const zd a0 = zscale(zsub(q ? bc1 : bc0, sw), 1.0 / (q ? SA1 : SA0));
+    __syncwarp();
+    // forward sweep a_n = alpha_n a_{n-2} + beta_n, chain n = q+2, q+4, ..., top
+    zd bv[EM];
+    double av[EM];
+#pragma unroll
+    for (int s = 0; s < EM; ++s) {
+        const int jj = i0 + s;
+        bv[s] = zzero();
+        av[s] = 1.0;
+        if (s < E && jj < cnt) {
+            bv[s] = sh[jj + 1];
+            av[s] = ah[jj + 1];
+        }
+    }
+    Mc = 1.0;
+    Gc = zzero();
+#pragma unroll
+    for (int s = 0; s < EM; ++s)
+        if (s < E && i0 + s < cnt) {
+            Gc = zaxpy(bv[s], av[s], Gc);
+            Mc *= av[s];
+        }
+    warp_scan_affine(Mc, Gc, lane);
+    const double Me = __shfl_up_sync(0xffffffffu, Mc, 1);
+    const zd Ge = warp_excl_z(Gc, lane);
+    xv = (lane == 0) ? a0 : zaxpy(Ge, Me, a0);
+#pragma unroll
+    for (int s = 0; s < EM; ++s) {
+        const int jj = i0 + s;
+        if (s < E && jj < cnt) {
+            xv = zaxpy(bv[s], av[s], xv);
+            xh[jj + 1] = xv;
+        }
+    }
+    if (lane == 0) xh[0] = a0;
+    tsync(t);
+}
+
 // Tau Helmholtz solve: x holds f on entry and a on exit; scr (distinct) holds
 // the intermediate beta.  alpha, invden, W are the column's elimination
 // factors in the parity layout (shared memory, staged by col_stage_factors);
 // SA0/SA1 and bc0/bc1 are the wall-row sums and data of the two parities.
 // Warp q solves the parity-q system alone.
+template <int PL>
 CF_DEV void col_helm_body(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
                           const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
                           const Team& t) {
     const int P = t.P, Ny = P + 1, q = t.q, lane = t.lane, hs = t.hs;
     const int top = q ? P - 1 : P;
     const int cnt = (top - q) / 2;  // backward chain n = top, top-2, ..., q+2
-    const int E = ((cnt + 31) >> 5) | 1;
+    const int E = run_len(cnt);
     const int i0 = lane * E;
+    if constexpr (PL != 0) {
+        col_helm_runs<PL>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t, top, cnt, E, i0);
+        return;
+    }
     zd* xh = x + q * hs;
     zd* sh = scr + q * hs;
     const double* ah = alpha + q * hs;
@@ -240,17 +375,18 @@ CF_DEV void col_helm_body(zd* x, zd* scr, const double* alpha, const double* inv
     if (lane == 0) xh[0] = a0;
     tsync(t);
 }
+template <int PL>
 CF_DEV_NOINLINE void col_helm_ool(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
                                   const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0,
                                   zd bc1, const Team t) {
-    col_helm_body(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
+    col_helm_body<PL>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
 }
 template <int PL>
 CF_DEV void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
                      const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
                      const Team& t) {
-    if constexpr (col_ool<PL>()) col_helm_ool(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
-    else col_helm_body(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
+    if constexpr (col_ool<PL>()) col_helm_ool<PL>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
+    else col_helm_body<PL>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
 }
 
 // DCT-I (REDFT00) of complex x[0..P] in place (parity layout).  z and z2 are
@@ -311,20 +447,43 @@ CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const F
         // odd outputs X_{2m+1}, m = 0..H-1: X_1 plus prefix sums of
         // i (Z_m - Z_{P-m}), in runs of E (odd) consecutive m per lane
         const int lane = t.lane;
-        const int E = ((H + 31) >> 5) | 1;
+        const int E = run_len(H);
         const int m0 = lane * E;
-        zd tot = zzero();
-        for (int s = 0; s < E; ++s) {
-            const int m = m0 + s;
-            if (m >= 1 && m < H) tot = zadd(tot, zmuli(zsub(Z[fpos(m)], Z[fpos(P - m)])));
-        }
-        zd run = zadd(x1, warp_excl_z(warp_scan_z(tot, lane), lane));
         zd* xo = x + hs;  // X_{2m+1} at xo[m]
-        for (int s = 0; s < E; ++s) {
-            const int m = m0 + s;
-            if (m < H) {
-                if (m >= 1) run = zadd(run, zmuli(zsub(Z[fpos(m)], Z[fpos(P - m)])));
-                xo[m] = run;
+        if constexpr (PL != 0) {
+            constexpr int EM = run_max<PL>();
+            zd d[EM];
+#pragma unroll
+            for (int s = 0; s < EM; ++s) {
+                const int m = m0 + s;
+                d[s] = (s < E && m >= 1 && m < H) ? zmuli(zsub(Z[fpos(m)], Z[fpos(P - m)])) : zzero();
+            }
+            zd tot = zzero();
+#pragma unroll
+            for (int s = 0; s < EM; ++s)
+                if (s < E && m0 + s >= 1 && m0 + s < H) tot = zadd(tot, d[s]);
+            zd run = zadd(x1, warp_excl_z(warp_scan_z(tot, lane), lane));
+#pragma unroll
+            for (int s = 0; s < EM; ++s) {
+                const int m = m0 + s;
+                if (s < E && m < H) {
+                    if (m >= 1) run = zadd(run, d[s]);
+                    xo[m] = run;
+                }
+            }
+        } else {
+            zd tot = zzero();
+            for (int s = 0; s < E; ++s) {
+                const int m = m0 + s;
+                if (m >= 1 && m < H) tot = zadd(tot, zmuli(zsub(Z[fpos(m)], Z[fpos(P - m)])));
+            }
+            zd run = zadd(x1, warp_excl_z(warp_scan_z(tot, lane), lane));
+            for (int s = 0; s < E; ++s) {
+                const int m = m0 + s;
+                if (m < H) {
+                    if (m >= 1) run = zadd(run, zmuli(zsub(Z[fpos(m)], Z[fpos(P - m)])));
+                    xo[m] = run;
+                }
             }
         }
     } else {
@@ -459,26 +618,35 @@ CF_DEV void col_redft00_pair(zd* xa, zd* xb, zd* z, int bs, const zd* __restrict
     else col_team_fft2_body<PL>(z, bs, pl, t);
     if (t.q == 1) {
         const int lane = t.lane;
-        const int E = ((H + 31) >> 5) | 1;
+        const int E = run_len(H);
         const int m0 = lane * E;
-        zd ta = zzero(), tb = zzero();
-        for (int s = 0; s < E; ++s) {
+        constexpr int EM = run_max<PL>();
+        zd da[EM], db[EM];
+#pragma unroll
+        for (int s = 0; s < EM; ++s) {
             const int m = m0 + s;
-            if (m >= 1 && m < H) {
-                ta = zadd(ta, zmuli(zsub(z[fpos(m)], z[fpos(P - m)])));
-                tb = zadd(tb, zmuli(zsub(zb[fpos(m)], zb[fpos(P - m)])));
-            }
+            const bool in = s < E && m >= 1 && m < H;
+            da[s] = in ? zmuli(zsub(z[fpos(m)], z[fpos(P - m)])) : zzero();
+            db[s] = in ? zmuli(zsub(zb[fpos(m)], zb[fpos(P - m)])) : zzero();
         }
+        zd ta = zzero(), tb = zzero();
+#pragma unroll
+        for (int s = 0; s < EM; ++s)
+            if (s < E && m0 + s >= 1 && m0 + s < H) {
+                ta = zadd(ta, da[s]);
+                tb = zadd(tb, db[s]);
+            }
         zd ra = zadd(x1a, warp_excl_z(warp_scan_z(ta, lane), lane));
         zd rb = zadd(x1b, warp_excl_z(warp_scan_z(tb, lane), lane));
         zd* xoa = xa + hs;
         zd* xob = xb + hs;
-        for (int s = 0; s < E; ++s) {
+#pragma unroll
+        for (int s = 0; s < EM; ++s) {
             const int m = m0 + s;
-            if (m < H) {
+            if (s < E && m < H) {
                 if (m >= 1) {
-                    ra = zadd(ra, zmuli(zsub(z[fpos(m)], z[fpos(P - m)])));
-                    rb = zadd(rb, zmuli(zsub(zb[fpos(m)], zb[fpos(P - m)])));
+                    ra = zadd(ra, da[s]);
+                    rb = zadd(rb, db[s]);
                 }
                 xoa[m] = ra;
                 xob[m] = rb;

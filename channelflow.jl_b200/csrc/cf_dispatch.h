@@ -18,7 +18,15 @@ static_assert(CF_NCOL == 1 || CF_NCOL == 2, "column teams use named barriers 1 a
 typedef void (*ColKernel)(ColParams);
 typedef void (*FftKernel)(FftParams);
 typedef void (*DiagKernel)(ColParams, double*, double*);
-typedef void (*ColBatchKernel)(const ColParams*);
+typedef void (*ColBatchKernel)(const ColParams*, int, int, unsigned*);
+// Variants of the batched column kernel the ensemble autotuner chooses from:
+// (columns per block, blocks per SM of the register bound).  Variant 0 is the
+// single-instance kernel's shape; 1-5 exist for P <= 128 (fewer registers,
+// more blocks per SM).
+#define CF_COL_BATCH_VARIANTS 6
+static constexpr int kColBatchNcol[CF_COL_BATCH_VARIANTS] = {CF_NCOL, 2, 2, 1, 1, 1};
+static constexpr int kColBatchMinb[CF_COL_BATCH_VARIANTS] = {0, 6, 8, 8, 12, 16};
+__host__ __device__ constexpr bool col_batch_variants(int P) { return P != 0 && P <= 128; }
 typedef void (*FftBatchKernel)(const FftParams*);
 typedef void (*FftTmaKernel)(FftParams, FftMaps);
 
@@ -28,6 +36,9 @@ enum {
     KC_STAGE_MXD, KC_PREP_MXD, KC_COUNT
 };
 enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_XPASS_CONV, KF_XPASS_DIV, KF_XPASS2, KF_XPASS_IP, KF_XPASS_CONV_IP, KF_XPASS_DIV_IP, KF_COUNT };
+// rows per block of the batched x-pass variants (KF_XPASS: 2; the others for
+// short rows, chosen by the ensemble autotuner)
+enum { KF_XPASS_R4 = KF_COUNT, KF_XPASS_R8, KF_XPASS_R16 };
 
 // defined for P in CF_COL_LENGTHS and 0 (cf_inst_col.cu)
 template <int P>
@@ -35,7 +46,7 @@ ColKernel col_kernel_for(int which);
 template <int P>
 DiagKernel diag_kernel_for();
 template <int P>
-ColBatchKernel col_batch_kernel_for();
+ColBatchKernel col_batch_kernel_for(int variant);
 // defined for L in CF_STATIC_FFT_LENGTHS and 0 (cf_inst_fft.cu); f32: the
 // FP32 transforms of the mixed-precision form
 template <int L>

@@ -525,8 +525,8 @@ static int build_neumann(cf_engine* h) {
 static int col_stride(const cf_engine* h) { return 2 * col_half_stride(h->P) + 2; }
 static int col_zstride(const cf_engine* h) { return std::max(2 * col_half_stride(h->P), fft_bufsz(h->P)); }
 // per column: 6 vectors, 2 transform buffers and 4 complex of team scratch
-static size_t col_smem(const cf_engine* h) {
-    return ((size_t)CF_NCOL * (6 * col_stride(h) + 2 * col_zstride(h)) + 4 * CF_NCOL) * sizeof(zd);
+static size_t col_smem(const cf_engine* h, int ncol = CF_NCOL) {
+    return ((size_t)ncol * (6 * col_stride(h) + 2 * col_zstride(h)) + 4 * ncol) * sizeof(zd);
 }
 
 static ColParams col_params(const cf_engine* h) {
@@ -1787,13 +1787,24 @@ static void host_synth(const cf_engine* h, uint64_t seed, double amp, int shape,
 // shared memory), and the classes run as parallel branches of one CUDA graph
 // per step: 12 launches per class per step, whatever the instance count.
 // ---------------------------------------------------------------------------
-static ColBatchKernel col_batch_kernel(int P) {
+static ColBatchKernel col_batch_kernel(int P, int variant) {
     switch (P) {
 #define CF_CASE(N) \
-    case N: return col_batch_kernel_for<N>();
+    case N: return col_batch_kernel_for<N>(variant);
         CF_COL_LENGTHS(CF_CASE)
 #undef CF_CASE
-        default: return col_batch_kernel_for<0>();
+        default: return col_batch_kernel_for<0>(variant);
+    }
+}
+// the variants that exist for a class's Chebyshev length (the compile-time
+// lengths up to 128 have all of them)
+static int col_batch_nvariants(int P) {
+    switch (P) {
+#define CF_CASE(N) \
+    case N: return col_batch_variants(N) ? CF_COL_BATCH_VARIANTS : 1;
+        CF_COL_LENGTHS(CF_CASE)
+#undef CF_CASE
+        default: return 1;
     }
 }
 static FftBatchKernel fft_batch_kernel(int which, int L) {
@@ -1809,6 +1820,18 @@ static FftBatchKernel fft_batch_kernel(int which, int L) {
 struct BatchClass {
     int Nx = 0, Ny = 0, Nz = 0;
     std::vector<int> members;
+    // the column kernel's schedule, chosen by autotune_batch: variant (columns
+    // per block, register bound) and persistent launch (grid pgrid) or one
+    // block per item; counters of the persistent launches (one per stage)
+    int var = 0;
+    bool persist = false;
+    unsigned pgrid = 0;
+    unsigned* d_counter = nullptr;
+    double step_ms = 0.0;
+    // the periodic kernels' shapes, also chosen by autotune_batch: columns
+    // per z block (0: the instances' own) and rows per x-pass block
+    int tkz = 0;
+    int xkind = KF_XPASS;
     FftParams* d_fft = nullptr;
     ColParams* d_col[3] = {nullptr, nullptr, nullptr};
     std::vector<FftParams> h_fft;
@@ -1820,6 +1843,7 @@ struct BatchClass {
 struct cf_batch {
     std::vector<cf_engine*> inst;
     std::vector<BatchClass> cls;
+    std::string schedule;  // what the autotuner measured and chose
     cudaStream_t stream = nullptr;
     cudaEvent_t fork = nullptr, done = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -1849,6 +1873,22 @@ static int batch_alloc(cf_batch* b, void** p, size_t bytes) {
     return CF_OK;
 }
 
+// The batched periodic kernels' shapes of a class: columns per z block
+// (their transform stride and shared memory follow from it) and rows per
+// x-pass block.
+static int class_tkz(const cf_batch* b, const BatchClass& c) { return c.tkz ? c.tkz : b->inst[c.members[0]]->tkz; }
+static int zbs_of(int Nzp, int tkz) { return fft_bufsz(Nzp) + (8 / tkz) % 8; }
+static size_t class_zsmem(const cf_batch* b, const BatchClass& c) {
+    const int tkz = class_tkz(b, c);
+    return (size_t)2 * tkz * zbs_of(b->inst[c.members[0]]->Nzp, tkz) * sizeof(zd);
+}
+static int xpass_rows(int xkind) {
+    return xkind == KF_XPASS_R4 ? 4 : (xkind == KF_XPASS_R8 ? 8 : (xkind == KF_XPASS_R16 ? 16 : 2));
+}
+static size_t class_xsmem(const cf_batch* b, const BatchClass& c) {
+    return (size_t)6 * xpass_rows(c.xkind) * xbs(b->inst[c.members[0]]) * sizeof(zd);
+}
+
 // Parameters of every instance (host copies refreshed from the instances,
 // so constraint changes made through an instance handle take effect).
 static int batch_upload(cf_batch* b) {
@@ -1856,6 +1896,9 @@ static int batch_upload(cf_batch* b) {
         for (size_t k = 0; k < c.members.size(); ++k) {
             cf_engine* h = b->inst[c.members[k]];
             c.h_fft[k] = fft_params(h);
+            const int tkz = class_tkz(b, c);
+            c.h_fft[k].tks = ilog2(tkz);
+            c.h_fft[k].bsz = zbs_of(h->Nzp, tkz);
             for (int j = 0; j < 3; ++j) c.h_col[j][k] = stage_col_params(h, j);
         }
         CU(cudaMemcpyAsync(c.d_fft, c.h_fft.data(), sizeof(FftParams) * c.h_fft.size(), cudaMemcpyHostToDevice,
@@ -1867,6 +1910,8 @@ static int batch_upload(cf_batch* b) {
     CU(cudaStreamSynchronize(b->stream));
     return CF_OK;
 }
+
+static int autotune_batch(cf_batch* b);
 
 int cf_create_batch(const cf_config* cfgs, int n, cf_batch** out) {
     if (!cfgs || n <= 0 || !out) return fail(CF_E_ARG, "null argument or empty ensemble");
@@ -1916,9 +1961,18 @@ int cf_create_batch(const cf_config* cfgs, int n, cf_batch** out) {
             if ((rc = batch_alloc(b, (void**)&c.d_col[j], sizeof(ColParams) * m))) return bail(rc);
         }
         const size_t smz = zsmem(r), smx = xsmem(r);
-        if ((rc = raise_smem_limit(col_batch_kernel(r->P), col_smem(r))) ||
-            (rc = raise_smem_limit(fft_batch_kernel(KF_ZINV, r->Nzp), smz)) ||
-            (rc = raise_smem_limit(fft_batch_kernel(KF_ZFWD, r->Nzp), smz)) ||
+        for (int v = 0; v < col_batch_nvariants(r->P); ++v)
+            if ((rc = raise_smem_limit(col_batch_kernel(r->P, v), col_smem(r, kColBatchNcol[v])))) return bail(rc);
+        if ((rc = batch_alloc(b, (void**)&c.d_counter, 3 * sizeof(unsigned)))) return bail(rc);
+        // the largest shapes the autotuner may choose
+        const size_t smz_max = std::max(smz, (size_t)2 * 32 * zbs_of(r->Nzp, 32) * sizeof(zd));
+        for (int xk : {KF_XPASS_R4, KF_XPASS_R8, KF_XPASS_R16}) {
+            const size_t need = (size_t)6 * xpass_rows(xk) * xbs(r) * sizeof(zd);
+            if (need <= (size_t)200 * 1024 && (rc = raise_smem_limit(fft_batch_kernel(xk, r->Nxp), need)))
+                return bail(rc);
+        }
+        if ((rc = raise_smem_limit(fft_batch_kernel(KF_ZINV, r->Nzp), std::min(smz_max, (size_t)200 * 1024))) ||
+            (rc = raise_smem_limit(fft_batch_kernel(KF_ZFWD, r->Nzp), std::min(smz_max, (size_t)200 * 1024))) ||
             (rc = raise_smem_limit(fft_batch_kernel(KF_XPASS, r->Nxp), smx)))
             return bail(rc);
         if (cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1927,21 +1981,194 @@ int cf_create_batch(const cf_config* cfgs, int n, cf_batch** out) {
     }
     int rc = batch_upload(b);
     if (rc) return bail(rc);
+    if ((rc = autotune_batch(b))) return bail(rc);
     *out = b;
     return CF_OK;
 }
 
 // The four launches of stage j for one size class on stream s.
-static int launch_class_stage(const cf_batch* b, const BatchClass& c, int j, cudaStream_t s) {
+// `which` selects the kernels (1 z-inverse, 2 x-pass, 4 z-forward, 8 column;
+// 15: the whole stage, as the graph launches it).
+static int launch_class_stage(const cf_batch* b, const BatchClass& c, int j, cudaStream_t s, int which = 15) {
     const cf_engine* r = b->inst[c.members[0]];
     const unsigned m = (unsigned)c.members.size();
-    const size_t smz = zsmem(r), smx = xsmem(r);
-    const unsigned gzx = (unsigned)((r->Nxh + r->tkz - 1) / r->tkz);
-    fft_batch_kernel(KF_ZINV, r->Nzp)<<<dim3(gzx, r->Ny, 6 * m), 256, smz, s>>>(c.d_fft);
-    fft_batch_kernel(KF_XPASS, r->Nxp)<<<dim3((r->Nzp + 1) / 2, r->Ny, m), 256, smx, s>>>(c.d_fft);
-    fft_batch_kernel(KF_ZFWD, r->Nzp)<<<dim3(gzx, r->Ny, 3 * m), 256, smz, s>>>(c.d_fft);
-    col_batch_kernel(r->P)<<<dim3(col_blocks(r), m), CF_NCOL * CF_TEAM, col_smem(r), s>>>(c.d_col[j]);
+    if (which & 1) {
+        const int tkz = class_tkz(b, c);
+        const unsigned gzx = (unsigned)((r->Nxh + tkz - 1) / tkz);
+        fft_batch_kernel(KF_ZINV, r->Nzp)<<<dim3(gzx, r->Ny, 6 * m), 256, class_zsmem(b, c), s>>>(c.d_fft);
+    }
+    if (which & 2) {
+        const int rows = xpass_rows(c.xkind);
+        fft_batch_kernel(c.xkind, r->Nxp)<<<dim3((r->Nzp + rows - 1) / rows, r->Ny, m), 256, class_xsmem(b, c), s>>>(
+            c.d_fft);
+    }
+    if (which & 4) {
+        const int tkz = class_tkz(b, c);
+        const unsigned gzx = (unsigned)((r->Nxh + tkz - 1) / tkz);
+        fft_batch_kernel(KF_ZFWD, r->Nzp)<<<dim3(gzx, r->Ny, 3 * m), 256, class_zsmem(b, c), s>>>(c.d_fft);
+    }
+    if (!(which & 8)) {
+        CU(cudaGetLastError());
+        return CF_OK;
+    }
+    const int ncol = kColBatchNcol[c.var];
+    const int nblk = (int)((r->B + ncol - 1) / ncol);
+    const ColBatchKernel ck = col_batch_kernel(r->P, c.var);
+    if (c.persist) {
+        CU(cudaMemsetAsync(c.d_counter + j, 0, sizeof(unsigned), s));
+        ck<<<c.pgrid, ncol * CF_TEAM, col_smem(r, ncol), s>>>(c.d_col[j], nblk, nblk * (int)m, c.d_counter + j);
+    } else {
+        ck<<<dim3((unsigned)nblk, m), ncol * CF_TEAM, col_smem(r, ncol), s>>>(c.d_col[j], nblk, nblk * (int)m, nullptr);
+    }
     CU(cudaGetLastError());
+    return CF_OK;
+}
+
+// The ensemble autotuner.  For every size class, each kernel of the stage is
+// timed alone over its candidate shapes (CUDA events around one launch per
+// stage, after one untimed launch) and the fastest shape is kept for the
+// ensemble's graph:
+//   z kernels   columns per block tkz (the instances' own, then x2, x4 .. 32)
+//   x-pass      rows per block 2, 4, 8, 16
+//   column      each variant (columns per block, register bound) in both
+//               schedules: one block per column block of every instance, or a
+//               persistent grid of the blocks that fit at once claiming the
+//               (instance, column block) items in order
+// The arithmetic per column and per row is the same in every shape, so the
+// choice changes no result.  It runs at creation on the zero state; the
+// members' state is zeroed again afterwards.
+static int autotune_batch(cf_batch* b) {
+    int rc = CF_OK;
+    for (cf_engine* h : b->inst) {
+        if ((rc = launch_prep(h, h->U, nullptr))) return rc;
+        CU(cudaStreamSynchronize(h->stream));
+    }
+    int dev = 0, nsm = 0, smax = 0;
+    CU(cudaGetDevice(&dev));
+    CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CU(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    // device time of the kernels `which` of one step of class c (ms), or < 0
+    auto time_class = [&](BatchClass& c, int which, float& ms) -> int {
+        int r2 = batch_upload(b);
+        for (int rep = 0; rep < 2 && !r2; ++rep) {
+            if (rep == 1 && cudaEventRecord(e0, b->stream) != cudaSuccess) r2 = fail(CF_E_CUDA, "event");
+            for (int j = 0; j < 3 && !r2; ++j) r2 = launch_class_stage(b, c, j, b->stream, which);
+            if (rep == 1 && !r2 && cudaEventRecord(e1, b->stream) != cudaSuccess) r2 = fail(CF_E_CUDA, "event");
+        }
+        if (r2) return r2;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+            return fail(CF_E_CUDA, "autotuner timing failed");
+        return CF_OK;
+    };
+    std::string out;
+    for (BatchClass& c : b->cls) {
+        const cf_engine* r = b->inst[c.members[0]];
+        const int m = (int)c.members.size();
+        char buf[1024];
+        std::snprintf(buf, sizeof buf, "%dx%dx%d x%d:", c.Nx, c.Ny, c.Nz, m);
+        std::string line = buf, cand;
+        float ms = 0.f, total = 0.f;
+        // z kernels
+        {
+            float best = 1e30f;
+            int bt = r->tkz;
+            cand.clear();
+            for (int tkz = r->tkz; tkz <= 32 && !rc; tkz *= 2) {
+                c.tkz = tkz;
+                if (class_zsmem(b, c) > (size_t)std::min(smax, 200 * 1024)) break;
+                if ((rc = time_class(c, 1 | 4, ms))) break;
+                std::snprintf(buf, sizeof buf, "%s%d: %.3f", cand.empty() ? "" : ", ", tkz, ms);
+                cand += buf;
+                if (ms < best) best = ms, bt = tkz;
+            }
+            if (rc) break;
+            c.tkz = bt;
+            total += best;
+            std::snprintf(buf, sizeof buf, " z kernels tkz=%d (%.3f ms; candidates %s)", bt, best, cand.c_str());
+            line += buf;
+        }
+        // x-pass
+        {
+            float best = 1e30f;
+            int bk = KF_XPASS;
+            cand.clear();
+            const int xkinds[] = {KF_XPASS, KF_XPASS_R4, KF_XPASS_R8, KF_XPASS_R16};
+            for (int xk : xkinds) {
+                c.xkind = xk;
+                if (xk != KF_XPASS && class_xsmem(b, c) > (size_t)200 * 1024) continue;
+                if ((rc = time_class(c, 2, ms))) break;
+                std::snprintf(buf, sizeof buf, "%s%d rows: %.3f", cand.empty() ? "" : ", ", xpass_rows(xk), ms);
+                cand += buf;
+                if (ms < best) best = ms, bk = xk;
+            }
+            if (rc) break;
+            c.xkind = bk;
+            total += best;
+            std::snprintf(buf, sizeof buf, "; x-pass %d rows per block (%.3f ms; candidates %s)", xpass_rows(bk), best,
+                          cand.c_str());
+            line += buf;
+        }
+        // column kernel
+        {
+            float best = 1e30f;
+            int bv = 0;
+            bool bp = false;
+            unsigned bg = 0;
+            cand.clear();
+            for (int v = 0; v < col_batch_nvariants(r->P) && !rc; ++v)
+                for (int pers = 0; pers < 2 && !rc; ++pers) {
+                    const int ncol = kColBatchNcol[v];
+                    const int nitems = (int)((r->B + ncol - 1) / ncol) * m;
+                    int occ = 0;
+                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, col_batch_kernel(r->P, v), ncol * CF_TEAM,
+                                                                      col_smem(r, ncol)) != cudaSuccess || occ < 1) {
+                        cudaGetLastError();
+                        continue;
+                    }
+                    c.var = v;
+                    c.persist = pers != 0;
+                    c.pgrid = (unsigned)std::min<long>(nitems, (long)occ * nsm);
+                    if (c.persist && (int)c.pgrid >= nitems) continue;  // one wave: the same as a block per item
+                    if ((rc = time_class(c, 8, ms))) break;
+                    std::snprintf(buf, sizeof buf, "%s(%d,%d,%s) %.3f", cand.empty() ? "" : ", ", ncol,
+                                  v ? kColBatchMinb[v] : 0, c.persist ? "persistent" : "grid", ms);
+                    cand += buf;
+                    if (ms < best) best = ms, bv = v, bp = c.persist, bg = c.pgrid;
+                }
+            if (rc) break;
+            c.var = bv;
+            c.persist = bp;
+            c.pgrid = bg;
+            total += best;
+            std::snprintf(buf, sizeof buf, "; column kernel ncol=%d minb=%d %s (%.3f ms; candidates (ncol,minb,schedule) %s)",
+                          kColBatchNcol[bv], bv ? kColBatchMinb[bv] : 0,
+                          bp ? ("persistent grid " + std::to_string(bg)).c_str() : "one block per item", best,
+                          cand.c_str());
+            line += buf;
+        }
+        c.step_ms = total;
+        std::snprintf(buf, sizeof buf, "; %.3f ms per step of the class alone\n", total);
+        out += line + buf;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if ((rc = batch_upload(b))) return rc;
+    // back to the zero state the members were created with
+    for (cf_engine* h : b->inst) {
+        const size_t fr = sizeof(zd) * h->nr;
+        for (int i = 0; i < 3; ++i) {
+            CU(cudaMemsetAsync(h->U[i], 0, fr, b->stream));
+            CU(cudaMemsetAsync(h->Q[i], 0, fr, b->stream));
+        }
+        CU(cudaMemsetAsync(h->Pf, 0, fr, b->stream));
+        h->nodal_valid = false;
+    }
+    CU(cudaStreamSynchronize(b->stream));
+    b->schedule = out;
     return CF_OK;
 }
 
@@ -2007,6 +2234,13 @@ int cf_step_batch(cf_batch* b, int nsteps) {
 }
 
 int cf_batch_last_launch_count(cf_batch* b) { return b ? b->last_launches : 0; }
+int cf_batch_schedule(cf_batch* b, char* buf, int cap) {
+    if (!b || !buf || cap < 1) return fail(CF_E_ARG, "null argument");
+    const int n = std::min((int)b->schedule.size(), cap - 1);
+    std::memcpy(buf, b->schedule.data(), (size_t)n);
+    buf[n] = 0;
+    return n;
+}
 void* cf_batch_stream(cf_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 // ---------------------------------------------------------------------------

@@ -779,3 +779,77 @@ __global__ void __launch_bounds__(256) k_xpass_batch(const FftParams* __restrict
     stage_params(&ps, pl + blockIdx.z);
     xpass_body<LX, zd>(ps, blockIdx.x, blockIdx.y);
 }
+
+// Rotational x-pass of R rows per block (R even), for short rows: two rows
+// leave most of a block's threads idle in the FFT passes (3 x 72 butterflies
+// of 256 at Nxp = 48), R rows keep them busy.  The same arithmetic per row as
+// xpass_body.  Slots 3r .. 3r+2 hold (u0+iu1, u2+iw0, w1+iw2) of row r; the
+// products of rows 2q, 2q+1 leave in slots 3q (n0+in1 of 2q), 3q+1 (of 2q+1)
+// and 3q+2 (n2 of 2q + i n2 of 2q+1).  smem 6 R bsx complex (XOR layout).
+template <int LX, int R>
+CF_DEV void xpass_rows_body(const FftParams& p, int bx, int n) {
+    static_assert(R % 2 == 0, "rows are paired in the forward transform");
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    zd* sm = reinterpret_cast<zd*>(fsm_raw);
+    const int z0 = R * bx;
+    const int nrow = min(R, p.Nzp - z0);
+    const int Nxp = LX ? LX : p.Nxp, Nxh = p.Nxh, bs = p.bsx;
+    const long row0 = ((long)n * p.Nzp + z0) * Nxh;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
+    zd* scr = sm + 3 * R * bs;
+    xpack<zd, 1, 3 * R, true>(sm, bs, Nxh, Nxp, xnyq, [&](int slot, int k, zd& X, zd& Y) {
+        const int r = slot / 3, f = slot - 3 * r;
+        if (r >= nrow) return;  // zeros for rows past the end
+        const long row = row0 + (long)r * Nxh;
+        X = zp_of<zd>(p, 2 * f)[row + k];
+        Y = zp_of<zd>(p, 2 * f + 1)[row + k];
+    });
+    __syncthreads();
+    zd* A = group_fft_L<true, LX, 1>(sm, scr, 3 * R, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
+    zd* Bf = (A == sm) ? scr : sm;
+    for (int e = threadIdx.x; e < (R / 2) * Nxp; e += blockDim.x) {
+        const int qd = e / Nxp, j = e - qd * Nxp, sj = swz(j);
+        const zd* ra = A + 6 * qd * bs;
+        const zd a0 = ra[0 * bs + sj], a1 = ra[1 * bs + sj], a2 = ra[2 * bs + sj];
+        const zd b0 = ra[3 * bs + sj], b1 = ra[4 * bs + sj], b2 = ra[5 * bs + sj];
+        // u = (a0.x, a0.y, a1.x), omega = (a1.y, a2.x, a2.y); likewise b
+        const double nA0 = a0.y * a2.y - a1.x * a2.x;
+        const double nA1 = a1.x * a1.y - a0.x * a2.y;
+        const double nA2 = a0.x * a2.x - a0.y * a1.y;
+        const double nB0 = b0.y * b2.y - b1.x * b2.x;
+        const double nB1 = b1.x * b1.y - b0.x * b2.y;
+        const double nB2 = b0.x * b2.x - b0.y * b1.y;
+        zd* o = Bf + 3 * qd * bs;
+        o[0 * bs + sj] = zmake(nA0, nA1);
+        o[1 * bs + sj] = zmake(nB0, nB1);
+        o[2 * bs + sj] = zmake(nA2, nB2);
+    }
+    __syncthreads();
+    const zd* F = group_fft_L<true, LX, 1>(Bf, A, 3 * R / 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
+    xunpack<zd, 1, 3 * R / 2, true>(F, bs, Nxh, Nxp, [&](int slot, int k, zd X, zd Y) {
+        const int qd = slot / 3, w = slot - 3 * qd;
+        const int rA = 2 * qd, rB = rA + 1;
+        const long rowA = row0 + (long)rA * Nxh, rowB = rowA + Nxh;
+        if (w == 0) {
+            if (rA < nrow) {
+                zp_of<zd>(p, 0)[rowA + k] = X;
+                zp_of<zd>(p, 1)[rowA + k] = Y;
+            }
+        } else if (w == 1) {
+            if (rB < nrow) {
+                zp_of<zd>(p, 0)[rowB + k] = X;
+                zp_of<zd>(p, 1)[rowB + k] = Y;
+            }
+        } else {
+            if (rA < nrow) zp_of<zd>(p, 2)[rowA + k] = X;
+            if (rB < nrow) zp_of<zd>(p, 2)[rowB + k] = Y;
+        }
+    });
+}
+// grid (ceil(Nzp/R), Ny, instances)
+template <int LX, int R>
+__global__ void __launch_bounds__(256) k_xpass_rows_batch(const FftParams* __restrict__ pl) {
+    __shared__ FftParams ps;
+    stage_params(&ps, pl + blockIdx.z);
+    xpass_rows_body<LX, R>(ps, blockIdx.x, blockIdx.y);
+}

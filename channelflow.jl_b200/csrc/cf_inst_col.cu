@@ -31,10 +31,20 @@ DiagKernel diag_kernel_for() {
     return k_column_diag<CF_NCOL, P>;
 }
 template <int P>
-ColBatchKernel col_batch_kernel_for() {
-    return k_column_stage_batch<CF_NCOL, P>;
+ColBatchKernel col_batch_kernel_for(int variant) {
+    if constexpr (col_batch_variants(P)) {
+        switch (variant) {
+            case 1: return k_column_stage_batch<2, P, 6>;
+            case 2: return k_column_stage_batch<2, P, 8>;
+            case 3: return k_column_stage_batch<1, P, 8>;
+            case 4: return k_column_stage_batch<1, P, 12>;
+            case 5: return k_column_stage_batch<1, P, 16>;
+            default: break;
+        }
+    }
+    return k_column_stage_batch<CF_NCOL, P, col_minblocks<CF_NCOL, P>()>;
 }
 
 template ColKernel col_kernel_for<CF_INST_P>(int);
 template DiagKernel diag_kernel_for<CF_INST_P>();
-template ColBatchKernel col_batch_kernel_for<CF_INST_P>();
+template ColBatchKernel col_batch_kernel_for<CF_INST_P>(int);

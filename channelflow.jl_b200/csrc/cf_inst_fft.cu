@@ -25,6 +25,9 @@ FftBatchKernel fft_batch_kernel_for(int which) {
     switch (which) {
         case KF_ZINV: return k_zinv_batch<L>;
         case KF_ZFWD: return k_zfwd_batch<L>;
+        case KF_XPASS_R4: return k_xpass_rows_batch<L, 4>;
+        case KF_XPASS_R8: return k_xpass_rows_batch<L, 8>;
+        case KF_XPASS_R16: return k_xpass_rows_batch<L, 16>;
         default: return k_xpass_batch<L>;
     }
 }

@@ -601,14 +601,33 @@ template <int NCOL, int PL, int FORM = NL_ROT>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_stage(ColParams p) {
     column_stage_body<NCOL, PL, 0, FORM>(p, blockIdx.x);
 }
-// Batched stage: blockIdx.y selects the instance of a size class, whose
-// parameters are staged in shared memory.
-template <int NCOL, int PL>
-__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>()))
-    k_column_stage_batch(const ColParams* __restrict__ pl) {
+// Batched stage over the instances of a size class: item (instance i,
+// column block bx), the instance's parameters staged in shared memory.
+// counter == null: one item per block, (bx, i) = (blockIdx.x, blockIdx.y).
+// Otherwise the launch is persistent: its blocks claim items in order
+// (instance-major, it = i * nblk + bx) from the counter, zeroed before the
+// launch, until all nitems are done.  MINB: blocks per SM the registers are
+// bounded for (the ensemble autotuner's choice).
+template <int NCOL, int PL, int MINB>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, MINB)
+    k_column_stage_batch(const ColParams* __restrict__ pl, int nblk, int nitems, unsigned* counter) {
     __shared__ ColParams ps;
-    stage_params(&ps, pl + blockIdx.y);
-    column_stage_body<NCOL, PL>(ps, blockIdx.x);
+    if (!counter) {
+        stage_params(&ps, pl + blockIdx.y);
+        column_stage_body<NCOL, PL>(ps, blockIdx.x);
+        return;
+    }
+    __shared__ int item;
+    for (;;) {
+        __syncthreads();  // every thread is done with the previous item
+        if (threadIdx.x == 0) item = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const int it = item;
+        if (it >= nitems) return;
+        const int inst = it / nblk;
+        stage_params(&ps, pl + inst);
+        column_stage_body<NCOL, PL>(ps, it - inst * nblk);
+    }
 }
 
 // Mixed-precision stages (MIX 1 and 2 of column_stage_body).

@@ -164,6 +164,13 @@ int cf_step_batch(cf_batch* b, int nsteps);
 int cf_batch_last_launch_count(cf_batch* b);
 /* the ensemble's CUDA stream (cudaStream_t) */
 void* cf_batch_stream(cf_batch* b);
+/* The launch schedule the ensemble's autotuner chose at cf_create_batch, as
+ * text: per size class the column kernel's variant (columns per block,
+ * register bound), its schedule (one block per column block of every
+ * instance, or a persistent grid claiming the items in order) and the timings
+ * of every candidate.  Writes at most cap - 1 characters and a NUL; returns
+ * the number written. */
+int cf_batch_schedule(cf_batch* b, char* buf, int cap);
 
 /* cf_nonlinear without allocating: U and N are staged in a fixed
  * module-scope device array of CF_NOALLOC_SCRATCH_BYTES (16 MiB) instead of

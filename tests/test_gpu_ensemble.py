@@ -57,6 +57,10 @@ def test_ensemble_matches_single_instances():
     ens.step(nsteps)
     # three size classes, 12 launches per class per step
     assert ens.launches() == 12 * 3 * nsteps
+    # the autotuner's choice per class is recorded (whatever it chose, the
+    # arithmetic per column is the same, so the twins below agree to rounding)
+    sched = ens.schedule()
+    assert sched.count("column kernel ncol=") == 3, sched
     for inst, t in zip(ens.instances, twins):
         t.advance(0.0, 2 * nsteps)
         Ue, Pe = inst.get_state()
