@@ -52,9 +52,12 @@ CONFIGS = {
     "c4": dict(ensemble=[((32, 33, 32), 128), ((48, 49, 48), 96), ((64, 65, 64), 32)],
                Lx=2 * math.pi / 1.14, Lz=2 * math.pi / 2.5, Re=(300.0, 500.0), amp=(0.05, 0.15), dt=0.01,
                profile="couette", constraint=None, shape=0, rho=0.8),
-    # large grid 512x385x512 (plain FP64 here)
+    # large mixed-precision grid 512x385x512 with the state stored in FP32 (FP64
+    # Helmholtz, influence-matrix and mean-mode solves); errors against an FP64
+    # run of the same 200 steps
     "c5": dict(Nx=512, Ny=385, Nz=512, Lx=2 * math.pi, Lz=math.pi, nu=(2 / 3) / 10900, dt=0.0015,
-               profile="poiseuille", constraint=(2 / 3, 0.0), amp=0.1, shape=1, rho=0.8),
+               profile="poiseuille", constraint=(2 / 3, 0.0), amp=0.1, shape=1, rho=0.8,
+               precision="mixed-f32state", err_steps=200),
 }
 METRIC = "steps/s @384x257x384: mixed vs FP64 plain (<=1e-9 rel err); ensemble agg steps/s"
 
@@ -67,16 +70,22 @@ def sizes(cfg):
     return Nr, Nq
 
 
-def model_bytes(cfg, s_nl=16):
+def model_bytes(cfg, s_nl=None, s_state=None):
     """Algorithmic bytes per kernel launch (fixed byte model of the step).
 
-    per stage (rotational form): 16*19*Nr (U, P, Q read/write 14; responses
-    and factors 5) + s_nl*(18*Nr + 18*Nq) (N read 3, nodes written 6,
-    z-inverse 6->6, x-pass 6->3, z-forward 3->3).  Convective form: z-inverse
-    6->9, x-pass 9->3.  Divergence form: nodes written 3, z-inverse 3->3,
-    x-pass 3->6, z-forward 6->6, and k_column_div (counted with the column
-    kernel) 6->3.
+    per stage (rotational form): s_state*14*Nr (U, P, Q read/write) + 16*5*Nr
+    (Stokes responses and factors) + s_nl*(18*Nr + 18*Nq) (N read 3, nodes
+    written 6, z-inverse 6->6, x-pass 6->3, z-forward 3->3); s_state = s_nl =
+    16 for FP64, s_nl = 8 for the mixed forms' FP32 nodal and padded fields,
+    s_state = 8 for the FP32 state.  Convective form: z-inverse 6->9, x-pass
+    9->3.  Divergence form: nodes written 3, z-inverse 3->3, x-pass 3->6,
+    z-forward 6->6, and k_column_div (counted with the column kernel) 6->3.
     """
+    prec = cfg.get("precision", "fp64")
+    if s_nl is None:
+        s_nl = 16 if prec == "fp64" else 8
+    if s_state is None:
+        s_state = 8 if prec == "mixed-f32state" else 16
     Nr, Nq = sizes(cfg)
     form = cfg.get("form", "rotational")
     if form == "convective":
@@ -89,7 +98,7 @@ def model_bytes(cfg, s_nl=16):
         "zinv": s_nl * (6 * Nr + 6 * Nq),
         "xpass": s_nl * (9 * Nq),
         "zfwd": s_nl * (3 * Nq + 3 * Nr),
-        "column": 16 * 19 * Nr + s_nl * 9 * Nr,
+        "column": s_state * 14 * Nr + 16 * 5 * Nr + s_nl * 9 * Nr,
     }
 
 
@@ -307,7 +316,9 @@ def workload_desc(cfg):
     return {"grid": [cfg["Nx"], cfg["Ny"], cfg["Nz"]], "Lx": cfg["Lx"], "Lz": cfg["Lz"], "nu": cfg["nu"],
             "dt": cfg["dt"], "profile": cfg["profile"],
             "constraint": ("bulkvelocity" if cfg["constraint"] else "pressuregradient(0,0)"),
-            "form": cfg.get("form", "rotational"), "precision": "fp64 plain",
+            "form": cfg.get("form", "rotational"),
+            "precision": ("fp64 plain" if cfg.get("precision", "fp64") == "fp64"
+                          else MIXED_DESC[cfg["precision"]]),
             "l2": "state larger than L2 (no flush needed)"}
 
 
@@ -483,7 +494,32 @@ MIXED_DESC = {
                 "remainders, three products, FP32 accumulation); FP64 Stokes solve and state",
     "mixed-bf16": "FP32 periodic transforms and products; tensor-core Chebyshev transforms (three BF16 pieces per "
                   "operand, six BF16 products, FP32 accumulation); FP64 Stokes solve and state",
+    "mixed-f32state": "FP32 periodic transforms and products; velocity, pressure and RK history stored in FP32 "
+                      "(widened to FP64 in every stage); FP64 Chebyshev transforms, Helmholtz, influence-matrix, "
+                      "mean-mode and flux-constraint solves",
 }
+
+
+def errors_vs_fp64(pb, U0, P0, fp64, nerr):
+    """Error of every reported result of problem pb against the FP64 engine
+    after nerr steps from (U0, P0) (fp64: fp64_reference_run's result)."""
+    Ur, dr, gr = fp64
+    pb.set_state(U0, P0)
+    _, gm = pb.advance(0.0, nerr)
+    Um, _ = pb.get_state()
+    dm = pb.diagnostics()
+
+    def rerr(a, b):
+        return float(abs(a - b) / max(abs(b), 1e-300))
+
+    return {"steps": nerr,
+            "velocity_rel_l2": float(np.linalg.norm(Um - Ur) / np.linalg.norm(Ur)),
+            "energy_rel": rerr(dm[0], dr[0]),
+            "dissipation_rel": rerr(dm[1], dr[1]),
+            "wall_shear_upper_rel": rerr(dm[3], dr[3]),
+            "wall_shear_lower_rel": rerr(dm[4], dr[4]),
+            "flux_gradient_rel": rerr(gm[0], gr[0]),
+            "max_div_mixed": float(dm[2]), "max_div_fp64": float(dr[2])}
 
 
 def fp64_reference_run(cfg, g, U0, P0, nerr):
@@ -546,26 +582,9 @@ def measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, fp64, nerr, preci
                      # TF32 operands (the TF32 tensor rate is half the BF16 one)
                      "tensor_frac_of_type_peak": ((nprod * flops / t / 1e12) / (tc_peak * (0.5 if nprod == 3 else 1.0))
                                                   if tc_peak else None)}
-    # error against the FP64 step
-    Ur, dr, gr = fp64
-    mx.set_state(U0, P0)
-    _, gm = mx.advance(0.0, nerr)
-    Um, _ = mx.get_state()
-    dm = mx.diagnostics()
-
-    def rerr(a, b):
-        return float(abs(a - b) / max(abs(b), 1e-300))
-
     out = {"value": args.steps / (ms / 1e3), "unit": "steps/s", "ms_per_step": ms / args.steps,
            "kernel_ms_per_launch": kavg, "gpu_launches": launches,
-           "error_vs_fp64": {"steps": nerr,
-                             "velocity_rel_l2": float(np.linalg.norm(Um - Ur) / np.linalg.norm(Ur)),
-                             "energy_rel": rerr(dm[0], dr[0]),
-                             "dissipation_rel": rerr(dm[1], dr[1]),
-                             "wall_shear_upper_rel": rerr(dm[3], dr[3]),
-                             "wall_shear_lower_rel": rerr(dm[4], dr[4]),
-                             "flux_gradient_rel": rerr(gm[0], gr[0]),
-                             "max_div_mixed": float(dm[2]), "max_div_fp64": float(dr[2])},
+           "error_vs_fp64": errors_vs_fp64(mx, U0, P0, fp64, nerr),
            "precision": MIXED_DESC[precision]}
     if cheb:
         out["tensor_core_transforms"] = cheb
@@ -592,8 +611,11 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--form", default="rotational", choices=["rotational", "convective", "divergence"],
                     help="nonlinear form of the FP64 step (the mixed form runs the rotational one)")
-    ap.add_argument("--err-steps", type=int, default=1000,
-                    help="steps after which the mixed forms' errors against FP64 are taken")
+    ap.add_argument("--err-steps", type=int, default=None,
+                    help="steps after which the mixed forms' errors against FP64 are taken (default: the "
+                         "configuration's, else 1000)")
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed", "mixed-tc", "mixed-bf16", "mixed-f32state"],
+                    help="precision of the timed step (default: the configuration's, else fp64)")
     ap.add_argument("--no-c4", action="store_true", help="skip the ensemble measurement of the default line")
     ap.add_argument("--grid", default=None,
                     help="Nx,Ny,Nz replacing the configuration's grid (smaller cases for profiling)")
@@ -602,7 +624,10 @@ def main():
     if args.grid:
         cfg["Nx"], cfg["Ny"], cfg["Nz"] = (int(v) for v in args.grid.split(","))
     cfg["form"] = args.form
-    if args.form != "rotational":
+    cfg["precision"] = args.precision or cfg.get("precision", "fp64")
+    if args.err_steps is None:
+        args.err_steps = cfg.get("err_steps", 1000)
+    if args.form != "rotational" or cfg["precision"] != "fp64":
         args.no_mixed = True
     if args.impl == "reference":
         # rank 0 alone times the CPU reference; other ranks exit without work
@@ -620,10 +645,12 @@ def main():
     import cfb200
 
     g = cfb200.Grid(cfg["Nx"], cfg["Ny"], cfg["Nz"], cfg["Lx"], cfg["Lz"])
+    prec = cfg["precision"]
     if cfg["profile"] == "couette":
-        pb = cfb200.CouetteFlow(g, cfg["nu"], cfg["dt"], form=args.form)
+        pb = cfb200.CouetteFlow(g, cfg["nu"], cfg["dt"], form=args.form, precision=prec)
     else:
-        pb = cfb200.PoiseuilleFlow(g, cfg["nu"], cfg["dt"], bulkvelocity=cfg["constraint"], form=args.form)
+        pb = cfb200.PoiseuilleFlow(g, cfg["nu"], cfg["dt"], bulkvelocity=cfg["constraint"], form=args.form,
+                                   precision=prec)
     cfb200.lib().cf_random_state(pb.handle, 1000 + rank, cfg["amp"], cfg["shape"], cfg["rho"])
     U0, P0 = pb.get_state()
     stream = torch.cuda.ExternalStream(pb.stream_ptr())
@@ -668,7 +695,7 @@ def main():
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_kind,
                 "traffic": (traffic_from_profiles(knames[dom], args.config)
-                            if not args.grid and args.form == "rotational" else None),
+                            if not args.grid and args.form == "rotational" and prec == "fp64" else None),
                 "algorithmic_bytes_per_launch": mb[dom],
                 "kernel_ms_per_launch": kavg,
                 "step_model_bytes": 3 * sum(mb.values()),
@@ -699,7 +726,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "mixed f32/f64", "data": "synthetic",
         "config": {"workload": args.config, **workload_desc(cfg), "parallelism": f"replicas x{world}"},
         "grid_point_steps_per_s": value * cfg["Nx"] * cfg["Ny"] * cfg["Nz"],
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
@@ -709,11 +736,17 @@ def main():
         "gpu_launches": launches,
         "diagnostics": {"kinetic_energy": diag[0], "dissipation": diag[1], "max_div": diag[2]},
     }
+    if prec != "fp64":
+        # the timed precision's errors against an FP64 run of the same steps
+        fp64 = fp64_reference_run(cfg, g, U0, P0, args.err_steps)
+        line["error_vs_fp64"] = errors_vs_fp64(pb, U0, P0, fp64, args.err_steps)
+        line["kernel_GBs"] = {k: mb[k] / (kavg[k] * 1e-3) / 1e9 for k in kavg}
     if not args.no_mixed:
         fp64 = fp64_reference_run(cfg, g, U0, P0, args.err_steps)
         line["mixed"] = {}
-        for prec, key in (("mixed", "default"), ("mixed-tc", "tensor_core_tf32"), ("mixed-bf16", "tensor_core_bf16")):
-            m = measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, fp64, args.err_steps, precision=prec)
+        for mprec, key in (("mixed", "default"), ("mixed-tc", "tensor_core_tf32"), ("mixed-bf16", "tensor_core_bf16"),
+                           ("mixed-f32state", "fp32_state")):
+            m = measure_mixed(args, cfg, g, U0, P0, torch, max_over_ranks, fp64, args.err_steps, precision=mprec)
             m["speedup_vs_fp64_plain"] = m["value"] / (value / world)
             line["mixed"][key] = m
     if not args.no_c4 and args.config == "c3" and not args.grid:

@@ -39,7 +39,7 @@ class _Config(ctypes.Structure):
                 ("constraint", ctypes.c_int), ("c1", ctypes.c_double), ("c2", ctypes.c_double),
                 ("precision", ctypes.c_int), ("form", ctypes.c_int)]
 
-PRECISIONS = {"fp64": 0, "mixed": 1, "mixed-tc": 2, "mixed-bf16": 3}
+PRECISIONS = {"fp64": 0, "mixed": 1, "mixed-tc": 2, "mixed-bf16": 3, "mixed-f32state": 4}
 # NonLinearTerm forms (src/nonlinear.jl:10-17): CF_FORM_* of cfb200.h
 FORMS = {"rotational": 0, "convective": 1, "divergence": 2}
 

@@ -133,6 +133,14 @@ CF_DEV void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memo
 // until the bulk stores of this thread have read their shared memory (bounded
 // by construction: the copies are in flight and complete)
 CF_DEV void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// Hint: bring [p, p + bytes) into L2 (one bulk prefetch, no completion to
+// wait for).  The range is narrowed to whole 16-byte granules inside it, so
+// no byte outside the caller's range (inside one allocation) is named.
+CF_DEV void l2_prefetch(const void* p, size_t bytes) {
+    const uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15, e = ((uintptr_t)p + bytes) & ~(uintptr_t)15;
+    if (e > a)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
+}
 
 // Copy of one instance's parameters into shared memory (batched launches:
 // the block's instance is picked by a grid coordinate).

@@ -8,7 +8,9 @@
 #include "cf_fftkernels.cuh"
 #include "cf_kernels.cuh"
 
+#ifndef CF_NCOL
 #define CF_NCOL 2
+#endif
 static_assert(CF_NCOL == 1 || CF_NCOL == 2, "column teams use named barriers 1 and 2");
 
 // Column-kernel lengths P and periodic lengths L with compile-time
@@ -33,7 +35,7 @@ typedef void (*FftTmaKernel)(FftParams, FftMaps);
 enum {
     KC_STAGE, KC_PREP, KC_NLOUT, KC_PROJECT, KC_PRESSURE, KC_STAGE_MX, KC_PREP_MX,
     KC_STAGE_CONV, KC_PREP_CONV, KC_STAGE_DIV, KC_PREP_DIV, KC_DIV, KC_PRESSURE_COEF,
-    KC_STAGE_MXD, KC_PREP_MXD, KC_COUNT
+    KC_STAGE_MXD, KC_PREP_MXD, KC_STAGE_MXS, KC_PREP_MXS, KC_COUNT
 };
 enum { KF_ZINV, KF_ZFWD, KF_XPASS, KF_XPASS_CONV, KF_XPASS_DIV, KF_XPASS2, KF_XPASS_IP, KF_XPASS_CONV_IP, KF_XPASS_DIV_IP, KF_COUNT };
 // rows per block of the batched x-pass variants (KF_XPASS: 2; the others for

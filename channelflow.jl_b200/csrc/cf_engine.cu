@@ -254,6 +254,14 @@ struct cf_engine {
     unsigned char *d_chebF = nullptr, *d_chebI = nullptr;  // transform-matrix images, pieces back to back
     int split = 0;  // tensor-core operand split: 0 TF32 head and remainder, 1 three BF16 pieces
     int chebNP = 0, chebKT = 0;
+    // CF_PRECISION_MIXED_F32STATE: the state the steps advance lives in
+    // U32, P32, Q32 (complex float); U and Pf keep the FP64 copy that the
+    // state entry points read and write.  valid64 / valid32: which copy is
+    // current (converted on demand by state_to64 / state_to32).
+    bool s32 = false;
+    void *U32[3] = {}, *P32 = nullptr, *Q32[3] = {};
+    zd* mean64 = nullptr;  // the mean-flow mode (column 0) of U, P, Q in FP64: [7][Ny]
+    bool valid64 = true, valid32 = true;
     int* d_cheberr = nullptr;
     double* d_diag = nullptr;  // diagnostics accumulators
     double* d_diagpart = nullptr;  // diagnostics block partials (3 per column block)
@@ -740,6 +748,82 @@ static int cheb_pieces(int split);
 static size_t cheb_piece_bytes(int Ny, int split);
 static ChebKernel cheb_kernel(int split);
 
+// ---- FP32 state (CF_PRECISION_MIXED_F32STATE): the FP64 copy of U and P
+// and the FP32 state the steps advance, converted on demand.
+// The mean-flow mode (column 0 of each field) stays FP64 in mean[f][n]:
+// rounding copies it there, widening takes it from there.
+struct StateCopy {
+    const void* src[4];
+    void* dst[4];
+    zd* mean;
+    long B;
+};
+static __global__ void __launch_bounds__(256) k_state_convert(StateCopy a, long n, int to32) {
+    const long tot = 4 * n, stride = (long)gridDim.x * blockDim.x, ny = n / a.B;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += stride) {
+        const int f = (int)(i / n);
+        const long e = i - f * n;
+        const bool mean = e % a.B == 0;
+        if (to32) {
+            const zd v = static_cast<const zd*>(a.src[f])[e];
+            static_cast<zf*>(a.dst[f])[e] = to_zf(v);
+            if (mean) a.mean[f * ny + e / a.B] = v;
+        } else {
+            static_cast<zd*>(a.dst[f])[e] =
+                mean ? a.mean[f * ny + e / a.B] : to_zd(static_cast<const zf*>(a.src[f])[e]);
+        }
+    }
+}
+static int state_convert(cf_engine* h, bool to32) {
+    StateCopy a;
+    for (int i = 0; i < 3; ++i) {
+        a.src[i] = to32 ? (const void*)h->U[i] : h->U32[i];
+        a.dst[i] = to32 ? h->U32[i] : (void*)h->U[i];
+    }
+    a.src[3] = to32 ? (const void*)h->Pf : h->P32;
+    a.dst[3] = to32 ? h->P32 : (void*)h->Pf;
+    a.mean = h->mean64;
+    a.B = h->B;
+    k_state_convert<<<4 * 148, 256, 0, h->stream>>>(a, h->nr, to32 ? 1 : 0);
+    CU(cudaGetLastError());
+    return CF_OK;
+}
+// the FP32 state made current before a step reads it (rounded from the FP64
+// copy after a state entry point wrote that)
+static int state_to32(cf_engine* h) {
+    if (!h->s32 || h->valid32) return CF_OK;
+    int rc = state_convert(h, true);
+    if (rc) return rc;
+    h->valid32 = true;
+    return CF_OK;
+}
+// the FP64 copy made current before an entry point reads it
+static int state_to64(cf_engine* h) {
+    if (!h->s32 || h->valid64) return CF_OK;
+    int rc = state_convert(h, false);
+    if (rc) return rc;
+    h->valid64 = true;
+    return CF_OK;
+}
+// after an entry point wrote the FP64 copy / a step advanced the FP32 state
+static void state_wrote64(cf_engine* h) {
+    if (h->s32) h->valid64 = true, h->valid32 = false;
+}
+static void state_stepped(cf_engine* h) {
+    if (h->s32) h->valid32 = true, h->valid64 = false;
+}
+// column-kernel parameters of the mixed form's own kernels: the FP32 state
+// buffers in place of the FP64 ones (F32STATE)
+static void mx_state(const cf_engine* h, ColParams& p) {
+    if (!h->s32) return;
+    for (int i = 0; i < 3; ++i) {
+        p.U[i] = static_cast<zd*>(h->U32[i]);
+        p.Q[i] = static_cast<zd*>(h->Q32[i]);
+    }
+    p.Pf = static_cast<zd*>(h->P32);
+    p.mean64 = h->mean64;
+}
+
 static FftParams fft_params32(const cf_engine* h) {
     FftParams f = fft_params(h);
     f.nod0 = h->nod32[0]; f.nod1 = h->nod32[1]; f.nod2 = h->nod32[2];
@@ -798,7 +882,9 @@ static int launch_stage_mx(cf_engine* h, int j, int* count) {
         ColParams p = stage_col_params(h, j);
         for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->nod32[i]);
         for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
-        col_kernel(KC_STAGE_MXD, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+        mx_state(h, p);
+        col_kernel(h->s32 ? KC_STAGE_MXS : KC_STAGE_MXD, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h),
+                                                                 h->stream>>>(p);
         if (count) *count += 1;
         CU(cudaGetLastError());
         return CF_OK;
@@ -816,7 +902,9 @@ static int launch_prep_mx(cf_engine* h, int* count) {
     ColParams p = col_params(h);
     if (!h->tc) {
         for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
-        col_kernel(KC_PREP_MXD, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+        mx_state(h, p);
+        col_kernel(h->s32 ? KC_PREP_MXS : KC_PREP_MXD, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h),
+                                                               h->stream>>>(p);
         if (count) *count += 1;
         CU(cudaGetLastError());
         return CF_OK;
@@ -851,6 +939,7 @@ static int check_status(cf_engine* h, bool with_state = true) {
 // z-forward, column, forward Chebyshev, inverse Chebyshev] summed over steps
 static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, double* kernel_ms) {
     int rc = CF_OK, cnt = 0;
+    if ((rc = state_to32(h))) return rc;
     if (!h->nodal_valid) {
         if ((rc = launch_prep_mx(h, &cnt))) return rc;
         h->nodal_valid = true;
@@ -868,6 +957,7 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
             void* const* io = h->tc ? h->coef32 : h->nod32;
             for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(io[i]);
             for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(io[i]);
+            mx_state(h, p);
             cudaEventRecord(ev[0], h->stream);
             launch_z(h, KF_ZINV, true, 6, f);
             cudaEventRecord(ev[1], h->stream);
@@ -877,8 +967,8 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
             cudaEventRecord(ev[3], h->stream);
             if (h->tc && (rc = launch_cheb(h, 3, false, nullptr))) break;
             cudaEventRecord(ev[4], h->stream);
-            col_kernel(h->tc ? KC_STAGE_MX : KC_STAGE_MXD, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h),
-                                                                  h->stream>>>(p);
+            col_kernel(h->tc ? KC_STAGE_MX : (h->s32 ? KC_STAGE_MXS : KC_STAGE_MXD), h->P)<<<
+                col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
             cudaEventRecord(ev[5], h->stream);
             if (h->tc && (rc = launch_cheb(h, 6, true, nullptr))) break;
             cudaEventRecord(ev[6], h->stream);
@@ -893,6 +983,7 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
             }
         }
     for (int k = 0; k < 7; ++k) cudaEventDestroy(ev[k]);
+    state_stepped(h);
     if (rc) return rc;
     if ((rc = check_status(h))) return rc;
     h->last_launches = cnt + (h->tc ? 18 : 12) * nsteps;
@@ -1035,13 +1126,15 @@ static int validate_and_size(cf_engine* h, const cf_config* c) {
     if (!(std::isfinite(c->nu) && c->nu > 0)) return fail(CF_E_ARG, "nu must be finite and positive");
     if (c->constraint != 0 && c->constraint != 1) return fail(CF_E_ARG, "unknown constraint kind");
     if (c->precision != CF_PRECISION_FP64 && c->precision != CF_PRECISION_MIXED &&
-        c->precision != CF_PRECISION_MIXED_TC && c->precision != CF_PRECISION_MIXED_BF16)
+        c->precision != CF_PRECISION_MIXED_TC && c->precision != CF_PRECISION_MIXED_BF16 &&
+        c->precision != CF_PRECISION_MIXED_F32STATE)
         return fail(CF_E_ARG, "unknown precision mode");
     if ((c->precision == CF_PRECISION_MIXED_TC || c->precision == CF_PRECISION_MIXED_BF16) && c->Ny > 512)
         return fail(CF_E_UNSUPPORTED, "the tensor-core Chebyshev transforms support Ny <= 512");
     h->mixed = c->precision != CF_PRECISION_FP64;
     h->tc = c->precision == CF_PRECISION_MIXED_TC || c->precision == CF_PRECISION_MIXED_BF16;
     h->split = c->precision == CF_PRECISION_MIXED_BF16 ? 1 : 0;
+    h->s32 = c->precision == CF_PRECISION_MIXED_F32STATE;
     if (c->form != CF_FORM_ROTATIONAL && c->form != CF_FORM_CONVECTIVE && c->form != CF_FORM_DIVERGENCE)
         return fail(CF_E_ARG, "unknown nonlinear form");
     if (h->mixed && c->form != CF_FORM_ROTATIONAL)
@@ -1253,6 +1346,19 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
             if (h->tc && (rc = dalloc(h, &h->coef32[i], sizeof(zf) * h->nr))) return bail(rc);
         }
     }
+    if (h->s32) {
+        const size_t f32 = sizeof(zf) * h->nr;
+        for (int i = 0; i < 3; ++i) {
+            if ((rc = dalloc(h, &h->U32[i], f32))) return bail(rc);
+            if ((rc = dalloc(h, &h->Q32[i], f32))) return bail(rc);
+            cudaMemset(h->U32[i], 0, f32);
+            cudaMemset(h->Q32[i], 0, f32);
+        }
+        if ((rc = dalloc(h, &h->P32, f32))) return bail(rc);
+        cudaMemset(h->P32, 0, f32);
+        if ((rc = dalloc(h, (void**)&h->mean64, sizeof(zd) * 7 * h->Ny))) return bail(rc);
+        cudaMemset(h->mean64, 0, sizeof(zd) * 7 * h->Ny);
+    }
     if (h->mixed && h->tc) {
         std::vector<unsigned char> fimg, iimg;
         cheb_images(h->Ny, 0, 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1)), h->split, fimg, h->chebNP, h->chebKT);
@@ -1308,11 +1414,14 @@ int cf_set_state(cf_handle* h, const double* U, const double* P) {
     CU(cudaMemcpyAsync(h->Pf, P, fr, cudaMemcpyHostToDevice, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     h->nodal_valid = false;
+    state_wrote64(h);
     return CF_OK;
 }
 int cf_get_state(cf_handle* h, double* U, double* P) {
     if (!h || !U) return fail(CF_E_ARG, "null argument");
     DeviceGuard dg_(h->device);
+    int rc;
+    if ((rc = state_to64(h))) return rc;
     const size_t fr = sizeof(zd) * h->nr;
     for (int i = 0; i < 3; ++i) CU(cudaMemcpyAsync(U + 2 * i * h->nr, h->U[i], fr, cudaMemcpyDeviceToHost, h->stream));
     if (P) CU(cudaMemcpyAsync(P, h->Pf, fr, cudaMemcpyDeviceToHost, h->stream));
@@ -1327,11 +1436,14 @@ int cf_set_state_device(cf_handle* h, const void* U, const void* P) {
         CU(cudaMemcpyAsync(h->U[i], (const char*)U + i * fr, fr, cudaMemcpyDeviceToDevice, h->stream));
     CU(cudaMemcpyAsync(h->Pf, P, fr, cudaMemcpyDeviceToDevice, h->stream));
     h->nodal_valid = false;
+    state_wrote64(h);
     return CF_OK;
 }
 int cf_get_state_device(cf_handle* h, void* U, void* P) {
     if (!h || !U) return fail(CF_E_ARG, "null argument");
     DeviceGuard dg_(h->device);
+    int rc;
+    if ((rc = state_to64(h))) return rc;
     const size_t fr = sizeof(zd) * h->nr;
     for (int i = 0; i < 3; ++i)
         CU(cudaMemcpyAsync((char*)U + i * fr, h->U[i], fr, cudaMemcpyDeviceToDevice, h->stream));
@@ -1344,12 +1456,14 @@ int cf_step(cf_handle* h, double t, int nsteps, double* t_out, double* grads_out
     DeviceGuard dg_(h->device);
     if (nsteps < 0) return fail(CF_E_ARG, "nsteps must be nonnegative");
     int rc, cnt = 0;
+    if ((rc = state_to32(h))) return rc;
     if (!h->nodal_valid) {
         if ((rc = h->mixed ? launch_prep_mx(h, &cnt) : launch_prep(h, h->U, &cnt))) return rc;
         h->nodal_valid = true;
     }
     if ((rc = build_graph(h))) return rc;
     for (int s = 0; s < nsteps; ++s) CU(cudaGraphLaunch(h->graph, h->stream));
+    if (nsteps > 0) state_stepped(h);
     cnt += (h->mixed && h->tc ? 18 : step_launches(h)) * nsteps;
     h->last_launches = cnt;
     if (t_out) *t_out = t + nsteps * h->dt;
@@ -1369,6 +1483,7 @@ int cf_step_dt(cf_handle* h, double t, double dt, double* t_out, double* grads_o
     DeviceGuard dg_(h->device);
     if (!(std::isfinite(dt) && dt > 0)) return fail(CF_E_ARG, "dt must be finite and positive");
     if (dt == h->dt) return cf_step(h, t, 1, t_out, grads_out);
+    if (h->s32) return fail(CF_E_UNSUPPORTED, "a step of another duration is not supported with the FP32 state");
     int rc, cnt = 0;
     if (h->tdt != dt) {
         // the factors may still be read by an earlier step of this kind
@@ -1421,7 +1536,7 @@ int cf_step_host(cf_handle* h, double* U, double* P, double t, int nsteps, doubl
     DeviceGuard dg_(h->device);
     if (nsteps < 0) return fail(CF_E_ARG, "nsteps must be nonnegative");
     int rc;
-    if (nsteps == 0 || (h->mixed && h->tc)) {
+    if (nsteps == 0 || (h->mixed && h->tc) || h->s32) {
         // the tensor-core form transforms all columns in one launch: no chunks
         if ((rc = cf_set_state(h, U, P)) || (rc = cf_step(h, t, nsteps, t_out, grads_out))) return rc;
         return cf_get_state(h, U, P);
@@ -1636,6 +1751,7 @@ int cf_random_state(cf_handle* h, unsigned long long seed, double amp, int shape
     if ((rc = pressure_dev(h, h->U, h->Pf))) return rc;
     if ((rc = check_status(h, false))) return rc;
     h->nodal_valid = false;
+    state_wrote64(h);
     return CF_OK;
 }
 
@@ -1665,7 +1781,7 @@ int cf_diagnostics(cf_handle* h, double* out) {
     if (!h || !out) return fail(CF_E_ARG, "null argument");
     DeviceGuard dg_(h->device);
     int rc;
-    if ((rc = ensure_diag(h))) return rc;
+    if ((rc = ensure_diag(h)) || (rc = state_to64(h))) return rc;
     CU(cudaMemsetAsync(h->d_diag, 0, 8 * sizeof(double), h->stream));
     ColParams p = col_params(h);
     diag_kernel(h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p, h->d_diag, h->d_diagpart);
@@ -1689,7 +1805,7 @@ int cf_power_input(cf_handle* h, int with_base, double dPdx, double dPdz, double
     if (!(std::isfinite(dPdx) && std::isfinite(dPdz))) return fail(CF_E_ARG, "pressure gradient must be finite");
     DeviceGuard dg_(h->device);
     int rc;
-    if ((rc = ensure_diag(h))) return rc;
+    if ((rc = ensure_diag(h)) || (rc = state_to64(h))) return rc;
     k_power_input<<<1, 32, 0, h->stream>>>(h->U[0], h->U[2], with_base ? h->d_base : nullptr, (long)h->Nz * h->Nxh,
                                            h->Ny, h->nu, dPdx, dPdz, h->d_diag + 6);
     CU(cudaGetLastError());

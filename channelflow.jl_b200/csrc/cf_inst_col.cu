@@ -17,6 +17,8 @@ ColKernel col_kernel_for(int which) {
         case KC_PREP_MX: return k_column_prep<CF_NCOL, P, 1>;
         case KC_STAGE_MXD: return k_column_stage_mx<CF_NCOL, P, 2>;
         case KC_PREP_MXD: return k_column_prep<CF_NCOL, P, 2>;
+        case KC_STAGE_MXS: return k_column_stage_mx<CF_NCOL, P, 3>;
+        case KC_PREP_MXS: return k_column_prep<CF_NCOL, P, 3>;
         case KC_STAGE_CONV: return k_column_stage<CF_NCOL, P, NL_CONV>;
         case KC_PREP_CONV: return k_column_prep<CF_NCOL, P, 0, NL_CONV>;
         case KC_STAGE_DIV: return k_column_stage<CF_NCOL, P, NL_DIV>;

@@ -62,6 +62,9 @@ struct ColParams {
     const zd* cs_tab;  // (cos, sin)(pi n / P)
     const double* helm_tab;  // [3][Ny] degree coefficients of the integrated tau rows
     double fnorm;  // 1 / (Nxp Nzp (Ny-1))
+    // FP32 state (column_stage_body MIX 3): the mean-flow mode (column 0)
+    // kept in FP64, [7][Ny]: U0, U1, U2, P, Q0, Q1, Q2
+    zd* mean64;
 };
 
 // one of three pointers without indexing an array at run time
@@ -179,6 +182,38 @@ CF_DEV void tile_load_async(zd* sm, int cs, int hs, const zd* g, int c0, int Ny,
     else tile_load_async_body<NCOL>(sm, cs, hs, g, c0, Ny, B);
 }
 CF_DEV void tile_wait() { cp_async_wait<0>(); }
+// FP32 tile of NCOL adjacent columns copied asynchronously into a dense
+// staging run (element n NCOL + t; 8-byte cp.async per complex float, zero
+// fill outside the grid); the caller commits and waits.  tile_widen then
+// moves a staged tile into the parity layout as FP64 (the caller separates
+// the two with a __syncthreads); where the tile holds column 0 (c0 == 0) and
+// m64 is given, that column comes from m64 (the FP64 mean-flow mode) instead.
+template <int NCOL>
+CF_DEV void tile_stage32(zf* st, const zf* g, int c0, int Ny, int B) {
+    const int tot = Ny * NCOL;
+    for (int e = threadIdx.x; e < tot; e += NCOL * CF_TEAM) {
+        const int n = e / NCOL, t = e - n * NCOL;
+        const int c = c0 + t;
+        const bool ok = c < B;
+        cp_async_el<8>(st + e, ok ? g + (long)n * B + c : g, ok);
+    }
+}
+template <int NCOL>
+CF_DEV void tile_widen(zd* sm, int cs, int hs, const zf* st, int Ny, int c0, const zd* m64) {
+    const int tot = Ny * NCOL;
+    const bool mean = c0 == 0 && m64 != nullptr;
+    for (int e = threadIdx.x; e < tot; e += NCOL * CF_TEAM) {
+        const int n = e / NCOL, t = e - n * NCOL;
+        sm[t * cs + ppos(n, hs)] = (mean && t == 0) ? m64[n] : to_zd(st[e]);
+    }
+}
+// column 0 of a tile (c0 == 0) written in FP64 to m64 (the mean-flow mode
+// of an FP32 state)
+template <int NCOL>
+CF_DEV void tile_store_mean(const zd* sm, int hs, zd* m64, int Ny, int c0) {
+    if (c0 != 0) return;
+    for (int n = threadIdx.x; n < Ny; n += NCOL * CF_TEAM) m64[n] = sm[ppos(n, hs)];
+}
 
 template <int NCOL, class G>
 CF_DEV void tile_store_body(const zd* sm, int cs, int hs, G* __restrict__ g, int c0, int Ny, int B) {
@@ -448,12 +483,16 @@ CF_DEV void store_three(const Ctx& X, const ColParams& p, int r0, int r1, int r2
 //      coefficients (normalised by the transform; p.Nn holds zf arrays) and
 //      the new velocity and vorticity leave as FP32 coefficients in p.nod
 //   2  FP32 nodal fields in and out, Chebyshev transforms here in FP64
+//   3  as 2, with the state (U, P and the history Q) stored in FP32 in
+//      global memory: p.U, p.Pf and p.Q hold zf arrays, widened to FP64 in
+//      shared memory, and the stage's arithmetic stays FP64
 // FORM: the nonlinear form; the divergence form's term arrives as FP64
 // coefficients (from k_column_div), the others' at the nodes.
 template <int NCOL, int PL, int MIX = 0, int FORM = NL_ROT>
 CF_DEV void column_stage_body(const ColParams& p, int bx) {
     constexpr bool NCOEF = MIX == 1 || FORM == NL_DIV;  // N arrives as coefficients
     constexpr bool F32 = MIX != 0;                       // FP32 N in, FP32 fields out
+    constexpr bool S32 = MIX == 3;                       // FP32 state in global memory
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, bx);
     const Team& t = X.t;
@@ -473,7 +512,18 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     // right-hand-side region not yet written (1, then 2), and for i = 2, whose
     // right-hand side takes region 2, Q_2 goes there (consumed before the
     // right-hand side is formed) and U_2 to region 5.
-    tile_load_async<NCOL, PL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);  // completed with N_0
+    if (!S32) tile_load_async<NCOL, PL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);  // completed with N_0
+    // The block's Stokes-bank data (read in Phase B) start on their way to
+    // L2 now, so that Phase B's reads of them wait on L2, not on DRAM.
+    if (threadIdx.x == 0 && c0 < p.B) {
+        const long nc = min(NCOL, p.B - c0), Ny = p.Ny;
+        const BankDev& bk = p.bank;
+        l2_prefetch(bk.fac_p + c0 * 3 * Ny, nc * 3 * Ny * sizeof(double));
+        l2_prefetch(bk.fac_v + c0 * 3 * Ny, nc * 3 * Ny * sizeof(double));
+        l2_prefetch(bk.resp + c0 * 6 * Ny, nc * 6 * Ny * sizeof(double));
+        l2_prefetch(bk.colsc + c0 * 8, nc * 8 * sizeof(double));
+        l2_prefetch(bk.sa + c0 * 4, nc * 4 * sizeof(double));
+    }
     double gold[2] = {p.c1, p.c2};
     zd bulkN0 = zzero(), bulkN2 = zzero(), wR0 = zzero(), wL0 = zzero(), wR2 = zzero(), wL2 = zzero();
 #pragma unroll 1
@@ -482,11 +532,31 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         zd* Q_i = sel3(p.Q[0], p.Q[1], p.Q[2], i);
         zd* U_i = sel3(p.U[0], p.U[1], p.U[2], i);
         const int qreg = (i == 2) ? 2 : 5, ureg = (i == 2) ? 5 : i + 1;
-        if (p.stage > 0) tile_load_async<NCOL, PL>(X.reg(qreg), cs, hs, Q_i, c0, p.Ny, p.B);
-        tile_load_async<NCOL, PL>(X.reg(ureg), cs, hs, U_i, c0, p.Ny, p.B);
-        if (F32) tile_load<NCOL, PL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
-        else tile_load_async<NCOL, PL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
-        tile_wait();
+        if constexpr (S32) {
+            // the component's FP32 tiles (and P with the first) copied into
+            // the transform buffers, free until the forward transform, then
+            // widened into their regions
+            zf* st = reinterpret_cast<zf*>(X.reg(6));
+            const int T = NCOL * p.Ny;
+            tile_stage32<NCOL>(st, reinterpret_cast<const zf*>(U_i), c0, p.Ny, p.B);
+            tile_stage32<NCOL>(st + T, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
+            if (p.stage > 0) tile_stage32<NCOL>(st + 2 * T, reinterpret_cast<const zf*>(Q_i), c0, p.Ny, p.B);
+            if (i == 0) tile_stage32<NCOL>(st + 3 * T, reinterpret_cast<const zf*>(p.Pf), c0, p.Ny, p.B);
+            cp_async_commit();
+            tile_wait();
+            __syncthreads();
+            const long ny = p.Ny;
+            tile_widen<NCOL>(X.reg(ureg), cs, hs, st, p.Ny, c0, p.mean64 + i * ny);
+            tile_widen<NCOL>(X.reg(4), cs, hs, st + T, p.Ny, c0, nullptr);
+            if (p.stage > 0) tile_widen<NCOL>(X.reg(qreg), cs, hs, st + 2 * T, p.Ny, c0, p.mean64 + (4 + i) * ny);
+            if (i == 0) tile_widen<NCOL>(X.reg(3), cs, hs, st + 3 * T, p.Ny, c0, p.mean64 + 3 * ny);
+        } else {
+            if (p.stage > 0) tile_load_async<NCOL, PL>(X.reg(qreg), cs, hs, Q_i, c0, p.Ny, p.B);
+            tile_load_async<NCOL, PL>(X.reg(ureg), cs, hs, U_i, c0, p.Ny, p.B);
+            if (F32) tile_load<NCOL, PL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
+            else tile_load_async<NCOL, PL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
+            tile_wait();
+        }
         __syncthreads();
         if (valid) {
             if (!NCOEF) {
@@ -507,7 +577,14 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
             }
         }
         __syncthreads();
-        if (p.store_q) tile_store<NCOL, PL>(X.reg(4), cs, hs, Q_i, c0, p.Ny, p.B);
+        if (p.store_q) {
+            if (S32) {
+                tile_store<NCOL, PL>(X.reg(4), cs, hs, reinterpret_cast<zf*>(Q_i), c0, p.Ny, p.B);
+                tile_store_mean<NCOL>(X.reg(4), hs, p.mean64 + (4 + i) * (long)p.Ny, p.Ny, c0);
+            } else {
+                tile_store<NCOL, PL>(X.reg(4), cs, hs, Q_i, c0, p.Ny, p.B);
+            }
+        }
         if (valid) {
             zd* U = X.col(ureg);
             zd* Qn = X.col(4);
@@ -582,10 +659,22 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         }
     }
     __syncthreads();
-    tile_store<NCOL, PL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
-    tile_store<NCOL, PL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
-    tile_store<NCOL, PL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
-    tile_store<NCOL, PL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
+    if constexpr (S32) {
+        tile_store<NCOL, PL>(X.reg(0), cs, hs, reinterpret_cast<zf*>(p.U[0]), c0, p.Ny, p.B);
+        tile_store<NCOL, PL>(X.reg(4), cs, hs, reinterpret_cast<zf*>(p.U[1]), c0, p.Ny, p.B);
+        tile_store<NCOL, PL>(X.reg(2), cs, hs, reinterpret_cast<zf*>(p.U[2]), c0, p.Ny, p.B);
+        tile_store<NCOL, PL>(X.reg(3), cs, hs, reinterpret_cast<zf*>(p.Pf), c0, p.Ny, p.B);
+        const long ny = p.Ny;
+        tile_store_mean<NCOL>(X.reg(0), hs, p.mean64, p.Ny, c0);
+        tile_store_mean<NCOL>(X.reg(4), hs, p.mean64 + ny, p.Ny, c0);
+        tile_store_mean<NCOL>(X.reg(2), hs, p.mean64 + 2 * ny, p.Ny, c0);
+        tile_store_mean<NCOL>(X.reg(3), hs, p.mean64 + 3 * ny, p.Ny, c0);
+    } else {
+        tile_store<NCOL, PL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+        tile_store<NCOL, PL>(X.reg(4), cs, hs, p.U[1], c0, p.Ny, p.B);
+        tile_store<NCOL, PL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+        tile_store<NCOL, PL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);
+    }
     if (p.skip_nodal) return;
     __syncthreads();
     // ---------------- Phase C: total velocity, vorticity, nodal values
@@ -630,7 +719,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, MINB)
     }
 }
 
-// Mixed-precision stages (MIX 1 and 2 of column_stage_body).
+// Mixed-precision stages (MIX 1, 2 and 3 of column_stage_body).
 template <int NCOL, int PL, int MIX>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_stage_mx(ColParams p) {
     column_stage_body<NCOL, PL, MIX>(p, blockIdx.x);
@@ -638,16 +727,31 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
 
 // Nodal fields of the nonlinear form (velocity and vorticity for the
 // rotational form) from the state U (used after set_state); MIX 1: their FP32
-// Chebyshev coefficients instead; MIX 2: FP32 nodal values.
+// Chebyshev coefficients instead; MIX 2: FP32 nodal values; MIX 3: as 2, from
+// an FP32 state.
 template <int NCOL, int PL, int MIX = 0, int FORM = NL_ROT>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_prep(ColParams p) {
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, blockIdx.x);
     const int cs = X.cs, hs = X.t.hs, c0 = X.c0;
-    tile_load_async<NCOL, PL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
-    tile_load_async<NCOL, PL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
-    tile_load_async<NCOL, PL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
-    tile_wait();
+    if constexpr (MIX == 3) {
+        // FP32 state staged in the transform buffers and widened (column 0,
+        // the mean-flow mode, from its FP64 copy)
+        zf* st = reinterpret_cast<zf*>(X.reg(6));
+        const int T = NCOL * p.Ny;
+        for (int i = 0; i < 3; ++i)
+            tile_stage32<NCOL>(st + i * T, reinterpret_cast<const zf*>(sel3(p.U[0], p.U[1], p.U[2], i)), c0, p.Ny,
+                               p.B);
+        cp_async_commit();
+        tile_wait();
+        __syncthreads();
+        for (int i = 0; i < 3; ++i) tile_widen<NCOL>(X.reg(i), cs, hs, st + i * T, p.Ny, c0, p.mean64 + i * (long)p.Ny);
+    } else {
+        tile_load_async<NCOL, PL>(X.reg(0), cs, hs, p.U[0], c0, p.Ny, p.B);
+        tile_load_async<NCOL, PL>(X.reg(1), cs, hs, p.U[1], c0, p.Ny, p.B);
+        tile_load_async<NCOL, PL>(X.reg(2), cs, hs, p.U[2], c0, p.Ny, p.B);
+        tile_wait();
+    }
     __syncthreads();
     if (X.valid)
         col_prep_nodal<PL, MIX == 1, FORM>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6),

@@ -52,11 +52,19 @@ extern "C" {
  * between FP32 coefficient and nodal fields; Ny <= 512.  MIXED_BF16: as
  * MIXED_TC with the contractions on the BF16 tensor cores, each operand
  * split into three BF16 pieces (24 significant bits) and the six products of
- * order >= 2^-16 accumulated in FP32. */
+ * order >= 2^-16 accumulated in FP32.  MIXED_F32STATE: as MIXED with the
+ * state (velocity, pressure and the RK history) stored in FP32 in device
+ * memory; every stage widens it to FP64 for the right-hand side, the tau
+ * Helmholtz solves, the influence-matrix and tau corrections, the mean mode
+ * and the flux constraint, and rounds the new state to FP32.  The state
+ * crosses the C ABI in FP64 as for every precision (cf_set_state rounds it,
+ * cf_get_state widens it); cf_step_host runs as cf_set_state + cf_step +
+ * cf_get_state, and cf_step_dt is not supported (CF_E_UNSUPPORTED). */
 #define CF_PRECISION_FP64 0
 #define CF_PRECISION_MIXED 1
 #define CF_PRECISION_MIXED_TC 2
 #define CF_PRECISION_MIXED_BF16 3
+#define CF_PRECISION_MIXED_F32STATE 4
 
 /* Nonlinear form of NonLinearTerm(...; form) (src/nonlinear.jl:11-17, 113-199).
  * ROTATIONAL: u x curl(u) with the modified pressure (the default);

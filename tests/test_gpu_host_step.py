@@ -76,7 +76,7 @@ def test_chained_host_steps_and_device_steps_agree(form):
     b.close()
 
 
-@pytest.mark.parametrize("precision", ["mixed", "mixed-tc"])
+@pytest.mark.parametrize("precision", ["mixed", "mixed-tc", "mixed-f32state"])
 def test_host_step_mixed(precision):
     dims = (16, 17, 16)
     a, b = make(dims, precision=precision), make(dims, precision=precision)
