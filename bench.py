@@ -723,6 +723,15 @@ def main():
     state_bytes = 4 * 16 * Nr
 
     diag = pb.diagnostics()
+    # the diagnostics recorded on the device after every step (cf_step_record,
+    # no host synchronisation between steps): their cost per evaluation
+    krec = max(2, min(args.steps, 5))
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record(stream)
+    t, _, _ = pb.advance_recorded(t, krec, 1)
+    r1.record(stream)
+    r1.synchronize()
+    rec_ms = r0.elapsed_time(r1) / krec
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -734,7 +743,10 @@ def main():
         "roofline": roofline,
         "clocks": clocks,
         "gpu_launches": launches,
-        "diagnostics": {"kinetic_energy": diag[0], "dissipation": diag[1], "max_div": diag[2]},
+        "diagnostics": {"kinetic_energy": diag[0], "dissipation": diag[1], "max_div": diag[2],
+                        "recorded_every_step": {"ms_per_step": rec_ms, "ms_per_evaluation": rec_ms - ms_per_step,
+                                                "how": "cf_step_record with every = 1 over %d steps, CUDA events"
+                                                       % krec}},
     }
     if prec != "fp64":
         # the timed precision's errors against an FP64 run of the same steps

@@ -51,7 +51,7 @@ EXPORTS = ["cf_create", "cf_destroy", "cf_set_constraint", "cf_set_state", "cf_g
            "cf_destroy_batch", "cf_batch_size", "cf_batch_instance", "cf_step_batch",
            "cf_batch_last_launch_count", "cf_batch_stream", "cf_cheb_transform", "cf_step_dt",
            "cf_step_host", "cf_power_input", "cf_device_bytes", "cf_set_wait_limit", "cf_cheb_transform_split",
-           "cf_batch_schedule"]
+           "cf_batch_schedule", "cf_step_record"]
 
 # return codes of cfb200.h
 CF_E_ARG, CF_E_SINGULAR, CF_E_NOMEM, CF_E_CUDA, CF_E_UNSUPPORTED, CF_E_NONFINITE = -1, -2, -3, -4, -5, -6
@@ -103,6 +103,7 @@ def lib():
         L.cf_stream.argtypes = [ctypes.c_void_p]
         L.cf_stream.restype = ctypes.c_void_p
         L.cf_power_input.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double, _D]
+        L.cf_step_record.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D, _D, _D]
         L.cf_device_bytes.argtypes = [ctypes.c_void_p]
         L.cf_device_bytes.restype = ctypes.c_longlong
         L.cf_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_long]
@@ -332,6 +333,21 @@ class ChannelFlowProblem:
         out = np.zeros(5)
         _check(lib().cf_diagnostics(self._h, _ptr(out)))
         return out
+
+    RECORD_COLUMNS = ("t", "kinetic_energy", "dissipation", "max_div", "wall_shear_upper", "wall_shear_lower",
+                      "dPdx", "dPdz", "power_input")
+
+    def advance_recorded(self, t, nsteps, every):
+        """Advance nsteps steps with the diagnostics recorded on the device
+        after every `every` steps (cf_step_record; no host synchronisation
+        between steps): returns (t + nsteps*dt, last gradients, rows), rows an
+        (nsteps // every, 9) array with the columns RECORD_COLUMNS."""
+        rows = np.zeros((int(nsteps) // int(every), 9)) if every > 0 else np.zeros((0, 9))
+        buf = rows if rows.size else np.zeros(9)
+        tout = ctypes.c_double()
+        g = np.zeros(2)
+        _check(lib().cf_step_record(self._h, float(t), int(nsteps), int(every), _ptr(buf), ctypes.byref(tout), _ptr(g)))
+        return tout.value, tuple(g), rows
 
     def power_input(self, pressuregradient=(0.0, 0.0), with_base=False):
         """power_input(U, nu; pressuregradient) (src/postprocessing.jl:113-128) of

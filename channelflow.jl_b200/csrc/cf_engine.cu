@@ -264,6 +264,8 @@ struct cf_engine {
     bool valid64 = true, valid32 = true;
     int* d_cheberr = nullptr;
     double* d_diag = nullptr;  // diagnostics accumulators
+    double* d_rec = nullptr;   // rows of diagnostics recorded between steps (cf_step_record)
+    int rec_cap = 0;           // rows d_rec holds
     double* d_diagpart = nullptr;  // diagnostics block partials (3 per column block)
     cudaGraphExec_t graph = nullptr;
     int last_launches = 0;
@@ -1795,6 +1797,76 @@ int cf_diagnostics(cf_handle* h, double* out) {
     out[2] = acc[2];
     out[3] = h->nu * acc[3];
     out[4] = h->nu * acc[4];
+    return CF_OK;
+}
+
+// One row of recorded diagnostics into acc[0..7] on the handle's stream, no
+// host synchronisation: the block partials of k_column_diag summed by
+// k_diag_reduce (acc[0..2]), the wall derivatives (acc[3..4]), the step's
+// last gradients (acc[5..6]) and the total-flow power input with those
+// gradients (acc[7]).
+static int record_diag(cf_engine* h, double* acc, int* count) {
+    int rc;
+    if ((rc = state_to64(h))) return rc;
+    ColParams p = col_params(h);
+    diag_kernel(h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p, acc, h->d_diagpart);
+    k_diag_reduce<<<1, 1024, 0, h->stream>>>(h->d_diagpart, (int)col_blocks(h), acc);
+    CU(cudaMemcpyAsync(acc + 5, h->d_grad, 2 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    k_power_input<<<1, 32, 0, h->stream>>>(h->U[0], h->U[2], h->d_base, (long)h->Nz * h->Nxh, h->Ny, h->nu, 0.0,
+                                           0.0, acc + 7, h->d_grad);
+    CU(cudaGetLastError());
+    *count += 3;
+    return CF_OK;
+}
+
+int cf_step_record(cf_handle* h, double t, int nsteps, int every, double* series, double* t_out,
+                   double* grads_out) {
+    if (!h || !series) return fail(CF_E_ARG, "null argument");
+    if (nsteps < 0 || every <= 0) return fail(CF_E_ARG, "nsteps must be nonnegative and every positive");
+    DeviceGuard dg_(h->device);
+    int rc;
+    const int nrec = nsteps / every;
+    if ((rc = ensure_diag(h))) return rc;
+    if (nrec > h->rec_cap) {
+        const int cap = std::max(nrec, 64);
+        if ((rc = dalloc(h, (void**)&h->d_rec, (size_t)cap * 8 * sizeof(double)))) return rc;
+        h->rec_cap = cap;
+    }
+    int cnt = 0;
+    double tc = t;
+    for (int r = 0; r < nrec; ++r) {
+        if ((rc = cf_step(h, tc, every, &tc, nullptr))) return rc;
+        cnt += h->last_launches;
+        if ((rc = record_diag(h, h->d_rec + 8L * r, &cnt))) return rc;
+    }
+    if (nsteps > nrec * every) {
+        if ((rc = cf_step(h, tc, nsteps - nrec * every, &tc, nullptr))) return rc;
+        cnt += h->last_launches;
+    }
+    std::vector<double> acc((size_t)nrec * 8);
+    if (nrec) CU(cudaMemcpyAsync(acc.data(), h->d_rec, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    double g[2];
+    CU(cudaMemcpyAsync(g, h->d_grad, 16, cudaMemcpyDeviceToHost, h->stream));
+    if ((rc = check_status(h))) return rc;
+    for (int r = 0; r < nrec; ++r) {
+        const double* a = acc.data() + 8L * r;
+        double* o = series + 9L * r;
+        o[0] = t + (double)(r + 1) * every * h->dt;
+        o[1] = a[0] / 2;
+        o[2] = h->nu * a[1];
+        o[3] = a[2];
+        o[4] = h->nu * a[3];
+        o[5] = h->nu * a[4];
+        o[6] = a[5];
+        o[7] = a[6];
+        o[8] = a[7];
+    }
+    h->last_launches = cnt;
+    if (t_out) *t_out = tc;
+    if (grads_out) {
+        grads_out[0] = g[0];
+        grads_out[1] = g[1];
+    }
     return CF_OK;
 }
 

@@ -980,6 +980,55 @@ CF_DEV double diag_form(const zd* a, const double* mom, const Team& t) {
     return warp_sum_d(s);
 }
 
+// The same form for a compile-time length, register-tiled over the upper
+// triangle of E x E blocks.  The nq indices of a parity form NB = ceil(nq/E)
+// blocks; the NB (NB + 1) / 2 block pairs (b <= c) are dealt to the lanes in
+// turn (pair k to lane k mod 32), so every lane does the same number of pairs
+// and no lane walks a longer triangle row than another.  A pair needs its 2E
+// coefficients, 2E - 1 Hankel moments mom[jb + ic + q + k] and 2E - 1
+// Toeplitz moments mom[|ic - jb - (E-1) + k|] (k = 0 .. 2E-2) for its E x E
+// terms (a moment load feeds E FMA pairs); an off-diagonal pair stands for
+// its mirror image too (M is symmetric: weight 2).  Indices past the table
+// are clamped to finite entries whose coefficients are zero.
+template <int PL>
+CF_DEV double diag_form_tiled(const zd* a, const double* mom, const Team& t) {
+    constexpr int E = run_max<PL>();
+    const int q = t.q, qo = q * t.hs, nq = pcount(q, t.P), P = t.P;
+    const int NB = (nq + E - 1) / E, npair = NB * (NB + 1) / 2;
+    double s = 0.0;
+    for (int k = t.lane; k < npair; k += 32) {
+        // row b of the triangle starts at pair b NB - b (b - 1) / 2
+        const double w = 2.0 * NB + 1.0;
+        int b = (int)((w - sqrt(w * w - 8.0 * k)) * 0.5);
+        while (b > 0 && b * NB - b * (b - 1) / 2 > k) --b;
+        while ((b + 1) * NB - (b + 1) * b / 2 <= k) ++b;
+        const int c = b + (k - (b * NB - b * (b - 1) / 2));
+        const int jb = b * E, ic = c * E;
+        double H[2 * E - 1], T[2 * E - 1];
+        zd aj[E], ai[E];
+#pragma unroll
+        for (int m = 0; m < 2 * E - 1; ++m) {
+            H[m] = mom[min(jb + ic + q + m, P)];
+            T[m] = mom[min(abs(ic - jb - (E - 1) + m), P)];
+        }
+#pragma unroll
+        for (int u = 0; u < E; ++u) {
+            aj[u] = (jb + u < nq) ? a[qo + jb + u] : zzero();
+            ai[u] = (ic + u < nq) ? a[qo + ic + u] : zzero();
+        }
+        double ps = 0.0;
+#pragma unroll
+        for (int d = 0; d < E; ++d) {
+            zd acc = zzero();
+#pragma unroll
+            for (int u = 0; u < E; ++u) acc = zaxpy(acc, H[d + u] + T[u - d + E - 1], ai[u]);
+            ps += aj[d].x * acc.x + aj[d].y * acc.y;  // Re(conj(a_j) sum_i (2 M_ji) a_i)
+        }
+        s += (b < c ? 2.0 : 1.0) * ps;
+    }
+    return 0.5 * warp_sum_d(s);
+}
+
 template <int NCOL, int PL>
 __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_diag(ColParams p,
                                                                                              double* acc,
@@ -1034,8 +1083,13 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
             const double w = X.ix == 0 ? 1.0 : 2.0;
 #pragma unroll 1
             for (int f = 0; f < 3; ++f) {
-                e += diag_form(sel3(U0, U1, U2, f), mom, t);
-                dis += diag_form(sel3(W0, W1, W2, f), mom, t);
+                if constexpr (PL != 0) {
+                    e += diag_form_tiled<PL>(sel3(U0, U1, U2, f), mom, t);
+                    dis += diag_form_tiled<PL>(sel3(W0, W1, W2, f), mom, t);
+                } else {
+                    e += diag_form(sel3(U0, U1, U2, f), mom, t);
+                    dis += diag_form(sel3(W0, W1, W2, f), mom, t);
+                }
             }
             e *= w;
             dis *= w;
@@ -1101,8 +1155,13 @@ static __global__ void __launch_bounds__(1024) k_diag_reduce(const double* __res
 // column (0,0) of the (Ny, Nz, Nxh) layout has stride Nz * Nxh.
 static __global__ void __launch_bounds__(32) k_power_input(const zd* __restrict__ u, const zd* __restrict__ w,
                                                          const double* __restrict__ base, long stride, int Ny,
-                                                         double nu, double gx, double gz, double* out) {
+                                                         double nu, double gx, double gz, double* out,
+                                                         const double* __restrict__ gdev = nullptr) {
     const int lane = threadIdx.x;
+    if (gdev) {  // the gradients from device memory (the step's own, recorded without a host round trip)
+        gx = gdev[0];
+        gz = gdev[1];
+    }
     double tot = 0.0;
 #pragma unroll 1
     for (int i = 0; i < 2; ++i) {

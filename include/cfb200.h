@@ -221,6 +221,19 @@ int cf_diagnostics(cf_handle* h, double* out);
  * laminar_power_input at :175-181 for a zero perturbation). */
 int cf_power_input(cf_handle* h, int with_base, double dPdx, double dPdz, double* out);
 
+/* step! repeated nsteps times (as cf_step) with the flow's diagnostics
+ * recorded on the device after every `every` steps, with no host
+ * synchronisation until the end: the monitoring a production run does
+ * between steps (`record`, examples/mkm590/run.jl:221-256, with the quantities of
+ * postprocessing.jl:80-128).  series receives nsteps/every rows of 9
+ * doubles: t, kinetic energy, dissipation rate, max |div u|, nu du/dy(+1) and
+ * nu du/dy(-1) of the (0,0) mode (cf_diagnostics' five values), the step's
+ * last mean gradients (dPdx, dPdz) and the total-flow power input with those
+ * gradients (cf_power_input with the base profile).  Waits for the steps;
+ * reports CF_E_NONFINITE as cf_step with grads_out does. */
+int cf_step_record(cf_handle* h, double t, int nsteps, int every, double* series, double* t_out,
+                   double* grads_out);
+
 /* step! like cf_step without the CUDA graph, with CUDA events around every
  * kernel class; kernel_ms[0..5] receives the summed device time of the
  * z-inverse, x-pass, z-forward and column kernels and (mixed precision) the
