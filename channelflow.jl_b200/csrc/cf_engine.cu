@@ -835,12 +835,22 @@ static FftParams fft_params32(const cf_engine* h) {
     f.stoff = (int)zstage_off(h, sizeof(zf));
     return f;
 }
+// FP32 x-pass: in place, one row per block, where the length has an in-place
+// plan (Nxp = 512, 576); else two rows per block between ping-pong buffers
+static void launch_xpass32(cf_engine* h, const FftParams& f) {
+    if (h->Nxp == 512 || h->Nxp == 576) {
+        const int bs = h->Nxp == 512 ? fft_bufsz_pos<2>(512) : fft_bufsz_pos<2>(576);
+        fft_kernel(KF_XPASS_IP, h->Nxp, true)<<<dim3((unsigned)h->Nzp, (unsigned)h->Ny), 256,
+                                                 3 * bs * sizeof(zf), h->stream>>>(f);
+        return;
+    }
+    dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
+    fft_kernel(KF_XPASS, h->Nxp, true)<<<gx, 256, xsmem(h) / 2, h->stream>>>(f);
+}
 static int launch_periodic32(cf_engine* h, int* count) {
     FftParams f = fft_params32(h);
-    const size_t smx = xsmem(h) / 2;  // complex float buffers
     launch_z(h, KF_ZINV, true, 6, f);
-    dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
-    fft_kernel(KF_XPASS, h->Nxp, true)<<<gx, 256, smx, h->stream>>>(f);
+    launch_xpass32(h, f);
     launch_z(h, KF_ZFWD, true, 3, f);
     if (count) *count += 3;
     CU(cudaGetLastError());
@@ -950,8 +960,6 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
     for (int k = 0; k < 7; ++k) CU(cudaEventCreate(&ev[k]));
     for (int k = 0; k < 6; ++k) kernel_ms[k] = 0.0;
     FftParams f = fft_params32(h);
-    const size_t smx = xsmem(h) / 2;
-    dim3 gx((unsigned)((h->Nzp + 1) / 2), (unsigned)h->Ny);
     const int order[6] = {0, 1, 2, 4, 3, 5};  // launch order -> kernel_ms slot
     for (int s = 0; s < nsteps && rc == CF_OK; ++s)
         for (int j = 0; j < 3 && rc == CF_OK; ++j) {
@@ -963,7 +971,7 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
             cudaEventRecord(ev[0], h->stream);
             launch_z(h, KF_ZINV, true, 6, f);
             cudaEventRecord(ev[1], h->stream);
-            fft_kernel(KF_XPASS, h->Nxp, true)<<<gx, 256, smx, h->stream>>>(f);
+            launch_xpass32(h, f);
             cudaEventRecord(ev[2], h->stream);
             launch_z(h, KF_ZFWD, true, 3, f);
             cudaEventRecord(ev[3], h->stream);

@@ -52,10 +52,21 @@ __host__ __device__ constexpr int fft_bufsz(int L) { return ((L + (L >> 3) + 1) 
 // e are XOR-ed with bits 3-5 and 6-8, spreading the strided stores over the
 // bank groups as well, at a few more integer operations per access.
 CF_DEV int swz(int e) { return e ^ (((e >> 3) ^ (e >> 6)) & 7); }
-// position of element e in a buffer of layout POS (0 padded, 1 XOR-swizzled)
+// The padded layout for 8-byte (complex float) elements: one pad slot after
+// every 16 elements.  A warp's 8-byte accesses at a stride of 8 elements then
+// fall on distinct bank pairs (the 1-in-8 padding leaves them 2-way
+// conflicted for 8-byte elements).
+CF_DEV int fpos16(int e) { return e + (e >> 4); }
+// position of element e in a buffer of layout POS (0 padded 1 in 8, 1
+// XOR-swizzled, 2 padded 1 in 16)
 template <int POS>
 CF_DEV int bpos(int e) {
-    return POS ? swz(e) : fpos(e);
+    return POS == 1 ? swz(e) : (POS == 2 ? fpos16(e) : fpos(e));
+}
+// complex slots a transform buffer of length L occupies in layout POS
+template <int POS>
+__host__ __device__ constexpr int fft_bufsz_pos(int L) {
+    return POS == 2 ? ((L + (L >> 4) + 1) + 7) & ~7 : (POS == 1 ? (L + 7) & ~7 : fft_bufsz(L));
 }
 
 template <class Z>
@@ -352,11 +363,50 @@ CF_DEV void fft_static_ip(Z* buf, int nb, int bs, const Z* tw, int sgn, int tid,
     fft_pass_static_ip<BLOCK, POS, L, Ns, R>(buf, nb, bs, tw, sgn, tid, nth, bar);
     if constexpr (sizeof...(Rest) > 0) fft_static_ip<Z, BLOCK, POS, L, Ns * R, Rest...>(buf, nb, bs, tw, sgn, tid, nth, bar);
 }
+// First pass (Ns = 1) of an in-place transform whose inputs come from a
+// functor instead of the buffer: thread (b, j), b < nb, j < L/R, takes
+// get(b, j + r L/R) for r < R (from global memory, or computed from other
+// buffers), and writes its R outputs to positions R j + r of transform b, as
+// fft_pass_static_ip's first pass does after reading them from the buffer.
+// The inputs never pass through shared memory: no staging pass, no barrier
+// before the first pass.  read_buf: get reads the buffer itself, so a group
+// barrier separates the reads from the writes.  Ends with a group barrier.
+template <bool BLOCK, int POS, int L, int R, class Z, class Get>
+CF_DEV void fft_pass_first_ip(Z* buf, int nb, int bs, int sgn, int tid, int nth, int bar, bool read_buf,
+                              const Get& get) {
+    constexpr int NBf = L / R;
+    constexpr bool LIN_ST = POS == 0 && (8 % R == 0);
+    const bool act = tid < nb * NBf;
+    const int b = act ? tid / NBf : 0, j = tid - b * NBf;
+    Z v[R];
+    if (act) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = get(b, j + r * NBf);
+        dft_small<R>(v, sgn);
+    }
+    if (read_buf) group_sync<BLOCK>(bar, nth);
+    if (act) {
+        Z* d = buf + (long)b * bs;
+        const int po = bpos<POS>(R * j);
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[LIN_ST ? po + r : bpos<POS>(R * j + r)] = v[r];
+    }
+    group_sync<BLOCK>(bar, nth);
+}
+
 // lengths with an in-place plan, and the most butterflies of one transform's
 // passes (nb times it must not exceed the group's threads)
 template <int L>
 __host__ __device__ constexpr int fft_ip_butterflies() {
     return L == 512 ? 64 : (L == 576 ? 72 : 0);
+}
+// The passes after a first radix-8 pass (fft_pass_first_ip) of the in-place plans.
+template <bool BLOCK, int L, int POS = 0, class Z>
+CF_DEV void group_fft_ip_rest8(Z* a, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {
+    static_assert(L == 512 || L == 576, "no in-place plan for this length");
+    const Z* tw = plan_tw<Z>(pl);
+    if constexpr (L == 512) fft_static_ip<Z, BLOCK, POS, 512, 8, 8, 8>(a, nb, bs, tw, sgn, tid, nth, bar);
+    else fft_static_ip<Z, BLOCK, POS, 576, 8, 8, 9>(a, nb, bs, tw, sgn, tid, nth, bar);
 }
 template <bool BLOCK, int L, int POS = 0, class Z>
 CF_DEV void group_fft_ip(Z* a, int nb, int bs, const FftPlan& pl, int sgn, int tid, int nth, int bar) {

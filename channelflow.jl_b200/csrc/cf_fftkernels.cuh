@@ -29,6 +29,10 @@
 #ifndef CF_XPASS_IP_KPT
 #define CF_XPASS_IP_KPT 1
 #endif
+#ifndef CF_XPASS_IP32_BLOCKS
+#define CF_XPASS_IP32_BLOCKS 5
+#endif
+
 
 struct FftParams {
     int Nx, Nz, Nxh, Ny, Nzp, Nxp;
@@ -475,37 +479,44 @@ CF_DEV void xpass_row_body(const FftParams& p, int z, int n) {
 // The same with the transforms in place (lengths with an in-place plan, whose
 // butterflies fit the block's threads: 3 x 72 at Nxp = 576): three slots of
 // fft_bufsz(Nxp), half the shared memory, so more blocks fit per SM.  The
-// product at x point j reads and writes slots 0-2 at j only (one thread per
-// j), so it runs in place without a barrier of its own.
-template <int LX>
+// products n = u x omega are formed inside the first forward pass, from the
+// three inverse-transformed slots, instead of in a pass of their own (the
+// same arithmetic, one read-write sweep and one barrier fewer: 2.21 -> 2.15
+// ms at 384x257x384).  Loading the packed spectra straight into the first
+// inverse pass as well was measured slower (2.44 ms: every mode is then
+// loaded twice, for k and Nxp - k, and the loads in flight spill registers).
+// Z = zd (FP64, layout POS 0) or zf (the mixed forms' FP32 transforms, layout
+// POS 2: padded 1 in 16, conflict-free for 8-byte elements).
+template <int LX, class Z = zd, int POS = 0>
 CF_DEV void xpass_row_ip_body(const FftParams& p, int z, int n) {
     static_assert(3 * fft_ip_butterflies<LX>() <= 256, "one butterfly per thread");
     extern __shared__ __align__(128) unsigned char fsm_raw[];
-    zd* sm = reinterpret_cast<zd*>(fsm_raw);
-    const int Nxh = p.Nxh, bs = p.bsxp;
+    Z* sm = reinterpret_cast<Z*>(fsm_raw);
+    constexpr int bs = fft_bufsz_pos<POS>(LX);
+    const int Nxh = p.Nxh;
     const long row = ((long)n * p.Nzp + z) * Nxh;
     const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1;
-    xpack<zd, 0, 3, false, CF_XPASS_IP_KPT>(sm, bs, Nxh, LX, xnyq, [&](int slot, int k, zd& X, zd& Y) {
-        X = zp_of<zd>(p, 2 * slot)[row + k];
-        Y = zp_of<zd>(p, 2 * slot + 1)[row + k];
+    xpack<Z, POS, 3, false, CF_XPASS_IP_KPT>(sm, bs, Nxh, LX, xnyq, [&](int slot, int k, Z& X, Z& Y) {
+        X = zp_of<Z>(p, 2 * slot)[row + k];
+        Y = zp_of<Z>(p, 2 * slot + 1)[row + k];
     });
     __syncthreads();
-    group_fft_ip<true, LX, 0>(sm, 3, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
-    for (int j = threadIdx.x; j < LX; j += blockDim.x) {
-        const int sj = fpos(j);
-        const zd a0 = sm[sj], a1 = sm[bs + sj], a2 = sm[2 * bs + sj];
-        // u = (a0.x, a0.y, a1.x), omega = (a1.y, a2.x, a2.y)
-        sm[sj] = zmake(a0.y * a2.y - a1.x * a2.x, a1.x * a1.y - a0.x * a2.y);
-        sm[bs + sj] = zmake(a0.x * a2.x - a0.y * a1.y, 0.0);
-    }
-    __syncthreads();
-    group_fft_ip<true, LX, 0>(sm, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
-    xunpack<zd, 0, 2, false>(sm, bs, Nxh, LX, [&](int slot, int k, zd X, zd Y) {
+    group_fft_ip<true, LX, POS>(sm, 3, bs, p.plX, +1, threadIdx.x, blockDim.x, 0);
+    // u = (a0.x, a0.y, a1.x), omega = (a1.y, a2.x, a2.y); slots (n0 + i n1, n2)
+    auto product = [&](int s, int x) -> Z {
+        const int sx = bpos<POS>(x);
+        const Z a0 = sm[sx], a1 = sm[bs + sx], a2 = sm[2 * bs + sx];
+        if (s == 0) return cmake<Z>(a0.y * a2.y - a1.x * a2.x, a1.x * a1.y - a0.x * a2.y);
+        return cmake<Z>(a0.x * a2.x - a0.y * a1.y, 0.0);
+    };
+    fft_pass_first_ip<true, POS, LX, 8>(sm, 2, bs, -1, threadIdx.x, blockDim.x, 0, true, product);
+    group_fft_ip_rest8<true, LX, POS>(sm, 2, bs, p.plX, -1, threadIdx.x, blockDim.x, 0);
+    xunpack<Z, POS, 2, false>(sm, bs, Nxh, LX, [&](int slot, int k, Z X, Z Y) {
         if (slot == 0) {
-            zp_of<zd>(p, 0)[row + k] = X;
-            zp_of<zd>(p, 1)[row + k] = Y;
+            zp_of<Z>(p, 0)[row + k] = X;
+            zp_of<Z>(p, 1)[row + k] = Y;
         } else {
-            zp_of<zd>(p, 2)[row + k] = X;
+            zp_of<Z>(p, 2)[row + k] = X;
         }
     });
 }
@@ -731,6 +742,11 @@ __global__ void __launch_bounds__(256, (sizeof(Z) == 16 ? 3 : 4)) k_xpass(FftPar
 template <int LX>
 __global__ void __launch_bounds__(256, CF_XPASS_IP_BLOCKS) k_xpass_ip(FftParams p) {
     if constexpr (fft_ip_butterflies<LX>() > 0) xpass_row_ip_body<LX>(p, blockIdx.x, blockIdx.y);
+}
+// the same in FP32 (mixed forms): 14.8 KB of shared memory at Nxp = 576
+template <int LX>
+__global__ void __launch_bounds__(256, CF_XPASS_IP32_BLOCKS) k_xpass_ip32(FftParams p) {
+    if constexpr (fft_ip_butterflies<LX>() > 0) xpass_row_ip_body<LX, zf, 2>(p, blockIdx.x, blockIdx.y);
 }
 template <int LX>
 __global__ void __launch_bounds__(256) k_xpass2(FftParams p) {

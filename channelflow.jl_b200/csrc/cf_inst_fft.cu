@@ -14,7 +14,7 @@ FftKernel fft_kernel_for(int which, bool f32) {
         case KF_XPASS_CONV: return k_xpass_conv<L>;
         case KF_XPASS_DIV: return k_xpass_div<L>;
         case KF_XPASS2: return k_xpass2<L>;
-        case KF_XPASS_IP: return k_xpass_ip<L>;
+        case KF_XPASS_IP: return f32 ? k_xpass_ip32<L> : k_xpass_ip<L>;
         case KF_XPASS_CONV_IP: return k_xpass_conv_ip<L>;
         case KF_XPASS_DIV_IP: return k_xpass_div_ip<L>;
         default: return f32 ? k_xpass<L, zf> : k_xpass<L, zd>;
