@@ -219,6 +219,12 @@ struct cf_engine {
     // TMA row transfers of the z kernels (maps of the FP64 and the FP32 fields)
     FftMaps maps64, maps32;
     bool tma64 = false, tma32 = false;
+    // columns per block of the FP32 z-inverse without TMA: twice the FP64
+    // groups' (rows of 8-byte elements gathered in segments as long as the
+    // FP64 kernels'; measured 1.31 -> 1.02 ms at 384x257x384, while the
+    // z-forward, whose stores are the strided side, is faster at tkz: 0.54
+    // against 0.66 ms)
+    int tkz32 = 0;
     int zbox = 0, zpbox = 0;  // rows per TMA box (nodal, z-padded)
     // status words written by the kernels, read and cleared by check_status:
     // [0] a TMA wait of a z kernel gave up, [1] a tensor-core wait gave up,
@@ -323,6 +329,8 @@ static int rup8(int x) { return (x + 7) & ~7; }
 // unpacking and multi-transform FFT passes are free of bank conflicts
 // (simulated: 1.22 wavefronts per ideal one at tkz = 2 with the odd stride).
 static int zbs(const cf_engine* h) { return fft_bufsz(h->Nzp) + (8 / h->tkz) % 8; }
+static int zbs_t(const cf_engine* h, int tkz) { return fft_bufsz(h->Nzp) + (8 / tkz) % 8; }
+static size_t zsmem_t(const cf_engine* h, int tkz, size_t es) { return (size_t)2 * tkz * zbs_t(h, tkz) * es; }
 static int xbs(const cf_engine* h) { return rup8(h->Nxp); }
 static size_t zsmem(const cf_engine* h) { return (size_t)2 * h->tkz * zbs(h) * sizeof(zd); }
 // TMA z kernels: the first transform buffer, then (128-aligned) the second,
@@ -588,11 +596,19 @@ static FftParams fft_params(const cf_engine* h) {
 // the TMA kernels when the maps could be encoded, else the gather kernels
 static void launch_z(cf_engine* h, int which, bool f32, int nf, const FftParams& f) {
     const dim3 g((unsigned)((h->Nxh + h->tkz - 1) / h->tkz), (unsigned)h->Ny, (unsigned)nf);
-    if (f32 ? h->tma32 : h->tma64)
+    if (f32 ? h->tma32 : h->tma64) {
         fft_tma_kernel(which, h->Nzp, f32)<<<g, 256, zsmem_tma(h, f32 ? sizeof(zf) : sizeof(zd)), h->stream>>>(
             f, f32 ? h->maps32 : h->maps64);
-    else
-        fft_kernel(which, h->Nzp, f32)<<<g, 256, f32 ? zsmem(h) / 2 : zsmem(h), h->stream>>>(f);
+    } else if (f32) {
+        const int t = which == KF_ZINV ? h->tkz32 : h->tkz;
+        FftParams ft = f;
+        ft.tks = ilog2(t);
+        ft.bsz = zbs_t(h, t);
+        const dim3 g32((unsigned)((h->Nxh + t - 1) / t), (unsigned)h->Ny, (unsigned)nf);
+        fft_kernel(which, h->Nzp, true)<<<g32, 256, zsmem_t(h, t, sizeof(zf)), h->stream>>>(ft);
+    } else {
+        fft_kernel(which, h->Nzp, false)<<<g, 256, zsmem(h), h->stream>>>(f);
+    }
 }
 
 // Launch shapes of the periodic transforms of the handle's nonlinear form:
@@ -1073,6 +1089,11 @@ static void encode_maps(cf_engine* h) {
         for (int i = 0; i < 6 && ok; ++i) ok = encode_field(h, &h->maps32.zp[i], h->zp32[i], h->Nzp, h->zpbox, true);
         h->tma32 = ok && zstage_rows(h) <= zbs(h) && zsmem_tma(h, sizeof(zf)) <= (size_t)227 * 1024;
     }
+    h->tkz32 = h->tkz;
+    if (h->mixed && !h->tma32) {
+        const int t = std::min(2 * h->tkz, 32);
+        if ((size_t)2 * t * zbs_t(h, t) * sizeof(zf) <= (size_t)74 * 1024) h->tkz32 = t;
+    }
 }
 
 // Raise a kernel's dynamic shared-memory limit to at least `need`.  The limit
@@ -1115,8 +1136,8 @@ static int set_attrs(cf_engine* h) {
         if ((rc = raise_smem_limit(fft_tma_kernel(KF_ZFWD, h->Nzp, true), zsmem_tma(h, sizeof(zf))))) return rc;
     }
     if (h->mixed) {
-        if ((rc = raise_smem_limit(fft_kernel(KF_ZINV, h->Nzp, true), need[1] / 2))) return rc;
-        if ((rc = raise_smem_limit(fft_kernel(KF_ZFWD, h->Nzp, true), need[1] / 2))) return rc;
+        if ((rc = raise_smem_limit(fft_kernel(KF_ZINV, h->Nzp, true), zsmem_t(h, h->tkz32, sizeof(zf))))) return rc;
+        if ((rc = raise_smem_limit(fft_kernel(KF_ZFWD, h->Nzp, true), zsmem_t(h, h->tkz, sizeof(zf))))) return rc;
         if ((rc = raise_smem_limit(fft_kernel(KF_XPASS, h->Nxp, true), need[2] / 2))) return rc;
     }
     if (h->mixed && h->tc) {
