@@ -553,9 +553,19 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         } else {
             if (p.stage > 0) tile_load_async<NCOL, PL>(X.reg(qreg), cs, hs, Q_i, c0, p.Ny, p.B);
             tile_load_async<NCOL, PL>(X.reg(ureg), cs, hs, U_i, c0, p.Ny, p.B);
-            if (F32) tile_load<NCOL, PL>(X.reg(4), cs, hs, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
-            else tile_load_async<NCOL, PL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
-            tile_wait();
+            if (F32) {
+                // the FP32 term copied into the (still free) transform
+                // buffers beside the FP64 tiles, then widened into region 4
+                zf* st = reinterpret_cast<zf*>(X.reg(6));
+                tile_stage32<NCOL>(st, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
+                cp_async_commit();
+                tile_wait();
+                __syncthreads();
+                tile_widen<NCOL>(X.reg(4), cs, hs, st, p.Ny, c0, nullptr);
+            } else {
+                tile_load_async<NCOL, PL>(X.reg(4), cs, hs, Nn_i, c0, p.Ny, p.B);
+                tile_wait();
+            }
         }
         __syncthreads();
         if (valid) {
