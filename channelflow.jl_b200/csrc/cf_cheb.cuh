@@ -349,3 +349,311 @@ __global__ void __launch_bounds__(128, 1) k_cheb_mma(ChebParams p) {
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
 }
+
+// ---- the transform folded by the symmetry of the DCT-I, persistent ------------
+// T[n][P-k] = (-1)^n T[n][k] (the cosine's reflection; the endpoint weights
+// are symmetric), so with S_k = X_k + X_{P-k} (k < P/2), S_{P/2} = X_{P/2},
+// and D_k = X_k - X_{P-k} (k < P/2), H = P/2:
+//   Y[2m]   = sum_{k=0}^{H}   T[2m][k]   S_k      (H + 1 outputs, H + 1 inputs)
+//   Y[2m+1] = sum_{k=0}^{H-1} T[2m+1][k] D_k      (H outputs, H inputs)
+// (T[2m+1][H] = cos(pi (2m+1) / 2) = 0): two products of half the size, half
+// the MMAs of the full one.  Each CTA owns one parity q (its folded T^T
+// resident in shared memory for the whole launch, loaded once) and walks the
+// items (field, tile of 128 columns) of its pair of CTAs; the even and odd
+// CTAs of a pair take the same items in the same order, so the second read of
+// a tile's X rows comes from L2.
+//   warps 0-7  producers: thread t takes column t % 128 of the tile and
+//              half t / 128 of a K-step's 16 inputs (8 inputs and their
+//              mirrors, so two threads per column keep twice the loads in
+//              flight); forms S or D, splits the operand (TF32 head and
+//              remainder, or three BF16 pieces), writes it into a stage of
+//              the A ring and arrives on the stage's full barrier
+//   warp 12    one thread issues the MMAs of a stage when it is full and
+//              commits to its empty barrier; after an item's last K-step it
+//              commits to the item's accumulator barrier.  Two accumulators
+//              (TMEM columns 0 and 256) let an item's MMAs run while the
+//              previous item is read out.  The warp also owns the TMEM
+//              allocation (512 columns: one CTA per SM).
+//   warps 8-11 epilogue: warp w reads TMEM lanes 32 (w - 8) .. +31 (its
+//              columns of the tile), writes rows 2m + q of Y, and releases
+//              the accumulator.
+// Every wait is bounded: a wait that gives up sets p.err and the shared
+// abort flag, every role leaves its loop, and the MMA thread waits for its
+// MMAs in flight (one final commit) before the TMEM is freed.
+struct ChebSymParams {
+    int P;                 // Ny - 1 (even)
+    int N[2], Npad[2];     // outputs per parity (H + 1, H) and the MMA N (multiple of 16, <= 256)
+    int Kpad[2];           // inputs per parity padded to K-steps of 16
+    int nst;               // A stages
+    long C;                // real columns per field
+    int nf, ntiles;        // fields, tiles of 128 columns per field
+    const float* X[CF_CHEB_MAXF];
+    float* Y[CF_CHEB_MAXF];
+    const unsigned char* B[2];  // folded T^T images per parity: pieces back to back, bbytes[q] each
+    unsigned bbytes[2];
+    int* err;
+    long spins;
+};
+
+template <int SPLIT>
+__host__ __device__ constexpr unsigned cheb_sym_apiece() {
+    return 128u * 16u * (SPLIT ? 2u : 4u);  // one A piece of a K-step (128 columns x 16 inputs)
+}
+
+template <int SPLIT>
+__global__ void __launch_bounds__(416, 1) k_cheb_sym(ChebSymParams p) {
+    using S = ChebSplit<SPLIT>;
+    constexpr int NPC = S::NPC;
+    constexpr int EPC = 16 / S::ES;  // inputs per 16-byte chunk
+    constexpr unsigned APB = cheb_sym_apiece<SPLIT>();
+    extern __shared__ __align__(1024) unsigned char csm[];
+    const int q = blockIdx.x & 1, pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int P = p.P, H = P >> 1;
+    const int Npad = p.Npad[q], Nq = p.N[q], nks = p.Kpad[q] / 16, nst = p.nst;
+    const unsigned BPB = p.bbytes[q];
+    const unsigned BPBmax = p.bbytes[0] > p.bbytes[1] ? p.bbytes[0] : p.bbytes[1];
+    unsigned char* Bs = csm;
+    unsigned char* As = csm + NPC * BPBmax;
+    uint64_t* full = reinterpret_cast<uint64_t*>(As + (size_t)nst * NPC * APB);
+    uint64_t* empty = full + nst;
+    uint64_t* accf = empty + nst;
+    uint64_t* acce = accf + 2;
+    uint64_t* fin = acce + 2;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+    const long C = p.C;
+    const int nitems = p.nf * p.ntiles;
+
+    if (warp == 12) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < nst; ++s) {
+            mbar_init(smem_u32(full + s), 256);
+            mbar_init(smem_u32(empty + s), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(accf + b), 1);
+            mbar_init(smem_u32(acce + b), 128);
+        }
+        mbar_init(smem_u32(fin), 1);
+        *abort_flag = 0;
+    }
+    // the folded T^T of this parity, resident for the whole launch
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(p.B[q]);
+        uint4* dst = reinterpret_cast<uint4*>(Bs);
+        const int n16 = (int)(NPC * BPB / 16);
+        for (int i = tid; i < n16; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    fence_async_smem();
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const long spins = p.spins;
+
+    if (warp < 8) {
+        // ---------------- producers
+        // The items' K-steps form one sequence; the 16 X values of the step
+        // after next are requested into registers before the current one is
+        // folded, split and written, so two steps' loads are in flight while
+        // a step is converted.  Step, item and stage counters advance incrementally (no
+        // divisions in the loop).
+        const int col = tid & 127, half = tid >> 7;
+        const int nitm = nitems > pair ? (nitems - pair + npairs - 1) / npairs : 0;
+        const int nsteps = nitm * nks;
+        // the step to load next: item itl, K-step ksl, its row pointer base and column
+        int itl = pair, ksl = 0;
+        const float* Xl = nullptr;
+        long cl = 0;
+        bool cinl = false;
+        auto item_cols = [&](int it) {
+            const int f = it / p.ntiles;
+            Xl = p.X[f];
+            cl = (long)(it - f * p.ntiles) * 128 + col;
+            cinl = cl < C;
+        };
+        auto load_next = [&](float* a, float* b) {
+            if (ksl == 0) item_cols(itl);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int k = 16 * ksl + 8 * half + r;
+                a[r] = (cinl && k <= H) ? __ldg(Xl + (long)k * C + cl) : 0.0f;
+                b[r] = (cinl && k < H) ? __ldg(Xl + (long)(P - k) * C + cl) : 0.0f;
+            }
+            if (++ksl == nks) {
+                ksl = 0;
+                itl += npairs;
+            }
+        };
+        // three steps in registers: the current one and the next two in flight
+        float ca[8], cb[8], na[8], nb[8], ma[8], mb[8];
+        if (nsteps > 0) load_next(ca, cb);
+        if (nsteps > 1) load_next(na, nb);
+        int ks = 0, s = 0, u = 0;
+        for (int g = 0; g < nsteps && !*abort_flag; ++g) {
+            if (g + 2 < nsteps) load_next(ma, mb);
+            float v[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int k = 16 * ks + 8 * half + r;
+                v[r] = q == 0 ? ca[r] + cb[r] : (k < H ? ca[r] - cb[r] : 0.0f);
+            }
+            if (u >= 1 && !mbar_wait(smem_u32(empty + s), (uint32_t)((u - 1) & 1), spins)) {
+                *abort_flag = 1;
+                atomicExch(p.err, 1);
+                break;
+            }
+            unsigned char* Ast = As + (size_t)s * NPC * APB;
+            if constexpr (SPLIT == 0) {
+                // chunks 2 half, 2 half + 1 (four inputs each)
+#pragma unroll
+                for (int jj = 0; jj < 2; ++jj) {
+                    const float* w = v + 4 * jj;
+                    float4 h = make_float4(tf32_round(w[0]), tf32_round(w[1]), tf32_round(w[2]), tf32_round(w[3]));
+                    float4 l = make_float4(tf32_round(w[0] - h.x), tf32_round(w[1] - h.y), tf32_round(w[2] - h.z),
+                                           tf32_round(w[3] - h.w));
+                    const unsigned o = ((2 * half + jj) * 128 + col) * 16;
+                    *reinterpret_cast<float4*>(Ast + o) = h;
+                    *reinterpret_cast<float4*>(Ast + APB + o) = l;
+                }
+            } else {
+                // chunk half (eight inputs)
+                uint32_t w[3][4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    uint16_t a0, a1, a2, b0, b1, b2;
+                    bf16_split3(v[2 * e], a0, a1, a2);
+                    bf16_split3(v[2 * e + 1], b0, b1, b2);
+                    w[0][e] = (uint32_t)a0 | ((uint32_t)b0 << 16);
+                    w[1][e] = (uint32_t)a1 | ((uint32_t)b1 << 16);
+                    w[2][e] = (uint32_t)a2 | ((uint32_t)b2 << 16);
+                }
+                const unsigned o = (half * 128 + col) * 16;
+#pragma unroll
+                for (int pc = 0; pc < 3; ++pc)
+                    *reinterpret_cast<uint4*>(Ast + pc * APB + o) = make_uint4(w[pc][0], w[pc][1], w[pc][2], w[pc][3]);
+            }
+            fence_async_smem();
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(full + s)) : "memory");
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                ca[r] = na[r];
+                cb[r] = nb[r];
+                na[r] = ma[r];
+                nb[r] = mb[r];
+            }
+            if (++ks == nks) ks = 0;
+            if (++s == nst) {
+                s = 0;
+                ++u;
+            }
+        }
+    } else if (warp < 12) {
+        // ---------------- epilogue
+        const int ew = warp - 8;
+        int li = 0;
+        for (int it = pair; it < nitems && !*abort_flag; it += npairs, ++li) {
+            const int bsel = li & 1;
+            if (!mbar_wait(smem_u32(accf + bsel), (uint32_t)((li >> 1) & 1), spins)) {
+                *abort_flag = 1;
+                atomicExch(p.err, 1);
+                break;
+            }
+            tc_fence_after();
+            const int f = it / p.ntiles;
+            const long c = (long)(it - f * p.ntiles) * 128 + 32 * ew + lane;
+            float* Y = p.Y[f];
+            const uint32_t ta = tmem + ((uint32_t)(32 * ew) << 16) + (uint32_t)(bsel * 256);
+            for (int n0 = 0; n0 < Npad; n0 += 16) {
+                float v[16];
+                tmem_ld16(ta + (uint32_t)n0, v);
+                if (c < C) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const int m = n0 + i;
+                        if (m < Nq) Y[(long)(2 * m + q) * C + c] = v[i];
+                    }
+                }
+            }
+            tc_fence_before();
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(acce + bsel)) : "memory");
+        }
+    } else if (lane == 0) {
+        // ---------------- MMA issue
+        const int kstep = SPLIT ? 16 : 8;  // K per MMA
+        const uint32_t idesc = SPLIT ? umma_idesc_bf16(128, Npad) : umma_idesc_tf32(128, Npad);
+        int s = 0, u = 0;  // stage of the next fill consumed, and its use
+        int li = 0;
+        bool issued = false;
+        for (int it = pair; it < nitems && !*abort_flag; it += npairs, ++li) {
+            const int bsel = li & 1;
+            if (li >= 2 && !mbar_wait(smem_u32(acce + bsel), (uint32_t)(((li >> 1) - 1) & 1), spins)) {
+                *abort_flag = 1;
+                atomicExch(p.err, 1);
+                break;
+            }
+            tc_fence_after();
+            const uint32_t d = tmem + (uint32_t)(bsel * 256);
+            bool ok = true;
+            for (int ks = 0; ks < nks; ++ks) {
+                if (!mbar_wait(smem_u32(full + s), (uint32_t)(u & 1), spins)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t abase = smem_u32(As + (size_t)s * NPC * APB);
+                for (int kk = 0; kk < 16 / kstep; ++kk) {
+                    const uint32_t aoff = kk * (kstep / EPC) * 128 * 16;
+                    const uint32_t boff = (uint32_t)((16 * ks + kk * kstep) / EPC) * Npad * 16;
+                    uint64_t ad[NPC], bd[NPC];
+#pragma unroll
+                    for (int pc = 0; pc < NPC; ++pc) {
+                        ad[pc] = umma_desc(abase + pc * APB + aoff, 128 * 16, 128);
+                        bd[pc] = umma_desc(smem_u32(Bs + pc * BPB) + boff, Npad * 16, 128);
+                    }
+                    const uint32_t acc0 = (ks > 0 || kk > 0) ? 1u : 0u;
+                    if constexpr (SPLIT == 0) {
+                        umma_tf32(d, ad[0], bd[0], idesc, acc0);
+                        umma_tf32(d, ad[0], bd[1], idesc, 1u);
+                        umma_tf32(d, ad[1], bd[0], idesc, 1u);
+                    } else {
+                        umma_f16(d, ad[0], bd[0], idesc, acc0);
+                        umma_f16(d, ad[0], bd[1], idesc, 1u);
+                        umma_f16(d, ad[1], bd[0], idesc, 1u);
+                        umma_f16(d, ad[0], bd[2], idesc, 1u);
+                        umma_f16(d, ad[1], bd[1], idesc, 1u);
+                        umma_f16(d, ad[2], bd[0], idesc, 1u);
+                    }
+                }
+                issued = true;
+                umma_commit(smem_u32(empty + s));
+                if (++s == nst) {
+                    s = 0;
+                    ++u;
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                atomicExch(p.err, 1);
+                break;
+            }
+            umma_commit(smem_u32(accf + bsel));
+        }
+        // every MMA issued by this thread is complete before the TMEM is freed
+        if (issued) {
+            umma_commit(smem_u32(fin));
+            if (!mbar_wait(smem_u32(fin), 0)) atomicExch(p.err, 1);
+        }
+    }
+    __syncwarp();  // warp 12 reconverges (lane 0 issued the MMAs)
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 12) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+}

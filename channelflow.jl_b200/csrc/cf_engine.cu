@@ -195,6 +195,13 @@ static void parallel_for(long n, F f) {
 // ===========================================================================
 // Engine
 // ===========================================================================
+// sizes of the folded tensor-core Chebyshev transform (cheb_sym_dims)
+struct ChebSymDims {
+    int N[2], Npad[2], Kpad[2], nst;
+    unsigned bbytes[2];
+    size_t smem;
+};
+
 struct DevBank {
     double *fac_p = nullptr, *fac_v = nullptr, *resp = nullptr, *colsc = nullptr, *sa = nullptr, *meanc = nullptr;
     double meanc_mean = 0.0, nu = 0.0, lambda = 0.0;
@@ -260,6 +267,8 @@ struct cf_engine {
     unsigned char *d_chebF = nullptr, *d_chebI = nullptr;  // transform-matrix images, pieces back to back
     int split = 0;  // tensor-core operand split: 0 TF32 head and remainder, 1 three BF16 pieces
     int chebNP = 0, chebKT = 0;
+    bool chebsym = false;  // the folded, persistent transform (k_cheb_sym) is used
+    ChebSymDims symd;
     // CF_PRECISION_MIXED_F32STATE: the state the steps advance lives in
     // U32, P32, Q32 (complex float); U and Pf keep the FP64 copy that the
     // state entry points read and write.  valid64 / valid32: which copy is
@@ -757,6 +766,7 @@ static void drop_graph(cf_engine* h) {
 // inverse Chebyshev transform of the six fields on the tensor cores, in place.
 // ---------------------------------------------------------------------------
 typedef void (*ChebKernel)(ChebParams);
+typedef void (*ChebSymKernel)(ChebSymParams);
 static void cheb_images(int Ny, int inverse, double scale, int split, std::vector<unsigned char>& img, int& NP,
                         int& nkt);
 static size_t cheb_smem(int NPs, int split);
@@ -765,6 +775,11 @@ static void cheb_dims(int Ny, int& NPs, int& nsplit, int& NP);
 static int cheb_pieces(int split);
 static size_t cheb_piece_bytes(int Ny, int split);
 static ChebKernel cheb_kernel(int split);
+static bool cheb_sym_dims(int Ny, int split, ChebSymDims& d);
+static void cheb_sym_images(int Ny, int inverse, double scale, int split, const ChebSymDims& d,
+                            std::vector<unsigned char>& img);
+static ChebSymKernel cheb_sym_kernel(int split);
+static int cheb_sym_grid(long C, int nf);
 
 // ---- FP32 state (CF_PRECISION_MIXED_F32STATE): the FP64 copy of U and P
 // and the FP32 state the steps advance, converted on demand.
@@ -877,6 +892,35 @@ static int launch_periodic32(cf_engine* h, int* count) {
 // nodal values, nod32).  Out of place: the two blocks that share a column tile
 // when the output degrees are split both read all of its input rows.
 static int launch_cheb(cf_engine* h, int nf, bool inverse, int* count) {
+    if (h->chebsym) {
+        ChebSymParams q;
+        std::memset(&q, 0, sizeof(q));
+        const ChebSymDims& d = h->symd;
+        q.P = h->P;
+        for (int i = 0; i < 2; ++i) {
+            q.N[i] = d.N[i];
+            q.Npad[i] = d.Npad[i];
+            q.Kpad[i] = d.Kpad[i];
+            q.bbytes[i] = d.bbytes[i];
+        }
+        q.nst = d.nst;
+        q.C = 2 * h->B;
+        q.nf = nf;
+        q.ntiles = (int)((q.C + 127) / 128);
+        for (int f = 0; f < nf; ++f) {
+            q.X[f] = static_cast<const float*>(inverse ? h->coef32[f] : h->nod32[f]);
+            q.Y[f] = static_cast<float*>(inverse ? h->nod32[f] : h->coef32[f]);
+        }
+        const unsigned char* img = inverse ? h->d_chebI : h->d_chebF;
+        q.B[0] = img;
+        q.B[1] = img + (size_t)cheb_pieces(h->split) * d.bbytes[0];
+        q.err = h->d_cheberr;
+        q.spins = h->wait_spins;
+        cheb_sym_kernel(h->split)<<<cheb_sym_grid(q.C, nf), 416, d.smem, h->stream>>>(q);
+        if (count) *count += 1;
+        CU(cudaGetLastError());
+        return CF_OK;
+    }
     ChebParams p;
     std::memset(&p, 0, sizeof(p));
     p.Ny = h->Ny;
@@ -1144,6 +1188,7 @@ static int set_attrs(cf_engine* h) {
         int NPs, nsplit, NPt;
         cheb_dims(h->Ny, NPs, nsplit, NPt);
         if ((rc = raise_smem_limit(cheb_kernel(h->split), cheb_smem(NPs, h->split)))) return rc;
+        if (h->chebsym && (rc = raise_smem_limit(cheb_sym_kernel(h->split), h->symd.smem))) return rc;
     }
     return CF_OK;
 }
@@ -1392,8 +1437,15 @@ int cf_create(const cf_config* cfg, cf_handle** out) {
     }
     if (h->mixed && h->tc) {
         std::vector<unsigned char> fimg, iimg;
-        cheb_images(h->Ny, 0, 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1)), h->split, fimg, h->chebNP, h->chebKT);
-        cheb_images(h->Ny, 1, 1.0, h->split, iimg, h->chebNP, h->chebKT);
+        const double fscale = 1.0 / ((double)h->Nxp * h->Nzp * (h->Ny - 1));
+        h->chebsym = cheb_sym_dims(h->Ny, h->split, h->symd);
+        if (h->chebsym) {
+            cheb_sym_images(h->Ny, 0, fscale, h->split, h->symd, fimg);
+            cheb_sym_images(h->Ny, 1, 1.0, h->split, h->symd, iimg);
+        } else {
+            cheb_images(h->Ny, 0, fscale, h->split, fimg, h->chebNP, h->chebKT);
+            cheb_images(h->Ny, 1, 1.0, h->split, iimg, h->chebNP, h->chebKT);
+        }
         if ((rc = dalloc(h, (void**)&h->d_chebF, fimg.size()))) return bail(rc);
         if ((rc = dalloc(h, (void**)&h->d_chebI, iimg.size()))) return bail(rc);
         if (cudaMemcpy(h->d_chebF, fimg.data(), fimg.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -2567,6 +2619,94 @@ static size_t cheb_smem(int NPs, int split) {
 }
 static ChebKernel cheb_kernel(int split) { return split ? k_cheb_mma<1> : k_cheb_mma<0>; }
 
+// The folded transform (k_cheb_sym): per parity q the outputs n = 2m + q
+// (N[0] = P/2 + 1, N[1] = P/2), the inputs (P/2 + 1 and P/2), both padded to
+// 16; the folded T^T of each parity resident in shared memory with nst A
+// stages (4 .. 2).  False when it does not fit (large Ny): the unfolded
+// kernel runs.
+static bool cheb_sym_dims(int Ny, int split, ChebSymDims& d) {
+    const int P = Ny - 1, H = P / 2;
+    if (P < 4 || P % 2) return false;
+    d.N[0] = H + 1;
+    d.N[1] = H;
+    const int es = split ? 2 : 4, npc = cheb_pieces(split), epc = 16 / es;
+    for (int q = 0; q < 2; ++q) {
+        d.Npad[q] = (d.N[q] + 15) & ~15;
+        d.Kpad[q] = (d.N[q] + 15) & ~15;
+        d.bbytes[q] = (unsigned)((d.Kpad[q] / epc) * d.Npad[q] * 16);
+    }
+    if (d.Npad[0] > 256) return false;
+    const size_t apb = (size_t)128 * 16 * es;
+    for (int nst = 4; nst >= 2; --nst) {
+        const size_t sm = (size_t)npc * std::max(d.bbytes[0], d.bbytes[1]) + (size_t)nst * npc * apb +
+                          (size_t)(2 * nst + 5) * 8 + 16;
+        if (sm <= (size_t)227 * 1024) {
+            d.nst = nst;
+            d.smem = sm;
+            return true;
+        }
+    }
+    return false;
+}
+// Folded T^T images: parity 0's pieces, then parity 1's, each piece
+// [Kpad / EPC chunks][Npad rows][16 bytes] with input k of row m at chunk
+// k / EPC, element k % EPC (the layout of cheb_images over all K at once);
+// row m of parity q is output n = 2m + q, its inputs k < N[q] (parity 0: k =
+// 0..P/2, the last multiplying X_{P/2} alone; parity 1: k = 0..P/2 - 1).
+static void cheb_sym_images(int Ny, int inverse, double scale, int split, const ChebSymDims& d,
+                            std::vector<unsigned char>& img) {
+    const int P = Ny - 1, npc = cheb_pieces(split);
+    img.assign((size_t)npc * (d.bbytes[0] + d.bbytes[1]), 0);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    size_t base = 0;
+    for (int q = 0; q < 2; ++q) {
+        const size_t pb = d.bbytes[q];
+        for (int m = 0; m < d.N[q]; ++m)
+            for (int k = 0; k < d.N[q]; ++k) {
+                const int n = 2 * m + q;
+                const long mm = ((long)n * k) % (2L * P);
+                const double c = (double)cosl(pi * (long double)mm / (long double)P);
+                double t;
+                if (inverse) {
+                    t = c;
+                } else {
+                    const double e = (n == 0 || n == P) ? 0.5 : 1.0, w = (k == 0 || k == P) ? 1.0 : 2.0;
+                    t = scale * e * w * c;
+                }
+                if (split == 0) {
+                    const float th = host_tf32((float)t);
+                    const float tl = host_tf32((float)(t - (double)th));
+                    const size_t o = ((size_t)(k / 4) * d.Npad[q] + m) * 16 + (k % 4) * 4;
+                    std::memcpy(&img[base + o], &th, 4);
+                    std::memcpy(&img[base + pb + o], &tl, 4);
+                } else {
+                    const float tf = (float)t;
+                    const uint16_t b0 = host_bf16(tf);
+                    const float r1 = tf - bf16_value(b0);
+                    const uint16_t b1 = host_bf16(r1);
+                    const uint16_t b2 = host_bf16(r1 - bf16_value(b1));
+                    const size_t o = ((size_t)(k / 8) * d.Npad[q] + m) * 16 + (k % 8) * 2;
+                    std::memcpy(&img[base + o], &b0, 2);
+                    std::memcpy(&img[base + pb + o], &b1, 2);
+                    std::memcpy(&img[base + 2 * pb + o], &b2, 2);
+                }
+            }
+        base += (size_t)npc * pb;
+    }
+}
+static ChebSymKernel cheb_sym_kernel(int split) { return split ? k_cheb_sym<1> : k_cheb_sym<0>; }
+// two CTAs (one per parity) per pair, a pair per two SMs, no more pairs than items
+static int cheb_sym_grid(long C, int nf) {
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 2) nsm = 2;
+    }
+    const long items = (long)nf * ((C + 127) / 128);
+    return 2 * (int)std::max(1L, std::min((long)(nsm / 2), items));
+}
+
 int cf_cheb_transform_split(const float* X, float* Y, int Ny, long C, int nfields, int inverse, double scale,
                             int split) {
     if (!X || !Y) return fail(CF_E_ARG, "null argument");
@@ -2574,8 +2714,11 @@ int cf_cheb_transform_split(const float* X, float* Y, int Ny, long C, int nfield
     if (C < 1 || nfields < 1 || nfields > CF_CHEB_MAXF) return fail(CF_E_ARG, "need C >= 1 and 1..6 fields");
     if (split != 0 && split != 1) return fail(CF_E_ARG, "split must be 0 (TF32) or 1 (BF16)");
     std::vector<unsigned char> img;
-    int NP, nkt;
-    cheb_images(Ny, inverse, scale, split, img, NP, nkt);
+    int NP = 0, nkt = 0;
+    ChebSymDims sd;
+    const bool sym = cheb_sym_dims(Ny, split, sd);
+    if (sym) cheb_sym_images(Ny, inverse, scale, split, sd, img);
+    else cheb_images(Ny, inverse, scale, split, img, NP, nkt);
     const size_t pb = cheb_piece_bytes(Ny, split);
     const size_t fb = sizeof(float) * (size_t)Ny * C;
     float *dX = nullptr, *dY = nullptr;
@@ -2600,9 +2743,34 @@ int cf_cheb_transform_split(const float* X, float* Y, int Ny, long C, int nfield
             rc = fail(CF_E_CUDA, "upload failed");
             break;
         }
+        if (sym) {
+            if ((rc = raise_smem_limit(cheb_sym_kernel(split), sd.smem))) break;
+            ChebSymParams q;
+            std::memset(&q, 0, sizeof(q));
+            q.P = Ny - 1;
+            for (int i = 0; i < 2; ++i) {
+                q.N[i] = sd.N[i];
+                q.Npad[i] = sd.Npad[i];
+                q.Kpad[i] = sd.Kpad[i];
+                q.bbytes[i] = sd.bbytes[i];
+            }
+            q.nst = sd.nst;
+            q.C = C;
+            q.nf = nfields;
+            q.ntiles = (int)((C + 127) / 128);
+            for (int f = 0; f < nfields; ++f) {
+                q.X[f] = dX + (size_t)f * Ny * C;
+                q.Y[f] = dY + (size_t)f * Ny * C;
+            }
+            q.B[0] = dB;
+            q.B[1] = dB + (size_t)cheb_pieces(split) * sd.bbytes[0];
+            q.err = derr;
+            q.spins = CF_WAIT_SPINS;
+            cheb_sym_kernel(split)<<<cheb_sym_grid(C, nfields), 416, sd.smem>>>(q);
+        }
         int NPs, nsplit, NPt;
         cheb_dims(Ny, NPs, nsplit, NPt);
-        if ((rc = raise_smem_limit(cheb_kernel(split), cheb_smem(NPs, split)))) break;
+        if (!sym && (rc = raise_smem_limit(cheb_kernel(split), cheb_smem(NPs, split)))) break;
         ChebParams p;
         std::memset(&p, 0, sizeof(p));
         p.Ny = Ny;
@@ -2619,7 +2787,7 @@ int cf_cheb_transform_split(const float* X, float* Y, int Ny, long C, int nfield
         p.err = derr;
         p.spins = CF_WAIT_SPINS;
         dim3 grid((unsigned)((C + CF_CHEB_MT - 1) / CF_CHEB_MT), (unsigned)nfields, (unsigned)nsplit);
-        cheb_kernel(split)<<<grid, 128, cheb_smem(NPs, split)>>>(p);
+        if (!sym) cheb_kernel(split)<<<grid, 128, cheb_smem(NPs, split)>>>(p);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) {
