@@ -49,6 +49,7 @@ struct Team {
     int P;     // highest degree (even)
     int hs;    // half stride: col_half_stride(P)
     zd* xch;   // four complex of team scratch in shared memory
+    double* sc;  // the column's Stokes-bank scalars (colsc 8, sa 4), staged by col_stage_scalars
 };
 
 // Team barrier.  The ids are literal (a run-time id makes the compiler reserve

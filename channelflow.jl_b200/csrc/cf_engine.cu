@@ -551,9 +551,9 @@ static int build_neumann(cf_engine* h) {
 // stride is 2 mod 8 complex (bank groups of the two-column tiles)
 static int col_stride(const cf_engine* h) { return 2 * col_half_stride(h->P) + 2; }
 static int col_zstride(const cf_engine* h) { return std::max(2 * col_half_stride(h->P), fft_bufsz(h->P)); }
-// per column: 6 vectors, 2 transform buffers and 4 complex of team scratch
+// per column: 6 vectors, 2 transform buffers and CF_TEAM_SCRATCH complex of team scratch
 static size_t col_smem(const cf_engine* h, int ncol = CF_NCOL) {
-    return ((size_t)ncol * (6 * col_stride(h) + 2 * col_zstride(h)) + 4 * ncol) * sizeof(zd);
+    return ((size_t)ncol * (6 * col_stride(h) + 2 * col_zstride(h)) + CF_TEAM_SCRATCH * ncol) * sizeof(zd);
 }
 
 static ColParams col_params(const cf_engine* h) {

@@ -81,6 +81,10 @@ constexpr int col_minblocks() {
     return (PL == 0 || PL >= 256) ? 6 / NCOL : 8 / NCOL;
 }
 
+// Team scratch per column in shared memory (complex units): four for the
+// team's exchanges, six holding the column's 12 Stokes-bank scalars.
+#define CF_TEAM_SCRATCH 10
+
 // Common set-up of a column kernel: the calling thread's team and column.
 template <int NCOL, int PL>
 struct ColCtx {
@@ -100,7 +104,8 @@ struct ColCtx {
         t.bar = 1 + tm;
         t.P = PL ? PL : p.P;
         t.hs = col_half_stride(t.P);
-        t.xch = sm + (long)NCOL * (6 * cs + 2 * zs) + 4 * tm;
+        t.xch = sm + (long)NCOL * (6 * cs + 2 * zs) + CF_TEAM_SCRATCH * tm;
+        t.sc = reinterpret_cast<double*>(t.xch + 4);
         c0 = (bx + p.bofs) * NCOL;
         c = c0 + tm;
         valid = c < p.B;
@@ -113,6 +118,22 @@ struct ColCtx {
     }
     CF_DEV zd* col(int r) const { return reg(r) + (threadIdx.x / CF_TEAM) * (r < 6 ? cs : zs); }
 };
+
+// The column's Stokes-bank scalars (colsc: inf00 inf01 inf10 inf11 sigma1
+// sigma2 shift kappa2p; sa: SA_even/odd pressure, SA_even/odd velocity)
+// copied asynchronously into the team scratch (t.sc[0..7], t.sc[8..11]) at the
+// start of a kernel, so that the Stokes solve reads them from shared memory
+// instead of waiting on a global load at each use.  Completed by the
+// kernel's first tile_wait and block barrier.
+template <class Ctx>
+CF_DEV void col_stage_scalars(const Ctx& X, const BankDev& bk) {
+    const Team& t = X.t;
+    if (X.valid && t.tid < 12) {
+        const double* src = t.tid < 8 ? bk.colsc + (long)X.c * 8 + t.tid : bk.sa + (long)X.c * 4 + (t.tid - 8);
+        cp_async_el<8>(t.sc + t.tid, src, true);
+    }
+    cp_async_commit();
+}
 
 // Tile of NCOL adjacent columns x Ny degrees into shared memory (column t at
 // sm + t*cs, parity layout).  Each thread issues up to 8 loads before storing
@@ -278,9 +299,9 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
     const BankDev& bk = p.bank;
     const double k = p.ax * ix;
     const double l = p.bz * (iz <= (p.Nz >> 1) ? iz : iz - p.Nz);
-    const double* csc = bk.colsc + (long)c * 8;
-    const double* sa = bk.sa + (long)c * 4;
-    const double shift = __ldg(csc + 6);
+    const double* sc = t.sc;  // colsc[0..7], sa at sc + 8
+    const double* sa = sc + 8;
+    const double shift = sc[6];
     const double* fv = bk.fac_v + (long)c * 3 * Ny;
     // elimination factors staged in shared memory (parity layout): alpha,
     // invden in F0, W in F1
@@ -301,10 +322,24 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
                 x[o] = it ? zsub(x[o], R1[o]) : zadd(x[o], zadd(zmulis(R0[o], k), zmulis(R2[o], l)));
             }
             __syncwarp();
-            col_helm<PL>(x, A, fa, fi, fw, p.helm_tab, __ldg(sa + 2 * it), __ldg(sa + 2 * it + 1),
-                     it ? shift : __ldg(csc + 7), zzero(), zzero(), t);
+            col_helm<PL>(x, A, fa, fi, fw, p.helm_tab, sa[2 * it], sa[2 * it + 1], it ? shift : sc[7], zzero(),
+                         zzero(), t);
         }
-        // influence correction (batchedinfluence.jl:101-120)
+        // influence and tau corrections (batchedinfluence.jl:101-120, 148-160):
+        // this lane's response entries are requested first, so the loads
+        // overlap the reductions below (one memory round trip, not one per
+        // element)
+        const double* __restrict__ rs = bk.resp + (long)c * 6 * Ny;
+        constexpr int NIT = PL ? ((PL >> 1) + 1 + 31) / 32 : 1;
+        double rv[6][NIT];
+        if constexpr (PL != 0) {
+#pragma unroll
+            for (int u = 0; u < NIT; ++u) {
+                const int j = lane + 32 * u, n = 2 * j + q;
+#pragma unroll
+                for (int a = 0; a < 6; ++a) rv[a][u] = j < nq ? __ldg(rs + a * Ny + n) : 0.0;
+            }
+        }
         zd s = zzero();
         for (int j = lane; j < nq; j += 32) {
             const double n = 2.0 * j + q;
@@ -314,27 +349,48 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         team_xchg(t, warp_sum_z(s), s0, s1);
         // upper = -sum n^2 v_n, lower = sum (-1)^n n^2 v_n
         const zd up = zscale(zadd(s0, s1), -1.0), lo = zsub(s0, s1);
-        const double i00 = __ldg(csc + 0), i01 = __ldg(csc + 1), i10 = __ldg(csc + 2), i11 = __ldg(csc + 3);
+        const double i00 = sc[0], i01 = sc[1], i10 = sc[2], i11 = sc[3];
         const zd dp = zaxpy(zscale(up, i00), i01, lo);
         const zd dm = zaxpy(zscale(up, i10), i11, lo);
-        const double* rs = bk.resp + (long)c * 6 * Ny;
-        for (int j = lane; j < nq; j += 32) {
-            const int n = 2 * j + q, o = qo + j;
-            PT[o] = zaxpy(zaxpy(PT[o], __ldg(rs + n), dp), __ldg(rs + Ny + n), dm);
-            V[o] = zaxpy(zaxpy(V[o], __ldg(rs + 2 * Ny + n), dp), __ldg(rs + 3 * Ny + n), dm);
+        if constexpr (PL != 0) {
+#pragma unroll
+            for (int u = 0; u < NIT; ++u) {
+                const int j = lane + 32 * u, o = qo + j;
+                if (j < nq) {
+                    PT[o] = zaxpy(zaxpy(PT[o], rv[0][u], dp), rv[1][u], dm);
+                    V[o] = zaxpy(zaxpy(V[o], rv[2][u], dp), rv[3][u], dm);
+                }
+            }
+        } else {
+            for (int j = lane; j < nq; j += 32) {
+                const int n = 2 * j + q, o = qo + j;
+                PT[o] = zaxpy(zaxpy(PT[o], __ldg(rs + n), dp), __ldg(rs + Ny + n), dm);
+                V[o] = zaxpy(zaxpy(V[o], __ldg(rs + 2 * Ny + n), dp), __ldg(rs + 3 * Ny + n), dm);
+            }
         }
         tsync(t);
         // tau correction (batchedinfluence.jl:148-160); (Dp)_{P-1} = 2P p_P, (Dp)_P = 0
         const zd vP1 = V[ppos(P - 1, hs)], vP = V[ppos(P, hs)], pP = PT[ppos(P, hs)];
         const zd rP1 = R1[ppos(P - 1, hs)], rP = R1[ppos(P, hs)];
-        const zd ts1 = zscale(zsub(zaxpy(zscale(vP1, shift), 2.0 * P, pP), rP1), 1.0 / (1.0 - __ldg(csc + 4)));
-        const zd ts2 = zscale(zsub(zscale(vP, shift), rP), 1.0 / (1.0 - __ldg(csc + 5)));
+        const zd ts1 = zscale(zsub(zaxpy(zscale(vP1, shift), 2.0 * P, pP), rP1), 1.0 / (1.0 - sc[4]));
+        const zd ts2 = zscale(zsub(zscale(vP, shift), rP), 1.0 / (1.0 - sc[5]));
         tsync(t);
         const zd sp = q ? ts2 : ts1, sv = q ? ts1 : ts2;
-        for (int j = lane; j < nq; j += 32) {
-            const int n = 2 * j + q, o = qo + j;
-            PT[o] = zaxpy(PT[o], __ldg(rs + 4 * Ny + n), sp);
-            V[o] = zaxpy(V[o], __ldg(rs + 5 * Ny + n), sv);
+        if constexpr (PL != 0) {
+#pragma unroll
+            for (int u = 0; u < NIT; ++u) {
+                const int j = lane + 32 * u, o = qo + j;
+                if (j < nq) {
+                    PT[o] = zaxpy(PT[o], rv[4][u], sp);
+                    V[o] = zaxpy(V[o], rv[5][u], sv);
+                }
+            }
+        } else {
+            for (int j = lane; j < nq; j += 32) {
+                const int n = 2 * j + q, o = qo + j;
+                PT[o] = zaxpy(PT[o], __ldg(rs + 4 * Ny + n), sp);
+                V[o] = zaxpy(V[o], __ldg(rs + 5 * Ny + n), sv);
+            }
         }
         tsync(t);
     } else {
@@ -365,7 +421,7 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
     if (c == 0) col_stage_factors(fa, fw, fv, t);
 #pragma unroll 1
     for (int j = 0; j < 2; ++j)
-        col_helm<PL>(j ? R2 : R0, A, fa, fi, fw, p.helm_tab, __ldg(sa + 2), __ldg(sa + 3), shift, zzero(), zzero(), t);
+        col_helm<PL>(j ? R2 : R0, A, fa, fi, fw, p.helm_tab, sa[2], sa[3], shift, zzero(), zzero(), t);
     if (c == 0) {
         double gx, gz;
         if (p.cmode == 1) {
@@ -512,6 +568,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     // right-hand-side region not yet written (1, then 2), and for i = 2, whose
     // right-hand side takes region 2, Q_2 goes there (consumed before the
     // right-hand side is formed) and U_2 to region 5.
+    col_stage_scalars(X, p.bank);
     if (!S32) tile_load_async<NCOL, PL>(X.reg(3), cs, hs, p.Pf, c0, p.Ny, p.B);  // completed with N_0
     // The block's Stokes-bank data (read in Phase B) start on their way to
     // L2 now, so that Phase B's reads of them wait on L2, not on DRAM.
@@ -846,6 +903,8 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
     const double k = p.ax * X.ix;
     const double l = p.bz * (X.iz <= (p.Nz >> 1) ? X.iz : X.iz - p.Nz);
     const double kap2 = k * k + l * l;
+    col_stage_scalars(X, p.bank);
+    tile_wait();  // visible to the team after the loop's first block barrier
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
         tile_load<NCOL, PL>(X.reg(5), cs, hs, sel3(p.U[0], p.U[1], p.U[2], i), c0, p.Ny, p.B);
