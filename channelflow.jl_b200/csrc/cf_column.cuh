@@ -192,6 +192,25 @@ CF_DEV void col_stage_factors(double* fa, double* fw, const double* __restrict__
     __syncwarp();
 }
 
+// The same copies issued asynchronously (8-byte cp.async per value, one
+// commit group): the caller works on while they land, then completes them
+// with col_factors_wait before the solve reads them.
+CF_DEV void col_stage_factors_async(double* fa, double* fw, const double* __restrict__ src, const Team& t) {
+    const int P = t.P, Ny = P + 1, hs = t.hs, q = t.q;
+    const int nq = pcount(q, P);
+    for (int j = t.lane; j < nq; j += 32) {
+        const double* s = src + 2 * j + q;
+        cp_async_el<8>(fa + q * hs + j, s, true);
+        cp_async_el<8>(fa + 2 * hs + q * hs + j, s + Ny, true);
+        cp_async_el<8>(fw + q * hs + j, s + 2 * Ny, true);
+    }
+    cp_async_commit();
+}
+CF_DEV void col_factors_wait() {
+    cp_async_wait<0>();
+    __syncwarp();
+}
+
 // g_n of the integrated tau equation (n >= 2) from the right-hand side f
 // (parity half fh, f_m at fh[m >> 1]).  gt holds the degree-only coefficients:
 //   gt[n] = c_{n-2}/(4n(n-1)),  gt[Ny+n] = -[n<=P-2]/(2(n^2-1)),

@@ -311,17 +311,19 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
     if (c != 0) {
         // it = 0: pressure with zero wall values, (D^2 - kappa^2) p = D Ry + i k Rx + i l Rz
         // it = 1: normal velocity, (nu D^2 - shift) v = D p - Ry
+        // (the solve's factors are copied into F0, F1 while the derivative
+        // of its right-hand side is formed)
 #pragma unroll 1
         for (int it = 0; it < 2; ++it) {
             const double* fsrc = it ? fv : bk.fac_p + (long)c * 3 * Ny;
             zd* x = it ? V : PT;
-            col_stage_factors(fa, fw, fsrc, t);
+            col_stage_factors_async(fa, fw, fsrc, t);
             col_diff<PL>(it ? PT : R1, x, t);
             for (int j = lane; j < nq; j += 32) {
                 const int o = qo + j;
                 x[o] = it ? zsub(x[o], R1[o]) : zadd(x[o], zadd(zmulis(R0[o], k), zmulis(R2[o], l)));
             }
-            __syncwarp();
+            col_factors_wait();
             col_helm<PL>(x, A, fa, fi, fw, p.helm_tab, sa[2 * it], sa[2 * it + 1], it ? shift : sc[7], zzero(),
                          zzero(), t);
         }
