@@ -75,8 +75,10 @@ def test_tma_wait_gives_up_and_handle_recovers():
 
 
 def test_tensor_core_wait_gives_up_and_handle_recovers():
-    # Ny = 65: five K-tiles through two shared-memory stages, so a stage is
-    # waited for before it is reused
+    # Ny = 65: the folded transform (producers, MMA thread and epilogue
+    # handing stages and accumulators to each other through mbarriers); with a
+    # zero poll limit the first wait that is not already complete gives up,
+    # every role leaves, and the kernel waits for its MMAs before freeing TMEM
     g = cfb200.Grid(16, 65, 12, LX, LZ)
     pb = cfb200.CouetteFlow(g, 1 / 400, 0.01, precision="mixed-tc")
     st = cfb200.random_state(pb, 0.1, seed=8)
