@@ -2642,7 +2642,9 @@ static bool cheb_sym_dims(int Ny, int split, ChebSymDims& d) {
                           (size_t)(2 * nst + 5) * 8 + 16;
         if (sm <= (size_t)227 * 1024) {
             d.nst = nst;
-            d.smem = sm;
+            // at least half an SM's shared memory, so that one CTA runs per
+            // SM and its 512 TMEM columns are never contended
+            d.smem = std::max(sm, (size_t)116 * 1024);
             return true;
         }
     }
