@@ -85,7 +85,9 @@ def test_mixed_poiseuille_flux_matches_fp64_engine(precision):
 
 
 @pytest.mark.parametrize("precision", MIXED)
-@pytest.mark.parametrize("dims", [(9, 17, 7), (16, 17, 16), (48, 33, 40), (8, 257, 6)])
+# (384, 17, 4) and (341, 17, 4): the FP32 in-place x-pass at the padded
+# lengths 576 and 512
+@pytest.mark.parametrize("dims", [(9, 17, 7), (16, 17, 16), (48, 33, 40), (8, 257, 6), (384, 17, 4), (341, 17, 4)])
 def test_mixed_one_step_sizes(dims, precision):
     Nx, Ny, Nz = dims
     g = cfb200.Grid(Nx, Ny, Nz, 5.3, 7.1)

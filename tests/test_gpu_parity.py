@@ -44,8 +44,10 @@ def _oc(kw):
     return {}
 
 
+# (384, 9, 48) and (341, 9, 6): the in-place x-pass at the padded lengths 576
+# and 512 (Nx = 341: Nxp = 512)
 @pytest.mark.parametrize("dims", [(16, 17, 16), (32, 33, 32), (8, 9, 8), (9, 17, 7), (8, 81, 1), (6, 13, 10),
-                                  (48, 9, 384), (384, 9, 48)])
+                                  (48, 9, 384), (384, 9, 48), (341, 9, 6)])
 def test_nonlinear_term(dims):
     Nx, Ny, Nz = dims
     gpu, ref = pair(Nx, Ny, Nz, 5.3, 7.1, 0.01, 0.01)
