@@ -99,9 +99,15 @@ __host__ __device__ constexpr int run_max() {
 }
 
 // b = D a  (b != a).  Warp q writes the degrees of parity q of b from the
-// degrees of parity 1-q of a; b_P = 0.
-template <int PL>
+// degrees of parity 1-q of a; b_P = 0.  For a compile-time length, MODE 1
+// computes it in place (b == a: every lane's run is read before the team
+// barrier, written after it) and MODE 2 subtracts it (b -= D a, b != a).
+#define CF_DIFF_SET 0
+#define CF_DIFF_INPLACE 1
+#define CF_DIFF_SUB 2
+template <int PL, int MODE = CF_DIFF_SET>
 CF_DEV void col_diff_body(const zd* a, zd* b, const Team& t) {
+    static_assert(MODE == CF_DIFF_SET || PL != 0, "in-place and subtracting derivatives need a compile-time length");
     const int P = t.P, hs = t.hs, q = t.q, lane = t.lane;
     const int pin = 1 - q;                 // parity of the input chain
     const int top = pin ? P - 1 : P;       // m = top, top-2, ..., pin
@@ -125,12 +131,15 @@ CF_DEV void col_diff_body(const zd* a, zd* b, const Team& t) {
             if (s < E && i < cnt && m >= 1) tot = zaxpy(tot, (double)m, v[s]);
         }
         zd run = warp_excl_z(warp_scan_z(tot, lane), lane);
+        if (MODE == CF_DIFF_INPLACE) tsync(t);  // every input read before any output is written
 #pragma unroll
         for (int s = 0; s < EM; ++s) {
             const int i = i0 + s, m = top - 2 * i;
             if (s < E && i < cnt && m >= 1) {
                 run = zaxpy(run, (double)m, v[s]);
-                bh[(m - 1) >> 1] = (m == 1) ? run : zscale(run, 2.0);
+                const zd d = (m == 1) ? run : zscale(run, 2.0);
+                zd& o = bh[(m - 1) >> 1];
+                o = MODE == CF_DIFF_SUB ? zsub(o, d) : d;
             }
         }
     } else {
@@ -150,15 +159,15 @@ CF_DEV void col_diff_body(const zd* a, zd* b, const Team& t) {
             }
         }
     }
-    if (q == 0 && lane == 0) bh[P >> 1] = zzero();
+    if (MODE != CF_DIFF_SUB && q == 0 && lane == 0) bh[P >> 1] = zzero();
     tsync(t);
 }
-template <int PL>
-CF_DEV_NOINLINE void col_diff_ool(const zd* a, zd* b, const Team t) { col_diff_body<PL>(a, b, t); }
-template <int PL>
+template <int PL, int MODE = CF_DIFF_SET>
+CF_DEV_NOINLINE void col_diff_ool(const zd* a, zd* b, const Team t) { col_diff_body<PL, MODE>(a, b, t); }
+template <int PL, int MODE = CF_DIFF_SET>
 CF_DEV void col_diff(const zd* a, zd* b, const Team& t) {
-    if constexpr (col_ool<PL>()) col_diff_ool<PL>(a, b, t);
-    else col_diff_body<PL>(a, b, t);
+    if constexpr (col_ool<PL>()) col_diff_ool<PL, MODE>(a, b, t);
+    else col_diff_body<PL, MODE>(a, b, t);
 }
 
 // The three elimination factor rows of a column (alpha, invden, W: src,
@@ -227,8 +236,11 @@ CF_DEV zd helm_g(const zd* fh, const double* __restrict__ gt, int n, int P) {
 // arithmetic in the same order, with each lane's run unrolled and its
 // intermediate terms (g_n invden_n and the map factors of the backward sweep,
 // beta and alpha of the forward sweep) kept in registers between the two
-// passes of each sweep instead of being loaded again.
-template <int PL>
+// passes of each sweep instead of being loaded again.  GF: the factors are
+// read from their global rows in natural order (alpha = the row base,
+// invden at + Ny, W at + 2 Ny; invden and W unused) instead of from the
+// parity-layout copy in shared memory.
+template <int PL, bool GF = false>
 CF_DEV void col_helm_runs(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
                           const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
                           const Team& t, int top, int cnt, int E, int i0) {
@@ -236,9 +248,13 @@ CF_DEV void col_helm_runs(zd* x, zd* scr, const double* alpha, const double* inv
     const int P = t.P, Ny = P + 1, q = t.q, lane = t.lane, hs = t.hs;
     zd* xh = x + q * hs;
     zd* sh = scr + q * hs;
-    const double* ah = alpha + q * hs;
-    const double* ih = invden + q * hs;
-    const double* wh = W + q * hs;
+    const double* ah = GF ? alpha : alpha + q * hs;
+    const double* ih = GF ? alpha : invden + q * hs;
+    const double* wh = GF ? alpha : W + q * hs;
+    // factor of degree n (the parity-q half holds degree n at n >> 1)
+    auto IH = [&](int n) { return GF ? __ldg(ih + Ny + n) : ih[n >> 1]; };
+    auto WH = [&](int n) { return GF ? __ldg(wh + 2 * Ny + n) : wh[n >> 1]; };
+    auto AH = [&](int j) { return GF ? __ldg(ah + 2 * j + q) : ah[j]; };
     // backward sweep beta_n = invden_n (g_n - u_n beta_{n+2}) as maps G + M x
     zd g[EM];
     double Ms[EM];
@@ -249,7 +265,7 @@ CF_DEV void col_helm_runs(zd* x, zd* scr, const double* alpha, const double* inv
         Ms[s] = 1.0;
         if (s < E && i < cnt) {
             const int n = top - 2 * i;
-            const double id = ih[n >> 1];
+            const double id = IH(n);
             Ms[s] = th1 * __ldg(gt + 2 * Ny + n) * id;
             g[s] = zscale(helm_g(xh, gt, n, P), id);
         }
@@ -272,7 +288,7 @@ CF_DEV void col_helm_runs(zd* x, zd* scr, const double* alpha, const double* inv
             const int n = top - 2 * i;
             xv = zaxpy(g[s], Ms[s], xv);
             sh[n >> 1] = xv;
-            sw = zaxpy(sw, wh[n >> 1], xv);
+            sw = zaxpy(sw, WH(n), xv);
         }
     }
     sw = warp_sum_z(sw);
@@ -288,7 +304,7 @@ CF_DEV void col_helm_runs(zd* x, zd* scr, const double* alpha, const double* inv
         av[s] = 1.0;
         if (s < E && jj < cnt) {
             bv[s] = sh[jj + 1];
-            av[s] = ah[jj + 1];
+            av[s] = AH(jj + 1);
         }
     }
     Mc = 1.0;
@@ -320,17 +336,18 @@ CF_DEV void col_helm_runs(zd* x, zd* scr, const double* alpha, const double* inv
 // factors in the parity layout (shared memory, staged by col_stage_factors);
 // SA0/SA1 and bc0/bc1 are the wall-row sums and data of the two parities.
 // Warp q solves the parity-q system alone.
-template <int PL>
+template <int PL, bool GF = false>
 CF_DEV void col_helm_body(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
                           const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
                           const Team& t) {
+    static_assert(!GF || PL != 0, "factors from global memory need a compile-time length");
     const int P = t.P, Ny = P + 1, q = t.q, lane = t.lane, hs = t.hs;
     const int top = q ? P - 1 : P;
     const int cnt = (top - q) / 2;  // backward chain n = top, top-2, ..., q+2
     const int E = run_len(cnt);
     const int i0 = lane * E;
     if constexpr (PL != 0) {
-        col_helm_runs<PL>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t, top, cnt, E, i0);
+        col_helm_runs<PL, GF>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t, top, cnt, E, i0);
         return;
     }
     zd* xh = x + q * hs;
@@ -395,18 +412,18 @@ CF_DEV void col_helm_body(zd* x, zd* scr, const double* alpha, const double* inv
     if (lane == 0) xh[0] = a0;
     tsync(t);
 }
-template <int PL>
+template <int PL, bool GF = false>
 CF_DEV_NOINLINE void col_helm_ool(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
                                   const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0,
                                   zd bc1, const Team t) {
-    col_helm_body<PL>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
+    col_helm_body<PL, GF>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
 }
-template <int PL>
+template <int PL, bool GF = false>
 CF_DEV void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, const double* W,
                      const double* __restrict__ gt, double SA0, double SA1, double th1, zd bc0, zd bc1,
                      const Team& t) {
-    if constexpr (col_ool<PL>()) col_helm_ool<PL>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
-    else col_helm_body<PL>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
+    if constexpr (col_ool<PL>()) col_helm_ool<PL, GF>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
+    else col_helm_body<PL, GF>(x, scr, alpha, invden, W, gt, SA0, SA1, th1, bc0, bc1, t);
 }
 
 // DCT-I (REDFT00) of complex x[0..P] in place (parity layout).  z and z2 are

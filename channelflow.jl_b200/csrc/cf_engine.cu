@@ -556,6 +556,24 @@ static size_t col_smem(const cf_engine* h, int ncol = CF_NCOL) {
     return ((size_t)ncol * (6 * col_stride(h) + 2 * col_zstride(h)) + CF_TEAM_SCRATCH * ncol) * sizeof(zd);
 }
 
+// The tensor-core forms' stage kernel at a compile-time length keeps six
+// regions per column and no transform buffers (its Chebyshev transforms run
+// outside): launched with zs = 0 and this shared memory.
+static bool col_static_len(int P) {
+    switch (P) {
+#define CF_CASE(N) \
+    case N: return true;
+        CF_COL_LENGTHS(CF_CASE)
+#undef CF_CASE
+        default: return false;
+    }
+}
+static bool stage_mx_noz(const cf_engine* h) { return h->tc && col_static_len(h->P); }
+static size_t stage_mx_smem(const cf_engine* h) {
+    if (!stage_mx_noz(h)) return col_smem(h);
+    return ((size_t)CF_NCOL * 6 * col_stride(h) + CF_TEAM_SCRATCH * CF_NCOL) * sizeof(zd);
+}
+
 static ColParams col_params(const cf_engine* h) {
     ColParams p;
     std::memset(&p, 0, sizeof(p));
@@ -965,7 +983,8 @@ static int launch_stage_mx(cf_engine* h, int j, int* count) {
     ColParams p = stage_col_params(h, j);
     for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->coef32[i]);
     for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->coef32[i]);
-    col_kernel(KC_STAGE_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    if (stage_mx_noz(h)) p.zs = 0;
+    col_kernel(KC_STAGE_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, stage_mx_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return launch_cheb(h, 6, true, count);
@@ -1028,6 +1047,7 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
             for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(io[i]);
             for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(io[i]);
             mx_state(h, p);
+            if (stage_mx_noz(h)) p.zs = 0;
             cudaEventRecord(ev[0], h->stream);
             launch_z(h, KF_ZINV, true, 6, f);
             cudaEventRecord(ev[1], h->stream);
@@ -1038,7 +1058,7 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
             if (h->tc && (rc = launch_cheb(h, 3, false, nullptr))) break;
             cudaEventRecord(ev[4], h->stream);
             col_kernel(h->tc ? KC_STAGE_MX : (h->s32 ? KC_STAGE_MXS : KC_STAGE_MXD), h->P)<<<
-                col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+                col_blocks(h), CF_NCOL * CF_TEAM, h->tc ? stage_mx_smem(h) : col_smem(h), h->stream>>>(p);
             cudaEventRecord(ev[5], h->stream);
             if (h->tc && (rc = launch_cheb(h, 6, true, nullptr))) break;
             cudaEventRecord(ev[6], h->stream);

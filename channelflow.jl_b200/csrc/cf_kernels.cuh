@@ -228,6 +228,30 @@ CF_DEV void tile_widen(zd* sm, int cs, int hs, const zf* st, int Ny, int c0, con
         sm[t * cs + ppos(n, hs)] = (mean && t == 0) ? m64[n] : to_zd(st[e]);
     }
 }
+// The same with the staged tile inside the destination region (its upper
+// half): every thread reads its elements into registers, the block
+// synchronises, then the FP64 values are written (for kernels without a free
+// transform buffer to stage in).  PL: a compile-time length.
+template <int NCOL, int PL>
+CF_DEV void tile_widen_inplace(zd* sm, int cs, int hs, const zf* st, int Ny) {
+    constexpr int NT = NCOL * CF_TEAM, K = (NCOL * (PL + 1) + NT - 1) / NT;
+    const int tot = Ny * NCOL;
+    zf v[K];
+#pragma unroll
+    for (int u = 0; u < K; ++u) {
+        const int e = threadIdx.x + u * NT;
+        v[u] = e < tot ? st[e] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < K; ++u) {
+        const int e = threadIdx.x + u * NT;
+        if (e < tot) {
+            const int n = e / NCOL, t = e - n * NCOL;
+            sm[t * cs + ppos(n, hs)] = to_zd(v[u]);
+        }
+    }
+}
 // column 0 of a tile (c0 == 0) written in FP64 to m64 (the mean-flow mode
 // of an FP32 state)
 template <int NCOL>
@@ -289,8 +313,10 @@ CF_DEV void col_inverse_y2(zd* xa, zd* xb, zd* z, zd* z2, const ColParams& p, co
 
 // Solve the Stokes problem of one column.  In: R0,R1,R2 (= Rx,Ry,Rz).
 // Out: u in R0, v in V, w in R2, p in PT.  A is scratch; F0, F1 hold the
-// staged elimination factors.  Returns the mean gradients for the (0,0) column.
-template <int PL>
+// staged elimination factors (GF: the solves read the factors from global
+// memory and F0, F1 are not used).  Returns the mean gradients for the (0,0)
+// column.
+template <int PL, bool GF = false>
 CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd* F1, const ColParams& p, int c,
                        int ix, int iz, const Team& t, double* gout) {
     const int P = t.P, Ny = P + 1, q = t.q, lane = t.lane, hs = t.hs;
@@ -317,15 +343,21 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         for (int it = 0; it < 2; ++it) {
             const double* fsrc = it ? fv : bk.fac_p + (long)c * 3 * Ny;
             zd* x = it ? V : PT;
-            col_stage_factors_async(fa, fw, fsrc, t);
+            if (!GF) col_stage_factors_async(fa, fw, fsrc, t);
             col_diff<PL>(it ? PT : R1, x, t);
             for (int j = lane; j < nq; j += 32) {
                 const int o = qo + j;
                 x[o] = it ? zsub(x[o], R1[o]) : zadd(x[o], zadd(zmulis(R0[o], k), zmulis(R2[o], l)));
             }
-            col_factors_wait();
-            col_helm<PL>(x, A, fa, fi, fw, p.helm_tab, sa[2 * it], sa[2 * it + 1], it ? shift : sc[7], zzero(),
-                         zzero(), t);
+            if constexpr (GF) {
+                __syncwarp();
+                col_helm<PL, true>(x, A, fsrc, nullptr, nullptr, p.helm_tab, sa[2 * it], sa[2 * it + 1],
+                                   it ? shift : sc[7], zzero(), zzero(), t);
+            } else {
+                col_factors_wait();
+                col_helm<PL>(x, A, fa, fi, fw, p.helm_tab, sa[2 * it], sa[2 * it + 1], it ? shift : sc[7], zzero(),
+                             zzero(), t);
+            }
         }
         // influence and tau corrections (batchedinfluence.jl:101-120, 148-160):
         // this lane's response entries are requested first, so the loads
@@ -420,10 +452,15 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         R2[o] = zsub(zmulis(PT[o], l), R2[o]);
     }
     __syncwarp();
-    if (c == 0) col_stage_factors(fa, fw, fv, t);
+    if (!GF && c == 0) col_stage_factors(fa, fw, fv, t);
 #pragma unroll 1
-    for (int j = 0; j < 2; ++j)
-        col_helm<PL>(j ? R2 : R0, A, fa, fi, fw, p.helm_tab, sa[2], sa[3], shift, zzero(), zzero(), t);
+    for (int j = 0; j < 2; ++j) {
+        if constexpr (GF)
+            col_helm<PL, true>(j ? R2 : R0, A, fv, nullptr, nullptr, p.helm_tab, sa[2], sa[3], shift, zzero(), zzero(),
+                               t);
+        else
+            col_helm<PL>(j ? R2 : R0, A, fa, fi, fw, p.helm_tab, sa[2], sa[3], shift, zzero(), zzero(), t);
+    }
     if (c == 0) {
         double gx, gz;
         if (p.cmode == 1) {
@@ -551,6 +588,10 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
     constexpr bool NCOEF = MIX == 1 || FORM == NL_DIV;  // N arrives as coefficients
     constexpr bool F32 = MIX != 0;                       // FP32 N in, FP32 fields out
     constexpr bool S32 = MIX == 3;                       // FP32 state in global memory
+    // tensor-core forms at a compile-time length: no transform buffers (the
+    // DCTs run outside; D^2 U in place, D P subtracted as it is formed, the
+    // Stokes factors read from L2), six regions per column
+    constexpr bool NOZ = MIX == 1 && PL != 0;
     extern __shared__ zd smem[];
     const ColCtx<NCOL, PL> X(smem, p, bx);
     const Team& t = X.t;
@@ -612,7 +653,15 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
         } else {
             if (p.stage > 0) tile_load_async<NCOL, PL>(X.reg(qreg), cs, hs, Q_i, c0, p.Ny, p.B);
             tile_load_async<NCOL, PL>(X.reg(ureg), cs, hs, U_i, c0, p.Ny, p.B);
-            if (F32) {
+            if (NOZ) {
+                // the FP32 term staged in the upper half of region 4 and widened in place
+                zf* st = reinterpret_cast<zf*>(X.reg(4)) + (long)NCOL * cs;
+                tile_stage32<NCOL>(st, reinterpret_cast<const zf*>(Nn_i), c0, p.Ny, p.B);
+                cp_async_commit();
+                tile_wait();
+                __syncthreads();
+                tile_widen_inplace<NCOL, PL>(X.reg(4), cs, hs, st, p.Ny);
+            } else if (F32) {
                 // the FP32 term copied into the (still free) transform
                 // buffers beside the FP64 tiles, then widened into region 4
                 zf* st = reinterpret_cast<zf*>(X.reg(6));
@@ -671,20 +720,39 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
                     wL2 = wl;
                 }
             }
-            col_diff<PL>(U, Z, t);
-            col_diff<PL>(Z, R, t);
-            // R = lambda U + nu (D^2 U - kappa^2 U) - d_i P + (B/C) Q
-            if (i == 1) col_diff<PL>(X.col(3), Z, t);
-            const zd* PT = X.col(3);
-            const double kl = (i == 0) ? k : l;
-            for (int j = lane; j < nq; j += 32) {
-                const int o = qo + j;
-                zd lap = zaxpy(R[o], -kap2, U[o]);
-                zd r = zaxpy(zscale(U[o], p.lambda), p.nu, lap);
-                zd dP = (i == 1) ? Z[o] : zmulis(PT[o], kl);
-                r = zsub(r, dP);
-                r = zaxpy(r, p.weight, Qn[o]);
-                R[o] = r;
+            if constexpr (NOZ) {
+                // R = lambda U + nu (D^2 U - kappa^2 U) - d_i P + (B/C) Q, the
+                // y derivative of P subtracted last
+                col_diff<PL>(U, R, t);
+                col_diff<PL, CF_DIFF_INPLACE>(R, R, t);
+                const zd* PT = X.col(3);
+                const double kl = (i == 0) ? k : l;
+                for (int j = lane; j < nq; j += 32) {
+                    const int o = qo + j;
+                    zd lap = zaxpy(R[o], -kap2, U[o]);
+                    zd r = zaxpy(zscale(U[o], p.lambda), p.nu, lap);
+                    if (i != 1) r = zsub(r, zmulis(PT[o], kl));
+                    r = zaxpy(r, p.weight, Qn[o]);
+                    R[o] = r;
+                }
+                __syncwarp();
+                if (i == 1) col_diff<PL, CF_DIFF_SUB>(PT, R, t);
+            } else {
+                col_diff<PL>(U, Z, t);
+                col_diff<PL>(Z, R, t);
+                // R = lambda U + nu (D^2 U - kappa^2 U) - d_i P + (B/C) Q
+                if (i == 1) col_diff<PL>(X.col(3), Z, t);
+                const zd* PT = X.col(3);
+                const double kl = (i == 0) ? k : l;
+                for (int j = lane; j < nq; j += 32) {
+                    const int o = qo + j;
+                    zd lap = zaxpy(R[o], -kap2, U[o]);
+                    zd r = zaxpy(zscale(U[o], p.lambda), p.nu, lap);
+                    zd dP = (i == 1) ? Z[o] : zmulis(PT[o], kl);
+                    r = zsub(r, dP);
+                    r = zaxpy(r, p.weight, Qn[o]);
+                    R[o] = r;
+                }
             }
         }
         __syncthreads();
@@ -719,8 +787,8 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
             tsync(t);
         } else {
             double g2[2];
-            col_stokes<PL>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7), p, c,
-                           X.ix, X.iz, t, g2);
+            col_stokes<PL, NOZ>(X.col(0), X.col(1), X.col(2), X.col(3), X.col(4), X.col(5), X.col(6), X.col(7), p,
+                                c, X.ix, X.iz, t, g2);
             if (c == 0 && t.tid == 0) {
                 p.grad_out[0] = g2[0];
                 p.grad_out[1] = g2[1];
@@ -788,9 +856,15 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, MINB)
     }
 }
 
-// Mixed-precision stages (MIX 1, 2 and 3 of column_stage_body).
+// Mixed-precision stages (MIX 1, 2 and 3 of column_stage_body).  MIX 1 at a
+// compile-time length takes six regions per column (no transform buffers),
+// so four blocks fit per SM at P = 256 and the registers are bounded for them.
 template <int NCOL, int PL, int MIX>
-__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k_column_stage_mx(ColParams p) {
+constexpr int col_minblocks_mx() {
+    return (MIX == 1 && PL != 0) ? 8 / NCOL : col_minblocks<NCOL, PL>();
+}
+template <int NCOL, int PL, int MIX>
+__global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks_mx<NCOL, PL, MIX>())) k_column_stage_mx(ColParams p) {
     column_stage_body<NCOL, PL, MIX>(p, blockIdx.x);
 }
 
