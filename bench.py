@@ -453,6 +453,7 @@ def measure_ensemble(args, cfg, rank, world, local, torch, dist):
         "clocks": clocks,
         "gpu_launches": launches,
         "diagnostics": {"kinetic_energy_sample": energies},
+        "schedule": [s for s in ens.schedule().splitlines() if s],
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = ensemble_cpu(cfg, members, os.cpu_count() or 1)

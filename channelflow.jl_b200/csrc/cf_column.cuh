@@ -1,10 +1,11 @@
 // cf_column.cuh -- per-column (one Fourier pair (k,l), all Chebyshev degrees)
-// device building blocks.  A team of two warps owns one column: warp q holds
-// the degrees of parity q.  A column vector lives in shared memory split by
+// device building blocks.  A team owns one column: two parity groups of
+// CF_COL_TW lanes (a warp each, or the two halves of one warp for the short
+// columns), group q holding the degrees of parity q.  A column vector lives in shared memory split by
 // parity, degree n at position (n & 1) * hs + (n >> 1) (hs = col_half_stride:
 // P/2 + 1 rounded up to 4 mod 8), so each parity is a contiguous half and the
 // recurrences below (which couple degrees of one parity only) run inside one
-// warp.
+// parity group.
 //
 // Reference arithmetic restated here:
 //  * Chebyshev derivative recurrence b_n = b_{n+2} + 2(n+1) a_{n+1}, b_0
@@ -22,12 +23,24 @@
 //
 // Chains of one parity are scanned in runs: each lane takes E consecutive
 // chain elements (E odd, so the stride-E shared-memory accesses of a warp hit
-// distinct bank groups) and the runs are combined by a warp scan.
+// distinct bank groups) and the runs are combined by a scan over the group.
 #pragma once
 #include "cf_common.cuh"
 #include "cf_fft.cuh"
 
-#define CF_TEAM 64  // threads per column
+// Lanes per parity group.  The short columns (compile-time P <= 64: at most
+// 33 degrees per parity) give each parity half a warp, so that one warp owns
+// a column and a column's instructions issue once, not once per parity warp;
+// the others give each parity a warp.  The column kernels of one length are
+// compiled in their own translation unit (CF_INST_P), so the width is a
+// constant of the unit; the host takes a length's team size from
+// col_team_threads (cf_dispatch.h).
+#if defined(CF_INST_P) && CF_INST_P != 0 && CF_INST_P <= 64
+#define CF_COL_TW 16
+#else
+#define CF_COL_TW 32
+#endif
+#define CF_TEAM (2 * CF_COL_TW)  // threads per column
 
 // The long columns (P >= 192, and the run-time-sized kernels) call the
 // repeated helpers below out of line (one copy each keeps those kernels'
@@ -38,25 +51,75 @@ __host__ __device__ constexpr bool col_ool() {
     return PL == 0 || PL >= 192;
 }
 
-// The two warps of one column.  Every routine below is called by all 64
-// threads of the team and ends with the team's barrier, after which all of its
-// outputs are visible to both warps.
+// The two parity groups of one column.  Every routine below is called by all
+// CF_TEAM threads of the team and ends with the team's barrier, after which
+// all of its outputs are visible to both groups.
 struct Team {
-    int q;     // parity owned by this warp (warp index in the team)
-    int lane;  // lane in the warp
-    int tid;   // 0..63
+    int q;     // parity owned by this group (group index in the team)
+    int lane;  // lane in the group (0 .. CF_COL_TW - 1)
+    int tid;   // 0 .. CF_TEAM - 1
     int bar;   // named barrier of the team (1 or 2)
+    unsigned gm;  // the group's lanes in its warp (the mask of its shuffles)
     int P;     // highest degree (even)
     int hs;    // half stride: col_half_stride(P)
     zd* xch;   // four complex of team scratch in shared memory
     double* sc;  // the column's Stokes-bank scalars (colsc 8, sa 4), staged by col_stage_scalars
 };
 
-// Team barrier.  The ids are literal (a run-time id makes the compiler reserve
-// all sixteen barriers of the block, which limits blocks per SM).
+// Team barrier (a team of one warp: the warp's).  The ids are literal (a
+// run-time id makes the compiler reserve all sixteen barriers of the block,
+// which limits blocks per SM).
 CF_DEV void tsync(const Team& t) {
+#if CF_COL_TW == 16
+    __syncwarp();
+#else
     if (t.bar == 1) asm volatile("bar.sync 1, 64;" ::: "memory");
     else asm volatile("bar.sync 2, 64;" ::: "memory");
+#endif
+}
+
+// Collectives of one parity group (its lanes, width CF_COL_TW): the mask names
+// the group's own lanes, so a group may call them in a branch the other group
+// of its warp does not take.
+CF_DEV double gshfl_up_d(double v, int d, const Team& t) { return __shfl_up_sync(t.gm, v, d, CF_COL_TW); }
+CF_DEV double gshfl_xor_d(double v, int m, const Team& t) { return __shfl_xor_sync(t.gm, v, m, CF_COL_TW); }
+CF_DEV zd gshfl_up_z(zd v, int d, const Team& t) {
+    return make_double2(gshfl_up_d(v.x, d, t), gshfl_up_d(v.y, d, t));
+}
+CF_DEV zd group_sum_z(zd v, const Team& t) {
+#pragma unroll
+    for (int m = CF_COL_TW / 2; m >= 1; m >>= 1) {
+        v.x += gshfl_xor_d(v.x, m, t);
+        v.y += gshfl_xor_d(v.y, m, t);
+    }
+    return v;
+}
+CF_DEV double group_sum_d(double v, const Team& t) {
+#pragma unroll
+    for (int m = CF_COL_TW / 2; m >= 1; m >>= 1) v += gshfl_xor_d(v, m, t);
+    return v;
+}
+// inclusive additive scan in lane order
+CF_DEV zd group_scan_z(zd v, const Team& t) {
+#pragma unroll
+    for (int d = 1; d < CF_COL_TW; d <<= 1) {
+        zd o = gshfl_up_z(v, d, t);
+        if (t.lane >= d) v = zadd(v, o);
+    }
+    return v;
+}
+// inclusive scan of affine maps f_i(x) = G_i + M_i x under composition in
+// lane order: the result of lane j is f_j o ... o f_0
+CF_DEV void group_scan_affine(double& M, zd& G, const Team& t) {
+#pragma unroll
+    for (int d = 1; d < CF_COL_TW; d <<= 1) {
+        double Mo = gshfl_up_d(M, d, t);
+        zd Go = gshfl_up_z(G, d, t);
+        if (t.lane >= d) {
+            G = zaxpy(G, M, Go);
+            M = M * Mo;
+        }
+    }
 }
 // Offset of the odd half: P/2 + 1 (the even degrees) rounded up to 4 mod 8
 // complex.  A loop over consecutive degrees puts the 8 threads of a 16-byte
@@ -71,8 +134,8 @@ CF_DEV int ppos(int n, int hs) { return (n & 1) * hs + (n >> 1); }
 // number of degrees of parity q in 0..P (P even)
 CF_DEV int pcount(int q, int P) { return q ? (P >> 1) : (P >> 1) + 1; }
 
-// Both warps obtain the warp-uniform value v of each warp: a from warp 0, b
-// from warp 1.
+// Both groups obtain the group-uniform value v of each group: a from group 0,
+// b from group 1.
 CF_DEV void team_xchg(const Team& t, zd v, zd& a, zd& b) {
     if (t.lane == 0) t.xch[t.q] = v;
     tsync(t);
@@ -81,21 +144,21 @@ CF_DEV void team_xchg(const Team& t, zd v, zd& a, zd& b) {
     tsync(t);
 }
 
-// Exclusive form of an inclusive warp scan result.
-CF_DEV zd warp_excl_z(zd inc, int lane) {
-    zd o = shfl_up_z(inc, 1);
-    return lane == 0 ? zzero() : o;
+// Exclusive form of an inclusive group scan result.
+CF_DEV zd group_excl_z(zd inc, const Team& t) {
+    zd o = gshfl_up_z(inc, 1, t);
+    return t.lane == 0 ? zzero() : o;
 }
 
-// Elements per lane of a chain of cnt elements scanned by one warp (odd),
+// Elements per lane of a chain of cnt elements scanned by one group (odd),
 // and its largest value for the chains of a compile-time length PL (chains
 // of at most (PL/2 + 1) elements): the loops over a lane's run are unrolled
 // to that bound, so the run's loads issue together and its values stay in
 // registers between the two passes of a scan.
-CF_DEV int run_len(int cnt) { return ((cnt + 31) >> 5) | 1; }
+CF_DEV int run_len(int cnt) { return ((cnt + CF_COL_TW - 1) / CF_COL_TW) | 1; }
 template <int PL>
 __host__ __device__ constexpr int run_max() {
-    return PL ? ((((PL >> 1) + 1) + 31) >> 5) | 1 : 0;
+    return PL ? ((((PL >> 1) + 1) + CF_COL_TW - 1) / CF_COL_TW) | 1 : 0;
 }
 
 // b = D a  (b != a).  Warp q writes the degrees of parity q of b from the
@@ -130,7 +193,7 @@ CF_DEV void col_diff_body(const zd* a, zd* b, const Team& t) {
             const int i = i0 + s, m = top - 2 * i;
             if (s < E && i < cnt && m >= 1) tot = zaxpy(tot, (double)m, v[s]);
         }
-        zd run = warp_excl_z(warp_scan_z(tot, lane), lane);
+        zd run = group_excl_z(group_scan_z(tot, t), t);
         if (MODE == CF_DIFF_INPLACE) tsync(t);  // every input read before any output is written
 #pragma unroll
         for (int s = 0; s < EM; ++s) {
@@ -149,7 +212,7 @@ CF_DEV void col_diff_body(const zd* a, zd* b, const Team& t) {
             const int m = top - 2 * i;
             if (i < cnt && m >= 1) tot = zaxpy(tot, (double)m, ah[m >> 1]);
         }
-        zd run = warp_excl_z(warp_scan_z(tot, lane), lane);
+        zd run = group_excl_z(group_scan_z(tot, t), t);
         for (int s = 0; s < E; ++s) {
             const int i = i0 + s;
             const int m = top - 2 * i;
@@ -179,18 +242,18 @@ CF_DEV void col_diff(const zd* a, zd* b, const Team& t) {
 CF_DEV void col_stage_factors(double* fa, double* fw, const double* __restrict__ src, const Team& t) {
     const int P = t.P, Ny = P + 1, hs = t.hs, q = t.q;
     const int nq = pcount(q, P);
-    for (int base = t.lane; base < nq; base += 5 * 32) {
+    for (int base = t.lane; base < nq; base += 5 * CF_COL_TW) {
         double v[3][5];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
             for (int u = 0; u < 5; ++u) {
-                const int j = base + 32 * u;
+                const int j = base + CF_COL_TW * u;
                 v[r][u] = j < nq ? __ldg(src + (long)r * Ny + 2 * j + q) : 0.0;
             }
 #pragma unroll
         for (int u = 0; u < 5; ++u) {
-            const int j = base + 32 * u;
+            const int j = base + CF_COL_TW * u;
             if (j < nq) {
                 fa[q * hs + j] = v[0][u];
                 fa[2 * hs + q * hs + j] = v[1][u];
@@ -207,7 +270,7 @@ CF_DEV void col_stage_factors(double* fa, double* fw, const double* __restrict__
 CF_DEV void col_stage_factors_async(double* fa, double* fw, const double* __restrict__ src, const Team& t) {
     const int P = t.P, Ny = P + 1, hs = t.hs, q = t.q;
     const int nq = pcount(q, P);
-    for (int j = t.lane; j < nq; j += 32) {
+    for (int j = t.lane; j < nq; j += CF_COL_TW) {
         const double* s = src + 2 * j + q;
         cp_async_el<8>(fa + q * hs + j, s, true);
         cp_async_el<8>(fa + 2 * hs + q * hs + j, s + Ny, true);
@@ -278,8 +341,8 @@ CF_DEV void col_helm_runs(zd* x, zd* scr, const double* alpha, const double* inv
             Gc = zaxpy(g[s], Ms[s], Gc);
             Mc *= Ms[s];
         }
-    warp_scan_affine(Mc, Gc, lane);
-    zd xv = warp_excl_z(Gc, lane);
+    group_scan_affine(Mc, Gc, t);
+    zd xv = group_excl_z(Gc, t);
     zd sw = zzero();
 #pragma unroll
     for (int s = 0; s < EM; ++s) {
@@ -291,7 +354,7 @@ CF_DEV void col_helm_runs(zd* x, zd* scr, const double* alpha, const double* inv
             sw = zaxpy(sw, WH(n), xv);
         }
     }
-    sw = warp_sum_z(sw);
+    sw = group_sum_z(sw, t);
     const zd a0 = zscale(zsub(q ? bc1 : bc0, sw), 1.0 / (q ? SA1 : SA0));
     __syncwarp();
     // forward sweep a_n = alpha_n a_{n-2} + beta_n, chain n = q+2, q+4, ..., top
@@ -315,9 +378,9 @@ CF_DEV void col_helm_runs(zd* x, zd* scr, const double* alpha, const double* inv
             Gc = zaxpy(bv[s], av[s], Gc);
             Mc *= av[s];
         }
-    warp_scan_affine(Mc, Gc, lane);
-    const double Me = __shfl_up_sync(0xffffffffu, Mc, 1);
-    const zd Ge = warp_excl_z(Gc, lane);
+    group_scan_affine(Mc, Gc, t);
+    const double Me = gshfl_up_d(Mc, 1, t);
+    const zd Ge = group_excl_z(Gc, t);
     xv = (lane == 0) ? a0 : zaxpy(Ge, Me, a0);
 #pragma unroll
     for (int s = 0; s < EM; ++s) {
@@ -368,8 +431,8 @@ CF_DEV void col_helm_body(zd* x, zd* scr, const double* alpha, const double* inv
             Mc *= M;
         }
     }
-    warp_scan_affine(Mc, Gc, lane);
-    zd xv = warp_excl_z(Gc, lane);
+    group_scan_affine(Mc, Gc, t);
+    zd xv = group_excl_z(Gc, t);
     zd sw = zzero();
     for (int s = 0; s < E; ++s) {
         const int i = i0 + s;
@@ -382,7 +445,7 @@ CF_DEV void col_helm_body(zd* x, zd* scr, const double* alpha, const double* inv
             sw = zaxpy(sw, wh[n >> 1], xv);
         }
     }
-    sw = warp_sum_z(sw);
+    sw = group_sum_z(sw, t);
     const zd a0 = zscale(zsub(q ? bc1 : bc0, sw), 1.0 / (q ? SA1 : SA0));
     __syncwarp();
     // forward sweep a_n = alpha_n a_{n-2} + beta_n, chain n = q+2, q+4, ..., top
@@ -397,9 +460,9 @@ CF_DEV void col_helm_body(zd* x, zd* scr, const double* alpha, const double* inv
             Mc *= M;
         }
     }
-    warp_scan_affine(Mc, Gc, lane);
-    const double Me = __shfl_up_sync(0xffffffffu, Mc, 1);
-    const zd Ge = warp_excl_z(Gc, lane);
+    group_scan_affine(Mc, Gc, t);
+    const double Me = gshfl_up_d(Mc, 1, t);
+    const zd Ge = group_excl_z(Gc, t);
     xv = (lane == 0) ? a0 : zaxpy(Ge, Me, a0);
     for (int s = 0; s < E; ++s) {
         const int jj = i0 + s;
@@ -475,7 +538,7 @@ CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const F
             x1 = zaxpy(x1, 2.0 * c.x, d);
         }
     }
-    x1 = warp_sum_z(x1);
+    x1 = group_sum_z(x1, t);
     if (t.lane == 0) t.xch[t.q] = x1;
     tsync(t);
     x1 = zadd(t.xch[0], t.xch[1]);
@@ -499,7 +562,7 @@ CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const F
 #pragma unroll
             for (int s = 0; s < EM; ++s)
                 if (s < E && m0 + s >= 1 && m0 + s < H) tot = zadd(tot, d[s]);
-            zd run = zadd(x1, warp_excl_z(warp_scan_z(tot, lane), lane));
+            zd run = zadd(x1, group_excl_z(group_scan_z(tot, t), t));
 #pragma unroll
             for (int s = 0; s < EM; ++s) {
                 const int m = m0 + s;
@@ -514,7 +577,7 @@ CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const F
                 const int m = m0 + s;
                 if (m >= 1 && m < H) tot = zadd(tot, zmuli(zsub(Z[fpos(m)], Z[fpos(P - m)])));
             }
-            zd run = zadd(x1, warp_excl_z(warp_scan_z(tot, lane), lane));
+            zd run = zadd(x1, group_excl_z(group_scan_z(tot, t), t));
             for (int s = 0; s < E; ++s) {
                 const int m = m0 + s;
                 if (m < H) {
@@ -524,7 +587,7 @@ CF_DEV void col_redft00(zd* x, zd* z, zd* z2, const zd* __restrict__ cs, const F
             }
         }
     } else {
-        for (int m = t.lane; m <= H; m += 32)
+        for (int m = t.lane; m <= H; m += CF_COL_TW)
             x[m] = (m == 0 || m == H) ? zscale(Z[fpos(m)], MODE == CF_DCT_FWD ? 1.0 : 2.0)
                                       : zadd(Z[fpos(m)], Z[fpos(P - m)]);
     }
@@ -642,8 +705,8 @@ CF_DEV void col_redft00_pair(zd* xa, zd* xb, zd* z, int bs, const zd* __restrict
             x1b = zaxpy(x1b, 2.0 * c.x, d2);
         }
     }
-    x1a = warp_sum_z(x1a);
-    x1b = warp_sum_z(x1b);
+    x1a = group_sum_z(x1a, t);
+    x1b = group_sum_z(x1b, t);
     if (t.lane == 0) {
         t.xch[t.q] = x1a;
         t.xch[2 + t.q] = x1b;
@@ -673,8 +736,8 @@ CF_DEV void col_redft00_pair(zd* xa, zd* xb, zd* z, int bs, const zd* __restrict
                 ta = zadd(ta, da[s]);
                 tb = zadd(tb, db[s]);
             }
-        zd ra = zadd(x1a, warp_excl_z(warp_scan_z(ta, lane), lane));
-        zd rb = zadd(x1b, warp_excl_z(warp_scan_z(tb, lane), lane));
+        zd ra = zadd(x1a, group_excl_z(group_scan_z(ta, t), t));
+        zd rb = zadd(x1b, group_excl_z(group_scan_z(tb, t), t));
         zd* xoa = xa + hs;
         zd* xob = xb + hs;
 #pragma unroll
@@ -691,7 +754,7 @@ CF_DEV void col_redft00_pair(zd* xa, zd* xb, zd* z, int bs, const zd* __restrict
         }
     } else {
         const double ew = MODE == CF_DCT_FWD ? 1.0 : 2.0;
-        for (int m = t.lane; m <= H; m += 32) {
+        for (int m = t.lane; m <= H; m += CF_COL_TW) {
             const bool end = m == 0 || m == H;
             xa[m] = end ? zscale(z[fpos(m)], ew) : zadd(z[fpos(m)], z[fpos(P - m)]);
             xb[m] = end ? zscale(zb[fpos(m)], ew) : zadd(zb[fpos(m)], zb[fpos(P - m)]);
@@ -705,11 +768,11 @@ CF_DEV void col_redft00_pair(zd* xa, zd* xb, zd* z, int bs, const zd* __restrict
 CF_DEV zd col_bulkmean(const zd* a, const Team& t) {
     zd s = zzero();
     if (t.q == 0) {
-        for (int j = t.lane; j <= (t.P >> 1); j += 32) {
+        for (int j = t.lane; j <= (t.P >> 1); j += CF_COL_TW) {
             const double n = 2.0 * j;
             s = (j == 0) ? zadd(s, a[0]) : zaxpy(s, 1.0 / (1.0 - n * n), a[j]);
         }
-        s = warp_sum_z(s);
+        s = group_sum_z(s, t);
     }
     zd m0, m1;
     team_xchg(t, s, m0, m1);
@@ -720,11 +783,11 @@ CF_DEV void col_wallderiv(const zd* a, const Team& t, zd& right, zd& left) {
     const int q = t.q, nq = pcount(q, t.P);
     const zd* ah = a + q * t.hs;
     zd s = zzero();
-    for (int j = t.lane; j < nq; j += 32) {
+    for (int j = t.lane; j < nq; j += CF_COL_TW) {
         const double n = 2.0 * j + q;
         s = zaxpy(s, n * n, ah[j]);
     }
-    s = warp_sum_z(s);
+    s = group_sum_z(s, t);
     zd s0, s1;
     team_xchg(t, s, s0, s1);
     right = zadd(s0, s1);

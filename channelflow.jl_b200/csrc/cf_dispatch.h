@@ -17,18 +17,33 @@ static_assert(CF_NCOL == 1 || CF_NCOL == 2, "column teams use named barriers 1 a
 // instantiations; other sizes use the run-time-sized one (argument 0).
 #define CF_COL_LENGTHS(X) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384)
 
+__host__ __device__ constexpr bool col_static_length(int P) {
+#define CF_CASE(N) P == N ||
+    return CF_COL_LENGTHS(CF_CASE) false;
+#undef CF_CASE
+}
+// Threads per column of the column kernels of length P: one warp (a half warp
+// per parity) for the compile-time lengths up to 64, two warps otherwise (the
+// CF_TEAM of the length's translation unit).
+__host__ __device__ constexpr int col_team_threads(int P) { return (col_static_length(P) && P <= 64) ? 32 : 64; }
+
 typedef void (*ColKernel)(ColParams);
 typedef void (*FftKernel)(FftParams);
 typedef void (*DiagKernel)(ColParams, double*, double*);
 typedef void (*ColBatchKernel)(const ColParams*, int, int, unsigned*);
 // Variants of the batched column kernel the ensemble autotuner chooses from:
-// (columns per block, blocks per SM of the register bound).  Variant 0 is the
+// (columns per block, blocks per SM of the register bound, for two-warp
+// teams; 3/2 as many blocks for one-warp teams).  Variant 0 is the
 // single-instance kernel's shape; 1-5 exist for P <= 128 (fewer registers,
 // more blocks per SM).
 #define CF_COL_BATCH_VARIANTS 6
 static constexpr int kColBatchNcol[CF_COL_BATCH_VARIANTS] = {CF_NCOL, 2, 2, 1, 1, 1};
 static constexpr int kColBatchMinb[CF_COL_BATCH_VARIANTS] = {0, 6, 8, 8, 12, 16};
 __host__ __device__ constexpr bool col_batch_variants(int P) { return P != 0 && P <= 128; }
+// blocks per SM of variant v at length P (the CF_MINB of cf_inst_col.cu)
+static inline int col_batch_minb(int P, int v) {
+    return col_team_threads(P) == 64 ? kColBatchMinb[v] : 3 * kColBatchMinb[v] / 2;
+}
 typedef void (*FftBatchKernel)(const FftParams*);
 typedef void (*FftTmaKernel)(FftParams, FftMaps);
 

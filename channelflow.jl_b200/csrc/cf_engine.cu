@@ -559,20 +559,14 @@ static size_t col_smem(const cf_engine* h, int ncol = CF_NCOL) {
 // The tensor-core forms' stage kernel at a compile-time length keeps six
 // regions per column and no transform buffers (its Chebyshev transforms run
 // outside): launched with zs = 0 and this shared memory.
-static bool col_static_len(int P) {
-    switch (P) {
-#define CF_CASE(N) \
-    case N: return true;
-        CF_COL_LENGTHS(CF_CASE)
-#undef CF_CASE
-        default: return false;
-    }
-}
-static bool stage_mx_noz(const cf_engine* h) { return h->tc && col_static_len(h->P); }
+static bool stage_mx_noz(const cf_engine* h) { return h->tc && col_static_length(h->P); }
 static size_t stage_mx_smem(const cf_engine* h) {
     if (!stage_mx_noz(h)) return col_smem(h);
     return ((size_t)CF_NCOL * 6 * col_stride(h) + CF_TEAM_SCRATCH * CF_NCOL) * sizeof(zd);
 }
+
+// threads per block of the handle's column kernels
+static int col_threads(const cf_engine* h) { return CF_NCOL * col_team_threads(h->P); }
 
 static ColParams col_params(const cf_engine* h) {
     ColParams p;
@@ -688,7 +682,7 @@ static int launch_periodic(cf_engine* h, int* count, zd* const* Nout = nullptr) 
     if (h->form == NL_DIV) {
         ColParams p = col_params(h);
         for (int i = 0; i < 3; ++i) p.Nout[i] = Nout ? Nout[i] : h->nod[i];
-        col_kernel(KC_DIV, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+        col_kernel(KC_DIV, h->P)<<<col_blocks(h), col_threads(h), col_smem(h), h->stream>>>(p);
         if (count) *count += 1;
         CU(cudaGetLastError());
     }
@@ -701,7 +695,7 @@ static int launch_prep(cf_engine* h, zd* const Usrc[3], int* count) {
     ColParams p = col_params(h);
     for (int i = 0; i < 3; ++i) p.U[i] = Usrc[i];
     const int kc = h->form == NL_CONV ? KC_PREP_CONV : (h->form == NL_DIV ? KC_PREP_DIV : KC_PREP);
-    col_kernel(kc, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    col_kernel(kc, h->P)<<<col_blocks(h), col_threads(h), col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return CF_OK;
@@ -725,7 +719,7 @@ static int launch_stage(cf_engine* h, int j, int* count) {
     int rc = launch_periodic(h, count);
     if (rc) return rc;
     ColParams p = stage_col_params(h, j);
-    col_kernel(stage_kernel_kind(h), h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    col_kernel(stage_kernel_kind(h), h->P)<<<col_blocks(h), col_threads(h), col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return CF_OK;
@@ -744,9 +738,9 @@ static int launch_step_profiled(cf_engine* h, cudaEvent_t* ev, double* acc) {
         if (h->form == NL_DIV) {
             ColParams pd = col_params(h);
             for (int i = 0; i < 3; ++i) pd.Nout[i] = h->nod[i];
-            col_kernel(KC_DIV, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(pd);
+            col_kernel(KC_DIV, h->P)<<<col_blocks(h), col_threads(h), col_smem(h), h->stream>>>(pd);
         }
-        col_kernel(stage_kernel_kind(h), h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+        col_kernel(stage_kernel_kind(h), h->P)<<<col_blocks(h), col_threads(h), col_smem(h), h->stream>>>(p);
         CU(cudaEventRecord(ev[4], h->stream));
         CU(cudaGetLastError());
         CU(cudaEventSynchronize(ev[4]));
@@ -973,7 +967,7 @@ static int launch_stage_mx(cf_engine* h, int j, int* count) {
         for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->nod32[i]);
         for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
         mx_state(h, p);
-        col_kernel(h->s32 ? KC_STAGE_MXS : KC_STAGE_MXD, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h),
+        col_kernel(h->s32 ? KC_STAGE_MXS : KC_STAGE_MXD, h->P)<<<col_blocks(h), col_threads(h), col_smem(h),
                                                                  h->stream>>>(p);
         if (count) *count += 1;
         CU(cudaGetLastError());
@@ -984,7 +978,7 @@ static int launch_stage_mx(cf_engine* h, int j, int* count) {
     for (int i = 0; i < 3; ++i) p.Nn[i] = static_cast<const zd*>(h->coef32[i]);
     for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->coef32[i]);
     if (stage_mx_noz(h)) p.zs = 0;
-    col_kernel(KC_STAGE_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, stage_mx_smem(h), h->stream>>>(p);
+    col_kernel(KC_STAGE_MX, h->P)<<<col_blocks(h), col_threads(h), stage_mx_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return launch_cheb(h, 6, true, count);
@@ -994,14 +988,14 @@ static int launch_prep_mx(cf_engine* h, int* count) {
     if (!h->tc) {
         for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->nod32[i]);
         mx_state(h, p);
-        col_kernel(h->s32 ? KC_PREP_MXS : KC_PREP_MXD, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h),
+        col_kernel(h->s32 ? KC_PREP_MXS : KC_PREP_MXD, h->P)<<<col_blocks(h), col_threads(h), col_smem(h),
                                                                h->stream>>>(p);
         if (count) *count += 1;
         CU(cudaGetLastError());
         return CF_OK;
     }
     for (int i = 0; i < 6; ++i) p.nod[i] = static_cast<zd*>(h->coef32[i]);
-    col_kernel(KC_PREP_MX, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    col_kernel(KC_PREP_MX, h->P)<<<col_blocks(h), col_threads(h), col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return launch_cheb(h, 6, true, count);
@@ -1058,7 +1052,7 @@ static int step_profiled_mx(cf_engine* h, double t, int nsteps, double* t_out, d
             if (h->tc && (rc = launch_cheb(h, 3, false, nullptr))) break;
             cudaEventRecord(ev[4], h->stream);
             col_kernel(h->tc ? KC_STAGE_MX : (h->s32 ? KC_STAGE_MXS : KC_STAGE_MXD), h->P)<<<
-                col_blocks(h), CF_NCOL * CF_TEAM, h->tc ? stage_mx_smem(h) : col_smem(h), h->stream>>>(p);
+                col_blocks(h), col_threads(h), h->tc ? stage_mx_smem(h) : col_smem(h), h->stream>>>(p);
             cudaEventRecord(ev[5], h->stream);
             if (h->tc && (rc = launch_cheb(h, 6, true, nullptr))) break;
             cudaEventRecord(ev[6], h->stream);
@@ -1309,7 +1303,7 @@ static int ensure_copy_stream(cf_engine* h) {
 static int launch_cols(cf_engine* h, int kind, ColParams p, unsigned b0, unsigned b1, int* count) {
     if (b1 <= b0) return CF_OK;
     p.bofs = (int)b0;
-    col_kernel(kind, h->P)<<<b1 - b0, CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    col_kernel(kind, h->P)<<<b1 - b0, col_threads(h), col_smem(h), h->stream>>>(p);
     if (count) *count += 1;
     CU(cudaGetLastError());
     return CF_OK;
@@ -1741,7 +1735,7 @@ static int launch_nonlinear(cf_engine* h, zd* const Us[3]) {
     if ((rc = launch_periodic(h, nullptr))) return rc;
     ColParams p = col_params(h);
     for (int i = 0; i < 3; ++i) p.Nout[i] = Us[i];
-    col_kernel(KC_NLOUT, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    col_kernel(KC_NLOUT, h->P)<<<col_blocks(h), col_threads(h), col_smem(h), h->stream>>>(p);
     CU(cudaGetLastError());
     return CF_OK;
 }
@@ -1790,7 +1784,7 @@ static int project_dev(cf_engine* h, zd* const Ud[3]) {
     else { p.cmode = 0; p.c1 = 0.0; p.c2 = 0.0; }
     double* gtmp = h->d_grad;
     p.grad_out = gtmp;
-    col_kernel(KC_PROJECT, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p);
+    col_kernel(KC_PROJECT, h->P)<<<col_blocks(h), col_threads(h), col_smem(h), h->stream>>>(p);
     CU(cudaGetLastError());
     return CF_OK;
 }
@@ -1805,7 +1799,7 @@ static int pressure_dev(cf_engine* h, zd* const Ud[3], zd* Pout) {
     p.Pf = Pout;
     p.bank = h->neum.view();
     // the divergence form's term arrives in nod[0..2] as coefficients
-    col_kernel(h->form == NL_DIV ? KC_PRESSURE_COEF : KC_PRESSURE, h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM,
+    col_kernel(h->form == NL_DIV ? KC_PRESSURE_COEF : KC_PRESSURE, h->P)<<<col_blocks(h), col_threads(h),
                                                                           col_smem(h), h->stream>>>(p);
     CU(cudaGetLastError());
     h->nodal_valid = false;
@@ -1887,7 +1881,7 @@ int cf_diagnostics(cf_handle* h, double* out) {
     if ((rc = ensure_diag(h)) || (rc = state_to64(h))) return rc;
     CU(cudaMemsetAsync(h->d_diag, 0, 8 * sizeof(double), h->stream));
     ColParams p = col_params(h);
-    diag_kernel(h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p, h->d_diag, h->d_diagpart);
+    diag_kernel(h->P)<<<col_blocks(h), col_threads(h), col_smem(h), h->stream>>>(p, h->d_diag, h->d_diagpart);
     k_diag_reduce<<<1, 1024, 0, h->stream>>>(h->d_diagpart, (int)col_blocks(h), h->d_diag);
     CU(cudaGetLastError());
     double acc[5];
@@ -1910,7 +1904,7 @@ static int record_diag(cf_engine* h, double* acc, int* count) {
     int rc;
     if ((rc = state_to64(h))) return rc;
     ColParams p = col_params(h);
-    diag_kernel(h->P)<<<col_blocks(h), CF_NCOL * CF_TEAM, col_smem(h), h->stream>>>(p, acc, h->d_diagpart);
+    diag_kernel(h->P)<<<col_blocks(h), col_threads(h), col_smem(h), h->stream>>>(p, acc, h->d_diagpart);
     k_diag_reduce<<<1, 1024, 0, h->stream>>>(h->d_diagpart, (int)col_blocks(h), acc);
     CU(cudaMemcpyAsync(acc + 5, h->d_grad, 2 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     k_power_input<<<1, 32, 0, h->stream>>>(h->U[0], h->U[2], h->d_base, (long)h->Nz * h->Nxh, h->Ny, h->nu, 0.0,
@@ -2305,9 +2299,9 @@ static int launch_class_stage(const cf_batch* b, const BatchClass& c, int j, cud
     const ColBatchKernel ck = col_batch_kernel(r->P, c.var);
     if (c.persist) {
         CU(cudaMemsetAsync(c.d_counter + j, 0, sizeof(unsigned), s));
-        ck<<<c.pgrid, ncol * CF_TEAM, col_smem(r, ncol), s>>>(c.d_col[j], nblk, nblk * (int)m, c.d_counter + j);
+        ck<<<c.pgrid, ncol * col_team_threads(r->P), col_smem(r, ncol), s>>>(c.d_col[j], nblk, nblk * (int)m, c.d_counter + j);
     } else {
-        ck<<<dim3((unsigned)nblk, m), ncol * CF_TEAM, col_smem(r, ncol), s>>>(c.d_col[j], nblk, nblk * (int)m, nullptr);
+        ck<<<dim3((unsigned)nblk, m), ncol * col_team_threads(r->P), col_smem(r, ncol), s>>>(c.d_col[j], nblk, nblk * (int)m, nullptr);
     }
     CU(cudaGetLastError());
     return CF_OK;
@@ -2412,7 +2406,7 @@ static int autotune_batch(cf_batch* b) {
                     const int ncol = kColBatchNcol[v];
                     const int nitems = (int)((r->B + ncol - 1) / ncol) * m;
                     int occ = 0;
-                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, col_batch_kernel(r->P, v), ncol * CF_TEAM,
+                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, col_batch_kernel(r->P, v), ncol * col_team_threads(r->P),
                                                                       col_smem(r, ncol)) != cudaSuccess || occ < 1) {
                         cudaGetLastError();
                         continue;
@@ -2423,7 +2417,7 @@ static int autotune_batch(cf_batch* b) {
                     if (c.persist && (int)c.pgrid >= nitems) continue;  // one wave: the same as a block per item
                     if ((rc = time_class(c, 8, ms))) break;
                     std::snprintf(buf, sizeof buf, "%s(%d,%d,%s) %.3f", cand.empty() ? "" : ", ", ncol,
-                                  v ? kColBatchMinb[v] : 0, c.persist ? "persistent" : "grid", ms);
+                                  v ? col_batch_minb(r->P, v) : 0, c.persist ? "persistent" : "grid", ms);
                     cand += buf;
                     if (ms < best) best = ms, bv = v, bp = c.persist, bg = c.pgrid;
                 }
@@ -2433,7 +2427,7 @@ static int autotune_batch(cf_batch* b) {
             c.pgrid = bg;
             total += best;
             std::snprintf(buf, sizeof buf, "; column kernel ncol=%d minb=%d %s (%.3f ms; candidates (ncol,minb,schedule) %s)",
-                          kColBatchNcol[bv], bv ? kColBatchMinb[bv] : 0,
+                          kColBatchNcol[bv], bv ? col_batch_minb(r->P, bv) : 0,
                           bp ? ("persistent grid " + std::to_string(bg)).c_str() : "one block per item", best,
                           cand.c_str());
             line += buf;

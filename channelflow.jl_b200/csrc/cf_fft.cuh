@@ -29,11 +29,12 @@ template <>
 CF_DEV const zf* plan_tw<zf>(const FftPlan& pl) { return pl.twf; }
 
 // Barrier of the thread group: a warp, the whole block (bar == 0), or a
-// 64-thread team on named barrier 1 or 2 (literal ids: a run-time id makes the
-// compiler reserve all sixteen barriers of the block).
+// column team on named barrier 1 or 2 (64 threads; a team of nth = 32 is one
+// warp and syncs as one; literal ids: a run-time id makes the compiler
+// reserve all sixteen barriers of the block).
 template <bool BLOCK>
-CF_DEV void group_sync(int bar, int) {
-    if (!BLOCK) __syncwarp();
+CF_DEV void group_sync(int bar, int nth) {
+    if (!BLOCK || (bar != 0 && nth == 32)) __syncwarp();
     else if (bar == 1) asm volatile("bar.sync 1, 64;" ::: "memory");
     else if (bar == 2) asm volatile("bar.sync 2, 64;" ::: "memory");
     else __syncthreads();

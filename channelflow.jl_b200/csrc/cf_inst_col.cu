@@ -5,6 +5,11 @@
 #ifndef CF_INST_P
 #error "compile with -DCF_INST_P=<length>"
 #endif
+static_assert(CF_TEAM == col_team_threads(CF_INST_P), "the unit's team size is the host's");
+// blocks per SM of a batched variant: n for two-warp teams, 3n/2 for one-warp
+// teams (a register bound between the two-warp variants' and twice as many
+// columns per SM)
+#define CF_MINB(n) (CF_TEAM == 64 ? (n) : 3 * (n) / 2)
 
 template <int P>
 ColKernel col_kernel_for(int which) {
@@ -36,11 +41,11 @@ template <int P>
 ColBatchKernel col_batch_kernel_for(int variant) {
     if constexpr (col_batch_variants(P)) {
         switch (variant) {
-            case 1: return k_column_stage_batch<2, P, 6>;
-            case 2: return k_column_stage_batch<2, P, 8>;
-            case 3: return k_column_stage_batch<1, P, 8>;
-            case 4: return k_column_stage_batch<1, P, 12>;
-            case 5: return k_column_stage_batch<1, P, 16>;
+            case 1: return k_column_stage_batch<2, P, CF_MINB(6)>;
+            case 2: return k_column_stage_batch<2, P, CF_MINB(8)>;
+            case 3: return k_column_stage_batch<1, P, CF_MINB(8)>;
+            case 4: return k_column_stage_batch<1, P, CF_MINB(12)>;
+            case 5: return k_column_stage_batch<1, P, CF_MINB(16)>;
             default: break;
         }
     }

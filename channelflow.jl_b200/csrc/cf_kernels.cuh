@@ -78,7 +78,7 @@ CF_DEV T* sel3(T* a, T* b, T* c, int i) {
 // smaller sizes are held to 128 registers (8 or more columns per SM).
 template <int NCOL, int PL>
 constexpr int col_minblocks() {
-    return (PL == 0 || PL >= 256) ? 6 / NCOL : 8 / NCOL;
+    return ((PL == 0 || PL >= 256) ? 6 / NCOL : 8 / NCOL) * (64 / CF_TEAM);
 }
 
 // Team scratch per column in shared memory (complex units): four for the
@@ -99,8 +99,9 @@ struct ColCtx {
         zs = p.zs;
         const int tm = threadIdx.x / CF_TEAM;
         t.tid = threadIdx.x - tm * CF_TEAM;
-        t.q = t.tid >> 5;
-        t.lane = t.tid & 31;
+        t.q = t.tid / CF_COL_TW;
+        t.lane = t.tid % CF_COL_TW;
+        t.gm = CF_COL_TW == 32 ? 0xffffffffu : (0xffffu << (threadIdx.x & 16));
         t.bar = 1 + tm;
         t.P = PL ? PL : p.P;
         t.hs = col_half_stride(t.P);
@@ -345,7 +346,7 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
             zd* x = it ? V : PT;
             if (!GF) col_stage_factors_async(fa, fw, fsrc, t);
             col_diff<PL>(it ? PT : R1, x, t);
-            for (int j = lane; j < nq; j += 32) {
+            for (int j = lane; j < nq; j += CF_COL_TW) {
                 const int o = qo + j;
                 x[o] = it ? zsub(x[o], R1[o]) : zadd(x[o], zadd(zmulis(R0[o], k), zmulis(R2[o], l)));
             }
@@ -364,23 +365,23 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         // overlap the reductions below (one memory round trip, not one per
         // element)
         const double* __restrict__ rs = bk.resp + (long)c * 6 * Ny;
-        constexpr int NIT = PL ? ((PL >> 1) + 1 + 31) / 32 : 1;
+        constexpr int NIT = PL ? ((PL >> 1) + 1 + CF_COL_TW - 1) / CF_COL_TW : 1;
         double rv[6][NIT];
         if constexpr (PL != 0) {
 #pragma unroll
             for (int u = 0; u < NIT; ++u) {
-                const int j = lane + 32 * u, n = 2 * j + q;
+                const int j = lane + CF_COL_TW * u, n = 2 * j + q;
 #pragma unroll
                 for (int a = 0; a < 6; ++a) rv[a][u] = j < nq ? __ldg(rs + a * Ny + n) : 0.0;
             }
         }
         zd s = zzero();
-        for (int j = lane; j < nq; j += 32) {
+        for (int j = lane; j < nq; j += CF_COL_TW) {
             const double n = 2.0 * j + q;
             s = zaxpy(s, n * n, V[qo + j]);
         }
         zd s0, s1;
-        team_xchg(t, warp_sum_z(s), s0, s1);
+        team_xchg(t, group_sum_z(s, t), s0, s1);
         // upper = -sum n^2 v_n, lower = sum (-1)^n n^2 v_n
         const zd up = zscale(zadd(s0, s1), -1.0), lo = zsub(s0, s1);
         const double i00 = sc[0], i01 = sc[1], i10 = sc[2], i11 = sc[3];
@@ -389,14 +390,14 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         if constexpr (PL != 0) {
 #pragma unroll
             for (int u = 0; u < NIT; ++u) {
-                const int j = lane + 32 * u, o = qo + j;
+                const int j = lane + CF_COL_TW * u, o = qo + j;
                 if (j < nq) {
                     PT[o] = zaxpy(zaxpy(PT[o], rv[0][u], dp), rv[1][u], dm);
                     V[o] = zaxpy(zaxpy(V[o], rv[2][u], dp), rv[3][u], dm);
                 }
             }
         } else {
-            for (int j = lane; j < nq; j += 32) {
+            for (int j = lane; j < nq; j += CF_COL_TW) {
                 const int n = 2 * j + q, o = qo + j;
                 PT[o] = zaxpy(zaxpy(PT[o], __ldg(rs + n), dp), __ldg(rs + Ny + n), dm);
                 V[o] = zaxpy(zaxpy(V[o], __ldg(rs + 2 * Ny + n), dp), __ldg(rs + 3 * Ny + n), dm);
@@ -413,14 +414,14 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         if constexpr (PL != 0) {
 #pragma unroll
             for (int u = 0; u < NIT; ++u) {
-                const int j = lane + 32 * u, o = qo + j;
+                const int j = lane + CF_COL_TW * u, o = qo + j;
                 if (j < nq) {
                     PT[o] = zaxpy(PT[o], rv[4][u], sp);
                     V[o] = zaxpy(V[o], rv[5][u], sv);
                 }
             }
         } else {
-            for (int j = lane; j < nq; j += 32) {
+            for (int j = lane; j < nq; j += CF_COL_TW) {
                 const int n = 2 * j + q, o = qo + j;
                 PT[o] = zaxpy(PT[o], __ldg(rs + 4 * Ny + n), sp);
                 V[o] = zaxpy(V[o], __ldg(rs + 5 * Ny + n), sv);
@@ -429,7 +430,7 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         tsync(t);
     } else {
         // mean mode (meanmode.jl:103-150): integrate Ry through degree P-1, gauge
-        for (int j = lane; j < nq; j += 32) {
+        for (int j = lane; j < nq; j += CF_COL_TW) {
             const int n = 2 * j + q, o = qo + j;
             zd v = zzero();
             if (n >= 1) {
@@ -446,7 +447,7 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
         tsync(t);
     }
     // tangential velocities: (nu D^2 - shift) u = i k p - Rx, likewise w
-    for (int j = lane; j < nq; j += 32) {
+    for (int j = lane; j < nq; j += CF_COL_TW) {
         const int o = qo + j;
         R0[o] = zsub(zmulis(PT[o], k), R0[o]);
         R2[o] = zsub(zmulis(PT[o], l), R2[o]);
@@ -471,7 +472,7 @@ CF_DEV void col_stokes(zd* R0, zd* R1, zd* R2, zd* PT, zd* V, zd* A, zd* F0, zd*
             gx = p.c1;
             gz = p.c2;
         }
-        for (int j = lane; j < nq; j += 32) {
+        for (int j = lane; j < nq; j += CF_COL_TW) {
             const int o = qo + j;
             const double r = __ldg(bk.meanc + 2 * j + q);
             R0[o] = zadd(R0[o], zmake(gx * r, 0.0));
@@ -500,13 +501,13 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
     const double k = p.ax * ix;
     const double l = p.bz * (iz <= (p.Nz >> 1) ? iz : iz - p.Nz);
     if (c == 0) {
-        for (int j = lane; j < nq; j += 32) U0[qo + j] = zadd(U0[qo + j], zmake(__ldg(p.base + 2 * j + q), 0.0));
+        for (int j = lane; j < nq; j += CF_COL_TW) U0[qo + j] = zadd(U0[qo + j], zmake(__ldg(p.base + 2 * j + q), 0.0));
         tsync(t);
     }
     if (FORM == NL_ROT) {
         col_diff<PL>(U2, W0, t);  // omega_x = D w - i l v
         col_diff<PL>(U0, W2, t);  // omega_z = i k v - D u
-        for (int j = lane; j < nq; j += 32) {
+        for (int j = lane; j < nq; j += CF_COL_TW) {
             const int o = qo + j;
             W0[o] = zsub(W0[o], zmulis(U1[o], l));
             if (MX) W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
@@ -540,7 +541,7 @@ CF_DEV void col_prep_nodal(zd* U0, zd* U1, zd* U2, zd* W0, zd* W1, zd* W2, zd* Z
         }
     }
     if (FORM == NL_ROT) {
-        for (int j = lane; j < nq; j += 32) {
+        for (int j = lane; j < nq; j += CF_COL_TW) {
             const int o = qo + j;
             W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
         }
@@ -691,7 +692,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
             if (p.stage > 0) {
                 zd* A = X.col(4);
                 const zd* Qo = X.col(qreg);
-                for (int j = lane; j < nq; j += 32) A[qo + j] = zaxpy(A[qo + j], p.Acoef, Qo[qo + j]);
+                for (int j = lane; j < nq; j += CF_COL_TW) A[qo + j] = zaxpy(A[qo + j], p.Acoef, Qo[qo + j]);
             }
         }
         __syncthreads();
@@ -727,7 +728,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
                 col_diff<PL, CF_DIFF_INPLACE>(R, R, t);
                 const zd* PT = X.col(3);
                 const double kl = (i == 0) ? k : l;
-                for (int j = lane; j < nq; j += 32) {
+                for (int j = lane; j < nq; j += CF_COL_TW) {
                     const int o = qo + j;
                     zd lap = zaxpy(R[o], -kap2, U[o]);
                     zd r = zaxpy(zscale(U[o], p.lambda), p.nu, lap);
@@ -744,7 +745,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
                 if (i == 1) col_diff<PL>(X.col(3), Z, t);
                 const zd* PT = X.col(3);
                 const double kl = (i == 0) ? k : l;
-                for (int j = lane; j < nq; j += 32) {
+                for (int j = lane; j < nq; j += CF_COL_TW) {
                     const int o = qo + j;
                     zd lap = zaxpy(R[o], -kap2, U[o]);
                     zd r = zaxpy(zscale(U[o], p.lambda), p.nu, lap);
@@ -769,7 +770,7 @@ CF_DEV void column_stage_body(const ColParams& p, int bx) {
             gold[0] = p.nu * (wR0.x - wL0.x) / 2 + p.nu_bm_curv + bulkN0.x;
             gold[1] = p.nu * (wR2.x - wL2.x) / 2 + bulkN2.x;
         }
-        for (int j = lane; j < nq; j += 32)
+        for (int j = lane; j < nq; j += CF_COL_TW)
             R0[qo + j] = zadd(R0[qo + j], zmake(2.0 * p.nu * __ldg(p.basecurv + 2 * j + q), 0.0));
         tsync(t);
         if (t.tid == 0) {
@@ -937,7 +938,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
             const zd* a = X.col(ra[r]);
             const zd* cz = X.col(rc[r]);
             zd* o = X.col(ro[r]);
-            for (int j = t.lane; j < nq; j += 32) {
+            for (int j = t.lane; j < nq; j += CF_COL_TW) {
                 const int e = qo + j;
                 o[e] = zadd(zadd(zmulis(a[e], k), D[e]), zmulis(cz[e], l));
             }
@@ -991,7 +992,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
             zd* R = X.col(i);
             col_diff<PL>(U, Z, t);
             col_diff<PL>(Z, R, t);
-            for (int j = t.lane; j < nq; j += 32) R[qo + j] = zscale(zaxpy(R[qo + j], -kap2, U[qo + j]), -1.0);
+            for (int j = t.lane; j < nq; j += CF_COL_TW) R[qo + j] = zscale(zaxpy(R[qo + j], -kap2, U[qo + j]), -1.0);
         }
         __syncthreads();
     }
@@ -1044,7 +1045,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
             col_zero(PT, t);
             tsync(t);
         } else if (c == 0) {
-            for (int j = lane; j < nq; j += 32) {
+            for (int j = lane; j < nq; j += CF_COL_TW) {
                 const int n = 2 * j + q;
                 zd v = zzero();
                 if (n >= 1) {
@@ -1061,7 +1062,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
         } else {
             col_diff<PL>(A1, PT, t);
             zd su = zzero();
-            for (int j = lane; j < nq; j += 32) {
+            for (int j = lane; j < nq; j += CF_COL_TW) {
                 const int n = 2 * j + q, o = qo + j;
                 PT[o] = zadd(PT[o], zadd(zmulis(A0[o], k), zmulis(A2[o], l)));
                 su = zadd(su, A1[o]);
@@ -1071,7 +1072,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
                 }
             }
             zd s0, s1;
-            team_xchg(t, warp_sum_z(su), s0, s1);
+            team_xchg(t, group_sum_z(su, t), s0, s1);
             const zd up = zadd(s0, s1), lo = zsub(s0, s1);
             const double* sa = p.bank.sa + (long)c * 4;
             // Neumann parity data: even rows (up - lo)/2, odd rows (up + lo)/2
@@ -1104,7 +1105,7 @@ CF_DEV double diag_form(const zd* a, const double* mom, const Team& t) {
     // have equal parity, so only even moments occur: mom[h] = mom(2h).
     const int q = t.q, qo = q * t.hs, nq = pcount(q, t.P);
     double s = 0.0;
-    for (int j = t.lane; j < nq; j += 32) {
+    for (int j = t.lane; j < nq; j += CF_COL_TW) {
         const int m = 2 * j + q;
         const zd am = a[qo + j];
         zd acc[4] = {zzero(), zzero(), zzero(), zzero()};
@@ -1122,13 +1123,13 @@ CF_DEV double diag_form(const zd* a, const double* mom, const Team& t) {
         const double Mmm = 0.5 * (mom[m] + mom[0]);
         s += Mmm * (am.x * am.x + am.y * am.y) + (am.x * off.x + am.y * off.y);  // Re(conj(a_m) ...)
     }
-    return warp_sum_d(s);
+    return group_sum_d(s, t);
 }
 
 // The same form for a compile-time length, register-tiled over the upper
 // triangle of E x E blocks.  The nq indices of a parity form NB = ceil(nq/E)
 // blocks; the NB (NB + 1) / 2 block pairs (b <= c) are dealt to the lanes in
-// turn (pair k to lane k mod 32), so every lane does the same number of pairs
+// turn (pair k to lane k mod CF_COL_TW), so every lane does the same number of pairs
 // and no lane walks a longer triangle row than another.  A pair needs its 2E
 // coefficients, 2E - 1 Hankel moments mom[jb + ic + q + k] and 2E - 1
 // Toeplitz moments mom[|ic - jb - (E-1) + k|] (k = 0 .. 2E-2) for its E x E
@@ -1141,7 +1142,7 @@ CF_DEV double diag_form_tiled(const zd* a, const double* mom, const Team& t) {
     const int q = t.q, qo = q * t.hs, nq = pcount(q, t.P), P = t.P;
     const int NB = (nq + E - 1) / E, npair = NB * (NB + 1) / 2;
     double s = 0.0;
-    for (int k = t.lane; k < npair; k += 32) {
+    for (int k = t.lane; k < npair; k += CF_COL_TW) {
         // row b of the triangle starts at pair b NB - b (b - 1) / 2
         const double w = 2.0 * NB + 1.0;
         int b = (int)((w - sqrt(w * w - 8.0 * k)) * 0.5);
@@ -1171,7 +1172,7 @@ CF_DEV double diag_form_tiled(const zd* a, const double* mom, const Team& t) {
         }
         s += (b < c ? 2.0 : 1.0) * ps;
     }
-    return 0.5 * warp_sum_d(s);
+    return 0.5 * group_sum_d(s, t);
 }
 
 template <int NCOL, int PL>
@@ -1206,7 +1207,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
         col_diff<PL>(U2, W0, t);
         col_diff<PL>(U0, W2, t);
         col_diff<PL>(U1, DV, t);
-        for (int j = lane; j < nq; j += 32) {
+        for (int j = lane; j < nq; j += CF_COL_TW) {
             const int o = qo + j;
             W0[o] = zsub(W0[o], zmulis(U1[o], l));
             W1[o] = zmuli(zsub(zscale(U0[o], l), zscale(U2[o], k)));
@@ -1240,8 +1241,9 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
             dis *= w;
         }
     }
-    // block partials (no same-address atomics: summed by k_diag_reduce)
-    const int wi = threadIdx.x >> 5;
+    // block partials, one per parity group (no same-address atomics: summed by
+    // k_diag_reduce)
+    const int wi = threadIdx.x / CF_COL_TW;
     if (lane == 0) {
         red[0][wi] = e;
         red[1][wi] = dis;
