@@ -35,7 +35,10 @@
 // compiled in their own translation unit (CF_INST_P), so the width is a
 // constant of the unit; the host takes a length's team size from
 // col_team_threads (cf_dispatch.h).
-#if defined(CF_INST_P) && CF_INST_P != 0 && CF_INST_P <= 64
+#ifndef CF_COL_TW_MAXP
+#define CF_COL_TW_MAXP 64  // longest compile-time length with one-warp teams
+#endif
+#if defined(CF_INST_P) && CF_INST_P != 0 && CF_INST_P <= CF_COL_TW_MAXP
 #define CF_COL_TW 16
 #else
 #define CF_COL_TW 32

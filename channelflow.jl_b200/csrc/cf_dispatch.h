@@ -25,7 +25,9 @@ __host__ __device__ constexpr bool col_static_length(int P) {
 // Threads per column of the column kernels of length P: one warp (a half warp
 // per parity) for the compile-time lengths up to 64, two warps otherwise (the
 // CF_TEAM of the length's translation unit).
-__host__ __device__ constexpr int col_team_threads(int P) { return (col_static_length(P) && P <= 64) ? 32 : 64; }
+__host__ __device__ constexpr int col_team_threads(int P) {
+    return (col_static_length(P) && P <= CF_COL_TW_MAXP) ? 32 : 64;
+}
 
 typedef void (*ColKernel)(ColParams);
 typedef void (*FftKernel)(FftParams);

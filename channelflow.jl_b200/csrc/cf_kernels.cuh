@@ -75,10 +75,13 @@ CF_DEV T* sel3(T* a, T* b, T* c, int i) {
 
 // Blocks per SM the column kernels are compiled for (bounds their registers):
 // at P >= 256 shared memory allows 6 columns per SM, so 168 registers; the
-// smaller sizes are held to 128 registers (8 or more columns per SM).
+// smaller sizes are held to 128 registers (8 or more columns per SM).  One-warp
+// teams: 16 columns per SM at P <= 64 (128 registers), 12 for the longer ones
+// (170 registers).
 template <int NCOL, int PL>
 constexpr int col_minblocks() {
-    return ((PL == 0 || PL >= 256) ? 6 / NCOL : 8 / NCOL) * (64 / CF_TEAM);
+    if constexpr (CF_TEAM == 32) return (PL <= 64 ? 16 : 12) / NCOL;  // one-warp teams: 16 or 12 columns
+    return (PL == 0 || PL >= 256) ? 6 / NCOL : 8 / NCOL;
 }
 
 // Team scratch per column in shared memory (complex units): four for the
