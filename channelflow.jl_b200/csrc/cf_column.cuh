@@ -40,8 +40,10 @@
 #endif
 #if defined(CF_INST_P) && CF_INST_P != 0 && CF_INST_P <= CF_COL_TW_MAXP
 #define CF_COL_TW 16
+#define CF_COL_TW_LOG2 4
 #else
 #define CF_COL_TW 32
+#define CF_COL_TW_LOG2 5
 #endif
 #define CF_TEAM (2 * CF_COL_TW)  // threads per column
 
@@ -62,7 +64,9 @@ struct Team {
     int lane;  // lane in the group (0 .. CF_COL_TW - 1)
     int tid;   // 0 .. CF_TEAM - 1
     int bar;   // named barrier of the team (1 or 2)
+#if CF_COL_TW == 16
     unsigned gm;  // the group's lanes in its warp (the mask of its shuffles)
+#endif
     int P;     // highest degree (even)
     int hs;    // half stride: col_half_stride(P)
     zd* xch;   // four complex of team scratch in shared memory
@@ -83,9 +87,14 @@ CF_DEV void tsync(const Team& t) {
 
 // Collectives of one parity group (its lanes, width CF_COL_TW): the mask names
 // the group's own lanes, so a group may call them in a branch the other group
-// of its warp does not take.
-CF_DEV double gshfl_up_d(double v, int d, const Team& t) { return __shfl_up_sync(t.gm, v, d, CF_COL_TW); }
-CF_DEV double gshfl_xor_d(double v, int m, const Team& t) { return __shfl_xor_sync(t.gm, v, m, CF_COL_TW); }
+// of its warp does not take (a whole warp: the constant full mask).
+#if CF_COL_TW == 16
+CF_DEV unsigned gmask(const Team& t) { return t.gm; }
+#else
+CF_DEV unsigned gmask(const Team&) { return 0xffffffffu; }
+#endif
+CF_DEV double gshfl_up_d(double v, int d, const Team& t) { return __shfl_up_sync(gmask(t), v, d, CF_COL_TW); }
+CF_DEV double gshfl_xor_d(double v, int m, const Team& t) { return __shfl_xor_sync(gmask(t), v, m, CF_COL_TW); }
 CF_DEV zd gshfl_up_z(zd v, int d, const Team& t) {
     return make_double2(gshfl_up_d(v.x, d, t), gshfl_up_d(v.y, d, t));
 }
@@ -158,10 +167,10 @@ CF_DEV zd group_excl_z(zd inc, const Team& t) {
 // of at most (PL/2 + 1) elements): the loops over a lane's run are unrolled
 // to that bound, so the run's loads issue together and its values stay in
 // registers between the two passes of a scan.
-CF_DEV int run_len(int cnt) { return ((cnt + CF_COL_TW - 1) / CF_COL_TW) | 1; }
+CF_DEV int run_len(int cnt) { return ((cnt + CF_COL_TW - 1) >> CF_COL_TW_LOG2) | 1; }
 template <int PL>
 __host__ __device__ constexpr int run_max() {
-    return PL ? ((((PL >> 1) + 1) + CF_COL_TW - 1) / CF_COL_TW) | 1 : 0;
+    return PL ? ((((PL >> 1) + 1) + CF_COL_TW - 1) >> CF_COL_TW_LOG2) | 1 : 0;
 }
 
 // b = D a  (b != a).  Warp q writes the degrees of parity q of b from the

@@ -102,9 +102,11 @@ struct ColCtx {
         zs = p.zs;
         const int tm = threadIdx.x / CF_TEAM;
         t.tid = threadIdx.x - tm * CF_TEAM;
-        t.q = t.tid / CF_COL_TW;
-        t.lane = t.tid % CF_COL_TW;
-        t.gm = CF_COL_TW == 32 ? 0xffffffffu : (0xffffu << (threadIdx.x & 16));
+        t.q = t.tid >> CF_COL_TW_LOG2;
+        t.lane = t.tid & (CF_COL_TW - 1);
+#if CF_COL_TW == 16
+        t.gm = 0xffffu << (threadIdx.x & 16);
+#endif
         t.bar = 1 + tm;
         t.P = PL ? PL : p.P;
         t.hs = col_half_stride(t.P);
