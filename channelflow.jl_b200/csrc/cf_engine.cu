@@ -2275,21 +2275,18 @@ int cf_create_batch(const cf_config* cfgs, int n, cf_batch** out) {
 static int launch_class_stage(const cf_batch* b, const BatchClass& c, int j, cudaStream_t s, int which = 15) {
     const cf_engine* r = b->inst[c.members[0]];
     const unsigned m = (unsigned)c.members.size();
-    if (which & 1) {
-        const int tkz = class_tkz(b, c);
-        const unsigned gzx = (unsigned)((r->Nxh + tkz - 1) / tkz);
-        fft_batch_kernel(KF_ZINV, r->Nzp)<<<dim3(gzx, r->Ny, 6 * m), 256, class_zsmem(b, c), s>>>(c.d_fft);
-    }
+    // z kernels: groups of tkz consecutive (y, kx) pairs
+    const int tkz = class_tkz(b, c);
+    const unsigned gzx = (unsigned)(((long)r->Ny * r->Nxh + tkz - 1) / tkz);
+    if (which & 1)
+        fft_batch_kernel(KF_ZINV, r->Nzp)<<<dim3(gzx, 1, 6 * m), 256, class_zsmem(b, c), s>>>(c.d_fft);
     if (which & 2) {
         const int rows = xpass_rows(c.xkind);
         fft_batch_kernel(c.xkind, r->Nxp)<<<dim3((r->Nzp + rows - 1) / rows, r->Ny, m), 256, class_xsmem(b, c), s>>>(
             c.d_fft);
     }
-    if (which & 4) {
-        const int tkz = class_tkz(b, c);
-        const unsigned gzx = (unsigned)((r->Nxh + tkz - 1) / tkz);
-        fft_batch_kernel(KF_ZFWD, r->Nzp)<<<dim3(gzx, r->Ny, 3 * m), 256, class_zsmem(b, c), s>>>(c.d_fft);
-    }
+    if (which & 4)
+        fft_batch_kernel(KF_ZFWD, r->Nzp)<<<dim3(gzx, 1, 3 * m), 256, class_zsmem(b, c), s>>>(c.d_fft);
     if (!(which & 8)) {
         CU(cudaGetLastError());
         return CF_OK;

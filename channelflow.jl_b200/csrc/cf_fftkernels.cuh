@@ -771,21 +771,105 @@ template <int LX>
 __global__ void __launch_bounds__(256) k_xpass_div(FftParams p) {
     xpass_div_body<LX, zd>(p, blockIdx.x, blockIdx.y);
 }
-// grid z = 6 * instances
+// The z kernels of the ensembles' small grids, with the block's tkz
+// transforms taken from consecutive (y, kx) pairs (pair y Nxh + kx) rather
+// than from one plane: a plane of Nxh = 17, 25 or 33 columns would otherwise
+// leave most of its last column group empty.  The transforms and their
+// arithmetic are those of zinv_body / zfwd_body.  A thread's transform t =
+// threadIdx.x & (tkz - 1) is the same in every loop below (the loops step by
+// the block size, a multiple of tkz), so its pair is found once.
+// grid: (ceil(Ny Nxh / tkz), 1, nfields).
+CF_DEV void zflat_pair(const FftParams& p, int bx, int& y, int& k, bool& ok) {
+    const int pair = (bx << p.tks) + (threadIdx.x & ((1 << p.tks) - 1));
+    ok = pair < p.Ny * p.Nxh;
+    y = ok ? pair / p.Nxh : 0;
+    k = pair - y * p.Nxh;
+}
+template <int LZ>
+CF_DEV void zinv_flat_body(const FftParams& p, int bx, int f) {
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    zd* sm = reinterpret_cast<zd*>(fsm_raw);
+    const int tks = p.tks, tkz = 1 << tks, tm = tkz - 1;
+    const int Nz = p.Nz, Nzp = LZ ? LZ : p.Nzp, Nxh = p.Nxh, bs = p.bsz;
+    zd* bufB = sm + tkz * bs;
+    const bool dz = f >= 6;
+    int y, k;
+    bool ok;
+    zflat_pair(p, bx, y, k, ok);
+    const zd* src = nod_of<zd>(p, dz ? f - 6 : f) + (long)y * Nz * Nxh + k;
+    zd* dst = zp_of<zd>(p, f) + (long)y * Nzp * Nxh + k;
+    const int xnyq = (p.Nx % 2 == 0) ? p.Nx / 2 : -1, znyq = (Nz % 2 == 0) ? Nz / 2 : -1;
+    const bool live = ok && k != xnyq;
+    const int gap0 = (Nz >> 1) + 1, gap1 = Nzp - (Nz - gap0);
+    for (int e = threadIdx.x; e < ((gap1 - gap0) << tks); e += blockDim.x)
+        sm[(e & tm) * bs + fpos(gap0 + (e >> tks))] = czero<zd>();
+    const int ntot = Nz << tks;
+    for (int base = threadIdx.x; base < ntot; base += 8 * 256) {
+        zd v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = base + u * 256;
+            const int iz = e >> tks;
+            v[u] = (e < ntot && live && iz != znyq) ? src[(long)iz * Nxh] : czero<zd>();
+            if (dz) v[u] = cmuli(v[u], p.bz * (double)(iz <= (Nz >> 1) ? iz : iz - Nz));
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = base + u * 256;
+            if (e < ntot) sm[(e & tm) * bs + fpos(zpad_index(e >> tks, Nz, Nzp))] = v[u];
+        }
+    }
+    __syncthreads();
+    const zd* res = group_fft_L<true, LZ>(sm, bufB, tkz, bs, p.plZ, +1, threadIdx.x, blockDim.x, 0);
+    for (int e = threadIdx.x; e < (Nzp << tks); e += blockDim.x)
+        if (ok) dst[(long)(e >> tks) * Nxh] = res[(e & tm) * bs + fpos(e >> tks)];
+}
+template <int LZ>
+CF_DEV void zfwd_flat_body(const FftParams& p, int bx, int f) {
+    extern __shared__ __align__(128) unsigned char fsm_raw[];
+    zd* sm = reinterpret_cast<zd*>(fsm_raw);
+    const int tks = p.tks, tkz = 1 << tks, tm = tkz - 1;
+    const int Nz = p.Nz, Nzp = LZ ? LZ : p.Nzp, Nxh = p.Nxh, bs = p.bsz;
+    zd* bufB = sm + tkz * bs;
+    int y, k;
+    bool ok;
+    zflat_pair(p, bx, y, k, ok);
+    const zd* src = zp_of<zd>(p, f) + (long)y * Nzp * Nxh + k;
+    zd* dst = nod_of<zd>(p, f) + (long)y * Nz * Nxh + k;
+    const int ntot = Nzp << tks;
+    for (int base = threadIdx.x; base < ntot; base += 8 * 256) {
+        zd v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = base + u * 256;
+            v[u] = (e < ntot && ok) ? src[(long)(e >> tks) * Nxh] : czero<zd>();
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = base + u * 256;
+            if (e < ntot) sm[(e & tm) * bs + fpos(e >> tks)] = v[u];
+        }
+    }
+    __syncthreads();
+    const zd* res = group_fft_L<true, LZ>(sm, bufB, tkz, bs, p.plZ, -1, threadIdx.x, blockDim.x, 0);
+    for (int e = threadIdx.x; e < (Nz << tks); e += blockDim.x)
+        if (ok) dst[(long)(e >> tks) * Nxh] = res[(e & tm) * bs + fpos(zpad_index(e >> tks, Nz, Nzp))];
+}
+// grid (ceil(Ny Nxh / tkz), 1, 6 * instances)
 template <int LZ>
 __global__ void __launch_bounds__(256) k_zinv_batch(const FftParams* __restrict__ pl) {
     __shared__ FftParams ps;
     const int inst = blockIdx.z / 6;
     stage_params(&ps, pl + inst);
-    zinv_body<LZ, zd>(ps, blockIdx.x, blockIdx.y, blockIdx.z - 6 * inst);
+    zinv_flat_body<LZ>(ps, blockIdx.x, blockIdx.z - 6 * inst);
 }
-// grid z = 3 * instances
+// grid (ceil(Ny Nxh / tkz), 1, 3 * instances)
 template <int LZ>
 __global__ void __launch_bounds__(256) k_zfwd_batch(const FftParams* __restrict__ pl) {
     __shared__ FftParams ps;
     const int inst = blockIdx.z / 3;
     stage_params(&ps, pl + inst);
-    zfwd_body<LZ, zd>(ps, blockIdx.x, blockIdx.y, blockIdx.z - 3 * inst);
+    zfwd_flat_body<LZ>(ps, blockIdx.x, blockIdx.z - 3 * inst);
 }
 // grid (ceil(Nzp/2), Ny, instances): two rows per block (the ensembles' grids
 // are small)
