@@ -173,10 +173,11 @@ int cf_batch_last_launch_count(cf_batch* b);
 /* the ensemble's CUDA stream (cudaStream_t) */
 void* cf_batch_stream(cf_batch* b);
 /* The launch schedule the ensemble's autotuner chose at cf_create_batch, as
- * text: per size class the column kernel's variant (columns per block,
- * register bound), its schedule (one block per column block of every
- * instance, or a persistent grid claiming the items in order) and the timings
- * of every candidate.  Writes at most cap - 1 characters and a NUL; returns
+ * text: per size class the z kernels' transforms per block, the x-pass rows
+ * per block, the column kernel's variant (columns per block, register bound)
+ * and its schedule (one block per column block of every instance, or a
+ * persistent grid claiming the items in order), with the timings of every
+ * candidate.  Writes at most cap - 1 characters and a NUL; returns
  * the number written. */
 int cf_batch_schedule(cf_batch* b, char* buf, int cap);
 
