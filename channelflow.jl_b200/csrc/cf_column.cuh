@@ -247,9 +247,9 @@ CF_DEV void col_diff(const zd* a, zd* b, const Team& t) {
 
 // The three elimination factor rows of a column (alpha, invden, W: src,
 // src + Ny, src + 2 Ny; Ny doubles each, natural order) into shared memory in
-// the parity layout: alpha and invden at fa and fa + 2 hs, W at fw.  Warp q
+// the parity layout: alpha and invden at fa and fa + 2 hs, W at fw.  Group q
 // copies its parity; all loads of a lane are issued before its first store
-// (one memory round trip for P <= 318).  Only warp q reads them afterwards,
+// (one memory round trip for P <= 318).  Only group q reads them afterwards,
 // so a warp barrier suffices.
 CF_DEV void col_stage_factors(double* fa, double* fw, const double* __restrict__ src, const Team& t) {
     const int P = t.P, Ny = P + 1, hs = t.hs, q = t.q;
@@ -508,7 +508,7 @@ CF_DEV void col_helm(zd* x, zd* scr, const double* alpha, const double* invden, 
 //   X_{2m} = Z_m + Z_{P-m},  X_1 = x_0 - x_P + 2 sum_{n=1}^{P-1} x_n cos(pi n/P),
 //   X_{2m+1} = X_{2m-1} + i (Z_m - Z_{P-m}).
 // cs[n] = (cos(pi n/P), sin(pi n/P)), n = 0..P.  P must be even.  After the
-// FFT, warp 0 writes the even outputs and warp 1 scans the odd ones.
+// FFT, group 0 writes the even outputs and group 1 scans the odd ones.
 // MODE 1 (forward transform of nodal values, ffts.jl:65-82 with
 // normalize_forward! :254-269): every output times `scale`, X_0 and X_P also
 // halved.  MODE 2 (inverse, icheb with doubled endpoints and the 1/2 of
@@ -776,7 +776,7 @@ CF_DEV void col_redft00_pair(zd* xa, zd* xb, zd* z, int bs, const zd* __restrict
 }
 
 // Mean over y (meanmode.jl:13-19): a0 + sum_{even n >= 2} a_n / (1 - n^2),
-// returned to both warps.
+// returned to both groups.
 CF_DEV zd col_bulkmean(const zd* a, const Team& t) {
     zd s = zzero();
     if (t.q == 0) {
@@ -790,7 +790,7 @@ CF_DEV zd col_bulkmean(const zd* a, const Team& t) {
     team_xchg(t, s, m0, m1);
     return m0;
 }
-// a'(+1) = sum n^2 a_n ; a'(-1) = sum (-1)^(n+1) n^2 a_n, returned to both warps
+// a'(+1) = sum n^2 a_n ; a'(-1) = sum (-1)^(n+1) n^2 a_n, returned to both groups
 CF_DEV void col_wallderiv(const zd* a, const Team& t, zd& right, zd& left) {
     const int q = t.q, nq = pcount(q, t.P);
     const zd* ah = a + q * t.hs;

@@ -1101,7 +1101,7 @@ __global__ void __launch_bounds__(NCOL * CF_TEAM, (col_minblocks<NCOL, PL>())) k
 // with M_mn = (mom(m+n) + mom(|m-n|))/2, mom(j) = 1/(1-j^2) for even j, 0 for
 // odd j (the Chebyshev inner product on [-1, 1] divided by 2), weighted 1 for
 // kx = 0 and 2 otherwise; Nyquist columns are skipped.  M couples degrees of
-// equal parity only, so warp q sums the parity-q part, and only the even
+// equal parity only, so parity group q sums the parity-q part, and only the even
 // moments occur (table mom[h] = mom(2h), h = 0..P).  Regions: 0-2 u, v, w;
 // 3-5 omega; 6 the moment table (block); 7 D v.
 CF_DEV double diag_form(const zd* a, const double* mom, const Team& t) {
