@@ -74,13 +74,15 @@ CF_DEV T* sel3(T* a, T* b, T* c, int i) {
 }
 
 // Blocks per SM the column kernels are compiled for (bounds their registers):
-// at P >= 256 shared memory allows 6 columns per SM, so 168 registers; the
+// at P = 256 shared memory allows 6 columns per SM, so 168 registers; at P =
+// 384 it allows 4, so the full 255 (at 168 the paired transforms spilled); the
 // smaller sizes are held to 128 registers (8 or more columns per SM).  One-warp
 // teams: 16 columns per SM at P <= 64 (128 registers), 12 for the longer ones
 // (170 registers).
 template <int NCOL, int PL>
 constexpr int col_minblocks() {
     if constexpr (CF_TEAM == 32) return (PL <= 64 ? 16 : 12) / NCOL;  // one-warp teams: 16 or 12 columns
+    if constexpr (PL >= 384) return 4 / NCOL;
     return (PL == 0 || PL >= 256) ? 6 / NCOL : 8 / NCOL;
 }
 
